@@ -1,0 +1,195 @@
+/* tptfem.h -- C ABI of the B200 (sm_100a) finite-element hot path.
+ *
+ * Drop-in boundary for tpt-fem's assemble -> CSR -> SPD-solve path.  The
+ * reference is a Rust workspace with no FFI of its own; each entry point below
+ * names the Rust function it replaces (path:line inside the tpt-fem project),
+ * so a Rust crate can bind it 1:1 (see INTEGRATION.md for the binding stub).
+ *
+ * Conventions
+ *  - Every function returns tptfem_status; on failure the context keeps a
+ *    message readable with tptfem_last_error().
+ *  - Pointers named `*_host` or documented as host arrays are plain host
+ *    memory owned by the caller; the library copies what it needs.
+ *  - Index arrays at the ABI are int64 (the reference's usize); the device
+ *    uses int32 and every conversion is range-checked (TPTFEM_ERR_INVALID_ARG
+ *    or TPTFEM_ERR_CREATION before any kernel launch).
+ *  - A context owns one CUDA stream on one device.  Calls on one context are
+ *    serialised by the caller; distinct contexts may be used from distinct
+ *    threads.  Handles (meshes, matrices, systems) belong to the context that
+ *    created them.
+ *  - The library never falls back to the CPU: without a usable CUDA device,
+ *    tptfem_create() fails with TPTFEM_ERR_DEVICE.
+ */
+#ifndef TPTFEM_H
+#define TPTFEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  CREATION/SYMBOLIC/NUMERIC mirror SparseError
+ * (crates/tpt-fem-sparse/src/lib.rs:67-74); MODEL_DIM_MISMATCH mirrors
+ * ElasticityError::ModelDimMismatch (crates/tpt-fem-elasticity/src/lib.rs:28-35). */
+typedef enum tptfem_status {
+  TPTFEM_OK = 0,
+  TPTFEM_ERR_CREATION = 1,
+  TPTFEM_ERR_SYMBOLIC = 2,
+  TPTFEM_ERR_NUMERIC = 3,
+  TPTFEM_ERR_MODEL_DIM_MISMATCH = 4,
+  TPTFEM_ERR_NOT_CONVERGED = 5,
+  TPTFEM_ERR_BREAKDOWN = 6,
+  TPTFEM_ERR_DEVICE = 7,
+  TPTFEM_ERR_TIMEOUT = 8,
+  TPTFEM_ERR_INVALID_ARG = 9,
+  TPTFEM_ERR_OUT_OF_MEMORY = 10
+} tptfem_status;
+
+/* Cell types (crates/tpt-fem-mesh CellType; linear cells on the device path). */
+enum { TPTFEM_CELL_QUAD4 = 3, TPTFEM_CELL_TET4 = 4 };
+
+/* ElasticModel (crates/tpt-fem-elasticity/src/lib.rs:56-66). */
+enum {
+  TPTFEM_MODEL_BAR_AXIAL = 0,
+  TPTFEM_MODEL_PLANE_STRESS = 1,
+  TPTFEM_MODEL_PLANE_STRAIN = 2,
+  TPTFEM_MODEL_CONTINUUM_3D = 3
+};
+
+/* Solvers for the reduced SPD system. */
+enum {
+  /* FP64 Jacobi-preconditioned CG: the plain method and the fallback. */
+  TPTFEM_SOLVER_JACOBI_PCG = 0,
+  /* FP32 Jacobi-PCG inner solves inside FP64 iterative refinement. */
+  TPTFEM_SOLVER_MP_PCG = 1
+};
+
+typedef struct tptfem_context tptfem_context;
+typedef struct tptfem_mesh tptfem_mesh;
+typedef struct tptfem_matrix tptfem_matrix;
+typedef struct tptfem_system tptfem_system;
+
+typedef struct tptfem_solver_opts {
+  int32_t solver;        /* TPTFEM_SOLVER_* */
+  int32_t max_outer;     /* MP: refinement steps cap (0 -> 50) */
+  double rel_tol;        /* stop at ||b - A x||_2 / ||b||_2 <= rel_tol, FP64 (0 -> 1e-10) */
+  double inner_rel_tol;  /* MP: inner FP32 reduction per refinement step (0 -> 1e-4) */
+  int64_t max_iter;      /* cap on total PCG iterations (0 -> 100000) */
+  int32_t batch;         /* PCG iterations per CUDA-graph launch (0 -> auto) */
+  int32_t reserved;
+} tptfem_solver_opts;
+
+typedef struct tptfem_solve_stats {
+  int64_t iterations;    /* total PCG iterations (inner iterations for MP) */
+  int32_t outer_steps;   /* refinement steps (1 for FP64 Jacobi-PCG) */
+  int32_t solver_used;   /* TPTFEM_SOLVER_* actually run (after any fallback) */
+  double rel_residual;   /* final TRUE residual ||b - A x||_2/||b||_2 in FP64 */
+  double setup_ms;       /* preconditioner set-up, device time */
+  double solve_ms;       /* iterations + residual checks, device time */
+  int32_t fell_back;     /* 1 if the requested method fell back to FP64 Jacobi-PCG */
+  int32_t reserved;
+} tptfem_solve_stats;
+
+/* ---- context ---------------------------------------------------------------- */
+const char* tptfem_version(void);
+tptfem_status tptfem_create(int device, tptfem_context** out);
+void tptfem_destroy(tptfem_context* ctx);
+/* Copies the last error message (NUL-terminated, truncated to len); returns its full length. */
+size_t tptfem_last_error(const tptfem_context* ctx, char* buf, size_t len);
+tptfem_status tptfem_synchronize(tptfem_context* ctx);
+
+/* ---- meshes (crates/tpt-fem-mesh/src/lib.rs:115-148) -------------------------- */
+/* Upload coords (n_nodes x coord_dim, row-major) and conn (n_elems x 4). */
+tptfem_status tptfem_mesh_upload(tptfem_context* ctx, int cell_type, int coord_dim, const double* coords,
+                                 int64_t n_nodes, const int64_t* conn, int64_t n_elems, tptfem_mesh** out);
+/* box_mesh(min, max, n) generated on the device (crates/tpt-fem-mesh-gen/src/lib.rs:422-495). */
+tptfem_status tptfem_mesh_box(tptfem_context* ctx, const double min[3], const double max[3], const int64_t n[3],
+                              tptfem_mesh** out);
+tptfem_status tptfem_mesh_sizes(const tptfem_mesh* mesh, int64_t* n_nodes, int64_t* n_elems, int* cell_type,
+                                int* coord_dim);
+tptfem_status tptfem_mesh_download(tptfem_context* ctx, const tptfem_mesh* mesh, double* coords, int64_t* conn);
+void tptfem_mesh_free(tptfem_mesh* mesh);
+
+/* ---- assembly ------------------------------------------------------------------
+ * Global stiffness in CSR, equal to Coo::to_csr(assemble(...)) of the reference:
+ * the pattern holds (row, col) iff at least one element contributed a non-zero
+ * value (zero-skip of crates/tpt-fem-assembly/src/lib.rs:469-472), and each value
+ * is the sum of element contributions in ascending element order
+ * (crates/tpt-fem-sparse/src/lib.rs:144-163), computed in the reference's FP64
+ * operation order without FMA contraction.
+ *
+ * `coef` is per element (per_element = 1, n_elems values) or one constant. */
+
+/* assemble(mesh, 1, poisson_element_matrix) -- crates/tpt-fem-thermal/src/lib.rs:132-160,
+ * crates/tpt-fem-assembly/src/lib.rs:458-480. */
+tptfem_status tptfem_assemble_poisson(tptfem_context* ctx, tptfem_mesh* mesh, const double* conductivity,
+                                      int per_element, int quad_order, tptfem_matrix** out);
+/* try_assemble(mesh, dim, elasticity_element_matrix) -- crates/tpt-fem-elasticity/src/lib.rs:262-309,
+ * crates/tpt-fem-assembly/src/lib.rs:428-450. */
+tptfem_status tptfem_assemble_elasticity(tptfem_context* ctx, tptfem_mesh* mesh, int model, const double* young,
+                                         int per_element, double poisson, int quad_order, tptfem_matrix** out);
+/* Recompute the values of `mat` for new coefficients, reusing its pattern.  If
+ * the new coefficients change which entries are non-zero, the pattern is rebuilt
+ * (the result still equals a fresh assemble). */
+tptfem_status tptfem_reassemble(tptfem_context* ctx, tptfem_matrix* mat, const double* coef, int per_element);
+/* Csr::nrows / ncols / nnz (crates/tpt-fem-sparse/src/lib.rs:51-63, 122-143). */
+tptfem_status tptfem_matrix_sizes(const tptfem_matrix* mat, int64_t* nrows, int64_t* ncols, int64_t* nnz);
+tptfem_status tptfem_matrix_download(tptfem_context* ctx, const tptfem_matrix* mat, int64_t* row_ptrs,
+                                     int64_t* col_ind, double* values);
+void tptfem_matrix_free(tptfem_matrix* mat);
+/* Csr::matvec (crates/tpt-fem-sparse/src/lib.rs:195-205): y has max(nrows, xlen) entries. */
+tptfem_status tptfem_csr_matvec(tptfem_context* ctx, const tptfem_matrix* mat, const double* x, int64_t xlen,
+                                double* y);
+
+/* ---- loads (host rhs arrays, overwritten / accumulated as documented) ---------- */
+/* rhs[n_nodes] = Poisson load loop of solve_poisson (crates/tpt-fem-thermal/src/lib.rs:224-230)
+ * for a constant source. */
+tptfem_status tptfem_load_poisson_source(tptfem_context* ctx, tptfem_mesh* mesh, double source, int quad_order,
+                                         double* rhs);
+/* rhs[n_nodes*dim] = body-force loop of solve_elasticity (crates/tpt-fem-elasticity/src/lib.rs:371-379). */
+tptfem_status tptfem_load_body(tptfem_context* ctx, tptfem_mesh* mesh, const double* body, int quad_order,
+                               double* rhs);
+/* rhs += apply_neumann (crates/tpt-fem-assembly/src/lib.rs:591-667) with the scalar flux
+ * g = traction[c] on boundary faces whose outward unit normal n has sign*n[axis] > 0.5
+ * (0 elsewhere), applied to component c of each of the dofs_per_node components. */
+tptfem_status tptfem_apply_traction(tptfem_context* ctx, tptfem_mesh* mesh, int dofs_per_node, int axis,
+                                    double sign, const double* traction, double* rhs);
+
+/* ---- Dirichlet reduction and solve ----------------------------------------------- */
+/* reduce_system (crates/tpt-fem-assembly/src/lib.rs:504-535) into a device-resident system. */
+tptfem_status tptfem_reduce_system(tptfem_context* ctx, const tptfem_matrix* mat, const double* rhs, int64_t n,
+                                   const int64_t* bc_dof, const double* bc_val, int64_t nbc, tptfem_system** out);
+tptfem_status tptfem_system_sizes(const tptfem_system* sys, int64_t* n_free, int64_t* nnz);
+/* Reduced CSR, fred and the free map, for inspection. */
+tptfem_status tptfem_system_download(tptfem_context* ctx, const tptfem_system* sys, int64_t* row_ptrs,
+                                     int64_t* col_ind, double* values, double* fred, int64_t* free_dofs);
+/* Solve the reduced system on the device; the solution stays resident. */
+tptfem_status tptfem_system_solve(tptfem_context* ctx, tptfem_system* sys, const tptfem_solver_opts* opts,
+                                  tptfem_solve_stats* stats);
+/* Full-length solution as solve_with_dirichlet returns it (crates/tpt-fem-assembly/src/lib.rs:549-558). */
+tptfem_status tptfem_system_solution(tptfem_context* ctx, const tptfem_system* sys, double* u);
+void tptfem_system_free(tptfem_system* sys);
+
+/* solve_with_dirichlet (crates/tpt-fem-assembly/src/lib.rs:543-559): reduce, solve, scatter. */
+tptfem_status tptfem_solve_with_dirichlet(tptfem_context* ctx, const tptfem_matrix* mat, const double* rhs,
+                                          int64_t n, const int64_t* bc_dof, const double* bc_val, int64_t nbc,
+                                          const tptfem_solver_opts* opts, double* u, tptfem_solve_stats* stats);
+
+/* solve_poisson with a constant source and no Neumann/Robin term
+ * (crates/tpt-fem-thermal/src/lib.rs:206-240).  u has n_nodes entries. */
+tptfem_status tptfem_solve_poisson(tptfem_context* ctx, tptfem_mesh* mesh, double conductivity, int quad_order,
+                                   double source, const int64_t* bc_dof, const double* bc_val, int64_t nbc,
+                                   const tptfem_solver_opts* opts, double* u, tptfem_solve_stats* stats);
+/* solve_elasticity with a constant body force (crates/tpt-fem-elasticity/src/lib.rs:355-381).
+ * u has n_nodes*dim entries. */
+tptfem_status tptfem_solve_elasticity(tptfem_context* ctx, tptfem_mesh* mesh, int model, double young,
+                                      double poisson, int quad_order, const double* body, const int64_t* bc_dof,
+                                      const double* bc_val, int64_t nbc, const tptfem_solver_opts* opts, double* u,
+                                      tptfem_solve_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TPTFEM_H */

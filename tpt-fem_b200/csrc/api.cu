@@ -1,0 +1,499 @@
+// api.cu -- the extern "C" boundary declared in include/tptfem.h.
+//
+// Every entry point validates its arguments on the host before any launch,
+// converts int64 indices to the device's int32 with range checks, and maps
+// internal errors to tptfem_status plus a message kept in the context.
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "objects.hpp"
+
+using namespace tptfem;
+
+namespace {
+
+// Csr::matvec (crates/tpt-fem-sparse/src/lib.rs:195-205): one thread per row,
+// sequential s += v * x[c] with explicit round-to-nearest (no FMA), so the
+// result matches the reference bit for bit.
+__global__ void matvec_exact(int64_t nrows, const int* __restrict__ rp, const int* __restrict__ ci,
+                             const double* __restrict__ va, const double* __restrict__ x, double* __restrict__ y) {
+  int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrows) return;
+  double s = 0.0;
+  for (int k = rp[r]; k < rp[r + 1]; ++k) s = __dadd_rn(s, __dmul_rn(va[k], x[ci[k]]));
+  y[r] = s;
+}
+
+tptfem_status fail(tptfem_context* ctx, tptfem_status st, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return st;
+}
+
+void set_device(tptfem_context* ctx) { TPT_CUDA(cudaSetDevice(ctx->device)); }
+
+#define API_TRY try {
+#define API_CATCH(ctx)                                                         \
+  }                                                                            \
+  catch (const Error& e) {                                                     \
+    return fail((ctx), e.status, e.msg);                                       \
+  }                                                                            \
+  catch (const std::bad_alloc&) {                                              \
+    return fail((ctx), TPTFEM_ERR_OUT_OF_MEMORY, "host allocation failed");    \
+  }                                                                            \
+  catch (...) {                                                                \
+    return fail((ctx), TPTFEM_ERR_DEVICE, "unexpected internal error");        \
+  }                                                                            \
+  return TPTFEM_OK;
+
+tptfem_solver_opts default_opts(const tptfem_solver_opts* o) {
+  tptfem_solver_opts d{};
+  d.solver = TPTFEM_SOLVER_JACOBI_PCG;
+  d.rel_tol = 1e-10;
+  if (o) d = *o;
+  return d;
+}
+
+void check_coef(const double* coef, int64_t count, const char* what) {
+  TPT_REQUIRE(coef != nullptr, TPTFEM_ERR_INVALID_ARG, std::string(what) + " is NULL");
+  for (int64_t i = 0; i < count; ++i)
+    TPT_REQUIRE(std::isfinite(coef[i]), TPTFEM_ERR_INVALID_ARG, std::string(what) + " holds a non-finite value");
+}
+
+std::unique_ptr<MatrixData> new_matrix(tptfem_context* ctx, tptfem_mesh* mesh, int physics, int model,
+                                       const double* coef, int per_element, double nu, int quad_order) {
+  TPT_REQUIRE(mesh && mesh->d, TPTFEM_ERR_INVALID_ARG, "mesh is NULL");
+  MeshData& m = *mesh->d;
+  TPT_REQUIRE(m.ctx == ctx, TPTFEM_ERR_INVALID_ARG, "mesh belongs to another context");
+  if (m.cell == TPTFEM_CELL_QUAD4)
+    TPT_REQUIRE(quad_order >= 1 && quad_order <= 5, TPTFEM_ERR_INVALID_ARG, "quad_order must be in 1..=5");
+  const int64_t count = per_element ? m.n_elems : 1;
+  check_coef(coef, count, physics ? "young" : "conductivity");
+  TPT_REQUIRE(std::isfinite(nu), TPTFEM_ERR_INVALID_ARG, "poisson ratio is not finite");
+  auto M = std::make_unique<MatrixData>();
+  M->ctx = ctx;
+  M->mesh = mesh->d;
+  M->physics = physics;
+  M->model = model;
+  M->nu = nu;
+  M->quad_order = quad_order;
+  M->per_element = per_element ? 1 : 0;
+  M->coef.alloc(count, ctx->stream);
+  M->coef.upload(coef, count);
+  assemble_matrix(*M);
+  return M;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tptfem_version(void) { return "tptfem-b200 0.1.0 (sm_100a)"; }
+
+tptfem_status tptfem_create(int device, tptfem_context** out) {
+  if (!out) return TPTFEM_ERR_INVALID_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return TPTFEM_ERR_DEVICE;
+  if (device < 0 || device >= count) return TPTFEM_ERR_INVALID_ARG;
+  tptfem_context* ctx = new (std::nothrow) tptfem_context;
+  if (!ctx) return TPTFEM_ERR_OUT_OF_MEMORY;
+  ctx->device = device;
+  try {
+    TPT_CUDA(cudaSetDevice(device));
+    int major = 0;
+    TPT_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+    TPT_REQUIRE(major == 10, TPTFEM_ERR_DEVICE, "this build targets sm_100a (B200)");
+    TPT_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    for (auto& e : ctx->ev) TPT_CUDA(cudaEventCreate(&e));
+    TPT_CUDA(cudaMalloc(&ctx->d_flag, 64));
+    TPT_CUDA(cudaMallocHost(&ctx->h_pinned, 64));
+  } catch (const Error& e) {
+    tptfem_destroy(ctx);
+    return e.status;
+  }
+  *out = ctx;
+  return TPTFEM_OK;
+}
+
+void tptfem_destroy(tptfem_context* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& e : ctx->ev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->d_flag) cudaFree(ctx->d_flag);
+  if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+size_t tptfem_last_error(const tptfem_context* ctx, char* buf, size_t len) {
+  if (!ctx) return 0;
+  const std::string& m = ctx->err;
+  if (buf && len) {
+    size_t n = m.size() < len - 1 ? m.size() : len - 1;
+    std::memcpy(buf, m.data(), n);
+    buf[n] = 0;
+  }
+  return m.size();
+}
+
+tptfem_status tptfem_synchronize(tptfem_context* ctx) {
+  if (!ctx) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  API_CATCH(ctx)
+}
+
+// ---- meshes -------------------------------------------------------------------
+
+tptfem_status tptfem_mesh_upload(tptfem_context* ctx, int cell_type, int coord_dim, const double* coords,
+                                 int64_t n_nodes, const int64_t* conn, int64_t n_elems, tptfem_mesh** out) {
+  if (!ctx || !out) return TPTFEM_ERR_INVALID_ARG;
+  *out = nullptr;
+  API_TRY
+  set_device(ctx);
+  TPT_REQUIRE(cell_type == TPTFEM_CELL_TET4 || cell_type == TPTFEM_CELL_QUAD4, TPTFEM_ERR_INVALID_ARG,
+              "cell_type must be TPTFEM_CELL_TET4 or TPTFEM_CELL_QUAD4");
+  TPT_REQUIRE(cell_type == TPTFEM_CELL_TET4 ? coord_dim == 3 : (coord_dim == 2 || coord_dim == 3),
+              TPTFEM_ERR_INVALID_ARG, "coord_dim must be 3 for Tet4 and 2 or 3 for Quad4");
+  TPT_REQUIRE(coords && conn, TPTFEM_ERR_INVALID_ARG, "coords/conn is NULL");
+  TPT_REQUIRE(n_nodes > 0 && n_nodes < (1LL << 31), TPTFEM_ERR_INVALID_ARG, "n_nodes out of range");
+  TPT_REQUIRE(n_elems > 0 && n_elems < (1LL << 29), TPTFEM_ERR_INVALID_ARG, "n_elems out of range");
+  for (int64_t i = 0; i < n_nodes * coord_dim; ++i)
+    TPT_REQUIRE(std::isfinite(coords[i]), TPTFEM_ERR_INVALID_ARG, "coords hold a non-finite value");
+  std::vector<int> c32((size_t)n_elems * 4);
+  for (int64_t i = 0; i < n_elems * 4; ++i) {
+    TPT_REQUIRE(conn[i] >= 0 && conn[i] < n_nodes, TPTFEM_ERR_INVALID_ARG, "connectivity entry out of range");
+    c32[i] = (int)conn[i];
+  }
+  auto m = std::make_shared<MeshData>();
+  m->ctx = ctx;
+  m->cell = cell_type;
+  m->cdim = coord_dim;
+  m->npe = 4;
+  m->n_nodes = n_nodes;
+  m->n_elems = n_elems;
+  m->coords.alloc(n_nodes * coord_dim, ctx->stream);
+  m->coords.upload(coords, n_nodes * coord_dim);
+  m->conn.alloc(n_elems * 4, ctx->stream);
+  m->conn.upload(c32.data(), c32.size());
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  *out = new tptfem_mesh{m};
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_mesh_box(tptfem_context* ctx, const double min[3], const double max[3], const int64_t n[3],
+                              tptfem_mesh** out) {
+  if (!ctx || !out || !min || !max || !n) return TPTFEM_ERR_INVALID_ARG;
+  *out = nullptr;
+  API_TRY
+  set_device(ctx);
+  auto m = std::make_shared<MeshData>();
+  m->ctx = ctx;
+  mesh_box(*m, min, max, n);
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  *out = new tptfem_mesh{m};
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_mesh_sizes(const tptfem_mesh* mesh, int64_t* n_nodes, int64_t* n_elems, int* cell_type,
+                                int* coord_dim) {
+  if (!mesh || !mesh->d) return TPTFEM_ERR_INVALID_ARG;
+  if (n_nodes) *n_nodes = mesh->d->n_nodes;
+  if (n_elems) *n_elems = mesh->d->n_elems;
+  if (cell_type) *cell_type = mesh->d->cell;
+  if (coord_dim) *coord_dim = mesh->d->cdim;
+  return TPTFEM_OK;
+}
+
+tptfem_status tptfem_mesh_download(tptfem_context* ctx, const tptfem_mesh* mesh, double* coords, int64_t* conn) {
+  if (!ctx || !mesh || !mesh->d) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  const MeshData& m = *mesh->d;
+  if (coords) m.coords.download(coords, m.n_nodes * m.cdim);
+  std::vector<int> c32;
+  if (conn) {
+    c32.resize(m.n_elems * 4);
+    m.conn.download(c32.data(), c32.size());
+  }
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (size_t i = 0; i < c32.size(); ++i) conn[i] = c32[i];
+  API_CATCH(ctx)
+}
+
+void tptfem_mesh_free(tptfem_mesh* mesh) { delete mesh; }
+
+// ---- assembly -----------------------------------------------------------------
+
+tptfem_status tptfem_assemble_poisson(tptfem_context* ctx, tptfem_mesh* mesh, const double* conductivity,
+                                      int per_element, int quad_order, tptfem_matrix** out) {
+  if (!ctx || !out) return TPTFEM_ERR_INVALID_ARG;
+  *out = nullptr;
+  API_TRY
+  set_device(ctx);
+  auto M = new_matrix(ctx, mesh, 0, 0, conductivity, per_element, 0.0, quad_order);
+  *out = new tptfem_matrix{std::move(M)};
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_assemble_elasticity(tptfem_context* ctx, tptfem_mesh* mesh, int model, const double* young,
+                                         int per_element, double poisson, int quad_order, tptfem_matrix** out) {
+  if (!ctx || !out) return TPTFEM_ERR_INVALID_ARG;
+  *out = nullptr;
+  API_TRY
+  set_device(ctx);
+  TPT_REQUIRE(model >= TPTFEM_MODEL_BAR_AXIAL && model <= TPTFEM_MODEL_CONTINUUM_3D, TPTFEM_ERR_INVALID_ARG,
+              "unknown elasticity model");
+  auto M = new_matrix(ctx, mesh, 1, model, young, per_element, poisson, quad_order);
+  *out = new tptfem_matrix{std::move(M)};
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_reassemble(tptfem_context* ctx, tptfem_matrix* mat, const double* coef, int per_element) {
+  if (!ctx || !mat || !mat->d) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  MatrixData& M = *mat->d;
+  const int64_t count = per_element ? M.mesh->n_elems : 1;
+  check_coef(coef, count, "coefficient");
+  if (M.coef.n != (size_t)count) M.coef.alloc(count, ctx->stream);
+  M.coef.upload(coef, count);
+  M.per_element = per_element ? 1 : 0;
+  if (!reassemble_values(M)) assemble_matrix(M);  // pattern changed: rebuild it
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_matrix_sizes(const tptfem_matrix* mat, int64_t* nrows, int64_t* ncols, int64_t* nnz) {
+  if (!mat || !mat->d) return TPTFEM_ERR_INVALID_ARG;
+  if (nrows) *nrows = mat->d->ref_nrows;
+  if (ncols) *ncols = mat->d->ref_ncols;
+  if (nnz) *nnz = mat->d->nnz;
+  return TPTFEM_OK;
+}
+
+tptfem_status tptfem_matrix_download(tptfem_context* ctx, const tptfem_matrix* mat, int64_t* row_ptrs,
+                                     int64_t* col_ind, double* values) {
+  if (!ctx || !mat || !mat->d) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  const MatrixData& M = *mat->d;
+  std::vector<int> rp(M.ref_nrows + 1), ci(M.nnz);
+  M.row_ptr.download(rp.data(), rp.size());
+  M.col.download(ci.data(), ci.size());
+  if (values) M.val.download(values, M.nnz);
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (row_ptrs)
+    for (size_t i = 0; i < rp.size(); ++i) row_ptrs[i] = rp[i];
+  if (col_ind)
+    for (size_t i = 0; i < ci.size(); ++i) col_ind[i] = ci[i];
+  API_CATCH(ctx)
+}
+
+void tptfem_matrix_free(tptfem_matrix* mat) { delete mat; }
+
+tptfem_status tptfem_csr_matvec(tptfem_context* ctx, const tptfem_matrix* mat, const double* x, int64_t xlen,
+                                double* y) {
+  if (!ctx || !mat || !mat->d || !x || !y) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  const MatrixData& M = *mat->d;
+  TPT_REQUIRE(xlen >= M.ref_ncols, TPTFEM_ERR_INVALID_ARG, "x is shorter than the matrix's column count");
+  cudaStream_t s = ctx->stream;
+  const int64_t ylen = std::max<int64_t>(M.ref_nrows, xlen);
+  DevBuf<double> dx, dy;
+  dx.alloc(std::max<int64_t>(xlen, M.nrows), s);
+  dx.zero();
+  dx.upload(x, xlen);
+  dy.alloc(std::max<int64_t>(ylen, M.nrows), s);
+  dy.zero();
+  matvec_exact<<<ceil_div(M.ref_nrows, 256), 256, 0, s>>>(M.ref_nrows, M.row_ptr.p, M.col.p, M.val.p, dx.p, dy.p);
+  TPT_CHECK_LAUNCH();
+  dy.download(y, ylen);
+  TPT_CUDA(cudaStreamSynchronize(s));
+  API_CATCH(ctx)
+}
+
+// ---- loads ----------------------------------------------------------------------
+
+tptfem_status tptfem_load_poisson_source(tptfem_context* ctx, tptfem_mesh* mesh, double source, int quad_order,
+                                         double* rhs) {
+  if (!ctx || !mesh || !mesh->d || !rhs) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  MeshData& m = *mesh->d;
+  if (m.cell == TPTFEM_CELL_QUAD4)
+    TPT_REQUIRE(quad_order >= 1 && quad_order <= 5, TPTFEM_ERR_INVALID_ARG, "quad_order must be in 1..=5");
+  TPT_REQUIRE(std::isfinite(source), TPTFEM_ERR_INVALID_ARG, "source is not finite");
+  DevBuf<double> d;
+  d.alloc(m.n_nodes, ctx->stream);
+  load_poisson_source(m, source, quad_order, d.p);
+  d.download(rhs, m.n_nodes);
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_load_body(tptfem_context* ctx, tptfem_mesh* mesh, const double* body, int quad_order,
+                               double* rhs) {
+  if (!ctx || !mesh || !mesh->d || !rhs || !body) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  MeshData& m = *mesh->d;
+  if (m.cell == TPTFEM_CELL_QUAD4)
+    TPT_REQUIRE(quad_order >= 1 && quad_order <= 5, TPTFEM_ERR_INVALID_ARG, "quad_order must be in 1..=5");
+  const int dim = m.cell == TPTFEM_CELL_TET4 ? 3 : 2;
+  check_coef(body, dim, "body force");
+  DevBuf<double> d;
+  d.alloc(m.n_nodes * dim, ctx->stream);
+  load_body(m, body, quad_order, d.p);
+  d.download(rhs, m.n_nodes * dim);
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_apply_traction(tptfem_context* ctx, tptfem_mesh* mesh, int dofs_per_node, int axis,
+                                    double sign, const double* traction, double* rhs) {
+  if (!ctx || !mesh || !mesh->d || !rhs || !traction) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  MeshData& m = *mesh->d;
+  TPT_REQUIRE(dofs_per_node >= 1 && dofs_per_node <= 3, TPTFEM_ERR_INVALID_ARG, "dofs_per_node must be 1..3");
+  check_coef(traction, dofs_per_node, "traction");
+  const int64_t n = m.n_nodes * dofs_per_node;
+  DevBuf<double> d;
+  d.alloc(n, ctx->stream);
+  d.upload(rhs, n);
+  apply_traction(m, dofs_per_node, axis, sign, traction, d.p);
+  d.download(rhs, n);
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  API_CATCH(ctx)
+}
+
+// ---- reduction and solve ------------------------------------------------------------
+
+tptfem_status tptfem_reduce_system(tptfem_context* ctx, const tptfem_matrix* mat, const double* rhs, int64_t n,
+                                   const int64_t* bc_dof, const double* bc_val, int64_t nbc, tptfem_system** out) {
+  if (!ctx || !mat || !mat->d || !rhs || !out || (nbc > 0 && (!bc_dof || !bc_val))) return TPTFEM_ERR_INVALID_ARG;
+  *out = nullptr;
+  API_TRY
+  set_device(ctx);
+  const MatrixData& M = *mat->d;
+  TPT_REQUIRE(n == M.nrows, TPTFEM_ERR_INVALID_ARG, "rhs length does not match the matrix dimension");
+  DevBuf<double> d;
+  d.alloc(n, ctx->stream);
+  d.upload(rhs, n);
+  auto S = reduce_system(ctx, M, d.p, bc_dof, bc_val, nbc);
+  *out = new tptfem_system{std::move(S)};
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_system_sizes(const tptfem_system* sys, int64_t* n_free, int64_t* nnz) {
+  if (!sys || !sys->d) return TPTFEM_ERR_INVALID_ARG;
+  if (n_free) *n_free = sys->d->n_free;
+  if (nnz) *nnz = sys->d->nnz;
+  return TPTFEM_OK;
+}
+
+tptfem_status tptfem_system_download(tptfem_context* ctx, const tptfem_system* sys, int64_t* row_ptrs,
+                                     int64_t* col_ind, double* values, double* fred, int64_t* free_dofs) {
+  if (!ctx || !sys || !sys->d) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  const SystemData& S = *sys->d;
+  std::vector<int> rp(S.n_free + 1), ci(S.nnz), fm(S.n_free);
+  S.row_ptr.download(rp.data(), rp.size());
+  S.col.download(ci.data(), ci.size());
+  S.free_map.download(fm.data(), fm.size());
+  if (values) S.val.download(values, S.nnz);
+  if (fred) S.fred.download(fred, S.n_free);
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (row_ptrs)
+    for (size_t i = 0; i < rp.size(); ++i) row_ptrs[i] = rp[i];
+  if (col_ind)
+    for (size_t i = 0; i < ci.size(); ++i) col_ind[i] = ci[i];
+  if (free_dofs)
+    for (size_t i = 0; i < fm.size(); ++i) free_dofs[i] = fm[i];
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_system_solve(tptfem_context* ctx, tptfem_system* sys, const tptfem_solver_opts* opts,
+                                  tptfem_solve_stats* stats) {
+  if (!ctx || !sys || !sys->d) return TPTFEM_ERR_INVALID_ARG;
+  tptfem_solve_stats st{};
+  tptfem_status rc = TPTFEM_OK;
+  try {
+    set_device(ctx);
+    system_solve(*sys->d, default_opts(opts), st);
+  } catch (const Error& e) {
+    rc = fail(ctx, e.status, e.msg);
+  } catch (...) {
+    rc = fail(ctx, TPTFEM_ERR_DEVICE, "unexpected internal error");
+  }
+  if (stats) *stats = st;
+  return rc;
+}
+
+tptfem_status tptfem_system_solution(tptfem_context* ctx, const tptfem_system* sys, double* u) {
+  if (!ctx || !sys || !sys->d || !u) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  const SystemData& S = *sys->d;
+  DevBuf<double> d;
+  d.alloc(S.n, ctx->stream);
+  system_solution(S, d.p);
+  d.download(u, S.n);
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  API_CATCH(ctx)
+}
+
+void tptfem_system_free(tptfem_system* sys) { delete sys; }
+
+tptfem_status tptfem_solve_with_dirichlet(tptfem_context* ctx, const tptfem_matrix* mat, const double* rhs,
+                                          int64_t n, const int64_t* bc_dof, const double* bc_val, int64_t nbc,
+                                          const tptfem_solver_opts* opts, double* u, tptfem_solve_stats* stats) {
+  if (!u) return TPTFEM_ERR_INVALID_ARG;
+  tptfem_system* sys = nullptr;
+  tptfem_status rc = tptfem_reduce_system(ctx, mat, rhs, n, bc_dof, bc_val, nbc, &sys);
+  if (rc != TPTFEM_OK) return rc;
+  rc = tptfem_system_solve(ctx, sys, opts, stats);
+  if (rc == TPTFEM_OK) rc = tptfem_system_solution(ctx, sys, u);
+  tptfem_system_free(sys);
+  return rc;
+}
+
+tptfem_status tptfem_solve_poisson(tptfem_context* ctx, tptfem_mesh* mesh, double conductivity, int quad_order,
+                                   double source, const int64_t* bc_dof, const double* bc_val, int64_t nbc,
+                                   const tptfem_solver_opts* opts, double* u, tptfem_solve_stats* stats) {
+  if (!ctx || !mesh || !mesh->d || !u) return TPTFEM_ERR_INVALID_ARG;
+  tptfem_matrix* K = nullptr;
+  tptfem_status rc = tptfem_assemble_poisson(ctx, mesh, &conductivity, 0, quad_order, &K);
+  if (rc != TPTFEM_OK) return rc;
+  std::vector<double> rhs(mesh->d->n_nodes);
+  rc = tptfem_load_poisson_source(ctx, mesh, source, quad_order, rhs.data());
+  if (rc == TPTFEM_OK)
+    rc = tptfem_solve_with_dirichlet(ctx, K, rhs.data(), (int64_t)rhs.size(), bc_dof, bc_val, nbc, opts, u, stats);
+  tptfem_matrix_free(K);
+  return rc;
+}
+
+tptfem_status tptfem_solve_elasticity(tptfem_context* ctx, tptfem_mesh* mesh, int model, double young,
+                                      double poisson, int quad_order, const double* body, const int64_t* bc_dof,
+                                      const double* bc_val, int64_t nbc, const tptfem_solver_opts* opts, double* u,
+                                      tptfem_solve_stats* stats) {
+  if (!ctx || !mesh || !mesh->d || !u || !body) return TPTFEM_ERR_INVALID_ARG;
+  tptfem_matrix* K = nullptr;
+  tptfem_status rc = tptfem_assemble_elasticity(ctx, mesh, model, &young, 0, poisson, quad_order, &K);
+  if (rc != TPTFEM_OK) return rc;
+  const int dim = mesh->d->cell == TPTFEM_CELL_TET4 ? 3 : 2;
+  std::vector<double> rhs(mesh->d->n_nodes * dim);
+  rc = tptfem_load_body(ctx, mesh, body, quad_order, rhs.data());
+  if (rc == TPTFEM_OK)
+    rc = tptfem_solve_with_dirichlet(ctx, K, rhs.data(), (int64_t)rhs.size(), bc_dof, bc_val, nbc, opts, u, stats);
+  tptfem_matrix_free(K);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,793 @@
+// assemble.cu -- element stiffness/load kernels and the element->CSR scatter.
+//
+// Design: "row gather".  One thread owns one global row (node n, component a)
+// and walks the elements incident to n in ascending element id.  For each it
+// recomputes the element geometry and the element-matrix ROW belonging to
+// (n, a), and adds every entry into a dense per-row accumulator over n's
+// neighbour columns (shared memory).  Because one thread adds the
+// contributions of an entry in element order starting from +0.0, the result
+// is bit-identical to Coo::to_csr's sequential duplicate sum
+// (crates/tpt-fem-sparse/src/lib.rs:144-163), with no atomics and no COO
+// triplet array in HBM.  A slot enters the pattern iff at least one element
+// contributed a value != 0.0, which is the reference's zero-skip
+// (crates/tpt-fem-assembly/src/lib.rs:469-472).
+//
+// The element formulas reproduce the reference's FP64 operation order
+// exactly; this file is compiled with -fmad=false so no multiply-add is
+// contracted.  Products with a structural zero of B or D are omitted: they
+// add a signed zero to a sum, which never changes a stored value.
+//
+// Reference functions restated here (crates/...):
+//   tpt-fem-element/src/lib.rs     624-740  Map, mat_det, mat_inv, physical_grad
+//   tpt-fem-thermal/src/lib.rs     132-196  poisson_element_matrix / source_vector
+//   tpt-fem-elasticity/src/lib.rs  197-348  constitutive, b_matrix, element matrix, body vector
+//   tpt-fem-assembly/src/lib.rs    394-420, 601-667  surface, apply_neumann_order
+#include <cmath>
+
+#include "objects.hpp"
+
+namespace tptfem {
+
+namespace {
+
+// ---- quadrature tables (host-computed with the reference's expressions) ----
+struct QuadTab {
+  int nq;
+  double w[25];
+  double ns[25][4];     // shape values per point and node
+  double lg[25][4][2];  // Quad4 reference gradients per point and node
+};
+__constant__ QuadTab c_cell;
+
+struct FaceTab {
+  int nq;
+  double w[4];
+  double ns[4][3];
+};
+__constant__ FaceTab c_face;
+
+// gauss_legendre (crates/tpt-fem-quadrature/src/lib.rs:118-162)
+bool gauss_legendre(int order, double* p, double* w) {
+  switch (order) {
+    case 1: p[0] = 0.0; w[0] = 2.0; return true;
+    case 2: p[0] = -1.0 / std::sqrt(3.0); p[1] = 1.0 / std::sqrt(3.0); w[0] = w[1] = 1.0; return true;
+    case 3:
+      p[0] = 0.0; p[1] = -std::sqrt(3.0 / 5.0); p[2] = std::sqrt(3.0 / 5.0);
+      w[0] = 8.0 / 9.0; w[1] = 5.0 / 9.0; w[2] = 5.0 / 9.0;
+      return true;
+    case 4: {
+      const double pp[4] = {-0.3399810435848563, 0.3399810435848563, -0.8611363115940526, 0.8611363115940526};
+      const double ww[4] = {0.6521451548625461, 0.6521451548625461, 0.3478548451374539, 0.3478548451374539};
+      for (int i = 0; i < 4; ++i) { p[i] = pp[i]; w[i] = ww[i]; }
+      return true;
+    }
+    case 5: {
+      const double pp[5] = {0.0, -0.5384693101056831, 0.5384693101056831, -0.9061798459386640, 0.9061798459386640};
+      const double ww[5] = {0.5688888888888889, 0.4786286704993665, 0.4786286704993665, 0.2369268850561891,
+                            0.2369268850561891};
+      for (int i = 0; i < 5; ++i) { p[i] = pp[i]; w[i] = ww[i]; }
+      return true;
+    }
+    default: return false;
+  }
+}
+
+// cell_quad (crates/tpt-fem-thermal/src/lib.rs:29-92) for Tet4 / Quad4, plus
+// the shape values and reference gradients at each point.
+QuadTab make_cell_tab(int cell, int order) {
+  QuadTab t{};
+  if (cell == TPTFEM_CELL_TET4) {  // tetrahedron(Degree2), quadrature:282-289; order ignored
+    const double a = 0.5854101966249685, b = 0.1381966011250105;
+    const double pts[4][3] = {{a, b, b}, {b, a, b}, {b, b, a}, {b, b, b}};
+    t.nq = 4;
+    for (int q = 0; q < 4; ++q) {
+      t.w[q] = 1.0 / 24.0;
+      double x = pts[q][0], y = pts[q][1], z = pts[q][2];
+      t.ns[q][0] = 1.0 - x - y - z;
+      t.ns[q][1] = x; t.ns[q][2] = y; t.ns[q][3] = z;
+    }
+    return t;
+  }
+  double p[5], w[5];
+  TPT_REQUIRE(gauss_legendre(order, p, w), TPTFEM_ERR_INVALID_ARG, "quad_order must be in 1..=5");
+  const double s[4] = {-1.0, 1.0, 1.0, -1.0}, tt[4] = {-1.0, -1.0, 1.0, 1.0};
+  int q = 0;
+  for (int ia = 0; ia < order; ++ia)
+    for (int ib = 0; ib < order; ++ib, ++q) {  // tensor_square: outer a, inner b (quadrature:180-191)
+      double x = p[ia], y = p[ib];
+      t.w[q] = w[ia] * w[ib];
+      for (int i = 0; i < 4; ++i) {  // Quad4 shape/grad (element:135-153)
+        t.ns[q][i] = 0.25 * (1.0 + s[i] * x) * (1.0 + tt[i] * y);
+        t.lg[q][i][0] = 0.25 * s[i] * (1.0 + tt[i] * y);
+        t.lg[q][i][1] = 0.25 * (1.0 + s[i] * x) * tt[i];
+      }
+    }
+  t.nq = q;
+  return t;
+}
+
+// face_quad (crates/tpt-fem-assembly/src/lib.rs:336-358) at FACE_QUAD_ORDER = 2.
+FaceTab make_face_tab(int cell) {
+  FaceTab f{};
+  if (cell == TPTFEM_CELL_TET4) {  // triangle(Degree2) on Tri3 faces
+    const double pts[3][2] = {{2.0 / 3.0, 1.0 / 6.0}, {1.0 / 6.0, 2.0 / 3.0}, {1.0 / 6.0, 1.0 / 6.0}};
+    f.nq = 3;
+    for (int q = 0; q < 3; ++q) {
+      f.w[q] = 1.0 / 6.0;
+      double x = pts[q][0], y = pts[q][1];
+      f.ns[q][0] = 1.0 - x - y; f.ns[q][1] = x; f.ns[q][2] = y;
+    }
+  } else {  // gauss_legendre(2) on Line2 edges
+    double p[2], w[2];
+    gauss_legendre(2, p, w);
+    f.nq = 2;
+    for (int q = 0; q < 2; ++q) {
+      f.w[q] = w[q];
+      f.ns[q][0] = (1.0 - p[q]) / 2.0;
+      f.ns[q][1] = (1.0 + p[q]) / 2.0;
+    }
+  }
+  return f;
+}
+
+// ---- element geometry ---------------------------------------------------------
+
+// Tet4: J[p][r] = X[r+1][p] - X[0][p] (what Map::from_nodes_and_grad's running
+// sum gives for the constant Tet4 gradients), det/inverse by cofactors in the
+// order of element:624-680, physical gradients as physical_grad's running sum.
+struct TetGeom {
+  double g[4][3];
+  double adet;
+};
+
+__device__ __forceinline__ bool tet_geom(const double (&X)[4][3], TetGeom& G) {
+  double m[9];
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) m[p * 3 + r] = X[r + 1][p] - X[0][p];
+  double c0 = m[4] * m[8] - m[5] * m[7];
+  double c1 = m[3] * m[8] - m[5] * m[6];
+  double c2 = m[3] * m[7] - m[4] * m[6];
+  double det = m[0] * c0 - m[1] * c1 + m[2] * c2;
+  double inv = 1.0 / det;
+  double iv[9];
+  iv[0] = c0 * inv;
+  iv[1] = (m[2] * m[7] - m[1] * m[8]) * inv;
+  iv[2] = (m[1] * m[5] - m[2] * m[4]) * inv;
+  iv[3] = (m[5] * m[6] - m[3] * m[8]) * inv;
+  iv[4] = (m[0] * m[8] - m[2] * m[6]) * inv;
+  iv[5] = (m[2] * m[3] - m[0] * m[5]) * inv;
+  iv[6] = c2 * inv;
+  iv[7] = (m[1] * m[6] - m[0] * m[7]) * inv;
+  iv[8] = (m[0] * m[4] - m[1] * m[3]) * inv;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    G.g[0][i] = (-iv[i] - iv[3 + i]) - iv[6 + i];
+    G.g[1][i] = iv[i];
+    G.g[2][i] = iv[3 + i];
+    G.g[3][i] = iv[6 + i];
+  }
+  G.adet = fabs(det);
+  return isfinite(inv) && isfinite(det);
+}
+
+// Quad4 at one quadrature point: J by the running sum over the 4 nodes.
+struct QuadGeom {
+  double g[4][2];
+  double adet;
+};
+
+__device__ __forceinline__ bool quad_geom(const double (&X)[4][2], int q, QuadGeom& G) {
+  double m[4];
+#pragma unroll
+  for (int p = 0; p < 2; ++p)
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      double s = X[0][p] * c_cell.lg[q][0][r];
+      s = s + X[1][p] * c_cell.lg[q][1][r];
+      s = s + X[2][p] * c_cell.lg[q][2][r];
+      s = s + X[3][p] * c_cell.lg[q][3][r];
+      m[p * 2 + r] = s;
+    }
+  double det = m[0] * m[3] - m[1] * m[2];
+  double inv = 1.0 / det;
+  double iv[4] = {m[3] * inv, -m[1] * inv, -m[2] * inv, m[0] * inv};
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int i = 0; i < 2; ++i) G.g[n][i] = c_cell.lg[q][n][0] * iv[i] + c_cell.lg[q][n][1] * iv[2 + i];
+  G.adet = fabs(det);
+  return isfinite(inv) && isfinite(det);
+}
+
+// ---- element rows -------------------------------------------------------------
+
+// Isotropic constitutive constants (elasticity:197-233) for one element.
+struct Dmat {
+  double d00, d01, dsh;  // diagonal normal, off-diagonal normal, shear
+};
+
+__device__ __forceinline__ Dmat make_d(int model, double e, double nu) {
+  Dmat D;
+  if (model == TPTFEM_MODEL_CONTINUUM_3D) {
+    double c = e / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    D.d00 = (1.0 - nu) * c;
+    D.d01 = c * nu;
+    D.dsh = (1.0 - 2.0 * nu) / 2.0 * c;
+  } else if (model == TPTFEM_MODEL_PLANE_STRESS) {
+    double c = e / (1.0 - nu * nu);
+    D.d00 = c;
+    D.d01 = c * nu;
+    D.dsh = c * (1.0 - nu) / 2.0;
+  } else {  // plane strain
+    double c = e / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    D.d00 = c * (1.0 - nu);
+    D.d01 = c * nu;
+    D.dsh = c * (1.0 - 2.0 * nu) / 2.0;
+  }
+  return D;
+}
+
+// sum_{s,t} (B_l[s][a] * D[s][t]) * B_j[t][b] over the structurally non-zero
+// terms, in the reference's s-major, t-minor order (elasticity:292-306).
+__device__ __forceinline__ double bdb3(const double* gl, const double* gj, int a, int b, const Dmat& D) {
+  const double m = D.d00, cn = D.d01, d = D.dsh;
+  switch (a * 3 + b) {
+    case 0: return ((gl[0] * m) * gj[0] + (gl[1] * d) * gj[1]) + (gl[2] * d) * gj[2];
+    case 1: return (gl[0] * cn) * gj[1] + (gl[1] * d) * gj[0];
+    case 2: return (gl[0] * cn) * gj[2] + (gl[2] * d) * gj[0];
+    case 3: return (gl[1] * cn) * gj[0] + (gl[0] * d) * gj[1];
+    case 4: return ((gl[1] * m) * gj[1] + (gl[0] * d) * gj[0]) + (gl[2] * d) * gj[2];
+    case 5: return (gl[1] * cn) * gj[2] + (gl[2] * d) * gj[1];
+    case 6: return (gl[2] * cn) * gj[0] + (gl[0] * d) * gj[2];
+    case 7: return (gl[2] * cn) * gj[1] + (gl[1] * d) * gj[2];
+    default: return ((gl[2] * m) * gj[2] + (gl[1] * d) * gj[1]) + (gl[0] * d) * gj[0];
+  }
+}
+
+__device__ __forceinline__ double bdb2(const double* gl, const double* gj, int a, int b, const Dmat& D) {
+  switch (a * 2 + b) {
+    case 0: return (gl[0] * D.d00) * gj[0] + (gl[1] * D.dsh) * gj[1];
+    case 1: return (gl[0] * D.d01) * gj[1] + (gl[1] * D.dsh) * gj[0];
+    case 2: return (gl[1] * D.d01) * gj[0] + (gl[0] * D.dsh) * gj[1];
+    default: return (gl[1] * D.d00) * gj[1] + (gl[0] * D.dsh) * gj[0];
+  }
+}
+
+struct ElemIn {
+  const double* coords;
+  int cdim;
+  const int* conn;
+  const double* coef;
+  int per_elem;
+  int model;
+  double nu;
+};
+
+template <int CELL>
+struct CellTraits;
+template <>
+struct CellTraits<TPTFEM_CELL_TET4> {
+  static constexpr int SD = 3;
+};
+template <>
+struct CellTraits<TPTFEM_CELL_QUAD4> {
+  static constexpr int SD = 2;
+};
+
+template <int CELL>
+__device__ __forceinline__ void load_elem(const ElemIn& in, int e, double (&X)[4][CellTraits<CELL>::SD],
+                                          int (&nodes)[4]) {
+  int4 c = reinterpret_cast<const int4*>(in.conn)[e];
+  nodes[0] = c.x; nodes[1] = c.y; nodes[2] = c.z; nodes[3] = c.w;
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int p = 0; p < CellTraits<CELL>::SD; ++p) X[j][p] = __ldg(in.coords + (int64_t)nodes[j] * in.cdim + p);
+}
+
+// Row (l, a) of the element matrix: out[j*DPN + b] for the element's 4 nodes.
+// PHYS 0: poisson_element_matrix with conductivity k; PHYS 1: elasticity.
+template <int CELL, int PHYS, int DPN>
+__device__ __forceinline__ bool element_row(const double (&X)[4][CellTraits<CELL>::SD], double coef, int model,
+                                            double nu, int l, int a, double (&out)[4 * DPN]) {
+  bool ok = true;
+  if constexpr (CELL == TPTFEM_CELL_TET4) {
+    TetGeom G;
+    ok = tet_geom(X, G);
+    const double w = c_cell.w[0];
+    if constexpr (PHYS == 0) {
+      const double wk = w * coef;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        double dot = G.g[l][0] * G.g[j][0] + G.g[l][1] * G.g[j][1] + G.g[l][2] * G.g[j][2];
+        double t = wk * dot * G.adet;
+        double v = t + t;  // four identical quadrature points, summed in order
+        v = v + t;
+        out[j] = v + t;
+      }
+    } else {
+      Dmat D = make_d(model, coef, nu);
+      const double wd = w * G.adet;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          double t = wd * bdb3(G.g[l], G.g[j], a, b, D);
+          double v = t + t;
+          v = v + t;
+          out[j * 3 + b] = v + t;
+        }
+    }
+  } else {  // Quad4: the Jacobian varies per point
+#pragma unroll
+    for (int i = 0; i < 4 * DPN; ++i) out[i] = 0.0;
+    Dmat D;
+    if constexpr (PHYS == 1) D = make_d(model, coef, nu);
+    const int nq = c_cell.nq;
+    for (int q = 0; q < nq; ++q) {
+      QuadGeom G;
+      ok &= quad_geom(X, q, G);
+      const double w = c_cell.w[q];
+      if constexpr (PHYS == 0) {
+        const double wk = w * coef;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          double dot = G.g[l][0] * G.g[j][0] + G.g[l][1] * G.g[j][1];
+          out[j] = out[j] + wk * dot * G.adet;
+        }
+      } else {
+        const double wd = w * G.adet;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int b = 0; b < 2; ++b) out[j * 2 + b] = out[j * 2 + b] + wd * bdb2(G.g[l], G.g[j], a, b, D);
+      }
+    }
+  }
+  return ok;
+}
+
+enum { MODE_COUNT = 0, MODE_FILL = 1, MODE_NUMERIC = 2 };
+
+struct RowArgs {
+  ElemIn in;
+  const int* ne_ptr;
+  const int* ne;
+  const uchar4* slot;
+  const int* nb_ptr;
+  const int* nb;
+  int64_t nrows;
+  int* row_cnt;        // COUNT
+  const int* row_ptr;  // FILL / NUMERIC
+  int* col;            // FILL writes, NUMERIC checks
+  double* val;
+  int* flag;           // bit 0: bad element geometry, bit 1: pattern changed
+  int maxc;            // accumulator slots per thread (max neighbours * DPN)
+};
+
+// One thread per global row.  Shared memory holds the row's dense accumulator
+// (double) and non-zero flags (byte), slot-major so a warp touches consecutive
+// words.
+template <int CELL, int PHYS, int DPN, int MODE>
+__global__ void __launch_bounds__(128) assemble_rows(RowArgs A) {
+  extern __shared__ double sh[];
+  const int T = blockDim.x;
+  const int tid = threadIdx.x;
+  const int64_t r = (int64_t)blockIdx.x * T + tid;
+  if (r >= A.nrows) return;
+  const int n = (int)(r / DPN), a = (int)(r % DPN);
+  const int nb0 = A.nb_ptr[n];
+  const int ncand = (A.nb_ptr[n + 1] - nb0) * DPN;
+  double* acc = sh;
+  unsigned char* nzf = reinterpret_cast<unsigned char*>(sh + (size_t)A.maxc * T);
+  for (int s = 0; s < ncand; ++s) {
+    acc[s * T + tid] = 0.0;
+    nzf[s * T + tid] = 0;
+  }
+  bool ok = true;
+  const int k1 = A.ne_ptr[n + 1];
+  for (int k = A.ne_ptr[n]; k < k1; ++k) {
+    const int pe = A.ne[k];
+    const int e = pe >> 2, l = pe & 3;
+    const uchar4 sl = A.slot[k];
+    double X[4][CellTraits<CELL>::SD];
+    int nodes[4];
+    load_elem<CELL>(A.in, e, X, nodes);
+    const double coef = A.in.coef[A.in.per_elem ? e : 0];
+    double out[4 * DPN];
+    ok &= element_row<CELL, PHYS, DPN>(X, coef, A.in.model, A.in.nu, l, a, out);
+    const int sj[4] = {sl.x, sl.y, sl.z, sl.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int b = 0; b < DPN; ++b) {
+        const int s = (sj[j] * DPN + b) * T + tid;
+        const double v = out[j * DPN + b];
+        acc[s] = acc[s] + v;
+        nzf[s] |= (unsigned char)(v != 0.0);
+      }
+  }
+  if (!ok) atomicOr(A.flag, 1);
+  if (MODE == MODE_COUNT) {
+    int c = 0;
+    for (int s = 0; s < ncand; ++s) c += nzf[s * T + tid];
+    A.row_cnt[r] = c;
+  } else {
+    int o = A.row_ptr[r];
+    const int end = A.row_ptr[r + 1];
+    bool same = true;
+    for (int s = 0; s < ncand; ++s) {
+      if (!nzf[s * T + tid]) continue;
+      const int cidx = A.nb[nb0 + s / DPN] * DPN + s % DPN;
+      if (MODE == MODE_FILL) {
+        A.col[o] = cidx;
+        A.val[o] = acc[s * T + tid];
+      } else {
+        if (o >= end || A.col[o] != cidx) { same = false; break; }
+        A.val[o] = acc[s * T + tid];
+      }
+      ++o;
+    }
+    if (MODE == MODE_NUMERIC && (!same || o != end)) atomicOr(A.flag, 2);
+  }
+}
+
+// ---- loads ----------------------------------------------------------------------
+
+struct LoadArgs {
+  ElemIn in;
+  const int* ne_ptr;
+  const int* ne;
+  int64_t n_nodes;
+  double b[3];  // source value (Poisson) or body force (elasticity)
+  double* rhs;
+  int* flag;
+};
+
+// rhs[n*DPN + a] = sum over incident elements (ascending id) of the element
+// load entry, like the reference's `rhs[node] += f[i]` loops.
+// KIND 0: poisson_source_vector (thermal:163-196); KIND 1: elasticity_body_vector (elasticity:312-348).
+template <int CELL, int KIND, int DPN>
+__global__ void load_rows(LoadArgs A) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= A.n_nodes) return;
+  double acc[DPN];
+#pragma unroll
+  for (int a = 0; a < DPN; ++a) acc[a] = 0.0;
+  bool ok = true;
+  for (int k = A.ne_ptr[n]; k < A.ne_ptr[n + 1]; ++k) {
+    const int e = A.ne[k] >> 2, l = A.ne[k] & 3;
+    double X[4][CellTraits<CELL>::SD];
+    int nodes[4];
+    load_elem<CELL>(A.in, e, X, nodes);
+    double f[DPN];
+#pragma unroll
+    for (int a = 0; a < DPN; ++a) f[a] = 0.0;
+    const int nq = c_cell.nq;
+    if constexpr (CELL == TPTFEM_CELL_TET4) {
+      TetGeom G;
+      ok &= tet_geom(X, G);
+      for (int q = 0; q < nq; ++q) {
+        const double w = c_cell.w[q], N = c_cell.ns[q][l];
+        if (KIND == 0) f[0] = f[0] + w * A.b[0] * N * G.adet;
+        else
+#pragma unroll
+          for (int a = 0; a < DPN; ++a) f[a] = f[a] + w * N * A.b[a] * G.adet;
+      }
+    } else {
+      for (int q = 0; q < nq; ++q) {
+        QuadGeom G;
+        ok &= quad_geom(X, q, G);
+        const double w = c_cell.w[q], N = c_cell.ns[q][l];
+        if (KIND == 0) f[0] = f[0] + w * A.b[0] * N * G.adet;
+        else
+#pragma unroll
+          for (int a = 0; a < DPN; ++a) f[a] = f[a] + w * N * A.b[a] * G.adet;
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < DPN; ++a) acc[a] = acc[a] + f[a];
+  }
+  if (!ok) atomicOr(A.flag, 1);
+#pragma unroll
+  for (int a = 0; a < DPN; ++a) A.rhs[n * DPN + a] = acc[a];
+}
+
+struct TractionArgs {
+  ElemIn in;
+  const int* ne_ptr;
+  const int* ne;
+  const unsigned char* bface;
+  int64_t n_nodes;
+  int dpn, axis;
+  double sign;
+  double t[3];
+  double* rhs;
+};
+
+// apply_neumann_order (assembly:601-667) with the face-selector flux, one
+// thread per node visiting its boundary faces in (element, face) order.
+template <int CELL>
+__global__ void traction_rows(TractionArgs A) {
+  constexpr int SD = CellTraits<CELL>::SD;
+  constexpr int FN = (CELL == TPTFEM_CELL_TET4) ? 3 : 2;
+  const int tet_f[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
+  const int quad_f[4][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}};
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= A.n_nodes) return;
+  double acc[3];
+  for (int c = 0; c < A.dpn; ++c) acc[c] = A.rhs[n * A.dpn + c];
+  for (int k = A.ne_ptr[n]; k < A.ne_ptr[n + 1]; ++k) {
+    const int e = A.ne[k] >> 2, l = A.ne[k] & 3;
+    const unsigned bm = A.bface[e];
+    if (!bm) continue;
+    double X[4][SD];
+    int nodes[4];
+    load_elem<CELL>(A.in, e, X, nodes);
+    for (int fi = 0; fi < 4; ++fi) {
+      if (!(bm & (1u << fi))) continue;
+      int fl[3];
+      int kpos = -1;
+      for (int q = 0; q < FN; ++q) {
+        fl[q] = (CELL == TPTFEM_CELL_TET4) ? tet_f[fi][q] : quad_f[fi][q];
+        if (fl[q] == l) kpos = q;
+      }
+      if (kpos < 0) continue;
+      // tangents from the face's reference gradients
+      double measure, nrm[SD];
+      if constexpr (CELL == TPTFEM_CELL_TET4) {
+        double t0[3], t1[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          t0[d] = X[fl[1]][d] - X[fl[0]][d];
+          t1[d] = X[fl[2]][d] - X[fl[0]][d];
+        }
+        double c[3] = {t0[1] * t1[2] - t0[2] * t1[1], t0[2] * t1[0] - t0[0] * t1[2], t0[0] * t1[1] - t0[1] * t1[0]};
+        measure = sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+        for (int d = 0; d < 3; ++d) nrm[d] = c[d] / measure;
+      } else {
+        double t[2];
+#pragma unroll
+        for (int d = 0; d < 2; ++d) t[d] = -0.5 * X[fl[0]][d] + 0.5 * X[fl[1]][d];
+        measure = sqrt(t[0] * t[0] + t[1] * t[1]);
+        double n0 = -t[1], n1 = t[0];
+        double ln = sqrt(n0 * n0 + n1 * n1);
+        nrm[0] = n0 / ln;
+        nrm[1] = n1 / ln;
+      }
+      // orient outward: face centroid minus element centroid (assembly:645-653)
+      double ec[SD], fc[SD], dd = 0.0;
+#pragma unroll
+      for (int d = 0; d < SD; ++d) {
+        double s = 0.0;
+        for (int j = 0; j < 4; ++j) s = s + X[j][d];
+        ec[d] = s / 4.0;
+        double f = 0.0;
+        for (int q = 0; q < FN; ++q) f = f + X[fl[q]][d];
+        fc[d] = f / (double)FN;
+      }
+      dd = nrm[0] * (fc[0] - ec[0]);
+      for (int d = 1; d < SD; ++d) dd = dd + nrm[d] * (fc[d] - ec[d]);
+      if (dd < 0.0)
+        for (int d = 0; d < SD; ++d) nrm[d] = -nrm[d];
+      const bool sel = nrm[A.axis] * A.sign > 0.5;
+      for (int q = 0; q < c_face.nq; ++q) {
+        const double wm = c_face.w[q] * measure, N = c_face.ns[q][kpos];
+        for (int c = 0; c < A.dpn; ++c) {
+          const double g = sel ? A.t[c] : 0.0;
+          acc[c] = acc[c] + wm * g * N;
+        }
+      }
+    }
+  }
+  for (int c = 0; c < A.dpn; ++c) A.rhs[n * A.dpn + c] = acc[c];
+}
+
+ElemIn elem_in(const MeshData& m, const double* coef, int per_elem, int model, double nu) {
+  ElemIn in;
+  in.coords = m.coords.p;
+  in.cdim = m.cdim;
+  in.conn = m.conn.p;
+  in.coef = coef;
+  in.per_elem = per_elem;
+  in.model = model;
+  in.nu = nu;
+  return in;
+}
+
+void set_cell_tab(const MeshData& m, int quad_order, cudaStream_t s) {
+  QuadTab t = make_cell_tab(m.cell, quad_order);
+  TPT_CUDA(cudaMemcpyToSymbolAsync(c_cell, &t, sizeof(t), 0, cudaMemcpyHostToDevice, s));
+}
+
+int read_flag(tptfem_context* ctx) {
+  TPT_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  return ctx->h_pinned[0];
+}
+
+template <int CELL, int PHYS, int DPN>
+void launch_rows(int mode, const RowArgs& A, cudaStream_t s) {
+  // Threads per block: the dense accumulator (9 bytes per slot and thread)
+  // must fit in shared memory.
+  int threads = 128;
+  while (threads > 32 && (size_t)threads * A.maxc * 9 > 200 * 1024) threads -= 32;
+  size_t smem = (size_t)threads * A.maxc * 9;
+  TPT_REQUIRE(smem <= 227 * 1024, TPTFEM_ERR_CREATION, "node valence too high for the device assembly path");
+  auto run = [&](auto kern) {
+    TPT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<ceil_div(A.nrows, threads), threads, smem, s>>>(A);
+    TPT_CHECK_LAUNCH();
+  };
+  if (mode == MODE_COUNT) run(assemble_rows<CELL, PHYS, DPN, MODE_COUNT>);
+  else if (mode == MODE_FILL) run(assemble_rows<CELL, PHYS, DPN, MODE_FILL>);
+  else run(assemble_rows<CELL, PHYS, DPN, MODE_NUMERIC>);
+}
+
+void dispatch_rows(const MatrixData& M, int mode, const RowArgs& A, cudaStream_t s) {
+  const int cell = M.mesh->cell;
+  if (cell == TPTFEM_CELL_TET4) {
+    if (M.physics == 0) launch_rows<TPTFEM_CELL_TET4, 0, 1>(mode, A, s);
+    else launch_rows<TPTFEM_CELL_TET4, 1, 3>(mode, A, s);
+  } else {
+    if (M.physics == 0) launch_rows<TPTFEM_CELL_QUAD4, 0, 1>(mode, A, s);
+    else launch_rows<TPTFEM_CELL_QUAD4, 1, 2>(mode, A, s);
+  }
+}
+
+RowArgs row_args(MatrixData& M) {
+  MeshData& m = *M.mesh;
+  RowArgs A;
+  A.in = elem_in(m, M.coef.p, M.per_element, M.model, M.nu);
+  A.ne_ptr = m.ne_ptr.p;
+  A.ne = m.ne.p;
+  A.slot = m.slot.p;
+  A.nb_ptr = m.nb_ptr.p;
+  A.nb = m.nb.p;
+  A.nrows = M.nrows;
+  A.row_cnt = nullptr;
+  A.row_ptr = M.row_ptr.p;
+  A.col = M.col.p;
+  A.val = M.val.p;
+  A.flag = M.ctx->d_flag;
+  A.maxc = m.max_nb * M.dpn;
+  return A;
+}
+
+// Largest row/column index with an entry, plus one (what Coo::to_csr reports
+// as nrows / ncols, crates/tpt-fem-sparse/src/lib.rs:124-139).
+__global__ void ref_dims(const int* __restrict__ rp, const int* __restrict__ col, int64_t nrows, int* out) {
+  int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrows) return;
+  int b = rp[r], e = rp[r + 1];
+  if (e > b) {
+    atomicMax(out, (int)r);
+    atomicMax(out + 1, col[e - 1]);
+  }
+}
+
+}  // namespace
+
+void assemble_matrix(MatrixData& M) {
+  MeshData& m = *M.mesh;
+  tptfem_context* ctx = M.ctx;
+  cudaStream_t s = ctx->stream;
+  TPT_REQUIRE(m.cell == TPTFEM_CELL_TET4 || m.cell == TPTFEM_CELL_QUAD4, TPTFEM_ERR_INVALID_ARG,
+              "device assembly supports Tet4 and Quad4 meshes");
+  if (M.physics == 1) {
+    bool okm = (m.cell == TPTFEM_CELL_TET4 && M.model == TPTFEM_MODEL_CONTINUUM_3D) ||
+               (m.cell == TPTFEM_CELL_QUAD4 &&
+                (M.model == TPTFEM_MODEL_PLANE_STRESS || M.model == TPTFEM_MODEL_PLANE_STRAIN));
+    TPT_REQUIRE(okm, TPTFEM_ERR_MODEL_DIM_MISMATCH,
+                "elasticity model/dimension mismatch: model is incompatible with the mesh's spatial dimension");
+  }
+  M.dpn = M.physics == 0 ? 1 : (m.cell == TPTFEM_CELL_TET4 ? 3 : 2);
+  mesh_build_adjacency(m);
+  set_cell_tab(m, M.quad_order, s);
+  M.nrows = m.n_nodes * M.dpn;
+  TPT_REQUIRE(M.nrows < (1LL << 31), TPTFEM_ERR_CREATION, "row count exceeds the int32 device index range");
+  DevBuf<int> cnt;
+  cnt.alloc(M.nrows + 1, s);
+  TPT_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), s));
+  RowArgs A = row_args(M);
+  A.row_cnt = cnt.p;
+  dispatch_rows(M, MODE_COUNT, A, s);
+  TPT_REQUIRE((read_flag(ctx) & 1) == 0, TPTFEM_ERR_NUMERIC,
+              "degenerate element: zero or non-finite Jacobian determinant");
+  M.row_ptr.alloc(M.nrows + 1, s);
+  M.nnz = exclusive_scan_i32(cnt.p, M.row_ptr.p, M.nrows, s);
+  M.col.alloc(M.nnz, s);
+  M.val.alloc(M.nnz, s);
+  A = row_args(M);
+  dispatch_rows(M, MODE_FILL, A, s);
+  DevBuf<int> dims;
+  dims.alloc(2, s);
+  TPT_CUDA(cudaMemsetAsync(dims.p, 0, 2 * sizeof(int), s));
+  ref_dims<<<ceil_div(M.nrows, 256), 256, 0, s>>>(M.row_ptr.p, M.col.p, M.nrows, dims.p);
+  TPT_CHECK_LAUNCH();
+  int hd[2];
+  TPT_CUDA(cudaMemcpyAsync(hd, dims.p, sizeof(hd), cudaMemcpyDeviceToHost, s));
+  TPT_CUDA(cudaStreamSynchronize(s));
+  M.ref_nrows = (int64_t)hd[0] + 1;
+  M.ref_ncols = (int64_t)hd[1] + 1;
+}
+
+bool reassemble_values(MatrixData& M) {
+  tptfem_context* ctx = M.ctx;
+  cudaStream_t s = ctx->stream;
+  set_cell_tab(*M.mesh, M.quad_order, s);
+  TPT_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), s));
+  RowArgs A = row_args(M);
+  dispatch_rows(M, MODE_NUMERIC, A, s);
+  int f = read_flag(ctx);
+  TPT_REQUIRE((f & 1) == 0, TPTFEM_ERR_NUMERIC, "degenerate element: zero or non-finite Jacobian determinant");
+  return (f & 2) == 0;
+}
+
+void load_poisson_source(MeshData& m, double src, int quad_order, double* d_rhs) {
+  tptfem_context* ctx = m.ctx;
+  cudaStream_t s = ctx->stream;
+  mesh_build_adjacency(m);
+  set_cell_tab(m, quad_order, s);
+  TPT_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), s));
+  LoadArgs A;
+  A.in = elem_in(m, nullptr, 0, 0, 0.0);
+  A.ne_ptr = m.ne_ptr.p;
+  A.ne = m.ne.p;
+  A.n_nodes = m.n_nodes;
+  A.b[0] = src; A.b[1] = A.b[2] = 0.0;
+  A.rhs = d_rhs;
+  A.flag = ctx->d_flag;
+  if (m.cell == TPTFEM_CELL_TET4) load_rows<TPTFEM_CELL_TET4, 0, 1><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
+  else load_rows<TPTFEM_CELL_QUAD4, 0, 1><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
+  TPT_CHECK_LAUNCH();
+  TPT_REQUIRE((read_flag(ctx) & 1) == 0, TPTFEM_ERR_NUMERIC, "degenerate element in load integration");
+}
+
+void load_body(MeshData& m, const double* body, int quad_order, double* d_rhs) {
+  tptfem_context* ctx = m.ctx;
+  cudaStream_t s = ctx->stream;
+  mesh_build_adjacency(m);
+  set_cell_tab(m, quad_order, s);
+  TPT_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), s));
+  LoadArgs A;
+  A.in = elem_in(m, nullptr, 0, 0, 0.0);
+  A.ne_ptr = m.ne_ptr.p;
+  A.ne = m.ne.p;
+  A.n_nodes = m.n_nodes;
+  A.b[0] = body[0]; A.b[1] = body[1]; A.b[2] = m.cell == TPTFEM_CELL_TET4 ? body[2] : 0.0;
+  A.rhs = d_rhs;
+  A.flag = ctx->d_flag;
+  if (m.cell == TPTFEM_CELL_TET4) load_rows<TPTFEM_CELL_TET4, 1, 3><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
+  else load_rows<TPTFEM_CELL_QUAD4, 1, 2><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
+  TPT_CHECK_LAUNCH();
+  TPT_REQUIRE((read_flag(ctx) & 1) == 0, TPTFEM_ERR_NUMERIC, "degenerate element in load integration");
+}
+
+void apply_traction(MeshData& m, int dpn, int axis, double sign, const double* t, double* d_rhs) {
+  cudaStream_t s = m.ctx->stream;
+  const int sd = m.cell == TPTFEM_CELL_TET4 ? 3 : 2;
+  TPT_REQUIRE(dpn >= 1 && dpn <= 3, TPTFEM_ERR_INVALID_ARG, "dofs_per_node must be 1..3");
+  TPT_REQUIRE(axis >= 0 && axis < sd, TPTFEM_ERR_INVALID_ARG, "axis out of range for the mesh dimension");
+  mesh_build_boundary_faces(m);
+  FaceTab f = make_face_tab(m.cell);
+  TPT_CUDA(cudaMemcpyToSymbolAsync(c_face, &f, sizeof(f), 0, cudaMemcpyHostToDevice, s));
+  TractionArgs A;
+  A.in = elem_in(m, nullptr, 0, 0, 0.0);
+  A.ne_ptr = m.ne_ptr.p;
+  A.ne = m.ne.p;
+  A.bface = m.bface.p;
+  A.n_nodes = m.n_nodes;
+  A.dpn = dpn;
+  A.axis = axis;
+  A.sign = sign;
+  for (int c = 0; c < 3; ++c) A.t[c] = c < dpn ? t[c] : 0.0;
+  A.rhs = d_rhs;
+  if (m.cell == TPTFEM_CELL_TET4) traction_rows<TPTFEM_CELL_TET4><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
+  else traction_rows<TPTFEM_CELL_QUAD4><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
+  TPT_CHECK_LAUNCH();
+}
+
+}  // namespace tptfem

@@ -1,0 +1,106 @@
+// objects.hpp -- the structs behind the opaque C-ABI handles and the internal
+// entry points the C ABI (api.cu) dispatches to.
+#pragma once
+#include <memory>
+#include <string>
+
+#include "common.cuh"
+
+struct tptfem_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  int* d_flag = nullptr;  // device error/validation flag scratch (one int)
+  int* h_pinned = nullptr;  // pinned staging (64 bytes)
+};
+
+namespace tptfem {
+
+// Device-resident mesh plus lazily built node->element adjacency.
+struct MeshData {
+  tptfem_context* ctx = nullptr;
+  int cell = TPTFEM_CELL_TET4;
+  int cdim = 3;   // coordinates stored per node
+  int npe = 4;    // nodes per element
+  int64_t n_nodes = 0, n_elems = 0;
+  DevBuf<double> coords;  // n_nodes x cdim (row-major)
+  DevBuf<int> conn;       // n_elems x npe
+  // node -> incident elements, sorted by element id: entries (eid << 2) | local_index
+  bool adj = false;
+  DevBuf<int> ne_ptr, ne;
+  // node -> sorted neighbour nodes (including itself)
+  DevBuf<int> nb_ptr, nb;
+  // per ne entry: position of each of the element's nodes in the node's neighbour list
+  DevBuf<uchar4> slot;
+  int max_nb = 0;   // largest neighbour count
+  int max_deg = 0;  // largest incident-element count
+  // per element bitmask of boundary faces (lazy)
+  bool bfaces = false;
+  DevBuf<unsigned char> bface;
+};
+
+struct MatrixData {
+  tptfem_context* ctx = nullptr;
+  std::shared_ptr<MeshData> mesh;
+  int physics = 0;  // 0 Poisson, 1 elasticity
+  int model = TPTFEM_MODEL_CONTINUUM_3D;
+  double nu = 0.0;
+  int quad_order = 2;
+  int dpn = 1;
+  int64_t nrows = 0, nnz = 0;
+  int64_t ref_nrows = 0, ref_ncols = 0;  // what Coo::to_csr would report
+  DevBuf<int> row_ptr, col;
+  DevBuf<double> val;
+  DevBuf<double> coef;  // n_elems or 1
+  int per_element = 0;
+};
+
+struct SolverWork;  // solver.cu
+
+struct SystemData {
+  tptfem_context* ctx = nullptr;
+  int64_t n = 0, n_free = 0, nnz = 0;
+  DevBuf<int> free_map;   // reduced -> full
+  DevBuf<int> row_ptr, col;
+  DevBuf<double> val;
+  DevBuf<float> val32;    // lazily converted FP32 copy for mixed precision
+  DevBuf<double> fred, x;
+  DevBuf<double> u_fixed;  // full-length vector holding the prescribed values
+  std::shared_ptr<SolverWork> work;
+  ~SystemData();
+};
+
+// mesh.cu
+void mesh_box(MeshData& m, const double mn[3], const double mx[3], const int64_t n[3]);
+void mesh_build_adjacency(MeshData& m);
+void mesh_build_boundary_faces(MeshData& m);
+
+// assemble.cu
+void assemble_matrix(MatrixData& A);             // symbolic + numeric
+bool reassemble_values(MatrixData& A);           // numeric; false if the pattern changed
+void load_poisson_source(MeshData& m, double s, int quad_order, double* d_rhs);
+void load_body(MeshData& m, const double* body, int quad_order, double* d_rhs);
+void apply_traction(MeshData& m, int dpn, int axis, double sign, const double* t, double* d_rhs);
+void csr_matvec_f64(tptfem_context* ctx, int64_t nrows, const int* rp, const int* ci, const double* va,
+                    const double* x, double* y);
+
+// reduce.cu
+std::unique_ptr<SystemData> reduce_system(tptfem_context* ctx, const MatrixData& A, const double* d_rhs,
+                                          const int64_t* bc_dof, const double* bc_val, int64_t nbc);
+void system_solution(const SystemData& S, double* d_u);
+
+// solver.cu
+void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats& st);
+
+}  // namespace tptfem
+
+struct tptfem_mesh {
+  std::shared_ptr<tptfem::MeshData> d;
+};
+struct tptfem_matrix {
+  std::unique_ptr<tptfem::MatrixData> d;
+};
+struct tptfem_system {
+  std::unique_ptr<tptfem::SystemData> d;
+};

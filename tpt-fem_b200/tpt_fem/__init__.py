@@ -1,0 +1,408 @@
+"""tpt_fem -- Python front end of the B200 finite-element hot path.
+
+Mirrors the reference's pyo3 module (crates/tpt-fem-py/src/lib.rs): a
+``Mesh`` class with ``box_mesh`` / ``node_count`` / ``coords`` /
+``nodes_on_plane`` / ``nodes_in_box`` and the solver functions
+``solve_poisson`` / ``solve_elasticity`` returning result objects with
+``values`` and ``to_numpy()``.  Below that it exposes the drop-in pieces of
+the path -- ``assemble_poisson``, ``assemble_elasticity``, ``Matrix.to_csr``,
+``reduce_system``, ``solve_with_dirichlet`` -- each a thin call through the C
+ABI of ``libtptfem.so`` (include/tptfem.h).  Every computation runs on the GPU;
+there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from ._native import (CELL_QUAD4, CELL_TET4, MODEL_BAR_AXIAL, MODEL_CONTINUUM_3D, MODEL_PLANE_STRAIN,
+                      MODEL_PLANE_STRESS, SOLVER_JACOBI_PCG, SOLVER_MP_PCG, SolverOpts, SolveStats)
+
+__all__ = [
+    "TptFemError", "Context", "Mesh", "Matrix", "System", "assemble_poisson", "assemble_elasticity",
+    "load_poisson_source", "load_body", "apply_traction", "reduce_system", "solve_with_dirichlet",
+    "solve_poisson", "solve_elasticity", "SolverOpts", "SolveStats", "CELL_TET4", "CELL_QUAD4",
+    "MODEL_CONTINUUM_3D", "MODEL_PLANE_STRESS", "MODEL_PLANE_STRAIN", "SOLVER_JACOBI_PCG", "SOLVER_MP_PCG",
+]
+
+
+class TptFemError(RuntimeError):
+    """A non-OK tptfem_status, with the context's message."""
+
+    def __init__(self, status, message):
+        self.status = status
+        self.name = N.STATUS_NAMES.get(status, str(status))
+        super().__init__(f"{self.name}: {message}")
+
+
+class Context:
+    """One device + one CUDA stream (tptfem_context)."""
+
+    _default = {}
+
+    def __init__(self, device=0):
+        self.lib = N.load()
+        h = C.c_void_p()
+        rc = self.lib.tptfem_create(device, C.byref(h))
+        if rc != N.OK:
+            raise TptFemError(rc, f"tptfem_create(device={device}) failed (no usable sm_100 GPU?)")
+        self.h = h
+        self.device = device
+
+    @classmethod
+    def default(cls, device=0):
+        if device not in cls._default:
+            cls._default[device] = Context(device)
+        return cls._default[device]
+
+    def check(self, rc):
+        if rc != N.OK:
+            buf = C.create_string_buffer(4096)
+            self.lib.tptfem_last_error(self.h, buf, len(buf))
+            raise TptFemError(rc, buf.value.decode(errors="replace"))
+
+    def synchronize(self):
+        self.check(self.lib.tptfem_synchronize(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tptfem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _ctx(ctx):
+    return ctx if ctx is not None else Context.default()
+
+
+class Mesh:
+    """A device-resident mesh (tptfem_mesh).  Mirrors tpt_fem.Mesh of the reference bindings."""
+
+    def __init__(self, handle, ctx):
+        self.h = handle
+        self.ctx = ctx
+        nn, ne = C.c_int64(), C.c_int64()
+        cell, cdim = C.c_int(), C.c_int()
+        ctx.check(ctx.lib.tptfem_mesh_sizes(handle, C.byref(nn), C.byref(ne), C.byref(cell), C.byref(cdim)))
+        self.n_nodes, self.n_elems, self.cell, self.cdim = nn.value, ne.value, cell.value, cdim.value
+        self._coords = None
+        self._conn = None
+
+    @staticmethod
+    def box_mesh(min, max, n, ctx=None):
+        """box_mesh(min, max, n) built on the device (crates/tpt-fem-mesh-gen/src/lib.rs:422-495)."""
+        ctx = _ctx(ctx)
+        h = C.c_void_p()
+        mn, mx, nn = N.f64(min), N.f64(max), N.i64(n)
+        ctx.check(ctx.lib.tptfem_mesh_box(ctx.h, N.ptr(mn), N.ptr(mx), N.ptr(nn), C.byref(h)))
+        return Mesh(h, ctx)
+
+    @staticmethod
+    def from_arrays(cell_type, coords, conn, ctx=None):
+        ctx = _ctx(ctx)
+        coords = N.f64(coords)
+        conn = N.i64(conn)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.tptfem_mesh_upload(ctx.h, cell_type, coords.shape[1], N.ptr(coords), coords.shape[0],
+                                             N.ptr(conn), conn.shape[0], C.byref(h)))
+        m = Mesh(h, ctx)
+        m._coords, m._conn = coords, conn
+        return m
+
+    def _download(self):
+        if self._coords is None:
+            c = np.zeros((self.n_nodes, self.cdim))
+            e = np.zeros((self.n_elems, 4), dtype=np.int64)
+            self.ctx.check(self.ctx.lib.tptfem_mesh_download(self.ctx.h, self.h, N.ptr(c), N.ptr(e)))
+            self._coords, self._conn = c, e
+
+    @property
+    def coords_array(self):
+        self._download()
+        return self._coords
+
+    @property
+    def conn_array(self):
+        self._download()
+        return self._conn
+
+    @property
+    def dim(self):
+        return 3 if self.cell == CELL_TET4 else 2
+
+    def node_count(self):
+        return self.n_nodes
+
+    def element_count(self):
+        return self.n_elems
+
+    def coords(self, i):
+        return [float(v) for v in self.coords_array[i]]
+
+    def nodes_on_plane(self, axis, coord, tol):
+        """Mesh::nodes_on_plane (crates/tpt-fem-mesh/src/lib.rs:425-431)."""
+        c = self.coords_array
+        col = c[:, axis] if axis < c.shape[1] else np.zeros(len(c))
+        return [int(i) for i in np.nonzero(np.abs(col - coord) <= tol)[0]]
+
+    def nodes_in_box(self, min, max):
+        """Mesh::nodes_in_box (crates/tpt-fem-mesh/src/lib.rs:435-447), tolerance 1e-12."""
+        c = self.coords_array
+        tol = 1e-12
+        ok = np.ones(len(c), dtype=bool)
+        for d in range(3):
+            v = c[:, d] if d < c.shape[1] else np.zeros(len(c))
+            ok &= (v >= min[d] - tol) & (v <= max[d] + tol)
+        return [int(i) for i in np.nonzero(ok)[0]]
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and self.ctx.h:
+            self.ctx.lib.tptfem_mesh_free(self.h)
+            self.h = None
+
+
+class Matrix:
+    """A device-resident CSR matrix (tptfem_matrix), equal to Coo::to_csr(assemble(...))."""
+
+    def __init__(self, handle, mesh):
+        self.h = handle
+        self.mesh = mesh
+        self.ctx = mesh.ctx
+        nr, nc, nz = C.c_int64(), C.c_int64(), C.c_int64()
+        self.ctx.check(self.ctx.lib.tptfem_matrix_sizes(handle, C.byref(nr), C.byref(nc), C.byref(nz)))
+        self.nrows, self.ncols, self.nnz = nr.value, nc.value, nz.value
+
+    def _refresh(self):
+        nr, nc, nz = C.c_int64(), C.c_int64(), C.c_int64()
+        self.ctx.check(self.ctx.lib.tptfem_matrix_sizes(self.h, C.byref(nr), C.byref(nc), C.byref(nz)))
+        self.nrows, self.ncols, self.nnz = nr.value, nc.value, nz.value
+
+    def to_csr(self):
+        """(row_ptrs, col_ind, values) as int64/int64/float64 numpy arrays."""
+        rp = np.zeros(self.nrows + 1, np.int64)
+        ci = np.zeros(self.nnz, np.int64)
+        va = np.zeros(self.nnz)
+        self.ctx.check(self.ctx.lib.tptfem_matrix_download(self.ctx.h, self.h, N.ptr(rp), N.ptr(ci), N.ptr(va)))
+        return rp, ci, va
+
+    def matvec(self, x):
+        """Csr::matvec (crates/tpt-fem-sparse/src/lib.rs:195-205), bit-exact."""
+        x = N.f64(x)
+        y = np.zeros(max(self.nrows, len(x)))
+        self.ctx.check(self.ctx.lib.tptfem_csr_matvec(self.ctx.h, self.h, N.ptr(x), len(x), N.ptr(y)))
+        return y
+
+    def reassemble(self, coef):
+        """New per-element (or constant) coefficients on the same mesh; pattern revalidated."""
+        coef = np.atleast_1d(N.f64(coef))
+        per = 1 if len(coef) > 1 or self.mesh.n_elems == 1 else 0
+        self.ctx.check(self.ctx.lib.tptfem_reassemble(self.ctx.h, self.h, N.ptr(coef), per))
+        self._refresh()
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and self.ctx.h:
+            self.ctx.lib.tptfem_matrix_free(self.h)
+            self.h = None
+
+
+def _coef(mesh, coef):
+    c = np.atleast_1d(N.f64(coef))
+    if len(c) == 1:
+        return c, 0
+    if len(c) != mesh.n_elems:
+        raise ValueError("coefficient array must hold one value per element or a single value")
+    return c, 1
+
+
+def assemble_poisson(mesh, conductivity, quad_order=2):
+    """assemble(mesh, 1, poisson_element_matrix) -> Matrix (thermal/src/lib.rs:132-160)."""
+    ctx = mesh.ctx
+    c, per = _coef(mesh, conductivity)
+    h = C.c_void_p()
+    ctx.check(ctx.lib.tptfem_assemble_poisson(ctx.h, mesh.h, N.ptr(c), per, quad_order, C.byref(h)))
+    return Matrix(h, mesh)
+
+
+_MODELS = {"bar": MODEL_BAR_AXIAL, "baraxial": MODEL_BAR_AXIAL, "planestress": MODEL_PLANE_STRESS,
+           "planestrain": MODEL_PLANE_STRAIN, "3d": MODEL_CONTINUUM_3D, "continuum": MODEL_CONTINUUM_3D,
+           "continuum3d": MODEL_CONTINUUM_3D}
+
+
+def parse_model(model):
+    """parse_model of the reference bindings (crates/tpt-fem-py/src/lib.rs:201-211)."""
+    if isinstance(model, int):
+        return model
+    key = model.lower().replace("-", "").replace("_", "")
+    if key not in _MODELS:
+        raise TptFemError(9, f"unknown elasticity model '{key}' (bar | plane-stress | plane-strain | 3d)")
+    return _MODELS[key]
+
+
+def assemble_elasticity(mesh, model, young, poisson, quad_order=2):
+    """try_assemble(mesh, dim, elasticity_element_matrix) -> Matrix (elasticity/src/lib.rs:262-309)."""
+    ctx = mesh.ctx
+    c, per = _coef(mesh, young)
+    h = C.c_void_p()
+    ctx.check(ctx.lib.tptfem_assemble_elasticity(ctx.h, mesh.h, parse_model(model), N.ptr(c), per, float(poisson),
+                                                 quad_order, C.byref(h)))
+    return Matrix(h, mesh)
+
+
+def load_poisson_source(mesh, source, quad_order=2):
+    rhs = np.zeros(mesh.n_nodes)
+    mesh.ctx.check(mesh.ctx.lib.tptfem_load_poisson_source(mesh.ctx.h, mesh.h, float(source), quad_order,
+                                                           N.ptr(rhs)))
+    return rhs
+
+
+def load_body(mesh, body, quad_order=2):
+    b = N.f64(body)
+    rhs = np.zeros(mesh.n_nodes * mesh.dim)
+    mesh.ctx.check(mesh.ctx.lib.tptfem_load_body(mesh.ctx.h, mesh.h, N.ptr(b), quad_order, N.ptr(rhs)))
+    return rhs
+
+
+def apply_traction(mesh, dofs_per_node, axis, sign, traction, rhs):
+    """rhs += apply_neumann with flux traction[c] on faces where sign*n[axis] > 0.5 (in place)."""
+    t = N.f64(traction)
+    assert rhs.dtype == np.float64 and rhs.flags["C_CONTIGUOUS"]
+    mesh.ctx.check(mesh.ctx.lib.tptfem_apply_traction(mesh.ctx.h, mesh.h, dofs_per_node, axis, float(sign),
+                                                      N.ptr(t), N.ptr(rhs)))
+    return rhs
+
+
+def _bcs(bcs):
+    if len(bcs) == 0:
+        return np.zeros(0, np.int64), np.zeros(0)
+    arr = list(bcs)
+    return N.i64([b[0] for b in arr]), N.f64([b[1] for b in arr])
+
+
+def _opts(solver=SOLVER_JACOBI_PCG, tol=1e-10, inner_tol=0.0, max_iter=0, max_outer=0, batch=0):
+    o = SolverOpts()
+    o.solver, o.rel_tol, o.inner_rel_tol, o.max_iter, o.max_outer, o.batch = solver, tol, inner_tol, max_iter, \
+        max_outer, batch
+    return o
+
+
+class System:
+    """Device-resident ReducedSystem (assembly/src/lib.rs:488-535) plus its solution."""
+
+    def __init__(self, handle, ctx, n):
+        self.h, self.ctx, self.n = handle, ctx, n
+        nf, nz = C.c_int64(), C.c_int64()
+        ctx.check(ctx.lib.tptfem_system_sizes(handle, C.byref(nf), C.byref(nz)))
+        self.n_free, self.nnz = nf.value, nz.value
+
+    def download(self):
+        """(row_ptrs, col_ind, values, fred, free)."""
+        rp = np.zeros(self.n_free + 1, np.int64)
+        ci = np.zeros(self.nnz, np.int64)
+        va = np.zeros(self.nnz)
+        fred = np.zeros(self.n_free)
+        free = np.zeros(self.n_free, np.int64)
+        self.ctx.check(self.ctx.lib.tptfem_system_download(self.ctx.h, self.h, N.ptr(rp), N.ptr(ci), N.ptr(va),
+                                                           N.ptr(fred), N.ptr(free)))
+        return rp, ci, va, fred, free
+
+    def solve(self, **kw):
+        o = _opts(**kw)
+        st = SolveStats()
+        rc = self.ctx.lib.tptfem_system_solve(self.ctx.h, self.h, C.byref(o), C.byref(st))
+        self.ctx.check(rc)
+        return st.as_dict()
+
+    def solution(self):
+        u = np.zeros(self.n)
+        self.ctx.check(self.ctx.lib.tptfem_system_solution(self.ctx.h, self.h, N.ptr(u)))
+        return u
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and self.ctx.h:
+            self.ctx.lib.tptfem_system_free(self.h)
+            self.h = None
+
+
+def reduce_system(mat, rhs, bcs):
+    ctx = mat.ctx
+    rhs = N.f64(rhs)
+    dof, val = _bcs(bcs)
+    h = C.c_void_p()
+    ctx.check(ctx.lib.tptfem_reduce_system(ctx.h, mat.h, N.ptr(rhs), len(rhs), N.ptr(dof), N.ptr(val), len(dof),
+                                           C.byref(h)))
+    return System(h, ctx, len(rhs))
+
+
+def solve_with_dirichlet(mat, rhs, bcs, **kw):
+    """solve_with_dirichlet (assembly/src/lib.rs:543-559) -> (u, stats dict)."""
+    ctx = mat.ctx
+    rhs = N.f64(rhs)
+    dof, val = _bcs(bcs)
+    u = np.zeros(len(rhs))
+    o = _opts(**kw)
+    st = SolveStats()
+    ctx.check(ctx.lib.tptfem_solve_with_dirichlet(ctx.h, mat.h, N.ptr(rhs), len(rhs), N.ptr(dof), N.ptr(val),
+                                                  len(dof), C.byref(o), N.ptr(u), C.byref(st)))
+    return u, st.as_dict()
+
+
+class PoissonSolution:
+    def __init__(self, mesh, values, stats):
+        self.mesh, self.values, self.stats = mesh, values, stats
+
+    def __len__(self):
+        return len(self.values)
+
+    def to_numpy(self):
+        return np.asarray(self.values, dtype=np.float64).reshape(self.mesh.node_count())
+
+
+class ElasticitySolution:
+    def __init__(self, mesh, values, dim, stats):
+        self.mesh, self.values, self.dim, self.stats = mesh, values, dim, stats
+
+    def __len__(self):
+        return len(self.values)
+
+    def to_numpy(self):
+        return np.asarray(self.values, dtype=np.float64).reshape(self.mesh.node_count(), self.dim)
+
+
+def solve_poisson(mesh, conductivity, quad_order, source, bcs, **kw):
+    """solve_poisson of the reference bindings (crates/tpt-fem-py/src/lib.rs:102-199), constant source."""
+    if callable(source):
+        raise NotImplementedError("callable sources: evaluate on quadrature points first")
+    ctx = mesh.ctx
+    dof, val = _bcs(bcs)
+    u = np.zeros(mesh.n_nodes)
+    o = _opts(**kw)
+    st = SolveStats()
+    ctx.check(ctx.lib.tptfem_solve_poisson(ctx.h, mesh.h, float(conductivity), quad_order, float(source),
+                                           N.ptr(dof), N.ptr(val), len(dof), C.byref(o), N.ptr(u), C.byref(st)))
+    return PoissonSolution(mesh, [float(v) for v in u], st.as_dict())
+
+
+def solve_elasticity(mesh, model, young, poisson, quad_order, bcs, body=None, **kw):
+    """solve_elasticity of the reference bindings (crates/tpt-fem-py/src/lib.rs:213-252).
+
+    ``bcs`` are (node_id, component, value) triples; zero body force unless ``body`` is given.
+    """
+    ctx = mesh.ctx
+    dim = mesh.dim
+    dofs = [(int(n) * dim + int(c), float(v)) for n, c, v in bcs]
+    dof, val = _bcs(dofs)
+    b = N.f64(body if body is not None else np.zeros(dim))
+    u = np.zeros(mesh.n_nodes * dim)
+    o = _opts(**kw)
+    st = SolveStats()
+    ctx.check(ctx.lib.tptfem_solve_elasticity(ctx.h, mesh.h, parse_model(model), float(young), float(poisson),
+                                              quad_order, N.ptr(b), N.ptr(dof), N.ptr(val), len(dof), C.byref(o),
+                                              N.ptr(u), C.byref(st)))
+    return ElasticitySolution(mesh, [float(v) for v in u], dim, st.as_dict())

@@ -1,0 +1,123 @@
+"""ctypes declarations of the C ABI in include/tptfem.h.
+
+Loads ``tpt-fem_b200/lib/libtptfem.so``.  There is no fallback: if the
+library is missing or the GPU is unusable, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libtptfem.so")
+
+OK = 0
+STATUS_NAMES = {
+    0: "OK", 1: "CREATION", 2: "SYMBOLIC", 3: "NUMERIC", 4: "MODEL_DIM_MISMATCH", 5: "NOT_CONVERGED",
+    6: "BREAKDOWN", 7: "DEVICE", 8: "TIMEOUT", 9: "INVALID_ARG", 10: "OUT_OF_MEMORY",
+}
+CELL_QUAD4, CELL_TET4 = 3, 4
+MODEL_BAR_AXIAL, MODEL_PLANE_STRESS, MODEL_PLANE_STRAIN, MODEL_CONTINUUM_3D = 0, 1, 2, 3
+SOLVER_JACOBI_PCG, SOLVER_MP_PCG = 0, 1
+
+
+class SolverOpts(C.Structure):
+    _fields_ = [("solver", C.c_int32), ("max_outer", C.c_int32), ("rel_tol", C.c_double),
+                ("inner_rel_tol", C.c_double), ("max_iter", C.c_int64), ("batch", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("iterations", C.c_int64), ("outer_steps", C.c_int32), ("solver_used", C.c_int32),
+                ("rel_residual", C.c_double), ("setup_ms", C.c_double), ("solve_ms", C.c_double),
+                ("fell_back", C.c_int32), ("reserved", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_vp = C.c_void_p
+_pp = C.POINTER(C.c_void_p)
+_i64 = C.c_int64
+_pi64 = C.POINTER(C.c_int64)
+_pd = C.POINTER(C.c_double)
+_pint = C.POINTER(C.c_int)
+
+SIGNATURES = {
+    "tptfem_version": (C.c_char_p, []),
+    "tptfem_create": (C.c_int, [C.c_int, _pp]),
+    "tptfem_destroy": (None, [_vp]),
+    "tptfem_last_error": (C.c_size_t, [_vp, C.c_char_p, C.c_size_t]),
+    "tptfem_synchronize": (C.c_int, [_vp]),
+    "tptfem_mesh_upload": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _i64, _vp, _i64, _pp]),
+    "tptfem_mesh_box": (C.c_int, [_vp, _vp, _vp, _vp, _pp]),
+    "tptfem_mesh_sizes": (C.c_int, [_vp, _pi64, _pi64, _pint, _pint]),
+    "tptfem_mesh_download": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "tptfem_mesh_free": (None, [_vp]),
+    "tptfem_assemble_poisson": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _pp]),
+    "tptfem_assemble_elasticity": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_int, C.c_double, C.c_int, _pp]),
+    "tptfem_reassemble": (C.c_int, [_vp, _vp, _vp, C.c_int]),
+    "tptfem_matrix_sizes": (C.c_int, [_vp, _pi64, _pi64, _pi64]),
+    "tptfem_matrix_download": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "tptfem_matrix_free": (None, [_vp]),
+    "tptfem_csr_matvec": (C.c_int, [_vp, _vp, _vp, _i64, _vp]),
+    "tptfem_load_poisson_source": (C.c_int, [_vp, _vp, C.c_double, C.c_int, _vp]),
+    "tptfem_load_body": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp]),
+    "tptfem_apply_traction": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_double, _vp, _vp]),
+    "tptfem_reduce_system": (C.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, _pp]),
+    "tptfem_system_sizes": (C.c_int, [_vp, _pi64, _pi64]),
+    "tptfem_system_download": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "tptfem_system_solve": (C.c_int, [_vp, _vp, C.POINTER(SolverOpts), C.POINTER(SolveStats)]),
+    "tptfem_system_solution": (C.c_int, [_vp, _vp, _vp]),
+    "tptfem_system_free": (None, [_vp]),
+    "tptfem_solve_with_dirichlet": (C.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, C.POINTER(SolverOpts), _vp,
+                                              C.POINTER(SolveStats)]),
+    "tptfem_solve_poisson": (C.c_int, [_vp, _vp, C.c_double, C.c_int, C.c_double, _vp, _vp, _i64,
+                                       C.POINTER(SolverOpts), _vp, C.POINTER(SolveStats)]),
+    "tptfem_solve_elasticity": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_double, C.c_int, _vp, _vp, _vp, _i64,
+                                          C.POINTER(SolverOpts), _vp, C.POINTER(SolveStats)]),
+}
+
+_lib = None
+
+
+def load():
+    """Load libtptfem.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libtptfem.so not found at {LIB_PATH}: run __graft_entry__.build() first")
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def declared_symbols(header=None):
+    """Function names declared in include/tptfem.h (for the export check)."""
+    import re
+    header = header or os.path.join(os.path.dirname(PKG_ROOT), "include", "tptfem.h")
+    text = open(header).read()
+    return sorted(set(re.findall(r"\b(tptfem_[a-z0-9_]+)\s*\(", text)))
+
+
+def ptr(a):
+    """Raw data pointer of a contiguous numpy array (or None)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def i64(a):
+    return np.ascontiguousarray(a, dtype=np.int64)

@@ -1,0 +1,68 @@
+"""Seeded synthetic inputs for the benchmark configurations.
+
+No dataset exists for this path; every input is generated here with a fixed
+seed, with the shapes and value distributions the benchmark configurations
+name:
+  * elasticity cantilever on box_mesh [0,L]x[0,1]x[0,1]: per-brick density
+    rho ~ U[0,1], 3x3x3 box-filter mean truncated at the boundary,
+    E = 1e-3 + (1 - 1e-3) * rho^3 per tet (6 tets per brick), nu = 0.3,
+    x = 0 clamped, uniform traction (0, 0, -1e-3) on x = L;
+  * the unit-cube elasticity case (E = 1) with the same clamp and traction.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def smoothed_density(n, seed):
+    """rho ~ U[0,1] per brick, then the mean over the 3x3x3 neighbourhood that lies inside the box."""
+    nx, ny, nz = n
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(0.0, 1.0, size=(nx, ny, nz))
+    pad = np.pad(r, 1)
+    one = np.pad(np.ones_like(r), 1)
+    s = np.zeros_like(r)
+    c = np.zeros_like(r)
+    for di in range(3):
+        for dj in range(3):
+            for dk in range(3):
+                s += pad[di:di + nx, dj:dj + ny, dk:dk + nz]
+                c += one[di:di + nx, dj:dj + ny, dk:dk + nz]
+    return s / c
+
+
+def simp_young(rho, emin=1e-3, p=3.0):
+    return emin + (1.0 - emin) * rho ** p
+
+
+def per_tet(brick_values):
+    """box_mesh numbers bricks (i, j, k) with k fastest and emits 6 tets per brick in order."""
+    return np.repeat(brick_values.reshape(-1), 6)
+
+
+def cantilever_young(n, seed=2024):
+    return per_tet(simp_young(smoothed_density(n, seed)))
+
+
+def clamp_x0_bcs(coords, dpn=3, tol=1e-9):
+    nodes = np.nonzero(np.abs(coords[:, 0]) <= tol)[0]
+    dof = (nodes[:, None] * dpn + np.arange(dpn)[None, :]).reshape(-1).astype(np.int64)
+    return dof, np.zeros(len(dof))
+
+
+def box_coords(mn, mx, n):
+    """box_mesh node coordinates (k fastest), the same values the device mesher writes."""
+    nx, ny, nz = n
+    i, j, k = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+    t = i.reshape(-1) / nx
+    u = j.reshape(-1) / ny
+    w = k.reshape(-1) / nz
+    return np.stack([mn[0] + t * (mx[0] - mn[0]), mn[1] + u * (mx[1] - mn[1]), mn[2] + w * (mx[2] - mn[2])], axis=1)
+
+
+CANTILEVERS = {
+    "cantilever_200x50x50": ([0.0, 0.0, 0.0], [4.0, 1.0, 1.0], [200, 50, 50]),
+    "cantilever_280x70x70": ([0.0, 0.0, 0.0], [4.0, 1.0, 1.0], [280, 70, 70]),
+    "cantilever_400x100x100": ([0.0, 0.0, 0.0], [4.0, 1.0, 1.0], [400, 100, 100]),
+    "cube_elasticity_64": ([0.0, 0.0, 0.0], [1.0, 1.0, 1.0], [64, 64, 64]),
+}
