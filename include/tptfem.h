@@ -62,8 +62,14 @@ enum {
 enum {
   /* FP64 Jacobi-preconditioned CG: the plain method and the fallback. */
   TPTFEM_SOLVER_JACOBI_PCG = 0,
-  /* FP32 Jacobi-PCG inner solves inside FP64 iterative refinement. */
-  TPTFEM_SOLVER_MP_PCG = 1
+  /* Mixed precision: FP32 matrix, vectors and Jacobi preconditioner inside
+   * FP64 reliable updates (true residual b - A x and solution in FP64). */
+  TPTFEM_SOLVER_MP_PCG = 1,
+  /* FP64 Krylov (operator, vectors, reliable updates) preconditioned by the
+   * factorised sparse approximate inverse M^-1 = G^T G, G = diag(s)(I + L) on
+   * the lower node-block pattern of the reduced matrix, classic FSAI values,
+   * the factor stored and applied in reduced precision (s^2 FP32, L FP16). */
+  TPTFEM_SOLVER_FSAI_MP_PCG = 2
 };
 
 typedef struct tptfem_context tptfem_context;
@@ -73,20 +79,25 @@ typedef struct tptfem_system tptfem_system;
 
 typedef struct tptfem_solver_opts {
   int32_t solver;        /* TPTFEM_SOLVER_* */
-  int32_t max_outer;     /* MP: refinement steps cap (0 -> 50) */
+  int32_t max_outer;     /* unused, kept 0 */
   double rel_tol;        /* stop at ||b - A x||_2 / ||b||_2 <= rel_tol, FP64 (0 -> 1e-10) */
-  double inner_rel_tol;  /* MP: inner FP32 reduction per refinement step (0 -> 1e-4) */
+  double inner_rel_tol;  /* reliable-update trigger: FP64 residual replacement once the
+                            recursive residual fell by this factor (0 -> 1e-3 FP64, 5e-2 FP32) */
   int64_t max_iter;      /* cap on total PCG iterations (0 -> 100000) */
   int32_t batch;         /* PCG iterations per CUDA-graph launch (0 -> auto) */
-  int32_t reserved;
+  int32_t flags;         /* TPTFEM_SOLVE_* bits */
 } tptfem_solver_opts;
+
+/* Recompute the preconditioner's values inside this solve (they are otherwise
+ * kept on the system from its first solve); its sparsity pattern is kept. */
+#define TPTFEM_SOLVE_FRESH_SETUP 1
 
 typedef struct tptfem_solve_stats {
   int64_t iterations;    /* total PCG iterations (inner iterations for MP) */
-  int32_t outer_steps;   /* refinement steps (1 for FP64 Jacobi-PCG) */
+  int32_t outer_steps;   /* FP64 true-residual (reliable) updates performed */
   int32_t solver_used;   /* TPTFEM_SOLVER_* actually run (after any fallback) */
   double rel_residual;   /* final TRUE residual ||b - A x||_2/||b||_2 in FP64 */
-  double setup_ms;       /* preconditioner set-up, device time */
+  double setup_ms;       /* preconditioner set-up, device time (first solve of a system) */
   double solve_ms;       /* iterations + residual checks, device time */
   int32_t fell_back;     /* 1 if the requested method fell back to FP64 Jacobi-PCG */
   int32_t reserved;
@@ -171,6 +182,19 @@ tptfem_status tptfem_system_solve(tptfem_context* ctx, tptfem_system* sys, const
 /* Full-length solution as solve_with_dirichlet returns it (crates/tpt-fem-assembly/src/lib.rs:549-558). */
 tptfem_status tptfem_system_solution(tptfem_context* ctx, const tptfem_system* sys, double* u);
 void tptfem_system_free(tptfem_system* sys);
+/* FSAI factor of the reduced system (no reference counterpart): builds the
+ * classic factor once (kept on the system) and returns nnz of L.  The
+ * download gives L (CSR, strictly lower, values widened from FP16) and
+ * sigma^2 (n_free values, widened from FP32); M^-1 = G^T G with
+ * G = diag(sigma)(I + L). */
+tptfem_status tptfem_system_fsai(tptfem_context* ctx, tptfem_system* sys, int64_t* nnz_l);
+tptfem_status tptfem_system_fsai_download(tptfem_context* ctx, const tptfem_system* sys, int64_t* l_row_ptrs,
+                                          int64_t* l_col_ind, double* l_values, double* sigma2);
+/* Diagnostic (no reference counterpart): average device time in ms of the
+ * solver's FP64 and FP32 CSR SpMV kernels on this system, `reps` launches each,
+ * timed with CUDA events on the context's stream.  Used for roofline reports. */
+tptfem_status tptfem_system_profile_spmv(tptfem_context* ctx, tptfem_system* sys, int reps, double* ms_f64,
+                                         double* ms_f32);
 
 /* solve_with_dirichlet (crates/tpt-fem-assembly/src/lib.rs:543-559): reduce, solve, scatter. */
 tptfem_status tptfem_solve_with_dirichlet(tptfem_context* ctx, const tptfem_matrix* mat, const double* rhs,

@@ -1006,6 +1006,61 @@ int orc_cell_quad(int cell, int order, double* pts, double* w) {
   return (int)p.size();
 }
 
+// ---- classic FSAI ----------------------------------------------------------------
+// NOT reference code (the reference has no iterative solver): CPU restatement
+// of Kolotilina-Yeremin FSAI on the lower-triangular pattern, the checker for
+// the device factor.  Row i: P = { j <= i in row i }, solve A[P,P] y = e_last
+// by dense Cholesky, G[i,P] = y / sqrt(y_last).  Returns nullptr when a
+// principal block is not positive definite.
+// lrp/lci: the strictly-lower pattern of each row (nullptr: tril(A) minus the
+// diagonal).  Output: CSR of G itself (pattern + diagonal, values y/sqrt(y_i)).
+OrcCsr* orc_fsai(i64 n, const i64* rp, const i64* ci, const double* va, const i64* lrp, const i64* lci) {
+  OrcCsr* o = new OrcCsr;
+  o->c.nrows = n; o->c.ncols = n;
+  o->c.row_ptrs.assign(n + 1, 0);
+  auto lookup = [&](i64 r, i64 c) {
+    const i64* b = ci + rp[r];
+    const i64* e = ci + rp[r + 1];
+    const i64* it = std::lower_bound(b, e, c);
+    return (it != e && *it == c) ? va[rp[r] + (it - b)] : 0.0;
+  };
+  for (i64 i = 0; i < n; ++i) {
+    vector<i64> P;
+    if (lrp) {
+      for (i64 k = lrp[i]; k < lrp[i + 1]; ++k) P.push_back(lci[k]);
+    } else {
+      for (i64 k = rp[i]; k < rp[i + 1]; ++k) if (ci[k] < i) P.push_back(ci[k]);
+    }
+    P.push_back(i);
+    size_t m = P.size();
+    vector<double> L(m * m, 0.0);
+    for (size_t a = 0; a < m; ++a)
+      for (size_t b = 0; b <= a; ++b) L[a * m + b] = lookup(P[a], P[b]);
+    for (size_t a = 0; a < m; ++a)
+      for (size_t b = 0; b <= a; ++b) {
+        double s = L[a * m + b];
+        for (size_t t = 0; t < b; ++t) s -= L[a * m + t] * L[b * m + t];
+        if (a == b) {
+          if (!(s > 0.0)) { delete o; g_err = "FSAI block not positive definite"; return nullptr; }
+          L[a * m + a] = std::sqrt(s);
+        } else {
+          L[a * m + b] = s / L[b * m + b];
+        }
+      }
+    vector<double> y(m, 0.0);
+    y[m - 1] = 1.0 / L[(m - 1) * m + (m - 1)];
+    for (i64 a = (i64)m - 1; a >= 0; --a) {
+      double s = y[a];
+      for (size_t t = a + 1; t < m; ++t) s -= L[t * m + a] * y[t];
+      y[a] = s / L[a * m + a];
+    }
+    double sc = 1.0 / std::sqrt(y[m - 1]);
+    for (size_t a = 0; a < m; ++a) { o->c.col_ind.push_back(P[a]); o->c.values.push_back(y[a] * sc); }
+    o->c.row_ptrs[i + 1] = (i64)o->c.col_ind.size();
+  }
+  return o;
+}
+
 int orc_max_threads() {
 #ifdef _OPENMP
   return omp_get_max_threads();

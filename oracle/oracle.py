@@ -86,6 +86,7 @@ def lib():
         "orc_max_threads": (C.c_int, []),
         "orc_map": (None, [C.c_int, _f64p, C.c_int, C.c_int, _f64p, _f64p, C.POINTER(C.c_double), _f64p]),
         "orc_cell_quad": (C.c_int, [C.c_int, C.c_int, _f64p, _f64p]),
+        "orc_fsai": (_vp, [_i64, _i64p, _i64p, _f64p, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -370,6 +371,55 @@ def cell_quad(cell, order):
     pts = np.zeros((64, rd)); w = np.zeros(64)
     nq = lib().orc_cell_quad(cell, order, pts, w)
     return pts[:nq].copy(), w[:nq].copy()
+
+
+def node_block_lower_pattern(csr, free, dpn):
+    """Strictly-lower node-block pattern of a reduced matrix (not reference code).
+
+    Row i may use every free dof j < i of every mesh node coupled in `csr` to
+    the node of i (nodes = full dof // dpn; `free` maps reduced -> full dof).
+    Returns (row_ptrs, col_ind) int64.
+    """
+    n = csr.nrows
+    node = np.asarray(free) // dpn
+    red = {int(g): i for i, g in enumerate(free)}
+    rows = []
+    i = 0
+    while i < n:
+        g1 = i
+        while g1 < n and node[g1] == node[i]:
+            g1 += 1
+        nodes = set()
+        for g in range(i, g1):
+            nodes |= set(int(v) for v in node[csr.col_ind[csr.row_ptrs[g]:csr.row_ptrs[g + 1]]])
+        cand = sorted(red[m * dpn + c] for m in nodes for c in range(dpn) if (m * dpn + c) in red)
+        for g in range(i, g1):
+            rows.append([j for j in cand if j < g])
+        i = g1
+    rp = np.zeros(n + 1, np.int64)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    ci = np.array([j for r in rows for j in r], dtype=np.int64)
+    return rp, ci
+
+
+def fsai(csr, pattern=None):
+    """Classic FSAI factor G (CSR incl. diagonal) of an SPD CSR matrix (not reference code).
+
+    pattern: optional (row_ptrs, col_ind) of the strictly-lower pattern; default tril(A).
+    """
+    if pattern is None:
+        h = lib().orc_fsai(csr.nrows, csr.row_ptrs, csr.col_ind, csr.values, None, None)
+    else:
+        lrp = np.ascontiguousarray(pattern[0], dtype=np.int64)
+        lci = np.ascontiguousarray(pattern[1], dtype=np.int64)
+        h = lib().orc_fsai(csr.nrows, csr.row_ptrs, csr.col_ind, csr.values, lrp.ctypes.data_as(C.c_void_p),
+                           lci.ctypes.data_as(C.c_void_p))
+    if not h:
+        raise OracleError(_err())
+    try:
+        return Csr._from_handle(h)
+    finally:
+        lib().orc_csr_free(h)
 
 
 def max_threads():

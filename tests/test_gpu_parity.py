@@ -204,7 +204,7 @@ def test_reduce_system_bit_exact(ctx):
     assert np.array_equal(rp, kc.row_ptrs) and np.array_equal(ci, kc.col_ind) and np.array_equal(va, kc.values)
 
 
-@pytest.mark.parametrize("solver", [F.SOLVER_JACOBI_PCG, F.SOLVER_MP_PCG])
+@pytest.mark.parametrize("solver", [F.SOLVER_JACOBI_PCG, F.SOLVER_MP_PCG, F.SOLVER_FSAI_MP_PCG])
 def test_config1_solution_vs_dense_lu(ctx, solver):
     c, e = box([8, 8, 8])
     m = F.Mesh.box_mesh([0, 0, 0], [1, 1, 1], [8, 8, 8], ctx=ctx)
@@ -229,10 +229,46 @@ def test_elasticity_solution_vs_dense_lu(ctx):
     bcs = [(3 * n + k, 0.0) for n in x0 for k in range(3)]
     coo = O.assemble_elasticity(O.Mesh(O.CELL_TET, c, e), O.MODEL_3D, E, 0.3, 2)
     u_ref = O.solve_with_dirichlet(coo, rhs, bcs)
-    for solver in (F.SOLVER_JACOBI_PCG, F.SOLVER_MP_PCG):
+    for solver in (F.SOLVER_JACOBI_PCG, F.SOLVER_MP_PCG, F.SOLVER_FSAI_MP_PCG):
         u, st = F.solve_with_dirichlet(K, rhs, bcs, solver=solver, tol=1e-13)
-        assert st["rel_residual"] <= 1e-13
+        assert st["rel_residual"] <= 1e-13 and st["solver_used"] == solver and not st["fell_back"]
         assert np.max(np.abs(u - u_ref)) <= 1e-10 * np.max(np.abs(u_ref))
+
+
+def _fsai_vs_oracle(S, dpn):
+    lrp, lci, lva, s2 = S.fsai()
+    rp, ci, va, fred, free = S.download()
+    csr = O.Csr(S.n_free, S.n_free, rp, ci, va)
+    prp, pci = O.node_block_lower_pattern(csr, free, dpn)
+    assert np.array_equal(lrp, prp) and np.array_equal(lci, pci)
+    G = O.fsai(csr, (prp, pci))
+    diag = G.values[G.row_ptrs[1:] - 1]  # the diagonal closes each row
+    assert np.allclose(s2, diag ** 2, rtol=2e-7, atol=0)
+    off = np.concatenate([G.values[G.row_ptrs[i]:G.row_ptrs[i + 1] - 1] / diag[i] for i in range(S.n_free)])
+    want = off.astype(np.float16).astype(np.float64)
+    assert np.all(np.abs(lva - want) <= 1e-3 * np.abs(want) + 1e-7)
+
+
+def test_fsai_factor_elasticity_matches_oracle(ctx):
+    c, e = box([4, 3, 3], mx=(2.0, 1.0, 1.0))
+    c = jitter(c, 0.03, 21)
+    E = np.random.default_rng(22).uniform(0.01, 1.0, len(e))
+    m = F.Mesh.from_arrays(F.CELL_TET4, c, e, ctx=ctx)
+    K = F.assemble_elasticity(m, "3d", E, 0.3, 2)
+    x0 = [int(i) for i in O.nodes_on_plane(c, 0, 0.0, 1e-9)]
+    # clamp x=0 and one component of one extra node: partial nodes must work
+    bcs = [(3 * n + k, 0.0) for n in x0 for k in range(3)] + [(3 * (len(c) - 1) + 1, 0.0)]
+    S = F.reduce_system(K, np.ones(K.nrows), bcs)
+    _fsai_vs_oracle(S, 3)
+
+
+def test_fsai_factor_poisson_is_tril_pattern(ctx):
+    c, e = box([5, 5, 4])
+    c = jitter(c, 0.03, 23)
+    m = F.Mesh.from_arrays(F.CELL_TET4, c, e, ctx=ctx)
+    K = F.assemble_poisson(m, np.exp(np.random.default_rng(24).normal(size=len(e))), 2)
+    S = F.reduce_system(K, np.ones(K.nrows), unit_cube_bcs(c))
+    _fsai_vs_oracle(S, 1)
 
 
 def test_quad_linear_patch_reproduced(ctx):

@@ -451,6 +451,34 @@ tptfem_status tptfem_system_solution(tptfem_context* ctx, const tptfem_system* s
 
 void tptfem_system_free(tptfem_system* sys) { delete sys; }
 
+tptfem_status tptfem_system_fsai(tptfem_context* ctx, tptfem_system* sys, int64_t* nnz_l) {
+  if (!ctx || !sys || !sys->d || !nnz_l) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  const int64_t nnz = system_fsai_classic(*sys->d);
+  TPT_REQUIRE(nnz >= 0, TPTFEM_ERR_NUMERIC, "FSAI factor failed (a principal block is not SPD or a row is too long)");
+  *nnz_l = nnz;
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_system_fsai_download(tptfem_context* ctx, const tptfem_system* sys, int64_t* l_row_ptrs,
+                                          int64_t* l_col_ind, double* l_values, double* sigma2) {
+  if (!ctx || !sys || !sys->d) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  system_fsai_download(*sys->d, l_row_ptrs, l_col_ind, l_values, sigma2);
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_system_profile_spmv(tptfem_context* ctx, tptfem_system* sys, int reps, double* ms_f64,
+                                         double* ms_f32) {
+  if (!ctx || !sys || !sys->d || !ms_f64 || !ms_f32 || reps < 1) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  system_profile_spmv(*sys->d, reps, ms_f64, ms_f32);
+  API_CATCH(ctx)
+}
+
 tptfem_status tptfem_solve_with_dirichlet(tptfem_context* ctx, const tptfem_matrix* mat, const double* rhs,
                                           int64_t n, const int64_t* bc_dof, const double* bc_val, int64_t nbc,
                                           const tptfem_solver_opts* opts, double* u, tptfem_solve_stats* stats) {

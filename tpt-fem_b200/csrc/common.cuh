@@ -1,5 +1,6 @@
 // common.cuh -- internal plumbing shared by the tptfem CUDA sources.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 

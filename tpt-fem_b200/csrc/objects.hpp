@@ -58,10 +58,24 @@ struct MatrixData {
 
 struct SolverWork;  // solver.cu
 
+// FSAI factor G = diag(sigma) (I + L): sigma^2 (FP32, one per row) and the
+// strictly lower L (FP16, CSR) with its explicit transpose (CSR, FP16);
+// perm[k_t] = index in L of transposed entry k_t.
+struct FsaiFactor {
+  int64_t n = 0, nnz = 0;
+  bool ready_pattern = false;
+  bool overflow = false;  // some pattern row exceeded the device limit
+  DevBuf<int> rp, ci, trp, tci, perm;
+  DevBuf<float> sigma2;
+  DevBuf<__half> va, tva;
+};
+
 struct SystemData {
   tptfem_context* ctx = nullptr;
   int64_t n = 0, n_free = 0, nnz = 0;
+  int dpn = 1;            // dofs per mesh node of the full system
   DevBuf<int> free_map;   // reduced -> full
+  DevBuf<int> red_map;    // full -> reduced, -1 for fixed dofs
   DevBuf<int> row_ptr, col;
   DevBuf<double> val;
   DevBuf<float> val32;    // lazily converted FP32 copy for mixed precision
@@ -90,7 +104,18 @@ std::unique_ptr<SystemData> reduce_system(tptfem_context* ctx, const MatrixData&
                                           const int64_t* bc_dof, const double* bc_val, int64_t nbc);
 void system_solution(const SystemData& S, double* d_u);
 
+// fsai.cu
+struct SystemData;
+void fsai_build_pattern(const SystemData& S, FsaiFactor& F);
+bool fsai_classic(const SystemData& S, FsaiFactor& F);
+// Install FP64 device values (sigma^2 per row, L per pattern entry); false if
+// a value is not finite / positive or outside the FP16 range.
+bool fsai_set_values(const SystemData& S, FsaiFactor& F, const double* d_sig2, const double* d_lva);
+
 // solver.cu
+int64_t system_fsai_classic(SystemData& S);  // builds (once) the classic factor; -1 on failure
+void system_fsai_download(const SystemData& S, int64_t* rp, int64_t* ci, double* lva, double* sig2);
+void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32);
 void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats& st);
 
 }  // namespace tptfem

@@ -82,6 +82,12 @@ __global__ void reduced_fill(const int* __restrict__ rp, const int* __restrict__
   fred[i] = r;
 }
 
+__global__ void reduced_index(const int* __restrict__ first, const int* __restrict__ red, int64_t n,
+                              int* __restrict__ red_map) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) red_map[i] = first[i] == INT_MAX ? red[i] : -1;
+}
+
 __global__ void fixed_values(const int* __restrict__ last, const double* __restrict__ bc_val, int64_t n,
                              double* __restrict__ u_fixed) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -109,6 +115,7 @@ std::unique_ptr<SystemData> reduce_system(tptfem_context* ctx, const MatrixData&
   auto S = std::make_unique<SystemData>();
   S->ctx = ctx;
   S->n = n;
+  S->dpn = A.dpn;
   DevBuf<int> dof, first, last, red, cnt;
   DevBuf<double> val;
   dof.alloc(nbc, s);
@@ -130,6 +137,9 @@ std::unique_ptr<SystemData> reduce_system(tptfem_context* ctx, const MatrixData&
   S->n_free = exclusive_scan_i32(cnt.p, red.p, n, s);
   S->free_map.alloc(S->n_free, s);
   free_lists<<<ceil_div(n, 256), 256, 0, s>>>(first.p, red.p, n, S->free_map.p);
+  TPT_CHECK_LAUNCH();
+  S->red_map.alloc(n, s);
+  reduced_index<<<ceil_div(n, 256), 256, 0, s>>>(first.p, red.p, n, S->red_map.p);
   TPT_CHECK_LAUNCH();
   DevBuf<int> rcnt;
   rcnt.alloc(S->n_free + 1, s);

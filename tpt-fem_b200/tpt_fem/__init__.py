@@ -18,13 +18,15 @@ import numpy as np
 
 from . import _native as N
 from ._native import (CELL_QUAD4, CELL_TET4, MODEL_BAR_AXIAL, MODEL_CONTINUUM_3D, MODEL_PLANE_STRAIN,
-                      MODEL_PLANE_STRESS, SOLVER_JACOBI_PCG, SOLVER_MP_PCG, SolverOpts, SolveStats)
+                      MODEL_PLANE_STRESS, SOLVER_FSAI_MP_PCG, SOLVER_JACOBI_PCG, SOLVER_MP_PCG, SolverOpts,
+                      SolveStats)
 
 __all__ = [
     "TptFemError", "Context", "Mesh", "Matrix", "System", "assemble_poisson", "assemble_elasticity",
     "load_poisson_source", "load_body", "apply_traction", "reduce_system", "solve_with_dirichlet",
     "solve_poisson", "solve_elasticity", "SolverOpts", "SolveStats", "CELL_TET4", "CELL_QUAD4",
     "MODEL_CONTINUUM_3D", "MODEL_PLANE_STRESS", "MODEL_PLANE_STRAIN", "SOLVER_JACOBI_PCG", "SOLVER_MP_PCG",
+    "SOLVER_FSAI_MP_PCG",
 ]
 
 
@@ -285,10 +287,11 @@ def _bcs(bcs):
     return N.i64([b[0] for b in arr]), N.f64([b[1] for b in arr])
 
 
-def _opts(solver=SOLVER_JACOBI_PCG, tol=1e-10, inner_tol=0.0, max_iter=0, max_outer=0, batch=0):
+def _opts(solver=SOLVER_JACOBI_PCG, tol=1e-10, inner_tol=0.0, max_iter=0, max_outer=0, batch=0, fresh_setup=False):
     o = SolverOpts()
     o.solver, o.rel_tol, o.inner_rel_tol, o.max_iter, o.max_outer, o.batch = solver, tol, inner_tol, max_iter, \
         max_outer, batch
+    o.flags = N.SOLVE_FRESH_SETUP if fresh_setup else 0
     return o
 
 
@@ -318,6 +321,24 @@ class System:
         rc = self.ctx.lib.tptfem_system_solve(self.ctx.h, self.h, C.byref(o), C.byref(st))
         self.ctx.check(rc)
         return st.as_dict()
+
+    def profile_spmv(self, reps=20):
+        """Average device ms of the solver's FP64 and FP32 SpMV kernels on this system."""
+        a, b = C.c_double(), C.c_double()
+        self.ctx.check(self.ctx.lib.tptfem_system_profile_spmv(self.ctx.h, self.h, reps, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def fsai(self):
+        """Classic FSAI factor: (L row_ptrs, L cols, L values, sigma^2); G = diag(sigma)(I + L)."""
+        nnz = C.c_int64()
+        self.ctx.check(self.ctx.lib.tptfem_system_fsai(self.ctx.h, self.h, C.byref(nnz)))
+        rp = np.zeros(self.n_free + 1, np.int64)
+        ci = np.zeros(nnz.value, np.int64)
+        va = np.zeros(nnz.value)
+        s2 = np.zeros(self.n_free)
+        self.ctx.check(self.ctx.lib.tptfem_system_fsai_download(self.ctx.h, self.h, N.ptr(rp), N.ptr(ci), N.ptr(va),
+                                                                N.ptr(s2)))
+        return rp, ci, va, s2
 
     def solution(self):
         u = np.zeros(self.n)

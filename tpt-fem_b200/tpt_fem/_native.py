@@ -20,13 +20,14 @@ STATUS_NAMES = {
 }
 CELL_QUAD4, CELL_TET4 = 3, 4
 MODEL_BAR_AXIAL, MODEL_PLANE_STRESS, MODEL_PLANE_STRAIN, MODEL_CONTINUUM_3D = 0, 1, 2, 3
-SOLVER_JACOBI_PCG, SOLVER_MP_PCG = 0, 1
+SOLVER_JACOBI_PCG, SOLVER_MP_PCG, SOLVER_FSAI_MP_PCG = 0, 1, 2
+SOLVE_FRESH_SETUP = 1
 
 
 class SolverOpts(C.Structure):
     _fields_ = [("solver", C.c_int32), ("max_outer", C.c_int32), ("rel_tol", C.c_double),
                 ("inner_rel_tol", C.c_double), ("max_iter", C.c_int64), ("batch", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("flags", C.c_int32)]
 
 
 class SolveStats(C.Structure):
@@ -72,6 +73,9 @@ SIGNATURES = {
     "tptfem_system_solve": (C.c_int, [_vp, _vp, C.POINTER(SolverOpts), C.POINTER(SolveStats)]),
     "tptfem_system_solution": (C.c_int, [_vp, _vp, _vp]),
     "tptfem_system_free": (None, [_vp]),
+    "tptfem_system_profile_spmv": (C.c_int, [_vp, _vp, C.c_int, _pd, _pd]),
+    "tptfem_system_fsai": (C.c_int, [_vp, _vp, _pi64]),
+    "tptfem_system_fsai_download": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "tptfem_solve_with_dirichlet": (C.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, C.POINTER(SolverOpts), _vp,
                                               C.POINTER(SolveStats)]),
     "tptfem_solve_poisson": (C.c_int, [_vp, _vp, C.c_double, C.c_int, C.c_double, _vp, _vp, _i64,
