@@ -196,6 +196,29 @@ tptfem_status tptfem_system_fsai_download(tptfem_context* ctx, const tptfem_syst
 tptfem_status tptfem_system_profile_spmv(tptfem_context* ctx, tptfem_system* sys, int reps, double* ms_f64,
                                          double* ms_f32);
 
+/* Allocation-free check of a solution (no counterpart in the reference):
+ * relative residual ||b - A x||_2 / ||b||_2 of an n x n CSR system whose arrays
+ * (int32 row_ptrs[n+1] and col_ind, FP64 values, x[n], b[n]) are DEVICE memory
+ * owned by the caller, computed with compensated FP64 accumulation like the
+ * solver's own stopping test.  The result is written to the host double
+ * *rel_residual (||r||_2 itself when ||b||_2 = 0).
+ * For callers that must not let a library allocate device memory -- e.g. an
+ * application holding the whole GPU under a fixed memory budget, or a time-step
+ * loop that cannot absorb the device-wide synchronisation of cudaMalloc/cudaFree
+ * on every call.  It calls no cudaMalloc, cudaFree or allocating routine: its
+ * only scratch is a static 16,448-byte device array (2048 partial sums plus
+ * counters), resident on every GPU that loads the library until exit.
+ * Limits: 1 <= n <= 2147483646; column indices must lie in [0, n) (checked on
+ * the device: TPTFEM_ERR_INVALID_ARG).  `stream` is a cudaStream_t (NULL: the
+ * default stream); the call synchronises it before returning.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress) and
+ * should come before any stream capture.  Every call shares the array: calls
+ * whose kernels overlap on the GPU race and must be serialised by the caller.
+ * `err` (may be NULL) receives a message of at most err_len bytes. */
+tptfem_status tptfem_rel_residual_noalloc(int device, void* stream, int64_t n, const int32_t* row_ptrs,
+                                          const int32_t* col_ind, const double* values, const double* x,
+                                          const double* b, double* rel_residual, char* err, size_t err_len);
+
 /* solve_with_dirichlet (crates/tpt-fem-assembly/src/lib.rs:543-559): reduce, solve, scatter. */
 tptfem_status tptfem_solve_with_dirichlet(tptfem_context* ctx, const tptfem_matrix* mat, const double* rhs,
                                           int64_t n, const int64_t* bc_dof, const double* bc_val, int64_t nbc,

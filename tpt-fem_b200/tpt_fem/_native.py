@@ -75,6 +75,8 @@ SIGNATURES = {
     "tptfem_system_free": (None, [_vp]),
     "tptfem_system_profile_spmv": (C.c_int, [_vp, _vp, C.c_int, _pd, _pd]),
     "tptfem_system_fsai": (C.c_int, [_vp, _vp, _pi64]),
+    "tptfem_rel_residual_noalloc": (C.c_int, [C.c_int, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _pd, C.c_char_p,
+                                              C.c_size_t]),
     "tptfem_system_fsai_download": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "tptfem_solve_with_dirichlet": (C.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, C.POINTER(SolverOpts), _vp,
                                               C.POINTER(SolveStats)]),
