@@ -91,6 +91,9 @@ typedef struct tptfem_solver_opts {
 /* Recompute the preconditioner's values inside this solve (they are otherwise
  * kept on the system from its first solve); its sparsity pattern is kept. */
 #define TPTFEM_SOLVE_FRESH_SETUP 1
+/* Keep the scalar CSR operator and factor even where the node-block layout
+ * applies (for A/B measurements; must be given on a system's first solve). */
+#define TPTFEM_SOLVE_CSR_ONLY 2
 
 typedef struct tptfem_solve_stats {
   int64_t iterations;    /* total PCG iterations (inner iterations for MP) */
@@ -191,10 +194,12 @@ tptfem_status tptfem_system_fsai(tptfem_context* ctx, tptfem_system* sys, int64_
 tptfem_status tptfem_system_fsai_download(tptfem_context* ctx, const tptfem_system* sys, int64_t* l_row_ptrs,
                                           int64_t* l_col_ind, double* l_values, double* sigma2);
 /* Diagnostic (no reference counterpart): average device time in ms of the
- * solver's FP64 and FP32 CSR SpMV kernels on this system, `reps` launches each,
- * timed with CUDA events on the context's stream.  Used for roofline reports. */
+ * solver's SpMV kernels on this system -- FP64 CSR, FP32 CSR and FP64 node-block
+ * sliced-ELL (-1 when the system has partial node groups; *nb_bytes = the bytes
+ * that layout moves per launch) -- `reps` launches each, timed with CUDA events
+ * on the context's stream.  Used for roofline reports. */
 tptfem_status tptfem_system_profile_spmv(tptfem_context* ctx, tptfem_system* sys, int reps, double* ms_f64,
-                                         double* ms_f32);
+                                         double* ms_f32, double* ms_nb_f64, double* nb_bytes);
 
 /* Allocation-free check of a solution (no counterpart in the reference):
  * relative residual ||b - A x||_2 / ||b||_2 of an n x n CSR system whose arrays

@@ -271,6 +271,29 @@ def test_fsai_factor_poisson_is_tril_pattern(ctx):
     _fsai_vs_oracle(S, 1)
 
 
+@pytest.mark.parametrize("solver", [F.SOLVER_JACOBI_PCG, F.SOLVER_FSAI_MP_PCG])
+def test_node_block_layout_matches_scalar_csr(ctx, solver):
+    # The node-block operator/factor (used when every free node has all dofs
+    # free) must give the same solution as the scalar-CSR path.
+    c, e = box([6, 3, 3], mx=(2.0, 1.0, 1.0))
+    c = jitter(c, 0.03, 41)
+    E = np.random.default_rng(42).uniform(0.05, 1.0, len(e))
+    m = F.Mesh.from_arrays(F.CELL_TET4, c, e, ctx=ctx)
+    K = F.assemble_elasticity(m, "3d", E, 0.3, 2)
+    rhs = F.apply_traction(m, 3, 0, 1.0, [0.0, 0.0, -1e-3], np.zeros(K.nrows))
+    x0 = [int(i) for i in O.nodes_on_plane(c, 0, 0.0, 1e-9)]
+    bcs = [(3 * n + k, 0.0) for n in x0 for k in range(3)]
+    S1 = F.reduce_system(K, rhs, bcs)
+    S2 = F.reduce_system(K, rhs, bcs)
+    st1 = S1.solve(solver=solver, tol=1e-12)
+    st2 = S2.solve(solver=solver, tol=1e-12, csr_only=True)
+    u1, u2 = S1.solution(), S2.solution()
+    assert st1["rel_residual"] <= 1e-12 and st2["rel_residual"] <= 1e-12
+    assert abs(st1["iterations"] - st2["iterations"]) <= max(3, st2["iterations"] // 20)
+    assert np.max(np.abs(u1 - u2)) <= 1e-9 * np.max(np.abs(u2))
+    assert S1.profile_spmv(2)[2] > 0  # the node-block layout was built
+
+
 def test_quad_linear_patch_reproduced(ctx):
     # u = x + y is harmonic: P1/Q1 reproduce it exactly on a distorted mesh.
     c, e = quad_grid(6, 5)

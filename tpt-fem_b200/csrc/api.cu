@@ -471,11 +471,13 @@ tptfem_status tptfem_system_fsai_download(tptfem_context* ctx, const tptfem_syst
 }
 
 tptfem_status tptfem_system_profile_spmv(tptfem_context* ctx, tptfem_system* sys, int reps, double* ms_f64,
-                                         double* ms_f32) {
-  if (!ctx || !sys || !sys->d || !ms_f64 || !ms_f32 || reps < 1) return TPTFEM_ERR_INVALID_ARG;
+                                         double* ms_f32, double* ms_nb_f64, double* nb_bytes) {
+  if (!ctx || !sys || !sys->d || !ms_f64 || !ms_f32 || !ms_nb_f64 || !nb_bytes || reps < 1)
+    return TPTFEM_ERR_INVALID_ARG;
   API_TRY
   set_device(ctx);
-  system_profile_spmv(*sys->d, reps, ms_f64, ms_f32);
+  *nb_bytes = 0.0;
+  system_profile_spmv(*sys->d, reps, ms_f64, ms_f32, ms_nb_f64, nb_bytes);
   API_CATCH(ctx)
 }
 

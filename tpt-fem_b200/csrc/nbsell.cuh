@@ -1,0 +1,181 @@
+// nbsell.cuh -- NB-SELL apply kernels (see nbsell.cu for the layout).
+// One warp per chunk of 32 node groups, one thread per group; each thread
+// accumulates its DPN rows in registers.  Included by solver.cu.
+#pragma once
+#include <cuda_fp16.h>
+
+#include "solver_kernels.cuh"
+
+namespace tptfem {
+
+// y = K x (FP64 blocks); DOT: pq = x.y into st->pq (breakdown if <= 0).
+template <int DPN, bool DOT>
+__global__ void __launch_bounds__(SPMV_THREADS) nb_spmv(int ngroups, const int* __restrict__ cptr,
+                                                        const int* __restrict__ bcol,
+                                                        const double* __restrict__ bval,
+                                                        const double* __restrict__ x, double* __restrict__ y,
+                                                        PcgState* st, double* partials, bool skip_done) {
+  if (skip_done && st->done) return;
+  constexpr int D2 = DPN * DPN;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int nchunks = (ngroups + 31) >> 5;
+  double d[1] = {0.0};
+  for (int c = warp; c < nchunks; c += nw) {
+    const int g = c * 32 + lane;
+    if (g < ngroups) {
+      double acc[DPN];
+#pragma unroll
+      for (int a = 0; a < DPN; ++a) acc[a] = 0.0;
+      const int s1 = cptr[c + 1];
+      for (int s = cptr[c]; s < s1; ++s) {
+        const int J = bcol[(int64_t)s * 32 + lane];
+        double xj[DPN];
+#pragma unroll
+        for (int b = 0; b < DPN; ++b) xj[b] = __ldg(x + (int64_t)J * DPN + b);
+        const double* v = bval + (int64_t)s * D2 * 32 + lane;
+#pragma unroll
+        for (int a = 0; a < DPN; ++a)
+#pragma unroll
+          for (int b = 0; b < DPN; ++b) acc[a] += v[(a * DPN + b) * 32] * xj[b];
+      }
+#pragma unroll
+      for (int a = 0; a < DPN; ++a) {
+        y[(int64_t)g * DPN + a] = acc[a];
+        if (DOT) d[0] += x[(int64_t)g * DPN + a] * acc[a];
+      }
+    }
+  }
+  if (DOT) {
+    if (grid_sum<1>(d, partials, &st->ticket[0])) {
+      st->pq = d[0];
+      if (!(d[0] > 0.0)) st->done = 2;
+    }
+  }
+}
+
+// One FP16 block of a factor slot: 8 values in a 16-byte word (row-major
+// entries 0..7) plus the 9th entry (3x3) in a separate 2-byte array, so a lane
+// issues two loads per block.  For DPN < 3 the word holds all D2 entries.
+template <int DPN>
+__device__ __forceinline__ void load_half_block(const uint4* __restrict__ pack, const __half* __restrict__ tail,
+                                                int64_t idx, float (&v)[DPN * DPN]) {
+  const uint4 w = __ldg(pack + idx);
+  const __half2* h = reinterpret_cast<const __half2*>(&w);
+  float f[8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float2 p = __half22float2(h[i]);
+    f[2 * i] = p.x;
+    f[2 * i + 1] = p.y;
+  }
+#pragma unroll
+  for (int q = 0; q < DPN * DPN && q < 8; ++q) v[q] = f[q];
+  if constexpr (DPN * DPN == 9) v[8] = __half2float(tail[idx]);
+}
+
+// t = sigma^2 * (r + L r), L in packed FP16 blocks.  Skipped once done.
+template <int DPN>
+__global__ void __launch_bounds__(SPMV_THREADS) nb_fsai_lower(int ngroups, const int* __restrict__ cptr,
+                                                              const int* __restrict__ bcol,
+                                                              const uint4* __restrict__ pack,
+                                                              const __half* __restrict__ tail,
+                                                              const __half* __restrict__ dval,
+                                                              const float* __restrict__ sigma2,
+                                                              const double* __restrict__ r, double* __restrict__ t,
+                                                              const PcgState* st) {
+  if (st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int nchunks = (ngroups + 31) >> 5;
+  for (int c = warp; c < nchunks; c += nw) {
+    const int g = c * 32 + lane;
+    if (g >= ngroups) continue;
+    double own[DPN], acc[DPN];
+#pragma unroll
+    for (int a = 0; a < DPN; ++a) acc[a] = own[a] = r[(int64_t)g * DPN + a];
+    int q = 0;
+#pragma unroll
+    for (int a = 1; a < DPN; ++a)
+#pragma unroll
+      for (int b = 0; b < a; ++b, ++q)
+        acc[a] += (double)__half2float(dval[((int64_t)c * 3 + q) * 32 + lane]) * own[b];
+    const int s1 = cptr[c + 1];
+#pragma unroll 2
+    for (int s = cptr[c]; s < s1; ++s) {
+      const int64_t idx = (int64_t)s * 32 + lane;
+      const int J = bcol[idx];
+      double xj[DPN];
+#pragma unroll
+      for (int b = 0; b < DPN; ++b) xj[b] = __ldg(r + (int64_t)J * DPN + b);
+      float v[DPN * DPN];
+      load_half_block<DPN>(pack, tail, idx, v);
+#pragma unroll
+      for (int a = 0; a < DPN; ++a)
+#pragma unroll
+        for (int b = 0; b < DPN; ++b) acc[a] += (double)v[a * DPN + b] * xj[b];
+    }
+#pragma unroll
+    for (int a = 0; a < DPN; ++a) t[(int64_t)g * DPN + a] = (double)sigma2[(int64_t)g * DPN + a] * acc[a];
+  }
+}
+
+// z = t + L^T t (transposed packed FP16 blocks) and rz = r.z into st->rz[par ^ 1].
+template <int DPN>
+__global__ void __launch_bounds__(SPMV_THREADS) nb_fsai_upper_rz(int ngroups, const int* __restrict__ cptr,
+                                                                 const int* __restrict__ bcol,
+                                                                 const uint4* __restrict__ pack,
+                                                                 const __half* __restrict__ tail,
+                                                                 const __half* __restrict__ dval,
+                                                                 const double* __restrict__ t,
+                                                                 const double* __restrict__ r,
+                                                                 double* __restrict__ z, PcgState* st,
+                                                                 double* partials, int par) {
+  if (st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int nchunks = (ngroups + 31) >> 5;
+  double d[1] = {0.0};
+  for (int c = warp; c < nchunks; c += nw) {
+    const int g = c * 32 + lane;
+    if (g >= ngroups) continue;
+    double own[DPN], acc[DPN];
+#pragma unroll
+    for (int a = 0; a < DPN; ++a) acc[a] = own[a] = t[(int64_t)g * DPN + a];
+    int q = 0;
+#pragma unroll
+    for (int a = 1; a < DPN; ++a)
+#pragma unroll
+      for (int b = 0; b < a; ++b, ++q)
+        acc[b] += (double)__half2float(dval[((int64_t)c * 3 + q) * 32 + lane]) * own[a];
+    const int s1 = cptr[c + 1];
+#pragma unroll 2
+    for (int s = cptr[c]; s < s1; ++s) {
+      const int64_t idx = (int64_t)s * 32 + lane;
+      const int J = bcol[idx];
+      double xj[DPN];
+#pragma unroll
+      for (int b = 0; b < DPN; ++b) xj[b] = __ldg(t + (int64_t)J * DPN + b);
+      float v[DPN * DPN];
+      load_half_block<DPN>(pack, tail, idx, v);
+#pragma unroll
+      for (int a = 0; a < DPN; ++a)
+#pragma unroll
+        for (int b = 0; b < DPN; ++b) acc[a] += (double)v[a * DPN + b] * xj[b];
+    }
+#pragma unroll
+    for (int a = 0; a < DPN; ++a) {
+      z[(int64_t)g * DPN + a] = acc[a];
+      d[0] += r[(int64_t)g * DPN + a] * acc[a];
+    }
+  }
+  if (grid_sum<1>(d, partials, &st->ticket[3])) {
+    st->rz[par ^ 1] = d[0];
+    if (!(d[0] > 0.0)) st->done = 2;
+  }
+}
+
+}  // namespace tptfem

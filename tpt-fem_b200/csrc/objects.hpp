@@ -70,8 +70,23 @@ struct FsaiFactor {
   DevBuf<__half> va, tva;
 };
 
+// Node-block sliced-ELL copies of the operator and of the FSAI factor (nbsell.cu).
+struct NbSell {
+  int state = 0;  // 0 not tried, 1 built, 2 not applicable (partial node groups)
+  int dpn = 0, ngroups = 0, nchunks = 0;
+  int64_t k_slots = 0, l_slots = 0, u_slots = 0;
+  DevBuf<int> gptr, glist;  // group -> sorted neighbour groups
+  DevBuf<int> k_cptr, k_col;
+  DevBuf<double> k_val;
+  DevBuf<int> l_cptr, l_col, u_cptr, u_col, u_pos, nlow;
+  DevBuf<uint4> l_pack, u_pack;  // 8 FP16 block values per slot and lane
+  DevBuf<__half> l_tail, u_tail, l_diag;
+  bool factor_checked = false, factor_ok = false;
+};
+
 struct SystemData {
   tptfem_context* ctx = nullptr;
+  NbSell nb;
   int64_t n = 0, n_free = 0, nnz = 0;
   int dpn = 1;            // dofs per mesh node of the full system
   DevBuf<int> free_map;   // reduced -> full
@@ -112,10 +127,14 @@ bool fsai_classic(const SystemData& S, FsaiFactor& F);
 // a value is not finite / positive or outside the FP16 range.
 bool fsai_set_values(const SystemData& S, FsaiFactor& F, const double* d_sig2, const double* d_lva);
 
+// nbsell.cu
+bool nb_build_operator(SystemData& S);  // false when the system has partial node groups
+bool nb_fill_factor(SystemData& S, const FsaiFactor& F);  // false: factor rows not node-block shaped
+
 // solver.cu
 int64_t system_fsai_classic(SystemData& S);  // builds (once) the classic factor; -1 on failure
 void system_fsai_download(const SystemData& S, int64_t* rp, int64_t* ci, double* lva, double* sig2);
-void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32);
+void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32, double* ms_nb, double* nb_bytes);
 void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats& st);
 
 }  // namespace tptfem

@@ -30,6 +30,9 @@
 #include <cstdio>
 #include <cstdlib>
 
+#include <type_traits>
+
+#include "nbsell.cuh"
 #include "objects.hpp"
 #include "solver_kernels.cuh"
 
@@ -97,8 +100,36 @@ struct Engine {
   DevBuf<double> partials;
   DevBuf<PcgState> st;
   cudaGraphExec_t exec = nullptr;
+  // node-block sliced-ELL operator / FSAI factor (FP64 engines only)
+  const NbSell* nb = nullptr;
+  bool nb_op = false, nb_pc = false;
+  int nb_grid = 1;
   ~Engine() {
     if (exec) cudaGraphExecDestroy(exec);
+  }
+
+  void use_nb(const NbSell* N, bool op, bool pcnb) {
+    nb = N;
+    nb_op = op;
+    nb_pc = pcnb;
+    nb_grid = std::max(1, std::min(sm_count() * 8, ceil_div((int64_t)N->nchunks * 32, SPMV_THREADS)));
+    if (partials.n < 2 * (size_t)nb_grid + 2) partials.alloc(2 * (size_t)nb_grid + 2, partials.s);
+    if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+  }
+
+  // q = A p with the pq reduction (K1).
+  void op_dot(cudaStream_t s, const T* x, T* y) {
+    if constexpr (std::is_same<T, double>::value) {
+      if (nb_op) {
+        const NbSell& N = *nb;
+        if (N.dpn == 3) nb_spmv<3, true><<<nb_grid, SPMV_THREADS, 0, s>>>(N.ngroups, N.k_cptr.p, N.k_col.p, N.k_val.p, x, y, st.p, partials.p, true);
+        else if (N.dpn == 2) nb_spmv<2, true><<<nb_grid, SPMV_THREADS, 0, s>>>(N.ngroups, N.k_cptr.p, N.k_col.p, N.k_val.p, x, y, st.p, partials.p, true);
+        else nb_spmv<1, true><<<nb_grid, SPMV_THREADS, 0, s>>>(N.ngroups, N.k_cptr.p, N.k_col.p, N.k_val.p, x, y, st.p, partials.p, true);
+        TPT_CHECK_LAUNCH();
+        return;
+      }
+    }
+    launch_spmv<T, T, T, true>(lanes, spmv_grid, s, n, rp, ci, va, x, y, st.p, partials.p, true);
   }
 
   void setup(int n_, const int* rp_, const int* ci_, const T* va_, int64_t nnz, cudaStream_t s, int batch_) {
@@ -122,8 +153,25 @@ struct Engine {
     if (!z.p) { z.alloc(n, s); t.alloc(n, s); }
   }
 
-  // z = M r with the preconditioner, rz into slot `out_slot` (FSAI only).
+  // z = M r with the FSAI factor, rz into st->rz[par ^ 1].
   void apply_fsai(cudaStream_t s, int par) {
+    if constexpr (std::is_same<T, double>::value) {
+      if (nb_pc) {
+        const NbSell& N = *nb;
+#define TPT_NB_FSAI(D)                                                                                           \
+  nb_fsai_lower<D><<<nb_grid, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.l_pack.p, N.l_tail.p,     \
+                                                    N.l_diag.p, pc.sigma2, r.p, t.p, st.p);                       \
+  TPT_CHECK_LAUNCH();                                                                                            \
+  nb_fsai_upper_rz<D><<<nb_grid, SPMV_THREADS, 0, s>>>(N.ngroups, N.u_cptr.p, N.u_col.p, N.u_pack.p, N.u_tail.p,  \
+                                                       N.l_diag.p, t.p, r.p, z.p, st.p, partials.p, par);         \
+  TPT_CHECK_LAUNCH();
+        if (N.dpn == 3) { TPT_NB_FSAI(3) }
+        else if (N.dpn == 2) { TPT_NB_FSAI(2) }
+        else { TPT_NB_FSAI(1) }
+#undef TPT_NB_FSAI
+        return;
+      }
+    }
     fsai_apply(pc, n, r.p, t.p, z.p, st.p, partials.p, par, s);
   }
 
@@ -133,7 +181,7 @@ struct Engine {
     TPT_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int it = 0; it < batch; ++it) {
       const int par = it & 1;
-      launch_spmv<T, T, T, true>(lanes, spmv_grid, s, n, rp, ci, va, p.p, q.p, st.p, partials.p, true);
+      op_dot(s, p.p, q.p);
       if (pc.kind == PC_JACOBI) {
         pcg_update<T, true><<<vec_grid, VEC_THREADS, 0, s>>>(n, par, xl.p, r.p, p.p, q.p, dinv.p, st.p, partials.p);
         TPT_CHECK_LAUNCH();
@@ -348,7 +396,12 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
   if (o.flags & TPTFEM_SOLVE_FRESH_SETUP) {
     // keep patterns, graphs and buffers; recompute every value of the preconditioner
     if (solver == TPTFEM_SOLVER_FSAI_MP_PCG && W.fsai_ready) {
-      if (!fsai_classic(S, W.fsai)) { W.fsai_ready = false; W.fsai_failed = true; }
+      if (!fsai_classic(S, W.fsai)) {
+        W.fsai_ready = false;
+        W.fsai_failed = true;
+      } else if (W.f64_fsai.nb_pc) {
+        nb_fill_factor(S, W.fsai);
+      }
     } else if (solver == TPTFEM_SOLVER_JACOBI_PCG && W.f64_ready) {
       refresh_jacobi<double>(S, W.f64);
     } else if (solver == TPTFEM_SOLVER_MP_PCG && W.f32_ready) {
@@ -359,6 +412,8 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
     if (!W.fsai_ready && !W.fsai_failed) {
       if (fsai_classic(S, W.fsai)) {
         prepare_fsai_engine(S, W.f64_fsai, W.fsai, batch);
+        if (!(o.flags & TPTFEM_SOLVE_CSR_ONLY) && nb_build_operator(S))
+          W.f64_fsai.use_nb(&S.nb, true, nb_fill_factor(S, W.fsai));
         W.fsai_ready = true;
       } else {
         W.fsai_failed = true;
@@ -371,6 +426,7 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
   }
   if (solver == TPTFEM_SOLVER_JACOBI_PCG && !W.f64_ready) {
     prepare_jacobi<double>(S, W.f64, S.val.p, batch);
+    if (!(o.flags & TPTFEM_SOLVE_CSR_ONLY) && nb_build_operator(S)) W.f64.use_nb(&S.nb, true, false);
     W.f64_ready = true;
   }
   if (solver == TPTFEM_SOLVER_MP_PCG && !W.f32_ready) {
@@ -463,7 +519,7 @@ void system_fsai_download(const SystemData& S, int64_t* rp, int64_t* ci, double*
 // Average device time of the solver's SpMV kernels on this system (diagnostic
 // for the roofline report): FP64 and FP32 CSR, `reps` back-to-back launches
 // each, timed with events on the context stream.
-void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32) {
+void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32, double* ms_nb, double* nb_bytes) {
   cudaStream_t s = S.ctx->stream;
   ensure_work(S);
   ensure_val32(S);
@@ -494,6 +550,19 @@ void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32
     launch_spmv<float, float, float, false>(lanes, grid, s, (int)S.n_free, S.row_ptr.p, S.col.p, S.val32.p, x32.p,
                                             y32.p, nullptr, nullptr, false);
   });
+  *ms_nb = -1.0;
+  if (nb_build_operator(S)) {
+    const NbSell& N = S.nb;
+    const int g = std::max(1, std::min(sm_count() * 8, ceil_div((int64_t)N.nchunks * 32, SPMV_THREADS)));
+    *ms_nb = timeit([&] {
+      if (N.dpn == 3) nb_spmv<3, false><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.k_cptr.p, N.k_col.p, N.k_val.p, x64.p, y64.p, nullptr, nullptr, false);
+      else if (N.dpn == 2) nb_spmv<2, false><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.k_cptr.p, N.k_col.p, N.k_val.p, x64.p, y64.p, nullptr, nullptr, false);
+      else nb_spmv<1, false><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.k_cptr.p, N.k_col.p, N.k_val.p, x64.p, y64.p, nullptr, nullptr, false);
+      TPT_CHECK_LAUNCH();
+    });
+    *nb_bytes = (double)N.k_slots * 32 * (4 + 8 * N.dpn * N.dpn) + (double)(N.nchunks + 1) * 4 +
+                16.0 * (double)S.n_free;
+  }
 }
 
 void csr_matvec_f64(tptfem_context* ctx, int64_t nrows, const int* rp, const int* ci, const double* va,

@@ -287,11 +287,12 @@ def _bcs(bcs):
     return N.i64([b[0] for b in arr]), N.f64([b[1] for b in arr])
 
 
-def _opts(solver=SOLVER_JACOBI_PCG, tol=1e-10, inner_tol=0.0, max_iter=0, max_outer=0, batch=0, fresh_setup=False):
+def _opts(solver=SOLVER_JACOBI_PCG, tol=1e-10, inner_tol=0.0, max_iter=0, max_outer=0, batch=0, fresh_setup=False,
+          csr_only=False):
     o = SolverOpts()
     o.solver, o.rel_tol, o.inner_rel_tol, o.max_iter, o.max_outer, o.batch = solver, tol, inner_tol, max_iter, \
         max_outer, batch
-    o.flags = N.SOLVE_FRESH_SETUP if fresh_setup else 0
+    o.flags = (N.SOLVE_FRESH_SETUP if fresh_setup else 0) | (N.SOLVE_CSR_ONLY if csr_only else 0)
     return o
 
 
@@ -323,10 +324,11 @@ class System:
         return st.as_dict()
 
     def profile_spmv(self, reps=20):
-        """Average device ms of the solver's FP64 and FP32 SpMV kernels on this system."""
-        a, b = C.c_double(), C.c_double()
-        self.ctx.check(self.ctx.lib.tptfem_system_profile_spmv(self.ctx.h, self.h, reps, C.byref(a), C.byref(b)))
-        return a.value, b.value
+        """Average device ms of the solver's SpMV kernels: (FP64 CSR, FP32 CSR, FP64 node-block, node-block bytes)."""
+        a, b, c, d = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        self.ctx.check(self.ctx.lib.tptfem_system_profile_spmv(self.ctx.h, self.h, reps, C.byref(a), C.byref(b),
+                                                               C.byref(c), C.byref(d)))
+        return a.value, b.value, c.value, d.value
 
     def fsai(self):
         """Classic FSAI factor: (L row_ptrs, L cols, L values, sigma^2); G = diag(sigma)(I + L)."""

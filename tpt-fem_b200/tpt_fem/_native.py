@@ -22,6 +22,7 @@ CELL_QUAD4, CELL_TET4 = 3, 4
 MODEL_BAR_AXIAL, MODEL_PLANE_STRESS, MODEL_PLANE_STRAIN, MODEL_CONTINUUM_3D = 0, 1, 2, 3
 SOLVER_JACOBI_PCG, SOLVER_MP_PCG, SOLVER_FSAI_MP_PCG = 0, 1, 2
 SOLVE_FRESH_SETUP = 1
+SOLVE_CSR_ONLY = 2
 
 
 class SolverOpts(C.Structure):
@@ -73,7 +74,7 @@ SIGNATURES = {
     "tptfem_system_solve": (C.c_int, [_vp, _vp, C.POINTER(SolverOpts), C.POINTER(SolveStats)]),
     "tptfem_system_solution": (C.c_int, [_vp, _vp, _vp]),
     "tptfem_system_free": (None, [_vp]),
-    "tptfem_system_profile_spmv": (C.c_int, [_vp, _vp, C.c_int, _pd, _pd]),
+    "tptfem_system_profile_spmv": (C.c_int, [_vp, _vp, C.c_int, _pd, _pd, _pd, _pd]),
     "tptfem_system_fsai": (C.c_int, [_vp, _vp, _pi64]),
     "tptfem_rel_residual_noalloc": (C.c_int, [C.c_int, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _pd, C.c_char_p,
                                               C.c_size_t]),
