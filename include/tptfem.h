@@ -69,7 +69,13 @@ enum {
    * factorised sparse approximate inverse M^-1 = G^T G, G = diag(s)(I + L) on
    * the lower node-block pattern of the reduced matrix, classic FSAI values,
    * the factor stored and applied in reduced precision (s^2 FP32, L FP16). */
-  TPTFEM_SOLVER_FSAI_MP_PCG = 2
+  TPTFEM_SOLVER_FSAI_MP_PCG = 2,
+  /* As FSAI_MP_PCG with the factor's values emitted by the learned network
+   * attached with tptfem_system_attach_lfsai (same pattern, same FP16/FP32
+   * storage).  Falls back to FP64 Jacobi-PCG (stats.fell_back = 1) when the
+   * factor is invalid or the preconditioned iteration breaks down or does not
+   * converge. */
+  TPTFEM_SOLVER_LEARNED_FSAI_PCG = 3
 };
 
 typedef struct tptfem_context tptfem_context;
@@ -240,6 +246,30 @@ tptfem_status tptfem_solve_elasticity(tptfem_context* ctx, tptfem_mesh* mesh, in
                                       double poisson, int quad_order, const double* body, const int64_t* bc_dof,
                                       const double* bc_val, int64_t nbc, const tptfem_solver_opts* opts, double* u,
                                       tptfem_solve_stats* stats);
+
+/* ---- learned FSAI preconditioner (no counterpart in the reference) ----------
+ * A small message-passing network over the graph of the reduced matrix that
+ * emits the FSAI factor G = diag(s)(I + L) on the node-block lower pattern
+ * (SPD M^-1 = G^T G for any weights).  Trained on the device by the library's
+ * own forward/backward kernels on loss = mean_k ||G^ A^ G^T z_k - z_k||^2 / n
+ * (A^ = D^-1/2 A D^-1/2) over caller-supplied probe vectors z_k. */
+typedef struct tptfem_lfsai tptfem_lfsai;
+/* Number of FP32 parameters of the network. */
+int64_t tptfem_lfsai_param_count(void);
+/* New model on ctx's device, initialised from `seed` (starts as I - tril(A^)). */
+tptfem_status tptfem_lfsai_create(tptfem_context* ctx, uint64_t seed, tptfem_lfsai** out);
+void tptfem_lfsai_free(tptfem_lfsai* model);
+tptfem_status tptfem_lfsai_get_params(tptfem_context* ctx, const tptfem_lfsai* model, float* params);
+tptfem_status tptfem_lfsai_set_params(tptfem_context* ctx, tptfem_lfsai* model, const float* params);
+/* Loss on `sys` for m host probe vectors (n_free x m, row-major).  with_grad:
+ * ADD d loss/d params to the model's gradient buffer (and copy the
+ * accumulated gradient to `grad` when it is non-NULL). */
+tptfem_status tptfem_lfsai_loss(tptfem_context* ctx, tptfem_lfsai* model, tptfem_system* sys, const float* probes,
+                                int32_t m, int32_t with_grad, double* loss, float* grad);
+/* Adam step with the accumulated gradient (clipped to +-clip), then zero it. */
+tptfem_status tptfem_lfsai_adam(tptfem_context* ctx, tptfem_lfsai* model, double lr, double clip);
+/* Use `model` for TPTFEM_SOLVER_LEARNED_FSAI_PCG solves of `sys` (NULL detaches). */
+tptfem_status tptfem_system_attach_lfsai(tptfem_context* ctx, tptfem_system* sys, tptfem_lfsai* model);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,104 @@
+"""Learned FSAI on the GPU: device forward/backward against the CPU oracle,
+learned-preconditioned solves, what training gains over the plain method,
+and the fallback to FP64 Jacobi-PCG."""
+import numpy as np
+import pytest
+
+import tpt_fem as F
+from tpt_fem import lfsai as LF
+from tpt_fem import workloads as W
+from meshes import box, jitter
+from oracle import lfsai_oracle as L
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def cantilever_system(ctx, n, seed, jit=0.0):
+    mn, mx = [0.0, 0.0, 0.0], [4.0, 1.0, 1.0]
+    c, e = box(n, mn=mn, mx=mx)
+    if jit:
+        c = jitter(c, jit, seed)
+    E = W.cantilever_young(n, seed=seed)
+    m = F.Mesh.from_arrays(F.CELL_TET4, c, e, ctx=ctx)
+    K = F.assemble_elasticity(m, "3d", E, 0.3, 2)
+    rhs = F.apply_traction(m, 3, 0, 1.0, [0.0, 0.0, -1e-3], np.zeros(K.nrows))
+    dof, val = W.clamp_x0_bcs(c)
+    return F.reduce_system(K, rhs, list(zip(dof, val)))
+
+
+def oracle_graph(S):
+    rp, ci, va, fred, free = S.download()
+    lrp, lci, _, _ = S.fsai()
+    return L.Graph(rp, ci, va, free, 3, lrp, lci)
+
+
+def test_device_loss_and_gradient_match_oracle(ctx):
+    S = cantilever_system(ctx, [6, 2, 2], seed=5, jit=0.02)
+    model = LF.LearnedFsai(ctx, seed=3)
+    rng = np.random.default_rng(4)
+    p = model.get_params().astype(np.float64)
+    p += 0.2 * rng.standard_normal(p.size)  # exercise every gradient path (we, q != 0)
+    model.set_params(p.astype(np.float32))
+    p = model.get_params().astype(np.float64)
+    Z = rng.standard_normal((S.n_free, 4)).astype(np.float32)
+    loss, grad = model.loss(S, Z, grad=True)
+    g = oracle_graph(S)
+    oloss, ograd = L.loss_grad(p, g, Z.astype(np.float64))
+    assert abs(loss - oloss) <= 1e-4 * oloss
+    assert np.linalg.norm(grad - ograd) <= 2e-3 * np.linalg.norm(ograd)
+    # the gradient accumulates until an Adam step consumes it
+    _, grad2 = model.loss(S, Z, grad=True)
+    assert np.allclose(grad2, 2 * grad, rtol=1e-4, atol=1e-7 * np.max(np.abs(grad)))
+    model.adam(1e-3)
+    _, grad3 = model.loss(S, Z, grad=True)
+    assert np.linalg.norm(grad3) < 1.5 * np.linalg.norm(grad)
+
+
+def test_untrained_learned_solver_converges(ctx):
+    S = cantilever_system(ctx, [10, 3, 3], seed=6)
+    model = LF.LearnedFsai(ctx, seed=1)
+    model.attach(S)
+    st = S.solve(solver=F.SOLVER_LEARNED_FSAI_PCG, tol=1e-10)
+    assert st["solver_used"] == F.SOLVER_LEARNED_FSAI_PCG and not st["fell_back"]
+    assert st["rel_residual"] <= 1e-10
+
+
+def test_training_gains_over_jacobi_on_unseen_system(ctx):
+    rng = np.random.default_rng(0)
+    train = [cantilever_system(ctx, [12, 3, 3], seed=s) for s in (11, 12, 13)]
+    probes = [LF.pcg_residual_probes(S, 8, rng) for S in train]
+    model = LF.LearnedFsai(ctx, seed=2)
+    first = np.mean([model.loss(S, Z) for S, Z in zip(train, probes)])
+    for step in range(120):
+        k = step % len(train)
+        model.loss(train[k], probes[k], grad=True)
+        model.adam(3e-3)
+    last = np.mean([model.loss(S, Z) for S, Z in zip(train, probes)])
+    assert last < first
+    test = cantilever_system(ctx, [16, 4, 4], seed=99)
+    model.attach(test)
+    jac = test.solve(solver=F.SOLVER_JACOBI_PCG, tol=1e-10)
+    lrn = test.solve(solver=F.SOLVER_LEARNED_FSAI_PCG, tol=1e-10)
+    assert not lrn["fell_back"] and lrn["rel_residual"] <= 1e-10
+    assert lrn["iterations"] < 0.75 * jac["iterations"]
+
+
+def test_invalid_learned_factor_falls_back_to_jacobi(ctx):
+    S = cantilever_system(ctx, [8, 2, 2], seed=7)
+    model = LF.LearnedFsai(ctx, seed=4)
+    p = model.get_params()
+    p[L.OFF["w0"][0]] = 3.0e6  # L values far outside the FP16 range of the factor
+    model.set_params(p)
+    model.attach(S)
+    st = S.solve(solver=F.SOLVER_LEARNED_FSAI_PCG, tol=1e-10)
+    assert st["fell_back"] == 1 and st["solver_used"] == F.SOLVER_JACOBI_PCG
+    assert st["rel_residual"] <= 1e-10
+
+
+def test_weight_file_round_trip(ctx, tmp_path):
+    model = LF.LearnedFsai(ctx, seed=9)
+    path = tmp_path / "w.bin"
+    model.save(str(path))
+    again = LF.LearnedFsai.load(ctx, str(path))
+    assert np.array_equal(model.get_params(), again.get_params())

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <new>
 
+#include "lfsai.hpp"
 #include "objects.hpp"
 
 using namespace tptfem;
@@ -524,6 +525,97 @@ tptfem_status tptfem_solve_elasticity(tptfem_context* ctx, tptfem_mesh* mesh, in
     rc = tptfem_solve_with_dirichlet(ctx, K, rhs.data(), (int64_t)rhs.size(), bc_dof, bc_val, nbc, opts, u, stats);
   tptfem_matrix_free(K);
   return rc;
+}
+
+// ---- learned FSAI -----------------------------------------------------------------
+
+int64_t tptfem_lfsai_param_count(void) { return lf_param_count(); }
+
+tptfem_status tptfem_lfsai_create(tptfem_context* ctx, uint64_t seed, tptfem_lfsai** out) {
+  if (!ctx || !out) return TPTFEM_ERR_INVALID_ARG;
+  *out = nullptr;
+  API_TRY
+  set_device(ctx);
+  auto M = std::make_shared<LfModel>();
+  M->ctx = ctx;
+  const int np = lf_param_count();
+  std::vector<float> h(np);
+  lf_init_params(seed, h.data());
+  M->prm.alloc(np, ctx->stream);
+  M->prm.upload(h.data(), np);
+  M->grad.alloc(np, ctx->stream);
+  M->grad.zero();
+  M->m1.alloc(np, ctx->stream);
+  M->m1.zero();
+  M->m2.alloc(np, ctx->stream);
+  M->m2.zero();
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  *out = new tptfem_lfsai{M};
+  API_CATCH(ctx)
+}
+
+void tptfem_lfsai_free(tptfem_lfsai* model) { delete model; }
+
+tptfem_status tptfem_lfsai_get_params(tptfem_context* ctx, const tptfem_lfsai* model, float* params) {
+  if (!ctx || !model || !model->d || !params) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  model->d->prm.download(params, model->d->prm.n);
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_lfsai_set_params(tptfem_context* ctx, tptfem_lfsai* model, const float* params) {
+  if (!ctx || !model || !model->d || !params) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  for (size_t i = 0; i < model->d->prm.n; ++i)
+    TPT_REQUIRE(std::isfinite(params[i]), TPTFEM_ERR_INVALID_ARG, "parameters hold a non-finite value");
+  model->d->prm.upload(params, model->d->prm.n);
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_lfsai_loss(tptfem_context* ctx, tptfem_lfsai* model, tptfem_system* sys, const float* probes,
+                                int32_t m, int32_t with_grad, double* loss, float* grad) {
+  if (!ctx || !model || !model->d || !sys || !sys->d || !probes || !loss || m < 1) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  SystemData& S = *sys->d;
+  TPT_REQUIRE(S.n_free > 0 && S.n_free * (int64_t)m < (1LL << 31), TPTFEM_ERR_INVALID_ARG,
+              "n_free * m out of range for training");
+  FsaiFactor* F = nullptr;
+  LfGraph& G = system_lf_graph(S, &F);
+  DevBuf<float> z;
+  z.alloc(S.n_free * m, ctx->stream);
+  z.upload(probes, S.n_free * m);
+  LfModel& M = *model->d;
+  *loss = lf_loss_grad(S, *F, G, M.prm.p, with_grad ? M.grad.p : nullptr, z.p, m);
+  if (with_grad && grad) {
+    M.grad.download(grad, M.grad.n);
+    TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_lfsai_adam(tptfem_context* ctx, tptfem_lfsai* model, double lr, double clip) {
+  if (!ctx || !model || !model->d || !(lr > 0) || !(clip > 0)) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  LfModel& M = *model->d;
+  M.step += 1;
+  lf_adam_step(ctx->stream, (int)M.prm.n, M.prm.p, M.grad.p, M.m1.p, M.m2.p, M.step, (float)lr, (float)clip);
+  M.grad.zero();
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_system_attach_lfsai(tptfem_context* ctx, tptfem_system* sys, tptfem_lfsai* model) {
+  if (!ctx || !sys || !sys->d) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  sys->d->lmodel = model ? model->d : nullptr;
+  API_CATCH(ctx)
 }
 
 }  // extern "C"

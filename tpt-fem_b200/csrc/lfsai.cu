@@ -1,0 +1,693 @@
+// lfsai.cu -- learned factorised sparse approximate inverse.
+//
+// A small message-passing network over the graph of the reduced matrix emits
+// the FSAI factor's values on the node-block lower pattern (fsai.cu):
+//   A^ = D^-1/2 A D^-1/2                       (unit diagonal, scale free)
+//   h0_i  = [1, sum|a^_ij|, sum a^_ij, sum a^_ij^2, onehot(dof component), deg/40]
+//   h_l+1 = tanh(Ws h_l + Wa (|A^_off| h_l) + Wb (A^_off h_l) + b)   (2 layers, width 16)
+//   edge (i, j) of the pattern, j < i:
+//       z_ij = tanh(U h_i + V h_j + ue a^_ij + ce),  L^_ij = we . z_ij + w0 a^_ij
+//   sigma^_i^2 = exp(q . h_i + q0)
+//   G^ = diag(sigma^) (I + L^)  -> SPD G^T G for any parameters;
+//   G = G^ D^-1/2, i.e. sigma_i^2 = sigma^_i^2 / d_i, L_ij = L^_ij sqrt(d_i / d_j).
+// With we = 0, w0 = -1, q = q0 = 0 the network starts as the first-order
+// approximate inverse factor I - tril(A^).
+//
+// Training minimises  loss = 1/(m n) sum_k || G^ A^ G^T z_k - z_k ||^2  over
+// probe vectors z_k (random and PCG residuals), with hand-written forward and
+// backward kernels and Adam.  Everything is FP32 except the final conversion
+// of the factor to FP64/FP16 for the solver.  Weight gradients are summed with
+// block reductions and atomics (training is not bitwise reproducible; inference
+// is).  The matrix is taken as symmetric: the backward of A^ h uses A^ itself.
+#include <cmath>
+#include <cstring>
+
+#include "lfsai.hpp"
+
+namespace tptfem {
+
+namespace {
+
+constexpr int D0 = LF_D0, H = LF_H;
+constexpr int LF_THREADS = 128;
+
+struct Off {  // parameter offsets (floats)
+  int ws[LF_LAYERS], wa[LF_LAYERS], wb[LF_LAYERS], b[LF_LAYERS], din[LF_LAYERS];
+  int U, V, ue, ce, we, w0, q, q0, total;
+};
+
+Off offsets() {
+  Off o;
+  int p = 0;
+  for (int l = 0; l < LF_LAYERS; ++l) {
+    const int din = l == 0 ? D0 : H;
+    o.din[l] = din;
+    o.ws[l] = p; p += H * din;
+    o.wa[l] = p; p += H * din;
+    o.wb[l] = p; p += H * din;
+    o.b[l] = p; p += H;
+  }
+  o.U = p; p += H * H;
+  o.V = p; p += H * H;
+  o.ue = p; p += H;
+  o.ce = p; p += H;
+  o.we = p; p += H;
+  o.w0 = p; p += 1;
+  o.q = p; p += H;
+  o.q0 = p; p += 1;
+  o.total = p;
+  return o;
+}
+
+// ---- preparation ----------------------------------------------------------------
+
+// d^-1/2, A^ values, node features.
+__global__ void lf_prep(int n, int dpn, const int* __restrict__ rp, const int* __restrict__ ci,
+                        const double* __restrict__ va, const int* __restrict__ free_map, float* __restrict__ ahat,
+                        double* __restrict__ dis, float* __restrict__ x0) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double di = 1.0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k)
+    if (ci[k] == i) di = va[k];
+  dis[i] = 1.0 / sqrt(di);
+}
+
+__global__ void lf_prep2(int n, int dpn, const int* __restrict__ rp, const int* __restrict__ ci,
+                         const double* __restrict__ va, const int* __restrict__ free_map,
+                         const double* __restrict__ dis, float* __restrict__ ahat, float* __restrict__ x0) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float sa = 0.f, ss = 0.f, sq = 0.f;
+  int deg = 0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const int j = ci[k];
+    const float a = (float)(va[k] * dis[i] * dis[j]);
+    ahat[k] = a;
+    if (j != i) { sa += fabsf(a); ss += a; sq += a * a; ++deg; }
+  }
+  float* x = x0 + (int64_t)i * D0;
+  x[0] = 1.f; x[1] = sa; x[2] = ss; x[3] = sq;
+  const int comp = dpn > 1 ? free_map[i] % dpn : -1;
+  x[4] = comp == 0; x[5] = comp == 1; x[6] = comp == 2;
+  x[7] = deg / 40.f;
+}
+
+// A^ at the factor pattern entries (0 where A has no entry).
+__global__ void lf_pattern_values(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                  const float* __restrict__ ahat, const int* __restrict__ lrp,
+                                  const int* __restrict__ lci, float* __restrict__ al) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int k = rp[i];
+  const int ke = rp[i + 1];
+  for (int t = lrp[i]; t < lrp[i + 1]; ++t) {
+    const int j = lci[t];
+    while (k < ke && ci[k] < j) ++k;
+    al[t] = (k < ke && ci[k] == j) ? ahat[k] : 0.f;
+  }
+}
+
+// ---- network forward ----------------------------------------------------------------
+
+// Ya = |A^_off| X, Yb = A^_off X (rows of width DIN).  With ABS_ONLY... both always.
+template <int DIN>
+__global__ void lf_agg(int n, const int* __restrict__ rp, const int* __restrict__ ci, const float* __restrict__ ahat,
+                       const float* __restrict__ X, float* __restrict__ Ya, float* __restrict__ Yb) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float a[DIN], b[DIN];
+#pragma unroll
+  for (int c = 0; c < DIN; ++c) a[c] = b[c] = 0.f;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const int j = ci[k];
+    if (j == i) continue;
+    const float w = ahat[k], aw = fabsf(w);
+    const float* xj = X + (int64_t)j * DIN;
+#pragma unroll
+    for (int c = 0; c < DIN; ++c) {
+      const float v = __ldg(xj + c);
+      a[c] += aw * v;
+      b[c] += w * v;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < DIN; ++c) {
+    Ya[(int64_t)i * DIN + c] = a[c];
+    Yb[(int64_t)i * DIN + c] = b[c];
+  }
+}
+
+// H = tanh(Ws X + Wa Ya + Wb Yb + b)
+template <int DIN>
+__global__ void lf_layer(int n, const float* __restrict__ prm, int ows, int owa, int owb, int ob,
+                         const float* __restrict__ X, const float* __restrict__ Ya, const float* __restrict__ Yb,
+                         float* __restrict__ Hout) {
+  __shared__ float w[3 * H * DIN + H];
+  for (int t = threadIdx.x; t < H * DIN; t += blockDim.x) {
+    w[t] = prm[ows + t];
+    w[H * DIN + t] = prm[owa + t];
+    w[2 * H * DIN + t] = prm[owb + t];
+  }
+  for (int t = threadIdx.x; t < H; t += blockDim.x) w[3 * H * DIN + t] = prm[ob + t];
+  __syncthreads();
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float x[DIN], ya[DIN], yb[DIN];
+#pragma unroll
+  for (int c = 0; c < DIN; ++c) {
+    x[c] = X[(int64_t)i * DIN + c];
+    ya[c] = Ya[(int64_t)i * DIN + c];
+    yb[c] = Yb[(int64_t)i * DIN + c];
+  }
+#pragma unroll
+  for (int o = 0; o < H; ++o) {
+    float s = w[3 * H * DIN + o];
+#pragma unroll
+    for (int c = 0; c < DIN; ++c)
+      s += w[o * DIN + c] * x[c] + w[H * DIN + o * DIN + c] * ya[c] + w[2 * H * DIN + o * DIN + c] * yb[c];
+    Hout[(int64_t)i * H + o] = tanhf(s);
+  }
+}
+
+// P = U h, Q = V h, sigma^ = exp((q.h + q0) / 2)
+__global__ void lf_head_nodes(int n, const float* __restrict__ prm, Off o, const float* __restrict__ Hh,
+                              float* __restrict__ P, float* __restrict__ Q, float* __restrict__ sig) {
+  __shared__ float U[H * H], V[H * H], q[H + 1];
+  for (int t = threadIdx.x; t < H * H; t += blockDim.x) { U[t] = prm[o.U + t]; V[t] = prm[o.V + t]; }
+  for (int t = threadIdx.x; t < H; t += blockDim.x) q[t] = prm[o.q + t];
+  if (threadIdx.x == 0) q[H] = prm[o.q0];
+  __syncthreads();
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float h[H];
+#pragma unroll
+  for (int c = 0; c < H; ++c) h[c] = Hh[(int64_t)i * H + c];
+  float rho = q[H];
+#pragma unroll
+  for (int a = 0; a < H; ++a) {
+    float p = 0.f, qq = 0.f;
+#pragma unroll
+    for (int c = 0; c < H; ++c) { p += U[a * H + c] * h[c]; qq += V[a * H + c] * h[c]; }
+    P[(int64_t)i * H + a] = p;
+    Q[(int64_t)i * H + a] = qq;
+    rho += q[a] * h[a];
+  }
+  sig[i] = expf(0.5f * rho);
+}
+
+// L^_ij for every pattern entry.
+__global__ void lf_head_edges(int n, const float* __restrict__ prm, Off o, const int* __restrict__ lrp,
+                              const int* __restrict__ lci, const float* __restrict__ al, const float* __restrict__ P,
+                              const float* __restrict__ Q, float* __restrict__ lhat) {
+  __shared__ float ue[H], ce[H], we[H], w0;
+  for (int t = threadIdx.x; t < H; t += blockDim.x) { ue[t] = prm[o.ue + t]; ce[t] = prm[o.ce + t]; we[t] = prm[o.we + t]; }
+  if (threadIdx.x == 0) w0 = prm[o.w0];
+  __syncthreads();
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float p[H];
+#pragma unroll
+  for (int c = 0; c < H; ++c) p[c] = P[(int64_t)i * H + c];
+  for (int t = lrp[i]; t < lrp[i + 1]; ++t) {
+    const int j = lci[t];
+    const float a = al[t];
+    float s = w0 * a;
+#pragma unroll
+    for (int c = 0; c < H; ++c) s += we[c] * tanhf(p[c] + __ldg(Q + (int64_t)j * H + c) + ue[c] * a + ce[c]);
+    lhat[t] = s;
+  }
+}
+
+// ---- factor applies on m probe columns (row-major n x m) --------------------------
+
+// Y = G^ X : y_i = sig_i (x_i + sum_j L^_ij x_j)
+__global__ void lf_g(int n, int m, const int* __restrict__ lrp, const int* __restrict__ lci,
+                     const float* __restrict__ lhat, const float* __restrict__ sig, const float* __restrict__ X,
+                     float* __restrict__ Y) {
+  int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= (int64_t)n * m) return;
+  const int i = (int)(id / m), k = (int)(id % m);
+  float s = X[id];
+  for (int t = lrp[i]; t < lrp[i + 1]; ++t) s += lhat[t] * X[(int64_t)lci[t] * m + k];
+  Y[id] = sig[i] * s;
+}
+
+// Y = G^T X : y_i = sig_i x_i + sum_{j > i} L^_ji sig_j x_j  (transposed pattern)
+__global__ void lf_gt(int n, int m, const int* __restrict__ trp, const int* __restrict__ tci,
+                      const int* __restrict__ perm, const float* __restrict__ lhat, const float* __restrict__ sig,
+                      const float* __restrict__ X, float* __restrict__ Y) {
+  int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= (int64_t)n * m) return;
+  const int i = (int)(id / m), k = (int)(id % m);
+  float s = sig[i] * X[id];
+  for (int t = trp[i]; t < trp[i + 1]; ++t) {
+    const int j = tci[t];
+    s += lhat[perm[t]] * sig[j] * X[(int64_t)j * m + k];
+  }
+  Y[id] = s;
+}
+
+// Y = A^ X
+__global__ void lf_a(int n, int m, const int* __restrict__ rp, const int* __restrict__ ci,
+                     const float* __restrict__ ahat, const float* __restrict__ X, float* __restrict__ Y) {
+  int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= (int64_t)n * m) return;
+  const int i = (int)(id / m), k = (int)(id % m);
+  float s = 0.f;
+  for (int t = rp[i]; t < rp[i + 1]; ++t) s += ahat[t] * X[(int64_t)ci[t] * m + k];
+  Y[id] = s;
+}
+
+// E = W - Z, loss partial sums, GW = 2 E / (m n)
+__global__ void lf_residual(int64_t nm, const float* __restrict__ W, const float* __restrict__ Z,
+                            float* __restrict__ GW, double* __restrict__ loss, float scale) {
+  __shared__ double sh[LF_THREADS];
+  int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double e2 = 0.0;
+  if (id < nm) {
+    const float e = W[id] - Z[id];
+    GW[id] = 2.f * e * scale;
+    e2 = (double)e * e;
+  }
+  sh[threadIdx.x] = e2;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicAdd(loss, sh[0]);
+}
+
+// dG^ on the pattern and the diagonal, then dL^ and d rho (thread per row).
+//   dG^_ij = sum_k GW_ik V1_jk + Z_ik GU_jk
+__global__ void lf_dg(int n, int m, const int* __restrict__ lrp, const int* __restrict__ lci,
+                      const float* __restrict__ lhat, const float* __restrict__ sig, const float* __restrict__ GW,
+                      const float* __restrict__ V1, const float* __restrict__ Z, const float* __restrict__ GU,
+                      float* __restrict__ dlhat, float* __restrict__ drho) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  auto dg = [&](int j) {
+    float s = 0.f;
+    for (int k = 0; k < m; ++k)
+      s += GW[(int64_t)i * m + k] * V1[(int64_t)j * m + k] + Z[(int64_t)i * m + k] * GU[(int64_t)j * m + k];
+    return s;
+  };
+  float dsig = dg(i);
+  for (int t = lrp[i]; t < lrp[i + 1]; ++t) {
+    const float d = dg(lci[t]);
+    dlhat[t] = sig[i] * d;
+    dsig += lhat[t] * d;
+  }
+  drho[i] = 0.5f * sig[i] * dsig;
+}
+
+// Block-reduce NV floats per thread, then one atomicAdd per value and block.
+template <int NV>
+__device__ __forceinline__ void block_atomic(float (&v)[NV], float* out) {
+  __shared__ float sh[LF_THREADS / 32][NV];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < NV; ++c) {
+    float x = v[c];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[wid][c] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    float s = 0.f;
+    for (int w = 0; w < LF_THREADS / 32; ++w) s += sh[w][threadIdx.x];
+    atomicAdd(out + threadIdx.x, s);
+  }
+}
+
+// Edge head backward: gradients of we, w0, ue, ce; dP (per row) and dQ (atomics).
+__global__ void lf_head_edges_bwd(int n, const float* __restrict__ prm, Off o, float* __restrict__ grad,
+                                  const int* __restrict__ lrp, const int* __restrict__ lci,
+                                  const float* __restrict__ al, const float* __restrict__ P,
+                                  const float* __restrict__ Q, const float* __restrict__ dlhat,
+                                  float* __restrict__ dP, float* __restrict__ dQ) {
+  __shared__ float ue[H], ce[H], we[H];
+  for (int t = threadIdx.x; t < H; t += blockDim.x) { ue[t] = prm[o.ue + t]; ce[t] = prm[o.ce + t]; we[t] = prm[o.we + t]; }
+  __syncthreads();
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float gwe[H], gue[H], gce[H], gw0[1] = {0.f};
+#pragma unroll
+  for (int c = 0; c < H; ++c) gwe[c] = gue[c] = gce[c] = 0.f;
+  if (i < n) {
+    float p[H], dp[H];
+#pragma unroll
+    for (int c = 0; c < H; ++c) { p[c] = P[(int64_t)i * H + c]; dp[c] = 0.f; }
+    for (int t = lrp[i]; t < lrp[i + 1]; ++t) {
+      const int j = lci[t];
+      const float a = al[t], dl = dlhat[t];
+      gw0[0] += dl * a;
+#pragma unroll
+      for (int c = 0; c < H; ++c) {
+        const float z = tanhf(p[c] + Q[(int64_t)j * H + c] + ue[c] * a + ce[c]);
+        gwe[c] += dl * z;
+        const float da = dl * we[c] * (1.f - z * z);
+        gue[c] += da * a;
+        gce[c] += da;
+        dp[c] += da;
+        atomicAdd(dQ + (int64_t)j * H + c, da);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < H; ++c) dP[(int64_t)i * H + c] = dp[c];
+  }
+  block_atomic<H>(gwe, grad + o.we);
+  __syncthreads();
+  block_atomic<H>(gue, grad + o.ue);
+  __syncthreads();
+  block_atomic<H>(gce, grad + o.ce);
+  __syncthreads();
+  block_atomic<1>(gw0, grad + o.w0);
+}
+
+// out[a][b] += sum_i A_i[a] * B_i[b] (A rows of width DA, B rows of width DB); one
+// thread per (a, b), rows in tiles of 32 through shared memory.
+template <int DA, int DB>
+__global__ void lf_outer(int n, const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ out) {
+  __shared__ float ta[32][DA], tb[32][DB];
+  const int a = threadIdx.x / DB, b = threadIdx.x % DB;
+  float s = 0.f;
+  for (int base = blockIdx.x * 32; base < n; base += gridDim.x * 32) {
+    for (int t = threadIdx.x; t < 32 * DA; t += blockDim.x) {
+      const int r = base + t / DA;
+      ta[t / DA][t % DA] = r < n ? A[(int64_t)r * DA + t % DA] : 0.f;
+    }
+    for (int t = threadIdx.x; t < 32 * DB; t += blockDim.x) {
+      const int r = base + t / DB;
+      tb[t / DB][t % DB] = r < n ? B[(int64_t)r * DB + t % DB] : 0.f;
+    }
+    __syncthreads();
+    if (threadIdx.x < DA * DB)
+      for (int r = 0; r < 32; ++r) s += ta[r][a] * tb[r][b];
+    __syncthreads();
+  }
+  if (threadIdx.x < DA * DB) atomicAdd(out + a * DB + b, s);
+}
+
+// sum over rows of A (width D) into out[D]
+template <int D>
+__global__ void lf_colsum(int n, const float* __restrict__ A, float* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float v[D];
+#pragma unroll
+  for (int c = 0; c < D; ++c) v[c] = i < n ? A[(int64_t)i * D + c] : 0.f;
+  block_atomic<D>(v, out);
+}
+
+// Node head backward: dH = U^T dP + V^T dQ + q drho  (weights grads via lf_outer/lf_colsum)
+__global__ void lf_head_nodes_bwd(int n, const float* __restrict__ prm, Off o, const float* __restrict__ dP,
+                                  const float* __restrict__ dQ, const float* __restrict__ drho,
+                                  float* __restrict__ dH) {
+  __shared__ float U[H * H], V[H * H], q[H];
+  for (int t = threadIdx.x; t < H * H; t += blockDim.x) { U[t] = prm[o.U + t]; V[t] = prm[o.V + t]; }
+  for (int t = threadIdx.x; t < H; t += blockDim.x) q[t] = prm[o.q + t];
+  __syncthreads();
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float dp[H], dq[H];
+#pragma unroll
+  for (int c = 0; c < H; ++c) { dp[c] = dP[(int64_t)i * H + c]; dq[c] = dQ[(int64_t)i * H + c]; }
+  const float dr = drho[i];
+#pragma unroll
+  for (int c = 0; c < H; ++c) {
+    float s = q[c] * dr;
+#pragma unroll
+    for (int a = 0; a < H; ++a) s += U[a * H + c] * dp[a] + V[a * H + c] * dq[a];
+    dH[(int64_t)i * H + c] = s;
+  }
+}
+
+// Layer backward, per row: dpre = dH (1 - H^2); S = Ws^T dpre; Ta = Wa^T dpre; Tb = Wb^T dpre.
+template <int DIN>
+__global__ void lf_layer_bwd(int n, const float* __restrict__ prm, int ows, int owa, int owb,
+                             const float* __restrict__ Hout, const float* __restrict__ dH, float* __restrict__ dpre,
+                             float* __restrict__ S, float* __restrict__ Ta, float* __restrict__ Tb) {
+  __shared__ float w[3 * H * DIN];
+  for (int t = threadIdx.x; t < H * DIN; t += blockDim.x) {
+    w[t] = prm[ows + t];
+    w[H * DIN + t] = prm[owa + t];
+    w[2 * H * DIN + t] = prm[owb + t];
+  }
+  __syncthreads();
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float d[H];
+#pragma unroll
+  for (int o = 0; o < H; ++o) {
+    const float h = Hout[(int64_t)i * H + o];
+    d[o] = dH[(int64_t)i * H + o] * (1.f - h * h);
+    dpre[(int64_t)i * H + o] = d[o];
+  }
+#pragma unroll
+  for (int c = 0; c < DIN; ++c) {
+    float s = 0.f, a = 0.f, b = 0.f;
+#pragma unroll
+    for (int o = 0; o < H; ++o) {
+      s += w[o * DIN + c] * d[o];
+      a += w[H * DIN + o * DIN + c] * d[o];
+      b += w[2 * H * DIN + o * DIN + c] * d[o];
+    }
+    S[(int64_t)i * DIN + c] = s;
+    Ta[(int64_t)i * DIN + c] = a;
+    Tb[(int64_t)i * DIN + c] = b;
+  }
+}
+
+// dX = S + |A^_off| Ta + A^_off Tb
+template <int DIN>
+__global__ void lf_agg_bwd(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                           const float* __restrict__ ahat, const float* __restrict__ S, const float* __restrict__ Ta,
+                           const float* __restrict__ Tb, float* __restrict__ dX) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float s[DIN];
+#pragma unroll
+  for (int c = 0; c < DIN; ++c) s[c] = S[(int64_t)i * DIN + c];
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const int j = ci[k];
+    if (j == i) continue;
+    const float w = ahat[k], aw = fabsf(w);
+#pragma unroll
+    for (int c = 0; c < DIN; ++c) s[c] += aw * Ta[(int64_t)j * DIN + c] + w * Tb[(int64_t)j * DIN + c];
+  }
+#pragma unroll
+  for (int c = 0; c < DIN; ++c) dX[(int64_t)i * DIN + c] = s[c];
+}
+
+__global__ void lf_adam(int np, float* __restrict__ prm, const float* __restrict__ g, float* __restrict__ m1,
+                        float* __restrict__ m2, float lr, float b1, float b2, float eps, float c1, float c2,
+                        float clip) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  float gi = fminf(fmaxf(g[i], -clip), clip);
+  m1[i] = b1 * m1[i] + (1.f - b1) * gi;
+  m2[i] = b2 * m2[i] + (1.f - b2) * gi * gi;
+  prm[i] -= lr * (m1[i] / c1) / (sqrtf(m2[i] / c2) + eps);
+}
+
+// FP64 factor of A from the network output: sigma^2 = sig^2 / d_i, L_ij = L^_ij sqrt(d_i / d_j).
+__global__ void lf_to_factor(int n, const int* __restrict__ lrp, const int* __restrict__ lci,
+                             const float* __restrict__ lhat, const float* __restrict__ sig,
+                             const double* __restrict__ dis, double* __restrict__ sig2, double* __restrict__ lva) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double s = sig[i];
+  sig2[i] = s * s * dis[i] * dis[i];
+  for (int t = lrp[i]; t < lrp[i + 1]; ++t) lva[t] = (double)lhat[t] * dis[lci[t]] / dis[i];
+}
+
+int blocks(int64_t n) { return (int)((n + LF_THREADS - 1) / LF_THREADS); }
+
+}  // namespace
+
+int lf_param_count() { return offsets().total; }
+
+void lf_init_params(uint64_t seed, float* h) {
+  Off o = offsets();
+  uint64_t st = seed * 0x9E3779B97F4A7C15ull + 12345;
+  auto rnd = [&]() {  // splitmix64 -> uniform(-1, 1)
+    st += 0x9E3779B97F4A7C15ull;
+    uint64_t z = st;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (float)((double)(z >> 11) / 9007199254740992.0 * 2.0 - 1.0);
+  };
+  for (int i = 0; i < o.total; ++i) h[i] = 0.f;
+  for (int l = 0; l < LF_LAYERS; ++l) {
+    const float sc = 1.f / std::sqrt((float)(3 * o.din[l]));
+    for (int t = 0; t < H * o.din[l]; ++t) {
+      h[o.ws[l] + t] = sc * rnd();
+      h[o.wa[l] + t] = sc * rnd();
+      h[o.wb[l] + t] = sc * rnd();
+    }
+  }
+  const float sh = 1.f / std::sqrt((float)H);
+  for (int t = 0; t < H * H; ++t) { h[o.U + t] = sh * rnd(); h[o.V + t] = sh * rnd(); }
+  for (int t = 0; t < H; ++t) { h[o.ue + t] = sh * rnd(); h[o.ce + t] = 0.1f * rnd(); }
+  h[o.w0] = -1.f;  // we = q = q0 = 0: the first-order factor I - tril(A^)
+}
+
+void LfGraph::prepare(const SystemData& S, const FsaiFactor& F) {
+  cudaStream_t s = S.ctx->stream;
+  n = (int)S.n_free;
+  nnz = S.nnz;
+  nnzl = F.nnz;
+  ahat.alloc(std::max<int64_t>(nnz, 1), s);
+  dis.alloc(n, s);
+  x0.alloc((int64_t)n * D0, s);
+  al.alloc(std::max<int64_t>(nnzl, 1), s);
+  for (int l = 0; l < LF_LAYERS; ++l) {
+    const int din = l == 0 ? D0 : H;
+    ya[l].alloc((int64_t)n * din, s);
+    yb[l].alloc((int64_t)n * din, s);
+    h[l].alloc((int64_t)n * H, s);
+  }
+  P.alloc((int64_t)n * H, s);
+  Q.alloc((int64_t)n * H, s);
+  sig.alloc(n, s);
+  lhat.alloc(std::max<int64_t>(nnzl, 1), s);
+  lf_prep<<<blocks(n), LF_THREADS, 0, s>>>(n, S.dpn, S.row_ptr.p, S.col.p, S.val.p, S.free_map.p, ahat.p, dis.p, x0.p);
+  TPT_CHECK_LAUNCH();
+  lf_prep2<<<blocks(n), LF_THREADS, 0, s>>>(n, S.dpn, S.row_ptr.p, S.col.p, S.val.p, S.free_map.p, dis.p, ahat.p,
+                                            x0.p);
+  TPT_CHECK_LAUNCH();
+  lf_pattern_values<<<blocks(n), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, ahat.p, F.rp.p, F.ci.p, al.p);
+  TPT_CHECK_LAUNCH();
+  ready = true;
+}
+
+void lf_forward(const SystemData& S, const FsaiFactor& F, LfGraph& G, const float* prm) {
+  cudaStream_t s = S.ctx->stream;
+  const Off o = offsets();
+  const int n = G.n;
+  const float* in = G.x0.p;
+  for (int l = 0; l < LF_LAYERS; ++l) {
+    if (l == 0) {
+      lf_agg<D0><<<blocks(n), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, G.ahat.p, in, G.ya[l].p, G.yb[l].p);
+      TPT_CHECK_LAUNCH();
+      lf_layer<D0><<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o.ws[l], o.wa[l], o.wb[l], o.b[l], in, G.ya[l].p,
+                                                    G.yb[l].p, G.h[l].p);
+    } else {
+      lf_agg<H><<<blocks(n), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, G.ahat.p, in, G.ya[l].p, G.yb[l].p);
+      TPT_CHECK_LAUNCH();
+      lf_layer<H><<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o.ws[l], o.wa[l], o.wb[l], o.b[l], in, G.ya[l].p,
+                                                   G.yb[l].p, G.h[l].p);
+    }
+    TPT_CHECK_LAUNCH();
+    in = G.h[l].p;
+  }
+  lf_head_nodes<<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o, in, G.P.p, G.Q.p, G.sig.p);
+  TPT_CHECK_LAUNCH();
+  lf_head_edges<<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o, F.rp.p, F.ci.p, G.al.p, G.P.p, G.Q.p, G.lhat.p);
+  TPT_CHECK_LAUNCH();
+}
+
+double lf_loss_grad(const SystemData& S, const FsaiFactor& F, LfGraph& G, const float* prm, float* grad,
+                    const float* d_probes, int m) {
+  cudaStream_t s = S.ctx->stream;
+  const Off o = offsets();
+  const int n = G.n;
+  const int64_t nm = (int64_t)n * m;
+  lf_forward(S, F, G, prm);
+  DevBuf<float> U1, V1, W1, GW, GV, GU;
+  U1.alloc(nm, s); V1.alloc(nm, s); W1.alloc(nm, s); GW.alloc(nm, s); GV.alloc(nm, s); GU.alloc(nm, s);
+  DevBuf<double> loss;
+  loss.alloc(1, s);
+  loss.zero();
+  lf_gt<<<blocks(nm), LF_THREADS, 0, s>>>(n, m, F.trp.p, F.tci.p, F.perm.p, G.lhat.p, G.sig.p, d_probes, U1.p);
+  TPT_CHECK_LAUNCH();
+  lf_a<<<blocks(nm), LF_THREADS, 0, s>>>(n, m, S.row_ptr.p, S.col.p, G.ahat.p, U1.p, V1.p);
+  TPT_CHECK_LAUNCH();
+  lf_g<<<blocks(nm), LF_THREADS, 0, s>>>(n, m, F.rp.p, F.ci.p, G.lhat.p, G.sig.p, V1.p, W1.p);
+  TPT_CHECK_LAUNCH();
+  const float scale = 1.f / (float)nm;
+  lf_residual<<<blocks(nm), LF_THREADS, 0, s>>>(nm, W1.p, d_probes, GW.p, loss.p, scale);
+  TPT_CHECK_LAUNCH();
+  if (grad) {
+    lf_gt<<<blocks(nm), LF_THREADS, 0, s>>>(n, m, F.trp.p, F.tci.p, F.perm.p, G.lhat.p, G.sig.p, GW.p, GV.p);
+    TPT_CHECK_LAUNCH();
+    lf_a<<<blocks(nm), LF_THREADS, 0, s>>>(n, m, S.row_ptr.p, S.col.p, G.ahat.p, GV.p, GU.p);
+    TPT_CHECK_LAUNCH();
+    DevBuf<float> dl, drho, dP, dQ, dH, dpre, Sx, Ta, Tb, dX;
+    dl.alloc(std::max<int64_t>(G.nnzl, 1), s);
+    drho.alloc(n, s);
+    dP.alloc((int64_t)n * H, s);
+    dQ.alloc((int64_t)n * H, s);
+    dQ.zero();
+    dH.alloc((int64_t)n * H, s);
+    dpre.alloc((int64_t)n * H, s);
+    Sx.alloc((int64_t)n * H, s);
+    Ta.alloc((int64_t)n * H, s);
+    Tb.alloc((int64_t)n * H, s);
+    dX.alloc((int64_t)n * H, s);
+    lf_dg<<<blocks(n), LF_THREADS, 0, s>>>(n, m, F.rp.p, F.ci.p, G.lhat.p, G.sig.p, GW.p, V1.p, d_probes, GU.p, dl.p,
+                                           drho.p);
+    TPT_CHECK_LAUNCH();
+    lf_head_edges_bwd<<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o, grad, F.rp.p, F.ci.p, G.al.p, G.P.p, G.Q.p, dl.p,
+                                                       dP.p, dQ.p);
+    TPT_CHECK_LAUNCH();
+    const float* hl = G.h[LF_LAYERS - 1].p;
+    const int og = std::min(1024, std::max(1, n / 32));
+    lf_outer<H, H><<<og, 256, 0, s>>>(n, dP.p, hl, grad + o.U);
+    TPT_CHECK_LAUNCH();
+    lf_outer<H, H><<<og, 256, 0, s>>>(n, dQ.p, hl, grad + o.V);
+    TPT_CHECK_LAUNCH();
+    lf_outer<1, H><<<og, 256, 0, s>>>(n, drho.p, hl, grad + o.q);
+    TPT_CHECK_LAUNCH();
+    lf_colsum<1><<<blocks(n), LF_THREADS, 0, s>>>(n, drho.p, grad + o.q0);
+    TPT_CHECK_LAUNCH();
+    lf_head_nodes_bwd<<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o, dP.p, dQ.p, drho.p, dH.p);
+    TPT_CHECK_LAUNCH();
+    for (int l = LF_LAYERS - 1; l >= 0; --l) {
+      const float* xin = l == 0 ? G.x0.p : G.h[l - 1].p;
+      if (l == 0) {
+        lf_layer_bwd<D0><<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o.ws[l], o.wa[l], o.wb[l], G.h[l].p, dH.p, dpre.p,
+                                                         Sx.p, Ta.p, Tb.p);
+        TPT_CHECK_LAUNCH();
+        lf_outer<H, D0><<<og, 256, 0, s>>>(n, dpre.p, xin, grad + o.ws[l]);
+        lf_outer<H, D0><<<og, 256, 0, s>>>(n, dpre.p, G.ya[l].p, grad + o.wa[l]);
+        lf_outer<H, D0><<<og, 256, 0, s>>>(n, dpre.p, G.yb[l].p, grad + o.wb[l]);
+      } else {
+        lf_layer_bwd<H><<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o.ws[l], o.wa[l], o.wb[l], G.h[l].p, dH.p, dpre.p,
+                                                        Sx.p, Ta.p, Tb.p);
+        TPT_CHECK_LAUNCH();
+        lf_outer<H, H><<<og, 256, 0, s>>>(n, dpre.p, xin, grad + o.ws[l]);
+        lf_outer<H, H><<<og, 256, 0, s>>>(n, dpre.p, G.ya[l].p, grad + o.wa[l]);
+        lf_outer<H, H><<<og, 256, 0, s>>>(n, dpre.p, G.yb[l].p, grad + o.wb[l]);
+        TPT_CHECK_LAUNCH();
+        lf_agg_bwd<H><<<blocks(n), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, G.ahat.p, Sx.p, Ta.p, Tb.p, dX.p);
+        TPT_CHECK_LAUNCH();
+        TPT_CUDA(cudaMemcpyAsync(dH.p, dX.p, (size_t)n * H * sizeof(float), cudaMemcpyDeviceToDevice, s));
+      }
+      TPT_CHECK_LAUNCH();
+      lf_colsum<H><<<blocks(n), LF_THREADS, 0, s>>>(n, dpre.p, grad + o.b[l]);
+      TPT_CHECK_LAUNCH();
+    }
+  }
+  double h = 0.0;
+  TPT_CUDA(cudaMemcpyAsync(&h, loss.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+  TPT_CUDA(cudaStreamSynchronize(s));
+  return h / (double)nm;
+}
+
+void lf_adam_step(cudaStream_t s, int np, float* prm, const float* grad, float* m1, float* m2, int step, float lr,
+                  float clip) {
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - std::pow(b1, (float)step), c2 = 1.f - std::pow(b2, (float)step);
+  lf_adam<<<blocks(np), LF_THREADS, 0, s>>>(np, prm, grad, m1, m2, lr, b1, b2, 1e-8f, c1, c2, clip);
+  TPT_CHECK_LAUNCH();
+}
+
+void lf_factor_fp64(const SystemData& S, const FsaiFactor& F, const LfGraph& G, double* sig2, double* lva) {
+  lf_to_factor<<<blocks(G.n), LF_THREADS, 0, S.ctx->stream>>>(G.n, F.rp.p, F.ci.p, G.lhat.p, G.sig.p, G.dis.p, sig2,
+                                                              lva);
+  TPT_CHECK_LAUNCH();
+}
+
+}  // namespace tptfem

@@ -57,6 +57,7 @@ struct MatrixData {
 };
 
 struct SolverWork;  // solver.cu
+struct LfModel;     // lfsai.hpp
 
 // FSAI factor G = diag(sigma) (I + L): sigma^2 (FP32, one per row) and the
 // strictly lower L (FP16, CSR) with its explicit transpose (CSR, FP16);
@@ -97,6 +98,7 @@ struct SystemData {
   DevBuf<double> fred, x;
   DevBuf<double> u_fixed;  // full-length vector holding the prescribed values
   std::shared_ptr<SolverWork> work;
+  std::shared_ptr<LfModel> lmodel;  // network used by the learned-FSAI solver
   ~SystemData();
 };
 

@@ -32,6 +32,7 @@
 
 #include <type_traits>
 
+#include "lfsai.hpp"
 #include "nbsell.cuh"
 #include "objects.hpp"
 #include "solver_kernels.cuh"
@@ -216,8 +217,12 @@ struct SolverWork {
   Engine<double> f64;
   Engine<float> f32;       // Jacobi, FP32 Krylov
   Engine<double> f64_fsai; // FSAI (FP16 factor), FP64 Krylov
-  FsaiFactor fsai;
+  Engine<double> f64_lf;   // learned FSAI (FP16 factor), FP64 Krylov
+  FsaiFactor fsai, lf;
+  LfGraph lgraph;
+  const FsaiFactor* nb_factor = nullptr;  // factor whose blocks S.nb holds
   bool f64_ready = false, f32_ready = false, fsai_ready = false, fsai_failed = false;
+  bool lf_ready = false, lf_engine = false;
   DevBuf<double> rhi;   // FP64 true residual
   DevBuf<double> sc;    // scalars
   DevBuf<unsigned> tk;  // tickets for standalone reductions
@@ -373,7 +378,32 @@ void prepare_fsai_engine(SystemData& S, Engine<double>& E, const FsaiFactor& F, 
   E.pc.gt_rp = F.trp.p; E.pc.gt_ci = F.tci.p; E.pc.gt_va = F.tva.p;
 }
 
+// Learned factor values: network forward on this system, converted to the
+// FP64 factor of A and installed (sigma^2 FP32, L FP16).  False if invalid.
+bool learned_factor(SystemData& S, SolverWork& W) {
+  cudaStream_t s = S.ctx->stream;
+  fsai_build_pattern(S, W.lf);
+  if (W.lf.overflow) return false;
+  if (!W.lgraph.ready) W.lgraph.prepare(S, W.lf);
+  lf_forward(S, W.lf, W.lgraph, S.lmodel->prm.p);
+  DevBuf<double> sig2, lva;
+  sig2.alloc(W.lf.n, s);
+  lva.alloc(std::max<int64_t>(W.lf.nnz, 1), s);
+  lf_factor_fp64(S, W.lf, W.lgraph, sig2.p, lva.p);
+  return fsai_set_values(S, W.lf, sig2.p, lva.p);
+}
+
 }  // namespace
+
+LfGraph& system_lf_graph(SystemData& S, FsaiFactor** F) {
+  ensure_work(S);
+  SolverWork& W = *S.work;
+  fsai_build_pattern(S, W.lf);
+  TPT_REQUIRE(!W.lf.overflow, TPTFEM_ERR_CREATION, "factor pattern rows exceed the device limit");
+  if (!W.lgraph.ready) W.lgraph.prepare(S, W.lf);
+  *F = &W.lf;
+  return W.lgraph;
+}
 
 void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats& st) {
   tptfem_context* ctx = S.ctx;
@@ -383,8 +413,8 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
   int batch = o.batch > 0 ? o.batch : 32;
   batch += batch & 1;
   st = tptfem_solve_stats{};
-  TPT_REQUIRE(o.solver >= TPTFEM_SOLVER_JACOBI_PCG && o.solver <= TPTFEM_SOLVER_FSAI_MP_PCG, TPTFEM_ERR_INVALID_ARG,
-              "unknown solver");
+  TPT_REQUIRE(o.solver >= TPTFEM_SOLVER_JACOBI_PCG && o.solver <= TPTFEM_SOLVER_LEARNED_FSAI_PCG,
+              TPTFEM_ERR_INVALID_ARG, "unknown solver");
   int solver = o.solver;
   if (S.n_free == 0) {
     st.solver_used = solver;
@@ -392,7 +422,74 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
   }
   ensure_work(S);
   SolverWork& W = *S.work;
+  if (solver == TPTFEM_SOLVER_LEARNED_FSAI_PCG) {
+    TPT_REQUIRE(S.lmodel != nullptr, TPTFEM_ERR_INVALID_ARG, "no learned model attached to this system");
+    TPT_CUDA(cudaEventRecord(ctx->ev[0], s));
+    const bool fresh = (o.flags & TPTFEM_SOLVE_FRESH_SETUP) || !W.lf_ready;
+    bool ok = !fresh || learned_factor(S, W);
+    if (fresh && ok && !W.lf_engine) {
+      prepare_fsai_engine(S, W.f64_lf, W.lf, batch);
+      if (!(o.flags & TPTFEM_SOLVE_CSR_ONLY) && nb_build_operator(S)) {
+        const bool nbpc = nb_fill_factor(S, W.lf);
+        W.f64_lf.use_nb(&S.nb, true, nbpc);
+        if (nbpc) W.nb_factor = &W.lf;
+      }
+      W.lf_engine = true;
+    } else if (fresh && ok && W.f64_lf.nb_pc) {
+      nb_fill_factor(S, W.lf);
+      W.nb_factor = &W.lf;
+    }
+    W.lf_ready = ok;
+    if (ok) {
+      if (W.f64_lf.nb_pc && W.nb_factor != &W.lf) {
+        nb_fill_factor(S, W.lf);
+        W.nb_factor = &W.lf;
+      }
+      st.solver_used = solver;
+      TPT_CUDA(cudaEventRecord(ctx->ev[1], s));
+      const double bb = norm2_b(S);
+      const double bnorm = std::sqrt(bb);
+      int64_t iters = 0;
+      bool broke = false;
+      if (bb == 0.0) {
+        S.x.zero();
+      } else {
+        const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : 1e-3;
+        try {
+          iters = run_reliable<double>(S, W.f64_lf, tol, delta, max_it, bnorm, st);
+        } catch (const Error& e) {
+          if (e.status != TPTFEM_ERR_BREAKDOWN) throw;
+          broke = true;
+        }
+      }
+      const double rel = bb == 0.0 ? 0.0 : std::sqrt(true_residual2(S, S.x.p)) / bnorm;
+      if (!broke && rel <= tol) {
+        TPT_CUDA(cudaEventRecord(ctx->ev[2], s));
+        TPT_CUDA(cudaEventSynchronize(ctx->ev[2]));
+        float ms0 = 0.f, ms1 = 0.f;
+        TPT_CUDA(cudaEventElapsedTime(&ms0, ctx->ev[0], ctx->ev[1]));
+        TPT_CUDA(cudaEventElapsedTime(&ms1, ctx->ev[1], ctx->ev[2]));
+        st.iterations = iters;
+        st.rel_residual = rel;
+        st.setup_ms = ms0;
+        st.solve_ms = ms1;
+        return;
+      }
+    }
+    // the learned factor was invalid, broke down or did not converge: the plain
+    // FP64 Jacobi-PCG solves the system instead
+    tptfem_solver_opts fb = o;
+    fb.solver = TPTFEM_SOLVER_JACOBI_PCG;
+    system_solve(S, fb, st);
+    st.fell_back = 1;
+    return;
+  }
   TPT_CUDA(cudaEventRecord(ctx->ev[0], s));
+  if (solver == TPTFEM_SOLVER_FSAI_MP_PCG && W.fsai_ready && W.f64_fsai.nb_pc && W.nb_factor != &W.fsai &&
+      !(o.flags & TPTFEM_SOLVE_FRESH_SETUP)) {
+    nb_fill_factor(S, W.fsai);
+    W.nb_factor = &W.fsai;
+  }
   if (o.flags & TPTFEM_SOLVE_FRESH_SETUP) {
     // keep patterns, graphs and buffers; recompute every value of the preconditioner
     if (solver == TPTFEM_SOLVER_FSAI_MP_PCG && W.fsai_ready) {
@@ -401,6 +498,7 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
         W.fsai_failed = true;
       } else if (W.f64_fsai.nb_pc) {
         nb_fill_factor(S, W.fsai);
+        W.nb_factor = &W.fsai;
       }
     } else if (solver == TPTFEM_SOLVER_JACOBI_PCG && W.f64_ready) {
       refresh_jacobi<double>(S, W.f64);
@@ -412,8 +510,11 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
     if (!W.fsai_ready && !W.fsai_failed) {
       if (fsai_classic(S, W.fsai)) {
         prepare_fsai_engine(S, W.f64_fsai, W.fsai, batch);
-        if (!(o.flags & TPTFEM_SOLVE_CSR_ONLY) && nb_build_operator(S))
-          W.f64_fsai.use_nb(&S.nb, true, nb_fill_factor(S, W.fsai));
+        if (!(o.flags & TPTFEM_SOLVE_CSR_ONLY) && nb_build_operator(S)) {
+          const bool nbpc = nb_fill_factor(S, W.fsai);
+          W.f64_fsai.use_nb(&S.nb, true, nbpc);
+          if (nbpc) W.nb_factor = &W.fsai;
+        }
         W.fsai_ready = true;
       } else {
         W.fsai_failed = true;

@@ -18,7 +18,8 @@ import numpy as np
 
 from . import _native as N
 from ._native import (CELL_QUAD4, CELL_TET4, MODEL_BAR_AXIAL, MODEL_CONTINUUM_3D, MODEL_PLANE_STRAIN,
-                      MODEL_PLANE_STRESS, SOLVER_FSAI_MP_PCG, SOLVER_JACOBI_PCG, SOLVER_MP_PCG, SolverOpts,
+                      MODEL_PLANE_STRESS, SOLVER_FSAI_MP_PCG, SOLVER_JACOBI_PCG, SOLVER_LEARNED_FSAI_PCG,
+                      SOLVER_MP_PCG, SolverOpts,
                       SolveStats)
 
 __all__ = [
@@ -26,7 +27,7 @@ __all__ = [
     "load_poisson_source", "load_body", "apply_traction", "reduce_system", "solve_with_dirichlet",
     "solve_poisson", "solve_elasticity", "SolverOpts", "SolveStats", "CELL_TET4", "CELL_QUAD4",
     "MODEL_CONTINUUM_3D", "MODEL_PLANE_STRESS", "MODEL_PLANE_STRAIN", "SOLVER_JACOBI_PCG", "SOLVER_MP_PCG",
-    "SOLVER_FSAI_MP_PCG",
+    "SOLVER_FSAI_MP_PCG", "SOLVER_LEARNED_FSAI_PCG",
 ]
 
 

@@ -20,7 +20,7 @@ STATUS_NAMES = {
 }
 CELL_QUAD4, CELL_TET4 = 3, 4
 MODEL_BAR_AXIAL, MODEL_PLANE_STRESS, MODEL_PLANE_STRAIN, MODEL_CONTINUUM_3D = 0, 1, 2, 3
-SOLVER_JACOBI_PCG, SOLVER_MP_PCG, SOLVER_FSAI_MP_PCG = 0, 1, 2
+SOLVER_JACOBI_PCG, SOLVER_MP_PCG, SOLVER_FSAI_MP_PCG, SOLVER_LEARNED_FSAI_PCG = 0, 1, 2, 3
 SOLVE_FRESH_SETUP = 1
 SOLVE_CSR_ONLY = 2
 
@@ -76,6 +76,14 @@ SIGNATURES = {
     "tptfem_system_free": (None, [_vp]),
     "tptfem_system_profile_spmv": (C.c_int, [_vp, _vp, C.c_int, _pd, _pd, _pd, _pd]),
     "tptfem_system_fsai": (C.c_int, [_vp, _vp, _pi64]),
+    "tptfem_lfsai_param_count": (C.c_int64, []),
+    "tptfem_lfsai_create": (C.c_int, [_vp, C.c_uint64, _pp]),
+    "tptfem_lfsai_free": (None, [_vp]),
+    "tptfem_lfsai_get_params": (C.c_int, [_vp, _vp, _vp]),
+    "tptfem_lfsai_set_params": (C.c_int, [_vp, _vp, _vp]),
+    "tptfem_lfsai_loss": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int32, C.c_int32, _pd, _vp]),
+    "tptfem_lfsai_adam": (C.c_int, [_vp, _vp, C.c_double, C.c_double]),
+    "tptfem_system_attach_lfsai": (C.c_int, [_vp, _vp, _vp]),
     "tptfem_rel_residual_noalloc": (C.c_int, [C.c_int, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _pd, C.c_char_p,
                                               C.c_size_t]),
     "tptfem_system_fsai_download": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
