@@ -249,10 +249,11 @@ tptfem_status tptfem_solve_elasticity(tptfem_context* ctx, tptfem_mesh* mesh, in
 
 /* ---- learned FSAI preconditioner (no counterpart in the reference) ----------
  * A small message-passing network over the graph of the reduced matrix that
- * emits the FSAI factor G = diag(s)(I + L) on the node-block lower pattern
- * (SPD M^-1 = G^T G for any weights).  Trained on the device by the library's
- * own forward/backward kernels on loss = mean_k ||G^ A^ G^T z_k - z_k||^2 / n
- * (A^ = D^-1/2 A D^-1/2) over caller-supplied probe vectors z_k. */
+ * emits the off-diagonal values L of the FSAI factor G = diag(s)(I + L) on the
+ * node-block lower pattern; s_i = q_i^-1/2 with q_i = (e_i + L_i) A^ (e_i + L_i)^T
+ * (A^ = D^-1/2 A D^-1/2), so M^-1 = G^T G is SPD for any weights.  Trained on
+ * the device by the library's own forward/backward kernels on Kaporin's
+ * condition number of G^ A^ G^T: loss = (1/n) sum_i log q_i. */
 typedef struct tptfem_lfsai tptfem_lfsai;
 /* Number of FP32 parameters of the network. */
 int64_t tptfem_lfsai_param_count(void);
@@ -261,11 +262,10 @@ tptfem_status tptfem_lfsai_create(tptfem_context* ctx, uint64_t seed, tptfem_lfs
 void tptfem_lfsai_free(tptfem_lfsai* model);
 tptfem_status tptfem_lfsai_get_params(tptfem_context* ctx, const tptfem_lfsai* model, float* params);
 tptfem_status tptfem_lfsai_set_params(tptfem_context* ctx, tptfem_lfsai* model, const float* params);
-/* Loss on `sys` for m host probe vectors (n_free x m, row-major).  with_grad:
- * ADD d loss/d params to the model's gradient buffer (and copy the
- * accumulated gradient to `grad` when it is non-NULL). */
-tptfem_status tptfem_lfsai_loss(tptfem_context* ctx, tptfem_lfsai* model, tptfem_system* sys, const float* probes,
-                                int32_t m, int32_t with_grad, double* loss, float* grad);
+/* Loss on `sys`.  with_grad: ADD d loss/d params to the model's gradient
+ * buffer (and copy the accumulated gradient to `grad` when it is non-NULL). */
+tptfem_status tptfem_lfsai_loss(tptfem_context* ctx, tptfem_lfsai* model, tptfem_system* sys, int32_t with_grad,
+                                double* loss, float* grad);
 /* Adam step with the accumulated gradient (clipped to +-clip), then zero it. */
 tptfem_status tptfem_lfsai_adam(tptfem_context* ctx, tptfem_lfsai* model, double lr, double clip);
 /* Use `model` for TPTFEM_SOLVER_LEARNED_FSAI_PCG solves of `sys` (NULL detaches). */

@@ -4,6 +4,15 @@ The reference has no learned preconditioner; this numpy restatement (FP64) of
 the device network in tpt-fem_b200/csrc/lfsai.cu is the checker for the
 device's forward and backward kernels.  Its own analytic gradient is checked
 against central finite differences in tests/test_lfsai_oracle.py.
+
+Network (A^ = D^-1/2 A D^-1/2):
+  h0_i  = [1, sum|a^_ij|, sum a^_ij, sum a^_ij^2, onehot(dof component), deg/40]
+  h_l+1 = tanh(Ws h_l + Wa (|A^_off| h_l) + Wb (A^_off h_l) + b)
+  z_ij  = tanh(U h_i + V h_j + ue a^_ij + ce),  L^_ij = we . z_ij + w0 a^_ij
+  g_i   = e_i + L^_i,  q_i = g_i A^ g_i^T,  sig_i = q_i^-1/2
+  G^    = diag(sig) (I + L^)          (unit diagonal of G^ A^ G^T)
+Objective (Kaporin's condition number of G^ A^ G^T, up to the constant
+log det A^ / n):  loss = (1/n) sum_i log q_i.
 """
 from __future__ import annotations
 
@@ -20,8 +29,7 @@ def offsets():
         for name, size in (("ws", H * din), ("wa", H * din), ("wb", H * din), ("b", H)):
             o[f"{name}{l}"] = (p, size)
             p += size
-    for name, size in (("U", H * H), ("V", H * H), ("ue", H), ("ce", H), ("we", H), ("w0", 1), ("q", H),
-                       ("q0", 1)):
+    for name, size in (("U", H * H), ("V", H * H), ("ue", H), ("ce", H), ("we", H), ("w0", 1)):
         o[name] = (p, size)
         p += size
     o["total"] = p
@@ -48,8 +56,6 @@ class Graph:
         self.dis = 1.0 / np.sqrt(d)
         ah = sp.diags(self.dis) @ A @ sp.diags(self.dis)
         self.ahat = sp.csr_matrix(ah)
-        off = self.ahat - sp.diags(self.ahat.diagonal())
-        off.eliminate_zeros()
         # keep explicit structure of A's off-diagonal entries (zeros included)
         rows = np.repeat(np.arange(n), np.diff(rp))
         m = rows != ci
@@ -73,7 +79,16 @@ class Graph:
         self.al = np.asarray(full[self.lrow, self.lci]).ravel() if len(self.lci) else np.zeros(0)
 
 
-def forward(params, g, keep=False):
+def kaporin(g, lhat):
+    """q_i, W = (I + L^) A^ (rows of the pattern) and the loss (1/n) sum log q_i."""
+    Gt = sp.csr_matrix(sp.identity(g.n) + sp.csr_matrix((lhat, (g.lrow, g.lci)), shape=(g.n, g.n)))
+    W = sp.csr_matrix(Gt @ g.ahat)
+    q = np.asarray(W.multiply(Gt).sum(axis=1)).ravel()
+    w_lower = np.asarray(W[g.lrow, g.lci]).ravel() if len(g.lci) else np.zeros(0)
+    return q, w_lower, float(np.mean(np.log(q)))
+
+
+def forward(params, g):
     p = params.astype(np.float64)
     acts = []
     x = g.x0
@@ -87,37 +102,24 @@ def forward(params, g, keep=False):
         x = h
     U, V = view(p, "U", (H, H)), view(p, "V", (H, H))
     P, Q = x @ U.T, x @ V.T
-    rho = x @ view(p, "q") + view(p, "q0")[0]
-    sig = np.exp(0.5 * rho)
     ue, ce, we, w0 = view(p, "ue"), view(p, "ce"), view(p, "we"), view(p, "w0")[0]
     a = P[g.lrow] + Q[g.lci] + np.outer(g.al, ue) + ce
     z = np.tanh(a)
     lhat = w0 * g.al + z @ we
+    q, w_lower, loss = kaporin(g, lhat)
+    sig = 1.0 / np.sqrt(q)
     Lh = sp.csr_matrix((lhat, (g.lrow, g.lci)), shape=(g.n, g.n))
     G = sp.diags(sig) @ (sp.identity(g.n) + Lh)
-    out = dict(G=sp.csr_matrix(G), lhat=lhat, sig=sig, P=P, Q=Q, z=z, acts=acts, h=x)
-    return out
+    return dict(G=sp.csr_matrix(G), lhat=lhat, sig=sig, q=q, w_lower=w_lower, loss=loss, P=P, Q=Q, z=z,
+                acts=acts, h=x)
 
 
-def loss_grad(params, g, Z):
-    """Loss = mean over entries of (G^ A^ G^T Z - Z)^2 and its gradient (FP64)."""
+def loss_grad(params, g):
+    """Kaporin loss (1/n) sum_i log q_i and its gradient with respect to the parameters (FP64)."""
     f = forward(params, g)
-    G, A = f["G"], g.ahat
-    n, m = Z.shape
-    U1 = G.T @ Z
-    V1 = A @ U1
-    W1 = G @ V1
-    E = W1 - Z
-    loss = float(np.sum(E * E) / (n * m))
-    GW = 2.0 * E / (n * m)
-    GV = G.T @ GW
-    GU = A @ GV
-    sig, lhat = f["sig"], f["lhat"]
-    dGdiag = np.sum(GW * V1, axis=1) + np.sum(Z * GU, axis=1)
-    dGoff = np.sum(GW[g.lrow] * V1[g.lci], axis=1) + np.sum(Z[g.lrow] * GU[g.lci], axis=1)
-    dl = sig[g.lrow] * dGoff
-    dsig = dGdiag + np.bincount(g.lrow, weights=lhat * dGoff, minlength=n)
-    drho = 0.5 * sig * dsig
+    n = g.n
+    # d loss / d L^_ij = 2 W_ij / (n q_i)
+    dl = 2.0 * f["w_lower"] / (n * f["q"][g.lrow])
     p = params.astype(np.float64)
     grad = np.zeros_like(p)
 
@@ -138,9 +140,7 @@ def loss_grad(params, g, Z):
     h = f["h"]
     put("U", dP.T @ h)
     put("V", dQ.T @ h)
-    put("q", h.T @ drho)
-    put("q0", [drho.sum()])
-    dH = dP @ view(p, "U", (H, H)) + dQ @ view(p, "V", (H, H)) + np.outer(drho, view(p, "q"))
+    dH = dP @ view(p, "U", (H, H)) + dQ @ view(p, "V", (H, H))
     for l in reversed(range(LAYERS)):
         din = D0 if l == 0 else H
         x, ya, yb, hl = f["acts"][l]
@@ -152,4 +152,4 @@ def loss_grad(params, g, Z):
         if l > 0:
             ws, wa, wb = (view(p, f"{k}{l}", (H, din)) for k in ("ws", "wa", "wb"))
             dH = dpre @ ws + g.absoff @ (dpre @ wa) + g.off @ (dpre @ wb)
-    return loss, grad
+    return f["loss"], grad

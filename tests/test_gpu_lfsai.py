@@ -41,17 +41,16 @@ def test_device_loss_and_gradient_match_oracle(ctx):
     p += 0.2 * rng.standard_normal(p.size)  # exercise every gradient path (we, q != 0)
     model.set_params(p.astype(np.float32))
     p = model.get_params().astype(np.float64)
-    Z = rng.standard_normal((S.n_free, 4)).astype(np.float32)
-    loss, grad = model.loss(S, Z, grad=True)
+    loss, grad = model.loss(S, grad=True)
     g = oracle_graph(S)
-    oloss, ograd = L.loss_grad(p, g, Z.astype(np.float64))
-    assert abs(loss - oloss) <= 1e-4 * oloss
+    oloss, ograd = L.loss_grad(p, g)
+    assert abs(loss - oloss) <= 1e-4 * abs(oloss) + 1e-6
     assert np.linalg.norm(grad - ograd) <= 2e-3 * np.linalg.norm(ograd)
     # the gradient accumulates until an Adam step consumes it
-    _, grad2 = model.loss(S, Z, grad=True)
+    _, grad2 = model.loss(S, grad=True)
     assert np.allclose(grad2, 2 * grad, rtol=1e-4, atol=1e-7 * np.max(np.abs(grad)))
     model.adam(1e-3)
-    _, grad3 = model.loss(S, Z, grad=True)
+    _, grad3 = model.loss(S, grad=True)
     assert np.linalg.norm(grad3) < 1.5 * np.linalg.norm(grad)
 
 
@@ -65,23 +64,22 @@ def test_untrained_learned_solver_converges(ctx):
 
 
 def test_training_gains_over_jacobi_on_unseen_system(ctx):
-    rng = np.random.default_rng(0)
     train = [cantilever_system(ctx, [12, 3, 3], seed=s) for s in (11, 12, 13)]
-    probes = [LF.pcg_residual_probes(S, 8, rng) for S in train]
     model = LF.LearnedFsai(ctx, seed=2)
-    first = np.mean([model.loss(S, Z) for S, Z in zip(train, probes)])
-    for step in range(120):
-        k = step % len(train)
-        model.loss(train[k], probes[k], grad=True)
-        model.adam(3e-3)
-    last = np.mean([model.loss(S, Z) for S, Z in zip(train, probes)])
-    assert last < first
     test = cantilever_system(ctx, [16, 4, 4], seed=99)
     model.attach(test)
+    untrained = test.solve(solver=F.SOLVER_LEARNED_FSAI_PCG, tol=1e-10, fresh_setup=True)
+    first = np.mean([model.loss(S) for S in train])
+    for step in range(150):
+        model.loss(train[step % len(train)], grad=True)
+        model.adam(3e-3)
+    last = np.mean([model.loss(S) for S in train])
+    assert last < first
     jac = test.solve(solver=F.SOLVER_JACOBI_PCG, tol=1e-10)
-    lrn = test.solve(solver=F.SOLVER_LEARNED_FSAI_PCG, tol=1e-10)
+    lrn = test.solve(solver=F.SOLVER_LEARNED_FSAI_PCG, tol=1e-10, fresh_setup=True)
     assert not lrn["fell_back"] and lrn["rel_residual"] <= 1e-10
     assert lrn["iterations"] < 0.75 * jac["iterations"]
+    assert lrn["iterations"] <= untrained["iterations"]
 
 
 def test_invalid_learned_factor_falls_back_to_jacobi(ctx):

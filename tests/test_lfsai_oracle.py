@@ -1,4 +1,6 @@
-"""The learned-FSAI oracle's analytic gradient against central finite differences (CPU)."""
+"""The learned-FSAI oracle (CPU): its analytic gradient against central finite
+differences, its starting factor, and the Kaporin objective against the classic
+FSAI oracle (the objective's minimiser on a fixed pattern)."""
 import numpy as np
 
 from meshes import box
@@ -34,16 +36,15 @@ def random_params(seed):
 def test_oracle_gradient_matches_finite_differences():
     csr, free, lrp, lci = tiny_system()
     g = L.Graph(csr.row_ptrs, csr.col_ind, csr.values, free, 3, lrp, lci)
-    Z = np.random.default_rng(3).standard_normal((g.n, 3))
     p = random_params(7)
-    loss, grad = L.loss_grad(p, g, Z)
+    loss, grad = L.loss_grad(p, g)
     rng = np.random.default_rng(11)
     idx = rng.choice(len(p), size=60, replace=False)
     h = 1e-6
     for i in idx:
         e = np.zeros_like(p)
         e[i] = h
-        fd = (L.loss_grad(p + e, g, Z)[0] - L.loss_grad(p - e, g, Z)[0]) / (2 * h)
+        fd = (L.loss_grad(p + e, g)[0] - L.loss_grad(p - e, g)[0]) / (2 * h)
         assert abs(fd - grad[i]) <= 1e-6 * max(1.0, abs(fd)) + 1e-5 * np.max(np.abs(grad)), (i, fd, grad[i])
 
 
@@ -53,5 +54,30 @@ def test_initial_parameters_give_first_order_factor():
     p = np.zeros(L.OFF["total"])
     p[L.OFF["w0"][0]] = -1.0
     f = L.forward(p, g)
-    assert np.allclose(f["sig"], 1.0)
     assert np.allclose(f["lhat"], -g.al)
+    # diag(G^ A^ G^T) = 1 by construction
+    d = (f["G"] @ g.ahat @ f["G"].T).diagonal()
+    assert np.allclose(d, 1.0, rtol=1e-12)
+
+
+def fsai_offdiag(g):
+    csr = O.Csr(g.n, g.n, g.ahat.indptr.astype(np.int64), g.ahat.indices.astype(np.int64), g.ahat.data)
+    G = O.fsai(csr, (g.lrp, g.lci))
+    diag = G.values[G.row_ptrs[1:] - 1]
+    off = np.concatenate([G.values[G.row_ptrs[i]:G.row_ptrs[i + 1] - 1] for i in range(g.n)])
+    return off / diag[g.lrow], diag
+
+
+def test_classic_fsai_minimises_the_kaporin_objective():
+    csr, free, lrp, lci = tiny_system(2)
+    g = L.Graph(csr.row_ptrs, csr.col_ind, csr.values, free, 3, lrp, lci)
+    off, diag = fsai_offdiag(g)
+    q, w, loss = L.kaporin(g, off)
+    # stationarity: the gradient 2 w / (n q) vanishes at the FSAI values
+    assert np.max(np.abs(w)) <= 1e-10
+    # and the FSAI scaling is the objective's sig = q^-1/2
+    assert np.allclose(1.0 / np.sqrt(q), diag, rtol=1e-10)
+    rng = np.random.default_rng(5)
+    for _ in range(5):
+        assert L.kaporin(g, off + 0.05 * rng.standard_normal(off.size))[2] > loss
+    assert L.forward(random_params(3), g)["loss"] > loss

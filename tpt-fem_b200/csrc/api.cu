@@ -576,21 +576,17 @@ tptfem_status tptfem_lfsai_set_params(tptfem_context* ctx, tptfem_lfsai* model, 
   API_CATCH(ctx)
 }
 
-tptfem_status tptfem_lfsai_loss(tptfem_context* ctx, tptfem_lfsai* model, tptfem_system* sys, const float* probes,
-                                int32_t m, int32_t with_grad, double* loss, float* grad) {
-  if (!ctx || !model || !model->d || !sys || !sys->d || !probes || !loss || m < 1) return TPTFEM_ERR_INVALID_ARG;
+tptfem_status tptfem_lfsai_loss(tptfem_context* ctx, tptfem_lfsai* model, tptfem_system* sys, int32_t with_grad,
+                                double* loss, float* grad) {
+  if (!ctx || !model || !model->d || !sys || !sys->d || !loss) return TPTFEM_ERR_INVALID_ARG;
   API_TRY
   set_device(ctx);
   SystemData& S = *sys->d;
-  TPT_REQUIRE(S.n_free > 0 && S.n_free * (int64_t)m < (1LL << 31), TPTFEM_ERR_INVALID_ARG,
-              "n_free * m out of range for training");
+  TPT_REQUIRE(S.n_free > 0, TPTFEM_ERR_INVALID_ARG, "empty system");
   FsaiFactor* F = nullptr;
   LfGraph& G = system_lf_graph(S, &F);
-  DevBuf<float> z;
-  z.alloc(S.n_free * m, ctx->stream);
-  z.upload(probes, S.n_free * m);
   LfModel& M = *model->d;
-  *loss = lf_loss_grad(S, *F, G, M.prm.p, with_grad ? M.grad.p : nullptr, z.p, m);
+  *loss = lf_loss_grad(S, *F, G, M.prm.p, with_grad ? M.grad.p : nullptr);
   if (with_grad && grad) {
     M.grad.download(grad, M.grad.n);
     TPT_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -7,18 +7,23 @@
 //   h_l+1 = tanh(Ws h_l + Wa (|A^_off| h_l) + Wb (A^_off h_l) + b)   (2 layers, width 16)
 //   edge (i, j) of the pattern, j < i:
 //       z_ij = tanh(U h_i + V h_j + ue a^_ij + ce),  L^_ij = we . z_ij + w0 a^_ij
-//   sigma^_i^2 = exp(q . h_i + q0)
-//   G^ = diag(sigma^) (I + L^)  -> SPD G^T G for any parameters;
+//   g_i = e_i + L^_i,  q_i = g_i A^ g_i^T,  sigma^_i = q_i^-1/2
+//   G^ = diag(sigma^) (I + L^)  -> SPD G^T G for any parameters, diag(G^ A^ G^T) = 1;
 //   G = G^ D^-1/2, i.e. sigma_i^2 = sigma^_i^2 / d_i, L_ij = L^_ij sqrt(d_i / d_j).
-// With we = 0, w0 = -1, q = q0 = 0 the network starts as the first-order
-// approximate inverse factor I - tril(A^).
+// With we = 0, w0 = -1 the network starts as the first-order approximate
+// inverse factor I - tril(A^).
 //
-// Training minimises  loss = 1/(m n) sum_k || G^ A^ G^T z_k - z_k ||^2  over
-// probe vectors z_k (random and PCG residuals), with hand-written forward and
-// backward kernels and Adam.  Everything is FP32 except the final conversion
-// of the factor to FP64/FP16 for the solver.  Weight gradients are summed with
-// block reductions and atomics (training is not bitwise reproducible; inference
-// is).  The matrix is taken as symmetric: the backward of A^ h uses A^ itself.
+// Training minimises Kaporin's condition number of G^ A^ G^T,
+//   K = (tr(G^ A^ G^T) / n) / det(G^ A^ G^T)^(1/n),
+// which with the diagonal scaling above is  log K = (1/n) sum_i log q_i - log det(A^) / n.
+// The constant drops out: loss = (1/n) sum_i log q_i, d loss / d L^_ij = 2 (g_i A^)_j / (n q_i).
+// On a fixed pattern its minimiser is the classic FSAI factor (each row's dense
+// solve in fsai.cu); the network amortises those solves into a forward pass.
+// Forward and backward are hand-written kernels, Adam runs on the device.
+// Everything is FP32 except q (FP64 accumulation) and the final conversion of
+// the factor for the solver.  Weight gradients are summed with block
+// reductions and atomics (training is not bitwise reproducible; inference is).
+// The matrix is taken as symmetric: the backward of A^ h uses A^ itself.
 #include <cmath>
 #include <cstring>
 
@@ -30,10 +35,11 @@ namespace {
 
 constexpr int D0 = LF_D0, H = LF_H;
 constexpr int LF_THREADS = 128;
+constexpr int LF_MAXM = 48;  // longest pattern row incl. the diagonal (the FSAI pattern's bound)
 
 struct Off {  // parameter offsets (floats)
   int ws[LF_LAYERS], wa[LF_LAYERS], wb[LF_LAYERS], b[LF_LAYERS], din[LF_LAYERS];
-  int U, V, ue, ce, we, w0, q, q0, total;
+  int U, V, ue, ce, we, w0, total;
 };
 
 Off offsets() {
@@ -53,18 +59,15 @@ Off offsets() {
   o.ce = p; p += H;
   o.we = p; p += H;
   o.w0 = p; p += 1;
-  o.q = p; p += H;
-  o.q0 = p; p += 1;
   o.total = p;
   return o;
 }
 
 // ---- preparation ----------------------------------------------------------------
 
-// d^-1/2, A^ values, node features.
-__global__ void lf_prep(int n, int dpn, const int* __restrict__ rp, const int* __restrict__ ci,
-                        const double* __restrict__ va, const int* __restrict__ free_map, float* __restrict__ ahat,
-                        double* __restrict__ dis, float* __restrict__ x0) {
+// d^-1/2
+__global__ void lf_prep(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ va,
+                        double* __restrict__ dis) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double di = 1.0;
@@ -73,6 +76,7 @@ __global__ void lf_prep(int n, int dpn, const int* __restrict__ rp, const int* _
   dis[i] = 1.0 / sqrt(di);
 }
 
+// A^ values and node features.
 __global__ void lf_prep2(int n, int dpn, const int* __restrict__ rp, const int* __restrict__ ci,
                          const double* __restrict__ va, const int* __restrict__ free_map,
                          const double* __restrict__ dis, float* __restrict__ ahat, float* __restrict__ x0) {
@@ -110,7 +114,7 @@ __global__ void lf_pattern_values(int n, const int* __restrict__ rp, const int* 
 
 // ---- network forward ----------------------------------------------------------------
 
-// Ya = |A^_off| X, Yb = A^_off X (rows of width DIN).  With ABS_ONLY... both always.
+// Ya = |A^_off| X, Yb = A^_off X (rows of width DIN).
 template <int DIN>
 __global__ void lf_agg(int n, const int* __restrict__ rp, const int* __restrict__ ci, const float* __restrict__ ahat,
                        const float* __restrict__ X, float* __restrict__ Ya, float* __restrict__ Yb) {
@@ -170,20 +174,17 @@ __global__ void lf_layer(int n, const float* __restrict__ prm, int ows, int owa,
   }
 }
 
-// P = U h, Q = V h, sigma^ = exp((q.h + q0) / 2)
+// P = U h, Q = V h
 __global__ void lf_head_nodes(int n, const float* __restrict__ prm, Off o, const float* __restrict__ Hh,
-                              float* __restrict__ P, float* __restrict__ Q, float* __restrict__ sig) {
-  __shared__ float U[H * H], V[H * H], q[H + 1];
+                              float* __restrict__ P, float* __restrict__ Q) {
+  __shared__ float U[H * H], V[H * H];
   for (int t = threadIdx.x; t < H * H; t += blockDim.x) { U[t] = prm[o.U + t]; V[t] = prm[o.V + t]; }
-  for (int t = threadIdx.x; t < H; t += blockDim.x) q[t] = prm[o.q + t];
-  if (threadIdx.x == 0) q[H] = prm[o.q0];
   __syncthreads();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float h[H];
 #pragma unroll
   for (int c = 0; c < H; ++c) h[c] = Hh[(int64_t)i * H + c];
-  float rho = q[H];
 #pragma unroll
   for (int a = 0; a < H; ++a) {
     float p = 0.f, qq = 0.f;
@@ -191,9 +192,7 @@ __global__ void lf_head_nodes(int n, const float* __restrict__ prm, Off o, const
     for (int c = 0; c < H; ++c) { p += U[a * H + c] * h[c]; qq += V[a * H + c] * h[c]; }
     P[(int64_t)i * H + a] = p;
     Q[(int64_t)i * H + a] = qq;
-    rho += q[a] * h[a];
   }
-  sig[i] = expf(0.5f * rho);
 }
 
 // L^_ij for every pattern entry.
@@ -219,58 +218,56 @@ __global__ void lf_head_edges(int n, const float* __restrict__ prm, Off o, const
   }
 }
 
-// ---- factor applies on m probe columns (row-major n x m) --------------------------
-
-// Y = G^ X : y_i = sig_i (x_i + sum_j L^_ij x_j)
-__global__ void lf_g(int n, int m, const int* __restrict__ lrp, const int* __restrict__ lci,
-                     const float* __restrict__ lhat, const float* __restrict__ sig, const float* __restrict__ X,
-                     float* __restrict__ Y) {
-  int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= (int64_t)n * m) return;
-  const int i = (int)(id / m), k = (int)(id % m);
-  float s = X[id];
-  for (int t = lrp[i]; t < lrp[i + 1]; ++t) s += lhat[t] * X[(int64_t)lci[t] * m + k];
-  Y[id] = sig[i] * s;
-}
-
-// Y = G^T X : y_i = sig_i x_i + sum_{j > i} L^_ji sig_j x_j  (transposed pattern)
-__global__ void lf_gt(int n, int m, const int* __restrict__ trp, const int* __restrict__ tci,
-                      const int* __restrict__ perm, const float* __restrict__ lhat, const float* __restrict__ sig,
-                      const float* __restrict__ X, float* __restrict__ Y) {
-  int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= (int64_t)n * m) return;
-  const int i = (int)(id / m), k = (int)(id % m);
-  float s = sig[i] * X[id];
-  for (int t = trp[i]; t < trp[i + 1]; ++t) {
-    const int j = tci[t];
-    s += lhat[perm[t]] * sig[j] * X[(int64_t)j * m + k];
-  }
-  Y[id] = s;
-}
-
-// Y = A^ X
-__global__ void lf_a(int n, int m, const int* __restrict__ rp, const int* __restrict__ ci,
-                     const float* __restrict__ ahat, const float* __restrict__ X, float* __restrict__ Y) {
-  int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= (int64_t)n * m) return;
-  const int i = (int)(id / m), k = (int)(id % m);
-  float s = 0.f;
-  for (int t = rp[i]; t < rp[i + 1]; ++t) s += ahat[t] * X[(int64_t)ci[t] * m + k];
-  Y[id] = s;
-}
-
-// E = W - Z, loss partial sums, GW = 2 E / (m n)
-__global__ void lf_residual(int64_t nm, const float* __restrict__ W, const float* __restrict__ Z,
-                            float* __restrict__ GW, double* __restrict__ loss, float scale) {
+// Kaporin terms, per row i with pattern P = (lower pattern of i, i) (ascending,
+// i last) and g = (L^_i,P, 1):  w = A^[P,P] g,  q_i = g . w  (FP64 accumulation),
+// sig_i = q_i^-1/2,  d loss / d L^_ij = 2 w_j / (n q_i),  loss += log q_i.
+// Rows longer than LF_MAXM set bit 0 of *flag, a non-positive q sets bit 1.
+__global__ void lf_kaporin(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                           const float* __restrict__ ahat, const int* __restrict__ lrp, const int* __restrict__ lci,
+                           const float* __restrict__ lhat, float* __restrict__ sig, float* __restrict__ dlhat,
+                           double* __restrict__ loss, int* __restrict__ flag) {
   __shared__ double sh[LF_THREADS];
-  int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  double e2 = 0.0;
-  if (id < nm) {
-    const float e = W[id] - Z[id];
-    GW[id] = 2.f * e * scale;
-    e2 = (double)e * e;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double lq = 0.0;
+  if (i < n) {
+    const int l0 = lrp[i], m = lrp[i + 1] - l0 + 1;
+    if (m > LF_MAXM) {
+      atomicOr(flag, 1);
+      sig[i] = 1.f;
+    } else {
+      int P[LF_MAXM];
+      double g[LF_MAXM], w[LF_MAXM];
+      for (int a = 0; a < m - 1; ++a) { P[a] = lci[l0 + a]; g[a] = lhat[l0 + a]; }
+      P[m - 1] = i;
+      g[m - 1] = 1.0;
+      double q = 0.0;
+      for (int a = 0; a < m; ++a) {
+        const int r = P[a];
+        int k = rp[r], b = 0;
+        const int ke = rp[r + 1];
+        double s = 0.0;
+        while (k < ke && b < m) {  // merge of two ascending lists
+          const int c = ci[k];
+          if (c == P[b]) { s += (double)ahat[k] * g[b]; ++k; ++b; }
+          else if (c < P[b]) ++k;
+          else ++b;
+        }
+        w[a] = s;
+        q += g[a] * s;
+      }
+      if (!(q > 0.0)) {
+        atomicOr(flag, 2);
+        sig[i] = 1.f;
+      } else {
+        lq = log(q);
+        sig[i] = (float)(1.0 / sqrt(q));
+        if (dlhat)
+          for (int a = 0; a < m - 1; ++a) dlhat[l0 + a] = (float)(2.0 * w[a] / ((double)n * q));
+      }
+    }
   }
-  sh[threadIdx.x] = e2;
+  if (!loss) return;
+  sh[threadIdx.x] = lq;
   __syncthreads();
   for (int s = blockDim.x / 2; s > 0; s >>= 1) {
     if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
@@ -279,28 +276,7 @@ __global__ void lf_residual(int64_t nm, const float* __restrict__ W, const float
   if (threadIdx.x == 0) atomicAdd(loss, sh[0]);
 }
 
-// dG^ on the pattern and the diagonal, then dL^ and d rho (thread per row).
-//   dG^_ij = sum_k GW_ik V1_jk + Z_ik GU_jk
-__global__ void lf_dg(int n, int m, const int* __restrict__ lrp, const int* __restrict__ lci,
-                      const float* __restrict__ lhat, const float* __restrict__ sig, const float* __restrict__ GW,
-                      const float* __restrict__ V1, const float* __restrict__ Z, const float* __restrict__ GU,
-                      float* __restrict__ dlhat, float* __restrict__ drho) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  auto dg = [&](int j) {
-    float s = 0.f;
-    for (int k = 0; k < m; ++k)
-      s += GW[(int64_t)i * m + k] * V1[(int64_t)j * m + k] + Z[(int64_t)i * m + k] * GU[(int64_t)j * m + k];
-    return s;
-  };
-  float dsig = dg(i);
-  for (int t = lrp[i]; t < lrp[i + 1]; ++t) {
-    const float d = dg(lci[t]);
-    dlhat[t] = sig[i] * d;
-    dsig += lhat[t] * d;
-  }
-  drho[i] = 0.5f * sig[i] * dsig;
-}
+// ---- backward -------------------------------------------------------------------------
 
 // Block-reduce NV floats per thread, then one atomicAdd per value and block.
 template <int NV>
@@ -399,23 +375,20 @@ __global__ void lf_colsum(int n, const float* __restrict__ A, float* __restrict_
   block_atomic<D>(v, out);
 }
 
-// Node head backward: dH = U^T dP + V^T dQ + q drho  (weights grads via lf_outer/lf_colsum)
+// Node head backward: dH = U^T dP + V^T dQ  (weight gradients via lf_outer)
 __global__ void lf_head_nodes_bwd(int n, const float* __restrict__ prm, Off o, const float* __restrict__ dP,
-                                  const float* __restrict__ dQ, const float* __restrict__ drho,
-                                  float* __restrict__ dH) {
-  __shared__ float U[H * H], V[H * H], q[H];
+                                  const float* __restrict__ dQ, float* __restrict__ dH) {
+  __shared__ float U[H * H], V[H * H];
   for (int t = threadIdx.x; t < H * H; t += blockDim.x) { U[t] = prm[o.U + t]; V[t] = prm[o.V + t]; }
-  for (int t = threadIdx.x; t < H; t += blockDim.x) q[t] = prm[o.q + t];
   __syncthreads();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float dp[H], dq[H];
 #pragma unroll
   for (int c = 0; c < H; ++c) { dp[c] = dP[(int64_t)i * H + c]; dq[c] = dQ[(int64_t)i * H + c]; }
-  const float dr = drho[i];
 #pragma unroll
   for (int c = 0; c < H; ++c) {
-    float s = q[c] * dr;
+    float s = 0.f;
 #pragma unroll
     for (int a = 0; a < H; ++a) s += U[a * H + c] * dp[a] + V[a * H + c] * dq[a];
     dH[(int64_t)i * H + c] = s;
@@ -530,7 +503,7 @@ void lf_init_params(uint64_t seed, float* h) {
   const float sh = 1.f / std::sqrt((float)H);
   for (int t = 0; t < H * H; ++t) { h[o.U + t] = sh * rnd(); h[o.V + t] = sh * rnd(); }
   for (int t = 0; t < H; ++t) { h[o.ue + t] = sh * rnd(); h[o.ce + t] = 0.1f * rnd(); }
-  h[o.w0] = -1.f;  // we = q = q0 = 0: the first-order factor I - tril(A^)
+  h[o.w0] = -1.f;  // we = 0: the first-order factor I - tril(A^)
 }
 
 void LfGraph::prepare(const SystemData& S, const FsaiFactor& F) {
@@ -552,7 +525,8 @@ void LfGraph::prepare(const SystemData& S, const FsaiFactor& F) {
   Q.alloc((int64_t)n * H, s);
   sig.alloc(n, s);
   lhat.alloc(std::max<int64_t>(nnzl, 1), s);
-  lf_prep<<<blocks(n), LF_THREADS, 0, s>>>(n, S.dpn, S.row_ptr.p, S.col.p, S.val.p, S.free_map.p, ahat.p, dis.p, x0.p);
+  flag.alloc(1, s);
+  lf_prep<<<blocks(n), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, S.val.p, dis.p);
   TPT_CHECK_LAUNCH();
   lf_prep2<<<blocks(n), LF_THREADS, 0, s>>>(n, S.dpn, S.row_ptr.p, S.col.p, S.val.p, S.free_map.p, dis.p, ahat.p,
                                             x0.p);
@@ -562,7 +536,12 @@ void LfGraph::prepare(const SystemData& S, const FsaiFactor& F) {
   ready = true;
 }
 
-void lf_forward(const SystemData& S, const FsaiFactor& F, LfGraph& G, const float* prm) {
+namespace {
+
+// Network forward to L^ and, through the Kaporin kernel, sig (and, when dlhat
+// is given, the loss gradient with respect to L^; the loss sum goes to *loss).
+void forward_impl(const SystemData& S, const FsaiFactor& F, LfGraph& G, const float* prm, float* dlhat,
+                  double* loss) {
   cudaStream_t s = S.ctx->stream;
   const Off o = offsets();
   const int n = G.n;
@@ -582,41 +561,38 @@ void lf_forward(const SystemData& S, const FsaiFactor& F, LfGraph& G, const floa
     TPT_CHECK_LAUNCH();
     in = G.h[l].p;
   }
-  lf_head_nodes<<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o, in, G.P.p, G.Q.p, G.sig.p);
+  lf_head_nodes<<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o, in, G.P.p, G.Q.p);
   TPT_CHECK_LAUNCH();
   lf_head_edges<<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o, F.rp.p, F.ci.p, G.al.p, G.P.p, G.Q.p, G.lhat.p);
   TPT_CHECK_LAUNCH();
+  G.flag.zero();
+  lf_kaporin<<<blocks(n), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, G.ahat.p, F.rp.p, F.ci.p, G.lhat.p, G.sig.p,
+                                              dlhat, loss, G.flag.p);
+  TPT_CHECK_LAUNCH();
 }
 
-double lf_loss_grad(const SystemData& S, const FsaiFactor& F, LfGraph& G, const float* prm, float* grad,
-                    const float* d_probes, int m) {
+}  // namespace
+
+bool lf_forward(const SystemData& S, const FsaiFactor& F, LfGraph& G, const float* prm) {
+  forward_impl(S, F, G, prm, nullptr, nullptr);
+  int f = 0;
+  TPT_CUDA(cudaMemcpyAsync(&f, G.flag.p, sizeof(int), cudaMemcpyDeviceToHost, S.ctx->stream));
+  TPT_CUDA(cudaStreamSynchronize(S.ctx->stream));
+  return f == 0;
+}
+
+double lf_loss_grad(const SystemData& S, const FsaiFactor& F, LfGraph& G, const float* prm, float* grad) {
   cudaStream_t s = S.ctx->stream;
   const Off o = offsets();
   const int n = G.n;
-  const int64_t nm = (int64_t)n * m;
-  lf_forward(S, F, G, prm);
-  DevBuf<float> U1, V1, W1, GW, GV, GU;
-  U1.alloc(nm, s); V1.alloc(nm, s); W1.alloc(nm, s); GW.alloc(nm, s); GV.alloc(nm, s); GU.alloc(nm, s);
   DevBuf<double> loss;
   loss.alloc(1, s);
   loss.zero();
-  lf_gt<<<blocks(nm), LF_THREADS, 0, s>>>(n, m, F.trp.p, F.tci.p, F.perm.p, G.lhat.p, G.sig.p, d_probes, U1.p);
-  TPT_CHECK_LAUNCH();
-  lf_a<<<blocks(nm), LF_THREADS, 0, s>>>(n, m, S.row_ptr.p, S.col.p, G.ahat.p, U1.p, V1.p);
-  TPT_CHECK_LAUNCH();
-  lf_g<<<blocks(nm), LF_THREADS, 0, s>>>(n, m, F.rp.p, F.ci.p, G.lhat.p, G.sig.p, V1.p, W1.p);
-  TPT_CHECK_LAUNCH();
-  const float scale = 1.f / (float)nm;
-  lf_residual<<<blocks(nm), LF_THREADS, 0, s>>>(nm, W1.p, d_probes, GW.p, loss.p, scale);
-  TPT_CHECK_LAUNCH();
+  DevBuf<float> dl;
+  if (grad) dl.alloc(std::max<int64_t>(G.nnzl, 1), s);
+  forward_impl(S, F, G, prm, grad ? dl.p : nullptr, loss.p);
   if (grad) {
-    lf_gt<<<blocks(nm), LF_THREADS, 0, s>>>(n, m, F.trp.p, F.tci.p, F.perm.p, G.lhat.p, G.sig.p, GW.p, GV.p);
-    TPT_CHECK_LAUNCH();
-    lf_a<<<blocks(nm), LF_THREADS, 0, s>>>(n, m, S.row_ptr.p, S.col.p, G.ahat.p, GV.p, GU.p);
-    TPT_CHECK_LAUNCH();
-    DevBuf<float> dl, drho, dP, dQ, dH, dpre, Sx, Ta, Tb, dX;
-    dl.alloc(std::max<int64_t>(G.nnzl, 1), s);
-    drho.alloc(n, s);
+    DevBuf<float> dP, dQ, dH, dpre, Sx, Ta, Tb, dX;
     dP.alloc((int64_t)n * H, s);
     dQ.alloc((int64_t)n * H, s);
     dQ.zero();
@@ -626,9 +602,6 @@ double lf_loss_grad(const SystemData& S, const FsaiFactor& F, LfGraph& G, const 
     Ta.alloc((int64_t)n * H, s);
     Tb.alloc((int64_t)n * H, s);
     dX.alloc((int64_t)n * H, s);
-    lf_dg<<<blocks(n), LF_THREADS, 0, s>>>(n, m, F.rp.p, F.ci.p, G.lhat.p, G.sig.p, GW.p, V1.p, d_probes, GU.p, dl.p,
-                                           drho.p);
-    TPT_CHECK_LAUNCH();
     lf_head_edges_bwd<<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o, grad, F.rp.p, F.ci.p, G.al.p, G.P.p, G.Q.p, dl.p,
                                                        dP.p, dQ.p);
     TPT_CHECK_LAUNCH();
@@ -638,11 +611,7 @@ double lf_loss_grad(const SystemData& S, const FsaiFactor& F, LfGraph& G, const 
     TPT_CHECK_LAUNCH();
     lf_outer<H, H><<<og, 256, 0, s>>>(n, dQ.p, hl, grad + o.V);
     TPT_CHECK_LAUNCH();
-    lf_outer<1, H><<<og, 256, 0, s>>>(n, drho.p, hl, grad + o.q);
-    TPT_CHECK_LAUNCH();
-    lf_colsum<1><<<blocks(n), LF_THREADS, 0, s>>>(n, drho.p, grad + o.q0);
-    TPT_CHECK_LAUNCH();
-    lf_head_nodes_bwd<<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o, dP.p, dQ.p, drho.p, dH.p);
+    lf_head_nodes_bwd<<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o, dP.p, dQ.p, dH.p);
     TPT_CHECK_LAUNCH();
     for (int l = LF_LAYERS - 1; l >= 0; --l) {
       const float* xin = l == 0 ? G.x0.p : G.h[l - 1].p;
@@ -671,9 +640,14 @@ double lf_loss_grad(const SystemData& S, const FsaiFactor& F, LfGraph& G, const 
     }
   }
   double h = 0.0;
+  int f = 0;
   TPT_CUDA(cudaMemcpyAsync(&h, loss.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+  TPT_CUDA(cudaMemcpyAsync(&f, G.flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   TPT_CUDA(cudaStreamSynchronize(s));
-  return h / (double)nm;
+  TPT_REQUIRE(f == 0, TPTFEM_ERR_NUMERIC,
+              (f & 1) ? "learned FSAI: a factor pattern row exceeds the supported length"
+                      : "learned FSAI: q_i <= 0 (the matrix is not positive definite in FP32)");
+  return h / (double)n;
 }
 
 void lf_adam_step(cudaStream_t s, int np, float* prm, const float* grad, float* m1, float* m2, int step, float lr,

@@ -20,6 +20,7 @@ struct LfGraph {
   DevBuf<float> al;     // A^ at the factor pattern entries
   DevBuf<float> ya[LF_LAYERS], yb[LF_LAYERS], h[LF_LAYERS];
   DevBuf<float> P, Q, sig, lhat;
+  DevBuf<int> flag;     // lf_kaporin: bit 0 row too long, bit 1 q <= 0
   void prepare(const SystemData& S, const FsaiFactor& F);
 };
 
@@ -31,10 +32,10 @@ struct LfModel {
 
 int lf_param_count();
 void lf_init_params(uint64_t seed, float* host);
-void lf_forward(const SystemData& S, const FsaiFactor& F, LfGraph& G, const float* prm);
-// Loss (mean over probes and rows); when grad != nullptr adds d loss / d params to grad.
-double lf_loss_grad(const SystemData& S, const FsaiFactor& F, LfGraph& G, const float* prm, float* grad,
-                    const float* d_probes, int m);
+// Forward to L^ and sig; false if a row was too long or q_i <= 0.
+bool lf_forward(const SystemData& S, const FsaiFactor& F, LfGraph& G, const float* prm);
+// Kaporin loss (1/n) sum_i log q_i; when grad != nullptr adds d loss / d params to grad.
+double lf_loss_grad(const SystemData& S, const FsaiFactor& F, LfGraph& G, const float* prm, float* grad);
 void lf_adam_step(cudaStream_t s, int np, float* prm, const float* grad, float* m1, float* m2, int step, float lr,
                   float clip);
 void lf_factor_fp64(const SystemData& S, const FsaiFactor& F, const LfGraph& G, double* sig2, double* lva);

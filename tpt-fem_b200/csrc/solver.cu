@@ -385,7 +385,7 @@ bool learned_factor(SystemData& S, SolverWork& W) {
   fsai_build_pattern(S, W.lf);
   if (W.lf.overflow) return false;
   if (!W.lgraph.ready) W.lgraph.prepare(S, W.lf);
-  lf_forward(S, W.lf, W.lgraph, S.lmodel->prm.p);
+  if (!lf_forward(S, W.lf, W.lgraph, S.lmodel->prm.p)) return false;
   DevBuf<double> sig2, lva;
   sig2.alloc(W.lf.n, s);
   lva.alloc(std::max<int64_t>(W.lf.nnz, 1), s);

@@ -81,7 +81,7 @@ SIGNATURES = {
     "tptfem_lfsai_free": (None, [_vp]),
     "tptfem_lfsai_get_params": (C.c_int, [_vp, _vp, _vp]),
     "tptfem_lfsai_set_params": (C.c_int, [_vp, _vp, _vp]),
-    "tptfem_lfsai_loss": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int32, C.c_int32, _pd, _vp]),
+    "tptfem_lfsai_loss": (C.c_int, [_vp, _vp, _vp, C.c_int32, _pd, _vp]),
     "tptfem_lfsai_adam": (C.c_int, [_vp, _vp, C.c_double, C.c_double]),
     "tptfem_system_attach_lfsai": (C.c_int, [_vp, _vp, _vp]),
     "tptfem_rel_residual_noalloc": (C.c_int, [C.c_int, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _pd, C.c_char_p,

@@ -1,11 +1,10 @@
 """Learned FSAI preconditioner: model handle, weight files and training.
 
-The network and its forward/backward kernels live in libtptfem.so
-(csrc/lfsai.cu); this module drives them: it builds probe vectors (random
-vectors and residuals of Jacobi-PCG runs on the training systems), runs
-loss/gradient/Adam steps on the device and reads/writes a versioned weight file.
+The network, its Kaporin objective and its forward/backward kernels live in
+libtptfem.so (csrc/lfsai.cu); this module drives them: loss/gradient/Adam steps
+on the device and a versioned weight file.
 
-Weight file (little endian): 8-byte magic b"TPTLFSAI", u32 version (1), u32
+Weight file (little endian): 8-byte magic b"TPTLFSAI", u32 version (2), u32
 parameter count, then that many float32 values.
 """
 from __future__ import annotations
@@ -18,7 +17,7 @@ import numpy as np
 from . import _native as N
 
 MAGIC = b"TPTLFSAI"
-VERSION = 1
+VERSION = 2
 
 
 def param_count():
@@ -49,17 +48,12 @@ class LearnedFsai:
             raise ValueError(f"expected {self.n_params} parameters, got {p.size}")
         self.ctx.check(self.lib.tptfem_lfsai_set_params(self.ctx.h, self.h, N.ptr(p)))
 
-    def loss(self, system, probes, grad=False):
-        """Loss (and, with grad=True, the accumulated gradient) on `system` for probes (n_free x m)."""
-        z = np.ascontiguousarray(probes, dtype=np.float32)
-        if z.ndim == 1:
-            z = z[:, None].copy()
-        if z.shape[0] != system.n_free:
-            raise ValueError("probes must have n_free rows")
+    def loss(self, system, grad=False):
+        """Kaporin loss (1/n) sum_i log q_i on `system` (and, with grad=True, the accumulated gradient)."""
         out = C.c_double()
         g = np.zeros(self.n_params, np.float32) if grad else None
-        self.ctx.check(self.lib.tptfem_lfsai_loss(self.ctx.h, self.h, system.h, N.ptr(z), z.shape[1], int(grad),
-                                                  C.byref(out), N.ptr(g) if grad else None))
+        self.ctx.check(self.lib.tptfem_lfsai_loss(self.ctx.h, self.h, system.h, int(grad), C.byref(out),
+                                                  N.ptr(g) if grad else None))
         return (out.value, g) if grad else out.value
 
     def adam(self, lr, clip=1.0):
@@ -94,28 +88,3 @@ def read_weights(path):
     if count != param_count():
         raise ValueError(f"{path}: {count} parameters, the library's network has {param_count()}")
     return p
-
-
-def pcg_residual_probes(system, k, rng, iters=(5, 20, 60, 150)):
-    """Residual directions the plain method generates: b - A x_j after j Jacobi-PCG iterations
-    (normalised), plus Rademacher vectors; n_free x k float32."""
-    from . import SOLVER_JACOBI_PCG, TptFemError
-    rp, ci, va, fred, free = system.download()
-    cols = []
-    for j in iters:
-        if len(cols) >= k // 2:
-            break
-        try:
-            system.solve(solver=SOLVER_JACOBI_PCG, tol=1e-14, max_iter=j)
-        except TptFemError:
-            pass  # NOT_CONVERGED is expected: we want the iterate
-        x = system.solution()[free]
-        rows = np.repeat(np.arange(len(fred)), np.diff(rp))
-        Ax = np.bincount(rows, weights=va * x[ci], minlength=len(fred))
-        r = fred - Ax
-        nr = np.linalg.norm(r)
-        if nr > 0:
-            cols.append(r / nr * np.sqrt(len(r)))
-    while len(cols) < k:
-        cols.append(rng.choice([-1.0, 1.0], size=len(fred)))
-    return np.ascontiguousarray(np.stack(cols, axis=1), dtype=np.float32)

@@ -60,6 +60,38 @@ def box_coords(mn, mx, n):
     return np.stack([mn[0] + t * (mx[0] - mn[0]), mn[1] + u * (mx[1] - mn[1]), mn[2] + w * (mx[2] - mn[2])], axis=1)
 
 
+def tet_centroids(coords, conn):
+    return coords[conn].mean(axis=1)
+
+
+def grf_log_conductivity(points, seed, length=0.1, n_features=1024):
+    """Seeded Gaussian random field (mean 0, variance 1, squared-exponential
+    correlation of length `length`) by random Fourier features:
+    g(x) = sqrt(2/M) sum_m cos(w_m . x + phi_m), w_m ~ N(0, length^-2 I),
+    phi_m ~ U[0, 2 pi) (numpy PCG64 stream of `seed`).  Evaluated on the GPU
+    through torch when one is available (input generation only)."""
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((3, n_features)) / length
+    phi = rng.uniform(0.0, 2.0 * np.pi, n_features)
+    scale = np.sqrt(2.0 / n_features)
+    try:
+        import torch
+        if torch.cuda.is_available():
+            out = np.empty(len(points))
+            wt = torch.as_tensor(w, device="cuda")
+            pt = torch.as_tensor(phi, device="cuda")
+            for a in range(0, len(points), 1 << 20):
+                x = torch.as_tensor(points[a:a + (1 << 20)], device="cuda")
+                out[a:a + len(x)] = (torch.cos(x @ wt + pt).sum(dim=1) * scale).cpu().numpy()
+            return out
+    except ImportError:
+        pass
+    out = np.empty(len(points))
+    for a in range(0, len(points), 1 << 14):
+        out[a:a + (1 << 14)] = np.cos(points[a:a + (1 << 14)] @ w + phi).sum(axis=1) * scale
+    return out
+
+
 CANTILEVERS = {
     "cantilever_200x50x50": ([0.0, 0.0, 0.0], [4.0, 1.0, 1.0], [200, 50, 50]),
     "cantilever_280x70x70": ([0.0, 0.0, 0.0], [4.0, 1.0, 1.0], [280, 70, 70]),
