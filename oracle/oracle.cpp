@@ -1070,3 +1070,359 @@ int orc_max_threads() {
 }
 
 }  // extern "C"
+
+// ---- topology optimisation: crates/tpt-fem-topopt/src/lib.rs -----------------
+//
+// Restatement of topopt_simp (topopt:342-385) and its helpers, plus a second
+// mode with the density filter and the OC loop of the published 88-line SIMP
+// code (Andreassen, Clausen, Schevenels, Lazarov, Sigmund, Struct. Multidisc.
+// Optim. 43 (2011) 1-16), which the reference does not have.  The solve is
+// either the reference's own path (solve_with_dirichlet: reduce, CSR, dense LU)
+// or a banded Cholesky of the same reduced matrix in y-fastest node order
+// (for grids where an n^2 dense matrix is out of reach).
+namespace {
+
+const double TOPO_RHO_MIN = 1e-3, TOPO_RHO_MAX = 1.0, TOPO_OC_DAMP = 0.5;  // topopt:54-62
+
+// element_stiffness_unit (topopt:166-217), E = 1, 2x2 Gauss, square of side h.
+vector<double> topo_ke0(double nu, double h) {
+  const double c = 1.0 / (1.0 - nu * nu);
+  const double d[3][3] = {{c, c * nu, 0.0}, {c * nu, c, 0.0}, {0.0, 0.0, c * (1.0 - nu) / 2.0}};
+  vector<double> p, w;
+  gauss_legendre(2, p, w);
+  const double jdet = h * h / 4.0;
+  const double scale = 2.0 / h;
+  vector<double> ke(64, 0.0);
+  for (size_t a = 0; a < p.size(); ++a)
+    for (size_t b = 0; b < p.size(); ++b) {
+      vector<double> xi = {p[a], p[b]};
+      const double wt = w[a] * w[b];
+      vector<vector<double>> dn = ref_grad(QUAD, xi);
+      double bm[3][8] = {{0}};
+      for (int n = 0; n < 4; ++n) {
+        const double nx_ = scale * dn[n][0], ny_ = scale * dn[n][1];
+        bm[0][2 * n] = nx_;
+        bm[1][2 * n + 1] = ny_;
+        bm[2][2 * n] = ny_;
+        bm[2][2 * n + 1] = nx_;
+      }
+      double db[3][8];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 8; ++j) {
+          double s = 0.0;
+          for (int k = 0; k < 3; ++k) s += d[i][k] * bm[k][j];
+          db[i][j] = s;
+        }
+      for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < 8; ++j) {
+          double s = 0.0;
+          for (int k = 0; k < 3; ++k) s += bm[k][i] * db[k][j];
+          ke[i * 8 + j] += wt * jdet * s;
+        }
+    }
+  return ke;
+}
+
+struct TopoGrid {  // Grid::new(nelx + 1, nely + 1, h) (topopt:89-116)
+  i64 nx, ny, nelx, nely;
+  double h;
+  i64 n_elem() const { return nelx * nely; }
+  void nodes(i64 e, i64 out[4]) const {
+    const i64 ei = e % nelx, ej = e / nelx;
+    out[0] = ej * nx + ei;
+    out[1] = ej * nx + ei + 1;
+    out[2] = (ej + 1) * nx + ei + 1;
+    out[3] = (ej + 1) * nx + ei;
+  }
+  void center(i64 e, double c[2]) const {
+    c[0] = ((double)(e % nelx) + 0.5) * h;
+    c[1] = ((double)(e / nelx) + 0.5) * h;
+  }
+};
+
+// assemble (topopt:220-238): all 64 entries, E(rho) = emin + rho^p (e0 - emin).
+Coo topo_assemble(const TopoGrid& g, const vector<double>& rho, const vector<double>& ke0, double e0, double penal,
+                  double emin) {
+  Coo coo;
+  for (i64 e = 0; e < g.n_elem(); ++e) {
+    const double er = emin + std::pow(rho[e], penal) * (e0 - emin);
+    i64 nd[4];
+    g.nodes(e, nd);
+    i64 gd[8];
+    for (int k = 0; k < 4; ++k) { gd[2 * k] = 2 * nd[k]; gd[2 * k + 1] = 2 * nd[k] + 1; }
+    for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 8; ++j) coo.push(gd[i], gd[j], er * ke0[i * 8 + j]);
+  }
+  return coo;
+}
+
+// element_quad_form (topopt:241-254)
+double topo_quad_form(const vector<double>& ke0, const vector<double>& u, const i64 nd[4]) {
+  double ue[8];
+  for (int k = 0; k < 4; ++k) { ue[2 * k] = u[2 * nd[k]]; ue[2 * k + 1] = u[2 * nd[k] + 1]; }
+  double s = 0.0;
+  for (int i = 0; i < 8; ++i)
+    for (int j = 0; j < 8; ++j) s += ue[i] * ke0[i * 8 + j] * ue[j];
+  return s;
+}
+
+// filter_sensitivity (topopt:259-279).  The reference loops over every element
+// f; only f with d^2 <= R^2 contribute, so the loop here visits the window of
+// element rows/columns within R (+1) in the same ascending f order.
+vector<double> topo_filter_sensitivity(const TopoGrid& g, const vector<double>& raw, double radius) {
+  const double r2 = radius * radius;
+  const i64 w = (i64)std::floor(radius / g.h) + 1;
+  vector<double> out(raw.size(), 0.0);
+  for (i64 e = 0; e < g.n_elem(); ++e) {
+    double ce[2];
+    g.center(e, ce);
+    const i64 ei = e % g.nelx, ej = e / g.nelx;
+    double num = 0.0, den = 0.0;
+    for (i64 fj = std::max<i64>(0, ej - w); fj <= std::min(g.nely - 1, ej + w); ++fj)
+      for (i64 fi = std::max<i64>(0, ei - w); fi <= std::min(g.nelx - 1, ei + w); ++fi) {
+        const i64 f = fj * g.nelx + fi;
+        double cf[2];
+        g.center(f, cf);
+        const double dx = ce[0] - cf[0], dy = ce[1] - cf[1];
+        const double d2 = dx * dx + dy * dy;
+        if (d2 <= r2) {
+          const double wt = radius - std::sqrt(d2);
+          num += wt * raw[f];
+          den += wt;
+        }
+      }
+    out[e] = den > 0.0 ? num / den : raw[e];
+  }
+  return out;
+}
+
+// oc_update (topopt:284-331): 60 bisection steps on [1e-9, 1e9].
+vector<double> topo_oc_update(const vector<double>& rho, const vector<double>& sens, double vol_frac,
+                              double move_limit) {
+  const size_t n = rho.size();
+  const double target = vol_frac * (double)n;
+  vector<double> b(n);
+  for (size_t e = 0; e < n; ++e) b[e] = -sens[e];
+  auto cand = [&](size_t e, double lambda) {
+    const double ratio = b[e] > 0.0 ? std::pow(b[e] / lambda, TOPO_OC_DAMP) : 0.0;
+    const double c = rho[e] * ratio;
+    const double lo = std::max(rho[e] - move_limit, TOPO_RHO_MIN), hi = std::min(rho[e] + move_limit, TOPO_RHO_MAX);
+    return std::min(std::max(c, lo), hi);  // f64::clamp(lo, hi), lo <= hi here
+  };
+  double lo = 1e-9, hi = 1e9, lambda = 1.0;
+  for (int it = 0; it < 60; ++it) {
+    lambda = 0.5 * (lo + hi);
+    double sum = 0.0;
+    for (size_t e = 0; e < n; ++e) sum += cand(e, lambda);
+    if (sum > target) lo = lambda; else hi = lambda;
+  }
+  vector<double> out(n);
+  for (size_t e = 0; e < n; ++e) out[e] = cand(e, lambda);
+  return out;
+}
+
+// Density filter of the 88-line code: y = H x / Hs, H_ef = max(0, rmin - d_ef).
+void topo_density_filter(const TopoGrid& g, double rmin, const vector<double>& x, vector<double>& y,
+                         const vector<double>* scale_in = nullptr) {
+  const i64 w = (i64)std::ceil(rmin / g.h);
+  y.assign(x.size(), 0.0);
+  for (i64 e = 0; e < g.n_elem(); ++e) {
+    const i64 ei = e % g.nelx, ej = e / g.nelx;
+    double ce[2];
+    g.center(e, ce);
+    double num = 0.0, den = 0.0;
+    for (i64 fj = std::max<i64>(0, ej - w); fj <= std::min(g.nely - 1, ej + w); ++fj)
+      for (i64 fi = std::max<i64>(0, ei - w); fi <= std::min(g.nelx - 1, ei + w); ++fi) {
+        const i64 f = fj * g.nelx + fi;
+        double cf[2];
+        g.center(f, cf);
+        const double dx = ce[0] - cf[0], dy = ce[1] - cf[1];
+        const double wt = std::max(0.0, rmin - std::sqrt(dx * dx + dy * dy));
+        num += wt * (scale_in ? x[f] / (*scale_in)[f] : x[f]);
+        den += wt;
+      }
+    y[e] = scale_in ? num : num / den;
+  }
+}
+
+vector<double> topo_filter_weight_sums(const TopoGrid& g, double rmin) {
+  vector<double> ones(g.n_elem(), 1.0), hs;
+  const i64 w = (i64)std::ceil(rmin / g.h);
+  hs.assign(g.n_elem(), 0.0);
+  for (i64 e = 0; e < g.n_elem(); ++e) {
+    const i64 ei = e % g.nelx, ej = e / g.nelx;
+    double ce[2];
+    g.center(e, ce);
+    double den = 0.0;
+    for (i64 fj = std::max<i64>(0, ej - w); fj <= std::min(g.nely - 1, ej + w); ++fj)
+      for (i64 fi = std::max<i64>(0, ei - w); fi <= std::min(g.nelx - 1, ei + w); ++fi) {
+        double cf[2];
+        g.center(fj * g.nelx + fi, cf);
+        const double dx = ce[0] - cf[0], dy = ce[1] - cf[1];
+        den += std::max(0.0, rmin - std::sqrt(dx * dx + dy * dy));
+      }
+    hs[e] = den;
+  }
+  return hs;
+}
+
+// Reduced solve by banded Cholesky: free dofs renumbered y-fastest
+// (node (i, j) -> i * ny + j), band stored row-wise as A[r][r - c], c <= r.
+bool topo_banded_solve(const TopoGrid& g, const Coo& coo, const vector<double>& f,
+                       const vector<std::pair<i64, double>>& bcs, vector<double>& u, std::string& err) {
+  Reduced red = reduce_system(coo, f, bcs);
+  Csr k = to_csr(red.kred);
+  const i64 n = (i64)red.free.size();
+  vector<i64> newid(n), order(n);
+  for (i64 r = 0; r < n; ++r) {
+    const i64 dof = red.free[r], node = dof / 2;
+    order[r] = ((node % g.nx) * g.ny + node / g.nx) * 2 + dof % 2;
+  }
+  vector<i64> idx(n);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::sort(idx.begin(), idx.end(), [&](i64 a, i64 b) { return order[a] < order[b]; });
+  for (i64 p = 0; p < n; ++p) newid[idx[p]] = p;
+  i64 bw = 0;
+  for (i64 r = 0; r < k.nrows; ++r)
+    for (i64 t = k.row_ptrs[r]; t < k.row_ptrs[r + 1]; ++t) bw = std::max<i64>(bw, std::llabs(newid[r] - newid[k.col_ind[t]]));
+  const i64 W = bw + 1;
+  vector<double> B((size_t)n * W, 0.0);
+  for (i64 r = 0; r < k.nrows; ++r)
+    for (i64 t = k.row_ptrs[r]; t < k.row_ptrs[r + 1]; ++t) {
+      const i64 a = newid[r], c = newid[k.col_ind[t]];
+      if (c <= a) B[a * W + (a - c)] = k.values[t];
+    }
+  for (i64 j = 0; j < n; ++j) {  // L L^T, column j
+    double s = B[j * W];
+    for (i64 t = std::max<i64>(0, j - bw); t < j; ++t) s -= B[j * W + (j - t)] * B[j * W + (j - t)];
+    if (!(s > 0.0)) { err = "topopt banded Cholesky: matrix not positive definite"; return false; }
+    const double ljj = std::sqrt(s);
+    B[j * W] = ljj;
+    for (i64 i = j + 1; i <= std::min(n - 1, j + bw); ++i) {
+      double v = B[i * W + (i - j)];
+      for (i64 t = std::max<i64>(0, i - bw); t < j; ++t) v -= B[i * W + (i - t)] * B[j * W + (j - t)];
+      B[i * W + (i - j)] = v / ljj;
+    }
+  }
+  vector<double> y(n);
+  for (i64 r = 0; r < n; ++r) y[newid[r]] = red.fred[r];
+  for (i64 i = 0; i < n; ++i) {
+    double s = y[i];
+    for (i64 t = std::max<i64>(0, i - bw); t < i; ++t) s -= B[i * W + (i - t)] * y[t];
+    y[i] = s / B[i * W];
+  }
+  for (i64 i = n - 1; i >= 0; --i) {
+    double s = y[i];
+    for (i64 t = i + 1; t <= std::min(n - 1, i + bw); ++t) s -= B[t * W + (t - i)] * y[t];
+    y[i] = s / B[i * W];
+  }
+  u.assign(f.size(), 0.0);
+  for (i64 r = 0; r < n; ++r) u[red.free[r]] = y[newid[r]];
+  for (auto& b : bcs) u[b.first] = b.second;
+  return true;
+}
+
+struct TopoArgs {
+  i64 nelx, nely;
+  double h, e0, nu, vol_frac, penal, radius, move_limit, emin;
+  i64 max_iter;
+  int density_filter, banded;
+};
+
+// topopt_simp (topopt:342-385); with density_filter the 88-line code's filter,
+// sensitivity chain rule and OC loop on physical densities.
+bool topo_run(const TopoArgs& a, const vector<double>& f, const vector<std::pair<i64, double>>& bcs,
+              vector<double>& compliance, vector<double>& rho_out, std::string& err) {
+  TopoGrid g{a.nelx + 1, a.nely + 1, a.nelx, a.nely, a.h};
+  const i64 ne = g.n_elem();
+  const vector<double> ke0 = topo_ke0(a.nu, a.h);
+  vector<double> x(ne, a.vol_frac), phys = x, u;
+  auto fe = [&](const vector<double>& rho) {
+    Coo coo = topo_assemble(g, rho, ke0, a.e0, a.penal, a.emin);
+    return a.banded ? topo_banded_solve(g, coo, f, bcs, u, err) : solve_with_dirichlet(coo, f, bcs, u, err);
+  };
+  auto dot = [&]() {
+    double s = -0.0;
+    for (size_t i = 0; i < f.size(); ++i) s += f[i] * u[i];
+    return s;
+  };
+  compliance.clear();
+  if (!fe(phys)) return false;
+  compliance.push_back(dot());
+  vector<double> hs = a.density_filter ? topo_filter_weight_sums(g, a.radius) : vector<double>();
+  for (i64 it = 0; it < a.max_iter; ++it) {
+    if (!fe(phys)) return false;
+    compliance.push_back(dot());
+    vector<double> raw(ne);
+    for (i64 e = 0; e < ne; ++e) {
+      i64 nd[4];
+      g.nodes(e, nd);
+      const double q = topo_quad_form(ke0, u, nd);
+      raw[e] = -a.penal * std::pow(phys[e], a.penal - 1.0) * (a.e0 - a.emin) * q;
+    }
+    if (!a.density_filter) {
+      x = topo_oc_update(x, topo_filter_sensitivity(g, raw, a.radius), a.vol_frac, a.move_limit);
+      phys = x;
+    } else {
+      vector<double> dc, dv, ones(ne, 1.0);
+      topo_density_filter(g, a.radius, raw, dc, &hs);
+      topo_density_filter(g, a.radius, ones, dv, &hs);
+      double l1 = 0.0, l2 = 1e9;
+      vector<double> xn(ne);
+      const double target = a.vol_frac * (double)ne;
+      while ((l2 - l1) / (l1 + l2) > 1e-3) {
+        const double lmid = 0.5 * (l2 + l1);
+        for (i64 e = 0; e < ne; ++e) {
+          const double oc = x[e] * std::sqrt(-dc[e] / dv[e] / lmid);
+          xn[e] = std::max(0.0, std::max(x[e] - a.move_limit, std::min(1.0, std::min(x[e] + a.move_limit, oc))));
+        }
+        topo_density_filter(g, a.radius, xn, phys);
+        double s = 0.0;
+        for (i64 e = 0; e < ne; ++e) s += phys[e];
+        if (s > target) l1 = lmid; else l2 = lmid;
+      }
+      x = xn;
+    }
+  }
+  rho_out = a.density_filter ? phys : x;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_topopt_ke0(double nu, double h, double* out) {
+  vector<double> k = topo_ke0(nu, h);
+  std::copy(k.begin(), k.end(), out);
+}
+
+void orc_topopt_filter_sensitivity(i64 nelx, i64 nely, double h, const double* raw, double radius, double* out) {
+  TopoGrid g{nelx + 1, nely + 1, nelx, nely, h};
+  vector<double> r(raw, raw + nelx * nely);
+  vector<double> o = topo_filter_sensitivity(g, r, radius);
+  std::copy(o.begin(), o.end(), out);
+}
+
+void orc_topopt_oc_update(i64 n, const double* rho, const double* sens, double vol_frac, double move_limit,
+                          double* out) {
+  vector<double> o = topo_oc_update(vector<double>(rho, rho + n), vector<double>(sens, sens + n), vol_frac, move_limit);
+  std::copy(o.begin(), o.end(), out);
+}
+
+// Runs one instance; compliance_out holds max_iter + 1 values, rho_out nelx * nely.
+int orc_topopt(i64 nelx, i64 nely, double h, double e0, double nu, double vol_frac, double penal, double radius,
+               double move_limit, double emin, i64 max_iter, int density_filter, int banded, const double* f,
+               const i64* bc_dof, const double* bc_val, i64 nbc, double* compliance_out, double* rho_out) {
+  TopoArgs a{nelx, nely, h, e0, nu, vol_frac, penal, radius, move_limit, emin, max_iter, density_filter, banded};
+  vector<double> fv(f, f + 2 * (nelx + 1) * (nely + 1));
+  vector<std::pair<i64, double>> bcs;
+  for (i64 i = 0; i < nbc; ++i) bcs.push_back({bc_dof[i], bc_val[i]});
+  vector<double> c, r;
+  if (!topo_run(a, fv, bcs, c, r, g_err)) return 1;
+  std::copy(c.begin(), c.end(), compliance_out);
+  std::copy(r.begin(), r.end(), rho_out);
+  return 0;
+}
+
+}  // extern "C"

@@ -87,6 +87,12 @@ def lib():
         "orc_map": (None, [C.c_int, _f64p, C.c_int, C.c_int, _f64p, _f64p, C.POINTER(C.c_double), _f64p]),
         "orc_cell_quad": (C.c_int, [C.c_int, C.c_int, _f64p, _f64p]),
         "orc_fsai": (_vp, [_i64, _i64p, _i64p, _f64p, _vp, _vp]),
+        "orc_topopt_ke0": (None, [C.c_double, C.c_double, _f64p]),
+        "orc_topopt_filter_sensitivity": (None, [_i64, _i64, C.c_double, _f64p, C.c_double, _f64p]),
+        "orc_topopt_oc_update": (None, [_i64, _f64p, _f64p, C.c_double, C.c_double, _f64p]),
+        "orc_topopt": (C.c_int, [_i64, _i64, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                 C.c_double, C.c_double, C.c_double, _i64, C.c_int, C.c_int, _f64p, _i64p, _f64p,
+                                 _i64, _f64p, _f64p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -424,3 +430,68 @@ def fsai(csr, pattern=None):
 
 def max_threads():
     return lib().orc_max_threads()
+
+
+# ---- topology optimisation (crates/tpt-fem-topopt/src/lib.rs) ----------------
+
+TOPO_E_MIN_FACTOR = 1e-3  # topopt:54
+
+
+def topopt_ke0(nu, h):
+    """element_stiffness_unit (topopt:166-217) -> 8x8."""
+    out = np.zeros(64)
+    lib().orc_topopt_ke0(float(nu), float(h), out)
+    return out.reshape(8, 8)
+
+
+def topopt_filter_sensitivity(nelx, nely, h, raw, radius):
+    """filter_sensitivity (topopt:259-279) on Grid::new(nelx + 1, nely + 1, h)."""
+    raw = np.ascontiguousarray(raw, dtype=np.float64)
+    out = np.zeros(nelx * nely)
+    lib().orc_topopt_filter_sensitivity(nelx, nely, float(h), raw, float(radius), out)
+    return out
+
+
+def topopt_oc_update(rho, sens, vol_frac, move_limit):
+    """oc_update (topopt:284-331)."""
+    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    sens = np.ascontiguousarray(sens, dtype=np.float64)
+    out = np.zeros(len(rho))
+    lib().orc_topopt_oc_update(len(rho), rho, sens, float(vol_frac), float(move_limit), out)
+    return out
+
+
+def cantilever_load(nelx, nely, load=1.0, node=None):
+    """cantilever_load (topopt:398-415): left edge clamped, -y point load at the
+    bottom-right node (or at `node`) of Grid::new(nelx + 1, nely + 1, h)."""
+    nx, ny = nelx + 1, nely + 1
+    f = np.zeros(2 * nx * ny)
+    bcs = []
+    for j in range(ny):
+        n = j * nx
+        bcs += [(2 * n, 0.0), (2 * n + 1, 0.0)]
+    f[2 * (nx - 1 if node is None else node) + 1] = -load
+    return f, bcs
+
+
+def topopt(nelx, nely, vol_frac, radius, max_iter, f, bcs, h=1.0, e0=1.0, nu=0.3, penal=3.0, move_limit=0.2,
+           emin=None, density_filter=False, banded=None):
+    """topopt_simp (topopt:342-385) -> (compliance history (max_iter + 1), final densities).
+
+    density_filter=True: the density filter / OC loop of the published 88-line
+    SIMP code (not in the reference).  banded: solve by banded Cholesky instead
+    of the reference's dense LU (default: banded above 1000 dofs)."""
+    if emin is None:
+        emin = TOPO_E_MIN_FACTOR * e0
+    ndof = 2 * (nelx + 1) * (nely + 1)
+    if banded is None:
+        banded = ndof > 1000
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    assert len(f) == ndof
+    dof, val = _bcs(bcs)
+    comp = np.zeros(max_iter + 1)
+    rho = np.zeros(nelx * nely)
+    if lib().orc_topopt(nelx, nely, h, e0, nu, vol_frac, penal, radius, move_limit, emin, max_iter,
+                        int(density_filter), int(banded), f, dof, val, len(dof), comp, rho):
+        raise OracleError(_err())
+    return comp, rho
