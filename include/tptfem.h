@@ -271,6 +271,61 @@ tptfem_status tptfem_lfsai_adam(tptfem_context* ctx, tptfem_lfsai* model, double
 /* Use `model` for TPTFEM_SOLVER_LEARNED_FSAI_PCG solves of `sys` (NULL detaches). */
 tptfem_status tptfem_system_attach_lfsai(tptfem_context* ctx, tptfem_system* sys, tptfem_lfsai* model);
 
+/* ---- batched 2-D SIMP topology optimisation --------------------------------
+ * Replaces topopt_simp (crates/tpt-fem-topopt/src/lib.rs:342-385) for many
+ * independent instances: each instance is TopOptParams with a grid of
+ * nelx x nely unit-size elements (Grid::new(nelx + 1, nely + 1, h),
+ * topopt:89-116), its load vector and its Dirichlet list.  Per iteration the
+ * displacement solve is FP64 Jacobi-PCG on the matrix-free Q1 operator (the
+ * reference uses a dense LU) to relative residual opts.rel_tol.
+ * density_filter = 0 follows the reference exactly (E_min = emin, set it to
+ * 1e-3 * e0 as topopt:54 does; sensitivity filter topopt:259-279; OC
+ * topopt:284-331); density_filter = 1 uses the density filter and OC loop of
+ * the published 88-line SIMP code (not in the reference). */
+typedef struct tptfem_topopt_instance {
+  int32_t nelx, nely;      /* elements along x and y */
+  int32_t max_iter;        /* OC iterations (history has max_iter + 1 values) */
+  int32_t density_filter;  /* 0: reference sensitivity filter, 1: density filter */
+  double h, e0, nu, vol_frac, penal, filter_radius, move_limit, emin;
+  /* Loads: f (2 (nelx+1)(nely+1) values, node j*(nelx+1)+i, dofs interleaved)
+   * or, when f is NULL, one point load load_value at load_dof. */
+  const double* f;
+  int64_t load_dof;
+  double load_value;
+  /* Dirichlet (dof, value) pairs; NULL bc_dof clamps the whole left edge as
+   * cantilever_load (topopt:398-415) does.  NULL bc_val means all zero. */
+  const int64_t* bc_dof;
+  const double* bc_val;
+  int64_t nbc;
+} tptfem_topopt_instance;
+
+typedef struct tptfem_topopt_opts {
+  double rel_tol;         /* displacement solve tolerance (0: 1e-10) */
+  int32_t max_pcg_iter;   /* per solve (0: 50000) */
+  int32_t block_threads;  /* threads per instance: 256, 512, 1024, or 0 = autotune */
+  int32_t use_graph;      /* capture all iterations in one CUDA graph */
+  int32_t reserved;
+} tptfem_topopt_opts;
+
+typedef struct tptfem_topopt_stats {
+  double total_ms;         /* device time of all iterations (CUDA events) */
+  double tune_ms;          /* autotuner time (0 when the shape was cached) */
+  int64_t pcg_iterations;  /* summed over instances and iterations */
+  int32_t block_threads;   /* threads per instance used */
+  int32_t not_converged;   /* instances with a solve that hit max_pcg_iter or broke down */
+} tptfem_topopt_stats;
+
+/* Runs n instances.  compliance: sum over instances of (max_iter + 1) values,
+ * instance after instance (TopOptResult.compliance); densities: sum of
+ * nelx * nely values (TopOptResult.densities; the physical densities in
+ * density-filter mode).  Returns TPTFEM_ERR_NOT_CONVERGED (outputs still
+ * written) when a solve did not reach rel_tol. */
+tptfem_status tptfem_topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* instances, int32_t n,
+                                  const tptfem_topopt_opts* opts, double* compliance, double* densities,
+                                  tptfem_topopt_stats* stats);
+/* element_stiffness_unit (topopt:166-217): the 8x8 unit-modulus Q1 plane-stress matrix. */
+tptfem_status tptfem_topopt_element_stiffness(double nu, double h, double* ke);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,116 @@
+"""Batched topology optimisation on the GPU against the oracle restatement of
+the reference's topopt_simp (crates/tpt-fem-topopt/src/lib.rs:342-385), its own
+tests (topopt:421-495), and batch independence."""
+import numpy as np
+import pytest
+
+import tpt_fem as F
+from tpt_fem import topopt as T
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12  # displacement solve tolerance used for parity
+
+
+def params(nelx, nely, vf, radius, iters, **kw):
+    return T.TopOptParams(grid=T.Grid(nelx + 1, nely + 1, 1.0), vol_frac=vf, filter_radius=radius, max_iter=iters, **kw)
+
+
+def test_element_stiffness_is_bit_exact():
+    for nu, h in ((0.3, 1.0), (0.25, 0.5)):
+        assert np.array_equal(T.element_stiffness_unit(nu, h), O.topopt_ke0(nu, h))
+
+
+def check_against_oracle(res, P, f, bcs, rtol_c=1e-8, atol_rho=1e-7):
+    emin = T.E_MIN_FACTOR * P.e0 if P.emin is None else P.emin
+    oc, orho = O.topopt(P.grid.nelx, P.grid.nely, P.vol_frac, P.filter_radius, P.max_iter, f, bcs, h=P.grid.h,
+                        e0=P.e0, nu=P.nu, penal=P.penal, move_limit=P.move_limit, emin=emin,
+                        density_filter=P.density_filter)
+    assert np.max(np.abs(res.compliance - oc) / np.abs(oc)) <= rtol_c
+    assert np.max(np.abs(res.densities - orho)) <= atol_rho
+
+
+def test_reference_cantilever_test(ctx):
+    # topopt:421-452 through the GPU path, and against the oracle
+    P = params(19, 9, 0.5, 2.0, 40)
+    f, bcs = T.cantilever_load(P.grid)
+    res = T.topopt_simp(P, f, bcs, ctx=ctx, rel_tol=TOL)
+    assert len(res.densities) == P.grid.n_elem() and len(res.compliance) == 41
+    assert res.compliance[-1] < res.compliance[0]
+    assert abs(res.densities.sum() - 0.5 * P.grid.n_elem()) < 1e-6
+    assert np.all(np.diff(res.compliance) <= 1e-9)
+    check_against_oracle(res, P, f, bcs)
+
+
+def test_reference_full_volume_and_denser_tests(ctx):
+    # topopt:454-476 and topopt:478-495
+    P1 = params(15, 7, 1.0, 2.0, 10)
+    P2 = params(23, 11, 0.4, 2.0, 30)
+    f1, b1 = T.cantilever_load(P1.grid)
+    f2, b2 = T.cantilever_load(P2.grid)
+    (r1, r2), _ = T.topopt_batch(ctx, [(P1, f1, b1), (P2, f2, b2)], rel_tol=TOL)
+    assert abs(r1.densities.sum() - P1.grid.n_elem()) < 1e-6 and np.all(np.abs(r1.densities - 1.0) < 1e-6)
+    assert r2.compliance[-1] < r2.compliance[0]
+    check_against_oracle(r1, P1, f1, b1)
+    check_against_oracle(r2, P2, f2, b2)
+
+
+def test_density_filter_mode_matches_oracle(ctx):
+    # the configuration's settings: Emin 1e-9, density filter R 1.5, mid-right load
+    P = params(60, 20, 0.4, 1.5, 100, emin=1e-9, density_filter=True)
+    f, bcs = T.cantilever_load(P.grid, node=P.grid.nx * (P.grid.nely // 2) + P.grid.nelx)
+    res = T.topopt_simp(P, f, bcs, ctx=ctx, rel_tol=TOL)
+    assert res.compliance[-1] < 0.5 * res.compliance[0]
+    check_against_oracle(res, P, f, bcs, rtol_c=1e-6, atol_rho=1e-5)
+
+
+def test_batch_equals_single_runs_and_uneven_sizes(ctx):
+    rng = np.random.default_rng(3)
+    probs = []
+    for k, (nx, ny) in enumerate([(12, 4), (30, 10), (18, 6), (24, 8), (12, 4)]):
+        P = params(nx, ny, float(rng.uniform(0.3, 0.5)), 1.5, 15 + 5 * k, density_filter=bool(k % 2))
+        f, bcs = T.cantilever_load(P.grid, node=P.grid.nx * (ny // 2) + nx)
+        probs.append((P, f, bcs))
+    batch, st = T.topopt_batch(ctx, probs, rel_tol=TOL, block_threads=256)
+    assert st["block_threads"] == 256 and st["not_converged"] == 0
+    for (P, f, bcs), r in zip(probs, batch):
+        single, _ = T.topopt_batch(ctx, [(P, f, bcs)], rel_tol=TOL, block_threads=256)
+        assert np.array_equal(single[0].compliance, r.compliance)
+        assert np.array_equal(single[0].densities, r.densities)
+        check_against_oracle(r, P, f, bcs, rtol_c=1e-7, atol_rho=1e-6)
+
+
+def test_block_sizes_agree_and_autotuner_reports(ctx):
+    P = params(40, 12, 0.45, 1.5, 20)
+    f, bcs = T.cantilever_load(P.grid)
+    outs = [T.topopt_batch(ctx, [(P, f, bcs)], rel_tol=TOL, block_threads=nt)[0][0] for nt in (256, 512, 1024)]
+    for o in outs[1:]:
+        assert np.max(np.abs(o.compliance - outs[0].compliance) / outs[0].compliance) < 1e-9
+    res, st = T.topopt_batch(ctx, [(P, f, bcs)], rel_tol=TOL)
+    assert st["block_threads"] in (256, 512, 1024)
+    _, st2 = T.topopt_batch(ctx, [(P, f, bcs)], rel_tol=TOL)
+    assert st2["tune_ms"] == 0.0 and st2["block_threads"] == st["block_threads"]
+
+
+def test_nonzero_dirichlet_values_and_duplicates(ctx):
+    # lifting uses the first (dof, value) pair, the solution the last (assembly:525, 555-557)
+    P = params(8, 4, 0.5, 1.5, 5)
+    f, bcs = T.cantilever_load(P.grid)
+    bcs = [(d, 0.01 * (i % 3)) for i, (d, _) in enumerate(bcs)] + [(bcs[1][0], 0.02)]
+    res = T.topopt_simp(P, f, bcs, ctx=ctx, rel_tol=TOL)
+    check_against_oracle(res, P, f, bcs)
+
+
+def test_zero_iterations_and_invalid_input(ctx):
+    P = params(10, 5, 0.5, 1.5, 0)
+    f, bcs = T.cantilever_load(P.grid)
+    res = T.topopt_simp(P, f, bcs, ctx=ctx, rel_tol=TOL)
+    oc, orho = O.topopt(10, 5, 0.5, 1.5, 0, f, bcs)
+    assert len(res.compliance) == 1 and abs(res.compliance[0] - oc[0]) <= 1e-9 * oc[0]
+    assert np.all(res.densities == 0.5)
+    bad = params(10, 5, 1.5, 1.5, 3)
+    with pytest.raises(F.TptFemError):
+        T.topopt_simp(bad, f, bcs, ctx=ctx)
+    with pytest.raises(F.TptFemError):
+        T.topopt_simp(P, f, [(10 ** 6, 0.0)], ctx=ctx)

@@ -614,4 +614,20 @@ tptfem_status tptfem_system_attach_lfsai(tptfem_context* ctx, tptfem_system* sys
   API_CATCH(ctx)
 }
 
+tptfem_status tptfem_topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* instances, int32_t n,
+                                  const tptfem_topopt_opts* opts, double* compliance, double* densities,
+                                  tptfem_topopt_stats* stats) {
+  if (!ctx || !instances || n < 1 || !compliance || !densities) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  topopt_batch(ctx, instances, n, opts, compliance, densities, stats);
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_topopt_element_stiffness(double nu, double h, double* ke) {
+  if (!ke || !(h > 0) || !(nu > -1.0 && nu < 0.5)) return TPTFEM_ERR_INVALID_ARG;
+  topopt_element_stiffness(nu, h, ke);
+  return TPTFEM_OK;
+}
+
 }  // extern "C"

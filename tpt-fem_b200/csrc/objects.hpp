@@ -1,6 +1,7 @@
 // objects.hpp -- the structs behind the opaque C-ABI handles and the internal
 // entry points the C ABI (api.cu) dispatches to.
 #pragma once
+#include <map>
 #include <memory>
 #include <string>
 
@@ -13,6 +14,7 @@ struct tptfem_context {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int* d_flag = nullptr;  // device error/validation flag scratch (one int)
   int* h_pinned = nullptr;  // pinned staging (64 bytes)
+  std::map<uint64_t, int> topo_tuned;  // topopt autotuner: batch shape -> threads per instance
 };
 
 namespace tptfem {
@@ -138,6 +140,11 @@ int64_t system_fsai_classic(SystemData& S);  // builds (once) the classic factor
 void system_fsai_download(const SystemData& S, int64_t* rp, int64_t* ci, double* lva, double* sig2);
 void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32, double* ms_nb, double* nb_bytes);
 void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats& st);
+
+// topopt.cu
+void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, const tptfem_topopt_opts* opts,
+                  double* compliance, double* densities, tptfem_topopt_stats* stats);
+void topopt_element_stiffness(double nu, double h, double* ke);
 
 }  // namespace tptfem
 

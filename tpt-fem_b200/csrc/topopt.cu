@@ -1,0 +1,652 @@
+// topopt.cu -- batched 2-D SIMP topology optimisation (minimum compliance).
+//
+// Restates crates/tpt-fem-topopt/src/lib.rs (topopt_simp, topopt:342-385) for
+// many independent instances at once.  One CTA owns one instance for a whole
+// optimality-criteria iteration; one launch runs every phase of that iteration
+// for every instance:
+//   E_e = emin + rho_e^p (e0 - emin)                     (assemble, topopt:220-238)
+//   K(E) u = f with Dirichlet dofs, matrix-free Q1 apply from the unit element
+//     matrix (element_stiffness_unit, topopt:166-217), Jacobi-PCG in FP64,
+//     warm-started from the previous iteration's displacement
+//   c = f . u                                             (topopt:360,368)
+//   dc_e = -p rho^(p-1) (e0 - emin) u_e^T K0 u_e           (topopt:371-375)
+//   sensitivity filter (topopt:259-279) or the density filter of the 88-line
+//     SIMP code, then the OC bisection (oc_update, topopt:284-331)
+// The launches of all iterations are captured in one CUDA graph.  Instances
+// never wait on each other (no inter-CTA synchronisation); blocks are issued
+// largest instance first.  The block size (threads per instance) is chosen by
+// timing the first iteration with each candidate (the autotuner below) and
+// cached in the context per batch shape.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <numeric>
+
+#include "common.cuh"
+#include "objects.hpp"
+
+namespace tptfem {
+namespace {
+
+constexpr double RHO_MIN = 1e-3, RHO_MAX = 1.0, OC_DAMP = 0.5;  // topopt:54-62
+
+struct TopoInst {
+  int nelx, nely, nx, ny, ne, ndof;
+  int max_iter, density_filter, has_lift;
+  int64_t eoff, doff, hoff;
+  double h, e0, penal, vol_frac, radius, move, emin;
+  double ke0[64];  // element stiffness for E = 1, row-major 8 x 8
+};
+
+struct TopoArgs {
+  const TopoInst* inst;
+  const int* order;  // block -> instance, largest first
+  int iter;
+  int max_pcg;
+  double tol;
+  // element arrays (offset eoff)
+  double *x, *phys, *E, *raw, *sens, *xnew;
+  // dof arrays (offset doff)
+  const double *f, *ulift, *ufix;
+  const uint8_t* fixed;
+  double *u, *r, *p, *q, *dinv, *b;
+  double* hist;      // compliance history (offset hoff)
+  int* last_iters;   // per instance: PCG iterations of the latest solve
+  long long* total_iters;
+  int* flags;        // per instance: bit 0 PCG not converged, bit 1 breakdown
+};
+
+// Block-wide sums (deterministic for a fixed block size).
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double s = threadIdx.x < NT / 32 ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) sh[64] = s;
+  }
+  __syncthreads();
+  return sh[64];
+}
+
+template <int NT>
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) { sh[threadIdx.x >> 5] = a; sh[32 + (threadIdx.x >> 5)] = b; }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double s = threadIdx.x < NT / 32 ? sh[threadIdx.x] : 0.0;
+    double t = threadIdx.x < NT / 32 ? sh[32 + threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+      t += __shfl_xor_sync(0xffffffffu, t, o);
+    }
+    if (threadIdx.x == 0) { sh[64] = s; sh[65] = t; }
+  }
+  __syncthreads();
+  a = sh[64];
+  b = sh[65];
+}
+
+// local index of node (i, j) in the element whose origin is (i + di, j + dj),
+// di, dj in {-1, 0}; element node order 00, 10, 11, 01 (Quad4, topopt:99-109)
+__device__ __forceinline__ int local_node(int di, int dj) {
+  const int ox = -di, oy = -dj;
+  return oy == 0 ? ox : (ox == 1 ? 2 : 3);
+}
+
+// y = K(E) v on the grid's rows; rows of fixed dofs are set to 0 when `mask`.
+// Node (i, j) gathers its <= 4 incident elements (origins (i-1..i, j-1..j)); the
+// 3x3 node neighbourhood of v is loaded once.  Returns this thread's part of v.y.
+template <int NT>
+__device__ double apply_k(const TopoInst& I, const double* __restrict__ E, const double* __restrict__ v,
+                          double* __restrict__ y, const uint8_t* __restrict__ fixed, bool mask,
+                          const double* __restrict__ ke) {
+  const int nx = I.nx, ny = I.ny, nelx = I.nelx, nn = nx * ny;
+  double dot = 0.0;
+  for (int n = threadIdx.x; n < nn; n += NT) {
+    const int i = n % nx, j = n / nx;
+    double vn[3][3][2];
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx) {
+        const bool in = i + dx >= 0 && i + dx < nx && j + dy >= 0 && j + dy < ny;
+        const int m = n + dy * nx + dx;
+        vn[dy + 1][dx + 1][0] = in ? v[2 * m] : 0.0;
+        vn[dy + 1][dx + 1][1] = in ? v[2 * m + 1] : 0.0;
+      }
+    double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+    for (int dj = -1; dj <= 0; ++dj)
+#pragma unroll
+      for (int di = -1; di <= 0; ++di) {
+        const int ei = i + di, ej = j + dj;
+        if (ei < 0 || ei >= nelx || ej < 0 || ej >= I.nely) continue;
+        const double Ee = E[ej * nelx + ei];
+        const int ln = local_node(di, dj);
+        // element nodes in neighbourhood coordinates (row = y + 1, col = x + 1)
+        const int ry[4] = {dj + 1, dj + 1, dj + 2, dj + 2}, rx[4] = {di + 1, di + 2, di + 2, di + 1};
+        const double* k0 = ke + (2 * ln) * 8;
+        const double* k1 = k0 + 8;
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const double a = vn[ry[k]][rx[k]][0], b = vn[ry[k]][rx[k]][1];
+          s0 += k0[2 * k] * a + k0[2 * k + 1] * b;
+          s1 += k1[2 * k] * a + k1[2 * k + 1] * b;
+        }
+        y0 += Ee * s0;
+        y1 += Ee * s1;
+      }
+    if (mask) {
+      if (fixed[2 * n]) y0 = 0.0;
+      if (fixed[2 * n + 1]) y1 = 0.0;
+    }
+    y[2 * n] = y0;
+    y[2 * n + 1] = y1;
+    dot += vn[1][1][0] * y0 + vn[1][1][1] * y1;
+  }
+  return dot;
+}
+
+// Sum over the filter window of element e: w = R - d for d <= R (sensitivity
+// filter, topopt:259-279) or w = max(0, rmin - d) (density filter).  The term
+// is val[f] (1 when val is null), divided by div[f] when div is given.
+template <bool SENS>
+__device__ __forceinline__ void filter_window(const TopoInst& I, int e, const double* __restrict__ val,
+                                              const double* __restrict__ div, double& num, double& den) {
+  const int ei = e % I.nelx, ej = e / I.nelx;
+  const double R = I.radius, r2 = R * R, h = I.h;
+  const int w = SENS ? (int)floor(R / h) + 1 : (int)ceil(R / h);
+  const double cx = ((double)ei + 0.5) * h, cy = ((double)ej + 0.5) * h;
+  num = 0.0;
+  den = 0.0;
+  for (int fj = max(0, ej - w); fj <= min(I.nely - 1, ej + w); ++fj)
+    for (int fi = max(0, ei - w); fi <= min(I.nelx - 1, ei + w); ++fi) {
+      const double dx = cx - ((double)fi + 0.5) * h, dy = cy - ((double)fj + 0.5) * h;
+      const double d2 = dx * dx + dy * dy;
+      const int f = fj * I.nelx + fi;
+      double wt;
+      if (SENS) {
+        if (!(d2 <= r2)) continue;
+        wt = R - sqrt(d2);
+      } else {
+        wt = fmax(0.0, R - sqrt(d2));
+      }
+      double term = val ? val[f] : 1.0;
+      if (div) term /= div[f];
+      num += wt * term;
+      den += wt;
+    }
+}
+
+__device__ __forceinline__ double oc_candidate(double rho, double b, double lambda, double move) {
+  const double ratio = b > 0.0 ? pow(b / lambda, OC_DAMP) : 0.0;
+  const double c = rho * ratio;
+  const double lo = fmax(rho - move, RHO_MIN), hi = fmin(rho + move, RHO_MAX);
+  return fmin(fmax(c, lo), hi);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) topo_iteration(TopoArgs a) {
+  __shared__ double ke[64];
+  __shared__ double red[72];
+  __shared__ TopoInst I;
+  const int idx = a.order[blockIdx.x];
+  if (threadIdx.x == 0) I = a.inst[idx];
+  __syncthreads();
+  if (a.iter >= max(I.max_iter, 1)) return;
+  for (int t = threadIdx.x; t < 64; t += NT) ke[t] = I.ke0[t];
+  const int ne = I.ne, nd = I.ndof;
+  double* x = a.x + I.eoff;
+  double* phys = a.phys + I.eoff;
+  double* E = a.E + I.eoff;
+  double* raw = a.raw + I.eoff;
+  double* sens = a.sens + I.eoff;
+  double* xnew = a.xnew + I.eoff;
+  const double* f = a.f + I.doff;
+  const double* ufix = a.ufix + I.doff;
+  const uint8_t* fixed = a.fixed + I.doff;
+  double* u = a.u + I.doff;
+  double* r = a.r + I.doff;
+  double* p = a.p + I.doff;
+  double* q = a.q + I.doff;
+  double* dinv = a.dinv + I.doff;
+  double* b = a.b + I.doff;
+  const double emin = I.emin, de = I.e0 - I.emin;
+
+  if (a.iter == 0) {  // uniform start (topopt:353), zero initial guess
+    for (int e = threadIdx.x; e < ne; e += NT) { x[e] = I.vol_frac; phys[e] = I.vol_frac; }
+    for (int d = threadIdx.x; d < nd; d += NT) u[d] = 0.0;
+    if (threadIdx.x == 0) { a.total_iters[idx] = 0; a.flags[idx] = 0; }
+  }
+  __syncthreads();
+  // moduli (assemble, topopt:224)
+  for (int e = threadIdx.x; e < ne; e += NT) E[e] = emin + pow(phys[e], I.penal) * de;
+  __syncthreads();
+  // Jacobi diagonal of K_FF
+  for (int n = threadIdx.x; n < I.nx * I.ny; n += NT) {
+    const int i = n % I.nx, j = n / I.nx;
+    double d0 = 0.0, d1 = 0.0;
+    for (int dj = -1; dj <= 0; ++dj)
+      for (int di = -1; di <= 0; ++di) {
+        const int ei = i + di, ej = j + dj;
+        if (ei < 0 || ei >= I.nelx || ej < 0 || ej >= I.nely) continue;
+        const int ln = local_node(di, dj);
+        const double Ee = E[ej * I.nelx + ei];
+        d0 += Ee * ke[(2 * ln) * 8 + 2 * ln];
+        d1 += Ee * ke[(2 * ln + 1) * 8 + 2 * ln + 1];
+      }
+    dinv[2 * n] = fixed[2 * n] ? 0.0 : 1.0 / d0;
+    dinv[2 * n + 1] = fixed[2 * n + 1] ? 0.0 : 1.0 / d1;
+  }
+  // right-hand side: b = f_F - K_FD u_D (reduce_system lifting, first bcs value)
+  if (I.has_lift) {
+    apply_k<NT>(I, E, a.ulift + I.doff, q, fixed, false, ke);
+    __syncthreads();
+    for (int d = threadIdx.x; d < nd; d += NT) b[d] = fixed[d] ? 0.0 : f[d] - q[d];
+  } else {
+    for (int d = threadIdx.x; d < nd; d += NT) b[d] = fixed[d] ? 0.0 : f[d];
+  }
+  __syncthreads();
+  // r = b - K x0 (warm start), p = D^-1 r
+  apply_k<NT>(I, E, u, q, fixed, true, ke);
+  __syncthreads();
+  double rz = 0.0, rr = 0.0, bb = 0.0;
+  for (int d = threadIdx.x; d < nd; d += NT) {
+    const double rd = b[d] - q[d];
+    r[d] = rd;
+    const double z = dinv[d] * rd;
+    p[d] = z;
+    rz += rd * z;
+    rr += rd * rd;
+    bb += b[d] * b[d];
+  }
+  block_sum2<NT>(rz, rr, red);
+  bb = block_sum<NT>(bb, red);
+  const double stop = a.tol * a.tol * bb;
+  int it = 0;
+  bool conv = rr <= stop;
+  while (!conv && it < a.max_pcg) {
+    double pq = apply_k<NT>(I, E, p, q, fixed, true, ke);
+    pq = block_sum<NT>(pq, red);
+    if (!(pq > 0.0)) {
+      if (threadIdx.x == 0) atomicOr(a.flags + idx, 2);
+      break;
+    }
+    const double alpha = rz / pq;
+    double rzn = 0.0, rrn = 0.0;
+    for (int d = threadIdx.x; d < nd; d += NT) {
+      u[d] += alpha * p[d];
+      const double rd = r[d] - alpha * q[d];
+      r[d] = rd;
+      rzn += rd * dinv[d] * rd;
+      rrn += rd * rd;
+    }
+    block_sum2<NT>(rzn, rrn, red);
+    ++it;
+    conv = rrn <= stop;
+    if (conv) break;
+    const double beta = rzn / rz;
+    rz = rzn;
+    for (int d = threadIdx.x; d < nd; d += NT) p[d] = dinv[d] * r[d] + beta * p[d];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    a.last_iters[idx] = it;
+    a.total_iters[idx] += it;
+    if (!conv) atomicOr(a.flags + idx, 1);
+  }
+  // compliance c = f . u, u with the fixed dofs' (last) values (topopt:360,368)
+  double c = 0.0;
+  for (int d = threadIdx.x; d < nd; d += NT) c += f[d] * (fixed[d] ? ufix[d] : u[d]);
+  c = block_sum<NT>(c, red);
+  if (threadIdx.x == 0) {
+    if (a.iter == 0) a.hist[I.hoff] = c;
+    if (I.max_iter > 0) a.hist[I.hoff + a.iter + 1] = c;
+  }
+  if (I.max_iter == 0) return;  // the initial solve only (topopt:356-360)
+  // raw sensitivity (topopt:371-375), element_quad_form (topopt:241-254)
+  for (int e = threadIdx.x; e < ne; e += NT) {
+    const int ei = e % I.nelx, ej = e / I.nelx;
+    const int n0 = ej * I.nx + ei;
+    const int nodes[4] = {n0, n0 + 1, n0 + I.nx + 1, n0 + I.nx};
+    double ue[8];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int c2 = 0; c2 < 2; ++c2) {
+        const int d = 2 * nodes[k] + c2;
+        ue[2 * k + c2] = fixed[d] ? ufix[d] : u[d];
+      }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) s += ue[i] * ke[i * 8 + j] * ue[j];
+    raw[e] = -I.penal * pow(phys[e], I.penal - 1.0) * de * s;
+  }
+  __syncthreads();
+  if (!I.density_filter) {
+    // filter_sensitivity (topopt:259-279), then oc_update (topopt:284-331)
+    for (int e = threadIdx.x; e < ne; e += NT) {
+      double num, den;
+      filter_window<true>(I, e, raw, nullptr, num, den);
+      sens[e] = den > 0.0 ? num / den : raw[e];
+    }
+    __syncthreads();
+    const double target = I.vol_frac * (double)ne;
+    double lo = 1e-9, hi = 1e9, lambda = 1.0;
+    for (int k = 0; k < 60; ++k) {
+      lambda = 0.5 * (lo + hi);
+      double s = 0.0;
+      for (int e = threadIdx.x; e < ne; e += NT) s += oc_candidate(x[e], -sens[e], lambda, I.move);
+      s = block_sum<NT>(s, red);
+      if (s > target) lo = lambda; else hi = lambda;
+    }
+    for (int e = threadIdx.x; e < ne; e += NT) {
+      const double v = oc_candidate(x[e], -sens[e], lambda, I.move);
+      x[e] = v;
+      phys[e] = v;
+    }
+  } else {
+    // density filter (88-line code): dc = H (dc / Hs), dv = H (1 / Hs); OC on
+    // the design with the volume of the filtered (physical) densities.
+    // E (free until the next launch) holds Hs, sens = dc, raw = dv.
+    for (int e = threadIdx.x; e < ne; e += NT) {
+      double num, den;
+      filter_window<false>(I, e, nullptr, nullptr, num, den);
+      E[e] = den;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < ne; e += NT) {
+      double num, den;
+      filter_window<false>(I, e, raw, E, num, den);
+      sens[e] = num;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < ne; e += NT) {
+      double num, den;
+      filter_window<false>(I, e, nullptr, E, num, den);
+      raw[e] = num;
+    }
+    __syncthreads();
+    const double target = I.vol_frac * (double)ne;
+    double l1 = 0.0, l2 = 1e9;
+    for (int guard = 0; guard < 200 && (l2 - l1) / (l1 + l2) > 1e-3; ++guard) {
+      const double lmid = 0.5 * (l2 + l1);
+      for (int e = threadIdx.x; e < ne; e += NT) {
+        const double oc = x[e] * sqrt(fmax(0.0, -sens[e] / raw[e] / lmid));
+        xnew[e] = fmax(0.0, fmax(x[e] - I.move, fmin(1.0, fmin(x[e] + I.move, oc))));
+      }
+      __syncthreads();
+      double s = 0.0;
+      for (int e = threadIdx.x; e < ne; e += NT) {
+        double num, den;
+        filter_window<false>(I, e, xnew, nullptr, num, den);
+        const double v = num / E[e];
+        phys[e] = v;
+        s += v;
+      }
+      s = block_sum<NT>(s, red);
+      if (s > target) l1 = lmid; else l2 = lmid;
+    }
+    for (int e = threadIdx.x; e < ne; e += NT) x[e] = xnew[e];
+  }
+}
+
+void launch_nt(int nt, int nblocks, const TopoArgs& a, cudaStream_t s) {
+  switch (nt) {
+    case 256: topo_iteration<256><<<nblocks, 256, 0, s>>>(a); break;
+    case 512: topo_iteration<512><<<nblocks, 512, 0, s>>>(a); break;
+    default: topo_iteration<1024><<<nblocks, 1024, 0, s>>>(a); break;
+  }
+  TPT_CHECK_LAUNCH();
+}
+
+// element_stiffness_unit (topopt:166-217) in the reference's operation order
+// (host code, compiled without floating-point contraction).
+void element_stiffness_unit(double nu, double h, double* ke) {
+  const double c = 1.0 / (1.0 - nu * nu);
+  const double d[3][3] = {{c, c * nu, 0.0}, {c * nu, c, 0.0}, {0.0, 0.0, c * (1.0 - nu) / 2.0}};
+  const double gp[2] = {-1.0 / std::sqrt(3.0), 1.0 / std::sqrt(3.0)}, gw[2] = {1.0, 1.0};  // gauss_legendre(2)
+  const double jdet = h * h / 4.0, scale = 2.0 / h;
+  const double s4[4] = {-1.0, 1.0, 1.0, -1.0}, t4[4] = {-1.0, -1.0, 1.0, 1.0};  // Quad4 corners
+  for (int t = 0; t < 64; ++t) ke[t] = 0.0;
+  for (int qa = 0; qa < 2; ++qa)
+    for (int qb = 0; qb < 2; ++qb) {
+      const double xi = gp[qa], eta = gp[qb], w = gw[qa] * gw[qb];
+      double bm[3][8] = {{0}};
+      for (int n = 0; n < 4; ++n) {  // Quad4::grad (element:141-153), scaled to x, y
+        const double gx = 0.25 * s4[n] * (1.0 + t4[n] * eta), gy = 0.25 * (1.0 + s4[n] * xi) * t4[n];
+        const double nx_ = scale * gx, ny_ = scale * gy;
+        bm[0][2 * n] = nx_;
+        bm[1][2 * n + 1] = ny_;
+        bm[2][2 * n] = ny_;
+        bm[2][2 * n + 1] = nx_;
+      }
+      double db[3][8];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 8; ++j) {
+          double s = 0.0;
+          for (int k = 0; k < 3; ++k) s += d[i][k] * bm[k][j];
+          db[i][j] = s;
+        }
+      for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < 8; ++j) {
+          double s = 0.0;
+          for (int k = 0; k < 3; ++k) s += bm[k][i] * db[k][j];
+          ke[i * 8 + j] += w * jdet * s;
+        }
+    }
+}
+
+}  // namespace
+
+void topopt_element_stiffness(double nu, double h, double* ke) { element_stiffness_unit(nu, h, ke); }
+
+// Host driver: validate, pack, tune, capture, run.
+void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, const tptfem_topopt_opts* opts,
+                  double* compliance, double* densities, tptfem_topopt_stats* stats) {
+  cudaStream_t s = ctx->stream;
+  TPT_REQUIRE(n >= 1 && in && compliance && densities, TPTFEM_ERR_INVALID_ARG, "topopt: no instances or outputs");
+  const double tol = opts && opts->rel_tol > 0 ? opts->rel_tol : 1e-10;
+  const int max_pcg = opts && opts->max_pcg_iter > 0 ? opts->max_pcg_iter : 50000;
+  std::vector<TopoInst> inst(n);
+  int64_t eoff = 0, doff = 0, hoff = 0;
+  int launches = 0;
+  for (int k = 0; k < n; ++k) {
+    const tptfem_topopt_instance& P = in[k];
+    TPT_REQUIRE(P.nelx >= 1 && P.nely >= 1 && (int64_t)(P.nelx + 1) * (P.nely + 1) * 2 < (1LL << 30),
+                TPTFEM_ERR_INVALID_ARG, "topopt: grid size out of range");
+    TPT_REQUIRE(P.max_iter >= 0 && P.max_iter <= 100000, TPTFEM_ERR_INVALID_ARG, "topopt: max_iter out of range");
+    TPT_REQUIRE(P.h > 0 && P.e0 > 0 && P.nu > -1 && P.nu < 0.5 && P.vol_frac > 0 && P.vol_frac <= 1 &&
+                    P.penal >= 1 && P.filter_radius > 0 && P.move_limit > 0 && P.emin >= 0 && P.emin < P.e0,
+                TPTFEM_ERR_INVALID_ARG, "topopt: parameter out of range");
+    TopoInst& I = inst[k];
+    std::memset(&I, 0, sizeof(I));
+    I.nelx = P.nelx; I.nely = P.nely; I.nx = P.nelx + 1; I.ny = P.nely + 1;
+    I.ne = P.nelx * P.nely; I.ndof = 2 * I.nx * I.ny;
+    I.max_iter = P.max_iter; I.density_filter = P.density_filter != 0;
+    I.eoff = eoff; I.doff = doff; I.hoff = hoff;
+    I.h = P.h; I.e0 = P.e0; I.penal = P.penal; I.vol_frac = P.vol_frac; I.radius = P.filter_radius;
+    I.move = P.move_limit; I.emin = P.emin;
+    element_stiffness_unit(P.nu, P.h, I.ke0);
+    eoff += I.ne;
+    doff += I.ndof;
+    hoff += P.max_iter + 1;
+    launches = std::max(launches, std::max(P.max_iter, 1));  // max_iter 0 still solves once
+  }
+  // loads and Dirichlet data (first bcs value lifts, last overwrites: assembly:525,555-557)
+  std::vector<double> f(doff, 0.0), ulift(doff, 0.0), ufix(doff, 0.0);
+  std::vector<uint8_t> fixed(doff, 0);
+  for (int k = 0; k < n; ++k) {
+    const tptfem_topopt_instance& P = in[k];
+    TopoInst& I = inst[k];
+    double* fk = f.data() + I.doff;
+    if (P.f) {
+      for (int d = 0; d < I.ndof; ++d) {
+        TPT_REQUIRE(std::isfinite(P.f[d]), TPTFEM_ERR_INVALID_ARG, "topopt: non-finite load");
+        fk[d] = P.f[d];
+      }
+    } else {
+      TPT_REQUIRE(P.load_dof >= 0 && P.load_dof < I.ndof && std::isfinite(P.load_value), TPTFEM_ERR_INVALID_ARG,
+                  "topopt: point load out of range");
+      fk[P.load_dof] = P.load_value;
+    }
+    uint8_t* fx = fixed.data() + I.doff;
+    std::vector<uint8_t> seen(I.ndof, 0);
+    if (P.bc_dof) {
+      TPT_REQUIRE(P.nbc >= 0, TPTFEM_ERR_INVALID_ARG, "topopt: negative Dirichlet count");
+      for (int64_t t = 0; t < P.nbc; ++t) {
+        const int64_t d = P.bc_dof[t];
+        TPT_REQUIRE(d >= 0 && d < I.ndof, TPTFEM_ERR_INVALID_ARG, "topopt: Dirichlet dof out of range");
+        const double v = P.bc_val ? P.bc_val[t] : 0.0;
+        TPT_REQUIRE(std::isfinite(v), TPTFEM_ERR_INVALID_ARG, "topopt: non-finite Dirichlet value");
+        if (!seen[d]) { ulift[I.doff + d] = v; seen[d] = 1; }
+        ufix[I.doff + d] = v;
+        fx[d] = 1;
+      }
+    } else {  // cantilever_load (topopt:398-415): the whole left edge
+      for (int j = 0; j < I.ny; ++j) { fx[2 * j * I.nx] = 1; fx[2 * j * I.nx + 1] = 1; }
+    }
+    for (int d = 0; d < I.ndof; ++d) if (ulift[I.doff + d] != 0.0) I.has_lift = 1;
+  }
+  // largest instances first
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return (int64_t)inst[a].ndof * std::max(inst[a].max_iter, 1) > (int64_t)inst[b].ndof * std::max(inst[b].max_iter, 1);
+  });
+
+  DevBuf<TopoInst> d_inst;
+  DevBuf<int> d_order, d_last, d_flags;
+  DevBuf<long long> d_total;
+  DevBuf<double> ex, ephys, eE, eraw, esens, exnew, df, dlift, dfix, du, dr, dp, dq, ddinv, db, dhist;
+  DevBuf<uint8_t> dfixed;
+  d_inst.alloc(n, s); d_order.alloc(n, s); d_last.alloc(n, s); d_flags.alloc(n, s); d_total.alloc(n, s);
+  for (auto* v : {&ex, &ephys, &eE, &eraw, &esens, &exnew}) v->alloc(std::max<int64_t>(eoff, 1), s);
+  for (auto* v : {&df, &dlift, &dfix, &du, &dr, &dp, &dq, &ddinv, &db}) v->alloc(std::max<int64_t>(doff, 1), s);
+  dfixed.alloc(std::max<int64_t>(doff, 1), s);
+  dhist.alloc(std::max<int64_t>(hoff, 1), s);
+  d_inst.upload(inst.data(), n);
+  d_order.upload(order.data(), n);
+  df.upload(f.data(), doff);
+  dlift.upload(ulift.data(), doff);
+  dfix.upload(ufix.data(), doff);
+  dfixed.upload(fixed.data(), doff);
+  d_last.zero(); d_flags.zero(); d_total.zero(); dhist.zero();
+
+  TopoArgs a{};
+  a.inst = d_inst.p; a.order = d_order.p; a.iter = 0; a.max_pcg = max_pcg; a.tol = tol;
+  a.x = ex.p; a.phys = ephys.p; a.E = eE.p; a.raw = eraw.p; a.sens = esens.p; a.xnew = exnew.p;
+  a.f = df.p; a.ulift = dlift.p; a.ufix = dfix.p; a.fixed = dfixed.p;
+  a.u = du.p; a.r = dr.p; a.p = dp.p; a.q = dq.p; a.dinv = ddinv.p; a.b = db.p;
+  a.hist = dhist.p; a.last_iters = d_last.p; a.total_iters = d_total.p; a.flags = d_flags.p;
+
+  cudaEvent_t ev0 = ctx->ev[0], ev1 = ctx->ev[1], ev2 = ctx->ev[2];
+  float tune_ms = 0.f;
+  // autotuner: threads per instance, chosen by timing the first iteration
+  int nt = opts && (opts->block_threads == 256 || opts->block_threads == 512 || opts->block_threads == 1024)
+               ? opts->block_threads : 0;
+  uint64_t sig = 1469598103934665603ull;
+  for (int k = 0; k < n; ++k)
+    for (uint64_t v : {(uint64_t)inst[k].nelx, (uint64_t)inst[k].nely, (uint64_t)inst[k].density_filter})
+      sig = (sig ^ v) * 1099511628211ull;
+  if (!nt) {
+    auto it = ctx->topo_tuned.find(sig);
+    if (it != ctx->topo_tuned.end()) nt = it->second;
+  }
+  if (!nt) {
+    float best = 1e30f;
+    TPT_CUDA(cudaEventRecord(ev0, s));
+    for (int cand : {256, 512, 1024}) {
+      float ms = 0.f;
+      TPT_CUDA(cudaEventRecord(ev1, s));
+      a.iter = 0;
+      launch_nt(cand, n, a, s);
+      TPT_CUDA(cudaEventRecord(ev2, s));
+      TPT_CUDA(cudaEventSynchronize(ev2));
+      TPT_CUDA(cudaEventElapsedTime(&ms, ev1, ev2));
+      if (ms < best) { best = ms; nt = cand; }
+    }
+    TPT_CUDA(cudaEventRecord(ev1, s));
+    TPT_CUDA(cudaEventSynchronize(ev1));
+    TPT_CUDA(cudaEventElapsedTime(&tune_ms, ev0, ev1));
+    ctx->topo_tuned[sig] = nt;
+  }
+  // all iterations as one graph (iteration 0 re-initialises the state)
+  float run_ms = 0.f;
+  const bool graph = !opts || opts->use_graph;
+  cudaGraphExec_t exec = nullptr;
+  if (graph) {
+    cudaGraph_t g = nullptr;
+    TPT_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < launches; ++k) {
+      a.iter = k;
+      switch (nt) {
+        case 256: topo_iteration<256><<<n, 256, 0, s>>>(a); break;
+        case 512: topo_iteration<512><<<n, 512, 0, s>>>(a); break;
+        default: topo_iteration<1024><<<n, 1024, 0, s>>>(a); break;
+      }
+    }
+    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    TPT_CUDA(ce);
+    ce = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    TPT_CUDA(ce);
+  }
+  TPT_CUDA(cudaEventRecord(ev0, s));
+  if (graph) {
+    TPT_CUDA(cudaGraphLaunch(exec, s));
+  } else {
+    for (int k = 0; k < launches; ++k) {
+      a.iter = k;
+      launch_nt(nt, n, a, s);
+    }
+  }
+  TPT_CUDA(cudaEventRecord(ev1, s));
+  const cudaError_t se = cudaEventSynchronize(ev1);
+  if (exec) cudaGraphExecDestroy(exec);
+  TPT_CUDA(se);
+  TPT_CUDA(cudaGetLastError());
+  TPT_CUDA(cudaEventElapsedTime(&run_ms, ev0, ev1));
+  // results: reference-mode instances report the design, density-filter ones
+  // the physical (filtered) densities
+  std::vector<double> hist(std::max<int64_t>(hoff, 1)), xs(std::max<int64_t>(eoff, 1)), ps(std::max<int64_t>(eoff, 1));
+  std::vector<long long> total(n);
+  std::vector<int> flags(n);
+  dhist.download(hist.data(), hoff);
+  ex.download(xs.data(), eoff);
+  ephys.download(ps.data(), eoff);
+  d_total.download(total.data(), n);
+  d_flags.download(flags.data(), n);
+  TPT_CUDA(cudaStreamSynchronize(s));
+  std::copy(hist.begin(), hist.begin() + hoff, compliance);
+  for (const TopoInst& I : inst) {
+    const std::vector<double>& src = I.density_filter ? ps : xs;
+    std::copy(src.begin() + I.eoff, src.begin() + I.eoff + I.ne, densities + I.eoff);
+  }
+  long long tot = 0;
+  int bad = 0;
+  for (int k = 0; k < n; ++k) { tot += total[k]; bad += flags[k] != 0; }
+  if (stats) {
+    stats->total_ms = run_ms;
+    stats->tune_ms = tune_ms;
+    stats->pcg_iterations = tot;
+    stats->block_threads = nt;
+    stats->not_converged = bad;
+  }
+  TPT_REQUIRE(bad == 0, TPTFEM_ERR_NOT_CONVERGED, "topopt: a displacement solve did not converge");
+}
+
+}  // namespace tptfem

@@ -40,6 +40,27 @@ class SolveStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class TopoptInstance(C.Structure):
+    _fields_ = [("nelx", C.c_int32), ("nely", C.c_int32), ("max_iter", C.c_int32), ("density_filter", C.c_int32),
+                ("h", C.c_double), ("e0", C.c_double), ("nu", C.c_double), ("vol_frac", C.c_double),
+                ("penal", C.c_double), ("filter_radius", C.c_double), ("move_limit", C.c_double),
+                ("emin", C.c_double), ("f", C.c_void_p), ("load_dof", C.c_int64), ("load_value", C.c_double),
+                ("bc_dof", C.c_void_p), ("bc_val", C.c_void_p), ("nbc", C.c_int64)]
+
+
+class TopoptOpts(C.Structure):
+    _fields_ = [("rel_tol", C.c_double), ("max_pcg_iter", C.c_int32), ("block_threads", C.c_int32),
+                ("use_graph", C.c_int32), ("reserved", C.c_int32)]
+
+
+class TopoptStats(C.Structure):
+    _fields_ = [("total_ms", C.c_double), ("tune_ms", C.c_double), ("pcg_iterations", C.c_int64),
+                ("block_threads", C.c_int32), ("not_converged", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _vp = C.c_void_p
 _pp = C.POINTER(C.c_void_p)
 _i64 = C.c_int64
@@ -48,6 +69,9 @@ _pd = C.POINTER(C.c_double)
 _pint = C.POINTER(C.c_int)
 
 SIGNATURES = {
+    "tptfem_topopt_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]),
+    "tptfem_topopt_element_stiffness": (C.c_int, [C.c_double, C.c_double, C.c_void_p]),
     "tptfem_version": (C.c_char_p, []),
     "tptfem_create": (C.c_int, [C.c_int, _pp]),
     "tptfem_destroy": (None, [_vp]),
