@@ -4,11 +4,14 @@ nodes, 8,232,000 tets, 4,234,440 free dofs; per-tet E = 1e-3 + (1-1e-3) rho^3
 from a seeded smoothed density; nu = 0.3; x = 0 clamped; traction (0,0,-1e-3)
 on x = 4).  Inputs are synthetic (seeded), no dataset exists for this path.
 
-A step is one complete solve from x = 0 of the device-resident reduced system,
-preconditioner set-up included, stopping on the TRUE FP64 residual.  `value`
+A step is one complete solve from x = 0 of the device-resident reduced system
+with the learned-FSAI preconditioner (network forward on this system, factor
+conversion, FP64 PCG), set-up included, stopping on the TRUE FP64 residual.  `value`
 is the median device time of a step (CUDA events on the library's stream);
 `e2e` runs the same solve through the C ABI from host arrays (mesh upload,
-assembly, traction, Dirichlet reduction, solve, solution download).
+assembly, traction, Dirichlet reduction, learned factor, solve, solution
+download).  The plain method (FP64 Jacobi-PCG, CSR operator) is timed on the
+same GPU in the same run.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -185,15 +188,24 @@ def build_system(F, W, ctx, with_host=False):
     return mesh, K, S, E, rhs, dof, val
 
 
-def e2e_once(F, W, ctx, solver, host):
-    """Host arrays -> C ABI -> host solution; returns (seconds, h2d bytes, d2h bytes, stats)."""
+WEIGHTS = os.path.join(ROOT, "tpt-fem_b200", "weights", "lfsai_elasticity.bin")
+
+
+def e2e_once(F, LF, W, ctx, solver, host, model):
+    """Host arrays -> C ABI -> host solution; returns (seconds, h2d bytes, d2h bytes, stats).
+    Mesh upload, assembly, traction, Dirichlet reduction, the learned factor and
+    the solve all run inside the timed region."""
     coords, conn, E, dof, val = host
     cuda_sync()
     t0 = time.perf_counter()
     mesh = F.Mesh.from_arrays(F.CELL_TET4, coords, conn, ctx=ctx)
     K = F.assemble_elasticity(mesh, "3d", E, 0.3, 2)
     rhs = F.apply_traction(mesh, 3, 0, 1.0, [0.0, 0.0, -1e-3], np.zeros(K.nrows))
-    u, st = F.solve_with_dirichlet(K, rhs, list(zip(dof, val)), solver=solver, tol=TOL)
+    S = F.reduce_system(K, rhs, list(zip(dof, val)))
+    if solver == F.SOLVER_LEARNED_FSAI_PCG:
+        model.attach(S)
+    st = S.solve(solver=solver, tol=TOL, fresh_setup=True)
+    u = S.solution()
     ctx.synchronize()
     dt = time.perf_counter() - t0
     h2d = coords.nbytes + conn.nbytes + E.nbytes + 2 * rhs.nbytes + dof.nbytes + val.nbytes
@@ -201,20 +213,33 @@ def e2e_once(F, W, ctx, solver, host):
     return dt, h2d, d2h, st
 
 
+def seconds(st):
+    return (st["setup_ms"] + st["solve_ms"]) / 1e3
+
+
 def run_ours(args, world, rank, local):
     import tpt_fem as F
+    from tpt_fem import lfsai as LF
     from tpt_fem import workloads as W
     ctx = F.Context(local)
     mesh, K, S, E, rhs, dof, val = build_system(F, W, ctx)
-    solver = {"fsai": F.SOLVER_FSAI_MP_PCG, "jacobi": F.SOLVER_JACOBI_PCG, "mp": F.SOLVER_MP_PCG}[args.solver]
+    model = LF.LearnedFsai.load(ctx, WEIGHTS)
+    model.attach(S)
+    solver = {"learned": F.SOLVER_LEARNED_FSAI_PCG, "fsai": F.SOLVER_FSAI_MP_PCG, "jacobi": F.SOLVER_JACOBI_PCG,
+              "mp": F.SOLVER_MP_PCG}[args.solver]
     if args.profile:  # kernels of the timed steps only (for an ncu launch list)
         for _ in range(args.steps):
             S.solve(solver=solver, tol=TOL, fresh_setup=True)
         ctx.synchronize()
         return None
-    # FP64 Jacobi-PCG on the same GPU: the method the metric compares against
-    jac = S.solve(solver=F.SOLVER_JACOBI_PCG, tol=TOL, fresh_setup=True)
-    jac = S.solve(solver=F.SOLVER_JACOBI_PCG, tol=TOL, fresh_setup=True)
+    # The plain method the metric compares against: FP64 Jacobi-PCG with the
+    # CSR operator (warp-per-row SpMV); also the same method on the node-block
+    # operator, and classic FSAI, for the record.
+    S.solve(solver=F.SOLVER_JACOBI_PCG, tol=TOL, fresh_setup=True, csr_only=True)
+    jac = S.solve(solver=F.SOLVER_JACOBI_PCG, tol=TOL, fresh_setup=True, csr_only=True)
+    jac_nb = S.solve(solver=F.SOLVER_JACOBI_PCG, tol=TOL, fresh_setup=True)
+    S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=TOL, fresh_setup=True)
+    fsai = S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=TOL, fresh_setup=True)
     for _ in range(args.warmup):
         S.solve(solver=solver, tol=TOL, fresh_setup=True)
     barrier(world)
@@ -223,57 +248,69 @@ def run_ours(args, world, rank, local):
     with ClockSampler(local) as clk:
         t_wall = time.perf_counter()
         for _ in range(args.steps):
-            st = S.solve(solver=solver, tol=TOL, fresh_setup=True)
-            steps.append(st)
+            steps.append(S.solve(solver=solver, tol=TOL, fresh_setup=True))
         cuda_sync()
         t_wall = time.perf_counter() - t_wall
     barrier(world)
-    dev_s = [(st["setup_ms"] + st["solve_ms"]) / 1e3 for st in steps]
-    step_s = barrier_max(statistics.median(dev_s), world)
-    # roofline of the dominant kernel: the FP64 CSR SpMV of the Krylov operator
-    ms64, ms32, msnb, nb_bytes = S.profile_spmv(20)
+    step_s = barrier_max(statistics.median([seconds(st) for st in steps]), world)
+    # roofline of the dominant kernel: the Krylov operator y = K x
+    prof = S.profile_spmv(20)
     n, nnz = S.n_free, S.nnz
-    # algorithmic bytes of y = K x (CSR formula: values + int32 columns + row pointers + x + y)
-    spmv_bytes = nnz * (8 + 4) + 4 * (n + 1) + 8 * n + 8 * n
+    csr_bytes = nnz * (8 + 4) + 4 * (n + 1) + 8 * n + 8 * n  # CSR formula: values, int32 cols, row ptrs, x, y
     peak, peak_kind = measured_peaks()
-    op_ms = msnb if msnb > 0 else ms64
-    op_name = "nb_spmv<3> (node-block sliced ELL, FP64)" if msnb > 0 else "spmv_kernel<double> (CSR, FP64)"
-    achieved = spmv_bytes / (op_ms * 1e-3) / 1e9
+    if prof["nbs_ms"] > 0:
+        op_ms, op_bytes = prof["nbs_ms"], prof["nbs_bytes"]
+        op_name = "nb_spmv_sym<3> (node-block sliced ELL, symmetric half storage, FP64)"
+    elif prof["nb_ms"] > 0:
+        op_ms, op_bytes = prof["nb_ms"], prof["nb_bytes"]
+        op_name = "nb_spmv<3> (node-block sliced ELL, FP64)"
+    else:
+        op_ms, op_bytes = prof["csr_f64_ms"], csr_bytes
+        op_name = "spmv_kernel<double> (CSR, FP64)"
+    achieved = op_bytes / (op_ms * 1e-3) / 1e9
     out = None
     if rank == 0:
         coords = mesh.coords_array.copy()
         conn = mesh.conn_array.copy()
-        e2e = [e2e_once(F, W, ctx, solver, (coords, conn, E, dof, val)) for _ in range(2)]
+        e2e = [e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model) for _ in range(2)]
         e2e_s, h2d, d2h, e2e_st = min(e2e, key=lambda t: t[0])
         cpu = CpuSample()
         cpu_it_s, cpu_nnz, cpu_threads = cpu.seconds_per_iteration(), cpu.nnz, cpu.threads
         cpu_val = cpu_it_s * (nnz / cpu_nnz) * jac["iterations"]
         its = [st["iterations"] for st in steps]
-        kernels_per_it = 5 if solver == F.SOLVER_FSAI_MP_PCG else 3
-        launches = sum(st["iterations"] * kernels_per_it + st["outer_steps"] * 6 + 8 for st in steps)
+        fsai_like = solver in (F.SOLVER_FSAI_MP_PCG, F.SOLVER_LEARNED_FSAI_PCG)
+        kernels_per_it = 5 if fsai_like else 3
+        setup_kernels = 40 if solver == F.SOLVER_LEARNED_FSAI_PCG else 12
+        launches = sum(st["iterations"] * kernels_per_it + st["outer_steps"] * 6 + setup_kernels for st in steps)
         out = {
             "metric": METRIC, "value": step_s, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (FSAI factor f16/f32)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (factor f16/f32, network f32)",
             "data": "synthetic (seeded density field)",
             "config": {"workload": WORKLOAD, "mesh": [280, 70, 70], "nodes": int(mesh.n_nodes),
                        "tets": int(mesh.n_elems), "free_dofs": int(n), "nnz_reduced": int(nnz),
-                       "solver": args.solver, "tol": TOL, "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (matrix 1.85 GB)"},
+                       "solver": args.solver, "weights": os.path.relpath(WEIGHTS, ROOT), "tol": TOL,
+                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (matrix 1.85 GB)"},
             "solver_stats": {"iterations_median": statistics.median(its), "rel_residual": steps[-1]["rel_residual"],
                              "setup_ms": steps[-1]["setup_ms"], "solve_ms": steps[-1]["solve_ms"],
-                             "reliable_updates": steps[-1]["outer_steps"]},
-            "fp64_jacobi_pcg": {"seconds": (jac["setup_ms"] + jac["solve_ms"]) / 1e3,
-                                "iterations": jac["iterations"], "rel_residual": jac["rel_residual"]},
-            "speedup_vs_fp64_jacobi": ((jac["setup_ms"] + jac["solve_ms"]) / 1e3) / step_s,
+                             "reliable_updates": steps[-1]["outer_steps"], "fell_back": steps[-1]["fell_back"]},
+            "fp64_jacobi_pcg": {"seconds": seconds(jac), "iterations": jac["iterations"],
+                                "rel_residual": jac["rel_residual"], "operator": "CSR"},
+            "fp64_jacobi_pcg_node_block": {"seconds": seconds(jac_nb), "iterations": jac_nb["iterations"],
+                                           "rel_residual": jac_nb["rel_residual"]},
+            "classic_fsai_pcg": {"seconds": seconds(fsai), "iterations": fsai["iterations"],
+                                 "rel_residual": fsai["rel_residual"]},
+            "speedup_vs_fp64_jacobi": seconds(jac) / step_s,
+            "speedup_vs_fp64_jacobi_node_block": seconds(jac_nb) / step_s,
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "iterations": e2e_st["iterations"]},
             "roofline": {"bound": "hbm", "kernel": op_name, "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": None, "algorithmic_bytes": spmv_bytes, "ms": op_ms,
-                         "layout_bytes": nb_bytes if msnb > 0 else spmv_bytes,
-                         "layout_gbs": (nb_bytes if msnb > 0 else spmv_bytes) / (op_ms * 1e-3) / 1e9,
-                         "csr_f64_ms": ms64, "csr_f64_gbs": spmv_bytes / (ms64 * 1e-3) / 1e9},
+                         "traffic": None, "algorithmic_bytes": op_bytes, "ms": op_ms,
+                         "csr_formula_bytes": csr_bytes,
+                         "csr_formula_gbs": csr_bytes / (op_ms * 1e-3) / 1e9,
+                         "nb_full_ms": prof["nb_ms"], "csr_f64_ms": prof["csr_f64_ms"],
+                         "csr_f64_gbs": csr_bytes / (prof["csr_f64_ms"] * 1e-3) / 1e9},
             "cpu_baseline": {"value": cpu_val, "unit": "s", "cores": cpu_threads, "kind": "port",
                              "sample": f"oracle FP64 Jacobi-PCG, 40 iterations on the [140,35,35] cantilever "
                                        f"({cpu_nnz} nnz), scaled by nnz ratio {nnz / cpu_nnz:.2f} and by the "
@@ -314,7 +351,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--solver", default="fsai", choices=["fsai", "jacobi", "mp"])
+    ap.add_argument("--solver", default="learned", choices=["learned", "fsai", "jacobi", "mp"])
     ap.add_argument("--profile", action="store_true", help="run only the timed solves (ncu launch list)")
     args = ap.parse_args()
     world, rank, local = dist_setup()

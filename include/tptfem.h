@@ -98,8 +98,14 @@ typedef struct tptfem_solver_opts {
  * kept on the system from its first solve); its sparsity pattern is kept. */
 #define TPTFEM_SOLVE_FRESH_SETUP 1
 /* Keep the scalar CSR operator and factor even where the node-block layout
- * applies (for A/B measurements; must be given on a system's first solve). */
+ * applies (for A/B measurements).  For Jacobi-PCG it selects a separate
+ * CSR-only engine; for the FSAI solvers it must be given on the first solve. */
 #define TPTFEM_SOLVE_CSR_ONLY 2
+/* Node-block operator: use the full block storage of K instead of the default
+ * symmetric half storage (lower blocks + diagonal, the upper half applied as
+ * the transposes of the lower blocks; K is symmetric up to the FP64 rounding
+ * of its element matrices, and the FP64 true residual always uses K itself). */
+#define TPTFEM_SOLVE_FULL_OPERATOR 4
 
 typedef struct tptfem_solve_stats {
   int64_t iterations;    /* total PCG iterations (inner iterations for MP) */
@@ -200,12 +206,14 @@ tptfem_status tptfem_system_fsai(tptfem_context* ctx, tptfem_system* sys, int64_
 tptfem_status tptfem_system_fsai_download(tptfem_context* ctx, const tptfem_system* sys, int64_t* l_row_ptrs,
                                           int64_t* l_col_ind, double* l_values, double* sigma2);
 /* Diagnostic (no reference counterpart): average device time in ms of the
- * solver's SpMV kernels on this system -- FP64 CSR, FP32 CSR and FP64 node-block
- * sliced-ELL (-1 when the system has partial node groups; *nb_bytes = the bytes
- * that layout moves per launch) -- `reps` launches each, timed with CUDA events
- * on the context's stream.  Used for roofline reports. */
+ * solver's SpMV kernels on this system -- FP64 CSR, FP32 CSR, FP64 node-block
+ * sliced-ELL with full storage and with symmetric half storage (-1 when the
+ * system has partial node groups; *nb_bytes / *nbs_bytes = the bytes those
+ * layouts must move per launch) -- `reps` launches each, timed with CUDA
+ * events on the context's stream.  Used for roofline reports. */
 tptfem_status tptfem_system_profile_spmv(tptfem_context* ctx, tptfem_system* sys, int reps, double* ms_f64,
-                                         double* ms_f32, double* ms_nb_f64, double* nb_bytes);
+                                         double* ms_f32, double* ms_nb_f64, double* nb_bytes, double* ms_nbs_f64,
+                                         double* nbs_bytes);
 
 /* Allocation-free check of a solution (no counterpart in the reference):
  * relative residual ||b - A x||_2 / ||b||_2 of an n x n CSR system whose arrays

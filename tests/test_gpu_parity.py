@@ -285,13 +285,20 @@ def test_node_block_layout_matches_scalar_csr(ctx, solver):
     bcs = [(3 * n + k, 0.0) for n in x0 for k in range(3)]
     S1 = F.reduce_system(K, rhs, bcs)
     S2 = F.reduce_system(K, rhs, bcs)
-    st1 = S1.solve(solver=solver, tol=1e-12)
+    st1 = S1.solve(solver=solver, tol=1e-12)  # node-block, symmetric half storage
     st2 = S2.solve(solver=solver, tol=1e-12, csr_only=True)
     u1, u2 = S1.solution(), S2.solution()
     assert st1["rel_residual"] <= 1e-12 and st2["rel_residual"] <= 1e-12
     assert abs(st1["iterations"] - st2["iterations"]) <= max(3, st2["iterations"] // 20)
     assert np.max(np.abs(u1 - u2)) <= 1e-9 * np.max(np.abs(u2))
-    assert S1.profile_spmv(2)[2] > 0  # the node-block layout was built
+    st3 = S1.solve(solver=solver, tol=1e-12, full_operator=True)  # node-block, full storage
+    u3 = S1.solution()
+    assert st3["rel_residual"] <= 1e-12
+    assert abs(st3["iterations"] - st2["iterations"]) <= max(3, st2["iterations"] // 20)
+    assert np.max(np.abs(u3 - u2)) <= 1e-9 * np.max(np.abs(u2))
+    prof = S1.profile_spmv(2)
+    assert prof["nb_ms"] > 0 and prof["nbs_ms"] > 0  # both node-block layouts were built
+    assert prof["nbs_bytes"] < 0.75 * prof["nb_bytes"]
 
 
 def test_quad_linear_patch_reproduced(ctx):

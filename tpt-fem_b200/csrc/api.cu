@@ -472,13 +472,17 @@ tptfem_status tptfem_system_fsai_download(tptfem_context* ctx, const tptfem_syst
 }
 
 tptfem_status tptfem_system_profile_spmv(tptfem_context* ctx, tptfem_system* sys, int reps, double* ms_f64,
-                                         double* ms_f32, double* ms_nb_f64, double* nb_bytes) {
-  if (!ctx || !sys || !sys->d || !ms_f64 || !ms_f32 || !ms_nb_f64 || !nb_bytes || reps < 1)
+                                         double* ms_f32, double* ms_nb_f64, double* nb_bytes, double* ms_nbs_f64,
+                                         double* nbs_bytes) {
+  if (!ctx || !sys || !sys->d || !ms_f64 || !ms_f32 || !ms_nb_f64 || !nb_bytes || !ms_nbs_f64 || !nbs_bytes ||
+      reps < 1)
     return TPTFEM_ERR_INVALID_ARG;
   API_TRY
   set_device(ctx);
   *nb_bytes = 0.0;
-  system_profile_spmv(*sys->d, reps, ms_f64, ms_f32, ms_nb_f64, nb_bytes);
+  *nbs_bytes = 0.0;
+  *ms_nbs_f64 = -1.0;
+  system_profile_spmv(*sys->d, reps, ms_f64, ms_f32, ms_nb_f64, nb_bytes, ms_nbs_f64, nbs_bytes);
   API_CATCH(ctx)
 }
 

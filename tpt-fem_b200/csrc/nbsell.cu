@@ -208,7 +208,56 @@ __global__ void fill_factor(int ngroups, int dpn, const int* __restrict__ lrp, c
     for (int b = 0; b < a; ++b, ++q) ldiag[((int64_t)c * 3 + q) * 32 + lane] = lva[lrp[g * dpn + a] + dpn * nl + b];
 }
 
+// Symmetric half storage of K: the strictly-lower blocks in the L slot
+// structure, the diagonal blocks per chunk, and for each L^T slot (g, J > g)
+// the index of block (J, g) in the lower storage (its transpose is K_gJ).
+__global__ void fill_ksym(int ngroups, int dpn, const int* __restrict__ rp, const int* __restrict__ ci,
+                          const double* __restrict__ va, const int* __restrict__ lcptr, const int* __restrict__ lcol,
+                          const int* __restrict__ nlow, const int* __restrict__ ucptr, const int* __restrict__ upos,
+                          const int* __restrict__ ucol, double* __restrict__ lval, double* __restrict__ dval,
+                          int* __restrict__ ubase) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  const int c = g >> 5, lane = g & 31;
+  const int d2 = dpn * dpn;
+  const int nl = nlow[g];
+  for (int k = 0; k < lcptr[c + 1] - lcptr[c]; ++k) {
+    const int64_t s = (int64_t)lcptr[c] + k;
+    const int J = lcol[s * 32 + lane];
+    for (int a = 0; a < dpn; ++a)
+      for (int b = 0; b < dpn; ++b)
+        lval[(s * d2 + a * dpn + b) * 32 + lane] = k < nl ? csr_at(rp, ci, va, g * dpn + a, J * dpn + b) : 0.0;
+  }
+  for (int a = 0; a < dpn; ++a)
+    for (int b = 0; b < dpn; ++b)
+      dval[((int64_t)c * d2 + a * dpn + b) * 32 + lane] = csr_at(rp, ci, va, g * dpn + a, g * dpn + b);
+  for (int k = 0; k < ucptr[c + 1] - ucptr[c]; ++k) {
+    const int64_t idx = ((int64_t)ucptr[c] + k) * 32 + lane;
+    const int J = ucol[idx], p = upos[idx];
+    ubase[idx] = p < 0 ? -1 : (int)(((int64_t)lcptr[J >> 5] + p) * d2 * 32 + (J & 31));
+  }
+}
+
 }  // namespace
+
+void nb_build_sym(SystemData& S) {
+  NbSell& N = S.nb;
+  if (N.sym_built) return;
+  TPT_REQUIRE(N.state == 1, TPTFEM_ERR_INVALID_ARG, "symmetric operator needs the node-block layout");
+  cudaStream_t s = S.ctx->stream;
+  const int d2 = N.dpn * N.dpn;
+  TPT_REQUIRE(std::max<int64_t>(N.l_slots, 1) * 32 * d2 < (1LL << 31), TPTFEM_ERR_INVALID_ARG,
+              "symmetric operator: lower storage exceeds int32 indexing");
+  N.ks_lval.alloc(std::max<int64_t>(N.l_slots, 1) * 32 * d2, s);
+  N.ks_diag.alloc((int64_t)N.nchunks * 32 * d2, s);
+  N.ku_base.alloc(std::max<int64_t>(N.u_slots, 1) * 32, s);
+  N.ks_diag.zero();
+  fill_ksym<<<ceil_div(N.ngroups, 128), 128, 0, s>>>(N.ngroups, N.dpn, S.row_ptr.p, S.col.p, S.val.p, N.l_cptr.p,
+                                                     N.l_col.p, N.nlow.p, N.u_cptr.p, N.u_pos.p, N.u_col.p,
+                                                     N.ks_lval.p, N.ks_diag.p, N.ku_base.p);
+  TPT_CHECK_LAUNCH();
+  N.sym_built = true;
+}
 
 bool nb_build_operator(SystemData& S) {
   if (S.nb.state != 0) return S.nb.state == 1;

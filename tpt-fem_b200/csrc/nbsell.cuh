@@ -55,6 +55,84 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_spmv(int ngroups, const int* 
   }
 }
 
+// y = K x from the symmetric half storage (nb_build_sym): diagonal block,
+// strictly-lower blocks, and the transposes of the lower blocks of the upper
+// neighbours (read where their rows store them; those rows are processed by
+// nearby warps, so the second read of a block is mostly an L2 hit).
+// K is symmetric up to FP64 rounding of the element matrices; this operator
+// uses its lower half for both halves.
+template <int DPN, bool DOT>
+__global__ void __launch_bounds__(SPMV_THREADS) nb_spmv_sym(int ngroups, const int* __restrict__ lcptr,
+                                                            const int* __restrict__ lcol,
+                                                            const double* __restrict__ lval,
+                                                            const double* __restrict__ dval,
+                                                            const int* __restrict__ ucptr,
+                                                            const int* __restrict__ ucol,
+                                                            const int* __restrict__ ubase,
+                                                            const double* __restrict__ x, double* __restrict__ y,
+                                                            PcgState* st, double* partials, bool skip_done) {
+  if (skip_done && st->done) return;
+  constexpr int D2 = DPN * DPN;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int nchunks = (ngroups + 31) >> 5;
+  double d[1] = {0.0};
+  for (int c = warp; c < nchunks; c += nw) {
+    const int g = c * 32 + lane;
+    if (g < ngroups) {
+      double xg[DPN], acc[DPN];
+#pragma unroll
+      for (int b = 0; b < DPN; ++b) xg[b] = x[(int64_t)g * DPN + b];
+#pragma unroll
+      for (int a = 0; a < DPN; ++a) {
+        double s = 0.0;
+#pragma unroll
+        for (int b = 0; b < DPN; ++b) s += dval[((int64_t)c * D2 + a * DPN + b) * 32 + lane] * xg[b];
+        acc[a] = s;
+      }
+      const int l1 = lcptr[c + 1];
+      for (int s = lcptr[c]; s < l1; ++s) {
+        const int J = lcol[(int64_t)s * 32 + lane];
+        double xj[DPN];
+#pragma unroll
+        for (int b = 0; b < DPN; ++b) xj[b] = __ldg(x + (int64_t)J * DPN + b);
+        const double* v = lval + (int64_t)s * D2 * 32 + lane;
+#pragma unroll
+        for (int a = 0; a < DPN; ++a)
+#pragma unroll
+          for (int b = 0; b < DPN; ++b) acc[a] += v[(a * DPN + b) * 32] * xj[b];
+      }
+      const int u1 = ucptr[c + 1];
+      for (int s = ucptr[c]; s < u1; ++s) {
+        const int64_t idx = (int64_t)s * 32 + lane;
+        const int base = ubase[idx];
+        if (base < 0) continue;
+        const int J = ucol[idx];
+        double xj[DPN];
+#pragma unroll
+        for (int b = 0; b < DPN; ++b) xj[b] = __ldg(x + (int64_t)J * DPN + b);
+        const double* v = lval + base;
+#pragma unroll
+        for (int a = 0; a < DPN; ++a)
+#pragma unroll
+          for (int b = 0; b < DPN; ++b) acc[a] += __ldg(v + (b * DPN + a) * 32) * xj[b];
+      }
+#pragma unroll
+      for (int a = 0; a < DPN; ++a) {
+        y[(int64_t)g * DPN + a] = acc[a];
+        if (DOT) d[0] += xg[a] * acc[a];
+      }
+    }
+  }
+  if (DOT) {
+    if (grid_sum<1>(d, partials, &st->ticket[0])) {
+      st->pq = d[0];
+      if (!(d[0] > 0.0)) st->done = 2;
+    }
+  }
+}
+
 // One FP16 block of a factor slot: 8 values in a 16-byte word (row-major
 // entries 0..7) plus the 9th entry (3x3) in a separate 2-byte array, so a lane
 // issues two loads per block.  For DPN < 3 the word holds all D2 entries.

@@ -85,6 +85,11 @@ struct NbSell {
   DevBuf<uint4> l_pack, u_pack;  // 8 FP16 block values per slot and lane
   DevBuf<__half> l_tail, u_tail, l_diag;
   bool factor_checked = false, factor_ok = false;
+  // symmetric half storage of K: lower blocks in the L slots, diagonal blocks
+  // per chunk, and for each L^T slot the base index of the transposed block
+  bool sym_built = false;
+  DevBuf<double> ks_lval, ks_diag;
+  DevBuf<int> ku_base;
 };
 
 struct SystemData {
@@ -134,11 +139,13 @@ bool fsai_set_values(const SystemData& S, FsaiFactor& F, const double* d_sig2, c
 // nbsell.cu
 bool nb_build_operator(SystemData& S);  // false when the system has partial node groups
 bool nb_fill_factor(SystemData& S, const FsaiFactor& F);  // false: factor rows not node-block shaped
+void nb_build_sym(SystemData& S);  // after nb_build_operator succeeded
 
 // solver.cu
 int64_t system_fsai_classic(SystemData& S);  // builds (once) the classic factor; -1 on failure
 void system_fsai_download(const SystemData& S, int64_t* rp, int64_t* ci, double* lva, double* sig2);
-void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32, double* ms_nb, double* nb_bytes);
+void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32, double* ms_nb, double* nb_bytes,
+                         double* ms_nbs, double* nbs_bytes);
 void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats& st);
 
 // topopt.cu

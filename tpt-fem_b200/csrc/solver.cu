@@ -103,7 +103,7 @@ struct Engine {
   cudaGraphExec_t exec = nullptr;
   // node-block sliced-ELL operator / FSAI factor (FP64 engines only)
   const NbSell* nb = nullptr;
-  bool nb_op = false, nb_pc = false;
+  bool nb_op = false, nb_pc = false, nb_sym = false;
   int nb_grid = 1;
   ~Engine() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -121,6 +121,19 @@ struct Engine {
   // q = A p with the pq reduction (K1).
   void op_dot(cudaStream_t s, const T* x, T* y) {
     if constexpr (std::is_same<T, double>::value) {
+      if (nb_op && nb_sym) {
+        const NbSell& N = *nb;
+#define TPT_NB_SYM(D)                                                                                           \
+  nb_spmv_sym<D, true><<<nb_grid, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.ks_lval.p,          \
+                                                        N.ks_diag.p, N.u_cptr.p, N.u_col.p, N.ku_base.p, x, y,  \
+                                                        st.p, partials.p, true);
+        if (N.dpn == 3) { TPT_NB_SYM(3) }
+        else if (N.dpn == 2) { TPT_NB_SYM(2) }
+        else { TPT_NB_SYM(1) }
+#undef TPT_NB_SYM
+        TPT_CHECK_LAUNCH();
+        return;
+      }
       if (nb_op) {
         const NbSell& N = *nb;
         if (N.dpn == 3) nb_spmv<3, true><<<nb_grid, SPMV_THREADS, 0, s>>>(N.ngroups, N.k_cptr.p, N.k_col.p, N.k_val.p, x, y, st.p, partials.p, true);
@@ -214,14 +227,15 @@ struct Engine {
 };
 
 struct SolverWork {
-  Engine<double> f64;
+  Engine<double> f64;      // Jacobi, FP64 (node-block operator when the system allows it)
+  Engine<double> f64_csr;  // Jacobi, FP64, CSR operator only (TPTFEM_SOLVE_CSR_ONLY)
   Engine<float> f32;       // Jacobi, FP32 Krylov
   Engine<double> f64_fsai; // FSAI (FP16 factor), FP64 Krylov
   Engine<double> f64_lf;   // learned FSAI (FP16 factor), FP64 Krylov
   FsaiFactor fsai, lf;
   LfGraph lgraph;
   const FsaiFactor* nb_factor = nullptr;  // factor whose blocks S.nb holds
-  bool f64_ready = false, f32_ready = false, fsai_ready = false, fsai_failed = false;
+  bool f64_ready = false, f64_csr_ready = false, f32_ready = false, fsai_ready = false, fsai_failed = false;
   bool lf_ready = false, lf_engine = false;
   DevBuf<double> rhi;   // FP64 true residual
   DevBuf<double> sc;    // scalars
@@ -247,6 +261,19 @@ void ensure_work(SystemData& S) {
     S.work->tk.alloc(8, s);
     S.work->tk.zero();
     S.work->partials.alloc(4096, s);
+  }
+}
+
+// Node-block engines use the symmetric half storage of K unless the caller
+// asks for the full operator (TPTFEM_SOLVE_FULL_OPERATOR); switching drops the
+// engine's captured graph.
+void select_nb_mode(SystemData& S, Engine<double>& E, const tptfem_solver_opts& o) {
+  if (!E.nb_op) return;
+  const bool sym = !(o.flags & TPTFEM_SOLVE_FULL_OPERATOR);
+  if (sym) nb_build_sym(S);
+  if (E.nb_sym != sym) {
+    E.nb_sym = sym;
+    if (E.exec) { cudaGraphExecDestroy(E.exec); E.exec = nullptr; }
   }
 }
 
@@ -455,6 +482,7 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
         S.x.zero();
       } else {
         const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : 1e-3;
+        select_nb_mode(S, W.f64_lf, o);
         try {
           iters = run_reliable<double>(S, W.f64_lf, tol, delta, max_it, bnorm, st);
         } catch (const Error& e) {
@@ -500,7 +528,9 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
         nb_fill_factor(S, W.fsai);
         W.nb_factor = &W.fsai;
       }
-    } else if (solver == TPTFEM_SOLVER_JACOBI_PCG && W.f64_ready) {
+    } else if (solver == TPTFEM_SOLVER_JACOBI_PCG && (o.flags & TPTFEM_SOLVE_CSR_ONLY) && W.f64_csr_ready) {
+      refresh_jacobi<double>(S, W.f64_csr);
+    } else if (solver == TPTFEM_SOLVER_JACOBI_PCG && !(o.flags & TPTFEM_SOLVE_CSR_ONLY) && W.f64_ready) {
       refresh_jacobi<double>(S, W.f64);
     } else if (solver == TPTFEM_SOLVER_MP_PCG && W.f32_ready) {
       refresh_jacobi<float>(S, W.f32);
@@ -525,9 +555,14 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
       st.fell_back = 1;
     }
   }
-  if (solver == TPTFEM_SOLVER_JACOBI_PCG && !W.f64_ready) {
+  const bool csr_only = (o.flags & TPTFEM_SOLVE_CSR_ONLY) != 0;
+  if (solver == TPTFEM_SOLVER_JACOBI_PCG && csr_only && !W.f64_csr_ready) {
+    prepare_jacobi<double>(S, W.f64_csr, S.val.p, batch);
+    W.f64_csr_ready = true;
+  }
+  if (solver == TPTFEM_SOLVER_JACOBI_PCG && !csr_only && !W.f64_ready) {
     prepare_jacobi<double>(S, W.f64, S.val.p, batch);
-    if (!(o.flags & TPTFEM_SOLVE_CSR_ONLY) && nb_build_operator(S)) W.f64.use_nb(&S.nb, true, false);
+    if (nb_build_operator(S)) W.f64.use_nb(&S.nb, true, false);
     W.f64_ready = true;
   }
   if (solver == TPTFEM_SOLVER_MP_PCG && !W.f32_ready) {
@@ -544,12 +579,15 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
     S.x.zero();
   } else if (solver == TPTFEM_SOLVER_JACOBI_PCG) {
     const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : 1e-3;
-    iters = run_reliable<double>(S, W.f64, tol, delta, max_it, bnorm, st);
+    Engine<double>& EJ = csr_only ? W.f64_csr : W.f64;
+    select_nb_mode(S, EJ, o);
+    iters = run_reliable<double>(S, EJ, tol, delta, max_it, bnorm, st);
   } else if (solver == TPTFEM_SOLVER_MP_PCG) {
     const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : 0.05;
     iters = run_reliable<float>(S, W.f32, tol, delta, max_it, bnorm, st);
   } else {
     const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : 1e-3;
+    select_nb_mode(S, W.f64_fsai, o);
     iters = run_reliable<double>(S, W.f64_fsai, tol, delta, max_it, bnorm, st);
   }
   const double rel = bb == 0.0 ? 0.0 : std::sqrt(true_residual2(S, S.x.p)) / bnorm;
@@ -620,7 +658,8 @@ void system_fsai_download(const SystemData& S, int64_t* rp, int64_t* ci, double*
 // Average device time of the solver's SpMV kernels on this system (diagnostic
 // for the roofline report): FP64 and FP32 CSR, `reps` back-to-back launches
 // each, timed with events on the context stream.
-void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32, double* ms_nb, double* nb_bytes) {
+void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32, double* ms_nb, double* nb_bytes,
+                         double* ms_nbs, double* nbs_bytes) {
   cudaStream_t s = S.ctx->stream;
   ensure_work(S);
   ensure_val32(S);
@@ -663,6 +702,23 @@ void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32
     });
     *nb_bytes = (double)N.k_slots * 32 * (4 + 8 * N.dpn * N.dpn) + (double)(N.nchunks + 1) * 4 +
                 16.0 * (double)S.n_free;
+    nb_build_sym(S);
+    *ms_nbs = timeit([&] {
+#define TPT_NB_SYM(D)                                                                                             \
+  nb_spmv_sym<D, false><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.ks_lval.p, N.ks_diag.p,     \
+                                                   N.u_cptr.p, N.u_col.p, N.ku_base.p, x64.p, y64.p, nullptr,      \
+                                                   nullptr, false);
+      if (N.dpn == 3) { TPT_NB_SYM(3) }
+      else if (N.dpn == 2) { TPT_NB_SYM(2) }
+      else { TPT_NB_SYM(1) }
+#undef TPT_NB_SYM
+      TPT_CHECK_LAUNCH();
+    });
+    // bytes the half storage must move: lower and diagonal blocks, lower
+    // columns, upper columns and block indices, chunk pointers, x and y
+    const double d2 = (double)(N.dpn * N.dpn);
+    *nbs_bytes = (double)N.l_slots * 32 * (4 + 8 * d2) + (double)N.nchunks * 32 * 8 * d2 +
+                 (double)N.u_slots * 32 * 8 + 2.0 * (N.nchunks + 1) * 4 + 16.0 * (double)S.n_free;
   }
 }
 

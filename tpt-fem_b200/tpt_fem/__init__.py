@@ -289,11 +289,12 @@ def _bcs(bcs):
 
 
 def _opts(solver=SOLVER_JACOBI_PCG, tol=1e-10, inner_tol=0.0, max_iter=0, max_outer=0, batch=0, fresh_setup=False,
-          csr_only=False):
+          csr_only=False, full_operator=False):
     o = SolverOpts()
     o.solver, o.rel_tol, o.inner_rel_tol, o.max_iter, o.max_outer, o.batch = solver, tol, inner_tol, max_iter, \
         max_outer, batch
-    o.flags = (N.SOLVE_FRESH_SETUP if fresh_setup else 0) | (N.SOLVE_CSR_ONLY if csr_only else 0)
+    o.flags = (N.SOLVE_FRESH_SETUP if fresh_setup else 0) | (N.SOLVE_CSR_ONLY if csr_only else 0) | \
+        (N.SOLVE_FULL_OPERATOR if full_operator else 0)
     return o
 
 
@@ -325,11 +326,12 @@ class System:
         return st.as_dict()
 
     def profile_spmv(self, reps=20):
-        """Average device ms of the solver's SpMV kernels: (FP64 CSR, FP32 CSR, FP64 node-block, node-block bytes)."""
-        a, b, c, d = C.c_double(), C.c_double(), C.c_double(), C.c_double()
-        self.ctx.check(self.ctx.lib.tptfem_system_profile_spmv(self.ctx.h, self.h, reps, C.byref(a), C.byref(b),
-                                                               C.byref(c), C.byref(d)))
-        return a.value, b.value, c.value, d.value
+        """Average device ms of the solver's SpMV kernels as a dict: FP64 CSR, FP32 CSR, FP64 node-block
+        full storage and symmetric half storage (with the bytes those layouts move per launch)."""
+        v = [C.c_double() for _ in range(6)]
+        self.ctx.check(self.ctx.lib.tptfem_system_profile_spmv(self.ctx.h, self.h, reps, *[C.byref(x) for x in v]))
+        a, b, c, d, e, f = (x.value for x in v)
+        return {"csr_f64_ms": a, "csr_f32_ms": b, "nb_ms": c, "nb_bytes": d, "nbs_ms": e, "nbs_bytes": f}
 
     def fsai(self):
         """Classic FSAI factor: (L row_ptrs, L cols, L values, sigma^2); G = diag(sigma)(I + L)."""

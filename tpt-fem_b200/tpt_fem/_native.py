@@ -23,6 +23,7 @@ MODEL_BAR_AXIAL, MODEL_PLANE_STRESS, MODEL_PLANE_STRAIN, MODEL_CONTINUUM_3D = 0,
 SOLVER_JACOBI_PCG, SOLVER_MP_PCG, SOLVER_FSAI_MP_PCG, SOLVER_LEARNED_FSAI_PCG = 0, 1, 2, 3
 SOLVE_FRESH_SETUP = 1
 SOLVE_CSR_ONLY = 2
+SOLVE_FULL_OPERATOR = 4
 
 
 class SolverOpts(C.Structure):
@@ -98,7 +99,7 @@ SIGNATURES = {
     "tptfem_system_solve": (C.c_int, [_vp, _vp, C.POINTER(SolverOpts), C.POINTER(SolveStats)]),
     "tptfem_system_solution": (C.c_int, [_vp, _vp, _vp]),
     "tptfem_system_free": (None, [_vp]),
-    "tptfem_system_profile_spmv": (C.c_int, [_vp, _vp, C.c_int, _pd, _pd, _pd, _pd]),
+    "tptfem_system_profile_spmv": (C.c_int, [_vp, _vp, C.c_int, _pd, _pd, _pd, _pd, _pd, _pd]),
     "tptfem_system_fsai": (C.c_int, [_vp, _vp, _pi64]),
     "tptfem_lfsai_param_count": (C.c_int64, []),
     "tptfem_lfsai_create": (C.c_int, [_vp, C.c_uint64, _pp]),

@@ -98,3 +98,28 @@ CANTILEVERS = {
     "cantilever_400x100x100": ([0.0, 0.0, 0.0], [4.0, 1.0, 1.0], [400, 100, 100]),
     "cube_elasticity_64": ([0.0, 0.0, 0.0], [1.0, 1.0, 1.0], [64, 64, 64]),
 }
+
+
+TOPOPT_SIZES = [(60, 20), (90, 30), (120, 40), (180, 60), (240, 80)]
+
+
+def topopt_batch_problems(n=512, seed=7, max_iter=100):
+    """The batched 2-D SIMP workload: n plane-stress Q1 cantilevers, (nelx, nely)
+    drawn uniformly from TOPOPT_SIZES, vol_frac ~ U[0.3, 0.5], E0 = 1,
+    Emin = 1e-9, nu = 0.3, penalty 3, density filter radius 1.5 (h = 1), move
+    limit 0.2, left edge clamped, unit -y load at the mid-right node
+    (i = nelx, j = nely / 2), max_iter OC iterations.  Returns
+    [(TopOptParams, f, bcs), ...] for tpt_fem.topopt.topopt_batch."""
+    from .topopt import Grid, TopOptParams, cantilever_load
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(0, len(TOPOPT_SIZES), size=n)
+    vfs = rng.uniform(0.3, 0.5, size=n)
+    out = []
+    for k in range(n):
+        nelx, nely = TOPOPT_SIZES[sizes[k]]
+        g = Grid(nelx + 1, nely + 1, 1.0)
+        P = TopOptParams(grid=g, e0=1.0, nu=0.3, vol_frac=float(vfs[k]), penal=3.0, filter_radius=1.5,
+                         max_iter=max_iter, move_limit=0.2, emin=1e-9, density_filter=True)
+        f, bcs = cantilever_load(g, 1.0, node=g.nx * (nely // 2) + nelx)
+        out.append((P, f, bcs))
+    return out
