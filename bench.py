@@ -176,8 +176,10 @@ class CpuSample:
 
 # ---- our arm -----------------------------------------------------------------------
 
-def build_system(F, W, ctx, with_host=False):
+def build_system(F, W, ctx, mesh_cells=None):
     mn, mx, n = W.CANTILEVERS[WORKLOAD]
+    if mesh_cells:
+        n = list(mesh_cells)
     E = W.cantilever_young(n)
     mesh = F.Mesh.box_mesh(mn, mx, n, ctx=ctx)
     K = F.assemble_elasticity(mesh, "3d", E, 0.3, 2)
@@ -222,7 +224,7 @@ def run_ours(args, world, rank, local):
     from tpt_fem import lfsai as LF
     from tpt_fem import workloads as W
     ctx = F.Context(local)
-    mesh, K, S, E, rhs, dof, val = build_system(F, W, ctx)
+    mesh, K, S, E, rhs, dof, val = build_system(F, W, ctx, args.mesh if args.profile else None)
     model = LF.LearnedFsai.load(ctx, WEIGHTS)
     model.attach(S)
     solver = {"learned": F.SOLVER_LEARNED_FSAI_PCG, "fsai": F.SOLVER_FSAI_MP_PCG, "jacobi": F.SOLVER_JACOBI_PCG,
@@ -293,7 +295,9 @@ def run_ours(args, world, rank, local):
                        "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (matrix 1.85 GB)"},
             "solver_stats": {"iterations_median": statistics.median(its), "rel_residual": steps[-1]["rel_residual"],
                              "setup_ms": steps[-1]["setup_ms"], "solve_ms": steps[-1]["solve_ms"],
-                             "reliable_updates": steps[-1]["outer_steps"], "fell_back": steps[-1]["fell_back"]},
+                             "reliable_updates": steps[-1]["outer_steps"], "fell_back": steps[-1]["fell_back"],
+                             "step_s": [round(seconds(st), 4) for st in steps],
+                             "setup_ms_steps": [round(st["setup_ms"], 2) for st in steps]},
             "fp64_jacobi_pcg": {"seconds": seconds(jac), "iterations": jac["iterations"],
                                 "rel_residual": jac["rel_residual"], "operator": "CSR"},
             "fp64_jacobi_pcg_node_block": {"seconds": seconds(jac_nb), "iterations": jac_nb["iterations"],
@@ -353,6 +357,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--solver", default="learned", choices=["learned", "fsai", "jacobi", "mp"])
     ap.add_argument("--profile", action="store_true", help="run only the timed solves (ncu launch list)")
+    ap.add_argument("--mesh", type=int, nargs=3, default=None,
+                    help="with --profile: cantilever cells (a smaller case for ncu captures)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":

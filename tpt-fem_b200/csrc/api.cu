@@ -109,6 +109,14 @@ tptfem_status tptfem_create(int device, tptfem_context** out) {
     for (auto& e : ctx->ev) TPT_CUDA(cudaEventCreate(&e));
     TPT_CUDA(cudaMalloc(&ctx->d_flag, 64));
     TPT_CUDA(cudaMallocHost(&ctx->h_pinned, 64));
+    // Stream-ordered allocations (every temporary of the solver and the
+    // learned factor) come from the device's default pool; keep freed blocks
+    // in it instead of unmapping them at each synchronisation, so repeated
+    // solves reuse memory without remapping.  tptfem_destroy trims the pool.
+    cudaMemPool_t pool;
+    TPT_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = UINT64_MAX;
+    TPT_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
   } catch (const Error& e) {
     tptfem_destroy(ctx);
     return e.status;
@@ -126,6 +134,8 @@ void tptfem_destroy(tptfem_context* ctx) {
   if (ctx->d_flag) cudaFree(ctx->d_flag);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
   delete ctx;
 }
 

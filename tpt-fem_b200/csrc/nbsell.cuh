@@ -57,8 +57,11 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_spmv(int ngroups, const int* 
 
 // y = K x from the symmetric half storage (nb_build_sym): diagonal block,
 // strictly-lower blocks, and the transposes of the lower blocks of the upper
-// neighbours (read where their rows store them; those rows are processed by
-// nearby warps, so the second read of a block is mostly an L2 hit).
+// neighbours, read where their rows store them.  Step k handles lower slot k
+// and upper slot nu-1-k (upper columns descending): block (J, g) is then read
+// by row g in the same step in which row J reads it as its own lower block
+// (J's lower list is ascending), so the two reads of a block by concurrently
+// running warps are close in time and the second one is an L2 hit.
 // K is symmetric up to FP64 rounding of the element matrices; this operator
 // uses its lower half for both halves.
 template <int DPN, bool DOT>
@@ -91,32 +94,38 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_spmv_sym(int ngroups, const i
         for (int b = 0; b < DPN; ++b) s += dval[((int64_t)c * D2 + a * DPN + b) * 32 + lane] * xg[b];
         acc[a] = s;
       }
-      const int l1 = lcptr[c + 1];
-      for (int s = lcptr[c]; s < l1; ++s) {
-        const int J = lcol[(int64_t)s * 32 + lane];
-        double xj[DPN];
+      // lower slot k and upper slot (nu - 1 - k) in the same step
+      const int l0 = lcptr[c], nl = lcptr[c + 1] - l0;
+      const int u0 = ucptr[c], nu = ucptr[c + 1] - u0;
+      const int steps = nl > nu ? nl : nu;
+      for (int k = 0; k < steps; ++k) {
+        if (k < nu) {
+          const int64_t idx = (int64_t)(u0 + nu - 1 - k) * 32 + lane;
+          const int base = ubase[idx];
+          if (base >= 0) {
+            const int J = ucol[idx];
+            double xj[DPN];
 #pragma unroll
-        for (int b = 0; b < DPN; ++b) xj[b] = __ldg(x + (int64_t)J * DPN + b);
-        const double* v = lval + (int64_t)s * D2 * 32 + lane;
+            for (int b = 0; b < DPN; ++b) xj[b] = __ldg(x + (int64_t)J * DPN + b);
+            const double* v = lval + base;
 #pragma unroll
-        for (int a = 0; a < DPN; ++a)
+            for (int a = 0; a < DPN; ++a)
 #pragma unroll
-          for (int b = 0; b < DPN; ++b) acc[a] += v[(a * DPN + b) * 32] * xj[b];
-      }
-      const int u1 = ucptr[c + 1];
-      for (int s = ucptr[c]; s < u1; ++s) {
-        const int64_t idx = (int64_t)s * 32 + lane;
-        const int base = ubase[idx];
-        if (base < 0) continue;
-        const int J = ucol[idx];
-        double xj[DPN];
+              for (int b = 0; b < DPN; ++b) acc[a] += __ldg(v + (b * DPN + a) * 32) * xj[b];
+          }
+        }
+        if (k < nl) {
+          const int64_t s = l0 + k;
+          const int J = lcol[s * 32 + lane];
+          double xj[DPN];
 #pragma unroll
-        for (int b = 0; b < DPN; ++b) xj[b] = __ldg(x + (int64_t)J * DPN + b);
-        const double* v = lval + base;
+          for (int b = 0; b < DPN; ++b) xj[b] = __ldg(x + (int64_t)J * DPN + b);
+          const double* v = lval + s * D2 * 32 + lane;
 #pragma unroll
-        for (int a = 0; a < DPN; ++a)
+          for (int a = 0; a < DPN; ++a)
 #pragma unroll
-          for (int b = 0; b < DPN; ++b) acc[a] += __ldg(v + (b * DPN + a) * 32) * xj[b];
+            for (int b = 0; b < DPN; ++b) acc[a] += v[(a * DPN + b) * 32] * xj[b];
+        }
       }
 #pragma unroll
       for (int a = 0; a < DPN; ++a) {

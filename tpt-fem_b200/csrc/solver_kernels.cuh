@@ -217,19 +217,46 @@ __global__ void __launch_bounds__(SPMV_THREADS) fsai_upper_rz(int n, const int* 
 
 // ---- PCG vector kernels ------------------------------------------------------------
 
+template <typename T>
+struct Pair;
+template <>
+struct Pair<double> { using type = double2; };
+template <>
+struct Pair<float> { using type = float2; };
+
 // K2: alpha = rz/pq; xl += alpha p; r -= alpha q; rr (and, Jacobi, rz' = r.D^-1 r).
+// Two elements per thread and step (8- or 16-byte loads; vectors are whole
+// stream-ordered allocations, so 16-byte aligned).
 template <typename T, bool JACOBI>
 __global__ void __launch_bounds__(VEC_THREADS) pcg_update(int n, int par, T* __restrict__ xl, T* __restrict__ r,
                                                           const T* __restrict__ p, const T* __restrict__ q,
                                                           const T* __restrict__ dinv, PcgState* st,
                                                           double* partials) {
   if (st->done) return;
+  using V = typename Pair<T>::type;
   const double rz = st->rz[par];
   const T a = (T)(rz / st->pq);
   double v[2] = {0.0, 0.0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (int i = tid; i < (n >> 1); i += stride) {
+    V xv = reinterpret_cast<V*>(xl)[i], rv = reinterpret_cast<V*>(r)[i];
+    const V pv = reinterpret_cast<const V*>(p)[i], qv = reinterpret_cast<const V*>(q)[i];
+    xv.x += a * pv.x;
+    xv.y += a * pv.y;
+    rv.x = rv.x - a * qv.x;
+    rv.y = rv.y - a * qv.y;
+    reinterpret_cast<V*>(xl)[i] = xv;
+    reinterpret_cast<V*>(r)[i] = rv;
+    if (JACOBI) {
+      const V dv = reinterpret_cast<const V*>(dinv)[i];
+      v[0] += (double)rv.x * (double)(dv.x * rv.x) + (double)rv.y * (double)(dv.y * rv.y);
+    }
+    v[1] += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
+  }
+  if ((n & 1) && tid == 0) {
+    const int i = n - 1;
     xl[i] += a * p[i];
-    T ri = r[i] - a * q[i];
+    const T ri = r[i] - a * q[i];
     r[i] = ri;
     if (JACOBI) v[0] += (double)ri * (double)(dinv[i] * ri);
     v[1] += (double)ri * (double)ri;
@@ -251,9 +278,23 @@ __global__ void __launch_bounds__(VEC_THREADS) pcg_direction(int n, int par, con
                                                              T* __restrict__ p, const T* __restrict__ dinv,
                                                              const T* __restrict__ z, const PcgState* st) {
   if (st->done) return;
+  using V = typename Pair<T>::type;
   const T beta = (T)(st->rz[par ^ 1] / st->rz[par]);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    p[i] = (JACOBI ? dinv[i] * r[i] : z[i]) + beta * p[i];
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (int i = tid; i < (n >> 1); i += stride) {
+    V pv = reinterpret_cast<V*>(p)[i], zv;
+    if (JACOBI) {
+      const V dv = reinterpret_cast<const V*>(dinv)[i], rv = reinterpret_cast<const V*>(r)[i];
+      zv.x = dv.x * rv.x;
+      zv.y = dv.y * rv.y;
+    } else {
+      zv = reinterpret_cast<const V*>(z)[i];
+    }
+    pv.x = zv.x + beta * pv.x;
+    pv.y = zv.y + beta * pv.y;
+    reinterpret_cast<V*>(p)[i] = pv;
+  }
+  if ((n & 1) && tid == 0) p[n - 1] = (JACOBI ? dinv[n - 1] * r[n - 1] : z[n - 1]) + beta * p[n - 1];
 }
 
 __global__ void init_state(PcgState* st, int max_iters) {
