@@ -92,6 +92,8 @@ typedef struct tptfem_solver_opts {
   int64_t max_iter;      /* cap on total PCG iterations (0 -> 100000) */
   int32_t batch;         /* PCG iterations per CUDA-graph launch (0 -> auto) */
   int32_t flags;         /* TPTFEM_SOLVE_* bits */
+  int32_t coarse_aggregates;  /* TPTFEM_SOLVE_COARSE: target number of aggregates (0 -> 500) */
+  int32_t reserved;
 } tptfem_solver_opts;
 
 /* Recompute the preconditioner's values inside this solve (they are otherwise
@@ -106,6 +108,14 @@ typedef struct tptfem_solver_opts {
  * the transposes of the lower blocks; K is symmetric up to the FP64 rounding
  * of its element matrices, and the FP64 true residual always uses K itself). */
 #define TPTFEM_SOLVE_FULL_OPERATOR 4
+/* FSAI / learned-FSAI solvers: add an aggregation coarse correction,
+ * M^-1 = G^T G + P A_c^-1 P^T, with P the rigid-body modes (translations and
+ * rotations; constants for one dof per node) of the free nodes binned by
+ * coordinates into about coarse_aggregates boxes, A_c = P^T A P factorised in
+ * FP64 and applied as an FP32 inverse.  Needs full node groups and the mesh
+ * geometry (systems from tptfem_reduce_system); otherwise the solve runs
+ * without it (stats.coarse_size = 0). */
+#define TPTFEM_SOLVE_COARSE 8
 
 typedef struct tptfem_solve_stats {
   int64_t iterations;    /* total PCG iterations (inner iterations for MP) */
@@ -115,7 +125,7 @@ typedef struct tptfem_solve_stats {
   double setup_ms;       /* preconditioner set-up, device time (first solve of a system) */
   double solve_ms;       /* iterations + residual checks, device time */
   int32_t fell_back;     /* 1 if the requested method fell back to FP64 Jacobi-PCG */
-  int32_t reserved;
+  int32_t coarse_size;   /* dimension of the coarse space used (0: none) */
 } tptfem_solve_stats;
 
 /* ---- context ---------------------------------------------------------------- */
@@ -214,6 +224,14 @@ tptfem_status tptfem_system_fsai_download(tptfem_context* ctx, const tptfem_syst
 tptfem_status tptfem_system_profile_spmv(tptfem_context* ctx, tptfem_system* sys, int reps, double* ms_f64,
                                          double* ms_f32, double* ms_nb_f64, double* nb_bytes, double* ms_nbs_f64,
                                          double* nbs_bytes);
+
+/* Diagnostic (no reference counterpart): the aggregation coarse space of the
+ * system's last TPTFEM_SOLVE_COARSE solve -- number of aggregates, modes per
+ * aggregate, bins per axis and, when ainv is non-NULL, the FP32 inverse of
+ * A_c = P^T A P widened to FP64 ((na*nm)^2 values, row-major).  *na = 0 when
+ * no coarse space was built. */
+tptfem_status tptfem_system_coarse(tptfem_context* ctx, const tptfem_system* sys, int32_t* na, int32_t* nm,
+                                   int32_t* bins, double* ainv);
 
 /* Allocation-free check of a solution (no counterpart in the reference):
  * relative residual ||b - A x||_2 / ||b||_2 of an n x n CSR system whose arrays

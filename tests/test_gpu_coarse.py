@@ -1,0 +1,111 @@
+"""Two-level (FSAI + aggregation coarse space) solves on the GPU: the coarse
+matrix against the CPU oracle's P^T A P, convergence to the FP64 tolerance,
+agreement with the plain method, and the iterations it saves."""
+import numpy as np
+import pytest
+
+import tpt_fem as F
+from tpt_fem import lfsai as LF
+from tpt_fem import workloads as W
+from meshes import box, jitter
+from oracle import coarse_oracle as CO
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def cantilever(ctx, n, seed=3, jit=0.0):
+    mn, mx = [0.0, 0.0, 0.0], [4.0, 1.0, 1.0]
+    c, e = box(n, mn=mn, mx=mx)
+    if jit:
+        c = jitter(c, jit, seed)
+    m = F.Mesh.from_arrays(F.CELL_TET4, c, e, ctx=ctx)
+    K = F.assemble_elasticity(m, "3d", W.cantilever_young(n, seed=seed), 0.3, 2)
+    rhs = F.apply_traction(m, 3, 0, 1.0, [0.0, 0.0, -1e-3], np.zeros(K.nrows))
+    dof, val = W.clamp_x0_bcs(c)
+    return F.reduce_system(K, rhs, list(zip(dof, val))), c
+
+
+@pytest.mark.parametrize("jit", [0.0, 0.02])
+def test_coarse_matrix_matches_oracle(ctx, jit):
+    S, c = cantilever(ctx, [12, 4, 4], jit=jit)
+    st = S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=1e-12, coarse=True, coarse_aggregates=12)
+    assert st["coarse_size"] > 0 and st["rel_residual"] <= 1e-12
+    info = S.coarse(with_inverse=True)
+    rp, ci, va, fred, free = S.download()
+    Ac, P, na, nm = CO.coarse_matrix(rp, ci, va, c, free, 3, info["bins"])
+    assert (info["na"], info["nm"]) == (na, nm) and st["coarse_size"] == na * nm
+    ev_dev = np.sort(1.0 / np.linalg.eigvalsh(0.5 * (info["ainv"] + info["ainv"].T)))
+    ev_orc = np.sort(np.linalg.eigvalsh(Ac))
+    assert np.allclose(ev_dev, ev_orc, rtol=2e-4, atol=1e-6 * ev_orc.max())
+
+
+def test_two_level_solution_and_iterations(ctx):
+    S, c = cantilever(ctx, [32, 8, 8])
+    one = S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=1e-10)
+    u1 = S.solution()
+    two = S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=1e-10, coarse=True, coarse_aggregates=64, fresh_setup=True)
+    u2 = S.solution()
+    # direct solve of the same reduced system (scipy sparse LU) as the reference solution
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+    rp, ci, va, fred, free = S.download()
+    A = sp.csc_matrix(sp.csr_matrix((va, ci, rp), shape=(len(fred), len(fred))))
+    x = spl.spsolve(A, fred)
+    assert two["coarse_size"] > 0 and two["rel_residual"] <= 1e-10
+    assert two["iterations"] < 0.5 * one["iterations"]
+    scale = np.max(np.abs(x))
+    assert np.max(np.abs(u2[free] - x)) <= 1e-6 * scale and np.max(np.abs(u1[free] - x)) <= 1e-6 * scale
+    # deterministic: the same solve twice gives the same bits
+    again = S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=1e-10, coarse=True, coarse_aggregates=64, fresh_setup=True)
+    assert again["iterations"] == two["iterations"] and np.array_equal(S.solution(), u2)
+    # a different aggregate count rebuilds the coarse space on the same system
+    other = S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=1e-10, coarse=True, coarse_aggregates=16, fresh_setup=True)
+    assert not other["fell_back"] and 0 < other["coarse_size"] < two["coarse_size"]
+    assert other["rel_residual"] <= 1e-10 and other["iterations"] < one["iterations"]
+    back = S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=1e-10, coarse=True, coarse_aggregates=64, fresh_setup=True)
+    assert back["iterations"] == two["iterations"] and np.array_equal(S.solution(), u2)
+
+
+def test_learned_two_level(ctx):
+    S, c = cantilever(ctx, [32, 8, 8], seed=5)
+    model = LF.LearnedFsai(ctx, seed=1)
+    model.attach(S)
+    one = S.solve(solver=F.SOLVER_LEARNED_FSAI_PCG, tol=1e-10, fresh_setup=True)
+    two = S.solve(solver=F.SOLVER_LEARNED_FSAI_PCG, tol=1e-10, fresh_setup=True, coarse=True, coarse_aggregates=64)
+    assert not two["fell_back"] and two["coarse_size"] > 0 and two["rel_residual"] <= 1e-10
+    assert two["iterations"] < 0.5 * one["iterations"]
+
+
+def test_poisson_coarse_space(ctx):
+    c, e = box([16, 16, 16])
+    m = F.Mesh.from_arrays(F.CELL_TET4, c, e, ctx=ctx)
+    k = np.exp(np.random.default_rng(2).normal(0.0, 1.0, len(e)))
+    K = F.assemble_poisson(m, k, 2)
+    rhs = F.load_poisson_source(m, 1.0, 2)
+    on_b = np.nonzero(np.any((c < 1e-9) | (c > 1 - 1e-9), axis=1))[0]
+    S = F.reduce_system(K, rhs, [(int(i), 0.0) for i in on_b])
+    one = S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=1e-10)
+    two = S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=1e-10, coarse=True, coarse_aggregates=27, fresh_setup=True)
+    assert two["coarse_size"] > 0 and two["rel_residual"] <= 1e-10
+    assert two["iterations"] < one["iterations"]
+    info = S.coarse(with_inverse=True)
+    rp, ci, va, fred, free = S.download()
+    Ac, P, na, nm = CO.coarse_matrix(rp, ci, va, c, free, 1, info["bins"])
+    ev_dev = np.sort(1.0 / np.linalg.eigvalsh(0.5 * (info["ainv"] + info["ainv"].T)))
+    assert np.allclose(ev_dev, np.sort(np.linalg.eigvalsh(Ac)), rtol=2e-4)
+
+
+def test_coarse_not_applicable_runs_without_it(ctx):
+    # a roller support fixes one component only: partial node groups, no node-block layout
+    S, c = cantilever(ctx, [8, 3, 3])
+    c2, e = box([8, 3, 3], mn=[0.0, 0.0, 0.0], mx=[4.0, 1.0, 1.0])
+    m = F.Mesh.from_arrays(F.CELL_TET4, c2, e, ctx=ctx)
+    K = F.assemble_elasticity(m, "3d", 1.0, 0.3, 2)
+    rhs = F.apply_traction(m, 3, 0, 1.0, [0.0, 0.0, -1e-3], np.zeros(K.nrows))
+    x0 = [int(i) for i in O.nodes_on_plane(c2, 0, 0.0, 1e-9)]
+    bcs = [(3 * n, 0.0) for n in x0] + [(3 * x0[0] + 1, 0.0), (3 * x0[0] + 2, 0.0), (3 * x0[1] + 2, 0.0),
+                                        (3 * x0[-1] + 1, 0.0), (3 * x0[-1] + 2, 0.0)]
+    S2 = F.reduce_system(K, rhs, bcs)
+    st = S2.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=1e-10, coarse=True)
+    assert st["coarse_size"] == 0 and st["rel_residual"] <= 1e-10

@@ -3,6 +3,8 @@
 // Every entry point validates its arguments on the host before any launch,
 // converts int64 indices to the device's int32 with range checks, and maps
 // internal errors to tptfem_status plus a message kept in the context.
+#include <cusolverDn.h>
+
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -133,6 +135,7 @@ void tptfem_destroy(tptfem_context* ctx) {
     if (e) cudaEventDestroy(e);
   if (ctx->d_flag) cudaFree(ctx->d_flag);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+  if (ctx->cusolver) cusolverDnDestroy((cusolverDnHandle_t)ctx->cusolver);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
@@ -493,6 +496,25 @@ tptfem_status tptfem_system_profile_spmv(tptfem_context* ctx, tptfem_system* sys
   *nbs_bytes = 0.0;
   *ms_nbs_f64 = -1.0;
   system_profile_spmv(*sys->d, reps, ms_f64, ms_f32, ms_nb_f64, nb_bytes, ms_nbs_f64, nbs_bytes);
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_system_coarse(tptfem_context* ctx, const tptfem_system* sys, int32_t* na, int32_t* nm,
+                                   int32_t* bins, double* ainv) {
+  if (!ctx || !sys || !sys->d || !na || !nm) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  const SystemData& S = *sys->d;
+  *na = 0;
+  *nm = 0;
+  if (S.coarse.state == 1) {
+    int a = 0, m = 0;
+    coarse_download(S, &a, &m, S.coarse.ready ? ainv : nullptr);
+    *na = a;
+    *nm = m;
+    if (bins)
+      for (int d = 0; d < 3; ++d) bins[d] = S.coarse.bins[d];
+  }
   API_CATCH(ctx)
 }
 

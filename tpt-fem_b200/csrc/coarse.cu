@@ -1,0 +1,484 @@
+// coarse.cu -- aggregation coarse space with rigid-body modes for the
+// two-level (additive) preconditioner  M^-1 = G^T G + P A_c^-1 P^T.
+//
+// The slow modes left by a sparse approximate inverse on an elongated,
+// heterogeneous elastic body are smooth, near-rigid motions of large pieces
+// of it.  Free mesh nodes are binned by coordinates into boxes (aggregates);
+// on each aggregate the rigid-body modes (translations, and rotations about
+// its centroid) span the coarse space, orthonormalised per aggregate (modes
+// that an aggregate cannot carry, e.g. rotations of a single node, are
+// dropped).  A_c = P^T A P is formed with one operator product per (colour,
+// mode): aggregates are coloured by bin coordinates mod 3, so an aggregate has
+// at most one neighbour of each colour and P^T A (P e_{colour, mode}) yields
+// whole coarse columns without mixing.  A_c is factorised (cuSOLVER dpotrf /
+// dpotri, once per set-up, off the iteration path) and kept as an explicit
+// FP32 inverse, so each iteration adds one restriction, one coarse mat-vec
+// and a prolongation that is fused into the FSAI transpose kernel.
+// Requires the node-block layout (full node groups) and the mesh geometry.
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "modes.cuh"
+#include "objects.hpp"
+
+namespace tptfem {
+
+namespace {
+
+constexpr int CS_THREADS = 256;
+constexpr int CS_MAX_COARSE = 8192;
+
+__device__ __forceinline__ int colour_of(const int* b) { return (b[0] % 3) + 3 * (b[1] % 3) + 9 * (b[2] % 3); }
+
+// v = P e_{c, m}: orthonormal mode m on every aggregate of colour c, 0 elsewhere.
+template <int DPN>
+__global__ void cs_fill(int ngroups, const int* __restrict__ agg, const int* __restrict__ abin,
+                        const float* __restrict__ y, const double* __restrict__ T, int colour, int m,
+                        double* __restrict__ v) {
+  constexpr int NM = rigid_modes(DPN);
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  const int I = agg[g];
+  if (colour_of(abin + 3 * I) != colour) {
+#pragma unroll
+    for (int a = 0; a < DPN; ++a) v[(int64_t)g * DPN + a] = 0.0;
+    return;
+  }
+  double R[DPN][NM];
+  mode_rows<DPN>(y + 3 * (int64_t)g, R);
+  const double* t = T + (int64_t)I * NM * NM;
+#pragma unroll
+  for (int a = 0; a < DPN; ++a) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) s += R[a][k] * t[k * NM + m];
+    v[(int64_t)g * DPN + a] = s;
+  }
+}
+
+// Raw mode moments of one segment of an aggregate's group list:
+// smom[seg][k] = sum over its groups of (R_g^T w_g)_k, block-reduced in a
+// fixed order.
+template <int DPN>
+__global__ void __launch_bounds__(CS_THREADS) cs_moments(const int* __restrict__ sbeg, const int* __restrict__ send,
+                                                         const int* __restrict__ alist, const float* __restrict__ y,
+                                                         const double* __restrict__ w, double* __restrict__ smom) {
+  constexpr int NM = rigid_modes(DPN);
+  __shared__ double sh[CS_THREADS / 32][NM];
+  const int seg = blockIdx.x;
+  double s[NM];
+#pragma unroll
+  for (int k = 0; k < NM; ++k) s[k] = 0.0;
+  for (int t = sbeg[seg] + threadIdx.x; t < send[seg]; t += CS_THREADS) {
+    const int g = alist[t];
+    double R[DPN][NM];
+    mode_rows<DPN>(y + 3 * (int64_t)g, R);
+#pragma unroll
+    for (int a = 0; a < DPN; ++a) {
+      const double wa = w[(int64_t)g * DPN + a];
+#pragma unroll
+      for (int k = 0; k < NM; ++k) s[k] += R[a][k] * wa;
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NM; ++k) {
+    double x = s[k];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[wid][k] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < NM) {
+    double x = 0.0;
+    for (int q = 0; q < CS_THREADS / 32; ++q) x += sh[q][threadIdx.x];
+    smom[(int64_t)seg * NM + threadIdx.x] = x;
+  }
+}
+
+// Orthonormal-mode moments of aggregate I: T_I^T (sum of its segments' raw moments).
+__device__ __forceinline__ double agg_moment(int I, int mp, int nm, const int* __restrict__ aseg,
+                                             const double* __restrict__ smom, const double* __restrict__ T) {
+  const double* t = T + (int64_t)I * nm * nm;
+  double x = 0.0;
+  for (int k = 0; k < nm; ++k) {
+    double sk = 0.0;
+    for (int q = aseg[I]; q < aseg[I + 1]; ++q) sk += smom[(int64_t)q * nm + k];
+    x += t[k * nm + mp] * sk;
+  }
+  return x;
+}
+
+// Column block (J, m) of A_c from the moments of w = A P e_{c, m}: for each
+// aggregate I, J is its unique neighbour (itself included) of colour c.
+__global__ void cs_columns(int na, int nm, const int* __restrict__ abin, const int* __restrict__ bin2agg, int bx,
+                           int by, int bz, const int* __restrict__ aseg, const double* __restrict__ smom,
+                           const double* __restrict__ T, int colour, int m, double* __restrict__ Ac, int nc) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= na) return;
+  const int nbin[3] = {bx, by, bz};
+  int jb[3];
+  for (int d = 0; d < 3; ++d) {
+    const int want = (colour / (d == 0 ? 1 : (d == 1 ? 3 : 9))) % 3;
+    const int b = abin[3 * I + d];
+    jb[d] = -1;
+    for (int o = -1; o <= 1; ++o) {
+      const int c = b + o;
+      if (c >= 0 && c < nbin[d] && c % 3 == want) jb[d] = c;
+    }
+    if (jb[d] < 0) return;
+  }
+  const int J = bin2agg[((int64_t)jb[2] * by + jb[1]) * bx + jb[0]];
+  if (J < 0) return;
+  for (int mp = 0; mp < nm; ++mp)
+    Ac[((int64_t)I * nm + mp) * nc + (int64_t)J * nm + m] = agg_moment(I, mp, nm, aseg, smom, T);
+}
+
+// yc = P^T r from the segment moments.
+__global__ void cs_yc(int na, int nm, const int* __restrict__ aseg, const double* __restrict__ smom,
+                      const double* __restrict__ T, double* __restrict__ yc) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < na * nm) yc[j] = agg_moment(j / nm, j % nm, nm, aseg, smom, T);
+}
+
+// uc = A_c^-1 yc: one warp per row, FP32 matrix, FP64 accumulation.
+__global__ void __launch_bounds__(CS_THREADS) cs_gemv(int nc, const double* __restrict__ yc,
+                                                      const float* __restrict__ Ainv, double* __restrict__ uc) {
+  extern __shared__ double ys[];
+  for (int j = threadIdx.x; j < nc; j += blockDim.x) ys[j] = yc[j];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int row = blockIdx.x * (CS_THREADS / 32) + (threadIdx.x >> 5);
+  if (row >= nc) return;
+  const float* a = Ainv + (int64_t)row * nc;
+  double s = 0.0;
+  for (int j = lane; j < nc; j += 32) s += (double)a[j] * ys[j];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) uc[row] = s;
+}
+
+// Rows/columns of dropped modes are zero: put 1 on their diagonal.
+__global__ void cs_fix_diag(int nc, double* __restrict__ Ac) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nc && Ac[(int64_t)i * nc + i] == 0.0) Ac[(int64_t)i * nc + i] = 1.0;
+}
+
+// dpotri leaves the inverse in one triangle (column-major lower = row-major
+// upper of the stored array): mirror it and convert to FP32.
+__global__ void cs_symmetrize(int nc, const double* __restrict__ A, float* __restrict__ out) {
+  int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= (int64_t)nc * nc) return;
+  const int i = (int)(id / nc), j = (int)(id % nc);
+  // column-major lower triangle: element (r, c) with r >= c at A[c * nc + r]
+  const int r = i > j ? i : j, c = i > j ? j : i;
+  out[id] = (float)A[(int64_t)c * nc + r];
+}
+
+// Every operator block (g, h) must join aggregates at most one bin apart.
+__global__ void cs_check_adjacency(int ngroups, const int* __restrict__ gptr, const int* __restrict__ glist,
+                                   const int* __restrict__ gbin, int* __restrict__ flag) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  for (int t = gptr[g]; t < gptr[g + 1]; ++t) {
+    const int h = glist[t];
+    for (int d = 0; d < 3; ++d)
+      if (abs(gbin[3 * g + d] - gbin[3 * h + d]) > 1) atomicOr(flag, 1);
+  }
+}
+
+// Eigen-decomposition of a symmetric 3x3 matrix by cyclic Jacobi rotations
+// (host, once per aggregate): A = V diag(w) V^T, V column-major in v[3][3].
+void sym_eig3(double a[3][3], double w[3], double v[3][3]) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) v[i][j] = i == j;
+  for (int sweep = 0; sweep < 50; ++sweep) {
+    const double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
+    const double tr = a[0][0] * a[0][0] + a[1][1] * a[1][1] + a[2][2] * a[2][2];
+    if (off <= 1e-30 * (tr + 1e-300)) break;
+    for (int p = 0; p < 2; ++p)
+      for (int q = p + 1; q < 3; ++q) {
+        if (a[p][q] == 0.0) continue;
+        const double theta = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < 3; ++k) {  // A <- A J
+          const double akp = a[k][p], akq = a[k][q];
+          a[k][p] = c * akp - s * akq;
+          a[k][q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < 3; ++k) {  // A <- J^T A
+          const double apk = a[p][k], aqk = a[q][k];
+          a[p][k] = c * apk - s * aqk;
+          a[q][k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < 3; ++k) {
+          const double vkp = v[k][p], vkq = v[k][q];
+          v[k][p] = c * vkp - s * vkq;
+          v[k][q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  for (int i = 0; i < 3; ++i) w[i] = a[i][i];
+}
+
+int blocks_for(int64_t n) { return (int)((n + CS_THREADS - 1) / CS_THREADS); }
+
+}  // namespace
+
+bool coarse_build(SystemData& S, int target) {
+  CoarseSpace& C = S.coarse;
+  if (C.state && C.target == target) return C.state == 1;
+  C.state = 2;
+  C.target = target;
+  C.ready = false;
+  ++C.generation;
+  if (!S.mesh || S.nb.state != 1 || S.dpn < 1 || S.dpn > 3) return false;
+  cudaStream_t s = S.ctx->stream;
+  const MeshData& M = *S.mesh;
+  const int dpn = S.dpn, ng = S.nb.ngroups, nm = rigid_modes(dpn), cdim = M.cdim;
+  std::vector<int> fm(S.n_free);
+  std::vector<double> xyz((size_t)M.n_nodes * cdim);
+  S.free_map.download(fm.data(), fm.size());
+  M.coords.download(xyz.data(), xyz.size());
+  TPT_CUDA(cudaStreamSynchronize(s));
+  std::vector<double> pos((size_t)ng * 3, 0.0);
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int g = 0; g < ng; ++g) {
+    const int node = fm[(size_t)g * dpn] / dpn;
+    for (int d = 0; d < cdim && d < 3; ++d) {
+      const double x = xyz[(size_t)node * cdim + d];
+      pos[(size_t)g * 3 + d] = x;
+      lo[d] = std::min(lo[d], x);
+      hi[d] = std::max(hi[d], x);
+    }
+  }
+  double L[3], vol = 1.0;
+  int nact = 0;
+  for (int d = 0; d < 3; ++d) {
+    L[d] = d < cdim ? hi[d] - lo[d] : 0.0;
+    if (L[d] > 0) { vol *= L[d]; ++nact; }
+  }
+  if (nact == 0 || target < 1) return false;
+  double H = std::pow(vol / (double)target, 1.0 / nact);
+  std::vector<int> gbin((size_t)ng * 3), agg(ng), binid(ng);
+  std::vector<int> bin2agg;
+  int na = 0;
+  DevBuf<int> d_gbin, flag;
+  d_gbin.alloc((size_t)ng * 3, s);
+  flag.alloc(1, s);
+  bool ok = false;
+  for (int attempt = 0; attempt < 12 && !ok; ++attempt, H *= 1.25) {
+    for (int d = 0; d < 3; ++d) C.bins[d] = L[d] > 0 ? std::max(1, (int)std::floor(L[d] / H)) : 1;
+    const int64_t nbins = (int64_t)C.bins[0] * C.bins[1] * C.bins[2];
+    if (nbins > (1 << 24)) continue;
+    for (int g = 0; g < ng; ++g) {
+      int64_t b = 0;
+      for (int d = 2; d >= 0; --d) {
+        int k = 0;
+        if (L[d] > 0) k = std::min(C.bins[d] - 1, (int)std::floor((pos[(size_t)g * 3 + d] - lo[d]) / L[d] * C.bins[d]));
+        k = std::max(k, 0);
+        gbin[(size_t)g * 3 + d] = k;
+        b = b * C.bins[d] + k;
+      }
+      binid[g] = (int)b;
+    }
+    bin2agg.assign(nbins, -1);
+    for (int g = 0; g < ng; ++g) bin2agg[binid[g]] = 0;
+    na = 0;
+    for (auto& v : bin2agg)
+      if (v == 0) v = na++;
+    if ((int64_t)na * nm > CS_MAX_COARSE) continue;
+    for (int g = 0; g < ng; ++g) agg[g] = bin2agg[binid[g]];
+    d_gbin.upload(gbin.data(), gbin.size());
+    flag.zero();
+    cs_check_adjacency<<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, S.nb.gptr.p, S.nb.glist.p, d_gbin.p, flag.p);
+    TPT_CHECK_LAUNCH();
+    int f = 0;
+    flag.download(&f, 1);
+    TPT_CUDA(cudaStreamSynchronize(s));
+    ok = f == 0;
+  }
+  if (!ok) return false;
+  // aggregate lists, centroids, relative positions, orthonormal mode transforms
+  std::vector<int> aptr(na + 1, 0), alist(ng), abin((size_t)na * 3);
+  for (int g = 0; g < ng; ++g) aptr[agg[g] + 1]++;
+  for (int i = 0; i < na; ++i) aptr[i + 1] += aptr[i];
+  {
+    std::vector<int> fill(aptr.begin(), aptr.end() - 1);
+    for (int g = 0; g < ng; ++g) alist[fill[agg[g]]++] = g;
+  }
+  std::vector<double> cen((size_t)na * 3, 0.0);
+  for (int g = 0; g < ng; ++g)
+    for (int d = 0; d < 3; ++d) cen[(size_t)agg[g] * 3 + d] += pos[(size_t)g * 3 + d];
+  for (int i = 0; i < na; ++i) {
+    const double cnt = aptr[i + 1] - aptr[i];
+    for (int d = 0; d < 3; ++d) cen[(size_t)i * 3 + d] /= cnt;
+    const int g0 = alist[aptr[i]];
+    for (int d = 0; d < 3; ++d) abin[(size_t)i * 3 + d] = gbin[(size_t)g0 * 3 + d];
+  }
+  std::vector<float> yrel((size_t)ng * 3);
+  std::vector<double> inert((size_t)na * 9, 0.0);
+  for (int g = 0; g < ng; ++g) {
+    const int I = agg[g];
+    double yv[3];
+    for (int d = 0; d < 3; ++d) yv[d] = pos[(size_t)g * 3 + d] - cen[(size_t)I * 3 + d];
+    for (int d = 0; d < 3; ++d) yrel[(size_t)g * 3 + d] = (float)yv[d];
+    const double y2 = yv[0] * yv[0] + yv[1] * yv[1] + yv[2] * yv[2];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) inert[(size_t)I * 9 + a * 3 + b] += (a == b ? y2 : 0.0) - yv[a] * yv[b];
+  }
+  std::vector<double> T((size_t)na * nm * nm, 0.0);
+  for (int i = 0; i < na; ++i) {
+    double* t = T.data() + (size_t)i * nm * nm;
+    const double cnt = aptr[i + 1] - aptr[i];
+    const int ntr = dpn;  // translations
+    for (int k = 0; k < ntr; ++k) t[k * nm + k] = 1.0 / std::sqrt(cnt);
+    if (dpn == 2) {
+      const double iz = inert[(size_t)i * 9 + 8];  // sum of |y|^2 in the plane
+      if (iz > 1e-12 * cnt * H * H) t[2 * nm + 2] = 1.0 / std::sqrt(iz);
+    } else if (dpn == 3) {
+      double a[3][3], w[3], v[3][3];
+      for (int p = 0; p < 3; ++p)
+        for (int q = 0; q < 3; ++q) a[p][q] = inert[(size_t)i * 9 + p * 3 + q];
+      sym_eig3(a, w, v);
+      const double wmax = std::max(w[0], std::max(w[1], w[2]));
+      for (int q = 0; q < 3; ++q) {
+        if (!(w[q] > 1e-9 * wmax) || !(wmax > 1e-12 * cnt * H * H)) continue;
+        const double sc = 1.0 / std::sqrt(w[q]);
+        for (int p = 0; p < 3; ++p) t[(3 + p) * nm + 3 + q] = v[p][q] * sc;
+      }
+    }
+  }
+  // segments of at most CS_SEG groups per aggregate (restriction work items)
+  constexpr int CS_SEG = 1024;
+  std::vector<int> sb, se, aseg(na + 1, 0);
+  for (int i = 0; i < na; ++i) {
+    for (int t = aptr[i]; t < aptr[i + 1]; t += CS_SEG) {
+      sb.push_back(t);
+      se.push_back(std::min(aptr[i + 1], t + CS_SEG));
+    }
+    aseg[i + 1] = (int)sb.size();
+  }
+  C.nseg = (int)sb.size();
+  C.sbeg.alloc(C.nseg, s); C.sbeg.upload(sb.data(), C.nseg);
+  C.send.alloc(C.nseg, s); C.send.upload(se.data(), C.nseg);
+  C.aseg.alloc(na + 1, s); C.aseg.upload(aseg.data(), na + 1);
+  C.smom.alloc((size_t)C.nseg * nm, s);
+  C.na = na;
+  C.nm = nm;
+  C.nc = na * nm;
+  C.agg.alloc(ng, s); C.agg.upload(agg.data(), ng);
+  C.aptr.alloc(na + 1, s); C.aptr.upload(aptr.data(), na + 1);
+  C.alist.alloc(ng, s); C.alist.upload(alist.data(), ng);
+  C.abin.alloc((size_t)na * 3, s); C.abin.upload(abin.data(), abin.size());
+  C.bin2agg.alloc(bin2agg.size(), s); C.bin2agg.upload(bin2agg.data(), bin2agg.size());
+  C.y.alloc((size_t)ng * 3, s); C.y.upload(yrel.data(), yrel.size());
+  C.T.alloc(T.size(), s); C.T.upload(T.data(), T.size());
+  TPT_CUDA(cudaFuncSetAttribute(cs_gemv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(CS_MAX_COARSE * sizeof(double))));
+  C.Ac.alloc((size_t)C.nc * C.nc, s);
+  C.Ainv.alloc((size_t)C.nc * C.nc, s);
+  C.yc.alloc(C.nc, s);
+  C.uc.alloc(C.nc, s);
+  TPT_CUDA(cudaStreamSynchronize(s));  // host vectors above are released on return
+  C.state = 1;
+  return true;
+}
+
+bool coarse_assemble(SystemData& S) {
+  CoarseSpace& C = S.coarse;
+  C.ready = false;
+  if (C.state != 1) return false;
+  cudaStream_t s = S.ctx->stream;
+  const int ng = S.nb.ngroups, dpn = S.dpn, nc = C.nc;
+  C.Ac.zero();
+  DevBuf<double> v, w;
+  v.alloc(S.n_free, s);
+  w.alloc(S.n_free, s);
+  const int ncx = std::min(3, C.bins[0]), ncy = std::min(3, C.bins[1]), ncz = std::min(3, C.bins[2]);
+  for (int cz = 0; cz < ncz; ++cz)
+    for (int cy = 0; cy < ncy; ++cy)
+      for (int cx = 0; cx < ncx; ++cx) {
+        const int colour = cx + 3 * cy + 9 * cz;
+        for (int m = 0; m < C.nm; ++m) {
+#define TPT_CS_COL(D)                                                                                             \
+  cs_fill<D><<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, C.agg.p, C.abin.p, C.y.p, C.T.p, colour, m, v.p);           \
+  TPT_CHECK_LAUNCH();                                                                                             \
+  nb_operator_apply(S, v.p, w.p);                                                                                 \
+  cs_moments<D><<<C.nseg, CS_THREADS, 0, s>>>(C.sbeg.p, C.send.p, C.alist.p, C.y.p, w.p, C.smom.p);              \
+  TPT_CHECK_LAUNCH();                                                                                             \
+  cs_columns<<<blocks_for(C.na), CS_THREADS, 0, s>>>(C.na, C.nm, C.abin.p, C.bin2agg.p, C.bins[0], C.bins[1],       \
+                                                     C.bins[2], C.aseg.p, C.smom.p, C.T.p, colour, m, C.Ac.p, nc); \
+  TPT_CHECK_LAUNCH();
+          if (dpn == 3) { TPT_CS_COL(3) }
+          else if (dpn == 2) { TPT_CS_COL(2) }
+          else { TPT_CS_COL(1) }
+#undef TPT_CS_COL
+        }
+      }
+  cs_fix_diag<<<blocks_for(nc), CS_THREADS, 0, s>>>(nc, C.Ac.p);
+  TPT_CHECK_LAUNCH();
+  // Cholesky and inverse (symmetric: row-major storage = column-major storage)
+  cusolverDnHandle_t h = (cusolverDnHandle_t)S.ctx->cusolver;
+  if (!h) {
+    TPT_REQUIRE(cusolverDnCreate(&h) == CUSOLVER_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "cusolverDnCreate failed");
+    S.ctx->cusolver = h;
+  }
+  TPT_REQUIRE(cusolverDnSetStream(h, s) == CUSOLVER_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "cusolverDnSetStream failed");
+  int lw1 = 0, lw2 = 0;
+  TPT_REQUIRE(cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, nc, C.Ac.p, nc, &lw1) == CUSOLVER_STATUS_SUCCESS,
+              TPTFEM_ERR_DEVICE, "dpotrf_bufferSize failed");
+  TPT_REQUIRE(cusolverDnDpotri_bufferSize(h, CUBLAS_FILL_MODE_LOWER, nc, C.Ac.p, nc, &lw2) == CUSOLVER_STATUS_SUCCESS,
+              TPTFEM_ERR_DEVICE, "dpotri_bufferSize failed");
+  DevBuf<double> work;
+  work.alloc(std::max(1, std::max(lw1, lw2)), s);
+  DevBuf<int> info;
+  info.alloc(1, s);
+  int hinfo = 0;
+  TPT_REQUIRE(cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, nc, C.Ac.p, nc, work.p, lw1, info.p) ==
+                  CUSOLVER_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "dpotrf failed");
+  info.download(&hinfo, 1);
+  TPT_CUDA(cudaStreamSynchronize(s));
+  if (hinfo != 0) return false;  // coarse matrix not positive definite in FP64
+  TPT_REQUIRE(cusolverDnDpotri(h, CUBLAS_FILL_MODE_LOWER, nc, C.Ac.p, nc, work.p, lw2, info.p) ==
+                  CUSOLVER_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "dpotri failed");
+  info.download(&hinfo, 1);
+  TPT_CUDA(cudaStreamSynchronize(s));
+  if (hinfo != 0) return false;
+  cs_symmetrize<<<blocks_for((int64_t)nc * nc), CS_THREADS, 0, s>>>(nc, C.Ac.p, C.Ainv.p);
+  TPT_CHECK_LAUNCH();
+  C.ready = true;
+  return true;
+}
+
+void coarse_restrict_solve(const SystemData& S, const double* r, cudaStream_t s) {
+  const CoarseSpace& C = S.coarse;
+#define TPT_CS_R(D)                                                                                     \
+  cs_moments<D><<<C.nseg, CS_THREADS, 0, s>>>(C.sbeg.p, C.send.p, C.alist.p, C.y.p, r, C.smom.p); \
+  TPT_CHECK_LAUNCH();
+  if (S.dpn == 3) { TPT_CS_R(3) }
+  else if (S.dpn == 2) { TPT_CS_R(2) }
+  else { TPT_CS_R(1) }
+#undef TPT_CS_R
+  cs_yc<<<blocks_for(C.nc), CS_THREADS, 0, s>>>(C.na, C.nm, C.aseg.p, C.smom.p, C.T.p, C.yc.p);
+  TPT_CHECK_LAUNCH();
+  cs_gemv<<<(C.nc + CS_THREADS / 32 - 1) / (CS_THREADS / 32), CS_THREADS, (size_t)C.nc * sizeof(double), s>>>(
+      C.nc, C.yc.p, C.Ainv.p, C.uc.p);
+  TPT_CHECK_LAUNCH();
+}
+
+void coarse_download(const SystemData& S, int* na, int* nm, double* Ainv_out) {
+  const CoarseSpace& C = S.coarse;
+  if (na) *na = C.na;
+  if (nm) *nm = C.nm;
+  if (Ainv_out && C.ready) {  // the FP32 inverse of A_c, widened
+    std::vector<float> f((size_t)C.nc * C.nc);
+    C.Ainv.download(f.data(), f.size());
+    TPT_CUDA(cudaStreamSynchronize(S.ctx->stream));
+    for (size_t i = 0; i < f.size(); ++i) Ainv_out[i] = f[i];
+  }
+}
+
+}  // namespace tptfem

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_fp16.h>
 
+#include "modes.cuh"
 #include "solver_kernels.cuh"
 
 namespace tptfem {
@@ -209,7 +210,8 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_fsai_lower(int ngroups, const
   }
 }
 
-// z = t + L^T t (transposed packed FP16 blocks) and rz = r.z into st->rz[par ^ 1].
+// z = t + L^T t (transposed packed FP16 blocks) [+ P uc, the coarse
+// correction, when cs.agg is set] and rz = r.z into st->rz[par ^ 1].
 template <int DPN>
 __global__ void __launch_bounds__(SPMV_THREADS) nb_fsai_upper_rz(int ngroups, const int* __restrict__ cptr,
                                                                  const int* __restrict__ bcol,
@@ -219,7 +221,7 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_fsai_upper_rz(int ngroups, co
                                                                  const double* __restrict__ t,
                                                                  const double* __restrict__ r,
                                                                  double* __restrict__ z, PcgState* st,
-                                                                 double* partials, int par) {
+                                                                 double* partials, int par, CoarseArgs cs) {
   if (st->done) return;
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -252,6 +254,26 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_fsai_upper_rz(int ngroups, co
       for (int a = 0; a < DPN; ++a)
 #pragma unroll
         for (int b = 0; b < DPN; ++b) acc[a] += (double)v[a * DPN + b] * xj[b];
+    }
+    if (cs.agg) {  // z_g += R_g T_I uc_I
+      constexpr int NM = rigid_modes(DPN);
+      const int I = cs.agg[g];
+      const double* tI = cs.T + (int64_t)I * NM * NM;
+      const double* uI = cs.uc + (int64_t)I * NM;
+      double cm[NM];
+#pragma unroll
+      for (int k = 0; k < NM; ++k) {
+        double x = 0.0;
+#pragma unroll
+        for (int m = 0; m < NM; ++m) x += tI[k * NM + m] * uI[m];
+        cm[k] = x;
+      }
+      double R[DPN][NM];
+      mode_rows<DPN>(cs.y + 3 * (int64_t)g, R);
+#pragma unroll
+      for (int a = 0; a < DPN; ++a)
+#pragma unroll
+        for (int k = 0; k < NM; ++k) acc[a] += R[a][k] * cm[k];
     }
 #pragma unroll
     for (int a = 0; a < DPN; ++a) {

@@ -12,6 +12,7 @@ struct tptfem_context {
   cudaStream_t stream = nullptr;
   std::string err;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  void* cusolver = nullptr;  // cusolverDnHandle_t, created on first use
   int* d_flag = nullptr;  // device error/validation flag scratch (one int)
   int* h_pinned = nullptr;  // pinned staging (64 bytes)
   std::map<uint64_t, int> topo_tuned;  // topopt autotuner: batch shape -> threads per instance
@@ -92,9 +93,39 @@ struct NbSell {
   DevBuf<int> ku_base;
 };
 
+// Aggregation coarse space of a node-block system (coarse.cu): free mesh
+// nodes binned by coordinates into boxes (aggregates); per aggregate the
+// rigid-body modes (DPN 3: 3 translations + 3 rotations; DPN 2: 2 + 1;
+// DPN 1: the constant), orthonormalised; P = block diagonal of those modes;
+// A_c = P^T A P and its inverse (FP32) for the additive correction
+// z += P A_c^-1 P^T r.
+struct CoarseSpace {
+  int state = 0;  // 0 not tried, 1 geometry built, 2 not applicable
+  int target = 0;               // requested aggregate count the geometry was built for
+  int generation = 0;           // incremented by every (re)build: engines refresh their pointers
+  int na = 0, nm = 0, nc = 0;   // aggregates, modes per aggregate, coarse size
+  int nseg = 0;                 // segments of aggregate group lists (restriction work items)
+  DevBuf<int> sbeg, send;       // per segment: range in alist
+  DevBuf<int> aseg;             // aggregate -> its segments (na + 1)
+  DevBuf<double> smom;          // per segment: raw mode moments (nseg x nm)
+  int bins[3] = {1, 1, 1};
+  DevBuf<int> agg;              // per group: aggregate
+  DevBuf<int> aptr, alist;      // aggregate -> its groups, ascending
+  DevBuf<int> abin;             // per aggregate: bin coordinates (x, y, z)
+  DevBuf<int> bin2agg;          // per bin: aggregate or -1
+  DevBuf<float> y;              // per group: node position minus the aggregate centroid
+  DevBuf<double> T;             // per aggregate: nm x nm mode transform (columns orthonormal modes)
+  DevBuf<double> Ac;            // nc x nc, then its Cholesky factor / inverse (FP64)
+  DevBuf<float> Ainv;           // nc x nc inverse (FP32, symmetric, row-major)
+  DevBuf<double> yc, uc;        // coarse vectors
+  bool ready = false;           // Ainv holds the inverse for the current values
+};
+
 struct SystemData {
   tptfem_context* ctx = nullptr;
   NbSell nb;
+  CoarseSpace coarse;
+  std::shared_ptr<MeshData> mesh;  // geometry of the matrix the system was reduced from
   int64_t n = 0, n_free = 0, nnz = 0;
   int dpn = 1;            // dofs per mesh node of the full system
   DevBuf<int> free_map;   // reduced -> full
@@ -140,6 +171,14 @@ bool fsai_set_values(const SystemData& S, FsaiFactor& F, const double* d_sig2, c
 bool nb_build_operator(SystemData& S);  // false when the system has partial node groups
 bool nb_fill_factor(SystemData& S, const FsaiFactor& F);  // false: factor rows not node-block shaped
 void nb_build_sym(SystemData& S);  // after nb_build_operator succeeded
+
+// coarse.cu
+bool coarse_build(SystemData& S, int target_aggregates);  // geometry (once); false: not applicable
+bool coarse_assemble(SystemData& S);                      // A_c and its inverse for the current values
+void coarse_restrict_solve(const SystemData& S, const double* r, cudaStream_t s);  // uc = A_c^-1 P^T r
+void coarse_download(const SystemData& S, int* na, int* nm, double* Ainv_or_null);  // FP32 inverse, widened
+// solver.cu: y = A x with the system's node-block operator (no reduction)
+void nb_operator_apply(SystemData& S, const double* x, double* y);
 
 // solver.cu
 int64_t system_fsai_classic(SystemData& S);  // builds (once) the classic factor; -1 on failure

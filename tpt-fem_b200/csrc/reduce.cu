@@ -116,6 +116,7 @@ std::unique_ptr<SystemData> reduce_system(tptfem_context* ctx, const MatrixData&
   S->ctx = ctx;
   S->n = n;
   S->dpn = A.dpn;
+  S->mesh = A.mesh;
   DevBuf<int> dof, first, last, red, cnt;
   DevBuf<double> val;
   dof.alloc(nbc, s);

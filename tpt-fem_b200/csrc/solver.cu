@@ -112,6 +112,10 @@ struct Engine {
   const NbSell* nb = nullptr;
   bool nb_op = false, nb_pc = false, nb_sym = false;
   int nb_grid = 1;
+  // aggregation coarse correction (node-block FSAI engines only)
+  const SystemData* csys = nullptr;
+  int cgen = -1;  // coarse-space generation the pointers in cargs belong to
+  CoarseArgs cargs;
   ~Engine() {
     if (exec) cudaGraphExecDestroy(exec);
   }
@@ -183,8 +187,9 @@ struct Engine {
   nb_fsai_lower<D><<<nb_grid, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.l_pack.p, N.l_tail.p,     \
                                                     N.l_diag.p, pc.sigma2, r.p, t.p, st.p);                       \
   TPT_CHECK_LAUNCH();                                                                                            \
+  if (csys) coarse_restrict_solve(*csys, r.p, s);                                                                \
   nb_fsai_upper_rz<D><<<nb_grid, SPMV_THREADS, 0, s>>>(N.ngroups, N.u_cptr.p, N.u_col.p, N.u_pack.p, N.u_tail.p,  \
-                                                       N.l_diag.p, t.p, r.p, z.p, st.p, partials.p, par);         \
+                                                       N.l_diag.p, t.p, r.p, z.p, st.p, partials.p, par, cargs);  \
   TPT_CHECK_LAUNCH();
         if (N.dpn == 3) { TPT_NB_FSAI(3) }
         else if (N.dpn == 2) { TPT_NB_FSAI(2) }
@@ -282,6 +287,30 @@ void select_nb_mode(SystemData& S, Engine<double>& E, const tptfem_solver_opts& 
     E.nb_sym = sym;
     if (E.exec) { cudaGraphExecDestroy(E.exec); E.exec = nullptr; }
   }
+}
+
+// Coarse correction for an FSAI engine (TPTFEM_SOLVE_COARSE): geometry once
+// per system, A_c and its inverse whenever the preconditioner is set up
+// afresh.  Returns the coarse size in use (0: off).
+int select_coarse(SystemData& S, Engine<double>& E, const tptfem_solver_opts& o, bool fresh) {
+  bool want = (o.flags & TPTFEM_SOLVE_COARSE) && E.nb_pc;
+  if (want) want = coarse_build(S, o.coarse_aggregates > 0 ? o.coarse_aggregates : 500);
+  if (want && (fresh || !S.coarse.ready)) want = coarse_assemble(S);
+  if (want && !S.coarse.ready) want = false;
+  const SystemData* target = want ? &S : nullptr;
+  if (E.csys != target || (want && E.cgen != S.coarse.generation)) {
+    E.csys = target;
+    E.cgen = S.coarse.generation;
+    E.cargs = CoarseArgs{};
+    if (want) {
+      E.cargs.agg = S.coarse.agg.p;
+      E.cargs.y = S.coarse.y.p;
+      E.cargs.T = S.coarse.T.p;
+      E.cargs.uc = S.coarse.uc.p;
+    }
+    if (E.exec) { cudaGraphExecDestroy(E.exec); E.exec = nullptr; }
+  }
+  return want ? S.coarse.nc : 0;
 }
 
 void flag_check(tptfem_context* ctx, const char* msg) {
@@ -480,6 +509,8 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
         W.nb_factor = &W.lf;
       }
       st.solver_used = solver;
+      select_nb_mode(S, W.f64_lf, o);
+      st.coarse_size = select_coarse(S, W.f64_lf, o, fresh);
       TPT_CUDA(cudaEventRecord(ctx->ev[1], s));
       const double bb = norm2_b(S);
       const double bnorm = std::sqrt(bb);
@@ -489,7 +520,6 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
         S.x.zero();
       } else {
         const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : 1e-3;
-        select_nb_mode(S, W.f64_lf, o);
         try {
           iters = run_reliable<double>(S, W.f64_lf, tol, delta, max_it, bnorm, st);
         } catch (const Error& e) {
@@ -578,6 +608,10 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
     W.f32_ready = true;
   }
   st.solver_used = solver;
+  if (solver == TPTFEM_SOLVER_FSAI_MP_PCG) {
+    select_nb_mode(S, W.f64_fsai, o);
+    st.coarse_size = select_coarse(S, W.f64_fsai, o, (o.flags & TPTFEM_SOLVE_FRESH_SETUP) != 0);
+  }
   TPT_CUDA(cudaEventRecord(ctx->ev[1], s));
   const double bb = norm2_b(S);
   const double bnorm = std::sqrt(bb);
@@ -594,7 +628,6 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
     iters = run_reliable<float>(S, W.f32, tol, delta, max_it, bnorm, st);
   } else {
     const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : 1e-3;
-    select_nb_mode(S, W.f64_fsai, o);
     iters = run_reliable<double>(S, W.f64_fsai, tol, delta, max_it, bnorm, st);
   }
   const double rel = bb == 0.0 ? 0.0 : std::sqrt(true_residual2(S, S.x.p)) / bnorm;
@@ -727,6 +760,26 @@ void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32
     *nbs_bytes = (double)N.l_slots * 32 * (4 + 8 * d2) + (double)N.nchunks * 32 * 8 * d2 +
                  (double)N.u_slots * 32 * 8 + 2.0 * (N.nchunks + 1) * 4 + 16.0 * (double)S.n_free;
   }
+}
+
+void nb_operator_apply(SystemData& S, const double* x, double* y) {
+  const NbSell& N = S.nb;
+  cudaStream_t s = S.ctx->stream;
+  const int g = std::max(1, std::min(sm_count() * NB_BLOCKS_PER_SM, ceil_div((int64_t)N.nchunks * 32, SPMV_THREADS)));
+  if (N.sym_built) {
+#define TPT_NB_SYM(D)                                                                                             \
+  nb_spmv_sym<D, false><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.ks_lval.p, N.ks_diag.p,     \
+                                                   N.u_cptr.p, N.u_col.p, N.ku_base.p, x, y, nullptr, nullptr, false);
+    if (N.dpn == 3) { TPT_NB_SYM(3) }
+    else if (N.dpn == 2) { TPT_NB_SYM(2) }
+    else { TPT_NB_SYM(1) }
+#undef TPT_NB_SYM
+  } else {
+    if (N.dpn == 3) nb_spmv<3, false><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.k_cptr.p, N.k_col.p, N.k_val.p, x, y, nullptr, nullptr, false);
+    else if (N.dpn == 2) nb_spmv<2, false><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.k_cptr.p, N.k_col.p, N.k_val.p, x, y, nullptr, nullptr, false);
+    else nb_spmv<1, false><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.k_cptr.p, N.k_col.p, N.k_val.p, x, y, nullptr, nullptr, false);
+  }
+  TPT_CHECK_LAUNCH();
 }
 
 void csr_matvec_f64(tptfem_context* ctx, int64_t nrows, const int* rp, const int* ci, const double* va,

@@ -289,12 +289,13 @@ def _bcs(bcs):
 
 
 def _opts(solver=SOLVER_JACOBI_PCG, tol=1e-10, inner_tol=0.0, max_iter=0, max_outer=0, batch=0, fresh_setup=False,
-          csr_only=False, full_operator=False):
+          csr_only=False, full_operator=False, coarse=False, coarse_aggregates=0):
     o = SolverOpts()
     o.solver, o.rel_tol, o.inner_rel_tol, o.max_iter, o.max_outer, o.batch = solver, tol, inner_tol, max_iter, \
         max_outer, batch
     o.flags = (N.SOLVE_FRESH_SETUP if fresh_setup else 0) | (N.SOLVE_CSR_ONLY if csr_only else 0) | \
-        (N.SOLVE_FULL_OPERATOR if full_operator else 0)
+        (N.SOLVE_FULL_OPERATOR if full_operator else 0) | (N.SOLVE_COARSE if coarse else 0)
+    o.coarse_aggregates = coarse_aggregates
     return o
 
 
@@ -324,6 +325,21 @@ class System:
         rc = self.ctx.lib.tptfem_system_solve(self.ctx.h, self.h, C.byref(o), C.byref(st))
         self.ctx.check(rc)
         return st.as_dict()
+
+    def coarse(self, with_inverse=False):
+        """The coarse space of the last coarse solve: dict(na, nm, bins[, ainv])."""
+        na, nm = C.c_int32(), C.c_int32()
+        bins = np.zeros(3, np.int32)
+        self.ctx.check(self.ctx.lib.tptfem_system_coarse(self.ctx.h, self.h, C.byref(na), C.byref(nm), N.ptr(bins),
+                                                         None))
+        out = {"na": na.value, "nm": nm.value, "bins": bins.tolist()}
+        if with_inverse and na.value:
+            nc = na.value * nm.value
+            a = np.zeros((nc, nc))
+            self.ctx.check(self.ctx.lib.tptfem_system_coarse(self.ctx.h, self.h, C.byref(na), C.byref(nm),
+                                                             N.ptr(bins), N.ptr(a)))
+            out["ainv"] = a
+        return out
 
     def profile_spmv(self, reps=20):
         """Average device ms of the solver's SpMV kernels as a dict: FP64 CSR, FP32 CSR, FP64 node-block

@@ -24,21 +24,22 @@ SOLVER_JACOBI_PCG, SOLVER_MP_PCG, SOLVER_FSAI_MP_PCG, SOLVER_LEARNED_FSAI_PCG = 
 SOLVE_FRESH_SETUP = 1
 SOLVE_CSR_ONLY = 2
 SOLVE_FULL_OPERATOR = 4
+SOLVE_COARSE = 8
 
 
 class SolverOpts(C.Structure):
     _fields_ = [("solver", C.c_int32), ("max_outer", C.c_int32), ("rel_tol", C.c_double),
                 ("inner_rel_tol", C.c_double), ("max_iter", C.c_int64), ("batch", C.c_int32),
-                ("flags", C.c_int32)]
+                ("flags", C.c_int32), ("coarse_aggregates", C.c_int32), ("reserved", C.c_int32)]
 
 
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int64), ("outer_steps", C.c_int32), ("solver_used", C.c_int32),
                 ("rel_residual", C.c_double), ("setup_ms", C.c_double), ("solve_ms", C.c_double),
-                ("fell_back", C.c_int32), ("reserved", C.c_int32)]
+                ("fell_back", C.c_int32), ("coarse_size", C.c_int32)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class TopoptInstance(C.Structure):
@@ -70,6 +71,8 @@ _pd = C.POINTER(C.c_double)
 _pint = C.POINTER(C.c_int)
 
 SIGNATURES = {
+    "tptfem_system_coarse": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                       C.c_void_p, C.c_void_p]),
     "tptfem_topopt_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p]),
     "tptfem_topopt_element_stiffness": (C.c_int, [C.c_double, C.c_double, C.c_void_p]),
