@@ -5,8 +5,11 @@ from a seeded smoothed density; nu = 0.3; x = 0 clamped; traction (0,0,-1e-3)
 on x = 4).  Inputs are synthetic (seeded), no dataset exists for this path.
 
 A step is one complete solve from x = 0 of the device-resident reduced system
-with the learned-FSAI preconditioner (network forward on this system, factor
-conversion, FP64 PCG), set-up included, stopping on the TRUE FP64 residual.  `value`
+with the two-level learned preconditioner -- learned FSAI factor (network
+forward on this system, FP16 factor) plus the rigid-body aggregation coarse
+space (A_c = P^T A P assembled and inverted on this system) -- and FP64 PCG,
+set-up included, stopping on the TRUE FP64 residual.  --no-coarse times the
+single-level learned FSAI instead.  `value`
 is the median device time of a step (CUDA events on the library's stream);
 `e2e` runs the same solve through the C ABI from host arrays (mesh upload,
 assembly, traction, Dirichlet reduction, learned factor, solve, solution
@@ -193,7 +196,7 @@ def build_system(F, W, ctx, mesh_cells=None):
 WEIGHTS = os.path.join(ROOT, "tpt-fem_b200", "weights", "lfsai_elasticity.bin")
 
 
-def e2e_once(F, LF, W, ctx, solver, host, model):
+def e2e_once(F, LF, W, ctx, solver, host, model, coarse):
     """Host arrays -> C ABI -> host solution; returns (seconds, h2d bytes, d2h bytes, stats).
     Mesh upload, assembly, traction, Dirichlet reduction, the learned factor and
     the solve all run inside the timed region."""
@@ -206,7 +209,7 @@ def e2e_once(F, LF, W, ctx, solver, host, model):
     S = F.reduce_system(K, rhs, list(zip(dof, val)))
     if solver == F.SOLVER_LEARNED_FSAI_PCG:
         model.attach(S)
-    st = S.solve(solver=solver, tol=TOL, fresh_setup=True)
+    st = S.solve(solver=solver, tol=TOL, fresh_setup=True, coarse=coarse)
     u = S.solution()
     ctx.synchronize()
     dt = time.perf_counter() - t0
@@ -229,9 +232,10 @@ def run_ours(args, world, rank, local):
     model.attach(S)
     solver = {"learned": F.SOLVER_LEARNED_FSAI_PCG, "fsai": F.SOLVER_FSAI_MP_PCG, "jacobi": F.SOLVER_JACOBI_PCG,
               "mp": F.SOLVER_MP_PCG}[args.solver]
+    coarse = not args.no_coarse and solver in (F.SOLVER_LEARNED_FSAI_PCG, F.SOLVER_FSAI_MP_PCG)
     if args.profile:  # kernels of the timed steps only (for an ncu launch list)
         for _ in range(args.steps):
-            S.solve(solver=solver, tol=TOL, fresh_setup=True)
+            S.solve(solver=solver, tol=TOL, fresh_setup=True, coarse=coarse)
         ctx.synchronize()
         return None
     # The plain method the metric compares against: FP64 Jacobi-PCG with the
@@ -242,15 +246,19 @@ def run_ours(args, world, rank, local):
     jac_nb = S.solve(solver=F.SOLVER_JACOBI_PCG, tol=TOL, fresh_setup=True)
     S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=TOL, fresh_setup=True)
     fsai = S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=TOL, fresh_setup=True)
+    S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=TOL, fresh_setup=True, coarse=True)  # builds the coarse geometry
+    fsai2 = S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=TOL, fresh_setup=True, coarse=True)
+    lrn1 = S.solve(solver=F.SOLVER_LEARNED_FSAI_PCG, tol=TOL, fresh_setup=True)
+    lrn1 = S.solve(solver=F.SOLVER_LEARNED_FSAI_PCG, tol=TOL, fresh_setup=True)
     for _ in range(args.warmup):
-        S.solve(solver=solver, tol=TOL, fresh_setup=True)
+        S.solve(solver=solver, tol=TOL, fresh_setup=True, coarse=coarse)
     barrier(world)
     cuda_sync()
     steps = []
     with ClockSampler(local) as clk:
         t_wall = time.perf_counter()
         for _ in range(args.steps):
-            steps.append(S.solve(solver=solver, tol=TOL, fresh_setup=True))
+            steps.append(S.solve(solver=solver, tol=TOL, fresh_setup=True, coarse=coarse))
         cuda_sync()
         t_wall = time.perf_counter() - t_wall
     barrier(world)
@@ -274,15 +282,15 @@ def run_ours(args, world, rank, local):
     if rank == 0:
         coords = mesh.coords_array.copy()
         conn = mesh.conn_array.copy()
-        e2e = [e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model) for _ in range(2)]
+        e2e = [e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model, coarse) for _ in range(2)]
         e2e_s, h2d, d2h, e2e_st = min(e2e, key=lambda t: t[0])
         cpu = CpuSample()
         cpu_it_s, cpu_nnz, cpu_threads = cpu.seconds_per_iteration(), cpu.nnz, cpu.threads
         cpu_val = cpu_it_s * (nnz / cpu_nnz) * jac["iterations"]
         its = [st["iterations"] for st in steps]
         fsai_like = solver in (F.SOLVER_FSAI_MP_PCG, F.SOLVER_LEARNED_FSAI_PCG)
-        kernels_per_it = 5 if fsai_like else 3
-        setup_kernels = 40 if solver == F.SOLVER_LEARNED_FSAI_PCG else 12
+        kernels_per_it = (5 if fsai_like else 3) + (3 if coarse else 0)
+        setup_kernels = (40 if solver == F.SOLVER_LEARNED_FSAI_PCG else 12) + (4 * 27 + 8 if coarse else 0)
         launches = sum(st["iterations"] * kernels_per_it + st["outer_steps"] * 6 + setup_kernels for st in steps)
         out = {
             "metric": METRIC, "value": step_s, "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -291,11 +299,16 @@ def run_ours(args, world, rank, local):
             "data": "synthetic (seeded density field)",
             "config": {"workload": WORKLOAD, "mesh": [280, 70, 70], "nodes": int(mesh.n_nodes),
                        "tets": int(mesh.n_elems), "free_dofs": int(n), "nnz_reduced": int(nnz),
-                       "solver": args.solver, "weights": os.path.relpath(WEIGHTS, ROOT), "tol": TOL,
+                       "solver": args.solver + ("+coarse" if coarse else ""),
+                       "preconditioner": ("learned FSAI (FP16 factor) + " if solver == F.SOLVER_LEARNED_FSAI_PCG
+                                          else "FSAI + ") + ("rigid-body aggregation coarse space (FP32 inverse)"
+                                                             if coarse else "single level"),
+                       "weights": os.path.relpath(WEIGHTS, ROOT), "tol": TOL,
                        "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (matrix 1.85 GB)"},
             "solver_stats": {"iterations_median": statistics.median(its), "rel_residual": steps[-1]["rel_residual"],
                              "setup_ms": steps[-1]["setup_ms"], "solve_ms": steps[-1]["solve_ms"],
                              "reliable_updates": steps[-1]["outer_steps"], "fell_back": steps[-1]["fell_back"],
+                             "coarse_size": steps[-1]["coarse_size"],
                              "step_s": [round(seconds(st), 4) for st in steps],
                              "setup_ms_steps": [round(st["setup_ms"], 2) for st in steps]},
             "fp64_jacobi_pcg": {"seconds": seconds(jac), "iterations": jac["iterations"],
@@ -304,6 +317,10 @@ def run_ours(args, world, rank, local):
                                            "rel_residual": jac_nb["rel_residual"]},
             "classic_fsai_pcg": {"seconds": seconds(fsai), "iterations": fsai["iterations"],
                                  "rel_residual": fsai["rel_residual"]},
+            "classic_fsai_coarse_pcg": {"seconds": seconds(fsai2), "iterations": fsai2["iterations"],
+                                        "rel_residual": fsai2["rel_residual"], "coarse_size": fsai2["coarse_size"]},
+            "learned_fsai_single_level": {"seconds": seconds(lrn1), "iterations": lrn1["iterations"],
+                                          "rel_residual": lrn1["rel_residual"]},
             "speedup_vs_fp64_jacobi": seconds(jac) / step_s,
             "speedup_vs_fp64_jacobi_node_block": seconds(jac_nb) / step_s,
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
@@ -357,6 +374,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--solver", default="learned", choices=["learned", "fsai", "jacobi", "mp"])
     ap.add_argument("--profile", action="store_true", help="run only the timed solves (ncu launch list)")
+    ap.add_argument("--no-coarse", action="store_true", help="single-level preconditioner (no coarse space)")
     ap.add_argument("--mesh", type=int, nargs=3, default=None,
                     help="with --profile: cantilever cells (a smaller case for ncu captures)")
     args = ap.parse_args()

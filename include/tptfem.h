@@ -92,7 +92,8 @@ typedef struct tptfem_solver_opts {
   int64_t max_iter;      /* cap on total PCG iterations (0 -> 100000) */
   int32_t batch;         /* PCG iterations per CUDA-graph launch (0 -> auto) */
   int32_t flags;         /* TPTFEM_SOLVE_* bits */
-  int32_t coarse_aggregates;  /* TPTFEM_SOLVE_COARSE: target number of aggregates (0 -> 500) */
+  int32_t coarse_aggregates;  /* TPTFEM_SOLVE_COARSE: target number of aggregates
+                                 (0 -> node groups / 2800, between 8 and 1000) */
   int32_t reserved;
 } tptfem_solver_opts;
 

@@ -7,10 +7,10 @@
 // on each aggregate the rigid-body modes (translations, and rotations about
 // its centroid) span the coarse space, orthonormalised per aggregate (modes
 // that an aggregate cannot carry, e.g. rotations of a single node, are
-// dropped).  A_c = P^T A P is formed with one operator product per (colour,
-// mode): aggregates are coloured by bin coordinates mod 3, so an aggregate has
-// at most one neighbour of each colour and P^T A (P e_{colour, mode}) yields
-// whole coarse columns without mixing.  A_c is factorised (cuSOLVER dpotrf /
+// dropped).  A_c = P^T A P is formed with one multi-vector operator product
+// per colour (all modes at once): aggregates are coloured by bin coordinates
+// mod 3, so an aggregate has at most one neighbour of each colour and
+// P^T A (P E_colour) yields whole coarse columns without mixing.  A_c is factorised (cuSOLVER dpotrf /
 // dpotri, once per set-up, off the iteration path) and kept as an explicit
 // FP32 inverse, so each iteration adds one restriction, one coarse mat-vec
 // and a prolongation that is fused into the FSAI transpose kernel.
@@ -33,29 +33,76 @@ constexpr int CS_MAX_COARSE = 8192;
 
 __device__ __forceinline__ int colour_of(const int* b) { return (b[0] % 3) + 3 * (b[1] % 3) + 9 * (b[2] % 3); }
 
-// v = P e_{c, m}: orthonormal mode m on every aggregate of colour c, 0 elsewhere.
+// V[(g dpn + a) nm + m] = (P e_{c, m})_{g,a} for every mode m at once.
 template <int DPN>
-__global__ void cs_fill(int ngroups, const int* __restrict__ agg, const int* __restrict__ abin,
-                        const float* __restrict__ y, const double* __restrict__ T, int colour, int m,
-                        double* __restrict__ v) {
+__global__ void cs_fill_modes(int ngroups, const int* __restrict__ agg, const int* __restrict__ abin,
+                              const float* __restrict__ y, const double* __restrict__ T, int colour,
+                              double* __restrict__ V) {
   constexpr int NM = rigid_modes(DPN);
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ngroups) return;
   const int I = agg[g];
+  double* out = V + (int64_t)g * DPN * NM;
   if (colour_of(abin + 3 * I) != colour) {
 #pragma unroll
-    for (int a = 0; a < DPN; ++a) v[(int64_t)g * DPN + a] = 0.0;
+    for (int q = 0; q < DPN * NM; ++q) out[q] = 0.0;
     return;
   }
   double R[DPN][NM];
   mode_rows<DPN>(y + 3 * (int64_t)g, R);
   const double* t = T + (int64_t)I * NM * NM;
 #pragma unroll
-  for (int a = 0; a < DPN; ++a) {
-    double s = 0.0;
+  for (int a = 0; a < DPN; ++a)
 #pragma unroll
-    for (int k = 0; k < NM; ++k) s += R[a][k] * t[k * NM + m];
-    v[(int64_t)g * DPN + a] = s;
+    for (int m = 0; m < NM; ++m) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < NM; ++k) s += R[a][k] * t[k * NM + m];
+      out[a * NM + m] = s;
+    }
+}
+
+// Raw moments of every column m of W (interleaved) over one segment:
+// smom[(seg nm + m) nm + k] = sum over its groups of (R_g^T W_g[:, m])_k.
+template <int DPN>
+__global__ void __launch_bounds__(CS_THREADS) cs_moments_modes(const int* __restrict__ sbeg,
+                                                               const int* __restrict__ send,
+                                                               const int* __restrict__ alist,
+                                                               const float* __restrict__ y,
+                                                               const double* __restrict__ W,
+                                                               double* __restrict__ smom) {
+  constexpr int NM = rigid_modes(DPN);
+  __shared__ double sh[CS_THREADS / 32][NM * NM];
+  const int seg = blockIdx.x;
+  double s[NM * NM];
+#pragma unroll
+  for (int q = 0; q < NM * NM; ++q) s[q] = 0.0;
+  for (int t = sbeg[seg] + threadIdx.x; t < send[seg]; t += CS_THREADS) {
+    const int g = alist[t];
+    double R[DPN][NM];
+    mode_rows<DPN>(y + 3 * (int64_t)g, R);
+    const double* wg = W + (int64_t)g * DPN * NM;
+#pragma unroll
+    for (int a = 0; a < DPN; ++a)
+#pragma unroll
+      for (int m = 0; m < NM; ++m) {
+        const double wa = wg[a * NM + m];
+#pragma unroll
+        for (int k = 0; k < NM; ++k) s[m * NM + k] += R[a][k] * wa;
+      }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NM * NM; ++q) {
+    double x = s[q];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[wid][q] = x;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < NM * NM; q += CS_THREADS) {
+    double x = 0.0;
+    for (int w = 0; w < CS_THREADS / 32; ++w) x += sh[w][q];
+    smom[(int64_t)seg * NM * NM + q] = x;
   }
 }
 
@@ -111,11 +158,10 @@ __device__ __forceinline__ double agg_moment(int I, int mp, int nm, const int* _
   return x;
 }
 
-// Column block (J, m) of A_c from the moments of w = A P e_{c, m}: for each
-// aggregate I, J is its unique neighbour (itself included) of colour c.
-__global__ void cs_columns(int na, int nm, const int* __restrict__ abin, const int* __restrict__ bin2agg, int bx,
-                           int by, int bz, const int* __restrict__ aseg, const double* __restrict__ smom,
-                           const double* __restrict__ T, int colour, int m, double* __restrict__ Ac, int nc) {
+// Column blocks (J, all m) of A_c from the moments of W = A P E_c.
+__global__ void cs_columns_modes(int na, int nm, const int* __restrict__ abin, const int* __restrict__ bin2agg,
+                                 int bx, int by, int bz, const int* __restrict__ aseg, const double* __restrict__ smom,
+                                 const double* __restrict__ T, int colour, double* __restrict__ Ac, int nc) {
   const int I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= na) return;
   const int nbin[3] = {bx, by, bz};
@@ -132,8 +178,17 @@ __global__ void cs_columns(int na, int nm, const int* __restrict__ abin, const i
   }
   const int J = bin2agg[((int64_t)jb[2] * by + jb[1]) * bx + jb[0]];
   if (J < 0) return;
-  for (int mp = 0; mp < nm; ++mp)
-    Ac[((int64_t)I * nm + mp) * nc + (int64_t)J * nm + m] = agg_moment(I, mp, nm, aseg, smom, T);
+  const double* t = T + (int64_t)I * nm * nm;
+  for (int m = 0; m < nm; ++m)
+    for (int mp = 0; mp < nm; ++mp) {
+      double x = 0.0;
+      for (int k = 0; k < nm; ++k) {
+        double sk = 0.0;
+        for (int q = aseg[I]; q < aseg[I + 1]; ++q) sk += smom[((int64_t)q * nm + m) * nm + k];
+        x += t[k * nm + mp] * sk;
+      }
+      Ac[((int64_t)I * nm + mp) * nc + (int64_t)J * nm + m] = x;
+    }
 }
 
 // yc = P^T r from the segment moments.
@@ -394,29 +449,29 @@ bool coarse_assemble(SystemData& S) {
   cudaStream_t s = S.ctx->stream;
   const int ng = S.nb.ngroups, dpn = S.dpn, nc = C.nc;
   C.Ac.zero();
-  DevBuf<double> v, w;
-  v.alloc(S.n_free, s);
-  w.alloc(S.n_free, s);
+  DevBuf<double> v, w, mom;
+  v.alloc(S.n_free * C.nm, s);
+  w.alloc(S.n_free * C.nm, s);
+  mom.alloc((size_t)C.nseg * C.nm * C.nm, s);
   const int ncx = std::min(3, C.bins[0]), ncy = std::min(3, C.bins[1]), ncz = std::min(3, C.bins[2]);
   for (int cz = 0; cz < ncz; ++cz)
     for (int cy = 0; cy < ncy; ++cy)
       for (int cx = 0; cx < ncx; ++cx) {
         const int colour = cx + 3 * cy + 9 * cz;
-        for (int m = 0; m < C.nm; ++m) {
 #define TPT_CS_COL(D)                                                                                             \
-  cs_fill<D><<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, C.agg.p, C.abin.p, C.y.p, C.T.p, colour, m, v.p);           \
+  cs_fill_modes<D><<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, C.agg.p, C.abin.p, C.y.p, C.T.p, colour, v.p);        \
   TPT_CHECK_LAUNCH();                                                                                             \
-  nb_operator_apply(S, v.p, w.p);                                                                                 \
-  cs_moments<D><<<C.nseg, CS_THREADS, 0, s>>>(C.sbeg.p, C.send.p, C.alist.p, C.y.p, w.p, C.smom.p);              \
-  TPT_CHECK_LAUNCH();                                                                                             \
-  cs_columns<<<blocks_for(C.na), CS_THREADS, 0, s>>>(C.na, C.nm, C.abin.p, C.bin2agg.p, C.bins[0], C.bins[1],       \
-                                                     C.bins[2], C.aseg.p, C.smom.p, C.T.p, colour, m, C.Ac.p, nc); \
+  nb_operator_apply_modes(S, v.p, w.p);                                                                           \
+  cs_moments_modes<D><<<C.nseg, CS_THREADS, 0, s>>>(C.sbeg.p, C.send.p, C.alist.p, C.y.p, w.p, mom.p);           \
   TPT_CHECK_LAUNCH();
-          if (dpn == 3) { TPT_CS_COL(3) }
-          else if (dpn == 2) { TPT_CS_COL(2) }
-          else { TPT_CS_COL(1) }
+        if (dpn == 3) { TPT_CS_COL(3) }
+        else if (dpn == 2) { TPT_CS_COL(2) }
+        else { TPT_CS_COL(1) }
 #undef TPT_CS_COL
-        }
+        cs_columns_modes<<<blocks_for(C.na), CS_THREADS, 0, s>>>(C.na, C.nm, C.abin.p, C.bin2agg.p, C.bins[0],
+                                                                 C.bins[1], C.bins[2], C.aseg.p, mom.p, C.T.p,
+                                                                 colour, C.Ac.p, nc);
+        TPT_CHECK_LAUNCH();
       }
   cs_fix_diag<<<blocks_for(nc), CS_THREADS, 0, s>>>(nc, C.Ac.p);
   TPT_CHECK_LAUNCH();

@@ -143,6 +143,70 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_spmv_sym(int ngroups, const i
   }
 }
 
+// Y = K X for NV interleaved vectors (X[(row) * NV + v]) from the symmetric
+// half storage: each block is read once for all vectors.  Used to form
+// coarse-space products P^T A P (set-up only, not on the iteration path).
+template <int DPN, int NV>
+__global__ void __launch_bounds__(SPMV_THREADS) nb_spmv_sym_multi(int ngroups, const int* __restrict__ lcptr,
+                                                                  const int* __restrict__ lcol,
+                                                                  const double* __restrict__ lval,
+                                                                  const double* __restrict__ dval,
+                                                                  const int* __restrict__ ucptr,
+                                                                  const int* __restrict__ ucol,
+                                                                  const int* __restrict__ ubase,
+                                                                  const double* __restrict__ X,
+                                                                  double* __restrict__ Y) {
+  constexpr int D2 = DPN * DPN;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int nchunks = (ngroups + 31) >> 5;
+  for (int c = warp; c < nchunks; c += nw) {
+    const int g = c * 32 + lane;
+    if (g >= ngroups) continue;
+    double acc[DPN][NV];
+#pragma unroll
+    for (int a = 0; a < DPN; ++a)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) acc[a][v] = 0.0;
+    auto add = [&](const double (&blk)[D2], int J, bool transposed) {
+#pragma unroll
+      for (int b = 0; b < DPN; ++b)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          const double xv = __ldg(X + ((int64_t)J * DPN + b) * NV + v);
+#pragma unroll
+          for (int a = 0; a < DPN; ++a) acc[a][v] += (transposed ? blk[b * DPN + a] : blk[a * DPN + b]) * xv;
+        }
+    };
+    {
+      double blk[D2];
+#pragma unroll
+      for (int q = 0; q < D2; ++q) blk[q] = dval[((int64_t)c * D2 + q) * 32 + lane];
+      add(blk, g, false);
+    }
+    for (int s = lcptr[c]; s < lcptr[c + 1]; ++s) {
+      double blk[D2];
+#pragma unroll
+      for (int q = 0; q < D2; ++q) blk[q] = lval[((int64_t)s * D2 + q) * 32 + lane];
+      add(blk, lcol[(int64_t)s * 32 + lane], false);
+    }
+    for (int s = ucptr[c]; s < ucptr[c + 1]; ++s) {
+      const int64_t idx = (int64_t)s * 32 + lane;
+      const int base = ubase[idx];
+      if (base < 0) continue;
+      double blk[D2];
+#pragma unroll
+      for (int q = 0; q < D2; ++q) blk[q] = __ldg(lval + base + q * 32);
+      add(blk, ucol[idx], true);
+    }
+#pragma unroll
+    for (int a = 0; a < DPN; ++a)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) Y[((int64_t)g * DPN + a) * NV + v] = acc[a][v];
+  }
+}
+
 // One FP16 block of a factor slot: 8 values in a 16-byte word (row-major
 // entries 0..7) plus the 9th entry (3x3) in a separate 2-byte array, so a lane
 // issues two loads per block.  For DPN < 3 the word holds all D2 entries.

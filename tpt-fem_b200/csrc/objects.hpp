@@ -179,6 +179,8 @@ void coarse_restrict_solve(const SystemData& S, const double* r, cudaStream_t s)
 void coarse_download(const SystemData& S, int* na, int* nm, double* Ainv_or_null);  // FP32 inverse, widened
 // solver.cu: y = A x with the system's node-block operator (no reduction)
 void nb_operator_apply(SystemData& S, const double* x, double* y);
+// Y = A X for the rigid_modes(dpn) interleaved vectors of X (symmetric half storage)
+void nb_operator_apply_modes(SystemData& S, const double* X, double* Y);
 
 // solver.cu
 int64_t system_fsai_classic(SystemData& S);  // builds (once) the classic factor; -1 on failure

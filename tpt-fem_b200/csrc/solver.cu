@@ -294,7 +294,9 @@ void select_nb_mode(SystemData& S, Engine<double>& E, const tptfem_solver_opts& 
 // afresh.  Returns the coarse size in use (0: off).
 int select_coarse(SystemData& S, Engine<double>& E, const tptfem_solver_opts& o, bool fresh) {
   bool want = (o.flags & TPTFEM_SOLVE_COARSE) && E.nb_pc;
-  if (want) want = coarse_build(S, o.coarse_aggregates > 0 ? o.coarse_aggregates : 500);
+  // default: about one aggregate per 2800 node groups, between 8 and 1000
+  const int aggs = o.coarse_aggregates > 0 ? o.coarse_aggregates : std::max(8, std::min(1000, S.nb.ngroups / 2800));
+  if (want) want = coarse_build(S, aggs);
   if (want && (fresh || !S.coarse.ready)) want = coarse_assemble(S);
   if (want && !S.coarse.ready) want = false;
   const SystemData* target = want ? &S : nullptr;
@@ -779,6 +781,23 @@ void nb_operator_apply(SystemData& S, const double* x, double* y) {
     else if (N.dpn == 2) nb_spmv<2, false><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.k_cptr.p, N.k_col.p, N.k_val.p, x, y, nullptr, nullptr, false);
     else nb_spmv<1, false><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.k_cptr.p, N.k_col.p, N.k_val.p, x, y, nullptr, nullptr, false);
   }
+  TPT_CHECK_LAUNCH();
+}
+
+void nb_operator_apply_modes(SystemData& S, const double* X, double* Y) {
+  nb_build_sym(S);
+  const NbSell& N = S.nb;
+  cudaStream_t s = S.ctx->stream;
+  const int g = std::max(1, std::min(sm_count() * NB_BLOCKS_PER_SM, ceil_div((int64_t)N.nchunks * 32, SPMV_THREADS)));
+  if (N.dpn == 3)
+    nb_spmv_sym_multi<3, 6><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.ks_lval.p, N.ks_diag.p,
+                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y);
+  else if (N.dpn == 2)
+    nb_spmv_sym_multi<2, 3><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.ks_lval.p, N.ks_diag.p,
+                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y);
+  else
+    nb_spmv_sym_multi<1, 1><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.ks_lval.p, N.ks_diag.p,
+                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y);
   TPT_CHECK_LAUNCH();
 }
 
