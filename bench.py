@@ -351,6 +351,66 @@ def run_ours(args, world, rank, local):
     return out
 
 
+POISSON_WEIGHTS = os.path.join(ROOT, "tpt-fem_b200", "weights", "lfsai_poisson.bin")
+POISSON_TOL = 1e-8
+
+
+def run_poisson_grf(args, world, rank, local):
+    """Heterogeneous Poisson on 128^3 (2,000,376 free dofs) over unseen seeded
+    Gaussian-random-field conductivities: mean solve time to FP64 relative
+    residual 1e-8 with the learned preconditioner (Poisson weights, trained on
+    32^3 / 64^3 fields) vs FP64 Jacobi-PCG, per field, set-up included."""
+    import tpt_fem as F
+    from tpt_fem import lfsai as LF
+    from tpt_fem import workloads as W
+    ctx = F.Context(local)
+    model = LF.LearnedFsai.load(ctx, POISSON_WEIGHTS)
+    n = args.poisson_n
+    seeds = list(range(5000 + 100 * rank, 5000 + 100 * rank + args.fields))
+    methods = {"jacobi_csr": dict(solver=F.SOLVER_JACOBI_PCG, csr_only=True),
+               "learned": dict(solver=F.SOLVER_LEARNED_FSAI_PCG),
+               "learned_coarse": dict(solver=F.SOLVER_LEARNED_FSAI_PCG, coarse=True),
+               "classic_fsai": dict(solver=F.SOLVER_FSAI_MP_PCG)}
+    # one mesh and one reduced system; each field replaces the system's values
+    # (tptfem_system_refresh), keeping its structures, as a loop over fields does
+    prob = W.GrfPoisson(ctx, n)
+    S = prob.system(4999)
+    model.attach(S)
+    for _ in range(args.warmup):
+        for kw in methods.values():
+            S.solve(tol=POISSON_TOL, fresh_setup=True, **kw)
+    rec = {m: {"s": [], "it": [], "res": [], "fell_back": 0} for m in methods}
+    barrier(world)
+    with ClockSampler(local) as clk:
+        for sd in seeds:
+            S.refresh(prob.matrix(sd), prob.rhs)
+            for m, kw in methods.items():
+                st = S.solve(tol=POISSON_TOL, fresh_setup=True, **kw)
+                rec[m]["s"].append(seconds(st))
+                rec[m]["it"].append(st["iterations"])
+                rec[m]["res"].append(st["rel_residual"])
+                rec[m]["fell_back"] += st["fell_back"]
+    barrier(world)
+    mean = {m: barrier_max(float(np.mean(r["s"])), world) for m, r in rec.items()}
+    out = None
+    if rank == 0:
+        out = {"metric": "mean solve time to FP64 rel. residual 1e-8 over unseen GRF fields: learned vs FP64 Jacobi-PCG",
+               "value": mean["learned_coarse"], "unit": "s", "n_gpus": world, "steps": len(seeds),
+               "warmup": args.warmup, "ms_per_step": mean["learned_coarse"] * 1e3, "higher_is_better": False,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64 (factor f16/f32, network f32)",
+               "data": "synthetic (seeded Gaussian random fields, random Fourier features M=1024, l=0.1)",
+               "config": {"workload": f"poisson_grf_{n}^3", "mesh": [n, n, n], "fields": len(seeds),
+                          "field_seeds": [seeds[0], seeds[-1]], "weights": os.path.relpath(POISSON_WEIGHTS, ROOT),
+                          "tol": POISSON_TOL, "parallelism": f"replicas{world}"},
+               "methods": {m: {"mean_s": mean[m], "mean_iterations": float(np.mean(r["it"])),
+                               "max_rel_residual": float(np.max(r["res"])), "fell_back": r["fell_back"]}
+                           for m, r in rec.items()},
+               "speedup_learned_vs_jacobi": mean["jacobi_csr"] / mean["learned"],
+               "speedup_learned_coarse_vs_jacobi": mean["jacobi_csr"] / mean["learned_coarse"],
+               "clocks": clk.summary()}
+    return out
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
@@ -383,12 +443,18 @@ def main():
     ap.add_argument("--solver", default="learned", choices=["learned", "fsai", "jacobi", "mp"])
     ap.add_argument("--profile", action="store_true", help="run only the timed solves (ncu launch list)")
     ap.add_argument("--no-coarse", action="store_true", help="single-level preconditioner (no coarse space)")
+    ap.add_argument("--workload", default="cantilever", choices=["cantilever", "poisson_grf"],
+                    help="poisson_grf: the heterogeneous-Poisson learned-preconditioner configuration")
+    ap.add_argument("--fields", type=int, default=32, help="poisson_grf: unseen fields timed")
+    ap.add_argument("--poisson-n", type=int, default=128, help="poisson_grf: box_mesh cells per axis")
     ap.add_argument("--mesh", type=int, nargs=3, default=None,
                     help="with --profile: cantilever cells (a smaller case for ncu captures)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         out = run_reference(args, world, rank)
+    elif args.workload == "poisson_grf":
+        out = run_poisson_grf(args, world, rank, local)
     else:
         out = run_ours(args, world, rank, local)
     if rank == 0 and out is not None:

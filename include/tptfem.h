@@ -198,6 +198,16 @@ tptfem_status tptfem_apply_traction(tptfem_context* ctx, tptfem_mesh* mesh, int 
 /* reduce_system (crates/tpt-fem-assembly/src/lib.rs:504-535) into a device-resident system. */
 tptfem_status tptfem_reduce_system(tptfem_context* ctx, const tptfem_matrix* mat, const double* rhs, int64_t n,
                                    const int64_t* bc_dof, const double* bc_val, int64_t nbc, tptfem_system** out);
+/* New values for an existing reduced system: `mat` assembled on the same mesh
+ * with new coefficients (same sparsity pattern) and a new rhs; the Dirichlet
+ * set and every structure built for the system (node-block layout, factor
+ * patterns, coarse geometry, captured graphs) are kept, and each method sets
+ * its preconditioner up afresh on its next solve.  This is the reference's
+ * reduce_system (crates/tpt-fem-assembly/src/lib.rs:504-535) applied to new
+ * values without rebuilding the pattern, as in a loop over coefficient fields
+ * on one mesh.  TPTFEM_ERR_INVALID_ARG if the reduced pattern differs. */
+tptfem_status tptfem_system_refresh(tptfem_context* ctx, tptfem_system* sys, const tptfem_matrix* mat,
+                                    const double* rhs, int64_t n);
 tptfem_status tptfem_system_sizes(const tptfem_system* sys, int64_t* n_free, int64_t* nnz);
 /* Reduced CSR, fred and the free map, for inspection. */
 tptfem_status tptfem_system_download(tptfem_context* ctx, const tptfem_system* sys, int64_t* row_ptrs,

@@ -109,3 +109,40 @@ def test_coarse_not_applicable_runs_without_it(ctx):
     S2 = F.reduce_system(K, rhs, bcs)
     st = S2.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=1e-10, coarse=True)
     assert st["coarse_size"] == 0 and st["rel_residual"] <= 1e-10
+
+
+def test_refresh_matches_a_freshly_reduced_system(ctx):
+    # new coefficients on the same mesh: refreshed values equal a new reduction bit for bit,
+    # and every method solves the refreshed system as it solves the new one
+    mn, mx, n = [0.0, 0.0, 0.0], [4.0, 1.0, 1.0], [16, 4, 4]
+    c, e = box(n, mn=mn, mx=mx)
+    m = F.Mesh.from_arrays(F.CELL_TET4, c, e, ctx=ctx)
+    dof, val = W.clamp_x0_bcs(c)
+    bcs = list(zip(dof, val))
+    K1 = F.assemble_elasticity(m, "3d", W.cantilever_young(n, seed=1), 0.3, 2)
+    rhs1 = F.apply_traction(m, 3, 0, 1.0, [0.0, 0.0, -1e-3], np.zeros(K1.nrows))
+    S = F.reduce_system(K1, rhs1, bcs)
+    model = LF.LearnedFsai(ctx, seed=2)
+    model.attach(S)
+    kinds = [dict(solver=F.SOLVER_JACOBI_PCG, csr_only=True), dict(solver=F.SOLVER_FSAI_MP_PCG, coarse=True),
+             dict(solver=F.SOLVER_LEARNED_FSAI_PCG, coarse=True), dict(solver=F.SOLVER_JACOBI_PCG)]
+    for kw in kinds:
+        S.solve(tol=1e-10, **kw)
+    K2 = F.assemble_elasticity(m, "3d", W.cantilever_young(n, seed=2), 0.3, 2)
+    rhs2 = F.apply_traction(m, 3, 0, 1.0, [0.0, 0.0, -2e-3], np.zeros(K2.nrows))
+    S.refresh(K2, rhs2)
+    T = F.reduce_system(K2, rhs2, bcs)
+    model.attach(T)
+    for a, b in zip(S.download(), T.download()):
+        assert np.array_equal(a, b)
+    for kw in kinds:
+        sa = S.solve(tol=1e-10, **kw)
+        ua = S.solution()
+        sb = T.solve(tol=1e-10, **kw)
+        ub = T.solution()
+        assert sa["rel_residual"] <= 1e-10 and not sa["fell_back"]
+        assert sa["iterations"] == sb["iterations"] and np.array_equal(ua, ub)
+    # a matrix with another pattern is rejected
+    K3 = F.assemble_elasticity(F.Mesh.from_arrays(F.CELL_TET4, *box([8, 2, 2]), ctx=ctx), "3d", 1.0, 0.3, 2)
+    with pytest.raises(F.TptFemError):
+        S.refresh(K3, np.zeros(K3.nrows))

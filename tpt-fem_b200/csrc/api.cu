@@ -404,6 +404,23 @@ tptfem_status tptfem_reduce_system(tptfem_context* ctx, const tptfem_matrix* mat
   API_CATCH(ctx)
 }
 
+tptfem_status tptfem_system_refresh(tptfem_context* ctx, tptfem_system* sys, const tptfem_matrix* mat,
+                                    const double* rhs, int64_t n) {
+  if (!ctx || !sys || !sys->d || !mat || !mat->d || !rhs) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  SystemData& S = *sys->d;
+  TPT_REQUIRE(n == S.n, TPTFEM_ERR_INVALID_ARG, "rhs length does not match the system");
+  DevBuf<double> d;
+  d.alloc(n, ctx->stream);
+  d.upload(rhs, n);
+  const bool ok = system_refresh(S, *mat->d, d.p);
+  system_values_changed(S);  // values were (partly) overwritten either way
+  TPT_REQUIRE(ok, TPTFEM_ERR_INVALID_ARG,
+              "refresh: the matrix's pattern differs from the system's (reduce the system again)");
+  API_CATCH(ctx)
+}
+
 tptfem_status tptfem_system_sizes(const tptfem_system* sys, int64_t* n_free, int64_t* nnz) {
   if (!sys || !sys->d) return TPTFEM_ERR_INVALID_ARG;
   if (n_free) *n_free = sys->d->n_free;

@@ -259,6 +259,21 @@ void nb_build_sym(SystemData& S) {
   N.sym_built = true;
 }
 
+void nb_refresh_values(SystemData& S) {
+  NbSell& N = S.nb;
+  if (N.state != 1) return;
+  cudaStream_t s = S.ctx->stream;
+  fill_k<<<ceil_div(N.ngroups, 128), 128, 0, s>>>(N.ngroups, N.dpn, S.row_ptr.p, S.col.p, S.val.p, N.gptr.p,
+                                                  N.glist.p, N.k_cptr.p, N.k_col.p, N.k_val.p);
+  TPT_CHECK_LAUNCH();
+  if (N.sym_built) {
+    fill_ksym<<<ceil_div(N.ngroups, 128), 128, 0, s>>>(N.ngroups, N.dpn, S.row_ptr.p, S.col.p, S.val.p, N.l_cptr.p,
+                                                       N.l_col.p, N.nlow.p, N.u_cptr.p, N.u_pos.p, N.u_col.p,
+                                                       N.ks_lval.p, N.ks_diag.p, N.ku_base.p);
+    TPT_CHECK_LAUNCH();
+  }
+}
+
 bool nb_build_operator(SystemData& S) {
   if (S.nb.state != 0) return S.nb.state == 1;
   cudaStream_t s = S.ctx->stream;

@@ -135,6 +135,11 @@ struct SystemData {
   DevBuf<float> val32;    // lazily converted FP32 copy for mixed precision
   DevBuf<double> fred, x;
   DevBuf<double> u_fixed;  // full-length vector holding the prescribed values
+  // kept for tptfem_system_refresh: first bcs index per dof (INT_MAX: free),
+  // bcs values, rank of each free dof
+  DevBuf<int> bc_first, red_rank;
+  DevBuf<double> bc_vals;
+  int value_gen = 0;       // incremented when the values are refreshed
   std::shared_ptr<SolverWork> work;
   std::shared_ptr<LfModel> lmodel;  // network used by the learned-FSAI solver
   ~SystemData();
@@ -155,6 +160,9 @@ void csr_matvec_f64(tptfem_context* ctx, int64_t nrows, const int* rp, const int
                     const double* x, double* y);
 
 // reduce.cu
+// New values for an existing system (same matrix pattern, same Dirichlet set):
+// false if the matrix's reduced pattern differs from the system's.
+bool system_refresh(SystemData& S, const MatrixData& A, const double* d_rhs);
 std::unique_ptr<SystemData> reduce_system(tptfem_context* ctx, const MatrixData& A, const double* d_rhs,
                                           const int64_t* bc_dof, const double* bc_val, int64_t nbc);
 void system_solution(const SystemData& S, double* d_u);
@@ -171,6 +179,7 @@ bool fsai_set_values(const SystemData& S, FsaiFactor& F, const double* d_sig2, c
 bool nb_build_operator(SystemData& S);  // false when the system has partial node groups
 bool nb_fill_factor(SystemData& S, const FsaiFactor& F);  // false: factor rows not node-block shaped
 void nb_build_sym(SystemData& S);  // after nb_build_operator succeeded
+void nb_refresh_values(SystemData& S);  // refill the node-block values from S.val
 
 // coarse.cu
 bool coarse_build(SystemData& S, int target_aggregates);  // geometry (once); false: not applicable
@@ -188,6 +197,7 @@ void system_fsai_download(const SystemData& S, int64_t* rp, int64_t* ci, double*
 void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32, double* ms_nb, double* nb_bytes,
                          double* ms_nbs, double* nbs_bytes);
 void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats& st);
+void system_values_changed(SystemData& S);  // after the values of S.val / S.fred were replaced
 
 // topopt.cu
 void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, const tptfem_topopt_opts* opts,

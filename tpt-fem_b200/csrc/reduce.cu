@@ -82,6 +82,36 @@ __global__ void reduced_fill(const int* __restrict__ rp, const int* __restrict__
   fred[i] = r;
 }
 
+// Values of an existing reduced system from a matrix with the same pattern:
+// flags any column that differs from the system's.
+__global__ void reduced_refill(const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ va,
+                               const int* __restrict__ first, const int* __restrict__ red,
+                               const int* __restrict__ free_map, const double* __restrict__ bc_val,
+                               const double* __restrict__ rhs, int64_t n_free, const int* __restrict__ rrp,
+                               const int* __restrict__ rci, double* __restrict__ rva, double* __restrict__ fred,
+                               int* __restrict__ flag) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_free) return;
+  int f = free_map[i];
+  double r = rhs[f];
+  int o = rrp[i];
+  const int oe = rrp[i + 1];
+  for (int k = rp[f]; k < rp[f + 1]; ++k) {
+    int col = ci[k];
+    double v = va[k];
+    int fb = first[col];
+    if (fb != INT_MAX) {
+      r = __dsub_rn(r, __dmul_rn(v, bc_val[fb]));
+    } else {
+      if (o >= oe || rci[o] != red[col]) { atomicOr(flag, 1); return; }
+      rva[o] = v;
+      ++o;
+    }
+  }
+  if (o != oe) atomicOr(flag, 1);
+  fred[i] = r;
+}
+
 __global__ void reduced_index(const int* __restrict__ first, const int* __restrict__ red, int64_t n,
                               int* __restrict__ red_map) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -165,8 +195,28 @@ std::unique_ptr<SystemData> reduce_system(tptfem_context* ctx, const MatrixData&
   TPT_CHECK_LAUNCH();
   S->x.alloc(S->n_free, s);
   S->x.zero();
+  S->bc_first = std::move(first);
+  S->red_rank = std::move(red);
+  S->bc_vals = std::move(val);
   TPT_CUDA(cudaStreamSynchronize(s));
   return S;
+}
+
+bool system_refresh(SystemData& S, const MatrixData& A, const double* d_rhs) {
+  cudaStream_t s = S.ctx->stream;
+  TPT_REQUIRE(A.nrows == S.n && A.dpn == S.dpn, TPTFEM_ERR_INVALID_ARG,
+              "refresh: the matrix does not match the system's size");
+  TPT_CUDA(cudaMemsetAsync(S.ctx->d_flag, 0, sizeof(int), s));
+  if (S.n_free) {
+    reduced_refill<<<ceil_div(S.n_free, 256), 256, 0, s>>>(A.row_ptr.p, A.col.p, A.val.p, S.bc_first.p,
+                                                           S.red_rank.p, S.free_map.p, S.bc_vals.p, d_rhs, S.n_free,
+                                                           S.row_ptr.p, S.col.p, S.val.p, S.fred.p, S.ctx->d_flag);
+    TPT_CHECK_LAUNCH();
+  }
+  int flag = 0;
+  TPT_CUDA(cudaMemcpyAsync(&flag, S.ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TPT_CUDA(cudaStreamSynchronize(s));
+  return flag == 0;
 }
 
 void system_solution(const SystemData& S, double* d_u) {

@@ -249,6 +249,7 @@ struct SolverWork {
   const FsaiFactor* nb_factor = nullptr;  // factor whose blocks S.nb holds
   bool f64_ready = false, f64_csr_ready = false, f32_ready = false, fsai_ready = false, fsai_failed = false;
   bool lf_ready = false, lf_engine = false;
+  int seen_gen[8] = {-1, -1, -1, -1, -1, -1, -1, -1};  // per method: value generation last set up for
   DevBuf<double> rhi;   // FP64 true residual
   DevBuf<double> sc;    // scalars
   DevBuf<unsigned> tk;  // tickets for standalone reductions
@@ -470,8 +471,9 @@ LfGraph& system_lf_graph(SystemData& S, FsaiFactor** F) {
   return W.lgraph;
 }
 
-void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats& st) {
+void system_solve(SystemData& S, const tptfem_solver_opts& o_in, tptfem_solve_stats& st) {
   tptfem_context* ctx = S.ctx;
+  tptfem_solver_opts o = o_in;
   cudaStream_t s = ctx->stream;
   const double tol = o.rel_tol > 0 ? o.rel_tol : 1e-10;
   const int64_t max_it = o.max_iter > 0 ? o.max_iter : 100000;
@@ -487,6 +489,13 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats
   }
   ensure_work(S);
   SolverWork& W = *S.work;
+  {  // values changed by tptfem_system_refresh since this method last set up: set up afresh
+    const int slot = solver + ((o.flags & TPTFEM_SOLVE_CSR_ONLY) ? 4 : 0);
+    if (W.seen_gen[slot] != S.value_gen) {
+      if (W.seen_gen[slot] >= 0) o.flags |= TPTFEM_SOLVE_FRESH_SETUP;
+      W.seen_gen[slot] = S.value_gen;
+    }
+  }
   if (solver == TPTFEM_SOLVER_LEARNED_FSAI_PCG) {
     TPT_REQUIRE(S.lmodel != nullptr, TPTFEM_ERR_INVALID_ARG, "no learned model attached to this system");
     TPT_CUDA(cudaEventRecord(ctx->ev[0], s));
@@ -762,6 +771,17 @@ void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32
     *nbs_bytes = (double)N.l_slots * 32 * (4 + 8 * d2) + (double)N.nchunks * 32 * 8 * d2 +
                  (double)N.u_slots * 32 * 8 + 2.0 * (N.nchunks + 1) * 4 + 16.0 * (double)S.n_free;
   }
+}
+
+void system_values_changed(SystemData& S) {
+  ++S.value_gen;
+  if (S.val32.p) {  // the FP32 copy used by the mixed-precision engine is refreshed in place
+    to_f32<<<ceil_div(S.nnz, 256), 256, 0, S.ctx->stream>>>(S.nnz, S.val.p, S.val32.p);
+    TPT_CHECK_LAUNCH();
+  }
+  if (S.work) S.work->lgraph.ready = false;  // network inputs derive from the values
+  S.coarse.ready = false;
+  nb_refresh_values(S);
 }
 
 void nb_operator_apply(SystemData& S, const double* x, double* y) {

@@ -326,6 +326,11 @@ class System:
         self.ctx.check(rc)
         return st.as_dict()
 
+    def refresh(self, mat, rhs):
+        """New values (same mesh, same pattern, same Dirichlet set) for this system; structures are kept."""
+        rhs = N.f64(rhs)
+        self.ctx.check(self.ctx.lib.tptfem_system_refresh(self.ctx.h, self.h, mat.h, N.ptr(rhs), len(rhs)))
+
     def coarse(self, with_inverse=False):
         """The coarse space of the last coarse solve: dict(na, nm, bins[, ainv])."""
         na, nm = C.c_int32(), C.c_int32()

@@ -71,6 +71,7 @@ _pd = C.POINTER(C.c_double)
 _pint = C.POINTER(C.c_int)
 
 SIGNATURES = {
+    "tptfem_system_refresh": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "tptfem_system_coarse": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                        C.c_void_p, C.c_void_p]),
     "tptfem_topopt_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,

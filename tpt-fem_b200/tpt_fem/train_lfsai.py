@@ -44,13 +44,7 @@ def cantilever(ctx, n, seed):
 
 
 def grf_poisson(ctx, n, seed):
-    mesh = F.Mesh.box_mesh([0.0, 0.0, 0.0], [1.0, 1.0, 1.0], [n, n, n], ctx=ctx)
-    k = np.exp(W.grf_log_conductivity(W.tet_centroids(mesh.coords_array, mesh.conn_array), seed))
-    K = F.assemble_poisson(mesh, k, 2)
-    rhs = F.load_poisson_source(mesh, 1.0, 2)
-    c = mesh.coords_array
-    on_b = np.nonzero(np.any((c < 1e-9) | (c > 1 - 1e-9), axis=1))[0]
-    return F.reduce_system(K, rhs, [(int(i), 0.0) for i in on_b])
+    return W.grf_poisson_system(ctx, n, seed)
 
 
 FAMILIES = {

@@ -64,6 +64,58 @@ def tet_centroids(coords, conn):
     return coords[conn].mean(axis=1)
 
 
+def grf_at_centroids(coords, conn, seed, length=0.1, n_features=1024):
+    """grf_log_conductivity at the element centroids (computed on the GPU through
+    torch when one is available: input generation only)."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            rng = np.random.default_rng(seed)
+            w = rng.standard_normal((3, n_features)) / length
+            phi = rng.uniform(0.0, 2.0 * np.pi, n_features)
+            scale = np.sqrt(2.0 / n_features)
+            ct = torch.as_tensor(coords, device="cuda")
+            et = torch.as_tensor(conn, device="cuda")
+            wt = torch.as_tensor(w, device="cuda")
+            pt = torch.as_tensor(phi, device="cuda")
+            out = torch.empty(len(conn), dtype=torch.float64, device="cuda")
+            for a in range(0, len(conn), 1 << 20):
+                x = ct[et[a:a + (1 << 20)]].mean(dim=1)
+                out[a:a + len(x)] = torch.cos(x @ wt + pt).sum(dim=1) * scale
+            return out.cpu().numpy()
+    except ImportError:
+        pass
+    return grf_log_conductivity(tet_centroids(coords, conn), seed, length, n_features)
+
+
+class GrfPoisson:
+    """Heterogeneous Poisson on the unit cube, box_mesh [n, n, n]: k = exp(g) per
+    tet with g the seeded Gaussian random field at its centroid, f = 1,
+    u = 0 on all six faces, quadrature order 2.  One mesh; matrix() assembles
+    the operator of a field, system() reduces it."""
+
+    def __init__(self, ctx, n):
+        import tpt_fem as F
+        self.F = F
+        self.mesh = F.Mesh.box_mesh([0.0, 0.0, 0.0], [1.0, 1.0, 1.0], [n, n, n], ctx=ctx)
+        c = self.mesh.coords_array
+        self.coords, self.conn = c, self.mesh.conn_array
+        self.rhs = F.load_poisson_source(self.mesh, 1.0, 2)
+        on_b = np.nonzero(np.any((c < 1e-9) | (c > 1 - 1e-9), axis=1))[0]
+        self.bcs = [(int(i), 0.0) for i in on_b]
+
+    def matrix(self, seed):
+        return self.F.assemble_poisson(self.mesh, np.exp(grf_at_centroids(self.coords, self.conn, seed)), 2)
+
+    def system(self, seed):
+        return self.F.reduce_system(self.matrix(seed), self.rhs, self.bcs)
+
+
+def grf_poisson_system(ctx, n, seed):
+    """The reduced GrfPoisson system of one field on a fresh mesh."""
+    return GrfPoisson(ctx, n).system(seed)
+
+
 def grf_log_conductivity(points, seed, length=0.1, n_features=1024):
     """Seeded Gaussian random field (mean 0, variance 1, squared-exponential
     correlation of length `length`) by random Fourier features:
