@@ -10,7 +10,8 @@
 //   K   : all neighbour blocks, FP64; each of the DPN*DPN values is a
 //         contiguous run of 32 (one 256-byte warp load per value).
 //   L   : strictly-lower neighbour blocks (J < I), FP16, each lane's block
-//         packed in a 16-byte word (8 values) + a 2-byte tail (the 9th),
+//         packed in a 16-byte word (8 values) + a 2-byte tail (the 9th; for
+//         one dof per node the tail alone holds the value),
 //         + the strictly-lower part of the diagonal block;
 //   L^T : strictly-upper neighbour blocks (J > I) holding transposed blocks of
 //         L, same packing; it reuses L's diagonal part, transposed.
@@ -166,6 +167,10 @@ __global__ void check_factor_shape(int ngroups, int dpn, const int* __restrict__
 }
 
 __device__ __forceinline__ void store_block(uint4* pack, __half* tail, int64_t idx, const float* v, int d2) {
+  if (d2 == 1) {  // a single value: the 2-byte array holds it, the word stays unused
+    tail[idx] = __float2half(v[0]);
+    return;
+  }
   __half h[8];
   for (int q = 0; q < 8; ++q) h[q] = __float2half(q < d2 ? v[q] : 0.f);
   uint4 w;

@@ -209,22 +209,27 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_spmv_sym_multi(int ngroups, c
 
 // One FP16 block of a factor slot: 8 values in a 16-byte word (row-major
 // entries 0..7) plus the 9th entry (3x3) in a separate 2-byte array, so a lane
-// issues two loads per block.  For DPN < 3 the word holds all D2 entries.
+// issues two loads per block.  For DPN = 2 the word holds all 4 entries; for
+// DPN = 1 the single value is stored in the 2-byte array only.
 template <int DPN>
 __device__ __forceinline__ void load_half_block(const uint4* __restrict__ pack, const __half* __restrict__ tail,
                                                 int64_t idx, float (&v)[DPN * DPN]) {
-  const uint4 w = __ldg(pack + idx);
-  const __half2* h = reinterpret_cast<const __half2*>(&w);
-  float f[8];
+  if constexpr (DPN == 1) {  // one value: it lives in the 2-byte array alone
+    v[0] = __half2float(__ldg(tail + idx));
+  } else {
+    const uint4 w = __ldg(pack + idx);
+    const __half2* h = reinterpret_cast<const __half2*>(&w);
+    float f[8];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const float2 p = __half22float2(h[i]);
-    f[2 * i] = p.x;
-    f[2 * i + 1] = p.y;
+    for (int i = 0; i < 4; ++i) {
+      const float2 p = __half22float2(h[i]);
+      f[2 * i] = p.x;
+      f[2 * i + 1] = p.y;
+    }
+#pragma unroll
+    for (int q = 0; q < DPN * DPN && q < 8; ++q) v[q] = f[q];
+    if constexpr (DPN * DPN == 9) v[8] = __half2float(tail[idx]);
   }
-#pragma unroll
-  for (int q = 0; q < DPN * DPN && q < 8; ++q) v[q] = f[q];
-  if constexpr (DPN * DPN == 9) v[8] = __half2float(tail[idx]);
 }
 
 // t = sigma^2 * (r + L r), L in packed FP16 blocks.  Skipped once done.
