@@ -104,56 +104,46 @@ __device__ __forceinline__ int local_node(int di, int dj) {
 }
 
 // y = K(E) v on the grid's rows; rows of fixed dofs are set to 0 when `mask`.
-// Node (i, j) gathers its <= 4 incident elements (origins (i-1..i, j-1..j)); the
-// 3x3 node neighbourhood of v is loaded once.  Returns this thread's part of v.y.
+// Node (i, j) gathers its <= 4 incident elements (origins (i-1..i, j-1..j)),
+// each from its own 8 dof values (L1-resident), which keeps few values live.
+// Returns this thread's part of v.y.
 template <int NT>
 __device__ double apply_k(const TopoInst& I, const double* __restrict__ E, const double* __restrict__ v,
                           double* __restrict__ y, const uint8_t* __restrict__ fixed, bool mask,
                           const double* __restrict__ ke) {
-  const int nx = I.nx, ny = I.ny, nelx = I.nelx, nn = nx * ny;
+  const int nx = I.nx, nelx = I.nelx, nely = I.nely, nn = nx * I.ny;
   double dot = 0.0;
   for (int n = threadIdx.x; n < nn; n += NT) {
     const int i = n % nx, j = n / nx;
-    double vn[3][3][2];
-#pragma unroll
-    for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll
-      for (int dx = -1; dx <= 1; ++dx) {
-        const bool in = i + dx >= 0 && i + dx < nx && j + dy >= 0 && j + dy < ny;
-        const int m = n + dy * nx + dx;
-        vn[dy + 1][dx + 1][0] = in ? v[2 * m] : 0.0;
-        vn[dy + 1][dx + 1][1] = in ? v[2 * m + 1] : 0.0;
-      }
     double y0 = 0.0, y1 = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+      const int di = (q & 1) ? 0 : -1, dj = (q & 2) ? 0 : -1;
+      const int ei = i + di, ej = j + dj;
+      if (ei < 0 || ei >= nelx || ej < 0 || ej >= nely) continue;
+      const int n0 = ej * nx + ei;
+      const int ln = local_node(di, dj);
+      const double* k0 = ke + (2 * ln) * 8;
+      const double* k1 = k0 + 8;
+      const int nd[4] = {n0, n0 + 1, n0 + nx + 1, n0 + nx};
+      double s0 = 0.0, s1 = 0.0;
 #pragma unroll
-    for (int dj = -1; dj <= 0; ++dj)
-#pragma unroll
-      for (int di = -1; di <= 0; ++di) {
-        const int ei = i + di, ej = j + dj;
-        if (ei < 0 || ei >= nelx || ej < 0 || ej >= I.nely) continue;
-        const double Ee = E[ej * nelx + ei];
-        const int ln = local_node(di, dj);
-        // element nodes in neighbourhood coordinates (row = y + 1, col = x + 1)
-        const int ry[4] = {dj + 1, dj + 1, dj + 2, dj + 2}, rx[4] = {di + 1, di + 2, di + 2, di + 1};
-        const double* k0 = ke + (2 * ln) * 8;
-        const double* k1 = k0 + 8;
-        double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const double a = vn[ry[k]][rx[k]][0], b = vn[ry[k]][rx[k]][1];
-          s0 += k0[2 * k] * a + k0[2 * k + 1] * b;
-          s1 += k1[2 * k] * a + k1[2 * k + 1] * b;
-        }
-        y0 += Ee * s0;
-        y1 += Ee * s1;
+      for (int k = 0; k < 4; ++k) {
+        const double2 vv = __ldg(reinterpret_cast<const double2*>(v) + nd[k]);
+        s0 += k0[2 * k] * vv.x + k0[2 * k + 1] * vv.y;
+        s1 += k1[2 * k] * vv.x + k1[2 * k + 1] * vv.y;
       }
+      const double Ee = __ldg(E + ej * nelx + ei);
+      y0 += Ee * s0;
+      y1 += Ee * s1;
+    }
     if (mask) {
       if (fixed[2 * n]) y0 = 0.0;
       if (fixed[2 * n + 1]) y1 = 0.0;
     }
-    y[2 * n] = y0;
-    y[2 * n + 1] = y1;
-    dot += vn[1][1][0] * y0 + vn[1][1][1] * y1;
+    reinterpret_cast<double2*>(y)[n] = make_double2(y0, y1);
+    const double2 vn = reinterpret_cast<const double2*>(v)[n];
+    dot += vn.x * y0 + vn.y * y1;
   }
   return dot;
 }
@@ -197,7 +187,7 @@ __device__ __forceinline__ double oc_candidate(double rho, double b, double lamb
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT) topo_iteration(TopoArgs a) {
+__global__ void __launch_bounds__(NT, 1) topo_iteration(TopoArgs a) {
   __shared__ double ke[64];
   __shared__ double red[72];
   __shared__ TopoInst I;
