@@ -360,6 +360,31 @@ POISSON_WEIGHTS = os.path.join(ROOT, "tpt-fem_b200", "weights", "lfsai_poisson.b
 POISSON_TOL = 1e-8
 
 
+def poisson_cpu_baseline(n, jacobi_iters, n_sample=48):
+    """The plain method on the host: the oracle's FP64 Jacobi-PCG (all host
+    threads) on one n_sample^3 GRF field built by the oracle, 40 iterations,
+    scaled by the nnz ratio and by the GPU-measured Jacobi iteration count."""
+    from oracle import oracle as O
+    from tpt_fem import workloads as W
+    c, e = O.box_mesh([0.0, 0.0, 0.0], [1.0, 1.0, 1.0], [n_sample] * 3)
+    k = np.exp(W.grf_log_conductivity(W.tet_centroids(c, e), 4999))
+    m = O.Mesh(O.CELL_TET, c, e)
+    coo = O.assemble_poisson(m, k, 2)
+    rhs = O.load_poisson_source(m, 1.0, 2)
+    on_b = np.nonzero(np.any((c < 1e-9) | (c > 1 - 1e-9), axis=1))[0]
+    kred, fred, _ = O.reduce_system(coo, rhs, [(int(i), 0.0) for i in on_b])
+    csr = kred.to_csr()
+    threads = O.max_threads()
+    O.pcg_jacobi(csr, fred, tol=1e-30, max_it=3, nthreads=threads)
+    t0 = time.perf_counter()
+    _, it, _ = O.pcg_jacobi(csr, fred, tol=1e-30, max_it=40, nthreads=threads)
+    per_it = (time.perf_counter() - t0) / abs(it)
+    nnz_full = 7 * (n - 1) ** 3  # 7-point rows of the reduced n^3 system (interior nodes)
+    return {"value": per_it * (nnz_full / csr.nnz) * jacobi_iters, "unit": "s", "cores": threads, "kind": "port",
+            "sample": f"oracle FP64 Jacobi-PCG, 40 iterations on one {n_sample}^3 field ({csr.nnz} nnz), scaled by "
+                      f"nnz ratio and by the {jacobi_iters:.0f} Jacobi iterations measured at {n}^3"}
+
+
 def run_poisson_grf(args, world, rank, local):
     """Heterogeneous Poisson on 128^3 (2,000,376 free dofs) over unseen seeded
     Gaussian-random-field conductivities: mean solve time to FP64 relative
@@ -410,10 +435,31 @@ def run_poisson_grf(args, world, rank, local):
                "methods": {m: {"mean_s": mean[m], "mean_iterations": float(np.mean(r["it"])),
                                "max_rel_residual": float(np.max(r["res"])), "fell_back": r["fell_back"]}
                            for m, r in rec.items()},
+               "cpu_baseline": poisson_cpu_baseline(n, float(np.mean(rec["jacobi_csr"]["it"]))),
                "speedup_learned_vs_jacobi": mean["jacobi_csr"] / mean["learned"],
                "speedup_learned_coarse_vs_jacobi": mean["jacobi_csr"] / mean["learned_coarse"],
                "clocks": clk.summary()}
     return out
+
+
+def topopt_cpu_baseline(probs, oc_iters, gpu_seconds):
+    """The reference algorithm on the host (oracle restatement of topopt_simp,
+    banded Cholesky in place of its infeasible dense LU, one core): one 90x30
+    instance for a bounded number of OC iterations, scaled to the batch by
+    free-dof-iterations."""
+    from oracle import oracle as O
+    P, f, bcs = next((p for p in probs if p[0].grid.nelx == 90), probs[0])
+    its = 20
+    t0 = time.perf_counter()
+    O.topopt(P.grid.nelx, P.grid.nely, P.vol_frac, P.filter_radius, its, f, bcs, emin=P.emin,
+             density_filter=True, banded=True)
+    dt = time.perf_counter() - t0
+    per_dof_it = dt / (its * 2 * P.grid.n_nodes())
+    batch = per_dof_it * sum(2 * p.grid.n_nodes() for p, _, _ in probs) * oc_iters
+    return {"value": batch, "unit": "s", "cores": 1, "kind": "port",
+            "sample": f"oracle topopt_simp (density-filter mode, banded Cholesky), {its} OC iterations of one "
+                      f"{P.grid.nelx}x{P.grid.nely} instance ({dt:.2f} s), scaled by free-dof-iterations to the "
+                      f"batch", "gpu_speedup": batch / gpu_seconds}
 
 
 def run_topopt(args, world, rank, local):
@@ -448,6 +494,7 @@ def run_topopt(args, world, rank, local):
                           "solver": "Jacobi-PCG per instance, FP64, rel. tol 1e-10, warm start",
                           "parallelism": f"replicas{world}"},
                "batch_seconds": sec, "tune_ms": st["tune_ms"], "threads_per_instance": st["block_threads"],
+               "cpu_baseline": topopt_cpu_baseline(probs, args.oc_iters, sec),
                "pcg_iterations": st["pcg_iterations"],
                "compliance_final_over_initial": {"min": min(ratio), "median": float(np.median(ratio)),
                                                  "max": max(ratio)},

@@ -313,7 +313,7 @@ tptfem_status tptfem_system_attach_lfsai(tptfem_context* ctx, tptfem_system* sys
  * independent instances: each instance is TopOptParams with a grid of
  * nelx x nely unit-size elements (Grid::new(nelx + 1, nely + 1, h),
  * topopt:89-116), its load vector and its Dirichlet list.  Per iteration the
- * displacement solve is FP64 Jacobi-PCG on the matrix-free Q1 operator (the
+ * displacement solve is FP64 PCG on the matrix-free Q1 operator (the
  * reference uses a dense LU) to relative residual opts.rel_tol.
  * density_filter = 0 follows the reference exactly (E_min = emin, set it to
  * 1e-3 * e0 as topopt:54 does; sensitivity filter topopt:259-279; OC
@@ -341,7 +341,8 @@ typedef struct tptfem_topopt_opts {
   int32_t max_pcg_iter;   /* per solve (0: 50000) */
   int32_t block_threads;  /* threads per instance: 256, 512, 1024, or 0 = autotune */
   int32_t use_graph;      /* capture all iterations in one CUDA graph */
-  int32_t reserved;
+  int32_t plain_jacobi;   /* 1: Jacobi-PCG only; 0: Jacobi + per-instance coarse space of plane
+                             rigid modes on about 48 node-box aggregates (the default) */
 } tptfem_topopt_opts;
 
 typedef struct tptfem_topopt_stats {

@@ -114,3 +114,18 @@ def test_zero_iterations_and_invalid_input(ctx):
         T.topopt_simp(bad, f, bcs, ctx=ctx)
     with pytest.raises(F.TptFemError):
         T.topopt_simp(P, f, [(10 ** 6, 0.0)], ctx=ctx)
+
+
+def test_two_level_and_plain_jacobi_agree(ctx):
+    # the per-instance coarse space changes the iterations, not the optimisation
+    probs = []
+    for nx, ny in [(60, 20), (36, 12)]:
+        P = params(nx, ny, 0.4, 1.5, 30, emin=1e-9, density_filter=True)
+        f, bcs = T.cantilever_load(P.grid, node=P.grid.nx * (ny // 2) + nx)
+        probs.append((P, f, bcs))
+    two, st2 = T.topopt_batch(ctx, probs, rel_tol=TOL)
+    one, st1 = T.topopt_batch(ctx, probs, rel_tol=TOL, plain_jacobi=True)
+    assert st2["pcg_iterations"] < 0.75 * st1["pcg_iterations"]
+    for a, b in zip(two, one):
+        assert np.max(np.abs(a.compliance - b.compliance) / b.compliance) < 1e-8
+        assert np.max(np.abs(a.densities - b.densities)) < 1e-7

@@ -6,8 +6,10 @@
 // for every instance:
 //   E_e = emin + rho_e^p (e0 - emin)                     (assemble, topopt:220-238)
 //   K(E) u = f with Dirichlet dofs, matrix-free Q1 apply from the unit element
-//     matrix (element_stiffness_unit, topopt:166-217), Jacobi-PCG in FP64,
-//     warm-started from the previous iteration's displacement
+//     matrix (element_stiffness_unit, topopt:166-217), PCG in FP64 warm-started
+//     from the previous iteration's displacement, preconditioned by Jacobi plus
+//     an aggregation coarse space of plane rigid modes (M^-1 = D^-1 + P A_c^-1 P^T,
+//     A_c assembled and inverted inside the instance's CTA every OC iteration)
 //   c = f . u                                             (topopt:360,368)
 //   dc_e = -p rho^(p-1) (e0 - emin) u_e^T K0 u_e           (topopt:371-375)
 //   sensitivity filter (topopt:259-279) or the density filter of the 88-line
@@ -31,10 +33,13 @@ namespace {
 
 constexpr double RHO_MIN = 1e-3, RHO_MAX = 1.0, OC_DAMP = 0.5;  // topopt:54-62
 
+constexpr int TP_MAXC = 384;  // coarse unknowns per instance (3 modes x 128 aggregates)
+
 struct TopoInst {
   int nelx, nely, nx, ny, ne, ndof;
   int max_iter, density_filter, has_lift;
-  int64_t eoff, doff, hoff;
+  int ag, nax, nay, nc;  // coarse space: aggregates of ag x ag nodes, nax x nay of them, 3 modes each
+  int64_t eoff, doff, hoff, coff, toff;
   double h, e0, penal, vol_frac, radius, move, emin;
   double ke0[64];  // element stiffness for E = 1, row-major 8 x 8
 };
@@ -51,6 +56,9 @@ struct TopoArgs {
   const double *f, *ulift, *ufix;
   const uint8_t* fixed;
   double *u, *r, *p, *q, *dinv, *b;
+  double* Ac;        // coarse matrix, inverted in place (offset coff, nc x nc)
+  double* Tm;        // per aggregate: 3 x 3 mode transform (offset toff)
+  int coarse;        // 1: two-level preconditioner, 0: Jacobi only
   double* hist;      // compliance history (offset hoff)
   int* last_iters;   // per instance: PCG iterations of the latest solve
   long long* total_iters;
@@ -186,6 +194,231 @@ __device__ __forceinline__ double oc_candidate(double rho, double b, double lamb
   return fmin(fmax(c, lo), hi);
 }
 
+// ---- per-instance aggregation coarse space ----------------------------------------
+// Aggregates are boxes of ag x ag nodes (the last row/column of boxes takes the
+// remainder); each carries the three rigid modes of plane elasticity about the
+// centre of its node box -- x, y translation and rotation (-y, x) --
+// orthonormalised over its free dofs (modes it cannot carry are dropped).
+// Colour of an aggregate = (ax mod 3, ay mod 3): an aggregate has at most one
+// neighbour of each colour, so A_c = P^T K P comes column block by column block
+// from 9 x 3 operator products.
+
+struct AggBox {
+  int i0, i1, j0, j1;
+};
+
+__device__ __forceinline__ AggBox agg_box(const TopoInst& I, int A) {
+  const int ax = A % I.nax, ay = A / I.nax;
+  AggBox b;
+  b.i0 = ax * I.ag;
+  b.i1 = ax == I.nax - 1 ? I.nx - 1 : b.i0 + I.ag - 1;
+  b.j0 = ay * I.ag;
+  b.j1 = ay == I.nay - 1 ? I.ny - 1 : b.j0 + I.ag - 1;
+  return b;
+}
+
+__device__ __forceinline__ int agg_of(const TopoInst& I, int i, int j) {
+  return min(i / I.ag, I.nax - 1) + I.nax * min(j / I.ag, I.nay - 1);
+}
+
+// raw modes of node (i, j) of box b: R[a][k], a = dof component, k = mode
+__device__ __forceinline__ void modes2(const TopoInst& I, const AggBox& b, int i, int j, double (&R)[2][3]) {
+  const double x = (i - 0.5 * (b.i0 + b.i1)) * I.h, y = (j - 0.5 * (b.j0 + b.j1)) * I.h;
+  R[0][0] = 1.0; R[0][1] = 0.0; R[0][2] = -y;
+  R[1][0] = 0.0; R[1][1] = 1.0; R[1][2] = x;
+}
+
+// Orthonormal mode transform of every aggregate (warp per aggregate): Gram
+// matrix over free dofs G = L L^T (modes with no remaining weight dropped),
+// T = L^-T.
+template <int NT>
+__device__ void coarse_transforms(const TopoInst& I, const uint8_t* __restrict__ fixed, double* __restrict__ Tm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int na = I.nax * I.nay;
+  for (int A = warp; A < na; A += NT / 32) {
+    const AggBox b = agg_box(I, A);
+    const int w = b.i1 - b.i0 + 1, cnt = w * (b.j1 - b.j0 + 1);
+    double g[6] = {0, 0, 0, 0, 0, 0};  // 00 01 02 11 12 22
+    for (int t = lane; t < cnt; t += 32) {
+      const int i = b.i0 + t % w, j = b.j0 + t / w, n = j * I.nx + i;
+      double R[2][3];
+      modes2(I, b, i, j, R);
+      for (int c = 0; c < 2; ++c) {
+        if (fixed[2 * n + c]) continue;
+        g[0] += R[c][0] * R[c][0]; g[1] += R[c][0] * R[c][1]; g[2] += R[c][0] * R[c][2];
+        g[3] += R[c][1] * R[c][1]; g[4] += R[c][1] * R[c][2]; g[5] += R[c][2] * R[c][2];
+      }
+    }
+    for (int q = 0; q < 6; ++q)
+      for (int o = 16; o > 0; o >>= 1) g[q] += __shfl_xor_sync(0xffffffffu, g[q], o);
+    if (lane == 0) {
+      const double G[3][3] = {{g[0], g[1], g[2]}, {g[1], g[3], g[4]}, {g[2], g[4], g[5]}};
+      const double tr = g[0] + g[3] + g[5];
+      double L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      bool keep[3];
+      for (int k = 0; k < 3; ++k) {
+        double sk = G[k][k];
+        for (int q = 0; q < k; ++q) sk -= L[k][q] * L[k][q];
+        keep[k] = sk > 1e-10 * tr && tr > 0.0;
+        if (!keep[k]) continue;
+        L[k][k] = sqrt(sk);
+        for (int i2 = k + 1; i2 < 3; ++i2) {
+          double v = G[i2][k];
+          for (int q = 0; q < k; ++q) v -= L[i2][q] * L[k][q];
+          L[i2][k] = v / L[k][k];
+        }
+      }
+      double* T = Tm + (int64_t)A * 9;
+      for (int m = 0; m < 3; ++m) {  // column m of L^-1, then T[k][m] = Linv[m][k]
+        double xv[3];
+        for (int i2 = 0; i2 < 3; ++i2) {
+          if (!keep[i2]) { xv[i2] = 0.0; continue; }
+          double v = (i2 == m) ? 1.0 : 0.0;
+          for (int q = 0; q < i2; ++q) v -= L[i2][q] * xv[q];
+          xv[i2] = v / L[i2][i2];
+        }
+        for (int k = 0; k < 3; ++k) T[m * 3 + k] = keep[m] ? xv[k] : 0.0;  // T^T stored: row m = mode m
+      }
+    }
+  }
+}
+
+// s[k] = sum over aggregate A's nodes of R^T w (raw modes), warp-reduced (all lanes get it).
+__device__ __forceinline__ void agg_moments(const TopoInst& I, int A, const double* __restrict__ w, double (&s)[3]) {
+  const int lane = threadIdx.x & 31;
+  const AggBox b = agg_box(I, A);
+  const int wd = b.i1 - b.i0 + 1, cnt = wd * (b.j1 - b.j0 + 1);
+  s[0] = s[1] = s[2] = 0.0;
+  for (int t = lane; t < cnt; t += 32) {
+    const int i = b.i0 + t % wd, j = b.j0 + t / wd, n = j * I.nx + i;
+    double R[2][3];
+    modes2(I, b, i, j, R);
+    const double2 wn = reinterpret_cast<const double2*>(w)[n];
+    for (int k = 0; k < 3; ++k) s[k] += R[0][k] * wn.x + R[1][k] * wn.y;
+  }
+  for (int k = 0; k < 3; ++k)
+    for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
+}
+
+// A_c = P^T K_FF P, then its inverse in place (Gauss-Jordan; A_c is SPD).
+template <int NT>
+__device__ void coarse_assemble_invert(const TopoInst& I, const double* __restrict__ E,
+                                       const uint8_t* __restrict__ fixed, const double* __restrict__ ke,
+                                       const double* __restrict__ Tm, double* __restrict__ v, double* __restrict__ y,
+                                       double* __restrict__ Ac, double* __restrict__ fcol) {
+  const int nc = I.nc, na = I.nax * I.nay, nn = I.nx * I.ny;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int t = threadIdx.x; t < nc * nc; t += NT) Ac[t] = 0.0;
+  for (int cy = 0; cy < min(3, I.nay); ++cy)
+    for (int cx = 0; cx < min(3, I.nax); ++cx)
+      for (int m = 0; m < 3; ++m) {
+        __syncthreads();
+        for (int n = threadIdx.x; n < nn; n += NT) {  // v = P e_(colour, m), zero on fixed dofs
+          const int i = n % I.nx, j = n / I.nx, A = agg_of(I, i, j);
+          double v0 = 0.0, v1 = 0.0;
+          if ((A % I.nax) % 3 == cx && (A / I.nax) % 3 == cy) {
+            double R[2][3];
+            modes2(I, agg_box(I, A), i, j, R);
+            const double* T = Tm + (int64_t)A * 9 + m * 3;
+            v0 = fixed[2 * n] ? 0.0 : R[0][0] * T[0] + R[0][1] * T[1] + R[0][2] * T[2];
+            v1 = fixed[2 * n + 1] ? 0.0 : R[1][0] * T[0] + R[1][1] * T[1] + R[1][2] * T[2];
+          }
+          reinterpret_cast<double2*>(v)[n] = make_double2(v0, v1);
+        }
+        __syncthreads();
+        apply_k<NT>(I, E, v, y, fixed, true, ke);
+        __syncthreads();
+        for (int A = warp; A < na; A += NT / 32) {
+          const int ax = A % I.nax, ay = A / I.nax;
+          int jx = -1, jy = -1;
+          for (int o = -1; o <= 1; ++o) {
+            if (ax + o >= 0 && ax + o < I.nax && (ax + o) % 3 == cx) jx = ax + o;
+            if (ay + o >= 0 && ay + o < I.nay && (ay + o) % 3 == cy) jy = ay + o;
+          }
+          if (jx < 0 || jy < 0) continue;
+          const int J = jy * I.nax + jx;
+          double sk[3];
+          agg_moments(I, A, y, sk);
+          if (lane < 3) {
+            const double* T = Tm + (int64_t)A * 9 + lane * 3;  // mode `lane` of A
+            Ac[(int64_t)(A * 3 + lane) * nc + J * 3 + m] = T[0] * sk[0] + T[1] * sk[1] + T[2] * sk[2];
+          }
+        }
+      }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nc; i += NT)
+    if (Ac[(int64_t)i * nc + i] == 0.0) Ac[(int64_t)i * nc + i] = 1.0;  // dropped modes
+  for (int k = 0; k < nc; ++k) {  // in-place Gauss-Jordan inversion
+    __syncthreads();
+    for (int i = threadIdx.x; i < nc; i += NT) fcol[i] = Ac[(int64_t)i * nc + k];
+    __syncthreads();
+    const double piv = fcol[k];
+    for (int j = threadIdx.x; j < nc; j += NT)
+      Ac[(int64_t)k * nc + j] = (j == k ? 1.0 : Ac[(int64_t)k * nc + j]) / piv;
+    __syncthreads();
+    for (int t = threadIdx.x; t < nc * nc; t += NT) {
+      const int i = t / nc, j = t % nc;
+      if (i == k) continue;
+      const double akj = Ac[(int64_t)k * nc + j];
+      Ac[t] = (j == k ? 0.0 : Ac[t]) - fcol[i] * akj;
+    }
+  }
+  __syncthreads();
+}
+
+// uc = A_c^-1 P^T r and c_A = T_A uc_A (raw-mode coefficients per aggregate) into cm.
+template <int NT>
+__device__ void coarse_solve(const TopoInst& I, const double* __restrict__ Tm, const double* __restrict__ Ainv,
+                             const double* __restrict__ r, double* __restrict__ yc, double* __restrict__ uc,
+                             double* __restrict__ cm) {
+  const int nc = I.nc, na = I.nax * I.nay;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  for (int A = warp; A < na; A += NT / 32) {
+    double sk[3];
+    agg_moments(I, A, r, sk);
+    if (lane < 3) {
+      const double* T = Tm + (int64_t)A * 9 + lane * 3;
+      yc[A * 3 + lane] = T[0] * sk[0] + T[1] * sk[1] + T[2] * sk[2];
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nc; i += NT) {
+    const double* row = Ainv + (int64_t)i * nc;
+    double sum = 0.0;
+    for (int j = 0; j < nc; ++j) sum += row[j] * yc[j];
+    uc[i] = sum;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < na * 3; t += NT) {  // raw-mode coefficients: sum_m T[m][k] uc[m]
+    const int A = t / 3, k = t % 3;
+    const double* T = Tm + (int64_t)A * 9;
+    cm[t] = T[0 * 3 + k] * uc[A * 3 + 0] + T[1 * 3 + k] * uc[A * 3 + 1] + T[2 * 3 + k] * uc[A * 3 + 2];
+  }
+  __syncthreads();
+}
+
+// z = D^-1 r + P uc (cm holds the raw-mode coefficients); returns this thread's part of r.z
+template <int NT>
+__device__ double two_level_z(const TopoInst& I, const double* __restrict__ r, const double* __restrict__ dinv,
+                              const double* __restrict__ cm, double* __restrict__ z) {
+  double rz = 0.0;
+  for (int n = threadIdx.x; n < I.nx * I.ny; n += NT) {
+    const int i = n % I.nx, j = n / I.nx, A = agg_of(I, i, j);
+    double R[2][3];
+    modes2(I, agg_box(I, A), i, j, R);
+    const double2 rn = reinterpret_cast<const double2*>(r)[n];
+    const double2 dn = reinterpret_cast<const double2*>(dinv)[n];
+    const double c0 = cm[A * 3], c1 = cm[A * 3 + 1], c2 = cm[A * 3 + 2];
+    // fixed dofs: dinv = 0 and r = 0, and P is zero there (v is masked)
+    const double z0 = dn.x * rn.x + (dn.x != 0.0 ? R[0][0] * c0 + R[0][1] * c1 + R[0][2] * c2 : 0.0);
+    const double z1 = dn.y * rn.y + (dn.y != 0.0 ? R[1][0] * c0 + R[1][1] * c1 + R[1][2] * c2 : 0.0);
+    reinterpret_cast<double2*>(z)[n] = make_double2(z0, z1);
+    rz += rn.x * z0 + rn.y * z1;
+  }
+  return rz;
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT, 1) topo_iteration(TopoArgs a) {
   __shared__ double ke[64];
@@ -248,18 +481,34 @@ __global__ void __launch_bounds__(NT, 1) topo_iteration(TopoArgs a) {
     for (int d = threadIdx.x; d < nd; d += NT) b[d] = fixed[d] ? 0.0 : f[d];
   }
   __syncthreads();
-  // r = b - K x0 (warm start), p = D^-1 r
+  // two-level preconditioner (per-instance coarse space): transforms once, A_c^-1 per OC iteration
+  __shared__ double yc[TP_MAXC], uc[TP_MAXC], cm[TP_MAXC];
+  const bool two = a.coarse && I.nc > 0;
+  double* Ac = a.Ac + I.coff;
+  double* Tm = a.Tm + I.toff;
+  if (two) {
+    if (a.iter == 0) coarse_transforms<NT>(I, fixed, Tm);
+    __syncthreads();
+    coarse_assemble_invert<NT>(I, E, fixed, ke, Tm, p, q, Ac, yc);
+  }
+  // r = b - K x0 (warm start), z = M r, p = z
   apply_k<NT>(I, E, u, q, fixed, true, ke);
   __syncthreads();
   double rz = 0.0, rr = 0.0, bb = 0.0;
   for (int d = threadIdx.x; d < nd; d += NT) {
     const double rd = b[d] - q[d];
     r[d] = rd;
-    const double z = dinv[d] * rd;
-    p[d] = z;
-    rz += rd * z;
     rr += rd * rd;
     bb += b[d] * b[d];
+    if (!two) {
+      const double z = dinv[d] * rd;
+      p[d] = z;
+      rz += rd * z;
+    }
+  }
+  if (two) {
+    coarse_solve<NT>(I, Tm, Ac, r, yc, uc, cm);
+    rz = two_level_z<NT>(I, r, dinv, cm, p);
   }
   block_sum2<NT>(rz, rr, red);
   bb = block_sum<NT>(bb, red);
@@ -279,16 +528,25 @@ __global__ void __launch_bounds__(NT, 1) topo_iteration(TopoArgs a) {
       u[d] += alpha * p[d];
       const double rd = r[d] - alpha * q[d];
       r[d] = rd;
-      rzn += rd * dinv[d] * rd;
+      if (!two) rzn += rd * dinv[d] * rd;
       rrn += rd * rd;
     }
     block_sum2<NT>(rzn, rrn, red);
     ++it;
     conv = rrn <= stop;
     if (conv) break;
-    const double beta = rzn / rz;
-    rz = rzn;
-    for (int d = threadIdx.x; d < nd; d += NT) p[d] = dinv[d] * r[d] + beta * p[d];
+    if (two) {  // z = D^-1 r + P A_c^-1 P^T r into q
+      coarse_solve<NT>(I, Tm, Ac, r, yc, uc, cm);
+      rzn = two_level_z<NT>(I, r, dinv, cm, q);
+      rzn = block_sum<NT>(rzn, red);
+      const double beta = rzn / rz;
+      rz = rzn;
+      for (int d = threadIdx.x; d < nd; d += NT) p[d] = q[d] + beta * p[d];
+    } else {
+      const double beta = rzn / rz;
+      rz = rzn;
+      for (int d = threadIdx.x; d < nd; d += NT) p[d] = dinv[d] * r[d] + beta * p[d];
+    }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
@@ -452,7 +710,8 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
   const double tol = opts && opts->rel_tol > 0 ? opts->rel_tol : 1e-10;
   const int max_pcg = opts && opts->max_pcg_iter > 0 ? opts->max_pcg_iter : 50000;
   std::vector<TopoInst> inst(n);
-  int64_t eoff = 0, doff = 0, hoff = 0;
+  int64_t eoff = 0, doff = 0, hoff = 0, coff = 0, toff = 0;
+  const bool two_level = !(opts && opts->plain_jacobi);
   int launches = 0;
   for (int k = 0; k < n; ++k) {
     const tptfem_topopt_instance& P = in[k];
@@ -471,6 +730,20 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
     I.h = P.h; I.e0 = P.e0; I.penal = P.penal; I.vol_frac = P.vol_frac; I.radius = P.filter_radius;
     I.move = P.move_limit; I.emin = P.emin;
     element_stiffness_unit(P.nu, P.h, I.ke0);
+    // coarse space: about 48 aggregates of ag x ag nodes (at least 4 x 4)
+    I.ag = std::max(4, (int)std::ceil(std::sqrt((double)I.nx * I.ny / 48.0)));
+    I.nax = std::max(1, I.nx / I.ag);
+    I.nay = std::max(1, I.ny / I.ag);
+    while (3 * I.nax * I.nay > TP_MAXC) {
+      ++I.ag;
+      I.nax = std::max(1, I.nx / I.ag);
+      I.nay = std::max(1, I.ny / I.ag);
+    }
+    I.nc = two_level ? 3 * I.nax * I.nay : 0;
+    I.coff = coff;
+    I.toff = toff;
+    coff += (int64_t)I.nc * I.nc;
+    toff += (int64_t)I.nax * I.nay * 9;
     eoff += I.ne;
     doff += I.ndof;
     hoff += P.max_iter + 1;
@@ -521,13 +794,15 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
   DevBuf<TopoInst> d_inst;
   DevBuf<int> d_order, d_last, d_flags;
   DevBuf<long long> d_total;
-  DevBuf<double> ex, ephys, eE, eraw, esens, exnew, df, dlift, dfix, du, dr, dp, dq, ddinv, db, dhist;
+  DevBuf<double> ex, ephys, eE, eraw, esens, exnew, df, dlift, dfix, du, dr, dp, dq, ddinv, db, dhist, dAc, dTm;
   DevBuf<uint8_t> dfixed;
   d_inst.alloc(n, s); d_order.alloc(n, s); d_last.alloc(n, s); d_flags.alloc(n, s); d_total.alloc(n, s);
   for (auto* v : {&ex, &ephys, &eE, &eraw, &esens, &exnew}) v->alloc(std::max<int64_t>(eoff, 1), s);
   for (auto* v : {&df, &dlift, &dfix, &du, &dr, &dp, &dq, &ddinv, &db}) v->alloc(std::max<int64_t>(doff, 1), s);
   dfixed.alloc(std::max<int64_t>(doff, 1), s);
   dhist.alloc(std::max<int64_t>(hoff, 1), s);
+  dAc.alloc(std::max<int64_t>(coff, 1), s);
+  dTm.alloc(std::max<int64_t>(toff, 1), s);
   d_inst.upload(inst.data(), n);
   d_order.upload(order.data(), n);
   df.upload(f.data(), doff);
@@ -542,6 +817,7 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
   a.f = df.p; a.ulift = dlift.p; a.ufix = dfix.p; a.fixed = dfixed.p;
   a.u = du.p; a.r = dr.p; a.p = dp.p; a.q = dq.p; a.dinv = ddinv.p; a.b = db.p;
   a.hist = dhist.p; a.last_iters = d_last.p; a.total_iters = d_total.p; a.flags = d_flags.p;
+  a.Ac = dAc.p; a.Tm = dTm.p; a.coarse = two_level ? 1 : 0;
 
   cudaEvent_t ev0 = ctx->ev[0], ev1 = ctx->ev[1], ev2 = ctx->ev[2];
   float tune_ms = 0.f;
@@ -550,7 +826,8 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
                ? opts->block_threads : 0;
   uint64_t sig = 1469598103934665603ull;
   for (int k = 0; k < n; ++k)
-    for (uint64_t v : {(uint64_t)inst[k].nelx, (uint64_t)inst[k].nely, (uint64_t)inst[k].density_filter})
+    for (uint64_t v : {(uint64_t)inst[k].nelx, (uint64_t)inst[k].nely, (uint64_t)inst[k].density_filter,
+                       (uint64_t)inst[k].nc})
       sig = (sig ^ v) * 1099511628211ull;
   if (!nt) {
     auto it = ctx->topo_tuned.find(sig);

@@ -52,7 +52,7 @@ class TopoptInstance(C.Structure):
 
 class TopoptOpts(C.Structure):
     _fields_ = [("rel_tol", C.c_double), ("max_pcg_iter", C.c_int32), ("block_threads", C.c_int32),
-                ("use_graph", C.c_int32), ("reserved", C.c_int32)]
+                ("use_graph", C.c_int32), ("plain_jacobi", C.c_int32)]
 
 
 class TopoptStats(C.Structure):

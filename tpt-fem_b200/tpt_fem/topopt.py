@@ -84,7 +84,7 @@ def element_stiffness_unit(nu, h):
     return ke.reshape(8, 8)
 
 
-def topopt_batch(ctx, problems, rel_tol=1e-10, max_pcg_iter=0, block_threads=0, use_graph=True):
+def topopt_batch(ctx, problems, rel_tol=1e-10, max_pcg_iter=0, block_threads=0, use_graph=True, plain_jacobi=False):
     """Run [(TopOptParams, f, bcs), ...] (f/bcs None: cantilever_load) on ctx's GPU.
 
     Returns ([TopOptResult, ...], stats dict)."""
@@ -119,7 +119,8 @@ def topopt_batch(ctx, problems, rel_tol=1e-10, max_pcg_iter=0, block_threads=0, 
     nden = sum(P.grid.n_elem() for P, _, _ in problems)
     comp = np.zeros(ncomp)
     dens = np.zeros(nden)
-    opts = N.TopoptOpts(float(rel_tol), int(max_pcg_iter), int(block_threads), int(bool(use_graph)), 0)
+    opts = N.TopoptOpts(float(rel_tol), int(max_pcg_iter), int(block_threads), int(bool(use_graph)),
+                        int(bool(plain_jacobi)))
     st = N.TopoptStats()
     ctx.check(ctx.lib.tptfem_topopt_batch(ctx.h, C.cast(arr, C.c_void_p), n, C.byref(opts), N.ptr(comp), N.ptr(dens),
                                           C.byref(st)))
