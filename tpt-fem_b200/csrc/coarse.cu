@@ -33,7 +33,8 @@ constexpr int CS_MAX_COARSE = 8192;
 
 __device__ __forceinline__ int colour_of(const int* b) { return (b[0] % 3) + 3 * (b[1] % 3) + 9 * (b[2] % 3); }
 
-// V[(g dpn + a) nm + m] = (P e_{c, m})_{g,a} for every mode m at once.
+// V[(g dpn + a) nm + m] = (P e_{c, m})_{g,a} for every mode m at once
+// (colour < 0: every colour, i.e. P itself).
 template <int DPN>
 __global__ void cs_fill_modes(int ngroups, const int* __restrict__ agg, const int* __restrict__ abin,
                               const float* __restrict__ y, const double* __restrict__ T, int colour,
@@ -43,7 +44,7 @@ __global__ void cs_fill_modes(int ngroups, const int* __restrict__ agg, const in
   if (g >= ngroups) return;
   const int I = agg[g];
   double* out = V + (int64_t)g * DPN * NM;
-  if (colour_of(abin + 3 * I) != colour) {
+  if (colour >= 0 && colour_of(abin + 3 * I) != colour) {
 #pragma unroll
     for (int q = 0; q < DPN * NM; ++q) out[q] = 0.0;
     return;
@@ -158,39 +159,6 @@ __device__ __forceinline__ double agg_moment(int I, int mp, int nm, const int* _
   return x;
 }
 
-// Column blocks (J, all m) of A_c from the moments of W = A P E_c.
-__global__ void cs_columns_modes(int na, int nm, const int* __restrict__ abin, const int* __restrict__ bin2agg,
-                                 int bx, int by, int bz, const int* __restrict__ aseg, const double* __restrict__ smom,
-                                 const double* __restrict__ T, int colour, double* __restrict__ Ac, int nc) {
-  const int I = blockIdx.x * blockDim.x + threadIdx.x;
-  if (I >= na) return;
-  const int nbin[3] = {bx, by, bz};
-  int jb[3];
-  for (int d = 0; d < 3; ++d) {
-    const int want = (colour / (d == 0 ? 1 : (d == 1 ? 3 : 9))) % 3;
-    const int b = abin[3 * I + d];
-    jb[d] = -1;
-    for (int o = -1; o <= 1; ++o) {
-      const int c = b + o;
-      if (c >= 0 && c < nbin[d] && c % 3 == want) jb[d] = c;
-    }
-    if (jb[d] < 0) return;
-  }
-  const int J = bin2agg[((int64_t)jb[2] * by + jb[1]) * bx + jb[0]];
-  if (J < 0) return;
-  const double* t = T + (int64_t)I * nm * nm;
-  for (int m = 0; m < nm; ++m)
-    for (int mp = 0; mp < nm; ++mp) {
-      double x = 0.0;
-      for (int k = 0; k < nm; ++k) {
-        double sk = 0.0;
-        for (int q = aseg[I]; q < aseg[I + 1]; ++q) sk += smom[((int64_t)q * nm + m) * nm + k];
-        x += t[k * nm + mp] * sk;
-      }
-      Ac[((int64_t)I * nm + mp) * nc + (int64_t)J * nm + m] = x;
-    }
-}
-
 // yc = P^T r from the segment moments.
 __global__ void cs_yc(int na, int nm, const int* __restrict__ aseg, const double* __restrict__ smom,
                       const double* __restrict__ T, double* __restrict__ yc) {
@@ -212,6 +180,57 @@ __global__ void __launch_bounds__(CS_THREADS) cs_gemv(int nc, const double* __re
   for (int j = lane; j < nc; j += 32) s += (double)a[j] * ys[j];
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   if (lane == 0) uc[row] = s;
+}
+
+// cm = T uc per aggregate (raw-mode coefficients of P uc).
+__global__ void cs_raw(int na, int nm, const double* __restrict__ T, const double* __restrict__ uc,
+                       double* __restrict__ cm) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= na * nm) return;
+  const int I = t / nm, k = t % nm;
+  const double* tI = T + (int64_t)I * nm * nm + k * nm;
+  double x = 0.0;
+  for (int m = 0; m < nm; ++m) x += tI[m] * uc[(int64_t)I * nm + m];
+  cm[t] = x;
+}
+
+__global__ void cs_group_colour(int ngroups, const int* __restrict__ agg, const int* __restrict__ abin,
+                                unsigned char* __restrict__ gcol) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < ngroups) gcol[g] = (unsigned char)colour_of(abin + 3 * agg[g]);
+}
+
+// Column blocks (J, m) of A_c, one thread per (I, m, mp): J is I's unique
+// neighbour (itself included) of the colour; the moments of W = A P E_colour
+// give entry (I mp, J m).
+__global__ void cs_columns_par(int na, int nm, const int* __restrict__ abin, const int* __restrict__ bin2agg, int bx,
+                               int by, int bz, const int* __restrict__ aseg, const double* __restrict__ smom,
+                               const double* __restrict__ T, int colour, double* __restrict__ Ac, int nc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= na * nm * nm) return;
+  const int I = t / (nm * nm), m = (t / nm) % nm, mp = t % nm;
+  const int nbin[3] = {bx, by, bz};
+  int jb[3];
+  for (int d = 0; d < 3; ++d) {
+    const int want = (colour / (d == 0 ? 1 : (d == 1 ? 3 : 9))) % 3;
+    const int b = abin[3 * I + d];
+    jb[d] = -1;
+    for (int o = -1; o <= 1; ++o) {
+      const int c = b + o;
+      if (c >= 0 && c < nbin[d] && c % 3 == want) jb[d] = c;
+    }
+    if (jb[d] < 0) return;
+  }
+  const int J = bin2agg[((int64_t)jb[2] * by + jb[1]) * bx + jb[0]];
+  if (J < 0) return;
+  const double* tI = T + (int64_t)I * nm * nm;
+  double x = 0.0;
+  for (int k = 0; k < nm; ++k) {
+    double sk = 0.0;
+    for (int q = aseg[I]; q < aseg[I + 1]; ++q) sk += smom[((int64_t)q * nm + m) * nm + k];
+    x += tI[k * nm + mp] * sk;
+  }
+  Ac[((int64_t)I * nm + mp) * nc + (int64_t)J * nm + m] = x;
 }
 
 // Rows/columns of dropped modes are zero: put 1 on their diagonal.
@@ -437,6 +456,18 @@ bool coarse_build(SystemData& S, int target) {
   C.Ainv.alloc((size_t)C.nc * C.nc, s);
   C.yc.alloc(C.nc, s);
   C.uc.alloc(C.nc, s);
+  C.cm.alloc(C.nc, s);
+  C.Pfull.alloc((size_t)S.n_free * nm, s);
+  C.gcolour.alloc(ng, s);
+  cs_group_colour<<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, C.agg.p, C.abin.p, C.gcolour.p);
+  TPT_CHECK_LAUNCH();
+#define TPT_CS_P(D)                                                                                       \
+  cs_fill_modes<D><<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, C.agg.p, C.abin.p, C.y.p, C.T.p, -1, C.Pfull.p); \
+  TPT_CHECK_LAUNCH();
+  if (dpn == 3) { TPT_CS_P(3) }
+  else if (dpn == 2) { TPT_CS_P(2) }
+  else { TPT_CS_P(1) }
+#undef TPT_CS_P
   TPT_CUDA(cudaStreamSynchronize(s));  // host vectors above are released on return
   C.state = 1;
   return true;
@@ -447,10 +478,9 @@ bool coarse_assemble(SystemData& S) {
   C.ready = false;
   if (C.state != 1) return false;
   cudaStream_t s = S.ctx->stream;
-  const int ng = S.nb.ngroups, dpn = S.dpn, nc = C.nc;
+  const int dpn = S.dpn, nc = C.nc;
   C.Ac.zero();
-  DevBuf<double> v, w, mom;
-  v.alloc(S.n_free * C.nm, s);
+  DevBuf<double> w, mom;
   w.alloc(S.n_free * C.nm, s);
   mom.alloc((size_t)C.nseg * C.nm * C.nm, s);
   const int ncx = std::min(3, C.bins[0]), ncy = std::min(3, C.bins[1]), ncz = std::min(3, C.bins[2]);
@@ -458,19 +488,17 @@ bool coarse_assemble(SystemData& S) {
     for (int cy = 0; cy < ncy; ++cy)
       for (int cx = 0; cx < ncx; ++cx) {
         const int colour = cx + 3 * cy + 9 * cz;
+        nb_operator_apply_modes(S, C.Pfull.p, w.p, C.gcolour.p, colour);
 #define TPT_CS_COL(D)                                                                                             \
-  cs_fill_modes<D><<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, C.agg.p, C.abin.p, C.y.p, C.T.p, colour, v.p);        \
-  TPT_CHECK_LAUNCH();                                                                                             \
-  nb_operator_apply_modes(S, v.p, w.p);                                                                           \
   cs_moments_modes<D><<<C.nseg, CS_THREADS, 0, s>>>(C.sbeg.p, C.send.p, C.alist.p, C.y.p, w.p, mom.p);           \
   TPT_CHECK_LAUNCH();
         if (dpn == 3) { TPT_CS_COL(3) }
         else if (dpn == 2) { TPT_CS_COL(2) }
         else { TPT_CS_COL(1) }
 #undef TPT_CS_COL
-        cs_columns_modes<<<blocks_for(C.na), CS_THREADS, 0, s>>>(C.na, C.nm, C.abin.p, C.bin2agg.p, C.bins[0],
-                                                                 C.bins[1], C.bins[2], C.aseg.p, mom.p, C.T.p,
-                                                                 colour, C.Ac.p, nc);
+        cs_columns_par<<<blocks_for((int64_t)C.na * C.nm * C.nm), CS_THREADS, 0, s>>>(
+            C.na, C.nm, C.abin.p, C.bin2agg.p, C.bins[0], C.bins[1], C.bins[2], C.aseg.p, mom.p, C.T.p, colour,
+            C.Ac.p, nc);
         TPT_CHECK_LAUNCH();
       }
   cs_fix_diag<<<blocks_for(nc), CS_THREADS, 0, s>>>(nc, C.Ac.p);
@@ -521,6 +549,8 @@ void coarse_restrict_solve(const SystemData& S, const double* r, cudaStream_t s)
   TPT_CHECK_LAUNCH();
   cs_gemv<<<(C.nc + CS_THREADS / 32 - 1) / (CS_THREADS / 32), CS_THREADS, (size_t)C.nc * sizeof(double), s>>>(
       C.nc, C.yc.p, C.Ainv.p, C.uc.p);
+  TPT_CHECK_LAUNCH();
+  cs_raw<<<blocks_for(C.nc), CS_THREADS, 0, s>>>(C.na, C.nm, C.T.p, C.uc.p, C.cm.p);
   TPT_CHECK_LAUNCH();
 }
 

@@ -221,59 +221,73 @@ __global__ void lf_head_edges(int n, const float* __restrict__ prm, Off o, const
 // Kaporin terms, per row i with pattern P = (lower pattern of i, i) (ascending,
 // i last) and g = (L^_i,P, 1):  w = A^[P,P] g,  q_i = g . w  (FP64 accumulation),
 // sig_i = q_i^-1/2,  d loss / d L^_ij = 2 w_j / (n q_i),  loss += log q_i.
-// Rows longer than LF_MAXM set bit 0 of *flag, a non-positive q sets bit 1.
-__global__ void lf_kaporin(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                           const float* __restrict__ ahat, const int* __restrict__ lrp, const int* __restrict__ lci,
-                           const float* __restrict__ lhat, float* __restrict__ sig, float* __restrict__ dlhat,
-                           double* __restrict__ loss, int* __restrict__ flag) {
-  __shared__ double sh[LF_THREADS];
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per row: lanes take pattern entries a and a + 32 and merge row
+// P[a] of A^ with the pattern.  Rows longer than LF_MAXM set bit 0 of *flag,
+// a non-positive q sets bit 1.
+__global__ void __launch_bounds__(LF_THREADS) lf_kaporin_warp(int n, const int* __restrict__ rp,
+                                                              const int* __restrict__ ci,
+                                                              const float* __restrict__ ahat,
+                                                              const int* __restrict__ lrp,
+                                                              const int* __restrict__ lci,
+                                                              const float* __restrict__ lhat,
+                                                              float* __restrict__ sig, float* __restrict__ dlhat,
+                                                              double* __restrict__ loss, int* __restrict__ flag) {
+  constexpr int WPB = LF_THREADS / 32;
+  __shared__ int Ps[WPB][LF_MAXM];
+  __shared__ double gs[WPB][LF_MAXM];
+  __shared__ double lsum[WPB];
+  const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+  const int i = blockIdx.x * WPB + wb;
   double lq = 0.0;
   if (i < n) {
     const int l0 = lrp[i], m = lrp[i + 1] - l0 + 1;
     if (m > LF_MAXM) {
-      atomicOr(flag, 1);
-      sig[i] = 1.f;
+      if (lane == 0) { atomicOr(flag, 1); sig[i] = 1.f; }
     } else {
-      int P[LF_MAXM];
-      double g[LF_MAXM], w[LF_MAXM];
-      for (int a = 0; a < m - 1; ++a) { P[a] = lci[l0 + a]; g[a] = lhat[l0 + a]; }
-      P[m - 1] = i;
-      g[m - 1] = 1.0;
-      double q = 0.0;
-      for (int a = 0; a < m; ++a) {
-        const int r = P[a];
+      for (int a = lane; a < m - 1; a += 32) { Ps[wb][a] = lci[l0 + a]; gs[wb][a] = lhat[l0 + a]; }
+      if (lane == 0) { Ps[wb][m - 1] = i; gs[wb][m - 1] = 1.0; }
+      __syncwarp();
+      double w[2] = {0.0, 0.0}, qp = 0.0;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int a = lane + 32 * h;
+        if (a >= m) continue;
+        const int r = Ps[wb][a];
         int k = rp[r], b = 0;
         const int ke = rp[r + 1];
-        double s = 0.0;
+        double sacc = 0.0;
         while (k < ke && b < m) {  // merge of two ascending lists
-          const int c = ci[k];
-          if (c == P[b]) { s += (double)ahat[k] * g[b]; ++k; ++b; }
-          else if (c < P[b]) ++k;
+          const int c = ci[k], pb = Ps[wb][b];
+          if (c == pb) { sacc += (double)ahat[k] * gs[wb][b]; ++k; ++b; }
+          else if (c < pb) ++k;
           else ++b;
         }
-        w[a] = s;
-        q += g[a] * s;
+        w[h] = sacc;
+        qp += gs[wb][a] * sacc;
       }
-      if (!(q > 0.0)) {
-        atomicOr(flag, 2);
-        sig[i] = 1.f;
+      for (int o = 16; o > 0; o >>= 1) qp += __shfl_xor_sync(0xffffffffu, qp, o);
+      if (!(qp > 0.0)) {
+        if (lane == 0) { atomicOr(flag, 2); sig[i] = 1.f; }
       } else {
-        lq = log(q);
-        sig[i] = (float)(1.0 / sqrt(q));
-        if (dlhat)
-          for (int a = 0; a < m - 1; ++a) dlhat[l0 + a] = (float)(2.0 * w[a] / ((double)n * q));
+        if (lane == 0) { lq = log(qp); sig[i] = (float)(1.0 / sqrt(qp)); }
+        if (dlhat) {
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int a = lane + 32 * h;
+            if (a < m - 1) dlhat[l0 + a] = (float)(2.0 * w[h] / ((double)n * qp));
+          }
+        }
       }
     }
   }
   if (!loss) return;
-  sh[threadIdx.x] = lq;
+  if (lane == 0) lsum[wb] = lq;
   __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
-    __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q2 = 0; q2 < WPB; ++q2) t += lsum[q2];
+    atomicAdd(loss, t);
   }
-  if (threadIdx.x == 0) atomicAdd(loss, sh[0]);
 }
 
 // ---- backward -------------------------------------------------------------------------
@@ -566,8 +580,9 @@ void forward_impl(const SystemData& S, const FsaiFactor& F, LfGraph& G, const fl
   lf_head_edges<<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o, F.rp.p, F.ci.p, G.al.p, G.P.p, G.Q.p, G.lhat.p);
   TPT_CHECK_LAUNCH();
   G.flag.zero();
-  lf_kaporin<<<blocks(n), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, G.ahat.p, F.rp.p, F.ci.p, G.lhat.p, G.sig.p,
-                                              dlhat, loss, G.flag.p);
+  lf_kaporin_warp<<<ceil_div(n, LF_THREADS / 32), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, G.ahat.p, F.rp.p,
+                                                                      F.ci.p, G.lhat.p, G.sig.p, dlhat, loss,
+                                                                      G.flag.p);
   TPT_CHECK_LAUNCH();
 }
 

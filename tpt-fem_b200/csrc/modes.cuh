@@ -30,8 +30,7 @@ __device__ __forceinline__ void mode_rows(const float* __restrict__ y3, double (
 struct CoarseArgs {
   const int* agg = nullptr;    // per group: aggregate
   const float* y = nullptr;    // per group: relative position (3 floats)
-  const double* T = nullptr;   // per aggregate: nm x nm mode transform
-  const double* uc = nullptr;  // coarse solution (nm per aggregate)
+  const double* cm = nullptr;  // per aggregate: raw-mode coefficients T uc (nm values)
 };
 
 }  // namespace tptfem

@@ -147,7 +147,9 @@ __global__ void __launch_bounds__(SPMV_THREADS, 6) nb_spmv_sym(int ngroups, cons
 
 // Y = K X for NV interleaved vectors (X[(row) * NV + v]) from the symmetric
 // half storage: each block is read once for all vectors.  Used to form
-// coarse-space products P^T A P (set-up only, not on the iteration path).
+// coarse-space products P^T A P (set-up only, not on the iteration path):
+// with gcol set, the rows of groups whose colour differs from `colour` count
+// as zero, so X can hold P for every colour at once.
 template <int DPN, int NV>
 __global__ void __launch_bounds__(SPMV_THREADS) nb_spmv_sym_multi(int ngroups, const int* __restrict__ lcptr,
                                                                   const int* __restrict__ lcol,
@@ -157,7 +159,9 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_spmv_sym_multi(int ngroups, c
                                                                   const int* __restrict__ ucol,
                                                                   const int* __restrict__ ubase,
                                                                   const double* __restrict__ X,
-                                                                  double* __restrict__ Y) {
+                                                                  double* __restrict__ Y,
+                                                                  const unsigned char* __restrict__ gcol,
+                                                                  int colour) {
   constexpr int D2 = DPN * DPN;
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -172,6 +176,7 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_spmv_sym_multi(int ngroups, c
 #pragma unroll
       for (int v = 0; v < NV; ++v) acc[a][v] = 0.0;
     auto add = [&](const double (&blk)[D2], int J, bool transposed) {
+      if (gcol && __ldg(gcol + J) != colour) return;
 #pragma unroll
       for (int b = 0; b < DPN; ++b)
 #pragma unroll
@@ -326,19 +331,12 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_fsai_upper_rz(int ngroups, co
 #pragma unroll
         for (int b = 0; b < DPN; ++b) acc[a] += (double)v[a * DPN + b] * xj[b];
     }
-    if (cs.agg) {  // z_g += R_g T_I uc_I
+    if (cs.agg) {  // z_g += R_g cm_I, cm_I = T_I uc_I
       constexpr int NM = rigid_modes(DPN);
-      const int I = cs.agg[g];
-      const double* tI = cs.T + (int64_t)I * NM * NM;
-      const double* uI = cs.uc + (int64_t)I * NM;
+      const double* cI = cs.cm + (int64_t)cs.agg[g] * NM;
       double cm[NM];
 #pragma unroll
-      for (int k = 0; k < NM; ++k) {
-        double x = 0.0;
-#pragma unroll
-        for (int m = 0; m < NM; ++m) x += tI[k * NM + m] * uI[m];
-        cm[k] = x;
-      }
+      for (int k = 0; k < NM; ++k) cm[k] = __ldg(cI + k);
       double R[DPN][NM];
       mode_rows<DPN>(cs.y + 3 * (int64_t)g, R);
 #pragma unroll

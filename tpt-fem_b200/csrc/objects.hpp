@@ -118,6 +118,9 @@ struct CoarseSpace {
   DevBuf<double> Ac;            // nc x nc, then its Cholesky factor / inverse (FP64)
   DevBuf<float> Ainv;           // nc x nc inverse (FP32, symmetric, row-major)
   DevBuf<double> yc, uc;        // coarse vectors
+  DevBuf<double> cm;            // per aggregate: raw-mode coefficients of the prolongation, T uc
+  DevBuf<double> Pfull;         // P itself: per dof its nm orthonormal-mode values (geometry only)
+  DevBuf<unsigned char> gcolour;  // per group: colour of its aggregate
   bool ready = false;           // Ainv holds the inverse for the current values
 };
 
@@ -188,8 +191,9 @@ void coarse_restrict_solve(const SystemData& S, const double* r, cudaStream_t s)
 void coarse_download(const SystemData& S, int* na, int* nm, double* Ainv_or_null);  // FP32 inverse, widened
 // solver.cu: y = A x with the system's node-block operator (no reduction)
 void nb_operator_apply(SystemData& S, const double* x, double* y);
-// Y = A X for the rigid_modes(dpn) interleaved vectors of X (symmetric half storage)
-void nb_operator_apply_modes(SystemData& S, const double* X, double* Y);
+// Y = A X for the rigid_modes(dpn) interleaved vectors of X (symmetric half
+// storage); with gcol, only groups of colour `colour` contribute
+void nb_operator_apply_modes(SystemData& S, const double* X, double* Y, const unsigned char* gcol, int colour);
 
 // solver.cu
 int64_t system_fsai_classic(SystemData& S);  // builds (once) the classic factor; -1 on failure

@@ -308,8 +308,7 @@ int select_coarse(SystemData& S, Engine<double>& E, const tptfem_solver_opts& o,
     if (want) {
       E.cargs.agg = S.coarse.agg.p;
       E.cargs.y = S.coarse.y.p;
-      E.cargs.T = S.coarse.T.p;
-      E.cargs.uc = S.coarse.uc.p;
+      E.cargs.cm = S.coarse.cm.p;
     }
     if (E.exec) { cudaGraphExecDestroy(E.exec); E.exec = nullptr; }
   }
@@ -804,20 +803,20 @@ void nb_operator_apply(SystemData& S, const double* x, double* y) {
   TPT_CHECK_LAUNCH();
 }
 
-void nb_operator_apply_modes(SystemData& S, const double* X, double* Y) {
+void nb_operator_apply_modes(SystemData& S, const double* X, double* Y, const unsigned char* gcol, int colour) {
   nb_build_sym(S);
   const NbSell& N = S.nb;
   cudaStream_t s = S.ctx->stream;
   const int g = std::max(1, std::min(sm_count() * NB_BLOCKS_PER_SM, ceil_div((int64_t)N.nchunks * 32, SPMV_THREADS)));
   if (N.dpn == 3)
     nb_spmv_sym_multi<3, 6><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.ks_lval.p, N.ks_diag.p,
-                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y);
+                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y, gcol, colour);
   else if (N.dpn == 2)
     nb_spmv_sym_multi<2, 3><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.ks_lval.p, N.ks_diag.p,
-                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y);
+                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y, gcol, colour);
   else
     nb_spmv_sym_multi<1, 1><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.ks_lval.p, N.ks_diag.p,
-                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y);
+                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y, gcol, colour);
   TPT_CHECK_LAUNCH();
 }
 
