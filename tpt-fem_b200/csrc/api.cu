@@ -28,6 +28,19 @@ __global__ void matvec_exact(int64_t nrows, const int* __restrict__ rp, const in
   y[r] = s;
 }
 
+// conn64 -> conn32 with 0 <= c < n_nodes (bit 0 of *flag otherwise); finite coords (bit 1).
+__global__ void mesh_check_convert(int64_t nc, const int64_t* __restrict__ c64, int64_t n_nodes,
+                                   int* __restrict__ c32, int64_t nx, const double* __restrict__ x,
+                                   int* __restrict__ flag) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nc) {
+    const int64_t c = c64[i];
+    if (c < 0 || c >= n_nodes) atomicOr(flag, 1);
+    c32[i] = (c >= 0 && c < n_nodes) ? (int)c : 0;
+  }
+  if (i < nx && !isfinite(x[i])) atomicOr(flag, 2);
+}
+
 tptfem_status fail(tptfem_context* ctx, tptfem_status st, const std::string& msg) {
   if (ctx) ctx->err = msg;
   return st;
@@ -176,13 +189,6 @@ tptfem_status tptfem_mesh_upload(tptfem_context* ctx, int cell_type, int coord_d
   TPT_REQUIRE(coords && conn, TPTFEM_ERR_INVALID_ARG, "coords/conn is NULL");
   TPT_REQUIRE(n_nodes > 0 && n_nodes < (1LL << 31), TPTFEM_ERR_INVALID_ARG, "n_nodes out of range");
   TPT_REQUIRE(n_elems > 0 && n_elems < (1LL << 29), TPTFEM_ERR_INVALID_ARG, "n_elems out of range");
-  for (int64_t i = 0; i < n_nodes * coord_dim; ++i)
-    TPT_REQUIRE(std::isfinite(coords[i]), TPTFEM_ERR_INVALID_ARG, "coords hold a non-finite value");
-  std::vector<int> c32((size_t)n_elems * 4);
-  for (int64_t i = 0; i < n_elems * 4; ++i) {
-    TPT_REQUIRE(conn[i] >= 0 && conn[i] < n_nodes, TPTFEM_ERR_INVALID_ARG, "connectivity entry out of range");
-    c32[i] = (int)conn[i];
-  }
   auto m = std::make_shared<MeshData>();
   m->ctx = ctx;
   m->cell = cell_type;
@@ -193,8 +199,21 @@ tptfem_status tptfem_mesh_upload(tptfem_context* ctx, int cell_type, int coord_d
   m->coords.alloc(n_nodes * coord_dim, ctx->stream);
   m->coords.upload(coords, n_nodes * coord_dim);
   m->conn.alloc(n_elems * 4, ctx->stream);
-  m->conn.upload(c32.data(), c32.size());
-  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  {  // int64 connectivity -> int32 on the device, with the range and finiteness checks
+    DevBuf<int64_t> c64;
+    c64.alloc(n_elems * 4, ctx->stream);
+    c64.upload(conn, n_elems * 4);
+    TPT_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+    const int64_t nv = std::max<int64_t>(n_elems * 4, n_nodes * coord_dim);
+    mesh_check_convert<<<ceil_div(nv, 256), 256, 0, ctx->stream>>>(n_elems * 4, c64.p, n_nodes, m->conn.p,
+                                                                   n_nodes * coord_dim, m->coords.p, ctx->d_flag);
+    TPT_CHECK_LAUNCH();
+    int flag = 0;
+    TPT_CUDA(cudaMemcpyAsync(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+    TPT_REQUIRE(!(flag & 2), TPTFEM_ERR_INVALID_ARG, "coords hold a non-finite value");
+    TPT_REQUIRE(!(flag & 1), TPTFEM_ERR_INVALID_ARG, "connectivity entry out of range");
+  }
   *out = new tptfem_mesh{m};
   API_CATCH(ctx)
 }

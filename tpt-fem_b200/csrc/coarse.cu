@@ -262,6 +262,126 @@ __global__ void cs_check_adjacency(int ngroups, const int* __restrict__ gptr, co
   }
 }
 
+// ---- geometry of the coarse space (device) ----------------------------------------
+
+// Node position of every group (its first dof's node), zero-padded to 3-D.
+__global__ void cs_positions(int ngroups, int dpn, int cdim, const int* __restrict__ free_map,
+                             const double* __restrict__ coords, double* __restrict__ pos) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  const int node = free_map[(int64_t)g * dpn] / dpn;
+  for (int d = 0; d < 3; ++d) pos[(int64_t)g * 3 + d] = d < cdim ? coords[(int64_t)node * cdim + d] : 0.0;
+}
+
+// Per-block min (part[6b..6b+2]) and max (part[6b+3..]) of the positions.
+__global__ void __launch_bounds__(CS_THREADS) cs_bbox(int ngroups, const double* __restrict__ pos,
+                                                      double* __restrict__ part) {
+  __shared__ double sh[CS_THREADS][6];
+  double v[6] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x)
+    for (int d = 0; d < 3; ++d) {
+      const double x = pos[(int64_t)g * 3 + d];
+      v[d] = fmin(v[d], x);
+      v[3 + d] = fmax(v[3 + d], x);
+    }
+  for (int q = 0; q < 6; ++q) sh[threadIdx.x][q] = v[q];
+  __syncthreads();
+  for (int st = CS_THREADS / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int q = 0; q < 6; ++q)
+        sh[threadIdx.x][q] = q < 3 ? fmin(sh[threadIdx.x][q], sh[threadIdx.x + st][q])
+                                   : fmax(sh[threadIdx.x][q], sh[threadIdx.x + st][q]);
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) part[(int64_t)blockIdx.x * 6 + threadIdx.x] = sh[0][threadIdx.x];
+}
+
+// Bin of every group: k_d = min(bins_d - 1, floor((x_d - lo_d) / L_d * bins_d)).
+__global__ void cs_bin(int ngroups, const double* __restrict__ pos, double lx, double ly, double lz, double Lx,
+                       double Ly, double Lz, int bx, int by, int bz, int* __restrict__ gbin, int* __restrict__ binid,
+                       int* __restrict__ used) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  const double lo[3] = {lx, ly, lz}, L[3] = {Lx, Ly, Lz};
+  const int nb[3] = {bx, by, bz};
+  int64_t b = 0;
+  for (int d = 2; d >= 0; --d) {
+    int k = 0;
+    if (L[d] > 0) k = min(nb[d] - 1, (int)floor((pos[(int64_t)g * 3 + d] - lo[d]) / L[d] * nb[d]));
+    k = max(k, 0);
+    gbin[(int64_t)g * 3 + d] = k;
+    b = b * nb[d] + k;
+  }
+  binid[g] = (int)b;
+  used[b] = 1;
+}
+
+__global__ void cs_mark_empty(int64_t nbins, const int* __restrict__ used, int* __restrict__ bin2agg) {
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nbins && !used[b]) bin2agg[b] = -1;
+}
+
+__global__ void cs_group_agg(int ngroups, const int* __restrict__ binid, const int* __restrict__ bin2agg,
+                             int* __restrict__ agg) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < ngroups) agg[g] = bin2agg[binid[g]];
+}
+
+// Per aggregate (one block): centroid (stats[0..2]) and inertia about it
+// (stats[3..11], sum |y|^2 I - y y^T), in a fixed summation order; bin of
+// its first group.
+__global__ void __launch_bounds__(CS_THREADS) cs_aggregate_stats(const int* __restrict__ aptr,
+                                                                 const int* __restrict__ alist,
+                                                                 const double* __restrict__ pos,
+                                                                 const int* __restrict__ gbin,
+                                                                 double* __restrict__ stats, int* __restrict__ abin) {
+  __shared__ double sh[CS_THREADS][9];
+  __shared__ double cen[3];
+  const int A = blockIdx.x, b0 = aptr[A], b1 = aptr[A + 1];
+  double v[9];
+  for (int q = 0; q < 3; ++q) v[q] = 0.0;
+  for (int t = b0 + threadIdx.x; t < b1; t += CS_THREADS)
+    for (int d = 0; d < 3; ++d) v[d] += pos[(int64_t)alist[t] * 3 + d];
+  for (int q = 0; q < 3; ++q) sh[threadIdx.x][q] = v[q];
+  __syncthreads();
+  for (int st = CS_THREADS / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int q = 0; q < 3; ++q) sh[threadIdx.x][q] += sh[threadIdx.x + st][q];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) cen[threadIdx.x] = sh[0][threadIdx.x] / (double)(b1 - b0);
+  __syncthreads();
+  for (int q = 0; q < 9; ++q) v[q] = 0.0;
+  for (int t = b0 + threadIdx.x; t < b1; t += CS_THREADS) {
+    double y[3];
+    for (int d = 0; d < 3; ++d) y[d] = pos[(int64_t)alist[t] * 3 + d] - cen[d];
+    const double y2 = y[0] * y[0] + y[1] * y[1] + y[2] * y[2];
+    for (int a = 0; a < 3; ++a)
+      for (int c = 0; c < 3; ++c) v[a * 3 + c] += (a == c ? y2 : 0.0) - y[a] * y[c];
+  }
+  __syncthreads();
+  for (int q = 0; q < 9; ++q) sh[threadIdx.x][q] = v[q];
+  __syncthreads();
+  for (int st = CS_THREADS / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int q = 0; q < 9; ++q) sh[threadIdx.x][q] += sh[threadIdx.x + st][q];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) stats[(int64_t)A * 12 + threadIdx.x] = cen[threadIdx.x];
+  if (threadIdx.x < 9) stats[(int64_t)A * 12 + 3 + threadIdx.x] = sh[0][threadIdx.x];
+  if (threadIdx.x < 3) abin[A * 3 + threadIdx.x] = gbin[(int64_t)alist[b0] * 3 + threadIdx.x];
+}
+
+// y_g = position minus its aggregate's centroid (FP32).
+__global__ void cs_relative(int ngroups, const int* __restrict__ agg, const double* __restrict__ pos,
+                            const double* __restrict__ stats, float* __restrict__ y) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  const int A = agg[g];
+  for (int d = 0; d < 3; ++d)
+    y[(int64_t)g * 3 + d] = (float)(pos[(int64_t)g * 3 + d] - stats[(int64_t)A * 12 + d]);
+}
+
 // Eigen-decomposition of a symmetric 3x3 matrix by cyclic Jacobi rotations
 // (host, once per aggregate): A = V diag(w) V^T, V column-major in v[3][3].
 void sym_eig3(double a[3][3], double w[3], double v[3][3]) {
@@ -312,22 +432,25 @@ bool coarse_build(SystemData& S, int target) {
   cudaStream_t s = S.ctx->stream;
   const MeshData& M = *S.mesh;
   const int dpn = S.dpn, ng = S.nb.ngroups, nm = rigid_modes(dpn), cdim = M.cdim;
-  std::vector<int> fm(S.n_free);
-  std::vector<double> xyz((size_t)M.n_nodes * cdim);
-  S.free_map.download(fm.data(), fm.size());
-  M.coords.download(xyz.data(), xyz.size());
+  PhaseTimer tall(s, "coarse geometry");
+  // node position of every group and the bounding box (device)
+  DevBuf<double> pos, part;
+  pos.alloc((size_t)ng * 3, s);
+  const int pb = std::min(1024, blocks_for(ng));
+  part.alloc((size_t)pb * 6, s);
+  cs_positions<<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, dpn, cdim, S.free_map.p, M.coords.p, pos.p);
+  TPT_CHECK_LAUNCH();
+  cs_bbox<<<pb, CS_THREADS, 0, s>>>(ng, pos.p, part.p);
+  TPT_CHECK_LAUNCH();
+  std::vector<double> hp((size_t)pb * 6);
+  part.download(hp.data(), hp.size());
   TPT_CUDA(cudaStreamSynchronize(s));
-  std::vector<double> pos((size_t)ng * 3, 0.0);
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  for (int g = 0; g < ng; ++g) {
-    const int node = fm[(size_t)g * dpn] / dpn;
-    for (int d = 0; d < cdim && d < 3; ++d) {
-      const double x = xyz[(size_t)node * cdim + d];
-      pos[(size_t)g * 3 + d] = x;
-      lo[d] = std::min(lo[d], x);
-      hi[d] = std::max(hi[d], x);
+  for (int q = 0; q < pb; ++q)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = std::min(lo[d], hp[(size_t)q * 6 + d]);
+      hi[d] = std::max(hi[d], hp[(size_t)q * 6 + 3 + d]);
     }
-  }
   double L[3], vol = 1.0;
   int nact = 0;
   for (int d = 0; d < 3; ++d) {
@@ -336,97 +459,52 @@ bool coarse_build(SystemData& S, int target) {
   }
   if (nact == 0 || target < 1) return false;
   double H = std::pow(vol / (double)target, 1.0 / nact);
-  std::vector<int> gbin((size_t)ng * 3), agg(ng), binid(ng);
-  std::vector<int> bin2agg;
-  int na = 0;
-  DevBuf<int> d_gbin, flag;
-  d_gbin.alloc((size_t)ng * 3, s);
+  // bins (device), non-empty bins -> aggregates, adjacency check; coarsen until valid
+  DevBuf<int> gbin, binid, used, flag;
+  gbin.alloc((size_t)ng * 3, s);
+  binid.alloc(ng, s);
   flag.alloc(1, s);
+  int na = 0;
   bool ok = false;
   for (int attempt = 0; attempt < 12 && !ok; ++attempt, H *= 1.25) {
     for (int d = 0; d < 3; ++d) C.bins[d] = L[d] > 0 ? std::max(1, (int)std::floor(L[d] / H)) : 1;
     const int64_t nbins = (int64_t)C.bins[0] * C.bins[1] * C.bins[2];
     if (nbins > (1 << 24)) continue;
-    for (int g = 0; g < ng; ++g) {
-      int64_t b = 0;
-      for (int d = 2; d >= 0; --d) {
-        int k = 0;
-        if (L[d] > 0) k = std::min(C.bins[d] - 1, (int)std::floor((pos[(size_t)g * 3 + d] - lo[d]) / L[d] * C.bins[d]));
-        k = std::max(k, 0);
-        gbin[(size_t)g * 3 + d] = k;
-        b = b * C.bins[d] + k;
-      }
-      binid[g] = (int)b;
-    }
-    bin2agg.assign(nbins, -1);
-    for (int g = 0; g < ng; ++g) bin2agg[binid[g]] = 0;
-    na = 0;
-    for (auto& v : bin2agg)
-      if (v == 0) v = na++;
+    used.alloc(nbins + 1, s);
+    used.zero();
+    cs_bin<<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, pos.p, lo[0], lo[1], lo[2], L[0], L[1], L[2], C.bins[0],
+                                                   C.bins[1], C.bins[2], gbin.p, binid.p, used.p);
+    TPT_CHECK_LAUNCH();
+    C.bin2agg.alloc(nbins + 1, s);
+    na = (int)exclusive_scan_i32(used.p, C.bin2agg.p, nbins, s);  // rank of each non-empty bin
     if ((int64_t)na * nm > CS_MAX_COARSE) continue;
-    for (int g = 0; g < ng; ++g) agg[g] = bin2agg[binid[g]];
-    d_gbin.upload(gbin.data(), gbin.size());
     flag.zero();
-    cs_check_adjacency<<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, S.nb.gptr.p, S.nb.glist.p, d_gbin.p, flag.p);
+    cs_check_adjacency<<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, S.nb.gptr.p, S.nb.glist.p, gbin.p, flag.p);
     TPT_CHECK_LAUNCH();
     int f = 0;
     flag.download(&f, 1);
     TPT_CUDA(cudaStreamSynchronize(s));
     ok = f == 0;
+    if (ok) {  // empty bins -> -1
+      cs_mark_empty<<<blocks_for(nbins), CS_THREADS, 0, s>>>(nbins, used.p, C.bin2agg.p);
+      TPT_CHECK_LAUNCH();
+    }
   }
   if (!ok) return false;
-  // aggregate lists, centroids, relative positions, orthonormal mode transforms
-  std::vector<int> aptr(na + 1, 0), alist(ng), abin((size_t)na * 3);
+  // aggregate of every group; its group list by a stable counting sort (host)
+  C.agg.alloc(ng, s);
+  cs_group_agg<<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, binid.p, C.bin2agg.p, C.agg.p);
+  TPT_CHECK_LAUNCH();
+  std::vector<int> agg(ng), aptr(na + 1, 0), alist(ng);
+  C.agg.download(agg.data(), ng);
+  TPT_CUDA(cudaStreamSynchronize(s));
   for (int g = 0; g < ng; ++g) aptr[agg[g] + 1]++;
   for (int i = 0; i < na; ++i) aptr[i + 1] += aptr[i];
   {
     std::vector<int> fill(aptr.begin(), aptr.end() - 1);
     for (int g = 0; g < ng; ++g) alist[fill[agg[g]]++] = g;
   }
-  std::vector<double> cen((size_t)na * 3, 0.0);
-  for (int g = 0; g < ng; ++g)
-    for (int d = 0; d < 3; ++d) cen[(size_t)agg[g] * 3 + d] += pos[(size_t)g * 3 + d];
-  for (int i = 0; i < na; ++i) {
-    const double cnt = aptr[i + 1] - aptr[i];
-    for (int d = 0; d < 3; ++d) cen[(size_t)i * 3 + d] /= cnt;
-    const int g0 = alist[aptr[i]];
-    for (int d = 0; d < 3; ++d) abin[(size_t)i * 3 + d] = gbin[(size_t)g0 * 3 + d];
-  }
-  std::vector<float> yrel((size_t)ng * 3);
-  std::vector<double> inert((size_t)na * 9, 0.0);
-  for (int g = 0; g < ng; ++g) {
-    const int I = agg[g];
-    double yv[3];
-    for (int d = 0; d < 3; ++d) yv[d] = pos[(size_t)g * 3 + d] - cen[(size_t)I * 3 + d];
-    for (int d = 0; d < 3; ++d) yrel[(size_t)g * 3 + d] = (float)yv[d];
-    const double y2 = yv[0] * yv[0] + yv[1] * yv[1] + yv[2] * yv[2];
-    for (int a = 0; a < 3; ++a)
-      for (int b = 0; b < 3; ++b) inert[(size_t)I * 9 + a * 3 + b] += (a == b ? y2 : 0.0) - yv[a] * yv[b];
-  }
-  std::vector<double> T((size_t)na * nm * nm, 0.0);
-  for (int i = 0; i < na; ++i) {
-    double* t = T.data() + (size_t)i * nm * nm;
-    const double cnt = aptr[i + 1] - aptr[i];
-    const int ntr = dpn;  // translations
-    for (int k = 0; k < ntr; ++k) t[k * nm + k] = 1.0 / std::sqrt(cnt);
-    if (dpn == 2) {
-      const double iz = inert[(size_t)i * 9 + 8];  // sum of |y|^2 in the plane
-      if (iz > 1e-12 * cnt * H * H) t[2 * nm + 2] = 1.0 / std::sqrt(iz);
-    } else if (dpn == 3) {
-      double a[3][3], w[3], v[3][3];
-      for (int p = 0; p < 3; ++p)
-        for (int q = 0; q < 3; ++q) a[p][q] = inert[(size_t)i * 9 + p * 3 + q];
-      sym_eig3(a, w, v);
-      const double wmax = std::max(w[0], std::max(w[1], w[2]));
-      for (int q = 0; q < 3; ++q) {
-        if (!(w[q] > 1e-9 * wmax) || !(wmax > 1e-12 * cnt * H * H)) continue;
-        const double sc = 1.0 / std::sqrt(w[q]);
-        for (int p = 0; p < 3; ++p) t[(3 + p) * nm + 3 + q] = v[p][q] * sc;
-      }
-    }
-  }
-  // segments of at most CS_SEG groups per aggregate (restriction work items)
-  constexpr int CS_SEG = 1024;
+  constexpr int CS_SEG = 1024;  // segments of at most CS_SEG groups (restriction work items)
   std::vector<int> sb, se, aseg(na + 1, 0);
   for (int i = 0; i < na; ++i) {
     for (int t = aptr[i]; t < aptr[i + 1]; t += CS_SEG) {
@@ -435,20 +513,50 @@ bool coarse_build(SystemData& S, int target) {
     }
     aseg[i + 1] = (int)sb.size();
   }
+  C.na = na;
+  C.nm = nm;
+  C.nc = na * nm;
   C.nseg = (int)sb.size();
+  C.aptr.alloc(na + 1, s); C.aptr.upload(aptr.data(), na + 1);
+  C.alist.alloc(ng, s); C.alist.upload(alist.data(), ng);
   C.sbeg.alloc(C.nseg, s); C.sbeg.upload(sb.data(), C.nseg);
   C.send.alloc(C.nseg, s); C.send.upload(se.data(), C.nseg);
   C.aseg.alloc(na + 1, s); C.aseg.upload(aseg.data(), na + 1);
   C.smom.alloc((size_t)C.nseg * nm, s);
-  C.na = na;
-  C.nm = nm;
-  C.nc = na * nm;
-  C.agg.alloc(ng, s); C.agg.upload(agg.data(), ng);
-  C.aptr.alloc(na + 1, s); C.aptr.upload(aptr.data(), na + 1);
-  C.alist.alloc(ng, s); C.alist.upload(alist.data(), ng);
-  C.abin.alloc((size_t)na * 3, s); C.abin.upload(abin.data(), abin.size());
-  C.bin2agg.alloc(bin2agg.size(), s); C.bin2agg.upload(bin2agg.data(), bin2agg.size());
-  C.y.alloc((size_t)ng * 3, s); C.y.upload(yrel.data(), yrel.size());
+  // centroids, relative positions, inertia (device); mode transforms (host, per aggregate)
+  DevBuf<double> stats;
+  stats.alloc((size_t)na * 12, s);
+  C.abin.alloc((size_t)na * 3, s);
+  cs_aggregate_stats<<<na, CS_THREADS, 0, s>>>(C.aptr.p, C.alist.p, pos.p, gbin.p, stats.p, C.abin.p);
+  TPT_CHECK_LAUNCH();
+  C.y.alloc((size_t)ng * 3, s);
+  cs_relative<<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, C.agg.p, pos.p, stats.p, C.y.p);
+  TPT_CHECK_LAUNCH();
+  std::vector<double> st((size_t)na * 12);
+  stats.download(st.data(), st.size());
+  TPT_CUDA(cudaStreamSynchronize(s));
+  std::vector<double> T((size_t)na * nm * nm, 0.0);
+  for (int i = 0; i < na; ++i) {
+    double* t = T.data() + (size_t)i * nm * nm;
+    const double cnt = aptr[i + 1] - aptr[i];
+    const double* in = st.data() + (size_t)i * 12 + 3;  // inertia, row-major 3 x 3
+    for (int k = 0; k < dpn; ++k) t[k * nm + k] = 1.0 / std::sqrt(cnt);
+    if (dpn == 2) {
+      const double iz = in[8];  // sum of |y|^2 in the plane
+      if (iz > 1e-12 * cnt * H * H) t[2 * nm + 2] = 1.0 / std::sqrt(iz);
+    } else if (dpn == 3) {
+      double a[3][3], w[3], v[3][3];
+      for (int p2 = 0; p2 < 3; ++p2)
+        for (int q = 0; q < 3; ++q) a[p2][q] = in[p2 * 3 + q];
+      sym_eig3(a, w, v);
+      const double wmax = std::max(w[0], std::max(w[1], w[2]));
+      for (int q = 0; q < 3; ++q) {
+        if (!(w[q] > 1e-9 * wmax) || !(wmax > 1e-12 * cnt * H * H)) continue;
+        const double sc = 1.0 / std::sqrt(w[q]);
+        for (int p2 = 0; p2 < 3; ++p2) t[(3 + p2) * nm + 3 + q] = v[p2][q] * sc;
+      }
+    }
+  }
   C.T.alloc(T.size(), s); C.T.upload(T.data(), T.size());
   TPT_CUDA(cudaFuncSetAttribute(cs_gemv, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(CS_MAX_COARSE * sizeof(double))));

@@ -18,6 +18,8 @@
 #include <algorithm>
 #include <cmath>
 
+#include <climits>
+
 #include "objects.hpp"
 
 namespace tptfem {
@@ -84,17 +86,55 @@ __global__ void transpose_fill(int n, const int* __restrict__ grp, const int* __
   }
 }
 
-// Sort each L^T row by column (insertion sort; rows are short) -> deterministic.
+// Sort each L^T row by column -> deterministic.  One warp per row: rows of up
+// to 64 entries are bitonic-sorted in registers (2 keys per lane); longer rows
+// fall back to an insertion sort by one lane.
 __global__ void transpose_sort(int n, const int* __restrict__ trp, int* __restrict__ tci, int* __restrict__ perm) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int j = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (j >= n) return;
-  int b = trp[j], e = trp[j + 1];
-  for (int a = b + 1; a < e; ++a) {
-    int c = tci[a], p = perm[a];
-    int q = a - 1;
-    while (q >= b && tci[q] > c) { tci[q + 1] = tci[q]; perm[q + 1] = perm[q]; --q; }
-    tci[q + 1] = c;
-    perm[q + 1] = p;
+  const int b = trp[j], e = trp[j + 1], len = e - b;
+  if (len <= 1) return;
+  if (len > 64) {
+    if (lane == 0)
+      for (int a = b + 1; a < e; ++a) {
+        int c = tci[a], p = perm[a];
+        int q = a - 1;
+        while (q >= b && tci[q] > c) { tci[q + 1] = tci[q]; perm[q + 1] = perm[q]; --q; }
+        tci[q + 1] = c;
+        perm[q + 1] = p;
+      }
+    return;
+  }
+  int key[2], val[2];
+  for (int h = 0; h < 2; ++h) {
+    const int t = 2 * lane + h;
+    key[h] = t < len ? tci[b + t] : INT_MAX;
+    val[h] = t < len ? perm[b + t] : 0;
+  }
+  for (int k = 2; k <= 64; k <<= 1)
+    for (int d = k >> 1; d >= 1; d >>= 1) {
+      if (d == 1) {
+        const bool asc = ((2 * lane) & k) == 0;
+        if (asc ? key[0] > key[1] : key[0] < key[1]) {
+          int t = key[0]; key[0] = key[1]; key[1] = t;
+          t = val[0]; val[0] = val[1]; val[1] = t;
+        }
+      } else {
+        for (int h = 0; h < 2; ++h) {
+          const int el = 2 * lane + h, pe = el ^ d;
+          const int pk = __shfl_xor_sync(0xffffffffu, key[h], d >> 1);
+          const int pv = __shfl_xor_sync(0xffffffffu, val[h], d >> 1);
+          const bool asc = (el & k) == 0;
+          const bool take_min = (el < pe) == asc;
+          const bool swap = take_min ? pk < key[h] : pk > key[h];
+          if (swap) { key[h] = pk; val[h] = pv; }
+        }
+      }
+    }
+  for (int h = 0; h < 2; ++h) {
+    const int t = 2 * lane + h;
+    if (t < len) { tci[b + t] = key[h]; perm[b + t] = val[h]; }
   }
 }
 
@@ -201,7 +241,7 @@ void fsai_build_pattern(const SystemData& S, FsaiFactor& F) {
   cnt.zero();
   transpose_fill<<<ceil_div(n, 256), 256, 0, s>>>(n, F.rp.p, F.ci.p, F.trp.p, cnt.p, F.tci.p, F.perm.p);
   TPT_CHECK_LAUNCH();
-  transpose_sort<<<ceil_div(n, 256), 256, 0, s>>>(n, F.trp.p, F.tci.p, F.perm.p);
+  transpose_sort<<<ceil_div((int64_t)n * 32, 256), 256, 0, s>>>(n, F.trp.p, F.tci.p, F.perm.p);
   TPT_CHECK_LAUNCH();
   F.sigma2.alloc(n, s);
   F.va.alloc(F.nnz, s);

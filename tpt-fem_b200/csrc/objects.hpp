@@ -1,6 +1,9 @@
 // objects.hpp -- the structs behind the opaque C-ABI handles and the internal
 // entry points the C ABI (api.cu) dispatches to.
 #pragma once
+#include <cstdio>
+#include <cstdlib>
+#include <ctime>
 #include <map>
 #include <memory>
 #include <string>
@@ -19,6 +22,37 @@ struct tptfem_context {
 };
 
 namespace tptfem {
+
+// TPTFEM_DEBUG=1: one line per reliable update and per set-up phase on stderr.
+inline bool debug_trace() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = std::getenv("TPTFEM_DEBUG");
+    v = (e && e[0] == '1') ? 1 : 0;
+  }
+  return v == 1;
+}
+
+// TPTFEM_DEBUG=1: stream-synchronised wall time of a set-up phase on stderr.
+struct PhaseTimer {
+  cudaStream_t s;
+  const char* name;
+  double t0 = 0.0;
+  PhaseTimer(cudaStream_t stream, const char* n) : s(stream), name(n) {
+    if (debug_trace()) { cudaStreamSynchronize(s); t0 = now_ms(); }
+  }
+  ~PhaseTimer() {
+    if (debug_trace()) {
+      cudaStreamSynchronize(s);
+      std::fprintf(stderr, "[tptfem] %-28s %9.3f ms\n", name, now_ms() - t0);
+    }
+  }
+  static double now_ms() {
+    timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
+  }
+};
 
 // Device-resident mesh plus lazily built node->element adjacency.
 struct MeshData {

@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <ctime>
 
 #include <type_traits>
 
@@ -40,16 +41,6 @@
 namespace tptfem {
 
 namespace {
-
-// TPTFEM_DEBUG=1 prints one line per reliable update to stderr.
-bool debug_trace() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = std::getenv("TPTFEM_DEBUG");
-    v = (e && e[0] == '1') ? 1 : 0;
-  }
-  return v == 1;
-}
 
 // Node-block kernels: blocks per SM in the grid.  Far more than can be
 // resident (registers allow ~5): queued blocks start as others finish, which
@@ -295,6 +286,7 @@ void select_nb_mode(SystemData& S, Engine<double>& E, const tptfem_solver_opts& 
 // afresh.  Returns the coarse size in use (0: off).
 int select_coarse(SystemData& S, Engine<double>& E, const tptfem_solver_opts& o, bool fresh) {
   bool want = (o.flags & TPTFEM_SOLVE_COARSE) && E.nb_pc;
+  PhaseTimer timer(S.ctx->stream, "coarse space");
   // default: about one aggregate per 2800 node groups, between 8 and 1000
   const int aggs = o.coarse_aggregates > 0 ? o.coarse_aggregates : std::max(8, std::min(1000, S.nb.ngroups / 2800));
   if (want) want = coarse_build(S, aggs);
@@ -447,10 +439,20 @@ void prepare_fsai_engine(SystemData& S, Engine<double>& E, const FsaiFactor& F, 
 // FP64 factor of A and installed (sigma^2 FP32, L FP16).  False if invalid.
 bool learned_factor(SystemData& S, SolverWork& W) {
   cudaStream_t s = S.ctx->stream;
-  fsai_build_pattern(S, W.lf);
+  {
+    PhaseTimer t(S.ctx->stream, "factor pattern");
+    fsai_build_pattern(S, W.lf);
+  }
   if (W.lf.overflow) return false;
-  if (!W.lgraph.ready) W.lgraph.prepare(S, W.lf);
-  if (!lf_forward(S, W.lf, W.lgraph, S.lmodel->prm.p)) return false;
+  if (!W.lgraph.ready) {
+    PhaseTimer t(S.ctx->stream, "network inputs");
+    W.lgraph.prepare(S, W.lf);
+  }
+  {
+    PhaseTimer t(S.ctx->stream, "network forward + Kaporin");
+    if (!lf_forward(S, W.lf, W.lgraph, S.lmodel->prm.p)) return false;
+  }
+  PhaseTimer t(S.ctx->stream, "factor conversion");
   DevBuf<double> sig2, lva;
   sig2.alloc(W.lf.n, s);
   lva.alloc(std::max<int64_t>(W.lf.nnz, 1), s);
@@ -502,6 +504,7 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o_in, tptfem_solve_st
     bool ok = !fresh || learned_factor(S, W);
     if (fresh && ok && !W.lf_engine) {
       prepare_fsai_engine(S, W.f64_lf, W.lf, batch);
+      PhaseTimer t(S.ctx->stream, "engine + node-block layout");
       if (!(o.flags & TPTFEM_SOLVE_CSR_ONLY) && nb_build_operator(S)) {
         const bool nbpc = nb_fill_factor(S, W.lf);
         W.f64_lf.use_nb(&S.nb, true, nbpc);
@@ -519,7 +522,10 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o_in, tptfem_solve_st
         W.nb_factor = &W.lf;
       }
       st.solver_used = solver;
-      select_nb_mode(S, W.f64_lf, o);
+      {
+        PhaseTimer t(S.ctx->stream, "symmetric operator");
+        select_nb_mode(S, W.f64_lf, o);
+      }
       st.coarse_size = select_coarse(S, W.f64_lf, o, fresh);
       TPT_CUDA(cudaEventRecord(ctx->ev[1], s));
       const double bb = norm2_b(S);
