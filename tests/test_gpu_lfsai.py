@@ -54,6 +54,35 @@ def test_device_loss_and_gradient_match_oracle(ctx):
     assert np.linalg.norm(grad3) < 1.5 * np.linalg.norm(grad)
 
 
+def test_loss_and_gradient_with_partly_fixed_nodes_match_oracle(ctx):
+    """Nodes with some dofs fixed (a roller on the top face) leave the
+    node-block form: the row-wise Kaporin kernel serves them."""
+    n = [6, 2, 2]
+    mn, mx = [0.0, 0.0, 0.0], [4.0, 1.0, 1.0]
+    c, e = box(n, mn=mn, mx=mx)
+    c = jitter(c, 0.02, 7)
+    m = F.Mesh.from_arrays(F.CELL_TET4, c, e, ctx=ctx)
+    K = F.assemble_elasticity(m, "3d", W.cantilever_young(n, seed=7), 0.3, 2)
+    rhs = F.apply_traction(m, 3, 0, 1.0, [0.0, 0.0, -1e-3], np.zeros(K.nrows))
+    dof, val = W.clamp_x0_bcs(c)
+    top = np.nonzero(np.abs(c[:, 2] - 1.0) < 1e-9)[0]
+    bcs = list(zip(dof, val)) + [(3 * int(v) + 2, 0.0) for v in top]
+    S = F.reduce_system(K, rhs, bcs)
+    rp, ci, va, fred, free = S.download()
+    assert np.any(np.bincount(np.asarray(free) // 3) == 2)  # nodes with one dof fixed
+    model = LF.LearnedFsai(ctx, seed=3)
+    rng = np.random.default_rng(8)
+    p = model.get_params().astype(np.float64)
+    p += 0.2 * rng.standard_normal(p.size)
+    model.set_params(p.astype(np.float32))
+    p = model.get_params().astype(np.float64)
+    loss, grad = model.loss(S, grad=True)
+    lrp, lci, _, _ = S.fsai()
+    oloss, ograd = L.loss_grad(p, L.Graph(rp, ci, va, free, 3, lrp, lci))
+    assert abs(loss - oloss) <= 1e-4 * abs(oloss) + 1e-6
+    assert np.linalg.norm(grad - ograd) <= 2e-3 * np.linalg.norm(ograd)
+
+
 def test_untrained_learned_solver_converges(ctx):
     S = cantilever_system(ctx, [10, 3, 3], seed=6)
     model = LF.LearnedFsai(ctx, seed=1)

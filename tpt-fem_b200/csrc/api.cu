@@ -3,6 +3,7 @@
 // Every entry point validates its arguments on the host before any launch,
 // converts int64 indices to the device's int32 with range checks, and maps
 // internal errors to tptfem_status plus a message kept in the context.
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 
 #include <cmath>
@@ -149,6 +150,7 @@ void tptfem_destroy(tptfem_context* ctx) {
   if (ctx->d_flag) cudaFree(ctx->d_flag);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
   if (ctx->cusolver) cusolverDnDestroy((cusolverDnHandle_t)ctx->cusolver);
+  if (ctx->cublas) cublasDestroy((cublasHandle_t)ctx->cublas);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);

@@ -10,11 +10,12 @@
 // dropped).  A_c = P^T A P is formed with one multi-vector operator product
 // per colour (all modes at once): aggregates are coloured by bin coordinates
 // mod 3, so an aggregate has at most one neighbour of each colour and
-// P^T A (P E_colour) yields whole coarse columns without mixing.  A_c is factorised (cuSOLVER dpotrf /
-// dpotri, once per set-up, off the iteration path) and kept as an explicit
-// FP32 inverse, so each iteration adds one restriction, one coarse mat-vec
+// P^T A (P E_colour) yields whole coarse columns without mixing.  A_c is
+// factorised and inverted once per set-up, off the iteration path (cuSOLVER
+// dpotrf and trtri, one cuBLAS dsyrk), and kept as an explicit FP32 inverse, so each iteration adds one restriction, one coarse mat-vec
 // and a prolongation that is fused into the FSAI transpose kernel.
 // Requires the node-block layout (full node groups) and the mesh geometry.
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 
 #include <algorithm>
@@ -64,14 +65,16 @@ __global__ void cs_fill_modes(int ngroups, const int* __restrict__ agg, const in
 }
 
 // Raw moments of every column m of W (interleaved) over one segment:
-// smom[(seg nm + m) nm + k] = sum over its groups of (R_g^T W_g[:, m])_k.
+// smom[(seg nm + m) nm + k] = sum over its groups of (R_g^T W_g[:, m])_k;
+// groups without a neighbour of the colour are skipped.
 template <int DPN>
 __global__ void __launch_bounds__(CS_THREADS) cs_moments_modes(const int* __restrict__ sbeg,
                                                                const int* __restrict__ send,
                                                                const int* __restrict__ alist,
                                                                const float* __restrict__ y,
                                                                const double* __restrict__ W,
-                                                               double* __restrict__ smom) {
+                                                               double* __restrict__ smom,
+                                                               const unsigned* __restrict__ gmask, int colour) {
   constexpr int NM = rigid_modes(DPN);
   __shared__ double sh[CS_THREADS / 32][NM * NM];
   const int seg = blockIdx.x;
@@ -80,6 +83,7 @@ __global__ void __launch_bounds__(CS_THREADS) cs_moments_modes(const int* __rest
   for (int q = 0; q < NM * NM; ++q) s[q] = 0.0;
   for (int t = sbeg[seg] + threadIdx.x; t < send[seg]; t += CS_THREADS) {
     const int g = alist[t];
+    if (!((gmask[g] >> colour) & 1u)) continue;  // W_g is zero (and not written) for this colour
     double R[DPN][NM];
     mode_rows<DPN>(y + 3 * (int64_t)g, R);
     const double* wg = W + (int64_t)g * DPN * NM;
@@ -166,18 +170,30 @@ __global__ void cs_yc(int na, int nm, const int* __restrict__ aseg, const double
   if (j < na * nm) yc[j] = agg_moment(j / nm, j % nm, nm, aseg, smom, T);
 }
 
-// uc = A_c^-1 yc: one warp per row, FP32 matrix, FP64 accumulation.
-__global__ void __launch_bounds__(CS_THREADS) cs_gemv(int nc, const double* __restrict__ yc,
+// uc = A_c^-1 yc: one warp per row, FP32 matrix (row stride ld, a multiple of
+// 4, zero-padded), FP64 accumulation.  Each lane reads two adjacent matrix
+// entries and the matching two coarse-vector entries (16 contiguous bytes per
+// lane, so the shared-memory reads are conflict-free); eight loads per lane are
+// kept in flight.
+__global__ void __launch_bounds__(CS_THREADS) cs_gemv(int nc, int ld, const double* __restrict__ yc,
                                                       const float* __restrict__ Ainv, double* __restrict__ uc) {
   extern __shared__ double ys[];
-  for (int j = threadIdx.x; j < nc; j += blockDim.x) ys[j] = yc[j];
+  for (int j = threadIdx.x; j < ld; j += blockDim.x) ys[j] = j < nc ? yc[j] : 0.0;
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int row = blockIdx.x * (CS_THREADS / 32) + (threadIdx.x >> 5);
   if (row >= nc) return;
-  const float* a = Ainv + (int64_t)row * nc;
+  const float2* a = reinterpret_cast<const float2*>(Ainv + (int64_t)row * ld);
+  const double2* y2 = reinterpret_cast<const double2*>(ys);
+  const int n2 = ld >> 1;
   double s = 0.0;
-  for (int j = lane; j < nc; j += 32) s += (double)a[j] * ys[j];
+#pragma unroll 8
+  for (int j = lane; j < n2; j += 32) {
+    const float2 v = a[j];
+    const double2 w = y2[j];
+    s += (double)v.x * w.x;
+    s += (double)v.y * w.y;
+  }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   if (lane == 0) uc[row] = s;
 }
@@ -198,6 +214,19 @@ __global__ void cs_group_colour(int ngroups, const int* __restrict__ agg, const 
                                 unsigned char* __restrict__ gcol) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g < ngroups) gcol[g] = (unsigned char)colour_of(abin + 3 * agg[g]);
+}
+
+// Per group, the colours among its neighbour groups (itself included); per
+// chunk of 32 groups, their union.
+__global__ void cs_colour_masks(int ngroups, const int* __restrict__ gptr, const int* __restrict__ glist,
+                                const unsigned char* __restrict__ gcol, unsigned* __restrict__ gmask,
+                                unsigned* __restrict__ cmask) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  unsigned m = 0;
+  for (int t = gptr[g]; t < gptr[g + 1]; ++t) m |= 1u << gcol[glist[t]];
+  gmask[g] = m;
+  atomicOr(cmask + (g >> 5), m);
 }
 
 // Column blocks (J, m) of A_c, one thread per (I, m, mp): J is I's unique
@@ -239,12 +268,22 @@ __global__ void cs_fix_diag(int nc, double* __restrict__ Ac) {
   if (i < nc && Ac[(int64_t)i * nc + i] == 0.0) Ac[(int64_t)i * nc + i] = 1.0;
 }
 
-// dpotri leaves the inverse in one triangle (column-major lower = row-major
-// upper of the stored array): mirror it and convert to FP32.
-__global__ void cs_symmetrize(int nc, const double* __restrict__ A, float* __restrict__ out) {
+// Column-major lower triangle of A (diagonal included), zeros above it.
+__global__ void cs_lower_part(int nc, const double* __restrict__ A, double* __restrict__ out) {
   int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= (int64_t)nc * nc) return;
-  const int i = (int)(id / nc), j = (int)(id % nc);
+  const int c = (int)(id / nc), r = (int)(id % nc);  // element (r, c) at A[c * nc + r]
+  out[id] = r >= c ? A[id] : 0.0;
+}
+
+// The inverse is left in one triangle (column-major lower = row-major
+// upper of the stored array): mirror it and convert to FP32.
+// Rows of out have stride ld >= nc; the padding columns are zero.
+__global__ void cs_symmetrize(int nc, int ld, const double* __restrict__ A, float* __restrict__ out) {
+  int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= (int64_t)nc * ld) return;
+  const int i = (int)(id / ld), j = (int)(id % ld);
+  if (j >= nc) { out[id] = 0.0f; return; }
   // column-major lower triangle: element (r, c) with r >= c at A[c * nc + r]
   const int r = i > j ? i : j, c = i > j ? j : i;
   out[id] = (float)A[(int64_t)c * nc + r];
@@ -561,13 +600,20 @@ bool coarse_build(SystemData& S, int target) {
   TPT_CUDA(cudaFuncSetAttribute(cs_gemv, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(CS_MAX_COARSE * sizeof(double))));
   C.Ac.alloc((size_t)C.nc * C.nc, s);
-  C.Ainv.alloc((size_t)C.nc * C.nc, s);
+  C.ld = (C.nc + 3) & ~3;
+  C.Ainv.alloc((size_t)C.nc * C.ld, s);
   C.yc.alloc(C.nc, s);
   C.uc.alloc(C.nc, s);
   C.cm.alloc(C.nc, s);
   C.Pfull.alloc((size_t)S.n_free * nm, s);
   C.gcolour.alloc(ng, s);
   cs_group_colour<<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, C.agg.p, C.abin.p, C.gcolour.p);
+  TPT_CHECK_LAUNCH();
+  C.gmask.alloc(ng, s);
+  C.cmask.alloc(S.nb.nchunks, s);
+  C.cmask.zero();
+  cs_colour_masks<<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, S.nb.gptr.p, S.nb.glist.p, C.gcolour.p, C.gmask.p,
+                                                         C.cmask.p);
   TPT_CHECK_LAUNCH();
 #define TPT_CS_P(D)                                                                                       \
   cs_fill_modes<D><<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, C.agg.p, C.abin.p, C.y.p, C.T.p, -1, C.Pfull.p); \
@@ -596,9 +642,10 @@ bool coarse_assemble(SystemData& S) {
     for (int cy = 0; cy < ncy; ++cy)
       for (int cx = 0; cx < ncx; ++cx) {
         const int colour = cx + 3 * cy + 9 * cz;
-        nb_operator_apply_modes(S, C.Pfull.p, w.p, C.gcolour.p, colour);
+        nb_operator_apply_modes(S, C.Pfull.p, w.p, C.gcolour.p, colour, C.cmask.p);
 #define TPT_CS_COL(D)                                                                                             \
-  cs_moments_modes<D><<<C.nseg, CS_THREADS, 0, s>>>(C.sbeg.p, C.send.p, C.alist.p, C.y.p, w.p, mom.p);           \
+  cs_moments_modes<D><<<C.nseg, CS_THREADS, 0, s>>>(C.sbeg.p, C.send.p, C.alist.p, C.y.p, w.p, mom.p, C.gmask.p,   \
+                                                    colour);                                                      \
   TPT_CHECK_LAUNCH();
         if (dpn == 3) { TPT_CS_COL(3) }
         else if (dpn == 2) { TPT_CS_COL(2) }
@@ -618,13 +665,16 @@ bool coarse_assemble(SystemData& S) {
     S.ctx->cusolver = h;
   }
   TPT_REQUIRE(cusolverDnSetStream(h, s) == CUSOLVER_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "cusolverDnSetStream failed");
-  int lw1 = 0, lw2 = 0;
+  int lw1 = 0;
   TPT_REQUIRE(cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, nc, C.Ac.p, nc, &lw1) == CUSOLVER_STATUS_SUCCESS,
               TPTFEM_ERR_DEVICE, "dpotrf_bufferSize failed");
-  TPT_REQUIRE(cusolverDnDpotri_bufferSize(h, CUBLAS_FILL_MODE_LOWER, nc, C.Ac.p, nc, &lw2) == CUSOLVER_STATUS_SUCCESS,
-              TPTFEM_ERR_DEVICE, "dpotri_bufferSize failed");
+  size_t dws = 0, hws = 0;
+  TPT_REQUIRE(cusolverDnXtrtri_bufferSize(h, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, nc, CUDA_R_64F, C.Ac.p, nc,
+                                          &dws, &hws) == CUSOLVER_STATUS_SUCCESS,
+              TPTFEM_ERR_DEVICE, "trtri_bufferSize failed");
   DevBuf<double> work;
-  work.alloc(std::max(1, std::max(lw1, lw2)), s);
+  work.alloc(std::max<size_t>(1, std::max<size_t>((size_t)lw1, (dws + 7) / 8)), s);
+  std::vector<char> hwork(std::max<size_t>(hws, 1));
   DevBuf<int> info;
   info.alloc(1, s);
   int hinfo = 0;
@@ -633,12 +683,29 @@ bool coarse_assemble(SystemData& S) {
   info.download(&hinfo, 1);
   TPT_CUDA(cudaStreamSynchronize(s));
   if (hinfo != 0) return false;  // coarse matrix not positive definite in FP64
-  TPT_REQUIRE(cusolverDnDpotri(h, CUBLAS_FILL_MODE_LOWER, nc, C.Ac.p, nc, work.p, lw2, info.p) ==
-                  CUSOLVER_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "dpotri failed");
+  // A_c^-1 = L^-T L^-1: the factor inverted in place (trtri), its strictly
+  // upper part zeroed in a copy, and the product formed by one syrk into the
+  // lower triangle (a few large library calls instead of potri's many small ones)
+  TPT_REQUIRE(cusolverDnXtrtri(h, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, nc, CUDA_R_64F, C.Ac.p, nc, work.p,
+                               dws, hwork.data(), hws, info.p) == CUSOLVER_STATUS_SUCCESS,
+              TPTFEM_ERR_DEVICE, "trtri failed");
   info.download(&hinfo, 1);
   TPT_CUDA(cudaStreamSynchronize(s));
   if (hinfo != 0) return false;
-  cs_symmetrize<<<blocks_for((int64_t)nc * nc), CS_THREADS, 0, s>>>(nc, C.Ac.p, C.Ainv.p);
+  DevBuf<double> linv;
+  linv.alloc((size_t)nc * nc, s);
+  cs_lower_part<<<blocks_for((int64_t)nc * nc), CS_THREADS, 0, s>>>(nc, C.Ac.p, linv.p);
+  TPT_CHECK_LAUNCH();
+  cublasHandle_t hb = (cublasHandle_t)S.ctx->cublas;
+  if (!hb) {
+    TPT_REQUIRE(cublasCreate(&hb) == CUBLAS_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "cublasCreate failed");
+    S.ctx->cublas = hb;
+  }
+  TPT_REQUIRE(cublasSetStream(hb, s) == CUBLAS_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "cublasSetStream failed");
+  const double one = 1.0, zero = 0.0;
+  TPT_REQUIRE(cublasDsyrk(hb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, nc, nc, &one, linv.p, nc, &zero, C.Ac.p, nc) ==
+                  CUBLAS_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "dsyrk failed");
+  cs_symmetrize<<<blocks_for((int64_t)nc * C.ld), CS_THREADS, 0, s>>>(nc, C.ld, C.Ac.p, C.Ainv.p);
   TPT_CHECK_LAUNCH();
   C.ready = true;
   return true;
@@ -655,8 +722,8 @@ void coarse_restrict_solve(const SystemData& S, const double* r, cudaStream_t s)
 #undef TPT_CS_R
   cs_yc<<<blocks_for(C.nc), CS_THREADS, 0, s>>>(C.na, C.nm, C.aseg.p, C.smom.p, C.T.p, C.yc.p);
   TPT_CHECK_LAUNCH();
-  cs_gemv<<<(C.nc + CS_THREADS / 32 - 1) / (CS_THREADS / 32), CS_THREADS, (size_t)C.nc * sizeof(double), s>>>(
-      C.nc, C.yc.p, C.Ainv.p, C.uc.p);
+  cs_gemv<<<(C.nc + CS_THREADS / 32 - 1) / (CS_THREADS / 32), CS_THREADS, (size_t)C.ld * sizeof(double), s>>>(
+      C.nc, C.ld, C.yc.p, C.Ainv.p, C.uc.p);
   TPT_CHECK_LAUNCH();
   cs_raw<<<blocks_for(C.nc), CS_THREADS, 0, s>>>(C.na, C.nm, C.T.p, C.uc.p, C.cm.p);
   TPT_CHECK_LAUNCH();
@@ -667,10 +734,11 @@ void coarse_download(const SystemData& S, int* na, int* nm, double* Ainv_out) {
   if (na) *na = C.na;
   if (nm) *nm = C.nm;
   if (Ainv_out && C.ready) {  // the FP32 inverse of A_c, widened
-    std::vector<float> f((size_t)C.nc * C.nc);
+    std::vector<float> f((size_t)C.nc * C.ld);
     C.Ainv.download(f.data(), f.size());
     TPT_CUDA(cudaStreamSynchronize(S.ctx->stream));
-    for (size_t i = 0; i < f.size(); ++i) Ainv_out[i] = f[i];
+    for (int i = 0; i < C.nc; ++i)
+      for (int j = 0; j < C.nc; ++j) Ainv_out[(size_t)i * C.nc + j] = f[(size_t)i * C.ld + j];
   }
 }
 

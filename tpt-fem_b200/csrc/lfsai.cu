@@ -35,6 +35,7 @@ namespace {
 
 constexpr int D0 = LF_D0, H = LF_H;
 constexpr int LF_THREADS = 128;
+static_assert(D0 % 4 == 0 && H % 4 == 0, "feature widths are read four channels at a time");
 constexpr int LF_MAXM = 48;  // longest pattern row incl. the diagonal (the FSAI pattern's bound)
 
 struct Off {  // parameter offsets (floats)
@@ -76,20 +77,39 @@ __global__ void lf_prep(int n, const int* __restrict__ rp, const int* __restrict
   dis[i] = 1.0 / sqrt(di);
 }
 
+// Sub-warp of LF_LPR lanes per row: lanes stride over the row's entries, so
+// consecutive lanes read consecutive CSR entries.
+constexpr int LF_LPR = 8;
+
+__device__ __forceinline__ unsigned subwarp_mask(int width) {
+  const int base = (threadIdx.x & 31) & ~(width - 1);
+  return (width == 32 ? 0xffffffffu : ((1u << width) - 1u)) << base;
+}
+
 // A^ values and node features.
 __global__ void lf_prep2(int n, int dpn, const int* __restrict__ rp, const int* __restrict__ ci,
                          const double* __restrict__ va, const int* __restrict__ free_map,
                          const double* __restrict__ dis, float* __restrict__ ahat, float* __restrict__ x0) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(tid / LF_LPR), l = (int)(tid % LF_LPR);
+  if (i >= n) return;  // whole sub-warps leave together
+  const double di = dis[i];
   float sa = 0.f, ss = 0.f, sq = 0.f;
   int deg = 0;
-  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+  for (int k = rp[i] + l; k < rp[i + 1]; k += LF_LPR) {
     const int j = ci[k];
-    const float a = (float)(va[k] * dis[i] * dis[j]);
+    const float a = (float)(va[k] * di * dis[j]);
     ahat[k] = a;
     if (j != i) { sa += fabsf(a); ss += a; sq += a * a; ++deg; }
   }
+  const unsigned m = subwarp_mask(LF_LPR);
+  for (int o = LF_LPR / 2; o > 0; o >>= 1) {
+    sa += __shfl_xor_sync(m, sa, o, LF_LPR);
+    ss += __shfl_xor_sync(m, ss, o, LF_LPR);
+    sq += __shfl_xor_sync(m, sq, o, LF_LPR);
+    deg += __shfl_xor_sync(m, deg, o, LF_LPR);
+  }
+  if (l != 0) return;
   float* x = x0 + (int64_t)i * D0;
   x[0] = 1.f; x[1] = sa; x[2] = ss; x[3] = sq;
   const int comp = dpn > 1 ? free_map[i] % dpn : -1;
@@ -97,49 +117,50 @@ __global__ void lf_prep2(int n, int dpn, const int* __restrict__ rp, const int* 
   x[7] = deg / 40.f;
 }
 
-// A^ at the factor pattern entries (0 where A has no entry).
+// A^ at the factor pattern entries (0 where A has no entry): LF_LPR lanes per
+// row, one pattern entry per lane, a binary search in the row.
 __global__ void lf_pattern_values(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                                   const float* __restrict__ ahat, const int* __restrict__ lrp,
                                   const int* __restrict__ lci, float* __restrict__ al) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(tid / LF_LPR), l = (int)(tid % LF_LPR);
   if (i >= n) return;
-  int k = rp[i];
-  const int ke = rp[i + 1];
-  for (int t = lrp[i]; t < lrp[i + 1]; ++t) {
+  const int r0 = rp[i], r1 = rp[i + 1];
+  for (int t = lrp[i] + l; t < lrp[i + 1]; t += LF_LPR) {
     const int j = lci[t];
-    while (k < ke && ci[k] < j) ++k;
-    al[t] = (k < ke && ci[k] == j) ? ahat[k] : 0.f;
+    int lo = r0, hi = r1;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (ci[mid] < j) lo = mid + 1;
+      else hi = mid;
+    }
+    al[t] = (lo < r1 && ci[lo] == j) ? ahat[lo] : 0.f;
   }
 }
 
 // ---- network forward ----------------------------------------------------------------
 
-// Ya = |A^_off| X, Yb = A^_off X (rows of width DIN).
+// Ya = |A^_off| X, Yb = A^_off X (rows of width DIN): DIN / 4 lanes per row,
+// each accumulating four channels over the row in order (one 16-byte load of
+// X per entry and lane).
 template <int DIN>
 __global__ void lf_agg(int n, const int* __restrict__ rp, const int* __restrict__ ci, const float* __restrict__ ahat,
                        const float* __restrict__ X, float* __restrict__ Ya, float* __restrict__ Yb) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  constexpr int LPR = DIN / 4;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(tid / LPR), c4 = (int)(tid % LPR);
   if (i >= n) return;
-  float a[DIN], b[DIN];
-#pragma unroll
-  for (int c = 0; c < DIN; ++c) a[c] = b[c] = 0.f;
+  float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
   for (int k = rp[i]; k < rp[i + 1]; ++k) {
     const int j = ci[k];
     if (j == i) continue;
     const float w = ahat[k], aw = fabsf(w);
-    const float* xj = X + (int64_t)j * DIN;
-#pragma unroll
-    for (int c = 0; c < DIN; ++c) {
-      const float v = __ldg(xj + c);
-      a[c] += aw * v;
-      b[c] += w * v;
-    }
+    const float4 v = __ldg(reinterpret_cast<const float4*>(X + (int64_t)j * DIN) + c4);
+    a.x += aw * v.x; a.y += aw * v.y; a.z += aw * v.z; a.w += aw * v.w;
+    b.x += w * v.x; b.y += w * v.y; b.z += w * v.z; b.w += w * v.w;
   }
-#pragma unroll
-  for (int c = 0; c < DIN; ++c) {
-    Ya[(int64_t)i * DIN + c] = a[c];
-    Yb[(int64_t)i * DIN + c] = b[c];
-  }
+  reinterpret_cast<float4*>(Ya + (int64_t)i * DIN)[c4] = a;
+  reinterpret_cast<float4*>(Yb + (int64_t)i * DIN)[c4] = b;
 }
 
 // H = tanh(Ws X + Wa Ya + Wb Yb + b)
@@ -195,26 +216,31 @@ __global__ void lf_head_nodes(int n, const float* __restrict__ prm, Off o, const
   }
 }
 
-// L^_ij for every pattern entry.
+// L^_ij for every pattern entry: four lanes per row, each evaluating four
+// channels of z_ij; the four partial sums are added across the lanes.
 __global__ void lf_head_edges(int n, const float* __restrict__ prm, Off o, const int* __restrict__ lrp,
                               const int* __restrict__ lci, const float* __restrict__ al, const float* __restrict__ P,
                               const float* __restrict__ Q, float* __restrict__ lhat) {
-  __shared__ float ue[H], ce[H], we[H], w0;
-  for (int t = threadIdx.x; t < H; t += blockDim.x) { ue[t] = prm[o.ue + t]; ce[t] = prm[o.ce + t]; we[t] = prm[o.we + t]; }
-  if (threadIdx.x == 0) w0 = prm[o.w0];
-  __syncthreads();
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float p[H];
+  constexpr int LPR = H / 4;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(tid / LPR), c4 = (int)(tid % LPR);
+  if (i >= n) return;  // whole sub-warps leave together
+  float ue[4], ce[4], we[4];
 #pragma unroll
-  for (int c = 0; c < H; ++c) p[c] = P[(int64_t)i * H + c];
+  for (int u = 0; u < 4; ++u) { ue[u] = prm[o.ue + 4 * c4 + u]; ce[u] = prm[o.ce + 4 * c4 + u]; we[u] = prm[o.we + 4 * c4 + u]; }
+  const float w0 = prm[o.w0];
+  const float4 p = reinterpret_cast<const float4*>(P + (int64_t)i * H)[c4];
+  const unsigned m = subwarp_mask(LPR);
   for (int t = lrp[i]; t < lrp[i + 1]; ++t) {
     const int j = lci[t];
     const float a = al[t];
-    float s = w0 * a;
-#pragma unroll
-    for (int c = 0; c < H; ++c) s += we[c] * tanhf(p[c] + __ldg(Q + (int64_t)j * H + c) + ue[c] * a + ce[c]);
-    lhat[t] = s;
+    const float4 q = __ldg(reinterpret_cast<const float4*>(Q + (int64_t)j * H) + c4);
+    float v = we[0] * tanhf(p.x + q.x + ue[0] * a + ce[0]);
+    v += we[1] * tanhf(p.y + q.y + ue[1] * a + ce[1]);
+    v += we[2] * tanhf(p.z + q.z + ue[2] * a + ce[2]);
+    v += we[3] * tanhf(p.w + q.w + ue[3] * a + ce[3]);
+    for (int q2 = LPR / 2; q2 > 0; q2 >>= 1) v += __shfl_xor_sync(m, v, q2, LPR);
+    if (c4 == 0) lhat[t] = w0 * a + v;
   }
 }
 
@@ -286,6 +312,170 @@ __global__ void __launch_bounds__(LF_THREADS) lf_kaporin_warp(int n, const int* 
   if (threadIdx.x == 0) {
     double t = 0.0;
     for (int q2 = 0; q2 < WPB; ++q2) t += lsum[q2];
+    atomicAdd(loss, t);
+  }
+}
+
+// ---- node-block Kaporin terms --------------------------------------------------------
+//
+// When every free node has all its dofs free, row (g, a) of the factor has the
+// pattern (all dofs of g's lower neighbour nodes, ascending; then (g, b) for
+// b < a) and the rows of node g share their neighbour nodes H = (lower
+// neighbours of g, g).  With g_a = (L^_(g,a), 1 at (g,a), 0 after it) on the
+// dofs of H, w_a = A^[H,H] g_a and q_(g,a) = g_a . w_a; A^[H,H] is read as
+// dpn x dpn blocks, so one block serves dpn^2 scalar terms of all dpn rows.
+
+// Blocks of A^ on the node-group adjacency (zeroed beforehand): LF_LPR lanes
+// per scalar row g*dpn + a stride over its entries; each entry's block is found
+// by a binary search in g's neighbour groups (the list holds every group the
+// node's rows reach).
+__global__ void lf_blocks(int n, int dpn, const int* __restrict__ rp, const int* __restrict__ ci,
+                          const float* __restrict__ ahat, const int* __restrict__ gptr, const int* __restrict__ glist,
+                          float* __restrict__ ablk) {
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = (int)(tid / LF_LPR), l = (int)(tid % LF_LPR);
+  if (row >= n) return;
+  const int g = row / dpn, a = row % dpn, d2 = dpn * dpn;
+  const int t0 = gptr[g], t1 = gptr[g + 1];
+  for (int k = rp[row] + l; k < rp[row + 1]; k += LF_LPR) {
+    const int c = ci[k], J = c / dpn, b = c % dpn;
+    int lo = t0, hi = t1;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (glist[mid] < J) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo < t1) ablk[(int64_t)lo * d2 + a * dpn + b] = ahat[k];
+  }
+}
+
+// Every factor row's columns are the dofs of its node's lower neighbour groups
+// (as the node-block operator lists them), then its own lower dofs.
+__global__ void lf_check_blocks(int ngroups, int dpn, const int* __restrict__ lrp, const int* __restrict__ lci,
+                                const int* __restrict__ gptr, const int* __restrict__ glist,
+                                const int* __restrict__ nlow, int* __restrict__ flag) {
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (int64_t)ngroups * dpn) return;
+  const int g = (int)(tid / dpn), a = (int)(tid % dpn);
+  const int r0 = lrp[g * dpn + a], nl = nlow[g];
+  if (lrp[g * dpn + a + 1] - r0 != dpn * nl + a) { atomicOr(flag, 1); return; }
+  for (int p = 0; p < nl; ++p)
+    for (int b = 0; b < dpn; ++b)
+      if (lci[r0 + dpn * p + b] != glist[gptr[g] + p] * dpn + b) atomicOr(flag, 1);
+  for (int b = 0; b < a; ++b)
+    if (lci[r0 + dpn * nl + b] != g * dpn + b) atomicOr(flag, 1);
+}
+
+constexpr int KN_LANES = 8;  // lanes per node group (a structured tet mesh has 7 lower neighbours per node)
+
+// Kaporin terms of node group g's dpn rows (see above); KN_LANES lanes per
+// group, lane p owns pattern node H[p] (and H[p + KN_LANES], ...), merges that
+// node's neighbour list with H and accumulates w for all dpn rows.  Same
+// outputs and flags as lf_kaporin_warp.
+template <int D>
+__global__ void __launch_bounds__(LF_THREADS) lf_kaporin_nb(int ngroups, const int* __restrict__ gptr,
+                                                            const int* __restrict__ glist,
+                                                            const float* __restrict__ ablk,
+                                                            const int* __restrict__ lrp, const int* __restrict__ nlow,
+                                                            const float* __restrict__ lhat, float* __restrict__ sig,
+                                                            float* __restrict__ dlhat, double* __restrict__ loss,
+                                                            int* __restrict__ flag, int n) {
+  constexpr int MAXH = LF_MAXM / D;  // the scalar kernel's row bound, in nodes
+  constexpr int PASS = (MAXH + KN_LANES - 1) / KN_LANES;
+  constexpr int NPB = LF_THREADS / KN_LANES;
+  __shared__ int Hs[NPB][MAXH];
+  __shared__ float gv[NPB][D][MAXH][D];
+  __shared__ double lsum[LF_THREADS / 32];
+  const int slot = threadIdx.x / KN_LANES, l = threadIdx.x % KN_LANES;
+  const int g = blockIdx.x * NPB + slot;
+  const unsigned mask = subwarp_mask(KN_LANES);
+  double lq = 0.0;
+  if (g < ngroups) {  // uniform over the sub-warp
+    const int nl = nlow[g], nh = nl + 1;
+    if (D * nh > LF_MAXM) {  // the longest of the group's rows has D * nl + D entries
+      if (l < D) { atomicOr(flag, 1); sig[g * D + l] = 1.f; }
+    } else {
+      const int gp = gptr[g];
+      for (int p = l; p < nh; p += KN_LANES) Hs[slot][p] = p < nl ? glist[gp + p] : g;
+      for (int e = l; e < D * nh * D; e += KN_LANES) {
+        const int a = e / (nh * D), p = (e / D) % nh, b = e % D;
+        const int r0 = lrp[g * D + a];
+        float v;
+        if (p < nl) v = lhat[r0 + D * p + b];
+        else v = b < a ? lhat[r0 + D * nl + b] : (b == a ? 1.f : 0.f);
+        gv[slot][a][p][b] = v;
+      }
+      __syncwarp(mask);
+      double w[PASS][D][D];
+      double qp[D];
+#pragma unroll
+      for (int a = 0; a < D; ++a) qp[a] = 0.0;
+#pragma unroll
+      for (int ps = 0; ps < PASS; ++ps) {
+#pragma unroll
+        for (int a = 0; a < D; ++a)
+#pragma unroll
+          for (int b = 0; b < D; ++b) w[ps][a][b] = 0.0;
+        const int p = l + ps * KN_LANES;
+        if (p < nh) {
+          const int h = Hs[slot][p];
+          int q = 0;
+          for (int t = gptr[h]; t < gptr[h + 1] && q < nh; ++t) {
+            const int k = glist[t];
+            while (q < nh && Hs[slot][q] < k) ++q;
+            if (q < nh && Hs[slot][q] == k) {
+              float bb[D * D];
+#pragma unroll
+              for (int u = 0; u < D * D; ++u) bb[u] = ablk[(int64_t)t * D * D + u];
+#pragma unroll
+              for (int a = 0; a < D; ++a)
+#pragma unroll
+                for (int b = 0; b < D; ++b) {
+                  double acc = 0.0;
+#pragma unroll
+                  for (int c = 0; c < D; ++c) acc += (double)bb[b * D + c] * (double)gv[slot][a][q][c];
+                  w[ps][a][b] += acc;
+                }
+              ++q;
+            }
+          }
+#pragma unroll
+          for (int a = 0; a < D; ++a)
+#pragma unroll
+            for (int b = 0; b < D; ++b) qp[a] += (double)gv[slot][a][p][b] * w[ps][a][b];
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < D; ++a)
+        for (int o = KN_LANES / 2; o > 0; o >>= 1) qp[a] += __shfl_xor_sync(mask, qp[a], o, KN_LANES);
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        const int row = g * D + a;
+        if (!(qp[a] > 0.0)) {
+          if (l == 0) { atomicOr(flag, 2); sig[row] = 1.f; }
+          continue;
+        }
+        if (l == 0) { lq += log(qp[a]); sig[row] = (float)(1.0 / sqrt(qp[a])); }
+        if (!dlhat) continue;
+        const int r0 = lrp[row];
+#pragma unroll
+        for (int ps = 0; ps < PASS; ++ps) {
+          const int p = l + ps * KN_LANES;
+          if (p > nl) continue;
+#pragma unroll
+          for (int b = 0; b < D; ++b)
+            if (p < nl || b < a) dlhat[r0 + D * p + b] = (float)(2.0 * w[ps][a][b] / ((double)n * qp[a]));
+        }
+      }
+    }
+  }
+  if (!loss) return;
+  for (int o = 16; o > 0; o >>= 1) lq += __shfl_xor_sync(0xffffffffu, lq, o);
+  if ((threadIdx.x & 31) == 0) lsum[threadIdx.x >> 5] = lq;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q2 = 0; q2 < LF_THREADS / 32; ++q2) t += lsum[q2];
     atomicAdd(loss, t);
   }
 }
@@ -481,11 +671,15 @@ __global__ void lf_adam(int np, float* __restrict__ prm, const float* __restrict
 __global__ void lf_to_factor(int n, const int* __restrict__ lrp, const int* __restrict__ lci,
                              const float* __restrict__ lhat, const float* __restrict__ sig,
                              const double* __restrict__ dis, double* __restrict__ sig2, double* __restrict__ lva) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(tid / LF_LPR), l = (int)(tid % LF_LPR);
   if (i >= n) return;
-  const double s = sig[i];
-  sig2[i] = s * s * dis[i] * dis[i];
-  for (int t = lrp[i]; t < lrp[i + 1]; ++t) lva[t] = (double)lhat[t] * dis[lci[t]] / dis[i];
+  const double di = dis[i];
+  if (l == 0) {
+    const double s = sig[i];
+    sig2[i] = s * s * di * di;
+  }
+  for (int t = lrp[i] + l; t < lrp[i + 1]; t += LF_LPR) lva[t] = (double)lhat[t] * dis[lci[t]] / di;
 }
 
 int blocks(int64_t n) { return (int)((n + LF_THREADS - 1) / LF_THREADS); }
@@ -520,7 +714,7 @@ void lf_init_params(uint64_t seed, float* h) {
   h[o.w0] = -1.f;  // we = 0: the first-order factor I - tril(A^)
 }
 
-void LfGraph::prepare(const SystemData& S, const FsaiFactor& F) {
+void LfGraph::prepare(SystemData& S, const FsaiFactor& F) {
   cudaStream_t s = S.ctx->stream;
   n = (int)S.n_free;
   nnz = S.nnz;
@@ -542,11 +736,34 @@ void LfGraph::prepare(const SystemData& S, const FsaiFactor& F) {
   flag.alloc(1, s);
   lf_prep<<<blocks(n), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, S.val.p, dis.p);
   TPT_CHECK_LAUNCH();
-  lf_prep2<<<blocks(n), LF_THREADS, 0, s>>>(n, S.dpn, S.row_ptr.p, S.col.p, S.val.p, S.free_map.p, dis.p, ahat.p,
+  lf_prep2<<<blocks((int64_t)n * LF_LPR), LF_THREADS, 0, s>>>(n, S.dpn, S.row_ptr.p, S.col.p, S.val.p, S.free_map.p, dis.p, ahat.p,
                                             x0.p);
   TPT_CHECK_LAUNCH();
-  lf_pattern_values<<<blocks(n), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, ahat.p, F.rp.p, F.ci.p, al.p);
+  lf_pattern_values<<<blocks((int64_t)n * LF_LPR), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, ahat.p, F.rp.p, F.ci.p, al.p);
   TPT_CHECK_LAUNCH();
+  if (nb_checked < 0) {  // once per system: does the factor pattern have the node-block shape?
+    nb_checked = 0;
+    if (S.dpn <= 3 && nb_build_operator(S) && S.nb.dpn == S.dpn) {
+      const NbSell& N = S.nb;
+      flag.zero();
+      lf_check_blocks<<<blocks((int64_t)N.ngroups * N.dpn), LF_THREADS, 0, s>>>(N.ngroups, N.dpn, F.rp.p, F.ci.p,
+                                                                             N.gptr.p, N.glist.p, N.nlow.p, flag.p);
+      TPT_CHECK_LAUNCH();
+      int f = 0;
+      TPT_CUDA(cudaMemcpyAsync(&f, flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      TPT_CUDA(cudaStreamSynchronize(s));
+      nb_checked = f == 0 ? 1 : 0;
+    }
+  }
+  nb = nb_checked == 1;
+  if (nb) {
+    const NbSell& N = S.nb;
+    ablk.alloc(N.glist.n * N.dpn * N.dpn, s);
+    ablk.zero();
+    lf_blocks<<<blocks((int64_t)n * LF_LPR), LF_THREADS, 0, s>>>(n, N.dpn, S.row_ptr.p, S.col.p, ahat.p, N.gptr.p,
+                                                                  N.glist.p, ablk.p);
+    TPT_CHECK_LAUNCH();
+  }
   ready = true;
 }
 
@@ -562,12 +779,12 @@ void forward_impl(const SystemData& S, const FsaiFactor& F, LfGraph& G, const fl
   const float* in = G.x0.p;
   for (int l = 0; l < LF_LAYERS; ++l) {
     if (l == 0) {
-      lf_agg<D0><<<blocks(n), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, G.ahat.p, in, G.ya[l].p, G.yb[l].p);
+      lf_agg<D0><<<blocks((int64_t)n * (D0 / 4)), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, G.ahat.p, in, G.ya[l].p, G.yb[l].p);
       TPT_CHECK_LAUNCH();
       lf_layer<D0><<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o.ws[l], o.wa[l], o.wb[l], o.b[l], in, G.ya[l].p,
                                                     G.yb[l].p, G.h[l].p);
     } else {
-      lf_agg<H><<<blocks(n), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, G.ahat.p, in, G.ya[l].p, G.yb[l].p);
+      lf_agg<H><<<blocks((int64_t)n * (H / 4)), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, G.ahat.p, in, G.ya[l].p, G.yb[l].p);
       TPT_CHECK_LAUNCH();
       lf_layer<H><<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o.ws[l], o.wa[l], o.wb[l], o.b[l], in, G.ya[l].p,
                                                    G.yb[l].p, G.h[l].p);
@@ -577,12 +794,24 @@ void forward_impl(const SystemData& S, const FsaiFactor& F, LfGraph& G, const fl
   }
   lf_head_nodes<<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o, in, G.P.p, G.Q.p);
   TPT_CHECK_LAUNCH();
-  lf_head_edges<<<blocks(n), LF_THREADS, 0, s>>>(n, prm, o, F.rp.p, F.ci.p, G.al.p, G.P.p, G.Q.p, G.lhat.p);
+  lf_head_edges<<<blocks((int64_t)n * (H / 4)), LF_THREADS, 0, s>>>(n, prm, o, F.rp.p, F.ci.p, G.al.p, G.P.p, G.Q.p, G.lhat.p);
   TPT_CHECK_LAUNCH();
   G.flag.zero();
-  lf_kaporin_warp<<<ceil_div(n, LF_THREADS / 32), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, G.ahat.p, F.rp.p,
-                                                                      F.ci.p, G.lhat.p, G.sig.p, dlhat, loss,
-                                                                      G.flag.p);
+  if (G.nb) {
+    const NbSell& N = S.nb;
+    const int nb_blocks = ceil_div(N.ngroups, LF_THREADS / KN_LANES);
+#define TPT_LF_KN(D)                                                                                      \
+  lf_kaporin_nb<D><<<nb_blocks, LF_THREADS, 0, s>>>(N.ngroups, N.gptr.p, N.glist.p, G.ablk.p, F.rp.p, N.nlow.p, \
+                                                    G.lhat.p, G.sig.p, dlhat, loss, G.flag.p, n);
+    if (N.dpn == 3) { TPT_LF_KN(3) }
+    else if (N.dpn == 2) { TPT_LF_KN(2) }
+    else { TPT_LF_KN(1) }
+#undef TPT_LF_KN
+  } else {
+    lf_kaporin_warp<<<ceil_div(n, LF_THREADS / 32), LF_THREADS, 0, s>>>(n, S.row_ptr.p, S.col.p, G.ahat.p, F.rp.p,
+                                                                        F.ci.p, G.lhat.p, G.sig.p, dlhat, loss,
+                                                                        G.flag.p);
+  }
   TPT_CHECK_LAUNCH();
 }
 
@@ -674,7 +903,7 @@ void lf_adam_step(cudaStream_t s, int np, float* prm, const float* grad, float* 
 }
 
 void lf_factor_fp64(const SystemData& S, const FsaiFactor& F, const LfGraph& G, double* sig2, double* lva) {
-  lf_to_factor<<<blocks(G.n), LF_THREADS, 0, S.ctx->stream>>>(G.n, F.rp.p, F.ci.p, G.lhat.p, G.sig.p, G.dis.p, sig2,
+  lf_to_factor<<<blocks((int64_t)G.n * LF_LPR), LF_THREADS, 0, S.ctx->stream>>>(G.n, F.rp.p, F.ci.p, G.lhat.p, G.sig.p, G.dis.p, sig2,
                                                               lva);
   TPT_CHECK_LAUNCH();
 }

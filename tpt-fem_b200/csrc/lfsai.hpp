@@ -21,7 +21,12 @@ struct LfGraph {
   DevBuf<float> ya[LF_LAYERS], yb[LF_LAYERS], h[LF_LAYERS];
   DevBuf<float> P, Q, sig, lhat;
   DevBuf<int> flag;     // lf_kaporin: bit 0 row too long, bit 1 q <= 0
-  void prepare(const SystemData& S, const FsaiFactor& F);
+  // node-block form (all dofs of every free node free): A^ as dpn x dpn blocks
+  // on the node-group adjacency of the node-block operator, row-major per block
+  bool nb = false;
+  int nb_checked = -1;  // -1 not checked, 0 no, 1 yes (the pattern is fixed per system)
+  DevBuf<float> ablk;
+  void prepare(SystemData& S, const FsaiFactor& F);
 };
 
 struct LfModel {

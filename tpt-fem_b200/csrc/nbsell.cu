@@ -243,6 +243,42 @@ __global__ void fill_ksym(int ngroups, int dpn, const int* __restrict__ rp, cons
   }
 }
 
+// Values of the symmetric half storage from the CSR, structure kept: thread
+// (a, g) merges CSR row g*dpn+a with group g's lower slots (ascending block
+// columns, all below the diagonal block) and then the diagonal block.  Writes
+// for one (slot, a, b) are coalesced over the chunk's 32 lanes.
+__global__ void refill_ksym(int ngroups, int dpn, const int* __restrict__ rp, const int* __restrict__ ci,
+                            const double* __restrict__ va, const int* __restrict__ lcptr,
+                            const int* __restrict__ lcol, const int* __restrict__ nlow, double* __restrict__ lval,
+                            double* __restrict__ dval) {
+  const int lane = threadIdx.x & 31, a = threadIdx.x >> 5;  // blockDim = 32 * dpn
+  const int c = blockIdx.x, g = c * 32 + lane;
+  if (g >= ngroups || a >= dpn) return;
+  const int d2 = dpn * dpn, nl = nlow[g];
+  const int row = g * dpn + a;
+  int k = rp[row];
+  const int ke = rp[row + 1];
+  const int64_t s0 = lcptr[c], ns = lcptr[c + 1] - s0;
+  for (int64_t sl = 0; sl < ns; ++sl) {
+    const int64_t s = s0 + sl;
+    const int J = sl < nl ? lcol[s * 32 + lane] : -1;
+    for (int b = 0; b < dpn; ++b) {
+      double v = 0.0;
+      if (J >= 0) {
+        const int col = J * dpn + b;
+        while (k < ke && ci[k] < col) ++k;
+        if (k < ke && ci[k] == col) v = va[k];
+      }
+      lval[(s * d2 + a * dpn + b) * 32 + lane] = v;
+    }
+  }
+  for (int b = 0; b < dpn; ++b) {
+    const int col = g * dpn + b;
+    while (k < ke && ci[k] < col) ++k;
+    dval[((int64_t)c * d2 + a * dpn + b) * 32 + lane] = (k < ke && ci[k] == col) ? va[k] : 0.0;
+  }
+}
+
 }  // namespace
 
 void nb_build_sym(SystemData& S) {
@@ -262,20 +298,33 @@ void nb_build_sym(SystemData& S) {
                                                      N.ks_lval.p, N.ks_diag.p, N.ku_base.p);
   TPT_CHECK_LAUNCH();
   N.sym_built = true;
+  N.fresh_fill = true;
+}
+
+void nb_refill_values(SystemData& S, bool sym) {
+  NbSell& N = S.nb;
+  if (N.state != 1) return;
+  cudaStream_t s = S.ctx->stream;
+  if (sym && N.sym_built) {
+    refill_ksym<<<N.nchunks, 32 * N.dpn, 0, s>>>(N.ngroups, N.dpn, S.row_ptr.p, S.col.p, S.val.p, N.l_cptr.p,
+                                                 N.l_col.p, N.nlow.p, N.ks_lval.p, N.ks_diag.p);
+  } else {
+    fill_k<<<ceil_div(N.ngroups, 128), 128, 0, s>>>(N.ngroups, N.dpn, S.row_ptr.p, S.col.p, S.val.p, N.gptr.p,
+                                                    N.glist.p, N.k_cptr.p, N.k_col.p, N.k_val.p);
+    N.full_stale = false;
+  }
+  TPT_CHECK_LAUNCH();
+  N.fresh_fill = true;
 }
 
 void nb_refresh_values(SystemData& S) {
   NbSell& N = S.nb;
   if (N.state != 1) return;
-  cudaStream_t s = S.ctx->stream;
-  fill_k<<<ceil_div(N.ngroups, 128), 128, 0, s>>>(N.ngroups, N.dpn, S.row_ptr.p, S.col.p, S.val.p, N.gptr.p,
-                                                  N.glist.p, N.k_cptr.p, N.k_col.p, N.k_val.p);
-  TPT_CHECK_LAUNCH();
-  if (N.sym_built) {
-    fill_ksym<<<ceil_div(N.ngroups, 128), 128, 0, s>>>(N.ngroups, N.dpn, S.row_ptr.p, S.col.p, S.val.p, N.l_cptr.p,
-                                                       N.l_col.p, N.nlow.p, N.u_cptr.p, N.u_pos.p, N.u_col.p,
-                                                       N.ks_lval.p, N.ks_diag.p, N.ku_base.p);
-    TPT_CHECK_LAUNCH();
+  if (N.sym_built) {  // the full storage is refilled when a solve asks for it
+    nb_refill_values(S, true);
+    N.full_stale = true;
+  } else {
+    nb_refill_values(S, false);
   }
 }
 
@@ -321,6 +370,7 @@ bool nb_build_operator(SystemData& S) {
   fill_k<<<ceil_div(ng, 128), 128, 0, s>>>(ng, dpn, S.row_ptr.p, S.col.p, S.val.p, N.gptr.p, N.glist.p,
                                            N.k_cptr.p, N.k_col.p, N.k_val.p);
   TPT_CHECK_LAUNCH();
+  N.fresh_fill = true;
   // slot structure of L (lower) and L^T (upper)
   chunk_slots<<<cgrid, 256, 0, s>>>(ng, N.gptr.p, N.glist.p, 1, slots.p);
   TPT_CHECK_LAUNCH();
@@ -349,9 +399,10 @@ bool nb_build_operator(SystemData& S) {
   return true;
 }
 
-bool nb_fill_factor(SystemData& S, const FsaiFactor& F) {
+bool nb_factor_shape_ok(SystemData& S, const FsaiFactor& F) {
   NbSell& N = S.nb;
   cudaStream_t s = S.ctx->stream;
+  if (N.state != 1) return false;
   if (!N.factor_checked) {
     TPT_CUDA(cudaMemsetAsync(S.ctx->d_flag, 0, sizeof(int), s));
     check_factor_shape<<<ceil_div(N.ngroups, 256), 256, 0, s>>>(N.ngroups, N.dpn, F.rp.p, N.nlow.p, S.ctx->d_flag);
@@ -362,7 +413,13 @@ bool nb_fill_factor(SystemData& S, const FsaiFactor& F) {
     N.factor_checked = true;
     N.factor_ok = flag == 0;
   }
-  if (!N.factor_ok) return false;
+  return N.factor_ok;
+}
+
+bool nb_fill_factor(SystemData& S, const FsaiFactor& F) {
+  NbSell& N = S.nb;
+  cudaStream_t s = S.ctx->stream;
+  if (!nb_factor_shape_ok(S, F)) return false;
   fill_factor<<<ceil_div(N.ngroups, 128), 128, 0, s>>>(N.ngroups, N.dpn, F.rp.p, F.va.p, N.nlow.p, N.l_cptr.p,
                                                        N.l_col.p, N.u_cptr.p, N.u_col.p, N.u_pos.p, N.l_pack.p,
                                                        N.l_tail.p, N.u_pack.p, N.u_tail.p, N.l_diag.p);

@@ -149,7 +149,9 @@ __global__ void __launch_bounds__(SPMV_THREADS, 6) nb_spmv_sym(int ngroups, cons
 // half storage: each block is read once for all vectors.  Used to form
 // coarse-space products P^T A P (set-up only, not on the iteration path):
 // with gcol set, the rows of groups whose colour differs from `colour` count
-// as zero, so X can hold P for every colour at once.
+// as zero, so X can hold P for every colour at once; such blocks are not read.
+// With cmask set, chunks whose bit `colour` is clear (no group in them has a
+// neighbour of that colour) are skipped and their rows of Y left unwritten.
 template <int DPN, int NV>
 __global__ void __launch_bounds__(SPMV_THREADS) nb_spmv_sym_multi(int ngroups, const int* __restrict__ lcptr,
                                                                   const int* __restrict__ lcol,
@@ -161,13 +163,15 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_spmv_sym_multi(int ngroups, c
                                                                   const double* __restrict__ X,
                                                                   double* __restrict__ Y,
                                                                   const unsigned char* __restrict__ gcol,
-                                                                  int colour) {
+                                                                  int colour,
+                                                                  const unsigned* __restrict__ cmask) {
   constexpr int D2 = DPN * DPN;
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const int nchunks = (ngroups + 31) >> 5;
   for (int c = warp; c < nchunks; c += nw) {
+    if (cmask && !((cmask[c] >> colour) & 1u)) continue;  // uniform over the warp
     const int g = c * 32 + lane;
     if (g >= ngroups) continue;
     double acc[DPN][NV];
@@ -175,8 +179,8 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_spmv_sym_multi(int ngroups, c
     for (int a = 0; a < DPN; ++a)
 #pragma unroll
       for (int v = 0; v < NV; ++v) acc[a][v] = 0.0;
+    auto wanted = [&](int J) { return !gcol || __ldg(gcol + J) == colour; };
     auto add = [&](const double (&blk)[D2], int J, bool transposed) {
-      if (gcol && __ldg(gcol + J) != colour) return;
 #pragma unroll
       for (int b = 0; b < DPN; ++b)
 #pragma unroll
@@ -186,26 +190,30 @@ __global__ void __launch_bounds__(SPMV_THREADS) nb_spmv_sym_multi(int ngroups, c
           for (int a = 0; a < DPN; ++a) acc[a][v] += (transposed ? blk[b * DPN + a] : blk[a * DPN + b]) * xv;
         }
     };
-    {
+    if (wanted(g)) {
       double blk[D2];
 #pragma unroll
       for (int q = 0; q < D2; ++q) blk[q] = dval[((int64_t)c * D2 + q) * 32 + lane];
       add(blk, g, false);
     }
     for (int s = lcptr[c]; s < lcptr[c + 1]; ++s) {
+      const int J = lcol[(int64_t)s * 32 + lane];
+      if (!wanted(J)) continue;
       double blk[D2];
 #pragma unroll
       for (int q = 0; q < D2; ++q) blk[q] = lval[((int64_t)s * D2 + q) * 32 + lane];
-      add(blk, lcol[(int64_t)s * 32 + lane], false);
+      add(blk, J, false);
     }
     for (int s = ucptr[c]; s < ucptr[c + 1]; ++s) {
       const int64_t idx = (int64_t)s * 32 + lane;
       const int base = ubase[idx];
       if (base < 0) continue;
+      const int J = ucol[idx];
+      if (!wanted(J)) continue;
       double blk[D2];
 #pragma unroll
       for (int q = 0; q < D2; ++q) blk[q] = __ldg(lval + base + q * 32);
-      add(blk, ucol[idx], true);
+      add(blk, J, true);
     }
 #pragma unroll
     for (int a = 0; a < DPN; ++a)

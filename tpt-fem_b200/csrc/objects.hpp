@@ -16,6 +16,7 @@ struct tptfem_context {
   std::string err;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   void* cusolver = nullptr;  // cusolverDnHandle_t, created on first use
+  void* cublas = nullptr;    // cublasHandle_t, created on first use
   int* d_flag = nullptr;  // device error/validation flag scratch (one int)
   int* h_pinned = nullptr;  // pinned staging (64 bytes)
   std::map<uint64_t, int> topo_tuned;  // topopt autotuner: batch shape -> threads per instance
@@ -125,6 +126,8 @@ struct NbSell {
   bool sym_built = false;
   DevBuf<double> ks_lval, ks_diag;
   DevBuf<int> ku_base;
+  bool fresh_fill = false;  // values filled from the CSR since the last solve's set-up
+  bool full_stale = false;  // full-storage values predate the last value refresh
 };
 
 // Aggregation coarse space of a node-block system (coarse.cu): free mesh
@@ -138,6 +141,7 @@ struct CoarseSpace {
   int target = 0;               // requested aggregate count the geometry was built for
   int generation = 0;           // incremented by every (re)build: engines refresh their pointers
   int na = 0, nm = 0, nc = 0;   // aggregates, modes per aggregate, coarse size
+  int ld = 0;                   // row stride of Ainv (nc rounded up to a multiple of 4)
   int nseg = 0;                 // segments of aggregate group lists (restriction work items)
   DevBuf<int> sbeg, send;       // per segment: range in alist
   DevBuf<int> aseg;             // aggregate -> its segments (na + 1)
@@ -150,11 +154,13 @@ struct CoarseSpace {
   DevBuf<float> y;              // per group: node position minus the aggregate centroid
   DevBuf<double> T;             // per aggregate: nm x nm mode transform (columns orthonormal modes)
   DevBuf<double> Ac;            // nc x nc, then its Cholesky factor / inverse (FP64)
-  DevBuf<float> Ainv;           // nc x nc inverse (FP32, symmetric, row-major)
+  DevBuf<float> Ainv;           // nc x nc inverse (FP32, symmetric, row-major, stride ld)
   DevBuf<double> yc, uc;        // coarse vectors
   DevBuf<double> cm;            // per aggregate: raw-mode coefficients of the prolongation, T uc
   DevBuf<double> Pfull;         // P itself: per dof its nm orthonormal-mode values (geometry only)
   DevBuf<unsigned char> gcolour;  // per group: colour of its aggregate
+  DevBuf<unsigned> gmask;       // per group: bit c set iff a neighbour group (or itself) has colour c
+  DevBuf<unsigned> cmask;       // per chunk of 32 groups: OR of its groups' gmask
   bool ready = false;           // Ainv holds the inverse for the current values
 };
 
@@ -215,7 +221,9 @@ bool fsai_set_values(const SystemData& S, FsaiFactor& F, const double* d_sig2, c
 // nbsell.cu
 bool nb_build_operator(SystemData& S);  // false when the system has partial node groups
 bool nb_fill_factor(SystemData& S, const FsaiFactor& F);  // false: factor rows not node-block shaped
+bool nb_factor_shape_ok(SystemData& S, const FsaiFactor& F);  // factor rows = dpn * (lower neighbours) + a
 void nb_build_sym(SystemData& S);  // after nb_build_operator succeeded
+void nb_refill_values(SystemData& S, bool sym);  // operator values again from the CSR (symmetric or full storage)
 void nb_refresh_values(SystemData& S);  // refill the node-block values from S.val
 
 // coarse.cu
@@ -227,7 +235,8 @@ void coarse_download(const SystemData& S, int* na, int* nm, double* Ainv_or_null
 void nb_operator_apply(SystemData& S, const double* x, double* y);
 // Y = A X for the rigid_modes(dpn) interleaved vectors of X (symmetric half
 // storage); with gcol, only groups of colour `colour` contribute
-void nb_operator_apply_modes(SystemData& S, const double* X, double* Y, const unsigned char* gcol, int colour);
+void nb_operator_apply_modes(SystemData& S, const double* X, double* Y, const unsigned char* gcol, int colour,
+                             const unsigned* cmask);
 
 // solver.cu
 int64_t system_fsai_classic(SystemData& S);  // builds (once) the classic factor; -1 on failure

@@ -107,8 +107,23 @@ struct Engine {
   const SystemData* csys = nullptr;
   int cgen = -1;  // coarse-space generation the pointers in cargs belong to
   CoarseArgs cargs;
+  // side stream: the coarse restriction and solve run beside the FSAI lower pass
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   ~Engine() {
     if (exec) cudaGraphExecDestroy(exec);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
+  }
+
+  void ensure_side() {
+    if (side) return;
+    int lo = 0, hi = 0;
+    TPT_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    TPT_CUDA(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, hi));
+    TPT_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    TPT_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
   }
 
   void use_nb(const NbSell* N, bool op, bool pcnb) {
@@ -174,11 +189,18 @@ struct Engine {
     if constexpr (std::is_same<T, double>::value) {
       if (nb_pc) {
         const NbSell& N = *nb;
+        if (csys) {  // fork: P^T r and A_c^-1 on the side stream, concurrent with t = G r
+          ensure_side();
+          TPT_CUDA(cudaEventRecord(ev_fork, s));
+          TPT_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));
+          coarse_restrict_solve(*csys, r.p, side);
+          TPT_CUDA(cudaEventRecord(ev_join, side));
+        }
 #define TPT_NB_FSAI(D)                                                                                           \
   nb_fsai_lower<D><<<nb_grid, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.l_pack.p, N.l_tail.p,     \
                                                     N.l_diag.p, pc.sigma2, r.p, t.p, st.p);                       \
   TPT_CHECK_LAUNCH();                                                                                            \
-  if (csys) coarse_restrict_solve(*csys, r.p, s);                                                                \
+  if (csys) TPT_CUDA(cudaStreamWaitEvent(s, ev_join, 0));                                                        \
   nb_fsai_upper_rz<D><<<nb_grid, SPMV_THREADS, 0, s>>>(N.ngroups, N.u_cptr.p, N.u_col.p, N.u_pack.p, N.u_tail.p,  \
                                                        N.l_diag.p, t.p, r.p, z.p, st.p, partials.p, par, cargs);  \
   TPT_CHECK_LAUNCH();
@@ -271,10 +293,16 @@ void ensure_work(SystemData& S) {
 // Node-block engines use the symmetric half storage of K unless the caller
 // asks for the full operator (TPTFEM_SOLVE_FULL_OPERATOR); switching drops the
 // engine's captured graph.
+// Operator storage for this solve (symmetric half or full); on a fresh set-up
+// its values are taken from the CSR again unless they were filled since the
+// previous solve's set-up.
 void select_nb_mode(SystemData& S, Engine<double>& E, const tptfem_solver_opts& o) {
   if (!E.nb_op) return;
   const bool sym = !(o.flags & TPTFEM_SOLVE_FULL_OPERATOR);
   if (sym) nb_build_sym(S);
+  if (!sym && S.nb.full_stale) nb_refill_values(S, false);
+  else if ((o.flags & TPTFEM_SOLVE_FRESH_SETUP) && !S.nb.fresh_fill) nb_refill_values(S, sym);
+  S.nb.fresh_fill = false;
   if (E.nb_sym != sym) {
     E.nb_sym = sym;
     if (E.exec) { cudaGraphExecDestroy(E.exec); E.exec = nullptr; }
@@ -501,6 +529,7 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o_in, tptfem_solve_st
     TPT_REQUIRE(S.lmodel != nullptr, TPTFEM_ERR_INVALID_ARG, "no learned model attached to this system");
     TPT_CUDA(cudaEventRecord(ctx->ev[0], s));
     const bool fresh = (o.flags & TPTFEM_SOLVE_FRESH_SETUP) || !W.lf_ready;
+    if (o.flags & TPTFEM_SOLVE_FRESH_SETUP) W.lgraph.ready = false;  // A^ and node features from the values again
     bool ok = !fresh || learned_factor(S, W);
     if (fresh && ok && !W.lf_engine) {
       prepare_fsai_engine(S, W.f64_lf, W.lf, batch);
@@ -748,6 +777,7 @@ void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32
   });
   *ms_nb = -1.0;
   if (nb_build_operator(S)) {
+    if (S.nb.full_stale) nb_refill_values(S, false);
     const NbSell& N = S.nb;
     const int g = std::max(1, std::min(sm_count() * NB_BLOCKS_PER_SM, ceil_div((int64_t)N.nchunks * 32, SPMV_THREADS)));
     *ms_nb = timeit([&] {
@@ -809,20 +839,21 @@ void nb_operator_apply(SystemData& S, const double* x, double* y) {
   TPT_CHECK_LAUNCH();
 }
 
-void nb_operator_apply_modes(SystemData& S, const double* X, double* Y, const unsigned char* gcol, int colour) {
+void nb_operator_apply_modes(SystemData& S, const double* X, double* Y, const unsigned char* gcol, int colour,
+                             const unsigned* cmask) {
   nb_build_sym(S);
   const NbSell& N = S.nb;
   cudaStream_t s = S.ctx->stream;
   const int g = std::max(1, std::min(sm_count() * NB_BLOCKS_PER_SM, ceil_div((int64_t)N.nchunks * 32, SPMV_THREADS)));
   if (N.dpn == 3)
     nb_spmv_sym_multi<3, 6><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.ks_lval.p, N.ks_diag.p,
-                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y, gcol, colour);
+                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y, gcol, colour, cmask);
   else if (N.dpn == 2)
     nb_spmv_sym_multi<2, 3><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.ks_lval.p, N.ks_diag.p,
-                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y, gcol, colour);
+                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y, gcol, colour, cmask);
   else
     nb_spmv_sym_multi<1, 1><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.ks_lval.p, N.ks_diag.p,
-                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y, gcol, colour);
+                                                       N.u_cptr.p, N.u_col.p, N.ku_base.p, X, Y, gcol, colour, cmask);
   TPT_CHECK_LAUNCH();
 }
 
