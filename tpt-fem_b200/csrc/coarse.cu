@@ -12,7 +12,7 @@
 // mod 3, so an aggregate has at most one neighbour of each colour and
 // P^T A (P E_colour) yields whole coarse columns without mixing.  A_c is
 // factorised and inverted once per set-up, off the iteration path (cuSOLVER
-// dpotrf and trtri, one cuBLAS dsyrk), and kept as an explicit FP32 inverse, so each iteration adds one restriction, one coarse mat-vec
+// dpotrf, cuBLAS dtrsm and dsyrk), and kept as an explicit FP32 inverse, so each iteration adds one restriction, one coarse mat-vec
 // and a prolongation that is fused into the FSAI transpose kernel.
 // Requires the node-block layout (full node groups) and the mesh geometry.
 #include <cublas_v2.h>
@@ -268,12 +268,11 @@ __global__ void cs_fix_diag(int nc, double* __restrict__ Ac) {
   if (i < nc && Ac[(int64_t)i * nc + i] == 0.0) Ac[(int64_t)i * nc + i] = 1.0;
 }
 
-// Column-major lower triangle of A (diagonal included), zeros above it.
-__global__ void cs_lower_part(int nc, const double* __restrict__ A, double* __restrict__ out) {
+// The n x n identity (column-major = row-major).
+__global__ void cs_identity(int nc, double* __restrict__ out) {
   int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= (int64_t)nc * nc) return;
-  const int c = (int)(id / nc), r = (int)(id % nc);  // element (r, c) at A[c * nc + r]
-  out[id] = r >= c ? A[id] : 0.0;
+  out[id] = (id / nc == id % nc) ? 1.0 : 0.0;
 }
 
 // The inverse is left in one triangle (column-major lower = row-major
@@ -668,13 +667,8 @@ bool coarse_assemble(SystemData& S) {
   int lw1 = 0;
   TPT_REQUIRE(cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, nc, C.Ac.p, nc, &lw1) == CUSOLVER_STATUS_SUCCESS,
               TPTFEM_ERR_DEVICE, "dpotrf_bufferSize failed");
-  size_t dws = 0, hws = 0;
-  TPT_REQUIRE(cusolverDnXtrtri_bufferSize(h, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, nc, CUDA_R_64F, C.Ac.p, nc,
-                                          &dws, &hws) == CUSOLVER_STATUS_SUCCESS,
-              TPTFEM_ERR_DEVICE, "trtri_bufferSize failed");
   DevBuf<double> work;
-  work.alloc(std::max<size_t>(1, std::max<size_t>((size_t)lw1, (dws + 7) / 8)), s);
-  std::vector<char> hwork(std::max<size_t>(hws, 1));
+  work.alloc(std::max(1, lw1), s);
   DevBuf<int> info;
   info.alloc(1, s);
   int hinfo = 0;
@@ -683,18 +677,12 @@ bool coarse_assemble(SystemData& S) {
   info.download(&hinfo, 1);
   TPT_CUDA(cudaStreamSynchronize(s));
   if (hinfo != 0) return false;  // coarse matrix not positive definite in FP64
-  // A_c^-1 = L^-T L^-1: the factor inverted in place (trtri), its strictly
-  // upper part zeroed in a copy, and the product formed by one syrk into the
-  // lower triangle (a few large library calls instead of potri's many small ones)
-  TPT_REQUIRE(cusolverDnXtrtri(h, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, nc, CUDA_R_64F, C.Ac.p, nc, work.p,
-                               dws, hwork.data(), hws, info.p) == CUSOLVER_STATUS_SUCCESS,
-              TPTFEM_ERR_DEVICE, "trtri failed");
-  info.download(&hinfo, 1);
-  TPT_CUDA(cudaStreamSynchronize(s));
-  if (hinfo != 0) return false;
+  // A_c^-1 = L^-T L^-1: L^-1 from one triangular solve with the identity
+  // (lower triangular, zeros above), then one syrk into the lower triangle of
+  // Ac -- large library calls instead of potri's many small ones
   DevBuf<double> linv;
   linv.alloc((size_t)nc * nc, s);
-  cs_lower_part<<<blocks_for((int64_t)nc * nc), CS_THREADS, 0, s>>>(nc, C.Ac.p, linv.p);
+  cs_identity<<<blocks_for((int64_t)nc * nc), CS_THREADS, 0, s>>>(nc, linv.p);
   TPT_CHECK_LAUNCH();
   cublasHandle_t hb = (cublasHandle_t)S.ctx->cublas;
   if (!hb) {
@@ -703,6 +691,9 @@ bool coarse_assemble(SystemData& S) {
   }
   TPT_REQUIRE(cublasSetStream(hb, s) == CUBLAS_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "cublasSetStream failed");
   const double one = 1.0, zero = 0.0;
+  TPT_REQUIRE(cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nc, nc,
+                          &one, C.Ac.p, nc, linv.p, nc) == CUBLAS_STATUS_SUCCESS,
+              TPTFEM_ERR_DEVICE, "dtrsm failed");
   TPT_REQUIRE(cublasDsyrk(hb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, nc, nc, &one, linv.p, nc, &zero, C.Ac.p, nc) ==
                   CUBLAS_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "dsyrk failed");
   cs_symmetrize<<<blocks_for((int64_t)nc * C.ld), CS_THREADS, 0, s>>>(nc, C.ld, C.Ac.p, C.Ainv.p);
