@@ -88,7 +88,7 @@ typedef struct tptfem_solver_opts {
   int32_t max_outer;     /* unused, kept 0 */
   double rel_tol;        /* stop at ||b - A x||_2 / ||b||_2 <= rel_tol, FP64 (0 -> 1e-10) */
   double inner_rel_tol;  /* reliable-update trigger: FP64 residual replacement once the
-                            recursive residual fell by this factor (0 -> 1e-3 FP64, 5e-2 FP32) */
+                            recursive residual fell by this factor (0 -> 1e-6 FP64, 5e-2 FP32) */
   int64_t max_iter;      /* cap on total PCG iterations (0 -> 100000) */
   int32_t batch;         /* PCG iterations per CUDA-graph launch (0 -> auto) */
   int32_t flags;         /* TPTFEM_SOLVE_* bits */

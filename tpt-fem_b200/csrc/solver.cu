@@ -86,6 +86,12 @@ void launch_residual(int lanes, int grid, cudaStream_t s, int n, const int* rp, 
 
 }  // namespace
 
+// Default reliable-update trigger of the FP64 Krylov engines: the recursive
+// residual drifts little in FP64, so one intermediate replacement (at a drop of
+// 1e-6) and the final check suffice; every replacement costs a true residual
+// and a preconditioner application.
+constexpr double RELIABLE_DELTA_F64 = 1e-6;
+
 // Working-precision PCG engine with reliable updates.
 template <typename T>
 struct Engine {
@@ -564,7 +570,7 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o_in, tptfem_solve_st
       if (bb == 0.0) {
         S.x.zero();
       } else {
-        const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : 1e-3;
+        const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : RELIABLE_DELTA_F64;
         try {
           iters = run_reliable<double>(S, W.f64_lf, tol, delta, max_it, bnorm, st);
         } catch (const Error& e) {
@@ -664,7 +670,7 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o_in, tptfem_solve_st
   if (bb == 0.0) {
     S.x.zero();
   } else if (solver == TPTFEM_SOLVER_JACOBI_PCG) {
-    const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : 1e-3;
+    const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : RELIABLE_DELTA_F64;
     Engine<double>& EJ = csr_only ? W.f64_csr : W.f64;
     select_nb_mode(S, EJ, o);
     iters = run_reliable<double>(S, EJ, tol, delta, max_it, bnorm, st);
@@ -672,7 +678,7 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o_in, tptfem_solve_st
     const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : 0.05;
     iters = run_reliable<float>(S, W.f32, tol, delta, max_it, bnorm, st);
   } else {
-    const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : 1e-3;
+    const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : RELIABLE_DELTA_F64;
     iters = run_reliable<double>(S, W.f64_fsai, tol, delta, max_it, bnorm, st);
   }
   const double rel = bb == 0.0 ? 0.0 : std::sqrt(true_residual2(S, S.x.p)) / bnorm;
