@@ -202,7 +202,7 @@ WEIGHTS = os.path.join(ROOT, "tpt-fem_b200", "weights", "lfsai_elasticity.bin")
 # DRAM bytes (read + write) of one nb_spmv_sym<3> launch measured by ncu on the
 # 200x50x50 cantilever (520,200 node groups; profiles/ has the capture); the
 # bench case is scaled by its node-group count.
-NBS_TRAFFIC_200 = (356.351744 + 12.410880) * 1e6
+NBS_TRAFFIC_200 = (359.652352 + 12.161024) * 1e6
 NBS_GROUPS_200 = 520200
 
 
@@ -340,7 +340,7 @@ def run_ours(args, world, rank, local):
             "roofline": {"bound": "hbm", "kernel": op_name, "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "traffic_source": "ncu dram__bytes_read+write of nb_spmv_sym at "
-                         "200x50x50 (368.8 MB) scaled by node groups", "algorithmic_bytes": op_bytes, "ms": op_ms,
+                         "200x50x50 (371.8 MB) scaled by node groups", "algorithmic_bytes": op_bytes, "ms": op_ms,
                          "csr_formula_bytes": csr_bytes,
                          "csr_formula_gbs": csr_bytes / (op_ms * 1e-3) / 1e9,
                          "nb_full_ms": prof["nb_ms"], "csr_f64_ms": prof["csr_f64_ms"],
