@@ -491,7 +491,8 @@ def run_topopt(args, world, rank, local):
                "config": {"workload": "topopt_batch", "instances": args.instances, "oc_iterations": args.oc_iters,
                           "sizes": "nelx x nely from {60x20, 90x30, 120x40, 180x60, 240x80}",
                           "emin": 1e-9, "filter": "density, R 1.5", "dofs_per_iteration": dofs,
-                          "solver": "Jacobi-PCG per instance, FP64, rel. tol 1e-10, warm start",
+                          "solver": "two-level PCG per instance (Jacobi + plane rigid-mode aggregation coarse space), FP64, "
+                                    "rel. tol 1e-10, warm start",
                           "parallelism": f"replicas{world}"},
                "batch_seconds": sec, "tune_ms": st["tune_ms"], "threads_per_instance": st["block_threads"],
                "cpu_baseline": topopt_cpu_baseline(probs, args.oc_iters, sec),
