@@ -47,8 +47,9 @@ typedef enum tptfem_status {
   TPTFEM_ERR_OUT_OF_MEMORY = 10
 } tptfem_status;
 
-/* Cell types (crates/tpt-fem-mesh CellType; linear cells on the device path). */
-enum { TPTFEM_CELL_QUAD4 = 3, TPTFEM_CELL_TET4 = 4 };
+/* Cell types (crates/tpt-fem-mesh CellType, numbered from Line = 1; the linear
+   cells of the device path: Tri3 and Quad4 in 2-D, Tet4 in 3-D). */
+enum { TPTFEM_CELL_TRI3 = 2, TPTFEM_CELL_QUAD4 = 3, TPTFEM_CELL_TET4 = 4 };
 
 /* ElasticModel (crates/tpt-fem-elasticity/src/lib.rs:56-66). */
 enum {
@@ -138,7 +139,9 @@ size_t tptfem_last_error(const tptfem_context* ctx, char* buf, size_t len);
 tptfem_status tptfem_synchronize(tptfem_context* ctx);
 
 /* ---- meshes (crates/tpt-fem-mesh/src/lib.rs:115-148) -------------------------- */
-/* Upload coords (n_nodes x coord_dim, row-major) and conn (n_elems x 4). */
+/* Upload coords (n_nodes x coord_dim, row-major) and conn (n_elems x nodes per
+   cell: 3 for Tri3, 4 for Quad4 and Tet4), as MeshBuilder::add_node/add_element
+   would hold them (crates/tpt-fem-mesh/src/lib.rs:115-148). */
 tptfem_status tptfem_mesh_upload(tptfem_context* ctx, int cell_type, int coord_dim, const double* coords,
                                  int64_t n_nodes, const int64_t* conn, int64_t n_elems, tptfem_mesh** out);
 /* box_mesh(min, max, n) generated on the device (crates/tpt-fem-mesh-gen/src/lib.rs:422-495). */

@@ -39,3 +39,17 @@ def unit_cube_bcs(coords, dpn=1):
         for coord in (0.0, 1.0):
             nodes |= set(int(i) for i in O.nodes_on_plane(coords, axis, coord, 1e-9))
     return [(n * dpn + k, 0.0) for n in sorted(nodes) for k in range(dpn)]
+
+
+def tri_grid(nx, ny, lx=1.0, ly=1.0):
+    """Structured Tri3 grid: each cell of quad_grid split along alternating
+    diagonals into two counter-clockwise triangles."""
+    coords, quads = quad_grid(nx, ny, lx, ly)
+    tris = []
+    for k, (a, b, c, d) in enumerate(quads):
+        i, j = k % nx, k // nx
+        if (i + j) % 2 == 0:
+            tris += [[a, b, c], [a, c, d]]
+        else:
+            tris += [[a, b, d], [b, c, d]]
+    return coords, np.array(tris, dtype=np.int64)

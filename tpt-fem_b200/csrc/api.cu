@@ -82,7 +82,7 @@ std::unique_ptr<MatrixData> new_matrix(tptfem_context* ctx, tptfem_mesh* mesh, i
   TPT_REQUIRE(mesh && mesh->d, TPTFEM_ERR_INVALID_ARG, "mesh is NULL");
   MeshData& m = *mesh->d;
   TPT_REQUIRE(m.ctx == ctx, TPTFEM_ERR_INVALID_ARG, "mesh belongs to another context");
-  if (m.cell == TPTFEM_CELL_QUAD4)
+  if (m.cell == TPTFEM_CELL_QUAD4)  // Tet4 and Tri3 use one fixed rule and ignore quad_order
     TPT_REQUIRE(quad_order >= 1 && quad_order <= 5, TPTFEM_ERR_INVALID_ARG, "quad_order must be in 1..=5");
   const int64_t count = per_element ? m.n_elems : 1;
   check_coef(coef, count, physics ? "young" : "conductivity");
@@ -184,10 +184,11 @@ tptfem_status tptfem_mesh_upload(tptfem_context* ctx, int cell_type, int coord_d
   *out = nullptr;
   API_TRY
   set_device(ctx);
-  TPT_REQUIRE(cell_type == TPTFEM_CELL_TET4 || cell_type == TPTFEM_CELL_QUAD4, TPTFEM_ERR_INVALID_ARG,
-              "cell_type must be TPTFEM_CELL_TET4 or TPTFEM_CELL_QUAD4");
+  TPT_REQUIRE(cell_type == TPTFEM_CELL_TET4 || cell_type == TPTFEM_CELL_QUAD4 || cell_type == TPTFEM_CELL_TRI3,
+              TPTFEM_ERR_INVALID_ARG, "cell_type must be TPTFEM_CELL_TET4, TPTFEM_CELL_QUAD4 or TPTFEM_CELL_TRI3");
   TPT_REQUIRE(cell_type == TPTFEM_CELL_TET4 ? coord_dim == 3 : (coord_dim == 2 || coord_dim == 3),
-              TPTFEM_ERR_INVALID_ARG, "coord_dim must be 3 for Tet4 and 2 or 3 for Quad4");
+              TPTFEM_ERR_INVALID_ARG, "coord_dim must be 3 for Tet4 and 2 or 3 for Quad4 and Tri3");
+  const int npe = cell_type == TPTFEM_CELL_TRI3 ? 3 : 4;
   TPT_REQUIRE(coords && conn, TPTFEM_ERR_INVALID_ARG, "coords/conn is NULL");
   TPT_REQUIRE(n_nodes > 0 && n_nodes < (1LL << 31), TPTFEM_ERR_INVALID_ARG, "n_nodes out of range");
   TPT_REQUIRE(n_elems > 0 && n_elems < (1LL << 29), TPTFEM_ERR_INVALID_ARG, "n_elems out of range");
@@ -195,19 +196,19 @@ tptfem_status tptfem_mesh_upload(tptfem_context* ctx, int cell_type, int coord_d
   m->ctx = ctx;
   m->cell = cell_type;
   m->cdim = coord_dim;
-  m->npe = 4;
+  m->npe = npe;
   m->n_nodes = n_nodes;
   m->n_elems = n_elems;
   m->coords.alloc(n_nodes * coord_dim, ctx->stream);
   m->coords.upload(coords, n_nodes * coord_dim);
-  m->conn.alloc(n_elems * 4, ctx->stream);
+  m->conn.alloc(n_elems * npe, ctx->stream);
   {  // int64 connectivity -> int32 on the device, with the range and finiteness checks
     DevBuf<int64_t> c64;
-    c64.alloc(n_elems * 4, ctx->stream);
-    c64.upload(conn, n_elems * 4);
+    c64.alloc(n_elems * npe, ctx->stream);
+    c64.upload(conn, n_elems * npe);
     TPT_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
-    const int64_t nv = std::max<int64_t>(n_elems * 4, n_nodes * coord_dim);
-    mesh_check_convert<<<ceil_div(nv, 256), 256, 0, ctx->stream>>>(n_elems * 4, c64.p, n_nodes, m->conn.p,
+    const int64_t nv = std::max<int64_t>(n_elems * npe, n_nodes * coord_dim);
+    mesh_check_convert<<<ceil_div(nv, 256), 256, 0, ctx->stream>>>(n_elems * npe, c64.p, n_nodes, m->conn.p,
                                                                    n_nodes * coord_dim, m->coords.p, ctx->d_flag);
     TPT_CHECK_LAUNCH();
     int flag = 0;
@@ -252,7 +253,7 @@ tptfem_status tptfem_mesh_download(tptfem_context* ctx, const tptfem_mesh* mesh,
   if (coords) m.coords.download(coords, m.n_nodes * m.cdim);
   std::vector<int> c32;
   if (conn) {
-    c32.resize(m.n_elems * 4);
+    c32.resize(m.n_elems * m.npe);
     m.conn.download(c32.data(), c32.size());
   }
   TPT_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -360,7 +361,7 @@ tptfem_status tptfem_load_poisson_source(tptfem_context* ctx, tptfem_mesh* mesh,
   API_TRY
   set_device(ctx);
   MeshData& m = *mesh->d;
-  if (m.cell == TPTFEM_CELL_QUAD4)
+  if (m.cell == TPTFEM_CELL_QUAD4)  // Tet4 and Tri3 use one fixed rule and ignore quad_order
     TPT_REQUIRE(quad_order >= 1 && quad_order <= 5, TPTFEM_ERR_INVALID_ARG, "quad_order must be in 1..=5");
   TPT_REQUIRE(std::isfinite(source), TPTFEM_ERR_INVALID_ARG, "source is not finite");
   DevBuf<double> d;
@@ -377,7 +378,7 @@ tptfem_status tptfem_load_body(tptfem_context* ctx, tptfem_mesh* mesh, const dou
   API_TRY
   set_device(ctx);
   MeshData& m = *mesh->d;
-  if (m.cell == TPTFEM_CELL_QUAD4)
+  if (m.cell == TPTFEM_CELL_QUAD4)  // Tet4 and Tri3 use one fixed rule and ignore quad_order
     TPT_REQUIRE(quad_order >= 1 && quad_order <= 5, TPTFEM_ERR_INVALID_ARG, "quad_order must be in 1..=5");
   const int dim = m.cell == TPTFEM_CELL_TET4 ? 3 : 2;
   check_coef(body, dim, "body force");

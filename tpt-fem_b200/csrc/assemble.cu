@@ -72,7 +72,7 @@ bool gauss_legendre(int order, double* p, double* w) {
   }
 }
 
-// cell_quad (crates/tpt-fem-thermal/src/lib.rs:29-92) for Tet4 / Quad4, plus
+// cell_quad (crates/tpt-fem-thermal/src/lib.rs:29-92) for Tet4 / Tri3 / Quad4, plus
 // the shape values and reference gradients at each point.
 QuadTab make_cell_tab(int cell, int order) {
   QuadTab t{};
@@ -85,6 +85,17 @@ QuadTab make_cell_tab(int cell, int order) {
       double x = pts[q][0], y = pts[q][1], z = pts[q][2];
       t.ns[q][0] = 1.0 - x - y - z;
       t.ns[q][1] = x; t.ns[q][2] = y; t.ns[q][3] = z;
+    }
+    return t;
+  }
+  if (cell == TPTFEM_CELL_TRI3) {  // triangle(Degree2), quadrature:223-234; order ignored
+    const double pts[3][2] = {{2.0 / 3.0, 1.0 / 6.0}, {1.0 / 6.0, 2.0 / 3.0}, {1.0 / 6.0, 1.0 / 6.0}};
+    t.nq = 3;
+    for (int q = 0; q < 3; ++q) {
+      t.w[q] = 1.0 / 6.0;
+      double x = pts[q][0], y = pts[q][1];
+      t.ns[q][0] = 1.0 - x - y;  // Tri3 shape (element:106-120)
+      t.ns[q][1] = x; t.ns[q][2] = y;
     }
     return t;
   }
@@ -167,6 +178,33 @@ __device__ __forceinline__ bool tet_geom(const double (&X)[4][3], TetGeom& G) {
     G.g[1][i] = iv[i];
     G.g[2][i] = iv[3 + i];
     G.g[3][i] = iv[6 + i];
+  }
+  G.adet = fabs(det);
+  return isfinite(inv) && isfinite(det);
+}
+
+// Tri3: J[p][r] = X[r+1][p] - X[0][p] (the running sum of Map::from_nodes_and_grad
+// for the constant Tri3 gradients), det and inverse by the 2 x 2 cofactors of
+// element:624-680, physical gradients as physical_grad's running sum.
+struct TriGeom {
+  double g[3][2];
+  double adet;
+};
+
+__device__ __forceinline__ bool tri_geom(const double (&X)[4][2], TriGeom& G) {
+  double m[4];
+#pragma unroll
+  for (int p = 0; p < 2; ++p)
+#pragma unroll
+    for (int r = 0; r < 2; ++r) m[p * 2 + r] = X[r + 1][p] - X[0][p];
+  double det = m[0] * m[3] - m[1] * m[2];
+  double inv = 1.0 / det;
+  double iv[4] = {m[3] * inv, -m[1] * inv, -m[2] * inv, m[0] * inv};
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    G.g[0][i] = -iv[i] - iv[2 + i];
+    G.g[1][i] = iv[i];
+    G.g[2][i] = iv[2 + i];
   }
   G.adet = fabs(det);
   return isfinite(inv) && isfinite(det);
@@ -265,22 +303,36 @@ struct ElemIn {
   double nu;
 };
 
+// SD: spatial dimension; NV: nodes per element (arrays below hold 4 slots,
+// a Tri3 element uses the first 3).
 template <int CELL>
 struct CellTraits;
 template <>
 struct CellTraits<TPTFEM_CELL_TET4> {
-  static constexpr int SD = 3;
+  static constexpr int SD = 3, NV = 4;
 };
 template <>
 struct CellTraits<TPTFEM_CELL_QUAD4> {
-  static constexpr int SD = 2;
+  static constexpr int SD = 2, NV = 4;
+};
+template <>
+struct CellTraits<TPTFEM_CELL_TRI3> {
+  static constexpr int SD = 2, NV = 3;
 };
 
 template <int CELL>
 __device__ __forceinline__ void load_elem(const ElemIn& in, int e, double (&X)[4][CellTraits<CELL>::SD],
                                           int (&nodes)[4]) {
-  int4 c = reinterpret_cast<const int4*>(in.conn)[e];
-  nodes[0] = c.x; nodes[1] = c.y; nodes[2] = c.z; nodes[3] = c.w;
+  constexpr int NV = CellTraits<CELL>::NV;
+  if constexpr (NV == 4) {
+    int4 c = reinterpret_cast<const int4*>(in.conn)[e];
+    nodes[0] = c.x; nodes[1] = c.y; nodes[2] = c.z; nodes[3] = c.w;
+  } else {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) nodes[j] = __ldg(in.conn + (int64_t)e * NV + j);
+#pragma unroll
+    for (int j = NV; j < 4; ++j) nodes[j] = nodes[0];
+  }
 #pragma unroll
   for (int j = 0; j < 4; ++j)
 #pragma unroll
@@ -318,6 +370,31 @@ __device__ __forceinline__ bool element_row(const double (&X)[4][CellTraits<CELL
           double v = t + t;
           v = v + t;
           out[j * 3 + b] = v + t;
+        }
+    }
+  } else if constexpr (CELL == TPTFEM_CELL_TRI3) {  // constant Jacobian, three equal-weight points
+    TriGeom G;
+    ok = tri_geom(X, G);
+    const double w = c_cell.w[0];
+    if constexpr (PHYS == 0) {
+      const double wk = w * coef;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        double dot = G.g[l][0] * G.g[j][0] + G.g[l][1] * G.g[j][1];
+        double t = wk * dot * G.adet;
+        double v = t + t;  // three identical quadrature points, summed in order
+        out[j] = v + t;
+      }
+    } else {
+      Dmat D = make_d(model, coef, nu);
+      const double wd = w * G.adet;
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          double t = wd * bdb2(G.g[l], G.g[j], a, b, D);
+          double v = t + t;
+          out[j * 2 + b] = v + t;
         }
     }
   } else {  // Quad4: the Jacobian varies per point
@@ -400,7 +477,7 @@ __global__ void __launch_bounds__(128) assemble_rows(RowArgs A) {
     ok &= element_row<CELL, PHYS, DPN>(X, coef, A.in.model, A.in.nu, l, a, out);
     const int sj[4] = {sl.x, sl.y, sl.z, sl.w};
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < CellTraits<CELL>::NV; ++j)
 #pragma unroll
       for (int b = 0; b < DPN; ++b) {
         const int s = (sj[j] * DPN + b) * T + tid;
@@ -476,6 +553,16 @@ __global__ void load_rows(LoadArgs A) {
 #pragma unroll
           for (int a = 0; a < DPN; ++a) f[a] = f[a] + w * N * A.b[a] * G.adet;
       }
+    } else if constexpr (CELL == TPTFEM_CELL_TRI3) {
+      TriGeom G;
+      ok &= tri_geom(X, G);
+      for (int q = 0; q < nq; ++q) {
+        const double w = c_cell.w[q], N = c_cell.ns[q][l];
+        if (KIND == 0) f[0] = f[0] + w * A.b[0] * N * G.adet;
+        else
+#pragma unroll
+          for (int a = 0; a < DPN; ++a) f[a] = f[a] + w * N * A.b[a] * G.adet;
+      }
     } else {
       for (int q = 0; q < nq; ++q) {
         QuadGeom G;
@@ -513,8 +600,10 @@ template <int CELL>
 __global__ void traction_rows(TractionArgs A) {
   constexpr int SD = CellTraits<CELL>::SD;
   constexpr int FN = (CELL == TPTFEM_CELL_TET4) ? 3 : 2;
+  constexpr int NV = CellTraits<CELL>::NV, NF = (CELL == TPTFEM_CELL_TRI3) ? 3 : 4;
   const int tet_f[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
   const int quad_f[4][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}};
+  const int tri_f[3][2] = {{1, 2}, {2, 0}, {0, 1}};
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= A.n_nodes) return;
   double acc[3];
@@ -526,12 +615,12 @@ __global__ void traction_rows(TractionArgs A) {
     double X[4][SD];
     int nodes[4];
     load_elem<CELL>(A.in, e, X, nodes);
-    for (int fi = 0; fi < 4; ++fi) {
+    for (int fi = 0; fi < NF; ++fi) {
       if (!(bm & (1u << fi))) continue;
       int fl[3];
       int kpos = -1;
       for (int q = 0; q < FN; ++q) {
-        fl[q] = (CELL == TPTFEM_CELL_TET4) ? tet_f[fi][q] : quad_f[fi][q];
+        fl[q] = (CELL == TPTFEM_CELL_TET4) ? tet_f[fi][q] : (CELL == TPTFEM_CELL_TRI3 ? tri_f[fi][q] : quad_f[fi][q]);
         if (fl[q] == l) kpos = q;
       }
       if (kpos < 0) continue;
@@ -562,8 +651,8 @@ __global__ void traction_rows(TractionArgs A) {
 #pragma unroll
       for (int d = 0; d < SD; ++d) {
         double s = 0.0;
-        for (int j = 0; j < 4; ++j) s = s + X[j][d];
-        ec[d] = s / 4.0;
+        for (int j = 0; j < NV; ++j) s = s + X[j][d];
+        ec[d] = s / (double)NV;
         double f = 0.0;
         for (int q = 0; q < FN; ++q) f = f + X[fl[q]][d];
         fc[d] = f / (double)FN;
@@ -631,6 +720,9 @@ void dispatch_rows(const MatrixData& M, int mode, const RowArgs& A, cudaStream_t
   if (cell == TPTFEM_CELL_TET4) {
     if (M.physics == 0) launch_rows<TPTFEM_CELL_TET4, 0, 1>(mode, A, s);
     else launch_rows<TPTFEM_CELL_TET4, 1, 3>(mode, A, s);
+  } else if (cell == TPTFEM_CELL_TRI3) {
+    if (M.physics == 0) launch_rows<TPTFEM_CELL_TRI3, 0, 1>(mode, A, s);
+    else launch_rows<TPTFEM_CELL_TRI3, 1, 2>(mode, A, s);
   } else {
     if (M.physics == 0) launch_rows<TPTFEM_CELL_QUAD4, 0, 1>(mode, A, s);
     else launch_rows<TPTFEM_CELL_QUAD4, 1, 2>(mode, A, s);
@@ -674,11 +766,11 @@ void assemble_matrix(MatrixData& M) {
   MeshData& m = *M.mesh;
   tptfem_context* ctx = M.ctx;
   cudaStream_t s = ctx->stream;
-  TPT_REQUIRE(m.cell == TPTFEM_CELL_TET4 || m.cell == TPTFEM_CELL_QUAD4, TPTFEM_ERR_INVALID_ARG,
-              "device assembly supports Tet4 and Quad4 meshes");
+  TPT_REQUIRE(m.cell == TPTFEM_CELL_TET4 || m.cell == TPTFEM_CELL_QUAD4 || m.cell == TPTFEM_CELL_TRI3,
+              TPTFEM_ERR_INVALID_ARG, "device assembly supports Tet4, Quad4 and Tri3 meshes");
   if (M.physics == 1) {
     bool okm = (m.cell == TPTFEM_CELL_TET4 && M.model == TPTFEM_MODEL_CONTINUUM_3D) ||
-               (m.cell == TPTFEM_CELL_QUAD4 &&
+               ((m.cell == TPTFEM_CELL_QUAD4 || m.cell == TPTFEM_CELL_TRI3) &&
                 (M.model == TPTFEM_MODEL_PLANE_STRESS || M.model == TPTFEM_MODEL_PLANE_STRAIN));
     TPT_REQUIRE(okm, TPTFEM_ERR_MODEL_DIM_MISMATCH,
                 "elasticity model/dimension mismatch: model is incompatible with the mesh's spatial dimension");
@@ -741,6 +833,7 @@ void load_poisson_source(MeshData& m, double src, int quad_order, double* d_rhs)
   A.rhs = d_rhs;
   A.flag = ctx->d_flag;
   if (m.cell == TPTFEM_CELL_TET4) load_rows<TPTFEM_CELL_TET4, 0, 1><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
+  else if (m.cell == TPTFEM_CELL_TRI3) load_rows<TPTFEM_CELL_TRI3, 0, 1><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
   else load_rows<TPTFEM_CELL_QUAD4, 0, 1><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
   TPT_CHECK_LAUNCH();
   TPT_REQUIRE((read_flag(ctx) & 1) == 0, TPTFEM_ERR_NUMERIC, "degenerate element in load integration");
@@ -761,6 +854,7 @@ void load_body(MeshData& m, const double* body, int quad_order, double* d_rhs) {
   A.rhs = d_rhs;
   A.flag = ctx->d_flag;
   if (m.cell == TPTFEM_CELL_TET4) load_rows<TPTFEM_CELL_TET4, 1, 3><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
+  else if (m.cell == TPTFEM_CELL_TRI3) load_rows<TPTFEM_CELL_TRI3, 1, 2><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
   else load_rows<TPTFEM_CELL_QUAD4, 1, 2><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
   TPT_CHECK_LAUNCH();
   TPT_REQUIRE((read_flag(ctx) & 1) == 0, TPTFEM_ERR_NUMERIC, "degenerate element in load integration");
@@ -786,6 +880,7 @@ void apply_traction(MeshData& m, int dpn, int axis, double sign, const double* t
   for (int c = 0; c < 3; ++c) A.t[c] = c < dpn ? t[c] : 0.0;
   A.rhs = d_rhs;
   if (m.cell == TPTFEM_CELL_TET4) traction_rows<TPTFEM_CELL_TET4><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
+  else if (m.cell == TPTFEM_CELL_TRI3) traction_rows<TPTFEM_CELL_TRI3><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
   else traction_rows<TPTFEM_CELL_QUAD4><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
   TPT_CHECK_LAUNCH();
 }

@@ -148,19 +148,21 @@ __global__ void incidence_slots(const int* __restrict__ conn, int npe, const int
 
 // Boundary faces (crates/tpt-fem-assembly/src/lib.rs:563-583): a face is on the
 // boundary iff no other element holds all of its nodes.  Face tables follow
-// TET_FACES / QUAD_FACES (assembly:61-96).
+// TRI_FACES / QUAD_FACES / TET_FACES (assembly:46-96).
 __global__ void boundary_face_mask(const int* __restrict__ conn, int cell, int npe, const int* __restrict__ ne_ptr,
                                    const int* __restrict__ ne, int64_t n_elems, unsigned char* __restrict__ mask) {
   int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n_elems) return;
   const int tet_f[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
   const int quad_f[4][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}};
-  int nf = 4, fn = (cell == TPTFEM_CELL_TET4) ? 3 : 2;
+  const int tri_f[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+  const int nf = cell == TPTFEM_CELL_TRI3 ? 3 : 4, fn = (cell == TPTFEM_CELL_TET4) ? 3 : 2;
   unsigned char m = 0;
   for (int f = 0; f < nf; ++f) {
     int v[3];
     for (int q = 0; q < fn; ++q)
-      v[q] = conn[e * npe + (cell == TPTFEM_CELL_TET4 ? tet_f[f][q] : quad_f[f][q])];
+      v[q] = conn[e * npe + (cell == TPTFEM_CELL_TET4 ? tet_f[f][q]
+                                                       : (cell == TPTFEM_CELL_TRI3 ? tri_f[f][q] : quad_f[f][q]))];
     bool shared = false;
     for (int k = ne_ptr[v[0]]; k < ne_ptr[v[0] + 1] && !shared; ++k) {
       int o = ne[k] >> 2;

@@ -17,7 +17,7 @@ import ctypes as C
 import numpy as np
 
 from . import _native as N
-from ._native import (CELL_QUAD4, CELL_TET4, MODEL_BAR_AXIAL, MODEL_CONTINUUM_3D, MODEL_PLANE_STRAIN,
+from ._native import (CELL_QUAD4, CELL_TET4, CELL_TRI3, MODEL_BAR_AXIAL, MODEL_CONTINUUM_3D, MODEL_PLANE_STRAIN,
                       MODEL_PLANE_STRESS, SOLVER_FSAI_MP_PCG, SOLVER_JACOBI_PCG, SOLVER_LEARNED_FSAI_PCG,
                       SOLVER_MP_PCG, SolverOpts,
                       SolveStats)
@@ -25,7 +25,7 @@ from ._native import (CELL_QUAD4, CELL_TET4, MODEL_BAR_AXIAL, MODEL_CONTINUUM_3D
 __all__ = [
     "TptFemError", "Context", "Mesh", "Matrix", "System", "assemble_poisson", "assemble_elasticity",
     "load_poisson_source", "load_body", "apply_traction", "reduce_system", "solve_with_dirichlet",
-    "solve_poisson", "solve_elasticity", "SolverOpts", "SolveStats", "CELL_TET4", "CELL_QUAD4",
+    "solve_poisson", "solve_elasticity", "SolverOpts", "SolveStats", "CELL_TET4", "CELL_QUAD4", "CELL_TRI3",
     "MODEL_CONTINUUM_3D", "MODEL_PLANE_STRESS", "MODEL_PLANE_STRAIN", "SOLVER_JACOBI_PCG", "SOLVER_MP_PCG",
     "SOLVER_FSAI_MP_PCG", "SOLVER_LEARNED_FSAI_PCG",
 ]
@@ -122,7 +122,7 @@ class Mesh:
     def _download(self):
         if self._coords is None:
             c = np.zeros((self.n_nodes, self.cdim))
-            e = np.zeros((self.n_elems, 4), dtype=np.int64)
+            e = np.zeros((self.n_elems, 3 if self.cell == CELL_TRI3 else 4), dtype=np.int64)
             self.ctx.check(self.ctx.lib.tptfem_mesh_download(self.ctx.h, self.h, N.ptr(c), N.ptr(e)))
             self._coords, self._conn = c, e
 

@@ -18,7 +18,7 @@ STATUS_NAMES = {
     0: "OK", 1: "CREATION", 2: "SYMBOLIC", 3: "NUMERIC", 4: "MODEL_DIM_MISMATCH", 5: "NOT_CONVERGED",
     6: "BREAKDOWN", 7: "DEVICE", 8: "TIMEOUT", 9: "INVALID_ARG", 10: "OUT_OF_MEMORY",
 }
-CELL_QUAD4, CELL_TET4 = 3, 4
+CELL_TRI3, CELL_QUAD4, CELL_TET4 = 2, 3, 4
 MODEL_BAR_AXIAL, MODEL_PLANE_STRESS, MODEL_PLANE_STRAIN, MODEL_CONTINUUM_3D = 0, 1, 2, 3
 SOLVER_JACOBI_PCG, SOLVER_MP_PCG, SOLVER_FSAI_MP_PCG, SOLVER_LEARNED_FSAI_PCG = 0, 1, 2, 3
 SOLVE_FRESH_SETUP = 1
