@@ -166,6 +166,16 @@ void tptfem_mesh_free(tptfem_mesh* mesh);
  * crates/tpt-fem-assembly/src/lib.rs:458-480. */
 tptfem_status tptfem_assemble_poisson(tptfem_context* ctx, tptfem_mesh* mesh, const double* conductivity,
                                       int per_element, int quad_order, tptfem_matrix** out);
+/* assemble(mesh, 1, poisson_element_matrix) followed by apply_robin(mesh, 1, h, coo)
+ * (crates/tpt-fem-thermal/src/lib.rs:218-237, crates/tpt-fem-assembly/src/lib.rs:674-753):
+ * the Robin coefficient is robin_h on the boundary faces whose outward unit normal n
+ * has robin_sign * n[robin_axis] > 0.5 and zero on the others; robin_axis < 0 puts
+ * robin_h on every boundary face.  As in the reference, every pair of nodes of a
+ * boundary face gets a matrix entry (the Robin pushes are not zero-skipped) and the
+ * Robin terms are summed after the element terms.  Reassembly keeps the term. */
+tptfem_status tptfem_assemble_poisson_robin(tptfem_context* ctx, tptfem_mesh* mesh, const double* conductivity,
+                                            int per_element, int quad_order, int robin_axis, double robin_sign,
+                                            double robin_h, tptfem_matrix** out);
 /* try_assemble(mesh, dim, elasticity_element_matrix) -- crates/tpt-fem-elasticity/src/lib.rs:262-309,
  * crates/tpt-fem-assembly/src/lib.rs:428-450. */
 tptfem_status tptfem_assemble_elasticity(tptfem_context* ctx, tptfem_mesh* mesh, int model, const double* young,

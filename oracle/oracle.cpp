@@ -640,11 +640,56 @@ void apply_neumann(const OMesh& m, int dpn, flux_cb cb, void* ud, double* rhs, i
   }
 }
 
+// apply_robin_order (assembly:684-753): for every boundary face and face
+// quadrature point, h(x, n) N_k N_l is pushed onto `coo` for each pair (k, l)
+// of the face's nodes and each component, after whatever `coo` already holds
+// (solve_poisson calls it after `assemble`, thermal:235-237).  No zero-skip.
+void apply_robin(const OMesh& m, int dpn, flux_cb cb, void* ud, Coo& coo, int order) {
+  auto faces = faces_of(m.cell);
+  for (auto& bf : boundary_faces(m)) {
+    i64 eid = bf.first;
+    const FaceDef& f = faces[bf.second];
+    auto phys = elem_phys(m, eid);
+    vector<vector<double>> qp; vector<double> qw;
+    cell_quad(f.face, order, qp, qw);
+    int dim = (int)phys[0].size();
+    auto ec = mean_of(phys);
+    vector<vector<double>> fc;
+    for (int i : f.nodes) fc.push_back(phys[i]);
+    auto fcen = mean_of(fc);
+    for (size_t q = 0; q < qp.size(); ++q) {
+      double w = qw[q];
+      auto ns = ref_shape(f.face, qp[q]);
+      auto ng = ref_grad(f.face, qp[q]);
+      vector<double> xp(dim, 0.0);
+      for (size_t k = 0; k < f.nodes.size(); ++k)
+        for (int d = 0; d < dim; ++d) xp[d] += ns[k] * phys[f.nodes[k]][d];
+      size_t fd = ng[0].size();
+      vector<vector<double>> tangents(fd, vector<double>(dim, 0.0));
+      for (size_t mm = 0; mm < fd; ++mm)
+        for (size_t k = 0; k < f.nodes.size(); ++k)
+          for (int d = 0; d < dim; ++d) tangents[mm][d] += ng[k][mm] * phys[f.nodes[k]][d];
+      double measure; vector<double> normal;
+      surface(tangents, dim, measure, normal);
+      vector<double> dir(dim);
+      for (int d = 0; d < dim; ++d) dir[d] = fcen[d] - ec[d];
+      if (rsum_dot(normal, dir) < 0.0) for (auto& v : normal) v = -v;
+      double h = cb(xp.data(), normal.data(), dim, ud);
+      for (size_t k = 0; k < f.nodes.size(); ++k)
+        for (size_t l = 0; l < f.nodes.size(); ++l) {
+          i64 bi = m.elems[eid][f.nodes[k]] * dpn, bj = m.elems[eid][f.nodes[l]] * dpn;
+          for (int c = 0; c < dpn; ++c) coo.push(bi + c, bj + c, w * measure * h * ns[k] * ns[l]);
+        }
+    }
+  }
+}
+
 // Built-in flux: value `val` where the outward normal's `axis` component
 // times `sign` exceeds 0.5, zero elsewhere (a traction on one box face).
 struct FaceSel { int axis; double sign; double val; };
 double facesel_flux(const double*, const double* n, int, void* ud) {
   FaceSel* s = (FaceSel*)ud;
+  if (s->axis < 0) return s->val;  // every boundary face
   return (n[s->axis] * s->sign > 0.5) ? s->val : 0.0;
 }
 
@@ -877,6 +922,14 @@ void orc_apply_neumann_cb(OrcMesh* h, int dpn, flux_cb cb, void* ud, int order, 
 void orc_apply_traction(OrcMesh* h, int dpn, int axis, double sign, double val, unsigned comp_mask, double* rhs) {
   FaceSel s{axis, sign, val};
   apply_neumann(h->m, dpn, facesel_flux, &s, rhs, 2, comp_mask);
+}
+// apply_robin_order with the built-in face selector (axis < 0: every boundary face).
+void orc_apply_robin(OrcCoo* c, OrcMesh* h, int dpn, int axis, double sign, double val) {
+  FaceSel s{axis, sign, val};
+  apply_robin(h->m, dpn, facesel_flux, &s, c->c, 2);
+}
+void orc_apply_robin_cb(OrcCoo* c, OrcMesh* h, int dpn, flux_cb cb, void* ud, int order) {
+  apply_robin(h->m, dpn, cb, ud, c->c, order);
 }
 i64 orc_boundary_face_count(OrcMesh* h) { return (i64)boundary_faces(h->m).size(); }
 

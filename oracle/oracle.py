@@ -72,6 +72,8 @@ def lib():
         "orc_load_poisson_source_cb": (C.c_int, [_vp, SOURCE_CB, _vp, C.c_int, _f64p]),
         "orc_load_body": (C.c_int, [_vp, _f64p, C.c_int, _f64p]),
         "orc_apply_neumann_cb": (None, [_vp, C.c_int, FLUX_CB, _vp, C.c_int, C.c_uint, _f64p]),
+        "orc_apply_robin": (None, [_vp, _vp, C.c_int, C.c_int, C.c_double, C.c_double]),
+        "orc_apply_robin_cb": (None, [_vp, _vp, C.c_int, FLUX_CB, _vp, C.c_int]),
         "orc_apply_traction": (None, [_vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_uint, _f64p]),
         "orc_boundary_face_count": (_i64, [_vp]),
         "orc_reduce_system": (_vp, [_vp, _f64p, _i64, _i64p, _f64p, _i64]),
@@ -301,6 +303,22 @@ def apply_neumann(mesh, dpn, flux, rhs, order=2, comp_mask=0xFFFFFFFF):
 def apply_traction(mesh, dpn, axis, sign, value, comp_mask, rhs):
     lib().orc_apply_traction(mesh.h, dpn, axis, sign, value, comp_mask, rhs)
     return rhs
+
+
+def apply_robin(coo, mesh, dpn, coeff, order=2):
+    """apply_robin_order (assembly/src/lib.rs:684-753) onto `coo`; coeff(x, n) -> float."""
+    def cb(xp, nrm, dim, _ud):
+        return float(coeff([xp[i] for i in range(dim)], [nrm[i] for i in range(dim)]))
+    ccb = FLUX_CB(cb)
+    lib().orc_apply_robin_cb(coo.h, mesh.h, dpn, ccb, None, order)
+    return coo
+
+
+def apply_robin_selected(coo, mesh, dpn, axis, sign, h):
+    """apply_robin with h on the faces whose outward normal n has sign*n[axis] > 0.5
+    (axis < 0: every boundary face), zero elsewhere."""
+    lib().orc_apply_robin(coo.h, mesh.h, dpn, axis, sign, h)
+    return coo
 
 
 def boundary_face_count(mesh):

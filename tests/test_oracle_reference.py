@@ -228,3 +228,11 @@ def test_pcg_jacobi_matches_dense_lu_on_config1():
     x, it, rel = O.pcg_jacobi(kred.to_csr(), fred, tol=1e-13)
     assert it > 0 and rel < 1e-12
     assert np.max(np.abs(x - x_lu)) < 1e-12 * np.max(np.abs(x_lu))
+
+
+def test_robin_conserves_total_measure():  # assembly:835
+    m = O.Mesh(O.CELL_TRI, np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]]), np.array([[0, 1, 2]]))
+    coo = O.apply_robin(O.Coo(), m, 1, lambda x, n: 1.0)
+    assert abs(coo.to_csr().values.sum() - (2.0 + 2.0 ** 0.5)) < 1e-9
+    sel = O.apply_robin_selected(O.Coo(), m, 1, -1, 1.0, 1.0)
+    assert np.array_equal(sel.to_csr().values, coo.to_csr().values)

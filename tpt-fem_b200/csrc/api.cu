@@ -77,8 +77,14 @@ void check_coef(const double* coef, int64_t count, const char* what) {
     TPT_REQUIRE(std::isfinite(coef[i]), TPTFEM_ERR_INVALID_ARG, std::string(what) + " holds a non-finite value");
 }
 
+struct RobinSpec {
+  int on = 0, axis = -1;
+  double sign = 1.0, h = 0.0;
+};
+
 std::unique_ptr<MatrixData> new_matrix(tptfem_context* ctx, tptfem_mesh* mesh, int physics, int model,
-                                       const double* coef, int per_element, double nu, int quad_order) {
+                                       const double* coef, int per_element, double nu, int quad_order,
+                                       RobinSpec robin = RobinSpec{}) {
   TPT_REQUIRE(mesh && mesh->d, TPTFEM_ERR_INVALID_ARG, "mesh is NULL");
   MeshData& m = *mesh->d;
   TPT_REQUIRE(m.ctx == ctx, TPTFEM_ERR_INVALID_ARG, "mesh belongs to another context");
@@ -97,6 +103,10 @@ std::unique_ptr<MatrixData> new_matrix(tptfem_context* ctx, tptfem_mesh* mesh, i
   M->per_element = per_element ? 1 : 0;
   M->coef.alloc(count, ctx->stream);
   M->coef.upload(coef, count);
+  M->robin = robin.on;
+  M->robin_axis = robin.axis;
+  M->robin_sign = robin.sign;
+  M->robin_h = robin.h;
   assemble_matrix(*M);
   return M;
 }
@@ -272,6 +282,25 @@ tptfem_status tptfem_assemble_poisson(tptfem_context* ctx, tptfem_mesh* mesh, co
   API_TRY
   set_device(ctx);
   auto M = new_matrix(ctx, mesh, 0, 0, conductivity, per_element, 0.0, quad_order);
+  *out = new tptfem_matrix{std::move(M)};
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_assemble_poisson_robin(tptfem_context* ctx, tptfem_mesh* mesh, const double* conductivity,
+                                            int per_element, int quad_order, int robin_axis, double robin_sign,
+                                            double robin_h, tptfem_matrix** out) {
+  if (!ctx || !out) return TPTFEM_ERR_INVALID_ARG;
+  *out = nullptr;
+  API_TRY
+  set_device(ctx);
+  TPT_REQUIRE(std::isfinite(robin_h) && std::isfinite(robin_sign), TPTFEM_ERR_INVALID_ARG,
+              "robin coefficient or sign is not finite");
+  RobinSpec r;
+  r.on = 1;
+  r.axis = robin_axis < 0 ? -1 : robin_axis;
+  r.sign = robin_sign;
+  r.h = robin_h;
+  auto M = new_matrix(ctx, mesh, 0, 0, conductivity, per_element, 0.0, quad_order, r);
   *out = new tptfem_matrix{std::move(M)};
   API_CATCH(ctx)
 }

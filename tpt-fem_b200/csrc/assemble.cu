@@ -339,6 +339,79 @@ __device__ __forceinline__ void load_elem(const ElemIn& in, int e, double (&X)[4
     for (int p = 0; p < CellTraits<CELL>::SD; ++p) X[j][p] = __ldg(in.coords + (int64_t)nodes[j] * in.cdim + p);
 }
 
+// ---- boundary faces -------------------------------------------------------------
+
+template <int CELL>
+struct FaceTraits;
+template <>
+struct FaceTraits<TPTFEM_CELL_TET4> {
+  static constexpr int NF = 4, FN = 3;
+  __device__ static int node(int f, int q) {
+    const int t[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
+    return t[f][q];
+  }
+};
+template <>
+struct FaceTraits<TPTFEM_CELL_QUAD4> {
+  static constexpr int NF = 4, FN = 2;
+  __device__ static int node(int f, int q) {
+    const int t[4][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}};
+    return t[f][q];
+  }
+};
+template <>
+struct FaceTraits<TPTFEM_CELL_TRI3> {
+  static constexpr int NF = 3, FN = 2;
+  __device__ static int node(int f, int q) {
+    const int t[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+    return t[f][q];
+  }
+};
+
+// Measure and outward unit normal of face fl of an element, as
+// apply_neumann_order / apply_robin_order compute them (assembly:394-420,
+// 617-653): tangents from the face's reference gradients, the normal turned
+// to point from the element centroid to the face centroid.
+template <int CELL, int SD>
+__device__ __forceinline__ void face_geometry(const double (&X)[4][SD], const int (&fl)[3], double& measure,
+                                              double (&nrm)[SD]) {
+  constexpr int FN = FaceTraits<CELL>::FN, NV = CellTraits<CELL>::NV;
+  if constexpr (CELL == TPTFEM_CELL_TET4) {
+    double t0[3], t1[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      t0[d] = X[fl[1]][d] - X[fl[0]][d];
+      t1[d] = X[fl[2]][d] - X[fl[0]][d];
+    }
+    double c[3] = {t0[1] * t1[2] - t0[2] * t1[1], t0[2] * t1[0] - t0[0] * t1[2], t0[0] * t1[1] - t0[1] * t1[0]};
+    measure = sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    for (int d = 0; d < 3; ++d) nrm[d] = c[d] / measure;
+  } else {
+    double t[2];
+#pragma unroll
+    for (int d = 0; d < 2; ++d) t[d] = -0.5 * X[fl[0]][d] + 0.5 * X[fl[1]][d];
+    measure = sqrt(t[0] * t[0] + t[1] * t[1]);
+    double n0 = -t[1], n1 = t[0];
+    double ln = sqrt(n0 * n0 + n1 * n1);
+    nrm[0] = n0 / ln;
+    nrm[1] = n1 / ln;
+  }
+  double ec[SD], fc[SD];
+#pragma unroll
+  for (int d = 0; d < SD; ++d) {
+    double s = 0.0;
+    for (int j = 0; j < NV; ++j) s = s + X[j][d];
+    ec[d] = s / (double)NV;
+    double f = 0.0;
+    for (int q = 0; q < FN; ++q) f = f + X[fl[q]][d];
+    fc[d] = f / (double)FN;
+  }
+  double dd = nrm[0] * (fc[0] - ec[0]);
+  for (int d = 1; d < SD; ++d) dd = dd + nrm[d] * (fc[d] - ec[d]);
+  if (dd < 0.0)
+    for (int d = 0; d < SD; ++d) nrm[d] = -nrm[d];
+}
+
 // Row (l, a) of the element matrix: out[j*DPN + b] for the element's 4 nodes.
 // PHYS 0: poisson_element_matrix with conductivity k; PHYS 1: elasticity.
 template <int CELL, int PHYS, int DPN>
@@ -442,6 +515,11 @@ struct RowArgs {
   double* val;
   int* flag;           // bit 0: bad element geometry, bit 1: pattern changed
   int maxc;            // accumulator slots per thread (max neighbours * DPN)
+  // apply_robin term (robin != 0): h on the boundary faces selected by
+  // (raxis, rsign), every boundary face when raxis < 0
+  const unsigned char* bface;
+  int robin, raxis;
+  double rsign, rh;
 };
 
 // One thread per global row.  Shared memory holds the row's dense accumulator
@@ -485,6 +563,44 @@ __global__ void __launch_bounds__(128) assemble_rows(RowArgs A) {
         acc[s] = acc[s] + v;
         nzf[s] |= (unsigned char)(v != 0.0);
       }
+  }
+  if (A.robin) {
+    // apply_robin_order (assembly:684-753): after every element contribution,
+    // h N_k N_l w |face| for each selected boundary face holding this node, in
+    // (element, face, quadrature point) order; every pair gets an entry.
+    constexpr int SD = CellTraits<CELL>::SD, FN = FaceTraits<CELL>::FN, NF = FaceTraits<CELL>::NF;
+    for (int k = A.ne_ptr[n]; k < k1; ++k) {
+      const int pe = A.ne[k];
+      const int e = pe >> 2, l = pe & 3;
+      const unsigned bm = A.bface[e];
+      if (!bm) continue;
+      double X[4][SD];
+      int nodes[4];
+      load_elem<CELL>(A.in, e, X, nodes);
+      const uchar4 sl = A.slot[k];
+      const int sj[4] = {sl.x, sl.y, sl.z, sl.w};
+      for (int fi = 0; fi < NF; ++fi) {
+        if (!(bm & (1u << fi))) continue;
+        int fl[3];
+        int kpos = -1;
+        for (int q = 0; q < FN; ++q) {
+          fl[q] = FaceTraits<CELL>::node(fi, q);
+          if (fl[q] == l) kpos = q;
+        }
+        if (kpos < 0) continue;
+        double measure, nrm[SD];
+        face_geometry<CELL, SD>(X, fl, measure, nrm);
+        const double h = (A.raxis < 0 || nrm[A.raxis] * A.rsign > 0.5) ? A.rh : 0.0;
+        for (int q = 0; q < c_face.nq; ++q) {
+          const double wmh = c_face.w[q] * measure * h * c_face.ns[q][kpos];
+          for (int lf = 0; lf < FN; ++lf) {
+            const int s = (sj[fl[lf]] * DPN + a) * T + tid;
+            acc[s] = acc[s] + wmh * c_face.ns[q][lf];
+            nzf[s] = 1;
+          }
+        }
+      }
+    }
   }
   if (!ok) atomicOr(A.flag, 1);
   if (MODE == MODE_COUNT) {
@@ -599,11 +715,7 @@ struct TractionArgs {
 template <int CELL>
 __global__ void traction_rows(TractionArgs A) {
   constexpr int SD = CellTraits<CELL>::SD;
-  constexpr int FN = (CELL == TPTFEM_CELL_TET4) ? 3 : 2;
-  constexpr int NV = CellTraits<CELL>::NV, NF = (CELL == TPTFEM_CELL_TRI3) ? 3 : 4;
-  const int tet_f[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
-  const int quad_f[4][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}};
-  const int tri_f[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+  constexpr int FN = FaceTraits<CELL>::FN, NF = FaceTraits<CELL>::NF;
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= A.n_nodes) return;
   double acc[3];
@@ -620,47 +732,12 @@ __global__ void traction_rows(TractionArgs A) {
       int fl[3];
       int kpos = -1;
       for (int q = 0; q < FN; ++q) {
-        fl[q] = (CELL == TPTFEM_CELL_TET4) ? tet_f[fi][q] : (CELL == TPTFEM_CELL_TRI3 ? tri_f[fi][q] : quad_f[fi][q]);
+        fl[q] = FaceTraits<CELL>::node(fi, q);
         if (fl[q] == l) kpos = q;
       }
       if (kpos < 0) continue;
-      // tangents from the face's reference gradients
       double measure, nrm[SD];
-      if constexpr (CELL == TPTFEM_CELL_TET4) {
-        double t0[3], t1[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          t0[d] = X[fl[1]][d] - X[fl[0]][d];
-          t1[d] = X[fl[2]][d] - X[fl[0]][d];
-        }
-        double c[3] = {t0[1] * t1[2] - t0[2] * t1[1], t0[2] * t1[0] - t0[0] * t1[2], t0[0] * t1[1] - t0[1] * t1[0]};
-        measure = sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
-        for (int d = 0; d < 3; ++d) nrm[d] = c[d] / measure;
-      } else {
-        double t[2];
-#pragma unroll
-        for (int d = 0; d < 2; ++d) t[d] = -0.5 * X[fl[0]][d] + 0.5 * X[fl[1]][d];
-        measure = sqrt(t[0] * t[0] + t[1] * t[1]);
-        double n0 = -t[1], n1 = t[0];
-        double ln = sqrt(n0 * n0 + n1 * n1);
-        nrm[0] = n0 / ln;
-        nrm[1] = n1 / ln;
-      }
-      // orient outward: face centroid minus element centroid (assembly:645-653)
-      double ec[SD], fc[SD], dd = 0.0;
-#pragma unroll
-      for (int d = 0; d < SD; ++d) {
-        double s = 0.0;
-        for (int j = 0; j < NV; ++j) s = s + X[j][d];
-        ec[d] = s / (double)NV;
-        double f = 0.0;
-        for (int q = 0; q < FN; ++q) f = f + X[fl[q]][d];
-        fc[d] = f / (double)FN;
-      }
-      dd = nrm[0] * (fc[0] - ec[0]);
-      for (int d = 1; d < SD; ++d) dd = dd + nrm[d] * (fc[d] - ec[d]);
-      if (dd < 0.0)
-        for (int d = 0; d < SD; ++d) nrm[d] = -nrm[d];
+      face_geometry<CELL, SD>(X, fl, measure, nrm);
       const bool sel = nrm[A.axis] * A.sign > 0.5;
       for (int q = 0; q < c_face.nq; ++q) {
         const double wm = c_face.w[q] * measure, N = c_face.ns[q][kpos];
@@ -689,6 +766,15 @@ ElemIn elem_in(const MeshData& m, const double* coef, int per_elem, int model, d
 void set_cell_tab(const MeshData& m, int quad_order, cudaStream_t s) {
   QuadTab t = make_cell_tab(m.cell, quad_order);
   TPT_CUDA(cudaMemcpyToSymbolAsync(c_cell, &t, sizeof(t), 0, cudaMemcpyHostToDevice, s));
+}
+
+// Boundary faces and the face quadrature (FACE_QUAD_ORDER 2) for a Robin term.
+void set_robin_faces(MeshData& m, int axis, cudaStream_t s) {
+  const int sd = m.cell == TPTFEM_CELL_TET4 ? 3 : 2;
+  TPT_REQUIRE(axis < sd, TPTFEM_ERR_INVALID_ARG, "robin axis out of range for the mesh dimension");
+  mesh_build_boundary_faces(m);
+  FaceTab f = make_face_tab(m.cell);
+  TPT_CUDA(cudaMemcpyToSymbolAsync(c_face, &f, sizeof(f), 0, cudaMemcpyHostToDevice, s));
 }
 
 int read_flag(tptfem_context* ctx) {
@@ -745,6 +831,11 @@ RowArgs row_args(MatrixData& M) {
   A.val = M.val.p;
   A.flag = M.ctx->d_flag;
   A.maxc = m.max_nb * M.dpn;
+  A.bface = M.robin ? m.bface.p : nullptr;
+  A.robin = M.robin;
+  A.raxis = M.robin_axis;
+  A.rsign = M.robin_sign;
+  A.rh = M.robin_h;
   return A;
 }
 
@@ -778,6 +869,7 @@ void assemble_matrix(MatrixData& M) {
   M.dpn = M.physics == 0 ? 1 : (m.cell == TPTFEM_CELL_TET4 ? 3 : 2);
   mesh_build_adjacency(m);
   set_cell_tab(m, M.quad_order, s);
+  if (M.robin) set_robin_faces(m, M.robin_axis, s);
   M.nrows = m.n_nodes * M.dpn;
   TPT_REQUIRE(M.nrows < (1LL << 31), TPTFEM_ERR_CREATION, "row count exceeds the int32 device index range");
   DevBuf<int> cnt;
@@ -810,6 +902,7 @@ bool reassemble_values(MatrixData& M) {
   tptfem_context* ctx = M.ctx;
   cudaStream_t s = ctx->stream;
   set_cell_tab(*M.mesh, M.quad_order, s);
+  if (M.robin) set_robin_faces(*M.mesh, M.robin_axis, s);
   TPT_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), s));
   RowArgs A = row_args(M);
   dispatch_rows(M, MODE_NUMERIC, A, s);

@@ -92,6 +92,11 @@ struct MatrixData {
   DevBuf<double> val;
   DevBuf<double> coef;  // n_elems or 1
   int per_element = 0;
+  // apply_robin term added after the element contributions (Poisson): h on the
+  // boundary faces whose outward normal n has sign * n[axis] > 0.5 (axis < 0:
+  // every boundary face)
+  int robin = 0, robin_axis = -1;
+  double robin_sign = 1.0, robin_h = 0.0;
 };
 
 struct SolverWork;  // solver.cu

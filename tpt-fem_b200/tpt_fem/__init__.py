@@ -224,12 +224,22 @@ def _coef(mesh, coef):
     return c, 1
 
 
-def assemble_poisson(mesh, conductivity, quad_order=2):
-    """assemble(mesh, 1, poisson_element_matrix) -> Matrix (thermal/src/lib.rs:132-160)."""
+def assemble_poisson(mesh, conductivity, quad_order=2, robin=None):
+    """assemble(mesh, 1, poisson_element_matrix) -> Matrix (thermal/src/lib.rs:132-160).
+
+    robin=(axis, sign, h) adds apply_robin (assembly/src/lib.rs:674-753) with
+    coefficient h on the boundary faces whose outward normal n has
+    sign * n[axis] > 0.5 (axis=-1: every boundary face), as solve_poisson's
+    `robin` argument does (thermal/src/lib.rs:235-237)."""
     ctx = mesh.ctx
     c, per = _coef(mesh, conductivity)
     h = C.c_void_p()
-    ctx.check(ctx.lib.tptfem_assemble_poisson(ctx.h, mesh.h, N.ptr(c), per, quad_order, C.byref(h)))
+    if robin is None:
+        ctx.check(ctx.lib.tptfem_assemble_poisson(ctx.h, mesh.h, N.ptr(c), per, quad_order, C.byref(h)))
+    else:
+        axis, sign, coef = robin
+        ctx.check(ctx.lib.tptfem_assemble_poisson_robin(ctx.h, mesh.h, N.ptr(c), per, quad_order, int(axis),
+                                                        float(sign), float(coef), C.byref(h)))
     return Matrix(h, mesh)
 
 
