@@ -150,6 +150,13 @@ tptfem_status tptfem_mesh_box(tptfem_context* ctx, const double min[3], const do
 tptfem_status tptfem_mesh_sizes(const tptfem_mesh* mesh, int64_t* n_nodes, int64_t* n_elems, int* cell_type,
                                 int* coord_dim);
 tptfem_status tptfem_mesh_download(tptfem_context* ctx, const tptfem_mesh* mesh, double* coords, int64_t* conn);
+/* write_vtk / write_vtk_with_data (crates/tpt-fem-io-vtk/src/lib.rs:117-196): the mesh
+ * as a legacy BINARY unstructured-grid .vtk file (version 4.1, big-endian, points padded
+ * to 3-D) with n_fields per-node scalar fields (names[f]; values[f]: n_nodes doubles in
+ * host memory), byte for byte the reference writer's layout.  title NULL -> "tpt-fem mesh",
+ * the reference's title. */
+tptfem_status tptfem_mesh_write_vtk(tptfem_context* ctx, const tptfem_mesh* mesh, const char* path, const char* title,
+                                    int n_fields, const char* const* names, const double* const* values);
 void tptfem_mesh_free(tptfem_mesh* mesh);
 
 /* ---- assembly ------------------------------------------------------------------

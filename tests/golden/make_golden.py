@@ -8,6 +8,9 @@ Fixtures:
                         ``mesh_gen_box_structured.vtk``, written by
                         crates/tpt-fem/examples/mesh_gen_box.rs:15-21 from
                         box_mesh([0,0,0],[1,1,1],[4,4,4]).
+  vtk_digests.json      byte length and SHA-256 of those two files, the
+                        golden bytes of the reference's VTK writer
+                        (crates/tpt-fem-io-vtk/src/lib.rs:117-196).
   box6_thermal_mesh.npz points and connectivity of ``thermal_solve.vtk``
                         (box_mesh([6,6,6]) per crates/tpt-fem/examples/
                         thermal_solve.rs).  Its temperature field is stale
@@ -49,12 +52,25 @@ def parse_legacy_vtk(path):
     return out
 
 
+def write_digests():
+    import hashlib
+    import json
+    out = {}
+    for name in ("mesh_gen_box_structured.vtk", "thermal_solve.vtk"):
+        data = open(os.path.join(REF, name), "rb").read()
+        out[name] = {"bytes": len(data), "sha256": hashlib.sha256(data).hexdigest()}
+    with open(os.path.join(OUT, "vtk_digests.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+        f.write("\n")
+
+
 def main():
     g = parse_legacy_vtk(os.path.join(REF, "mesh_gen_box_structured.vtk"))
     np.savez_compressed(os.path.join(OUT, "box4_structured.npz"), points=g["points"], conn=g["conn"])
     t = parse_legacy_vtk(os.path.join(REF, "thermal_solve.vtk"))
     np.savez_compressed(os.path.join(OUT, "box6_thermal_mesh.npz"), points=t["points"], conn=t["conn"],
                         stale_temperature=t["stale_temperature"])
+    write_digests()
     print("wrote", OUT)
 
 

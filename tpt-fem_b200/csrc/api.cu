@@ -271,6 +271,23 @@ tptfem_status tptfem_mesh_download(tptfem_context* ctx, const tptfem_mesh* mesh,
   API_CATCH(ctx)
 }
 
+tptfem_status tptfem_mesh_write_vtk(tptfem_context* ctx, const tptfem_mesh* mesh, const char* path, const char* title,
+                                    int n_fields, const char* const* names, const double* const* values) {
+  if (!ctx || !mesh || !mesh->d || !path || n_fields < 0 || (n_fields > 0 && (!names || !values)))
+    return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  std::vector<std::string> nm;
+  std::vector<const double*> va;
+  for (int f = 0; f < n_fields; ++f) {
+    TPT_REQUIRE(names[f] && values[f], TPTFEM_ERR_INVALID_ARG, "field name or values is NULL");
+    nm.emplace_back(names[f]);
+    va.push_back(values[f]);
+  }
+  write_file(path, vtk_legacy_binary(*mesh->d, title ? title : "tpt-fem mesh", nm, va));
+  API_CATCH(ctx)
+}
+
 void tptfem_mesh_free(tptfem_mesh* mesh) { delete mesh; }
 
 // ---- assembly -----------------------------------------------------------------

@@ -7,6 +7,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 
@@ -227,6 +228,10 @@ bool fsai_set_values(const SystemData& S, FsaiFactor& F, const double* d_sig2, c
 bool nb_build_operator(SystemData& S);  // false when the system has partial node groups
 bool nb_fill_factor(SystemData& S, const FsaiFactor& F);  // false: factor rows not node-block shaped
 bool nb_factor_shape_ok(SystemData& S, const FsaiFactor& F);  // factor rows = dpn * (lower neighbours) + a
+// io_vtk.cu: write_vtk_with_data's legacy binary bytes for a device-resident mesh
+std::string vtk_legacy_binary(const MeshData& m, const std::string& title, const std::vector<std::string>& names,
+                              const std::vector<const double*>& values);
+void write_file(const char* path, const std::string& bytes);
 void nb_build_sym(SystemData& S);  // after nb_build_operator succeeded
 void nb_refill_values(SystemData& S, bool sym);  // operator values again from the CSR (symmetric or full storage)
 void nb_refresh_values(SystemData& S);  // refill the node-block values from S.val

@@ -149,6 +149,20 @@ class Mesh:
     def coords(self, i):
         return [float(v) for v in self.coords_array[i]]
 
+    def write_vtk(self, path, fields=None, title=None):
+        """write_vtk / write_vtk_with_data (io-vtk/src/lib.rs:117-196): legacy binary
+        .vtk with per-node scalar fields {name: values}, in the given order."""
+        fields = dict(fields or {})
+        names = (C.c_char_p * max(1, len(fields)))(*[k.encode() for k in fields])
+        arrs = [N.f64(v) for v in fields.values()]
+        for a in arrs:
+            if a.shape != (self.n_nodes,):
+                raise ValueError("each field needs one value per node")
+        ptrs = (C.c_void_p * max(1, len(arrs)))(*[a.ctypes.data for a in arrs])
+        self.ctx.check(self.ctx.lib.tptfem_mesh_write_vtk(self.ctx.h, self.h, str(path).encode(),
+                                                          title.encode() if title else None, len(arrs),
+                                                          C.cast(names, C.c_void_p), C.cast(ptrs, C.c_void_p)))
+
     def nodes_on_plane(self, axis, coord, tol):
         """Mesh::nodes_on_plane (crates/tpt-fem-mesh/src/lib.rs:425-431)."""
         c = self.coords_array
