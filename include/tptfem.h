@@ -157,6 +157,10 @@ tptfem_status tptfem_mesh_download(tptfem_context* ctx, const tptfem_mesh* mesh,
  * the reference's title. */
 tptfem_status tptfem_mesh_write_vtk(tptfem_context* ctx, const tptfem_mesh* mesh, const char* path, const char* title,
                                     int n_fields, const char* const* names, const double* const* values);
+/* write_exodus (crates/tpt-fem-io-exodus/src/lib.rs:384-563): the mesh as an Exodus II
+ * file in NetCDF-3 classic (CDF-1) form, one element block, coordinates in single
+ * precision, with the reference writer's dimensions, variables and byte layout. */
+tptfem_status tptfem_mesh_write_exodus(tptfem_context* ctx, const tptfem_mesh* mesh, const char* path);
 void tptfem_mesh_free(tptfem_mesh* mesh);
 
 /* ---- assembly ------------------------------------------------------------------

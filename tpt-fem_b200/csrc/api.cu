@@ -288,6 +288,14 @@ tptfem_status tptfem_mesh_write_vtk(tptfem_context* ctx, const tptfem_mesh* mesh
   API_CATCH(ctx)
 }
 
+tptfem_status tptfem_mesh_write_exodus(tptfem_context* ctx, const tptfem_mesh* mesh, const char* path) {
+  if (!ctx || !mesh || !mesh->d || !path) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  write_file(path, exodus_bytes(*mesh->d));
+  API_CATCH(ctx)
+}
+
 void tptfem_mesh_free(tptfem_mesh* mesh) { delete mesh; }
 
 // ---- assembly -----------------------------------------------------------------

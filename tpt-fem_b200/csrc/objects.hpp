@@ -232,6 +232,8 @@ bool nb_factor_shape_ok(SystemData& S, const FsaiFactor& F);  // factor rows = d
 std::string vtk_legacy_binary(const MeshData& m, const std::string& title, const std::vector<std::string>& names,
                               const std::vector<const double*>& values);
 void write_file(const char* path, const std::string& bytes);
+// io_exodus.cu: write_exodus's NetCDF-3 classic bytes for a device-resident mesh
+std::string exodus_bytes(const MeshData& m);
 void nb_build_sym(SystemData& S);  // after nb_build_operator succeeded
 void nb_refill_values(SystemData& S, bool sym);  // operator values again from the CSR (symmetric or full storage)
 void nb_refresh_values(SystemData& S);  // refill the node-block values from S.val

@@ -163,6 +163,10 @@ class Mesh:
                                                           title.encode() if title else None, len(arrs),
                                                           C.cast(names, C.c_void_p), C.cast(ptrs, C.c_void_p)))
 
+    def write_exodus(self, path):
+        """write_exodus (io-exodus/src/lib.rs:384-563): NetCDF-3 classic Exodus II file."""
+        self.ctx.check(self.ctx.lib.tptfem_mesh_write_exodus(self.ctx.h, self.h, str(path).encode()))
+
     def nodes_on_plane(self, axis, coord, tol):
         """Mesh::nodes_on_plane (crates/tpt-fem-mesh/src/lib.rs:425-431)."""
         c = self.coords_array
