@@ -218,6 +218,20 @@ tptfem_status tptfem_load_body(tptfem_context* ctx, tptfem_mesh* mesh, const dou
 tptfem_status tptfem_apply_traction(tptfem_context* ctx, tptfem_mesh* mesh, int dofs_per_node, int axis,
                                     double sign, const double* traction, double* rhs);
 
+/* ---- eigenvalues (crates/tpt-fem-eigen/src/lib.rs) ---------------------------------- */
+enum { TPTFEM_EIG_SMALLEST = 0, TPTFEM_EIG_LARGEST = 1 };  /* EigWhich (eigen:122-129) */
+/* lanczos_eigs (eigen:223-262): Lanczos from e_0 with full re-orthogonalisation and
+ * lanczos_dim vectors on the device matrix, Ritz pairs of the tridiagonal from the cyclic
+ * Jacobi method.  Writes *found = min(num, basis size) eigenvalues (ascending for
+ * SMALLEST, descending for LARGEST) and, when vectors != NULL, the unit Ritz vectors
+ * (found x nrows, row-major). */
+tptfem_status tptfem_lanczos_eigs(tptfem_context* ctx, const tptfem_matrix* mat, int num, int which,
+                                  int lanczos_dim, double* values, double* vectors, int* found);
+/* power_iteration (eigen:62-88): dominant eigenpair from x_i = i + 1, stopping when the
+ * Rayleigh quotient changes by less than tol * max(|lambda|, 1).  x (nrows) may be NULL. */
+tptfem_status tptfem_power_iteration(tptfem_context* ctx, const tptfem_matrix* mat, int max_iter, double tol,
+                                     double* lambda, double* x, int* iterations);
+
 /* ---- Dirichlet reduction and solve ----------------------------------------------- */
 /* reduce_system (crates/tpt-fem-assembly/src/lib.rs:504-535) into a device-resident system. */
 tptfem_status tptfem_reduce_system(tptfem_context* ctx, const tptfem_matrix* mat, const double* rhs, int64_t n,

@@ -296,6 +296,27 @@ tptfem_status tptfem_mesh_write_exodus(tptfem_context* ctx, const tptfem_mesh* m
   API_CATCH(ctx)
 }
 
+tptfem_status tptfem_lanczos_eigs(tptfem_context* ctx, const tptfem_matrix* mat, int num, int which,
+                                  int lanczos_dim, double* values, double* vectors, int* found) {
+  if (!ctx || !mat || !mat->d || (num > 0 && !values) || !found) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  TPT_REQUIRE(which == TPTFEM_EIG_SMALLEST || which == TPTFEM_EIG_LARGEST, TPTFEM_ERR_INVALID_ARG,
+              "which must be TPTFEM_EIG_SMALLEST or TPTFEM_EIG_LARGEST");
+  *found = lanczos_eigs(ctx, *mat->d, num, which == TPTFEM_EIG_LARGEST, lanczos_dim, values, vectors);
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_power_iteration(tptfem_context* ctx, const tptfem_matrix* mat, int max_iter, double tol,
+                                     double* lambda, double* x, int* iterations) {
+  if (!ctx || !mat || !mat->d || !lambda || max_iter < 0) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  const int it = power_iteration(ctx, *mat->d, max_iter, tol, lambda, x);
+  if (iterations) *iterations = it;
+  API_CATCH(ctx)
+}
+
 void tptfem_mesh_free(tptfem_mesh* mesh) { delete mesh; }
 
 // ---- assembly -----------------------------------------------------------------

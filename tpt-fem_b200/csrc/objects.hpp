@@ -232,6 +232,10 @@ bool nb_factor_shape_ok(SystemData& S, const FsaiFactor& F);  // factor rows = d
 std::string vtk_legacy_binary(const MeshData& m, const std::string& title, const std::vector<std::string>& names,
                               const std::vector<const double*>& values);
 void write_file(const char* path, const std::string& bytes);
+// eigen.cu: lanczos_eigs / power_iteration on a device matrix (returns pairs found / iterations)
+int lanczos_eigs(tptfem_context* ctx, const MatrixData& M, int num, int largest, int dim, double* values,
+                 double* vectors);
+int power_iteration(tptfem_context* ctx, const MatrixData& M, int max_iter, double tol, double* lambda, double* x_out);
 // io_exodus.cu: write_exodus's NetCDF-3 classic bytes for a device-resident mesh
 std::string exodus_bytes(const MeshData& m);
 void nb_build_sym(SystemData& S);  // after nb_build_operator succeeded

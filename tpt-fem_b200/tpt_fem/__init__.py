@@ -220,6 +220,25 @@ class Matrix:
         self.ctx.check(self.ctx.lib.tptfem_csr_matvec(self.ctx.h, self.h, N.ptr(x), len(x), N.ptr(y)))
         return y
 
+    def lanczos_eigs(self, num, which="smallest", lanczos_dim=None, vectors=True):
+        """lanczos_eigs (eigen/src/lib.rs:223-262) on the device -> [(value, unit vector or None)]."""
+        dim = lanczos_dim or self.nrows
+        vals = np.zeros(max(num, 1))
+        vecs = np.zeros((max(num, 1), self.nrows)) if vectors else None
+        found = C.c_int()
+        w = 1 if which == "largest" else 0
+        self.ctx.check(self.ctx.lib.tptfem_lanczos_eigs(self.ctx.h, self.h, num, w, dim, N.ptr(vals),
+                                                        N.ptr(vecs) if vectors else None, C.byref(found)))
+        return [(float(vals[i]), vecs[i].copy() if vectors else None) for i in range(found.value)]
+
+    def power_iteration(self, max_iter=200, tol=1e-12):
+        """power_iteration (eigen/src/lib.rs:62-88) on the device -> (lambda, x, iterations)."""
+        lam, it = C.c_double(), C.c_int()
+        x = np.zeros(self.nrows)
+        self.ctx.check(self.ctx.lib.tptfem_power_iteration(self.ctx.h, self.h, max_iter, tol, C.byref(lam),
+                                                           N.ptr(x), C.byref(it)))
+        return lam.value, x, it.value
+
     def reassemble(self, coef):
         """New per-element (or constant) coefficients on the same mesh; pattern revalidated."""
         coef = np.atleast_1d(N.f64(coef))

@@ -90,6 +90,8 @@ SIGNATURES = {
     "tptfem_assemble_poisson": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _pp]),
     "tptfem_mesh_write_vtk": (C.c_int, [_vp, _vp, C.c_char_p, C.c_char_p, C.c_int, _vp, _vp]),
     "tptfem_mesh_write_exodus": (C.c_int, [_vp, _vp, C.c_char_p]),
+    "tptfem_lanczos_eigs": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp]),
+    "tptfem_power_iteration": (C.c_int, [_vp, _vp, C.c_int, C.c_double, _vp, _vp, _vp]),
     "tptfem_assemble_poisson_robin": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                                 _pp]),
     "tptfem_assemble_elasticity": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_int, C.c_double, C.c_int, _pp]),
