@@ -499,7 +499,11 @@ __device__ __forceinline__ bool element_row(const double (&X)[4][CellTraits<CELL
   return ok;
 }
 
-enum { MODE_COUNT = 0, MODE_FILL = 1, MODE_NUMERIC = 2 };
+// COUNT: non-zeros per row; FILL: columns and values at row_ptr; NUMERIC: values
+// into an existing pattern (checked); PADDED: columns and values of row r at
+// r * maxc in a scratch array plus the count, compacted afterwards (one pass of
+// element work instead of COUNT + FILL).
+enum { MODE_COUNT = 0, MODE_FILL = 1, MODE_NUMERIC = 2, MODE_PADDED = 3 };
 
 struct RowArgs {
   ElemIn in;
@@ -606,6 +610,17 @@ __global__ void __launch_bounds__(128) assemble_rows(RowArgs A) {
   if (MODE == MODE_COUNT) {
     int c = 0;
     for (int s = 0; s < ncand; ++s) c += nzf[s * T + tid];
+    A.row_cnt[r] = c;
+  } else if (MODE == MODE_PADDED) {
+    int c = 0;
+    int* pc = A.col + r * A.maxc;
+    double* pv = A.val + r * A.maxc;
+    for (int s = 0; s < ncand; ++s) {
+      if (!nzf[s * T + tid]) continue;
+      pc[c] = A.nb[nb0 + s / DPN] * DPN + s % DPN;
+      pv[c] = acc[s * T + tid];
+      ++c;
+    }
     A.row_cnt[r] = c;
   } else {
     int o = A.row_ptr[r];
@@ -798,6 +813,7 @@ void launch_rows(int mode, const RowArgs& A, cudaStream_t s) {
   };
   if (mode == MODE_COUNT) run(assemble_rows<CELL, PHYS, DPN, MODE_COUNT>);
   else if (mode == MODE_FILL) run(assemble_rows<CELL, PHYS, DPN, MODE_FILL>);
+  else if (mode == MODE_PADDED) run(assemble_rows<CELL, PHYS, DPN, MODE_PADDED>);
   else run(assemble_rows<CELL, PHYS, DPN, MODE_NUMERIC>);
 }
 
@@ -851,6 +867,22 @@ __global__ void ref_dims(const int* __restrict__ rp, const int* __restrict__ col
   }
 }
 
+// Padded rows -> CSR: one warp per row, lanes over its entries.
+__global__ void compact_rows(int64_t nrows, int maxc, const int* __restrict__ pcol, const double* __restrict__ pval,
+                             const int* __restrict__ row_ptr, int* __restrict__ col, double* __restrict__ val) {
+  const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= nrows) return;
+  const int o = row_ptr[r], c = row_ptr[r + 1] - o;
+  for (int i = lane; i < c; i += 32) {
+    col[o + i] = pcol[r * maxc + i];
+    val[o + i] = pval[r * maxc + i];
+  }
+}
+
+// Scratch budget of the one-pass (padded) assembly; larger meshes count first.
+constexpr int64_t PADDED_ASSEMBLY_BYTES = 12LL << 30;
+
 }  // namespace
 
 void assemble_matrix(MatrixData& M) {
@@ -877,15 +909,35 @@ void assemble_matrix(MatrixData& M) {
   TPT_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), s));
   RowArgs A = row_args(M);
   A.row_cnt = cnt.p;
-  dispatch_rows(M, MODE_COUNT, A, s);
-  TPT_REQUIRE((read_flag(ctx) & 1) == 0, TPTFEM_ERR_NUMERIC,
-              "degenerate element: zero or non-finite Jacobian determinant");
-  M.row_ptr.alloc(M.nrows + 1, s);
-  M.nnz = exclusive_scan_i32(cnt.p, M.row_ptr.p, M.nrows, s);
-  M.col.alloc(M.nnz, s);
-  M.val.alloc(M.nnz, s);
-  A = row_args(M);
-  dispatch_rows(M, MODE_FILL, A, s);
+  const int64_t padded = M.nrows * (int64_t)A.maxc;
+  if (padded * 12 <= PADDED_ASSEMBLY_BYTES) {  // one element pass into padded rows, then compaction
+    DevBuf<int> pcol;
+    DevBuf<double> pval;
+    pcol.alloc(std::max<int64_t>(padded, 1), s);
+    pval.alloc(std::max<int64_t>(padded, 1), s);
+    A.col = pcol.p;
+    A.val = pval.p;
+    dispatch_rows(M, MODE_PADDED, A, s);
+    TPT_REQUIRE((read_flag(ctx) & 1) == 0, TPTFEM_ERR_NUMERIC,
+                "degenerate element: zero or non-finite Jacobian determinant");
+    M.row_ptr.alloc(M.nrows + 1, s);
+    M.nnz = exclusive_scan_i32(cnt.p, M.row_ptr.p, M.nrows, s);
+    M.col.alloc(M.nnz, s);
+    M.val.alloc(M.nnz, s);
+    compact_rows<<<ceil_div(M.nrows * 32, 256), 256, 0, s>>>(M.nrows, A.maxc, pcol.p, pval.p, M.row_ptr.p, M.col.p,
+                                                             M.val.p);
+    TPT_CHECK_LAUNCH();
+  } else {
+    dispatch_rows(M, MODE_COUNT, A, s);
+    TPT_REQUIRE((read_flag(ctx) & 1) == 0, TPTFEM_ERR_NUMERIC,
+                "degenerate element: zero or non-finite Jacobian determinant");
+    M.row_ptr.alloc(M.nrows + 1, s);
+    M.nnz = exclusive_scan_i32(cnt.p, M.row_ptr.p, M.nrows, s);
+    M.col.alloc(M.nnz, s);
+    M.val.alloc(M.nnz, s);
+    A = row_args(M);
+    dispatch_rows(M, MODE_FILL, A, s);
+  }
   DevBuf<int> dims;
   dims.alloc(2, s);
   TPT_CUDA(cudaMemsetAsync(dims.p, 0, 2 * sizeof(int), s));

@@ -216,30 +216,15 @@ __global__ void fill_factor(int ngroups, int dpn, const int* __restrict__ lrp, c
 // Symmetric half storage of K: the strictly-lower blocks in the L slot
 // structure, the diagonal blocks per chunk, and for each L^T slot (g, J > g)
 // the index of block (J, g) in the lower storage (its transpose is K_gJ).
-__global__ void fill_ksym(int ngroups, int dpn, const int* __restrict__ rp, const int* __restrict__ ci,
-                          const double* __restrict__ va, const int* __restrict__ lcptr, const int* __restrict__ lcol,
-                          const int* __restrict__ nlow, const int* __restrict__ ucptr, const int* __restrict__ upos,
-                          const int* __restrict__ ucol, double* __restrict__ lval, double* __restrict__ dval,
-                          int* __restrict__ ubase) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ngroups) return;
-  const int c = g >> 5, lane = g & 31;
-  const int d2 = dpn * dpn;
-  const int nl = nlow[g];
-  for (int k = 0; k < lcptr[c + 1] - lcptr[c]; ++k) {
-    const int64_t s = (int64_t)lcptr[c] + k;
-    const int J = lcol[s * 32 + lane];
-    for (int a = 0; a < dpn; ++a)
-      for (int b = 0; b < dpn; ++b)
-        lval[(s * d2 + a * dpn + b) * 32 + lane] = k < nl ? csr_at(rp, ci, va, g * dpn + a, J * dpn + b) : 0.0;
-  }
-  for (int a = 0; a < dpn; ++a)
-    for (int b = 0; b < dpn; ++b)
-      dval[((int64_t)c * d2 + a * dpn + b) * 32 + lane] = csr_at(rp, ci, va, g * dpn + a, g * dpn + b);
-  for (int k = 0; k < ucptr[c + 1] - ucptr[c]; ++k) {
-    const int64_t idx = ((int64_t)ucptr[c] + k) * 32 + lane;
+// One block of 32 threads per chunk; lanes past the last group are skipped.
+__global__ void upper_bases(int ngroups, int dpn, const int* __restrict__ lcptr, const int* __restrict__ ucptr,
+                            const int* __restrict__ ucol, const int* __restrict__ upos, int* __restrict__ ubase) {
+  const int c = blockIdx.x, lane = threadIdx.x;
+  if (c * 32 + lane >= ngroups) return;
+  for (int64_t s = ucptr[c]; s < ucptr[c + 1]; ++s) {
+    const int64_t idx = s * 32 + lane;
     const int J = ucol[idx], p = upos[idx];
-    ubase[idx] = p < 0 ? -1 : (int)(((int64_t)lcptr[J >> 5] + p) * d2 * 32 + (J & 31));
+    ubase[idx] = p < 0 ? -1 : (int)(((int64_t)lcptr[J >> 5] + p) * dpn * dpn * 32 + (J & 31));
   }
 }
 
@@ -293,9 +278,10 @@ void nb_build_sym(SystemData& S) {
   N.ks_diag.alloc((int64_t)N.nchunks * 32 * d2, s);
   N.ku_base.alloc(std::max<int64_t>(N.u_slots, 1) * 32, s);
   N.ks_diag.zero();
-  fill_ksym<<<ceil_div(N.ngroups, 128), 128, 0, s>>>(N.ngroups, N.dpn, S.row_ptr.p, S.col.p, S.val.p, N.l_cptr.p,
-                                                     N.l_col.p, N.nlow.p, N.u_cptr.p, N.u_pos.p, N.u_col.p,
-                                                     N.ks_lval.p, N.ks_diag.p, N.ku_base.p);
+  upper_bases<<<N.nchunks, 32, 0, s>>>(N.ngroups, N.dpn, N.l_cptr.p, N.u_cptr.p, N.u_col.p, N.u_pos.p, N.ku_base.p);
+  TPT_CHECK_LAUNCH();
+  refill_ksym<<<N.nchunks, 32 * N.dpn, 0, s>>>(N.ngroups, N.dpn, S.row_ptr.p, S.col.p, S.val.p, N.l_cptr.p,
+                                               N.l_col.p, N.nlow.p, N.ks_lval.p, N.ks_diag.p);
   TPT_CHECK_LAUNCH();
   N.sym_built = true;
   N.fresh_fill = true;
@@ -309,6 +295,10 @@ void nb_refill_values(SystemData& S, bool sym) {
     refill_ksym<<<N.nchunks, 32 * N.dpn, 0, s>>>(N.ngroups, N.dpn, S.row_ptr.p, S.col.p, S.val.p, N.l_cptr.p,
                                                  N.l_col.p, N.nlow.p, N.ks_lval.p, N.ks_diag.p);
   } else {
+    if (!N.k_val.p) {
+      N.k_col.alloc(std::max<int64_t>(N.k_slots, 1) * 32, s);
+      N.k_val.alloc(std::max<int64_t>(N.k_slots, 1) * 32 * N.dpn * N.dpn, s);
+    }
     fill_k<<<ceil_div(N.ngroups, 128), 128, 0, s>>>(N.ngroups, N.dpn, S.row_ptr.p, S.col.p, S.val.p, N.gptr.p,
                                                     N.glist.p, N.k_cptr.p, N.k_col.p, N.k_val.p);
     N.full_stale = false;
@@ -320,12 +310,8 @@ void nb_refill_values(SystemData& S, bool sym) {
 void nb_refresh_values(SystemData& S) {
   NbSell& N = S.nb;
   if (N.state != 1) return;
-  if (N.sym_built) {  // the full storage is refilled when a solve asks for it
-    nb_refill_values(S, true);
-    N.full_stale = true;
-  } else {
-    nb_refill_values(S, false);
-  }
+  if (N.sym_built) nb_refill_values(S, true);
+  N.full_stale = true;  // the full storage is refilled when a solve asks for it
 }
 
 bool nb_build_operator(SystemData& S) {
@@ -365,12 +351,7 @@ bool nb_build_operator(SystemData& S) {
   TPT_CHECK_LAUNCH();
   N.k_cptr.alloc(N.nchunks + 1, s);
   N.k_slots = exclusive_scan_i32(slots.p, N.k_cptr.p, N.nchunks, s);
-  N.k_col.alloc(N.k_slots * 32, s);
-  N.k_val.alloc(N.k_slots * 32 * dpn * dpn, s);
-  fill_k<<<ceil_div(ng, 128), 128, 0, s>>>(ng, dpn, S.row_ptr.p, S.col.p, S.val.p, N.gptr.p, N.glist.p,
-                                           N.k_cptr.p, N.k_col.p, N.k_val.p);
-  TPT_CHECK_LAUNCH();
-  N.fresh_fill = true;
+  N.full_stale = true;  // the full storage (1.7x the symmetric one) is filled when a solve asks for it
   // slot structure of L (lower) and L^T (upper)
   chunk_slots<<<cgrid, 256, 0, s>>>(ng, N.gptr.p, N.glist.p, 1, slots.p);
   TPT_CHECK_LAUNCH();

@@ -57,29 +57,45 @@ __global__ void reduced_counts(const int* __restrict__ rp, const int* __restrict
   cnt[i] = c;
 }
 
+// One warp per free row: lanes take 32 consecutive entries at a time; kept
+// (free-column) entries are placed by a ballot prefix count, and the lifting
+// terms of fixed columns are subtracted one by one in column order, as the
+// reference's loop does.
 __global__ void reduced_fill(const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ va,
                              const int* __restrict__ first, const int* __restrict__ red,
                              const int* __restrict__ free_map, const double* __restrict__ bc_val,
                              const double* __restrict__ rhs, int64_t n_free, const int* __restrict__ rrp,
                              int* __restrict__ rci, double* __restrict__ rva, double* __restrict__ fred) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_free) return;
-  int f = free_map[i];
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= n_free) return;  // whole warps leave together
+  const int f = free_map[i];
   double r = rhs[f];
   int o = rrp[i];
-  for (int k = rp[f]; k < rp[f + 1]; ++k) {
-    int col = ci[k];
-    double v = va[k];
-    int fb = first[col];
-    if (fb != INT_MAX) {
-      r = __dsub_rn(r, __dmul_rn(v, bc_val[fb]));
-    } else {
-      rci[o] = red[col];
-      rva[o] = v;
-      ++o;
+  const int k1 = rp[f + 1];
+  for (int k0 = rp[f]; k0 < k1; k0 += 32) {
+    const int k = k0 + lane;
+    const bool in = k < k1;
+    const int col = in ? ci[k] : 0;
+    const double v = in ? va[k] : 0.0;
+    const int fb = in ? first[col] : INT_MAX;
+    const bool fixed = in && fb != INT_MAX, kept = in && fb == INT_MAX;
+    const unsigned km = __ballot_sync(0xffffffffu, kept);
+    if (kept) {
+      const int pos = o + __popc(km & ((1u << lane) - 1u));
+      rci[pos] = red[col];
+      rva[pos] = v;
+    }
+    o += __popc(km);
+    unsigned fm = __ballot_sync(0xffffffffu, fixed);
+    const double prod = fixed ? __dmul_rn(v, bc_val[fb]) : 0.0;
+    while (fm) {
+      const int src = __ffs(fm) - 1;
+      r = __dsub_rn(r, __shfl_sync(0xffffffffu, prod, src));
+      fm &= fm - 1;
     }
   }
-  fred[i] = r;
+  if (lane == 0) fred[i] = r;
 }
 
 // Values of an existing reduced system from a matrix with the same pattern:
@@ -185,7 +201,7 @@ std::unique_ptr<SystemData> reduce_system(tptfem_context* ctx, const MatrixData&
   S->val.alloc(S->nnz, s);
   S->fred.alloc(S->n_free, s);
   if (S->n_free) {
-    reduced_fill<<<ceil_div(S->n_free, 256), 256, 0, s>>>(A.row_ptr.p, A.col.p, A.val.p, first.p, red.p,
+    reduced_fill<<<ceil_div(S->n_free * 32, 256), 256, 0, s>>>(A.row_ptr.p, A.col.p, A.val.p, first.p, red.p,
                                                           S->free_map.p, val.p, d_rhs, S->n_free, S->row_ptr.p,
                                                           S->col.p, S->val.p, S->fred.p);
     TPT_CHECK_LAUNCH();

@@ -826,6 +826,7 @@ void system_values_changed(SystemData& S) {
 }
 
 void nb_operator_apply(SystemData& S, const double* x, double* y) {
+  if (!S.nb.sym_built && S.nb.full_stale) nb_refill_values(S, false);
   const NbSell& N = S.nb;
   cudaStream_t s = S.ctx->stream;
   const int g = std::max(1, std::min(sm_count() * NB_BLOCKS_PER_SM, ceil_div((int64_t)N.nchunks * 32, SPMV_THREADS)));
