@@ -30,18 +30,6 @@ __global__ void matvec_exact(int64_t nrows, const int* __restrict__ rp, const in
 }
 
 // conn64 -> conn32 with 0 <= c < n_nodes (bit 0 of *flag otherwise); finite coords (bit 1).
-__global__ void mesh_check_convert(int64_t nc, const int64_t* __restrict__ c64, int64_t n_nodes,
-                                   int* __restrict__ c32, int64_t nx, const double* __restrict__ x,
-                                   int* __restrict__ flag) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nc) {
-    const int64_t c = c64[i];
-    if (c < 0 || c >= n_nodes) atomicOr(flag, 1);
-    c32[i] = (c >= 0 && c < n_nodes) ? (int)c : 0;
-  }
-  if (i < nx && !isfinite(x[i])) atomicOr(flag, 2);
-}
-
 tptfem_status fail(tptfem_context* ctx, tptfem_status st, const std::string& msg) {
   if (ctx) ctx->err = msg;
   return st;
@@ -91,7 +79,7 @@ std::unique_ptr<MatrixData> new_matrix(tptfem_context* ctx, tptfem_mesh* mesh, i
   if (m.cell == TPTFEM_CELL_QUAD4)  // Tet4 and Tri3 use one fixed rule and ignore quad_order
     TPT_REQUIRE(quad_order >= 1 && quad_order <= 5, TPTFEM_ERR_INVALID_ARG, "quad_order must be in 1..=5");
   const int64_t count = per_element ? m.n_elems : 1;
-  check_coef(coef, count, physics ? "young" : "conductivity");
+  TPT_REQUIRE(coef != nullptr, TPTFEM_ERR_INVALID_ARG, std::string(physics ? "young" : "conductivity") + " is NULL");
   TPT_REQUIRE(std::isfinite(nu), TPTFEM_ERR_INVALID_ARG, "poisson ratio is not finite");
   auto M = std::make_unique<MatrixData>();
   M->ctx = ctx;
@@ -102,7 +90,8 @@ std::unique_ptr<MatrixData> new_matrix(tptfem_context* ctx, tptfem_mesh* mesh, i
   M->quad_order = quad_order;
   M->per_element = per_element ? 1 : 0;
   M->coef.alloc(count, ctx->stream);
-  M->coef.upload(coef, count);
+  TPT_REQUIRE(host_to_device_finite(ctx, M->coef.p, coef, (size_t)count), TPTFEM_ERR_INVALID_ARG,
+              std::string(physics ? "young" : "conductivity") + " holds a non-finite value");
   M->robin = robin.on;
   M->robin_axis = robin.axis;
   M->robin_sign = robin.sign;
@@ -159,6 +148,7 @@ void tptfem_destroy(tptfem_context* ctx) {
     if (e) cudaEventDestroy(e);
   if (ctx->d_flag) cudaFree(ctx->d_flag);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+  if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
   if (ctx->cusolver) cusolverDnDestroy((cusolverDnHandle_t)ctx->cusolver);
   if (ctx->cublas) cublasDestroy((cublasHandle_t)ctx->cublas);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -210,23 +200,13 @@ tptfem_status tptfem_mesh_upload(tptfem_context* ctx, int cell_type, int coord_d
   m->n_nodes = n_nodes;
   m->n_elems = n_elems;
   m->coords.alloc(n_nodes * coord_dim, ctx->stream);
-  m->coords.upload(coords, n_nodes * coord_dim);
   m->conn.alloc(n_elems * npe, ctx->stream);
-  {  // int64 connectivity -> int32 on the device, with the range and finiteness checks
-    DevBuf<int64_t> c64;
-    c64.alloc(n_elems * npe, ctx->stream);
-    c64.upload(conn, n_elems * npe);
-    TPT_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
-    const int64_t nv = std::max<int64_t>(n_elems * npe, n_nodes * coord_dim);
-    mesh_check_convert<<<ceil_div(nv, 256), 256, 0, ctx->stream>>>(n_elems * npe, c64.p, n_nodes, m->conn.p,
-                                                                   n_nodes * coord_dim, m->coords.p, ctx->d_flag);
-    TPT_CHECK_LAUNCH();
-    int flag = 0;
-    TPT_CUDA(cudaMemcpyAsync(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    TPT_CUDA(cudaStreamSynchronize(ctx->stream));
-    TPT_REQUIRE(!(flag & 2), TPTFEM_ERR_INVALID_ARG, "coords hold a non-finite value");
-    TPT_REQUIRE(!(flag & 1), TPTFEM_ERR_INVALID_ARG, "connectivity entry out of range");
-  }
+  // int64 connectivity narrowed to int32 and range-checked, coordinates checked
+  // for finiteness, both on the host threads that stage the copies
+  TPT_REQUIRE(host_to_device_finite(ctx, m->coords.p, coords, (size_t)(n_nodes * coord_dim)),
+              TPTFEM_ERR_INVALID_ARG, "coords hold a non-finite value");
+  TPT_REQUIRE(host_to_device_ids(ctx, m->conn.p, conn, (size_t)(n_elems * npe), n_nodes), TPTFEM_ERR_INVALID_ARG,
+              "connectivity entry out of range");
   *out = new tptfem_mesh{m};
   API_CATCH(ctx)
 }
@@ -370,9 +350,10 @@ tptfem_status tptfem_reassemble(tptfem_context* ctx, tptfem_matrix* mat, const d
   set_device(ctx);
   MatrixData& M = *mat->d;
   const int64_t count = per_element ? M.mesh->n_elems : 1;
-  check_coef(coef, count, "coefficient");
+  TPT_REQUIRE(coef != nullptr, TPTFEM_ERR_INVALID_ARG, "coefficient is NULL");
   if (M.coef.n != (size_t)count) M.coef.alloc(count, ctx->stream);
-  M.coef.upload(coef, count);
+  TPT_REQUIRE(host_to_device_finite(ctx, M.coef.p, coef, (size_t)count), TPTFEM_ERR_INVALID_ARG,
+              "coefficient holds a non-finite value");
   M.per_element = per_element ? 1 : 0;
   if (!reassemble_values(M)) assemble_matrix(M);  // pattern changed: rebuild it
   API_CATCH(ctx)
@@ -476,10 +457,9 @@ tptfem_status tptfem_apply_traction(tptfem_context* ctx, tptfem_mesh* mesh, int 
   const int64_t n = m.n_nodes * dofs_per_node;
   DevBuf<double> d;
   d.alloc(n, ctx->stream);
-  d.upload(rhs, n);
+  host_to_device(ctx, d.p, rhs, n * sizeof(double));
   apply_traction(m, dofs_per_node, axis, sign, traction, d.p);
-  d.download(rhs, n);
-  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  device_to_host(ctx, rhs, d.p, n * sizeof(double));
   API_CATCH(ctx)
 }
 
@@ -495,7 +475,7 @@ tptfem_status tptfem_reduce_system(tptfem_context* ctx, const tptfem_matrix* mat
   TPT_REQUIRE(n == M.nrows, TPTFEM_ERR_INVALID_ARG, "rhs length does not match the matrix dimension");
   DevBuf<double> d;
   d.alloc(n, ctx->stream);
-  d.upload(rhs, n);
+  host_to_device(ctx, d.p, rhs, n * sizeof(double));
   auto S = reduce_system(ctx, M, d.p, bc_dof, bc_val, nbc);
   *out = new tptfem_system{std::move(S)};
   API_CATCH(ctx)
@@ -510,7 +490,7 @@ tptfem_status tptfem_system_refresh(tptfem_context* ctx, tptfem_system* sys, con
   TPT_REQUIRE(n == S.n, TPTFEM_ERR_INVALID_ARG, "rhs length does not match the system");
   DevBuf<double> d;
   d.alloc(n, ctx->stream);
-  d.upload(rhs, n);
+  host_to_device(ctx, d.p, rhs, n * sizeof(double));
   const bool ok = system_refresh(S, *mat->d, d.p);
   system_values_changed(S);  // values were (partly) overwritten either way
   TPT_REQUIRE(ok, TPTFEM_ERR_INVALID_ARG,
@@ -572,8 +552,7 @@ tptfem_status tptfem_system_solution(tptfem_context* ctx, const tptfem_system* s
   DevBuf<double> d;
   d.alloc(S.n, ctx->stream);
   system_solution(S, d.p);
-  d.download(u, S.n);
-  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  device_to_host(ctx, u, d.p, S.n * sizeof(double));
   API_CATCH(ctx)
 }
 

@@ -203,8 +203,15 @@ __global__ void factor_to_lowp(int n, int64_t nnz, const double* __restrict__ si
     const double v = lva[k];
     if (!isfinite(v) || fabs(v) > 6.0e4) atomicOr(flag, 4);  // outside FP16 range
     va16[k] = __double2half(v);
-    tva16[k] = __double2half(lva[perm[k]]);
+    if (perm) tva16[k] = __double2half(lva[perm[k]]);
   }
+}
+
+// Values of the explicit transpose from the FP16 factor: tva[k] = va[perm[k]].
+__global__ void transpose_values(int64_t nnz, const int* __restrict__ perm, const __half* __restrict__ va,
+                                 __half* __restrict__ tva) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nnz) tva[k] = va[perm[k]];
 }
 
 }  // namespace
@@ -230,7 +237,17 @@ void fsai_build_pattern(const SystemData& S, FsaiFactor& F) {
   nb_lower_pattern<true><<<ceil_div(n, 128), 128, 0, s>>>(n, S.dpn, S.row_ptr.p, S.col.p, S.free_map.p,
                                                            S.red_map.p, nullptr, F.rp.p, F.ci.p, S.ctx->d_flag);
   TPT_CHECK_LAUNCH();
-  // explicit transpose of L
+  F.sigma2.alloc(n, s);
+  F.va.alloc(F.nnz, s);
+  F.ready_pattern = true;
+}
+
+void fsai_build_transpose(const SystemData& S, FsaiFactor& F) {
+  if (F.transposed || !F.ready_pattern) return;
+  cudaStream_t s = S.ctx->stream;
+  const int n = (int)F.n;
+  DevBuf<int> cnt;
+  cnt.alloc(n + 1, s);
   cnt.zero();
   col_counts<<<ceil_div(std::max<int64_t>(F.nnz, 1), 256), 256, 0, s>>>(F.nnz, F.ci.p, cnt.p);
   TPT_CHECK_LAUNCH();
@@ -243,19 +260,23 @@ void fsai_build_pattern(const SystemData& S, FsaiFactor& F) {
   TPT_CHECK_LAUNCH();
   transpose_sort<<<ceil_div((int64_t)n * 32, 256), 256, 0, s>>>(n, F.trp.p, F.tci.p, F.perm.p);
   TPT_CHECK_LAUNCH();
-  F.sigma2.alloc(n, s);
-  F.va.alloc(F.nnz, s);
   F.tva.alloc(F.nnz, s);
-  F.ready_pattern = true;
+  if (F.values_set && F.nnz) {
+    transpose_values<<<ceil_div(F.nnz, 256), 256, 0, s>>>(F.nnz, F.perm.p, F.va.p, F.tva.p);
+    TPT_CHECK_LAUNCH();
+  }
+  F.transposed = true;
 }
 
 bool fsai_set_values(const SystemData& S, FsaiFactor& F, const double* d_sig2, const double* d_lva) {
   cudaStream_t s = S.ctx->stream;
   TPT_CUDA(cudaMemsetAsync(S.ctx->d_flag, 0, sizeof(int), s));
   const int64_t m = std::max<int64_t>(F.n, F.nnz);
-  factor_to_lowp<<<ceil_div(std::max<int64_t>(m, 1), 256), 256, 0, s>>>((int)F.n, F.nnz, d_sig2, d_lva, F.perm.p,
-                                                                        F.sigma2.p, F.va.p, F.tva.p, S.ctx->d_flag);
+  factor_to_lowp<<<ceil_div(std::max<int64_t>(m, 1), 256), 256, 0, s>>>(
+      (int)F.n, F.nnz, d_sig2, d_lva, F.transposed ? F.perm.p : nullptr, F.sigma2.p, F.va.p,
+      F.transposed ? F.tva.p : nullptr, S.ctx->d_flag);
   TPT_CHECK_LAUNCH();
+  F.values_set = true;
   int flag = 0;
   TPT_CUDA(cudaMemcpyAsync(&flag, S.ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
   TPT_CUDA(cudaStreamSynchronize(s));

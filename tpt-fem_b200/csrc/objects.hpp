@@ -20,6 +20,8 @@ struct tptfem_context {
   void* cublas = nullptr;    // cublasHandle_t, created on first use
   int* d_flag = nullptr;  // device error/validation flag scratch (one int)
   int* h_pinned = nullptr;  // pinned staging (64 bytes)
+  void* h_stage = nullptr;  // pinned staging of large user arrays (staging.cu), grown on demand
+  size_t h_stage_bytes = 0;
   std::map<uint64_t, int> topo_tuned;  // topopt autotuner: batch shape -> threads per instance
 };
 
@@ -110,6 +112,8 @@ struct FsaiFactor {
   int64_t n = 0, nnz = 0;
   bool ready_pattern = false;
   bool overflow = false;  // some pattern row exceeded the device limit
+  bool transposed = false;  // trp/tci/perm/tva built (only the row-wise CSR apply needs them)
+  bool values_set = false;
   DevBuf<int> rp, ci, trp, tci, perm;
   DevBuf<float> sigma2;
   DevBuf<__half> va, tva;
@@ -226,6 +230,7 @@ bool fsai_set_values(const SystemData& S, FsaiFactor& F, const double* d_sig2, c
 
 // nbsell.cu
 bool nb_build_operator(SystemData& S);  // false when the system has partial node groups
+void fsai_build_transpose(const SystemData& S, FsaiFactor& F);  // explicit L^T for the CSR apply (idempotent)
 bool nb_fill_factor(SystemData& S, const FsaiFactor& F);  // false: factor rows not node-block shaped
 bool nb_factor_shape_ok(SystemData& S, const FsaiFactor& F);  // factor rows = dpn * (lower neighbours) + a
 // io_vtk.cu: write_vtk_with_data's legacy binary bytes for a device-resident mesh
@@ -236,6 +241,12 @@ void write_file(const char* path, const std::string& bytes);
 int lanczos_eigs(tptfem_context* ctx, const MatrixData& M, int num, int largest, int dim, double* values,
                  double* vectors);
 int power_iteration(tptfem_context* ctx, const MatrixData& M, int max_iter, double tol, double* lambda, double* x_out);
+// staging.cu: large host arrays through the context's pinned buffer (host threads + one DMA);
+// the _ids / _finite variants narrow / check on the way and return false on a bad value.
+void host_to_device(tptfem_context* ctx, void* dst, const void* src, size_t bytes);
+void device_to_host(tptfem_context* ctx, void* dst, const void* src, size_t bytes);
+bool host_to_device_ids(tptfem_context* ctx, int* dst, const int64_t* src, size_t count, int64_t limit);
+bool host_to_device_finite(tptfem_context* ctx, double* dst, const double* src, size_t count);
 // io_exodus.cu: write_exodus's NetCDF-3 classic bytes for a device-resident mesh
 std::string exodus_bytes(const MeshData& m);
 void nb_build_sym(SystemData& S);  // after nb_build_operator succeeded

@@ -466,7 +466,16 @@ void prepare_fsai_engine(SystemData& S, Engine<double>& E, const FsaiFactor& F, 
   E.pc.grid = std::max(1, std::min(sm_count() * 8, ceil_div(F.n * E.pc.lanes, SPMV_THREADS)));
   E.pc.sigma2 = F.sigma2.p;
   E.pc.g_rp = F.rp.p; E.pc.g_ci = F.ci.p; E.pc.g_va = F.va.p;
-  E.pc.gt_rp = F.trp.p; E.pc.gt_ci = F.tci.p; E.pc.gt_va = F.tva.p;
+}
+
+// The row-wise CSR apply (no node-block factor) needs the explicit transpose.
+void ensure_csr_fsai(SystemData& S, Engine<double>& E, FsaiFactor& F) {
+  if (E.nb_pc) return;
+  fsai_build_transpose(S, F);
+  if (E.pc.gt_va != F.tva.p) {
+    E.pc.gt_rp = F.trp.p; E.pc.gt_ci = F.tci.p; E.pc.gt_va = F.tva.p;
+    if (E.exec) { cudaGraphExecDestroy(E.exec); E.exec = nullptr; }
+  }
 }
 
 // Learned factor values: network forward on this system, converted to the
@@ -572,6 +581,7 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o_in, tptfem_solve_st
       } else {
         const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : RELIABLE_DELTA_F64;
         try {
+          ensure_csr_fsai(S, W.f64_lf, W.lf);
           iters = run_reliable<double>(S, W.f64_lf, tol, delta, max_it, bnorm, st);
         } catch (const Error& e) {
           if (e.status != TPTFEM_ERR_BREAKDOWN) throw;
@@ -679,6 +689,7 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o_in, tptfem_solve_st
     iters = run_reliable<float>(S, W.f32, tol, delta, max_it, bnorm, st);
   } else {
     const double delta = o.inner_rel_tol > 0 ? o.inner_rel_tol : RELIABLE_DELTA_F64;
+    ensure_csr_fsai(S, W.f64_fsai, W.fsai);
     iters = run_reliable<double>(S, W.f64_fsai, tol, delta, max_it, bnorm, st);
   }
   const double rel = bb == 0.0 ? 0.0 : std::sqrt(true_residual2(S, S.x.p)) / bnorm;
