@@ -83,6 +83,7 @@ typedef struct tptfem_context tptfem_context;
 typedef struct tptfem_mesh tptfem_mesh;
 typedef struct tptfem_matrix tptfem_matrix;
 typedef struct tptfem_system tptfem_system;
+typedef struct tptfem_dist tptfem_dist;
 
 typedef struct tptfem_solver_opts {
   int32_t solver;        /* TPTFEM_SOLVER_* */
@@ -217,6 +218,39 @@ tptfem_status tptfem_load_body(tptfem_context* ctx, tptfem_mesh* mesh, const dou
  * (0 elsewhere), applied to component c of each of the dofs_per_node components. */
 tptfem_status tptfem_apply_traction(tptfem_context* ctx, tptfem_mesh* mesh, int dofs_per_node, int axis,
                                     double sign, const double* traction, double* rhs);
+
+/* ---- row-partitioned solve over several GPUs ---------------------------------------
+ * No counterpart in the reference (its solve is single-threaded).  The reduced system is
+ * split into contiguous row ranges row_starts[k] .. row_starts[k+1] (node-aligned: the
+ * x-slabs of a box mesh); rank k, on its own GPU, creates its part from the whole reduced
+ * system and runs FP64 Jacobi-PCG with the caller doing the communication each iteration:
+ *   tptfem_dist_start                           -> local r.r, r.z        (sum over ranks)
+ *   loop: tptfem_dist_pack; exchange (send_buf segment for rank q goes to q's ghost segment
+ *         for this rank, counts from tptfem_dist_counts); tptfem_dist_spmv_dot -> local p.q
+ *         (sum); alpha = r.z / p.q; tptfem_dist_update(alpha) -> local r.r, r.z (sum);
+ *         beta = r.z_new / r.z; tptfem_dist_direction(beta)
+ * Partial sums are reproducible; add the ranks' values in rank order for bitwise-equal runs. */
+tptfem_status tptfem_dist_create(tptfem_context* ctx, tptfem_system* sys, int rank, int size,
+                                 const int64_t* row_starts, tptfem_dist** out);
+/* owned rows, ghost entries, and per peer rank the send / receive counts (size entries each) */
+tptfem_status tptfem_dist_counts(const tptfem_dist* d, int64_t* n_owned, int64_t* n_ghost, int64_t* send_counts,
+                                 int64_t* recv_counts);
+/* device pointers: the packed send buffer (peers in rank order) and the ghost part of p
+ * (peers in rank order), for a device-side exchange such as NCCL send/recv */
+tptfem_status tptfem_dist_buffers(const tptfem_dist* d, double** send_buf, double** ghost_buf);
+tptfem_status tptfem_dist_start(tptfem_context* ctx, tptfem_dist* d, double out_rr_rz[2]);
+tptfem_status tptfem_dist_pack(tptfem_context* ctx, tptfem_dist* d);
+tptfem_status tptfem_dist_spmv_dot(tptfem_context* ctx, tptfem_dist* d, double* out_pq);
+tptfem_status tptfem_dist_update(tptfem_context* ctx, tptfem_dist* d, double alpha, double out_rr_rz[2]);
+tptfem_status tptfem_dist_direction(tptfem_context* ctx, tptfem_dist* d, double beta);
+/* the owned part of the reduced solution (n_owned doubles, host) */
+tptfem_status tptfem_dist_solution(tptfem_context* ctx, const tptfem_dist* d, double* x_owned);
+void tptfem_dist_free(tptfem_dist* d);
+/* nranks ranks on this context's GPU in lock step, the exchange done by device copies:
+ * the same arithmetic as nranks GPUs; x (n_free doubles, host), *relres the recursive
+ * residual at exit.  For testing the partitioned path on one device. */
+tptfem_status tptfem_dist_solve_local(tptfem_context* ctx, tptfem_system* sys, int nranks, double rel_tol,
+                                      int64_t max_iter, double* x, int64_t* iterations, double* relres);
 
 /* ---- eigenvalues (crates/tpt-fem-eigen/src/lib.rs) ---------------------------------- */
 enum { TPTFEM_EIG_SMALLEST = 0, TPTFEM_EIG_LARGEST = 1 };  /* EigWhich (eigen:122-129) */

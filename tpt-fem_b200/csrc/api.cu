@@ -297,6 +297,75 @@ tptfem_status tptfem_power_iteration(tptfem_context* ctx, const tptfem_matrix* m
   API_CATCH(ctx)
 }
 
+tptfem_status tptfem_dist_create(tptfem_context* ctx, tptfem_system* sys, int rank, int size,
+                                 const int64_t* row_starts, tptfem_dist** out) {
+  if (!ctx || !sys || !sys->d || !row_starts || !out) return TPTFEM_ERR_INVALID_ARG;
+  *out = nullptr;
+  API_TRY
+  set_device(ctx);
+  *out = new tptfem_dist{dist_create(ctx, *sys->d, rank, size, row_starts)};
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_dist_counts(const tptfem_dist* d, int64_t* n_owned, int64_t* n_ghost, int64_t* send_counts,
+                                 int64_t* recv_counts) {
+  if (!d || !d->d) return TPTFEM_ERR_INVALID_ARG;
+  const DistData& D = *d->d;
+  if (n_owned) *n_owned = D.nloc;
+  if (n_ghost) *n_ghost = D.nghost;
+  for (int k = 0; k < D.size; ++k) {
+    if (send_counts) send_counts[k] = D.send_off[k + 1] - D.send_off[k];
+    if (recv_counts) recv_counts[k] = D.recv_off[k + 1] - D.recv_off[k];
+  }
+  return TPTFEM_OK;
+}
+
+tptfem_status tptfem_dist_buffers(const tptfem_dist* d, double** send_buf, double** ghost_buf) {
+  if (!d || !d->d || !send_buf || !ghost_buf) return TPTFEM_ERR_INVALID_ARG;
+  *send_buf = d->d->send_buf.p;
+  *ghost_buf = d->d->p.p + d->d->nloc;
+  return TPTFEM_OK;
+}
+
+#define TPT_DIST_CALL(body)                        \
+  if (!ctx || !d || !d->d) return TPTFEM_ERR_INVALID_ARG; \
+  API_TRY                                          \
+  set_device(ctx);                                 \
+  body;                                            \
+  API_CATCH(ctx)
+
+tptfem_status tptfem_dist_start(tptfem_context* ctx, tptfem_dist* d, double out_rr_rz[2]) {
+  TPT_DIST_CALL(dist_start(*d->d, out_rr_rz))
+}
+tptfem_status tptfem_dist_pack(tptfem_context* ctx, tptfem_dist* d) { TPT_DIST_CALL(dist_pack(*d->d)) }
+tptfem_status tptfem_dist_spmv_dot(tptfem_context* ctx, tptfem_dist* d, double* out_pq) {
+  TPT_DIST_CALL(*out_pq = dist_spmv_dot(*d->d))
+}
+tptfem_status tptfem_dist_update(tptfem_context* ctx, tptfem_dist* d, double alpha, double out_rr_rz[2]) {
+  TPT_DIST_CALL(dist_update(*d->d, alpha, out_rr_rz))
+}
+tptfem_status tptfem_dist_direction(tptfem_context* ctx, tptfem_dist* d, double beta) {
+  TPT_DIST_CALL(dist_direction(*d->d, beta))
+}
+tptfem_status tptfem_dist_solution(tptfem_context* ctx, const tptfem_dist* d, double* x_owned) {
+  TPT_DIST_CALL({
+    if (d->d->nloc) device_to_host(ctx, x_owned, d->d->x.p, d->d->nloc * sizeof(double));
+  })
+}
+#undef TPT_DIST_CALL
+
+void tptfem_dist_free(tptfem_dist* d) { delete d; }
+
+tptfem_status tptfem_dist_solve_local(tptfem_context* ctx, tptfem_system* sys, int nranks, double rel_tol,
+                                      int64_t max_iter, double* x, int64_t* iterations, double* relres) {
+  if (!ctx || !sys || !sys->d || !x || !iterations || !relres) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  *iterations = dist_solve_local(ctx, *sys->d, nranks, rel_tol > 0 ? rel_tol : 1e-10, max_iter > 0 ? max_iter : 100000,
+                                 x, relres);
+  API_CATCH(ctx)
+}
+
 void tptfem_mesh_free(tptfem_mesh* mesh) { delete mesh; }
 
 // ---- assembly -----------------------------------------------------------------

@@ -1,0 +1,325 @@
+// dist.cu -- row-partitioned FP64 Jacobi-PCG over several ranks (one per GPU).
+//
+// The reduced system is split into contiguous, node-aligned row ranges (the
+// x-slabs of a box mesh, whose nodes are numbered x-major).  Rank k keeps its
+// rows with the columns renumbered: owned columns first (0..nloc), then the
+// ghost columns it reads from other ranks, sorted by global index, so the
+// ghosts of each peer form one contiguous run.  One PCG iteration needs one
+// exchange of p's ghost values and two all-reduces:
+//   pack p -> send | exchange | q = A_loc p, p.q | sum | x, r, z update, r.r, r.z | sum | p = z + beta p
+// This file does each rank's device work (C ABI tptfem_dist_*); the exchange
+// and the sums belong to the caller (NCCL over torch.distributed for ranks on
+// different GPUs), or to tptfem_dist_solve_local, which runs several ranks on
+// one device in lock step with device copies as the exchange.  Partial sums
+// are per-block values added in a fixed order, so results are reproducible.
+// The plain method only: Jacobi preconditioning, FP64 throughout.
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <vector>
+
+#include "objects.hpp"
+
+namespace tptfem {
+
+namespace {
+
+constexpr int DT_THREADS = 256, DT_LPR = 8;
+
+// q = A_loc p on the owned rows (DT_LPR lanes per row), per-block p.q partials.
+__global__ void __launch_bounds__(DT_THREADS) dist_spmv_dot(int64_t nloc, const int* __restrict__ rp,
+                                                            const int* __restrict__ ci,
+                                                            const double* __restrict__ va,
+                                                            const double* __restrict__ p, double* __restrict__ q,
+                                                            double* __restrict__ part) {
+  __shared__ double sh[DT_THREADS / DT_LPR];
+  const int64_t t = (int64_t)blockIdx.x * DT_THREADS + threadIdx.x;
+  const int64_t i = t / DT_LPR;
+  const int l = (int)(t % DT_LPR);
+  double s = 0.0;
+  if (i < nloc)
+    for (int k = rp[i] + l; k < rp[i + 1]; k += DT_LPR) s += va[k] * p[ci[k]];
+  const unsigned m = 0xffffffffu;
+  for (int o = DT_LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(m, s, o, DT_LPR);
+  double d = 0.0;
+  if (i < nloc && l == 0) {
+    q[i] = s;
+    d = p[i] * s;
+  }
+  if (l == 0) sh[threadIdx.x / DT_LPR] = d;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < DT_THREADS / DT_LPR; ++w) a += sh[w];
+    part[blockIdx.x] = a;
+  }
+}
+
+// x += a p, r -= a q, z = dinv r; per-block partials of r.r and r.z.
+__global__ void __launch_bounds__(DT_THREADS) dist_update(int64_t nloc, double a, double* __restrict__ x,
+                                                          double* __restrict__ r, double* __restrict__ z,
+                                                          const double* __restrict__ p,
+                                                          const double* __restrict__ q,
+                                                          const double* __restrict__ dinv,
+                                                          double* __restrict__ part) {
+  __shared__ double s1[DT_THREADS], s2[DT_THREADS];
+  const int64_t i = (int64_t)blockIdx.x * DT_THREADS + threadIdx.x;
+  double rr = 0.0, rz = 0.0;
+  if (i < nloc) {
+    x[i] += a * p[i];
+    const double ri = r[i] - a * q[i];
+    r[i] = ri;
+    const double zi = dinv[i] * ri;
+    z[i] = zi;
+    rr = ri * ri;
+    rz = ri * zi;
+  }
+  s1[threadIdx.x] = rr;
+  s2[threadIdx.x] = rz;
+  __syncthreads();
+  for (int o = DT_THREADS / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      s1[threadIdx.x] += s1[threadIdx.x + o];
+      s2[threadIdx.x] += s2[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = s1[0];
+    part[2 * blockIdx.x + 1] = s2[0];
+  }
+}
+
+__global__ void dist_direction(int64_t nloc, double beta, const double* __restrict__ z, double* __restrict__ p) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nloc) p[i] = z[i] + beta * p[i];
+}
+
+__global__ void dist_pack(int64_t ns, const int* __restrict__ idx, const double* __restrict__ p,
+                          double* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ns) out[i] = p[idx[i]];
+}
+
+__global__ void dist_diag(int64_t nloc, const int* __restrict__ rp, const int* __restrict__ ci,
+                          const double* __restrict__ va, double* __restrict__ dinv, int* __restrict__ flag) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nloc) return;
+  double d = 0.0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k)
+    if (ci[k] == i) d = va[k];
+  if (!(d > 0.0)) atomicOr(flag, 1);
+  dinv[i] = d > 0.0 ? 1.0 / d : 0.0;
+}
+
+}  // namespace
+
+double DistData::sum_parts(int nb, int stride, int which) {
+  TPT_CUDA(cudaMemcpyAsync(hpart.data(), part.p, (size_t)nb * stride * sizeof(double), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  TPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  double s = 0.0;
+  for (int b = 0; b < nb; ++b) s += hpart[(size_t)b * stride + which];
+  return s;
+}
+
+std::unique_ptr<DistData> dist_create(tptfem_context* ctx, SystemData& S, int rank, int size,
+                                      const int64_t* row_starts) {
+  TPT_REQUIRE(size >= 1 && rank >= 0 && rank < size, TPTFEM_ERR_INVALID_ARG, "bad rank / size");
+  TPT_REQUIRE(row_starts[0] == 0 && row_starts[size] == S.n_free, TPTFEM_ERR_INVALID_ARG,
+              "row_starts must run from 0 to the number of free dofs");
+  for (int k = 0; k < size; ++k)
+    TPT_REQUIRE(row_starts[k] <= row_starts[k + 1], TPTFEM_ERR_INVALID_ARG, "row_starts must be ascending");
+  cudaStream_t s = ctx->stream;
+  auto D = std::make_unique<DistData>();
+  D->ctx = ctx;
+  D->rank = rank;
+  D->size = size;
+  D->r0 = row_starts[rank];
+  D->r1 = row_starts[rank + 1];
+  D->nloc = D->r1 - D->r0;
+  const int64_t n = S.n_free;
+  // structure on the host, once: the whole pattern (every rank needs its
+  // peers' ghost lists to know what to send)
+  std::vector<int> hrp(n + 1), hci(S.nnz);
+  S.row_ptr.download(hrp.data(), n + 1);
+  S.col.download(hci.data(), S.nnz);
+  TPT_CUDA(cudaStreamSynchronize(s));
+  auto owner = [&](int64_t c) {
+    return (int)(std::upper_bound(row_starts, row_starts + size + 1, c) - row_starts - 1);
+  };
+  // ghosts of this rank: columns of its rows outside [r0, r1), sorted unique
+  std::vector<int> ghosts;
+  for (int64_t row = D->r0; row < D->r1; ++row)
+    for (int k = hrp[row]; k < hrp[row + 1]; ++k)
+      if (hci[k] < D->r0 || hci[k] >= D->r1) ghosts.push_back(hci[k]);
+  std::sort(ghosts.begin(), ghosts.end());
+  ghosts.erase(std::unique(ghosts.begin(), ghosts.end()), ghosts.end());
+  D->nghost = (int64_t)ghosts.size();
+  D->recv_off.assign(size + 1, 0);
+  for (int g : ghosts) D->recv_off[owner(g) + 1]++;
+  for (int k = 0; k < size; ++k) D->recv_off[k + 1] += D->recv_off[k];
+  // local CSR with renumbered columns
+  const int64_t k0 = hrp[D->r0], k1 = hrp[D->r1], nnzl = k1 - k0;
+  std::vector<int> lrp(D->nloc + 1), lci(nnzl);
+  for (int64_t row = D->r0; row <= D->r1; ++row) lrp[row - D->r0] = (int)(hrp[row] - k0);
+  for (int64_t k = k0; k < k1; ++k) {
+    const int c = hci[k];
+    lci[k - k0] = (c >= D->r0 && c < D->r1)
+                      ? (int)(c - D->r0)
+                      : (int)(D->nloc + (std::lower_bound(ghosts.begin(), ghosts.end(), c) - ghosts.begin()));
+  }
+  // send lists: for each peer q, the owned rows q reads, ascending (q's ghost order)
+  std::vector<int> sidx;
+  D->send_off.assign(size + 1, 0);
+  for (int qr = 0; qr < size; ++qr) {
+    std::vector<int> need;
+    if (qr != rank)
+      for (int64_t row = row_starts[qr]; row < row_starts[qr + 1]; ++row)
+        for (int k = hrp[row]; k < hrp[row + 1]; ++k)
+          if (hci[k] >= D->r0 && hci[k] < D->r1) need.push_back(hci[k]);
+    std::sort(need.begin(), need.end());
+    need.erase(std::unique(need.begin(), need.end()), need.end());
+    for (int c : need) sidx.push_back((int)(c - D->r0));
+    D->send_off[qr + 1] = D->send_off[qr] + (int64_t)need.size();
+  }
+  D->rp.alloc(D->nloc + 1, s);
+  D->rp.upload(lrp.data(), lrp.size());
+  D->ci.alloc(std::max<int64_t>(nnzl, 1), s);
+  D->ci.upload(lci.data(), nnzl);
+  D->va.alloc(std::max<int64_t>(nnzl, 1), s);
+  if (nnzl) TPT_CUDA(cudaMemcpyAsync(D->va.p, S.val.p + k0, nnzl * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  D->send_idx.alloc(std::max<size_t>(sidx.size(), 1), s);
+  D->send_idx.upload(sidx.data(), sidx.size());
+  D->send_buf.alloc(std::max<size_t>(sidx.size(), 1), s);
+  const int64_t nl = std::max<int64_t>(D->nloc, 1);
+  D->b.alloc(nl, s);
+  if (D->nloc)
+    TPT_CUDA(cudaMemcpyAsync(D->b.p, S.fred.p + D->r0, D->nloc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  D->dinv.alloc(nl, s);
+  D->x.alloc(nl, s);
+  D->r.alloc(nl, s);
+  D->z.alloc(nl, s);
+  D->q.alloc(nl, s);
+  D->p.alloc(D->nloc + D->nghost + 1, s);
+  D->blocks_spmv = std::max(1, ceil_div(D->nloc * DT_LPR, DT_THREADS));
+  D->blocks_vec = std::max(1, ceil_div(D->nloc, DT_THREADS));
+  D->part.alloc(2 * (size_t)std::max(D->blocks_spmv, D->blocks_vec), s);
+  D->hpart.resize(2 * (size_t)std::max(D->blocks_spmv, D->blocks_vec));
+  TPT_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), s));
+  if (D->nloc) {
+    dist_diag<<<ceil_div(D->nloc, 256), 256, 0, s>>>(D->nloc, D->rp.p, D->ci.p, D->va.p, D->dinv.p, ctx->d_flag);
+    TPT_CHECK_LAUNCH();
+  }
+  int flag = 0;
+  TPT_CUDA(cudaMemcpyAsync(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TPT_CUDA(cudaStreamSynchronize(s));
+  TPT_REQUIRE(flag == 0, TPTFEM_ERR_NUMERIC, "a diagonal entry is not positive");
+  return D;
+}
+
+// x = 0, r = b, z = dinv r, p = z; partial r.r and r.z into out[0..1].
+void dist_start(DistData& D, double* out) {
+  cudaStream_t s = D.ctx->stream;
+  if (D.nloc) {
+    TPT_CUDA(cudaMemsetAsync(D.x.p, 0, D.nloc * sizeof(double), s));
+    TPT_CUDA(cudaMemcpyAsync(D.r.p, D.b.p, D.nloc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    TPT_CUDA(cudaMemsetAsync(D.q.p, 0, D.nloc * sizeof(double), s));
+    TPT_CUDA(cudaMemsetAsync(D.p.p, 0, D.nloc * sizeof(double), s));
+  }
+  dist_update<<<D.blocks_vec, DT_THREADS, 0, s>>>(D.nloc, 0.0, D.x.p, D.r.p, D.z.p, D.p.p, D.q.p, D.dinv.p, D.part.p);
+  TPT_CHECK_LAUNCH();
+  out[0] = D.sum_parts(D.blocks_vec, 2, 0);
+  out[1] = D.sum_parts(D.blocks_vec, 2, 1);
+  dist_direction<<<D.blocks_vec, DT_THREADS, 0, s>>>(D.nloc, 0.0, D.z.p, D.p.p);
+  TPT_CHECK_LAUNCH();
+}
+
+void dist_pack(DistData& D) {
+  const int64_t ns = D.send_off[D.size];
+  if (ns) {
+    dist_pack<<<ceil_div(ns, 256), 256, 0, D.ctx->stream>>>(ns, D.send_idx.p, D.p.p, D.send_buf.p);
+    TPT_CHECK_LAUNCH();
+  }
+  TPT_CUDA(cudaStreamSynchronize(D.ctx->stream));  // the caller's exchange reads send_buf
+}
+
+double dist_spmv_dot(DistData& D) {
+  dist_spmv_dot<<<D.blocks_spmv, DT_THREADS, 0, D.ctx->stream>>>(D.nloc, D.rp.p, D.ci.p, D.va.p, D.p.p, D.q.p,
+                                                                 D.part.p);
+  TPT_CHECK_LAUNCH();
+  return D.sum_parts(D.blocks_spmv, 1, 0);
+}
+
+void dist_update(DistData& D, double alpha, double* out) {
+  dist_update<<<D.blocks_vec, DT_THREADS, 0, D.ctx->stream>>>(D.nloc, alpha, D.x.p, D.r.p, D.z.p, D.p.p, D.q.p,
+                                                              D.dinv.p, D.part.p);
+  TPT_CHECK_LAUNCH();
+  out[0] = D.sum_parts(D.blocks_vec, 2, 0);
+  out[1] = D.sum_parts(D.blocks_vec, 2, 1);
+}
+
+void dist_direction(DistData& D, double beta) {
+  dist_direction<<<D.blocks_vec, DT_THREADS, 0, D.ctx->stream>>>(D.nloc, beta, D.z.p, D.p.p);
+  TPT_CHECK_LAUNCH();
+}
+
+// Several ranks on one device in lock step, the exchange done by device copies.
+int64_t dist_solve_local(tptfem_context* ctx, SystemData& S, int nranks, double tol, int64_t max_iter, double* u_red,
+                         double* relres) {
+  TPT_REQUIRE(nranks >= 1, TPTFEM_ERR_INVALID_ARG, "nranks must be >= 1");
+  const int64_t groups = S.n_free / std::max(1, S.dpn);
+  std::vector<int64_t> starts(nranks + 1);
+  for (int k = 0; k <= nranks; ++k)
+    starts[k] = (S.n_free % S.dpn == 0) ? groups * k / nranks * S.dpn : S.n_free * k / nranks;
+  starts[nranks] = S.n_free;
+  std::vector<std::unique_ptr<DistData>> R;
+  for (int k = 0; k < nranks; ++k) R.push_back(dist_create(ctx, S, k, nranks, starts.data()));
+  cudaStream_t s = ctx->stream;
+  auto exchange = [&]() {
+    for (auto& d : R) dist_pack(*d);
+    for (int k = 0; k < nranks; ++k)
+      for (int q = 0; q < nranks; ++q) {
+        const int64_t cnt = R[q]->send_off[k + 1] - R[q]->send_off[k];
+        if (q == k || !cnt) continue;
+        TPT_CUDA(cudaMemcpyAsync(R[k]->p.p + R[k]->nloc + R[k]->recv_off[q], R[q]->send_buf.p + R[q]->send_off[k],
+                                 cnt * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      }
+  };
+  double rr = 0.0, rz = 0.0, bb = 0.0;
+  for (auto& d : R) {
+    double o[2];
+    dist_start(*d, o);
+    rr += o[0];
+    rz += o[1];
+  }
+  bb = rr;
+  int64_t it = 0;
+  const double target = tol * tol * bb;
+  while (rr > target && it < max_iter) {
+    exchange();
+    double pq = 0.0;
+    for (auto& d : R) pq += dist_spmv_dot(*d);
+    TPT_REQUIRE(pq > 0.0, TPTFEM_ERR_BREAKDOWN, "PCG breakdown: p.Ap <= 0");
+    const double alpha = rz / pq;
+    double nrr = 0.0, nrz = 0.0;
+    for (auto& d : R) {
+      double o[2];
+      dist_update(*d, alpha, o);
+      nrr += o[0];
+      nrz += o[1];
+    }
+    const double beta = nrz / rz;
+    rr = nrr;
+    rz = nrz;
+    for (auto& d : R) dist_direction(*d, beta);
+    ++it;
+  }
+  for (auto& d : R)
+    if (d->nloc) d->x.download(u_red + d->r0, d->nloc);
+  TPT_CUDA(cudaStreamSynchronize(s));
+  *relres = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;  // recursive residual
+  return it;
+}
+
+}  // namespace tptfem

@@ -247,6 +247,27 @@ void host_to_device(tptfem_context* ctx, void* dst, const void* src, size_t byte
 void device_to_host(tptfem_context* ctx, void* dst, const void* src, size_t bytes);
 bool host_to_device_ids(tptfem_context* ctx, int* dst, const int64_t* src, size_t count, int64_t limit);
 bool host_to_device_finite(tptfem_context* ctx, double* dst, const double* src, size_t count);
+// dist.cu: one rank of the row-partitioned FP64 Jacobi-PCG (see the file's header)
+struct DistData {
+  tptfem_context* ctx = nullptr;
+  int rank = 0, size = 1;
+  int64_t r0 = 0, r1 = 0, nloc = 0, nghost = 0;
+  DevBuf<int> rp, ci, send_idx;
+  DevBuf<double> va, dinv, b, x, r, z, p, q, send_buf, part;
+  std::vector<int64_t> send_off, recv_off;  // per peer rank: ranges in send_buf / in the ghost part of p
+  std::vector<double> hpart;
+  int blocks_spmv = 1, blocks_vec = 1;
+  double sum_parts(int nb, int stride, int which);
+};
+std::unique_ptr<DistData> dist_create(tptfem_context* ctx, SystemData& S, int rank, int size,
+                                      const int64_t* row_starts);
+void dist_start(DistData& D, double* out);
+void dist_pack(DistData& D);
+double dist_spmv_dot(DistData& D);
+void dist_update(DistData& D, double alpha, double* out);
+void dist_direction(DistData& D, double beta);
+int64_t dist_solve_local(tptfem_context* ctx, SystemData& S, int nranks, double tol, int64_t max_iter,
+                         double* u_red, double* relres);
 // io_exodus.cu: write_exodus's NetCDF-3 classic bytes for a device-resident mesh
 std::string exodus_bytes(const MeshData& m);
 void nb_build_sym(SystemData& S);  // after nb_build_operator succeeded
@@ -285,6 +306,9 @@ struct tptfem_mesh {
 };
 struct tptfem_matrix {
   std::unique_ptr<tptfem::MatrixData> d;
+};
+struct tptfem_dist {
+  std::unique_ptr<tptfem::DistData> d;
 };
 struct tptfem_system {
   std::unique_ptr<tptfem::SystemData> d;

@@ -91,6 +91,17 @@ SIGNATURES = {
     "tptfem_mesh_write_vtk": (C.c_int, [_vp, _vp, C.c_char_p, C.c_char_p, C.c_int, _vp, _vp]),
     "tptfem_mesh_write_exodus": (C.c_int, [_vp, _vp, C.c_char_p]),
     "tptfem_lanczos_eigs": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp]),
+    "tptfem_dist_create": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _vp, _pp]),
+    "tptfem_dist_counts": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "tptfem_dist_buffers": (C.c_int, [_vp, _pp, _pp]),
+    "tptfem_dist_start": (C.c_int, [_vp, _vp, _vp]),
+    "tptfem_dist_pack": (C.c_int, [_vp, _vp]),
+    "tptfem_dist_spmv_dot": (C.c_int, [_vp, _vp, _vp]),
+    "tptfem_dist_update": (C.c_int, [_vp, _vp, C.c_double, _vp]),
+    "tptfem_dist_direction": (C.c_int, [_vp, _vp, C.c_double]),
+    "tptfem_dist_solution": (C.c_int, [_vp, _vp, _vp]),
+    "tptfem_dist_free": (None, [_vp]),
+    "tptfem_dist_solve_local": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_int64, _vp, _vp, _vp]),
     "tptfem_power_iteration": (C.c_int, [_vp, _vp, C.c_int, C.c_double, _vp, _vp, _vp]),
     "tptfem_assemble_poisson_robin": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                                 _pp]),
