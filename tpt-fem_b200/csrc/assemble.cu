@@ -644,87 +644,77 @@ __global__ void __launch_bounds__(128) assemble_rows(RowArgs A) {
 
 // Tet4 rows, one warp per node: the node's rows (n, 0..DPN-1) against its
 // neighbour slots, lane k owning slot k (at most 32 neighbours) and holding
-// the DPN x DPN accumulators of that column block in registers.  The lanes
-// first compute the geometry of the node's incident elements (one element per
-// lane, into shared memory), then walk the elements in ascending id: the four
-// lanes whose slots an element touches add their block of the element row, so
-// every entry is summed in element order from +0.0 as in assemble_rows (and in
-// Coo::to_csr's duplicate sum).  Same modes and outputs as assemble_rows.
+// the DPN x DPN accumulators of that column block in registers.  First each
+// lane takes one incident element and computes the node's element-row blocks
+// against the element's four nodes (shared memory, with each block's slot);
+// then the lanes walk the elements in ascending id and the lane owning a
+// block's slot adds it, so every entry is summed in element order from +0.0
+// as in assemble_rows (and in Coo::to_csr's duplicate sum).  Same modes and
+// outputs as assemble_rows.
 constexpr int AN_WARPS = 4;     // warps per block
-constexpr int AN_MAXDEG = 64;   // incident elements per node handled here
+constexpr int AN_MAXDEG = 32;   // incident elements per node handled here (one per lane)
 
-template <int PHYS, int DPN, int MODE>
-__global__ void __launch_bounds__(32 * AN_WARPS) assemble_nodes_tet(RowArgs A, int64_t n_nodes) {
-  struct ElemG {
-    double g[4][3];
-    double adet, coef;
-    int l;
-    uchar4 slot;
-  };
-  __shared__ ElemG eg[AN_WARPS][AN_MAXDEG];
+template <int PHYS, int DPN>
+__global__ void __launch_bounds__(32 * AN_WARPS) assemble_nodes_tet(RowArgs A, int64_t n_nodes, int mode) {
+  constexpr int D2 = DPN * DPN;
+  __shared__ double blk[AN_WARPS][AN_MAXDEG][4][D2];
+  __shared__ uchar4 bslot[AN_WARPS][AN_MAXDEG];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t n = (int64_t)blockIdx.x * AN_WARPS + w;
   if (n >= n_nodes) return;  // whole warps leave together
   const int k0 = A.ne_ptr[n], deg = A.ne_ptr[n + 1] - k0;
   bool ok = true;
-  for (int i = lane; i < deg; i += 32) {
-    const int pe = A.ne[k0 + i];
-    const int e = pe >> 2;
+  if (lane < deg) {
+    const int pe = A.ne[k0 + lane];
+    const int e = pe >> 2, l = pe & 3;
     double X[4][3];
     int nodes[4];
     load_elem<TPTFEM_CELL_TET4>(A.in, e, X, nodes);
     TetGeom G;
-    ok &= tet_geom(X, G);
-    ElemG& o = eg[w][i];
+    ok = tet_geom(X, G);
+    const double coef = A.in.coef[A.in.per_elem ? e : 0];
+    const double w0 = c_cell.w[0];
+    if constexpr (PHYS == 0) {
+      const double wk = w0 * coef;
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+      for (int j = 0; j < 4; ++j) {
+        double dot = G.g[l][0] * G.g[j][0] + G.g[l][1] * G.g[j][1] + G.g[l][2] * G.g[j][2];
+        double t = wk * dot * G.adet;
+        double v = t + t;  // four identical quadrature points, summed in order
+        v = v + t;
+        blk[w][lane][j][0] = v + t;
+      }
+    } else {
+      const Dmat D = make_d(A.in.model, coef, A.in.nu);
+      const double wd = w0 * G.adet;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) o.g[j][d] = G.g[j][d];
-    o.adet = G.adet;
-    o.coef = A.in.coef[A.in.per_elem ? e : 0];
-    o.l = pe & 3;
-    o.slot = A.slot[k0 + i];
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int a = 0; a < DPN; ++a)
+#pragma unroll
+          for (int b = 0; b < DPN; ++b) {
+            double t = wd * bdb3(G.g[l], G.g[j], a, b, D);
+            double v = t + t;
+            v = v + t;
+            blk[w][lane][j][a * DPN + b] = v + t;
+          }
+    }
+    bslot[w][lane] = A.slot[k0 + lane];
   }
   __syncwarp();
-  double acc[DPN][DPN];
+  double acc[D2];
   unsigned nz = 0;  // bit a * DPN + b
 #pragma unroll
-  for (int a = 0; a < DPN; ++a)
-#pragma unroll
-    for (int b = 0; b < DPN; ++b) acc[a][b] = 0.0;
-  const double w0 = c_cell.w[0];
+  for (int q = 0; q < D2; ++q) acc[q] = 0.0;
   for (int i = 0; i < deg; ++i) {
-    const ElemG& o = eg[w][i];
-    const int sj[4] = {o.slot.x, o.slot.y, o.slot.z, o.slot.w};
-    int j = -1;
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-      if (sj[q] == lane) j = q;
+    const uchar4 sl = bslot[w][i];
+    const int j = sl.x == lane ? 0 : (sl.y == lane ? 1 : (sl.z == lane ? 2 : (sl.w == lane ? 3 : -1)));
     if (j < 0) continue;
-    const int l = o.l;
-    if constexpr (PHYS == 0) {
-      const double wk = w0 * o.coef;
-      double dot = o.g[l][0] * o.g[j][0] + o.g[l][1] * o.g[j][1] + o.g[l][2] * o.g[j][2];
-      double t = wk * dot * o.adet;
-      double v = t + t;  // four identical quadrature points, summed in order
-      v = v + t;
-      v = v + t;
-      acc[0][0] = acc[0][0] + v;
-      nz |= (unsigned)(v != 0.0);
-    } else {
-      const Dmat D = make_d(A.in.model, o.coef, A.in.nu);
-      const double wd = w0 * o.adet;
 #pragma unroll
-      for (int a = 0; a < DPN; ++a)
-#pragma unroll
-        for (int b = 0; b < DPN; ++b) {
-          double t = wd * bdb3(o.g[l], o.g[j], a, b, D);
-          double v = t + t;
-          v = v + t;
-          v = v + t;
-          acc[a][b] = acc[a][b] + v;
-          nz |= (unsigned)(v != 0.0) << (a * DPN + b);
-        }
+    for (int q = 0; q < D2; ++q) {
+      const double v = blk[w][i][j][q];
+      acc[q] = acc[q] + v;
+      nz |= (unsigned)(v != 0.0) << q;
     }
   }
   if (__any_sync(0xffffffffu, !ok) && lane == 0) atomicOr(A.flag, 1);
@@ -743,30 +733,28 @@ __global__ void __launch_bounds__(32 * AN_WARPS) assemble_nodes_tet(RowArgs A, i
     }
     const int total = __shfl_sync(0xffffffffu, pre, 31);
     int off = pre - cnt;
-    if (MODE == MODE_COUNT) {
+    if (mode == MODE_COUNT || mode == MODE_PADDED) {
       if (lane == 0) A.row_cnt[r] = total;
-      continue;
+      if (mode == MODE_COUNT) continue;
     }
-    if (MODE == MODE_PADDED && lane == 0) A.row_cnt[r] = total;
     int base = 0, end = 0;
-    if (MODE == MODE_PADDED) base = (int)0;
-    else {
+    if (mode != MODE_PADDED) {
       base = A.row_ptr[r];
       end = A.row_ptr[r + 1];
-      if (MODE == MODE_NUMERIC && lane == 0 && end - base != total) atomicOr(A.flag, 2);
+      if (mode == MODE_NUMERIC && lane == 0 && end - base != total) atomicOr(A.flag, 2);
     }
-    int* cdst = MODE == MODE_PADDED ? A.col + r * A.maxc : A.col + base;
-    double* vdst = MODE == MODE_PADDED ? A.val + r * A.maxc : A.val + base;
+    int* cdst = mode == MODE_PADDED ? A.col + r * A.maxc : A.col + base;
+    double* vdst = mode == MODE_PADDED ? A.val + r * A.maxc : A.val + base;
 #pragma unroll
     for (int b = 0; b < DPN; ++b) {
       if (!((rowbits >> b) & 1u)) continue;
       const int cidx = col0 + b;
-      if (MODE == MODE_NUMERIC) {
+      if (mode == MODE_NUMERIC) {
         if (base + off >= end || cdst[off] != cidx) atomicOr(A.flag, 2);
-        else vdst[off] = acc[a][b];
+        else vdst[off] = acc[a * DPN + b];
       } else {
         cdst[off] = cidx;
-        vdst[off] = acc[a][b];
+        vdst[off] = acc[a * DPN + b];
       }
       ++off;
     }
@@ -931,11 +919,7 @@ int read_flag(tptfem_context* ctx) {
 
 template <int PHYS, int DPN>
 void launch_nodes_tet(int mode, const RowArgs& A, int64_t n_nodes, cudaStream_t s) {
-  const int grid = ceil_div(n_nodes, AN_WARPS);
-  if (mode == MODE_COUNT) assemble_nodes_tet<PHYS, DPN, MODE_COUNT><<<grid, 32 * AN_WARPS, 0, s>>>(A, n_nodes);
-  else if (mode == MODE_FILL) assemble_nodes_tet<PHYS, DPN, MODE_FILL><<<grid, 32 * AN_WARPS, 0, s>>>(A, n_nodes);
-  else if (mode == MODE_PADDED) assemble_nodes_tet<PHYS, DPN, MODE_PADDED><<<grid, 32 * AN_WARPS, 0, s>>>(A, n_nodes);
-  else assemble_nodes_tet<PHYS, DPN, MODE_NUMERIC><<<grid, 32 * AN_WARPS, 0, s>>>(A, n_nodes);
+  assemble_nodes_tet<PHYS, DPN><<<ceil_div(n_nodes, AN_WARPS), 32 * AN_WARPS, 0, s>>>(A, n_nodes, mode);
   TPT_CHECK_LAUNCH();
 }
 
