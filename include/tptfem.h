@@ -385,8 +385,10 @@ tptfem_status tptfem_system_attach_lfsai(tptfem_context* ctx, tptfem_system* sys
  * independent instances: each instance is TopOptParams with a grid of
  * nelx x nely unit-size elements (Grid::new(nelx + 1, nely + 1, h),
  * topopt:89-116), its load vector and its Dirichlet list.  Per iteration the
- * displacement solve is FP64 PCG on the matrix-free Q1 operator (the
- * reference uses a dense LU) to relative residual opts.rel_tol.
+ * displacement solve is a banded FP64 Cholesky factorisation of K_FF (the
+ * reference uses a dense LU), refined to relative residual opts.rel_tol, or
+ * FP64 PCG on the matrix-free Q1 operator for grids too wide for the band
+ * kernel (see tptfem_topopt_opts.pcg_only).
  * density_filter = 0 follows the reference exactly (E_min = emin, set it to
  * 1e-3 * e0 as topopt:54 does; sensitivity filter topopt:259-279; OC
  * topopt:284-331); density_filter = 1 uses the density filter and OC loop of
@@ -415,6 +417,10 @@ typedef struct tptfem_topopt_opts {
   int32_t use_graph;      /* capture all iterations in one CUDA graph */
   int32_t plain_jacobi;   /* 1: Jacobi-PCG only; 0: Jacobi + per-instance coarse space of plane
                              rigid modes on about 48 node-box aggregates (the default) */
+  int32_t pcg_only;       /* 1: every instance by PCG; 0: instances whose grid is at most 110
+                             nodes across (half-bandwidth 2 min(nx, ny) + 3 <= 224) are solved
+                             by a banded Cholesky factor with iterative refinement to rel_tol,
+                             the others (and any factorisation that breaks down) by PCG */
 } tptfem_topopt_opts;
 
 typedef struct tptfem_topopt_stats {
@@ -423,6 +429,8 @@ typedef struct tptfem_topopt_stats {
   int64_t pcg_iterations;  /* summed over instances and iterations */
   int32_t block_threads;   /* threads per instance used */
   int32_t not_converged;   /* instances with a solve that hit max_pcg_iter or broke down */
+  int64_t refinement_steps; /* iterative-refinement steps of the direct solves, summed */
+  int32_t direct_instances; /* instances solved by the banded Cholesky factor */
 } tptfem_topopt_stats;
 
 /* Runs n instances.  compliance: sum over instances of (max_iter + 1) values,

@@ -123,9 +123,41 @@ def test_two_level_and_plain_jacobi_agree(ctx):
         P = params(nx, ny, 0.4, 1.5, 30, emin=1e-9, density_filter=True)
         f, bcs = T.cantilever_load(P.grid, node=P.grid.nx * (ny // 2) + nx)
         probs.append((P, f, bcs))
-    two, st2 = T.topopt_batch(ctx, probs, rel_tol=TOL)
-    one, st1 = T.topopt_batch(ctx, probs, rel_tol=TOL, plain_jacobi=True)
+    two, st2 = T.topopt_batch(ctx, probs, rel_tol=TOL, pcg_only=True)
+    one, st1 = T.topopt_batch(ctx, probs, rel_tol=TOL, plain_jacobi=True, pcg_only=True)
+    assert st1["direct_instances"] == 0 and st2["direct_instances"] == 0
     assert st2["pcg_iterations"] < 0.75 * st1["pcg_iterations"]
     for a, b in zip(two, one):
         assert np.max(np.abs(a.compliance - b.compliance) / b.compliance) < 1e-8
         assert np.max(np.abs(a.densities - b.densities)) < 1e-7
+
+
+def test_banded_cholesky_and_pcg_agree(ctx):
+    # the default direct solve (banded Cholesky + refinement) against two-level PCG,
+    # both to a 1e-12 residual, on grids banded along y (wide) and along x (tall)
+    probs = []
+    for nx, ny, dens in [(60, 20, True), (9, 31, False), (33, 12, True), (1, 5, False)]:
+        P = params(nx, ny, 0.4, 1.5, 12, emin=1e-9 if dens else None, density_filter=dens)
+        f, bcs = T.cantilever_load(P.grid, node=P.grid.nx * (ny // 2) + nx)
+        probs.append((P, f, bcs))
+    d, std = T.topopt_batch(ctx, probs, rel_tol=TOL)
+    p, stp = T.topopt_batch(ctx, probs, rel_tol=TOL, pcg_only=True)
+    assert std["direct_instances"] == len(probs) and std["not_converged"] == 0
+    assert std["pcg_iterations"] == 0 and stp["pcg_iterations"] > 0
+    for a, b in zip(d, p):
+        assert np.max(np.abs(a.compliance - b.compliance) / b.compliance) < 1e-9
+        assert np.max(np.abs(a.densities - b.densities)) < 1e-7
+
+
+def test_wide_grids_fall_back_to_pcg_in_the_same_batch(ctx):
+    # 112 x 112 elements: half-bandwidth 2 * 113 + 3 = 229 > 224, solved by PCG
+    probs = []
+    for nx, ny in [(112, 112), (24, 8)]:
+        P = params(nx, ny, 0.5, 1.5, 2)
+        f, bcs = T.cantilever_load(P.grid)
+        probs.append((P, f, bcs))
+    res, st = T.topopt_batch(ctx, probs, rel_tol=1e-10)
+    assert st["direct_instances"] == 1 and st["not_converged"] == 0 and st["pcg_iterations"] > 0
+    single, _ = T.topopt_batch(ctx, [probs[1]], rel_tol=1e-10)
+    assert np.max(np.abs(single[0].compliance - res[1].compliance) / res[1].compliance) < 1e-12
+    check_against_oracle(res[1], *probs[1])

@@ -39,7 +39,11 @@ struct TopoInst {
   int nelx, nely, nx, ny, ne, ndof;
   int max_iter, density_filter, has_lift;
   int ag, nax, nay, nc;  // coarse space: aggregates of ag x ag nodes, nax x nay of them, 3 modes each
-  int64_t eoff, doff, hoff, coff, toff;
+  // direct solve: banded Cholesky in the band ordering (node index i * ny + j when
+  // yfast, else j * nx + i; dof 2 * node + component), half-bandwidth bw, npad
+  // unknowns (ndof rounded up to the panel width; the extra ones are identity rows)
+  int direct, bw, yfast, npad;
+  int64_t eoff, doff, hoff, coff, toff, loff, yoff;
   double h, e0, penal, vol_frac, radius, move, emin;
   double ke0[64];  // element stiffness for E = 1, row-major 8 x 8
 };
@@ -63,6 +67,12 @@ struct TopoArgs {
   int* last_iters;   // per instance: PCG iterations of the latest solve
   long long* total_iters;
   int* flags;        // per instance: bit 0 PCG not converged, bit 1 breakdown
+  // direct solves
+  const int* dorder;       // block -> instance for the direct kernel, largest first
+  double* L;               // band factors (offset loff, npad x (bw + 1), column k holds L(k + d, k))
+  double* yb;              // band-ordered right-hand side / solution (offset yoff, npad)
+  int* direct_ok;          // per instance: 1 when this iteration's direct solve succeeded
+  long long* refine;       // per instance: iterative-refinement steps taken
 };
 
 // Block-wide sums (deterministic for a fixed block size).
@@ -419,6 +429,434 @@ __device__ double two_level_z(const TopoInst& I, const double* __restrict__ r, c
   return rz;
 }
 
+// ---- per-instance direct solve: banded Cholesky ------------------------------------
+// K_FF (fixed dofs replaced by identity rows and columns) is banded in the node
+// ordering that runs along the shorter grid direction: node (i, j) couples with
+// (i +- 1, j +- 1), so |row - col| <= bw = 2 min(nx, ny) + 3.  The factor L is
+// computed panel by panel (TD_NB columns) in one CTA, with the right-hand side
+// carried along as one extra row below the panel's R = bw + TD_NB rows, so that
+// the forward substitution comes out of the same elimination:
+//   1. A's entries of the panel's columns (rows >= the column, at most bw
+//      below) from the element moduli and the unit element matrix, one thread
+//      per (column, neighbour node); the right-hand-side row holds b;
+//   2. S = L(panel rows, earlier columns) L(panel columns, earlier columns)^T
+//      over the bw earlier columns (the right-hand-side row uses y of those
+//      columns), staged from the band storage in chunks of TD_JC columns that
+//      are prefetched into registers one chunk ahead; each thread accumulates
+//      a 4 x 4 tile of the panel in registers;
+//   3. P = A - S is eliminated in registers four columns at a time: the thread
+//      holding the 4 x 4 diagonal block factors it, the other threads of that
+//      column group eliminate their rows with it, then every later column is
+//      updated (two barriers per group);
+//   4. the columns are scaled by the pivots' inverse square roots into the band
+//      storage, and the right-hand-side row gives y of the panel's unknowns.
+// The backward substitution reads the stored panels in reverse.  The residual
+// of the result is checked on the matrix-free operator and, if needed,
+// corrected by iterative refinement with the stored factor.
+constexpr int TD_NT = 512;     // threads of the direct kernel
+constexpr int TD_NB = 32;      // panel width
+constexpr int TD_JC = 16;      // earlier columns staged per chunk
+constexpr int TD_MAXBW = 221;  // largest half-bandwidth: the panel's rows + the right-hand-side row in 4 x 4 tiles
+constexpr int TD_RSMAX = 256;  //   (at most TD_RSMAX / 4 row tiles x TD_NB / 4 column tiles = TD_NT threads)
+constexpr int TD_PF = (TD_JC * TD_RSMAX + TD_NT - 1) / TD_NT;  // prefetch registers per thread
+constexpr int TD_REFINE = 4;   // iterative-refinement steps at most
+static_assert((TD_RSMAX / 4) * (TD_NB / 4) <= TD_NT, "panel tiles must fit the block");
+static_assert(TD_NT == 16 * TD_NB, "backward dot products use 16 lanes per panel column");
+
+// rows stored per panel: R = bw + TD_NB matrix rows, the right-hand-side row R, padding to 4
+__host__ __device__ inline int td_rs(int bw) { return (bw + TD_NB + 1 + 3) & ~3; }
+__host__ __device__ inline int64_t td_smem_doubles(int bw) {
+  const int rs = td_rs(bw);
+  return (int64_t)TD_NB * rs + 2LL * TD_JC * rs + 8LL * rs;
+}
+static_assert(((TD_MAXBW + TD_NB + 1 + 3) & ~3) <= TD_RSMAX, "TD_MAXBW must fit TD_RSMAX");
+
+__device__ __forceinline__ int band_index(const TopoInst& I, int i, int j, int comp) {
+  return 2 * (I.yfast ? i * I.ny + j : j * I.nx + i) + comp;
+}
+
+// original dof (2 (j nx + i) + comp) of band unknown k < ndof
+__device__ __forceinline__ int band_to_dof(const TopoInst& I, int k) {
+  const int m = k >> 1, comp = k & 1;
+  const int i = I.yfast ? m / I.ny : m % I.nx;
+  const int j = I.yfast ? m % I.ny : m / I.nx;
+  return 2 * (j * I.nx + i) + comp;
+}
+
+__device__ __forceinline__ int dof_to_band(const TopoInst& I, int d) {
+  const int n = d >> 1;
+  return band_index(I, n % I.nx, n / I.nx, d & 1);
+}
+
+// Entries A(row, k) of band column k for the rows of node (i + di, j + dj),
+// both components, rows >= k, into col[row - K]: the sum over the elements
+// that hold both nodes.  Identity for fixed dofs and padding unknowns k >= ndof
+// (written by the node's own entry, di = dj = 0).
+__device__ void band_column_entries(const TopoInst& I, const double* __restrict__ E,
+                                    const uint8_t* __restrict__ fixed, const double* __restrict__ ke, int k, int K,
+                                    int di, int dj, double* __restrict__ col) {
+  const bool self = di == 0 && dj == 0;
+  if (k >= I.ndof) {
+    if (self) col[k - K] = 1.0;
+    return;
+  }
+  const int m = k >> 1, comp = k & 1;
+  const int i = I.yfast ? m / I.ny : m % I.nx;
+  const int j = I.yfast ? m % I.ny : m / I.nx;
+  if (fixed[2 * (j * I.nx + i) + comp]) {
+    if (self) col[k - K] = 1.0;
+    return;
+  }
+  const int i2 = i + di, j2 = j + dj;
+  if (i2 < 0 || i2 >= I.nx || j2 < 0 || j2 >= I.ny) return;
+  for (int c2 = 0; c2 < 2; ++c2) {
+    const int row = band_index(I, i2, j2, c2);
+    if (row < k || fixed[2 * (j2 * I.nx + i2) + c2]) continue;
+    double v = 0.0;
+    for (int ej = max(j, j2) - 1; ej <= min(j, j2); ++ej)
+      for (int ei = max(i, i2) - 1; ei <= min(i, i2); ++ei) {
+        if (ei < 0 || ei >= I.nelx || ej < 0 || ej >= I.nely) continue;
+        const int lc = 2 * local_node(ei - i, ej - j) + comp;
+        const int lr = 2 * local_node(ei - i2, ej - j2) + c2;
+        v += E[ej * I.nelx + ei] * ke[lr * 8 + lc];
+      }
+    col[row - K] = v;
+  }
+}
+
+// Panel K of L from the band storage into Pa (column-major, rows r = 0..R-1 of
+// the window starting at K; zero outside the band).
+template <int NT>
+__device__ void band_load_panel(int K, int bw, int RS, const double* Lb, double* Pa) {
+  const int R = bw + TD_NB, ld = bw + 1;
+  for (int q = threadIdx.x; q < TD_NB * RS; q += NT) {
+    const int c = q / RS, r = q - c * RS;
+    Pa[q] = (r >= c && r - c <= bw && r < R) ? Lb[(int64_t)(K + c) * ld + (r - c)] : 0.0;
+  }
+}
+
+// Forward substitution for panel K (L in Pa): y[K..K+NB) from the diagonal
+// block, then y[K+NB .. K+R) -= L(below) y[K..K+NB).
+template <int NT>
+__device__ void band_forward_panel(int K, int np, int bw, int RS, const double* Pa, double* yb, double* ysm) {
+  const int t = threadIdx.x, R = bw + TD_NB;
+  if (t < 32) {
+    double v = yb[K + t];
+    const double dl = 1.0 / Pa[t * RS + t];
+    double y = 0.0;
+    for (int c = 0; c < TD_NB; ++c) {
+      const double yc = __shfl_sync(0xffffffffu, v, c) * __shfl_sync(0xffffffffu, dl, c);
+      if (t == c) y = yc;
+      if (t > c) v -= Pa[c * RS + t] * yc;
+    }
+    yb[K + t] = y;
+    ysm[t] = y;
+  }
+  __syncthreads();
+  for (int r = TD_NB + t; r < R && K + r < np; r += NT) {
+    double s = 0.0;
+#pragma unroll 8
+    for (int c = 0; c < TD_NB; ++c) s += Pa[c * RS + r] * ysm[c];
+    yb[K + r] -= s;
+  }
+  __syncthreads();
+}
+
+// Backward substitution x = L^-T y over all panels, in place in yb.
+template <int NT>
+__device__ void band_backward(int np, int bw, int RS, const double* Lb, double* yb, double* Pa, double* tsm) {
+  const int t = threadIdx.x, R = bw + TD_NB;
+  for (int K = np - TD_NB; K >= 0; K -= TD_NB) {
+    band_load_panel<NT>(K, bw, RS, Lb, Pa);
+    __syncthreads();
+    {
+      const int c = t >> 4, s = t & 15;
+      double sum = 0.0;
+      for (int r = TD_NB + s; r < R && K + r < np; r += 16) sum += Pa[c * RS + r] * yb[K + r];
+      for (int o = 8; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      if (s == 0) tsm[c] = yb[K + c] - sum;
+    }
+    __syncthreads();
+    if (t < 32) {
+      double v = tsm[t];
+      const double dl = 1.0 / Pa[t * RS + t];
+      double x = 0.0;
+      for (int c = TD_NB - 1; c >= 0; --c) {
+        const double xc = __shfl_sync(0xffffffffu, v, c) * __shfl_sync(0xffffffffu, dl, c);
+        if (t == c) x = xc;
+        if (t < c) v -= Pa[t * RS + c] * xc;  // L(K + c, K + t)
+      }
+      yb[K + t] = x;
+    }
+    __syncthreads();
+  }
+}
+
+// Factor K_FF = L L^T into Lb and solve L y = yb in place.  False on a
+// non-positive pivot.
+template <int NT>
+__device__ bool band_factor_forward(const TopoInst& I, const double* __restrict__ E, const uint8_t* __restrict__ fixed,
+                                    const double* __restrict__ ke, double* Lb, double* yb, double* sm, double* piv,
+                                    int* bad) {
+  const int bw = I.bw, ld = bw + 1, np = I.npad;
+  const int R = bw + TD_NB, RS = td_rs(bw);  // row R: right-hand side
+  double* Pa = sm;                    // TD_NB x RS, column-major: A of the panel
+  double* Wc = sm + TD_NB * RS;       // 2 x TD_JC x RS: staged earlier columns
+  double* cg = Wc + 2 * TD_JC * RS;   // 4 x RS: the eliminated column group
+  double* cgs = cg + 4 * RS;          // 4 x RS: the same, divided by the pivots
+  __shared__ double dfac[16], dinv[4];
+  const int t = threadIdx.x;
+  const bool act = t < (RS / 4) * (TD_NB / 4);
+  const int tr = t >> 3, tc = t & 7;
+  const int r0 = 4 * tr, c0 = 4 * tc;
+  const int nw = TD_JC * RS;  // staged values per chunk
+  // staged value w = t + q NT sits at column w / RS, row w % RS: stepped without divisions
+  const int wj0 = t / RS, wr0 = t - wj0 * RS, wdj = NT / RS, wdr = NT - wdj * RS;
+  for (int K = 0; K < np; K += TD_NB) {
+    for (int q = t; q < TD_NB * RS; q += NT) Pa[q] = 0.0;
+    __syncthreads();
+    if (t < TD_NB * 9) {
+      const int c = t / 9, nb = t - 9 * c;
+      band_column_entries(I, E, fixed, ke, K + c, K, nb % 3 - 1, nb / 3 - 1, Pa + c * RS);
+      if (nb == 4) Pa[c * RS + R] = yb[K + c];
+    }
+    // S over chunk ch of the earlier columns: staged value w = j * RS + r holds
+    // L(K + r, jlo + ch * TD_JC + j), row R holds y of that column
+    const int jlo = max(0, K - bw), nch = (K - jlo + TD_JC - 1) / TD_JC;
+    double pre[TD_PF];
+#define TD_LOAD(ch)                                                                     \
+  {                                                                                     \
+    int gj = jlo + (ch) * TD_JC + wj0, r = wr0;                                         \
+    _Pragma("unroll") for (int q = 0; q < TD_PF; ++q) {                                 \
+      double v = 0.0;                                                                   \
+      const int d = K + r - gj;                                                         \
+      if (t + q * NT < nw && gj < K) {                                                  \
+        if (r == R) v = yb[gj];                                                         \
+        else if (d <= bw) v = Lb[(int64_t)gj * ld + d];                                 \
+      }                                                                                 \
+      pre[q] = v;                                                                       \
+      gj += wdj;                                                                        \
+      r += wdr;                                                                         \
+      if (r >= RS) { r -= RS; ++gj; }                                                   \
+    }                                                                                   \
+  }
+#define TD_STORE(buf)                                                                   \
+  {                                                                                     \
+    double* W_ = Wc + (buf) * nw;                                                       \
+    _Pragma("unroll") for (int q = 0; q < TD_PF; ++q) {                                 \
+      const int w = t + q * NT;                                                         \
+      if (w < nw) W_[w] = pre[q];                                                       \
+    }                                                                                   \
+  }
+    double acc[4][4];
+#pragma unroll
+    for (int a2 = 0; a2 < 4; ++a2)
+#pragma unroll
+      for (int b2 = 0; b2 < 4; ++b2) acc[a2][b2] = 0.0;
+    if (nch > 0) {
+      TD_LOAD(0);
+      TD_STORE(0);
+    }
+    __syncthreads();
+    // a tile's rows are zero in columns below K + r0 - bw (band), except the right-hand-side row
+    const bool rhs_tile = r0 + 3 >= R;
+    for (int ch = 0; ch < nch; ++ch) {
+      if (ch + 1 < nch) TD_LOAD(ch + 1);
+      const int j0 = jlo + ch * TD_JC;
+      const double* W = Wc + (ch & 1) * nw;
+      if (act && (rhs_tile || j0 + TD_JC - 1 >= K + r0 - bw)) {
+#pragma unroll 4
+        for (int j = 0; j < TD_JC; ++j) {
+          const double2 a01 = *reinterpret_cast<const double2*>(W + j * RS + r0);
+          const double2 a23 = *reinterpret_cast<const double2*>(W + j * RS + r0 + 2);
+          const double2 b01 = *reinterpret_cast<const double2*>(W + j * RS + c0);
+          const double2 b23 = *reinterpret_cast<const double2*>(W + j * RS + c0 + 2);
+          const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+          for (int a2 = 0; a2 < 4; ++a2)
+#pragma unroll
+            for (int b2 = 0; b2 < 4; ++b2) acc[a2][b2] += av[a2] * bv[b2];
+        }
+      }
+      if (ch + 1 < nch) TD_STORE((ch + 1) & 1);
+      __syncthreads();
+    }
+#undef TD_LOAD
+#undef TD_STORE
+    double p[4][4];
+#pragma unroll
+    for (int a2 = 0; a2 < 4; ++a2)
+#pragma unroll
+      for (int b2 = 0; b2 < 4; ++b2) p[a2][b2] = act ? Pa[(c0 + b2) * RS + r0 + a2] - acc[a2][b2] : 0.0;
+    // elimination, column group g = columns 4g .. 4g + 3
+    for (int g = 0; g < TD_NB / 4; ++g) {
+      if (act && tr == g && tc == g) {  // the diagonal block
+        bool okp = true;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const double pv = p[k][k];
+          okp = okp && pv > 0.0 && isfinite(pv);
+          const double iv = 1.0 / pv;
+          dinv[k] = iv;
+          piv[4 * g + k] = pv;
+#pragma unroll
+          for (int c2 = k + 1; c2 < 4; ++c2) {
+            const double f = p[c2][k] * iv;
+#pragma unroll
+            for (int r2 = c2; r2 < 4; ++r2) p[r2][c2] -= p[r2][k] * f;
+          }
+        }
+        if (!okp) *bad = 1;
+#pragma unroll
+        for (int a2 = 0; a2 < 4; ++a2)
+#pragma unroll
+          for (int b2 = 0; b2 < 4; ++b2) dfac[a2 * 4 + b2] = p[a2][b2];
+      }
+      __syncthreads();
+      if (act && tc == g) {  // the column group's other rows, then publish the group
+        if (tr != g) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int c2 = k + 1; c2 < 4; ++c2) {
+              const double f = dfac[c2 * 4 + k] * dinv[k];
+#pragma unroll
+              for (int a2 = 0; a2 < 4; ++a2) p[a2][c2] -= p[a2][k] * f;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+          for (int a2 = 0; a2 < 4; ++a2) {
+            cg[k * RS + r0 + a2] = p[a2][k];
+            cgs[k * RS + r0 + a2] = p[a2][k] * dinv[k];
+          }
+      }
+      __syncthreads();
+      if (act && tc > g) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          double l[4], f[4];
+#pragma unroll
+          for (int a2 = 0; a2 < 4; ++a2) l[a2] = cg[k * RS + r0 + a2];
+#pragma unroll
+          for (int b2 = 0; b2 < 4; ++b2) f[b2] = cgs[k * RS + c0 + b2];
+#pragma unroll
+          for (int a2 = 0; a2 < 4; ++a2)
+#pragma unroll
+            for (int b2 = 0; b2 < 4; ++b2) p[a2][b2] -= l[a2] * f[b2];
+        }
+      }
+    }
+    __syncthreads();
+    if (*bad) return false;
+    if (act) {
+#pragma unroll
+      for (int b2 = 0; b2 < 4; ++b2) {
+        const int c = c0 + b2;
+        const double sc = 1.0 / sqrt(piv[c]);
+#pragma unroll
+        for (int a2 = 0; a2 < 4; ++a2) {
+          const int r = r0 + a2;
+          if (r == R) yb[K + c] = p[a2][b2] * sc;
+          else if (r >= c && r - c <= bw && r < R) Lb[(int64_t)(K + c) * ld + (r - c)] = p[a2][b2] * sc;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  return true;
+}
+
+// One displacement solve per instance and OC iteration by the banded Cholesky
+// factor (instances marked direct; the others and failed ones are solved by
+// PCG in topo_iteration).  Writes u (original dof order) and b; moduli as in
+// topo_iteration.
+template <int NT>
+__global__ void __launch_bounds__(NT, 1) topo_direct(TopoArgs a) {
+  extern __shared__ __align__(16) double dsm[];
+  __shared__ double ke[64];
+  __shared__ double red[72];
+  __shared__ double piv[TD_NB], ysm[TD_NB], tsm[TD_NB];
+  __shared__ int bad;
+  __shared__ TopoInst I;
+  const int idx = a.dorder[blockIdx.x];
+  if (threadIdx.x == 0) {
+    I = a.inst[idx];
+    bad = 0;
+  }
+  __syncthreads();
+  if (a.iter >= max(I.max_iter, 1)) return;
+  for (int t = threadIdx.x; t < 64; t += NT) ke[t] = I.ke0[t];
+  const int ne = I.ne, nd = I.ndof, np = I.npad;
+  const double* phys = a.phys + I.eoff;
+  double* E = a.E + I.eoff;
+  const double* f = a.f + I.doff;
+  const uint8_t* fixed = a.fixed + I.doff;
+  double* u = a.u + I.doff;
+  double* r = a.r + I.doff;
+  double* q = a.q + I.doff;
+  double* b = a.b + I.doff;
+  double* Lb = a.L + I.loff;
+  double* yb = a.yb + I.yoff;
+  if (a.iter == 0 && threadIdx.x == 0) {
+    a.total_iters[idx] = 0;
+    a.flags[idx] = 0;
+    a.refine[idx] = 0;
+  }
+  const double emin = I.emin, de = I.e0 - I.emin;
+  for (int e = threadIdx.x; e < ne; e += NT) E[e] = emin + pow(a.iter == 0 ? I.vol_frac : phys[e], I.penal) * de;
+  __syncthreads();
+  if (I.has_lift) {
+    apply_k<NT>(I, E, a.ulift + I.doff, q, fixed, false, ke);
+    __syncthreads();
+    for (int d = threadIdx.x; d < nd; d += NT) b[d] = fixed[d] ? 0.0 : f[d] - q[d];
+  } else {
+    for (int d = threadIdx.x; d < nd; d += NT) b[d] = fixed[d] ? 0.0 : f[d];
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < np; k += NT) yb[k] = k < nd ? b[band_to_dof(I, k)] : 0.0;
+  __syncthreads();
+  const int RS = td_rs(I.bw);
+  bool ok = band_factor_forward<NT>(I, E, fixed, ke, Lb, yb, dsm, piv, &bad);
+  int steps = 0;
+  if (ok) {
+    band_backward<NT>(np, I.bw, RS, Lb, yb, dsm, tsm);
+    for (int d = threadIdx.x; d < nd; d += NT) u[d] = fixed[d] ? 0.0 : yb[dof_to_band(I, d)];
+    const double stop = a.tol * a.tol;
+    for (;;) {
+      __syncthreads();
+      apply_k<NT>(I, E, u, q, fixed, true, ke);
+      __syncthreads();
+      double rr = 0.0, bb = 0.0;
+      for (int d = threadIdx.x; d < nd; d += NT) {
+        const double rd = fixed[d] ? 0.0 : b[d] - q[d];
+        r[d] = rd;
+        rr += rd * rd;
+        bb += b[d] * b[d];
+      }
+      block_sum2<NT>(rr, bb, red);
+      if (rr <= stop * bb) break;
+      if (steps == TD_REFINE) { ok = false; break; }
+      ++steps;
+      for (int k = threadIdx.x; k < np; k += NT) yb[k] = k < nd ? r[band_to_dof(I, k)] : 0.0;
+      __syncthreads();
+      for (int K = 0; K < np; K += TD_NB) {
+        band_load_panel<NT>(K, I.bw, RS, Lb, dsm);
+        __syncthreads();
+        band_forward_panel<NT>(K, np, I.bw, RS, dsm, yb, ysm);
+      }
+      band_backward<NT>(np, I.bw, RS, Lb, yb, dsm, tsm);
+      for (int d = threadIdx.x; d < nd; d += NT)
+        if (!fixed[d]) u[d] += yb[dof_to_band(I, d)];
+    }
+  }
+  if (threadIdx.x == 0) {
+    a.direct_ok[idx] = ok ? 1 : 0;
+    a.refine[idx] += steps;
+  }
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT, 1) topo_iteration(TopoArgs a) {
   __shared__ double ke[64];
@@ -446,114 +884,120 @@ __global__ void __launch_bounds__(NT, 1) topo_iteration(TopoArgs a) {
   double* dinv = a.dinv + I.doff;
   double* b = a.b + I.doff;
   const double emin = I.emin, de = I.e0 - I.emin;
+  // solved by topo_direct in this iteration (u and b are set)
+  const bool solved = I.direct && a.direct_ok[idx];
 
   if (a.iter == 0) {  // uniform start (topopt:353), zero initial guess
     for (int e = threadIdx.x; e < ne; e += NT) { x[e] = I.vol_frac; phys[e] = I.vol_frac; }
-    for (int d = threadIdx.x; d < nd; d += NT) u[d] = 0.0;
-    if (threadIdx.x == 0) { a.total_iters[idx] = 0; a.flags[idx] = 0; }
+    if (!solved) {
+      for (int d = threadIdx.x; d < nd; d += NT) u[d] = 0.0;
+      if (threadIdx.x == 0 && !I.direct) { a.total_iters[idx] = 0; a.flags[idx] = 0; }
+    }
   }
   __syncthreads();
   // moduli (assemble, topopt:224)
   for (int e = threadIdx.x; e < ne; e += NT) E[e] = emin + pow(phys[e], I.penal) * de;
   __syncthreads();
-  // Jacobi diagonal of K_FF
-  for (int n = threadIdx.x; n < I.nx * I.ny; n += NT) {
-    const int i = n % I.nx, j = n / I.nx;
-    double d0 = 0.0, d1 = 0.0;
-    for (int dj = -1; dj <= 0; ++dj)
-      for (int di = -1; di <= 0; ++di) {
-        const int ei = i + di, ej = j + dj;
-        if (ei < 0 || ei >= I.nelx || ej < 0 || ej >= I.nely) continue;
-        const int ln = local_node(di, dj);
-        const double Ee = E[ej * I.nelx + ei];
-        d0 += Ee * ke[(2 * ln) * 8 + 2 * ln];
-        d1 += Ee * ke[(2 * ln + 1) * 8 + 2 * ln + 1];
-      }
-    dinv[2 * n] = fixed[2 * n] ? 0.0 : 1.0 / d0;
-    dinv[2 * n + 1] = fixed[2 * n + 1] ? 0.0 : 1.0 / d1;
-  }
-  // right-hand side: b = f_F - K_FD u_D (reduce_system lifting, first bcs value)
-  if (I.has_lift) {
-    apply_k<NT>(I, E, a.ulift + I.doff, q, fixed, false, ke);
-    __syncthreads();
-    for (int d = threadIdx.x; d < nd; d += NT) b[d] = fixed[d] ? 0.0 : f[d] - q[d];
-  } else {
-    for (int d = threadIdx.x; d < nd; d += NT) b[d] = fixed[d] ? 0.0 : f[d];
-  }
-  __syncthreads();
-  // two-level preconditioner (per-instance coarse space): transforms once, A_c^-1 per OC iteration
-  __shared__ double yc[TP_MAXC], uc[TP_MAXC], cm[TP_MAXC];
-  const bool two = a.coarse && I.nc > 0;
-  double* Ac = a.Ac + I.coff;
-  double* Tm = a.Tm + I.toff;
-  if (two) {
-    if (a.iter == 0) coarse_transforms<NT>(I, fixed, Tm);
-    __syncthreads();
-    coarse_assemble_invert<NT>(I, E, fixed, ke, Tm, p, q, Ac, yc);
-  }
-  // r = b - K x0 (warm start), z = M r, p = z
-  apply_k<NT>(I, E, u, q, fixed, true, ke);
-  __syncthreads();
-  double rz = 0.0, rr = 0.0, bb = 0.0;
-  for (int d = threadIdx.x; d < nd; d += NT) {
-    const double rd = b[d] - q[d];
-    r[d] = rd;
-    rr += rd * rd;
-    bb += b[d] * b[d];
-    if (!two) {
-      const double z = dinv[d] * rd;
-      p[d] = z;
-      rz += rd * z;
+  if (!solved) {
+    // Jacobi diagonal of K_FF
+    for (int n = threadIdx.x; n < I.nx * I.ny; n += NT) {
+      const int i = n % I.nx, j = n / I.nx;
+      double d0 = 0.0, d1 = 0.0;
+      for (int dj = -1; dj <= 0; ++dj)
+        for (int di = -1; di <= 0; ++di) {
+          const int ei = i + di, ej = j + dj;
+          if (ei < 0 || ei >= I.nelx || ej < 0 || ej >= I.nely) continue;
+          const int ln = local_node(di, dj);
+          const double Ee = E[ej * I.nelx + ei];
+          d0 += Ee * ke[(2 * ln) * 8 + 2 * ln];
+          d1 += Ee * ke[(2 * ln + 1) * 8 + 2 * ln + 1];
+        }
+      dinv[2 * n] = fixed[2 * n] ? 0.0 : 1.0 / d0;
+      dinv[2 * n + 1] = fixed[2 * n + 1] ? 0.0 : 1.0 / d1;
     }
-  }
-  if (two) {
-    coarse_solve<NT>(I, Tm, Ac, r, yc, uc, cm);
-    rz = two_level_z<NT>(I, r, dinv, cm, p);
-  }
-  block_sum2<NT>(rz, rr, red);
-  bb = block_sum<NT>(bb, red);
-  const double stop = a.tol * a.tol * bb;
-  int it = 0;
-  bool conv = rr <= stop;
-  while (!conv && it < a.max_pcg) {
-    double pq = apply_k<NT>(I, E, p, q, fixed, true, ke);
-    pq = block_sum<NT>(pq, red);
-    if (!(pq > 0.0)) {
-      if (threadIdx.x == 0) atomicOr(a.flags + idx, 2);
-      break;
-    }
-    const double alpha = rz / pq;
-    double rzn = 0.0, rrn = 0.0;
-    for (int d = threadIdx.x; d < nd; d += NT) {
-      u[d] += alpha * p[d];
-      const double rd = r[d] - alpha * q[d];
-      r[d] = rd;
-      if (!two) rzn += rd * dinv[d] * rd;
-      rrn += rd * rd;
-    }
-    block_sum2<NT>(rzn, rrn, red);
-    ++it;
-    conv = rrn <= stop;
-    if (conv) break;
-    if (two) {  // z = D^-1 r + P A_c^-1 P^T r into q
-      coarse_solve<NT>(I, Tm, Ac, r, yc, uc, cm);
-      rzn = two_level_z<NT>(I, r, dinv, cm, q);
-      rzn = block_sum<NT>(rzn, red);
-      const double beta = rzn / rz;
-      rz = rzn;
-      for (int d = threadIdx.x; d < nd; d += NT) p[d] = q[d] + beta * p[d];
+    // right-hand side: b = f_F - K_FD u_D (reduce_system lifting, first bcs value)
+    if (I.has_lift) {
+      apply_k<NT>(I, E, a.ulift + I.doff, q, fixed, false, ke);
+      __syncthreads();
+      for (int d = threadIdx.x; d < nd; d += NT) b[d] = fixed[d] ? 0.0 : f[d] - q[d];
     } else {
-      const double beta = rzn / rz;
-      rz = rzn;
-      for (int d = threadIdx.x; d < nd; d += NT) p[d] = dinv[d] * r[d] + beta * p[d];
+      for (int d = threadIdx.x; d < nd; d += NT) b[d] = fixed[d] ? 0.0 : f[d];
     }
     __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    a.last_iters[idx] = it;
-    a.total_iters[idx] += it;
-    if (!conv) atomicOr(a.flags + idx, 1);
-  }
+    // two-level preconditioner (per-instance coarse space): transforms once, A_c^-1 per OC iteration
+    __shared__ double yc[TP_MAXC], uc[TP_MAXC], cm[TP_MAXC];
+    const bool two = a.coarse && I.nc > 0;
+    double* Ac = a.Ac + I.coff;
+    double* Tm = a.Tm + I.toff;
+    if (two) {
+      if (a.iter == 0) coarse_transforms<NT>(I, fixed, Tm);
+      __syncthreads();
+      coarse_assemble_invert<NT>(I, E, fixed, ke, Tm, p, q, Ac, yc);
+    }
+    // r = b - K x0 (warm start), z = M r, p = z
+    apply_k<NT>(I, E, u, q, fixed, true, ke);
+    __syncthreads();
+    double rz = 0.0, rr = 0.0, bb = 0.0;
+    for (int d = threadIdx.x; d < nd; d += NT) {
+      const double rd = b[d] - q[d];
+      r[d] = rd;
+      rr += rd * rd;
+      bb += b[d] * b[d];
+      if (!two) {
+        const double z = dinv[d] * rd;
+        p[d] = z;
+        rz += rd * z;
+      }
+    }
+    if (two) {
+      coarse_solve<NT>(I, Tm, Ac, r, yc, uc, cm);
+      rz = two_level_z<NT>(I, r, dinv, cm, p);
+    }
+    block_sum2<NT>(rz, rr, red);
+    bb = block_sum<NT>(bb, red);
+    const double stop = a.tol * a.tol * bb;
+    int it = 0;
+    bool conv = rr <= stop;
+    while (!conv && it < a.max_pcg) {
+      double pq = apply_k<NT>(I, E, p, q, fixed, true, ke);
+      pq = block_sum<NT>(pq, red);
+      if (!(pq > 0.0)) {
+        if (threadIdx.x == 0) atomicOr(a.flags + idx, 2);
+        break;
+      }
+      const double alpha = rz / pq;
+      double rzn = 0.0, rrn = 0.0;
+      for (int d = threadIdx.x; d < nd; d += NT) {
+        u[d] += alpha * p[d];
+        const double rd = r[d] - alpha * q[d];
+        r[d] = rd;
+        if (!two) rzn += rd * dinv[d] * rd;
+        rrn += rd * rd;
+      }
+      block_sum2<NT>(rzn, rrn, red);
+      ++it;
+      conv = rrn <= stop;
+      if (conv) break;
+      if (two) {  // z = D^-1 r + P A_c^-1 P^T r into q
+        coarse_solve<NT>(I, Tm, Ac, r, yc, uc, cm);
+        rzn = two_level_z<NT>(I, r, dinv, cm, q);
+        rzn = block_sum<NT>(rzn, red);
+        const double beta = rzn / rz;
+        rz = rzn;
+        for (int d = threadIdx.x; d < nd; d += NT) p[d] = q[d] + beta * p[d];
+      } else {
+        const double beta = rzn / rz;
+        rz = rzn;
+        for (int d = threadIdx.x; d < nd; d += NT) p[d] = dinv[d] * r[d] + beta * p[d];
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      a.last_iters[idx] = it;
+      a.total_iters[idx] += it;
+      if (!conv) atomicOr(a.flags + idx, 1);
+    }
+  }  // !solved
   // compliance c = f . u, u with the fixed dofs' (last) values (topopt:360,368)
   double c = 0.0;
   for (int d = threadIdx.x; d < nd; d += NT) c += f[d] * (fixed[d] ? ufix[d] : u[d]);
@@ -712,6 +1156,11 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
   std::vector<TopoInst> inst(n);
   int64_t eoff = 0, doff = 0, hoff = 0, coff = 0, toff = 0;
   const bool two_level = !(opts && opts->plain_jacobi);
+  const bool allow_direct = !(opts && opts->pcg_only);
+  size_t free_b = 0, total_b = 0;
+  TPT_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const int64_t band_budget = (int64_t)(free_b / 2 / sizeof(double));  // factor storage, in doubles
+  int64_t loff = 0, yoff = 0;
   int launches = 0;
   for (int k = 0; k < n; ++k) {
     const tptfem_topopt_instance& P = in[k];
@@ -730,6 +1179,18 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
     I.h = P.h; I.e0 = P.e0; I.penal = P.penal; I.vol_frac = P.vol_frac; I.radius = P.filter_radius;
     I.move = P.move_limit; I.emin = P.emin;
     element_stiffness_unit(P.nu, P.h, I.ke0);
+    // direct solve when the band fits the kernel's panel and the factor fits the memory budget
+    I.yfast = I.ny <= I.nx;
+    I.bw = 2 * std::min(I.nx, I.ny) + 3;
+    I.npad = (I.ndof + TD_NB - 1) / TD_NB * TD_NB;
+    const int64_t lsize = (int64_t)I.npad * (I.bw + 1);
+    I.direct = allow_direct && I.bw <= TD_MAXBW && loff + lsize <= band_budget;
+    I.loff = loff;
+    I.yoff = yoff;
+    if (I.direct) {
+      loff += lsize;
+      yoff += I.npad;
+    }
     // coarse space: about 48 aggregates of ag x ag nodes (at least 4 x 4)
     I.ag = std::max(4, (int)std::ceil(std::sqrt((double)I.nx * I.ny / 48.0)));
     I.nax = std::max(1, I.nx / I.ag);
@@ -739,7 +1200,7 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
       I.nax = std::max(1, I.nx / I.ag);
       I.nay = std::max(1, I.ny / I.ag);
     }
-    I.nc = two_level ? 3 * I.nax * I.nay : 0;
+    I.nc = two_level && !I.direct ? 3 * I.nax * I.nay : 0;
     I.coff = coff;
     I.toff = toff;
     coff += (int64_t)I.nc * I.nc;
@@ -784,19 +1245,38 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
     }
     for (int d = 0; d < I.ndof; ++d) if (ulift[I.doff + d] != 0.0) I.has_lift = 1;
   }
-  // largest instances first
+  // largest instances first (an instance solved directly costs topo_iteration its filter and OC work only)
   std::vector<int> order(n);
   std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-    return (int64_t)inst[a].ndof * std::max(inst[a].max_iter, 1) > (int64_t)inst[b].ndof * std::max(inst[b].max_iter, 1);
+  auto weight = [&](int k) {
+    return (int64_t)inst[k].ndof * std::max(inst[k].max_iter, 1) * (inst[k].direct ? 1 : 64);
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return weight(a) > weight(b); });
+  // the direct kernel's blocks: largest band work (npad bw^2) first
+  std::vector<int> dorder;
+  int64_t td_smem = 0;
+  for (int k = 0; k < n; ++k)
+    if (inst[k].direct) {
+      dorder.push_back(k);
+      td_smem = std::max(td_smem, td_smem_doubles(inst[k].bw) * (int64_t)sizeof(double));
+    }
+  std::stable_sort(dorder.begin(), dorder.end(), [&](int a, int b) {
+    return (int64_t)inst[a].npad * inst[a].bw * inst[a].bw > (int64_t)inst[b].npad * inst[b].bw * inst[b].bw;
   });
+  const int ndirect = (int)dorder.size();
+  if (ndirect)
+    TPT_CUDA(cudaFuncSetAttribute(topo_direct<TD_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)td_smem));
 
   DevBuf<TopoInst> d_inst;
-  DevBuf<int> d_order, d_last, d_flags;
-  DevBuf<long long> d_total;
+  DevBuf<int> d_order, d_last, d_flags, d_dorder, d_ok;
+  DevBuf<long long> d_total, d_refine;
+  DevBuf<double> dL, dyb;
   DevBuf<double> ex, ephys, eE, eraw, esens, exnew, df, dlift, dfix, du, dr, dp, dq, ddinv, db, dhist, dAc, dTm;
   DevBuf<uint8_t> dfixed;
   d_inst.alloc(n, s); d_order.alloc(n, s); d_last.alloc(n, s); d_flags.alloc(n, s); d_total.alloc(n, s);
+  d_ok.alloc(n, s); d_refine.alloc(n, s); d_dorder.alloc(std::max(ndirect, 1), s);
+  dL.alloc(std::max<int64_t>(loff, 1), s);
+  dyb.alloc(std::max<int64_t>(yoff, 1), s);
   for (auto* v : {&ex, &ephys, &eE, &eraw, &esens, &exnew}) v->alloc(std::max<int64_t>(eoff, 1), s);
   for (auto* v : {&df, &dlift, &dfix, &du, &dr, &dp, &dq, &ddinv, &db}) v->alloc(std::max<int64_t>(doff, 1), s);
   dfixed.alloc(std::max<int64_t>(doff, 1), s);
@@ -809,7 +1289,8 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
   dlift.upload(ulift.data(), doff);
   dfix.upload(ufix.data(), doff);
   dfixed.upload(fixed.data(), doff);
-  d_last.zero(); d_flags.zero(); d_total.zero(); dhist.zero();
+  if (ndirect) d_dorder.upload(dorder.data(), ndirect);
+  d_last.zero(); d_flags.zero(); d_total.zero(); dhist.zero(); d_ok.zero(); d_refine.zero();
 
   TopoArgs a{};
   a.inst = d_inst.p; a.order = d_order.p; a.iter = 0; a.max_pcg = max_pcg; a.tol = tol;
@@ -818,6 +1299,12 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
   a.u = du.p; a.r = dr.p; a.p = dp.p; a.q = dq.p; a.dinv = ddinv.p; a.b = db.p;
   a.hist = dhist.p; a.last_iters = d_last.p; a.total_iters = d_total.p; a.flags = d_flags.p;
   a.Ac = dAc.p; a.Tm = dTm.p; a.coarse = two_level ? 1 : 0;
+  a.dorder = d_dorder.p; a.L = dL.p; a.yb = dyb.p; a.direct_ok = d_ok.p; a.refine = d_refine.p;
+  auto launch_direct = [&]() {
+    if (!ndirect) return;
+    topo_direct<TD_NT><<<ndirect, TD_NT, td_smem, s>>>(a);
+    TPT_CHECK_LAUNCH();
+  };
 
   cudaEvent_t ev0 = ctx->ev[0], ev1 = ctx->ev[1], ev2 = ctx->ev[2];
   float tune_ms = 0.f;
@@ -827,7 +1314,7 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
   uint64_t sig = 1469598103934665603ull;
   for (int k = 0; k < n; ++k)
     for (uint64_t v : {(uint64_t)inst[k].nelx, (uint64_t)inst[k].nely, (uint64_t)inst[k].density_filter,
-                       (uint64_t)inst[k].nc})
+                       (uint64_t)inst[k].nc, (uint64_t)inst[k].direct})
       sig = (sig ^ v) * 1099511628211ull;
   if (!nt) {
     auto it = ctx->topo_tuned.find(sig);
@@ -836,6 +1323,8 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
   if (!nt) {
     float best = 1e30f;
     TPT_CUDA(cudaEventRecord(ev0, s));
+    a.iter = 0;
+    launch_direct();  // the candidates time the remaining work of iteration 0
     for (int cand : {256, 512, 1024}) {
       float ms = 0.f;
       TPT_CUDA(cudaEventRecord(ev1, s));
@@ -860,6 +1349,7 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
     TPT_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < launches; ++k) {
       a.iter = k;
+      launch_direct();
       switch (nt) {
         case 256: topo_iteration<256><<<n, 256, 0, s>>>(a); break;
         case 512: topo_iteration<512><<<n, 512, 0, s>>>(a); break;
@@ -878,6 +1368,7 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
   } else {
     for (int k = 0; k < launches; ++k) {
       a.iter = k;
+      launch_direct();
       launch_nt(nt, n, a, s);
     }
   }
@@ -890,8 +1381,9 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
   // results: reference-mode instances report the design, density-filter ones
   // the physical (filtered) densities
   std::vector<double> hist(std::max<int64_t>(hoff, 1)), xs(std::max<int64_t>(eoff, 1)), ps(std::max<int64_t>(eoff, 1));
-  std::vector<long long> total(n);
+  std::vector<long long> total(n), refine(n);
   std::vector<int> flags(n);
+  d_refine.download(refine.data(), n);
   dhist.download(hist.data(), hoff);
   ex.download(xs.data(), eoff);
   ephys.download(ps.data(), eoff);
@@ -903,15 +1395,17 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
     const std::vector<double>& src = I.density_filter ? ps : xs;
     std::copy(src.begin() + I.eoff, src.begin() + I.eoff + I.ne, densities + I.eoff);
   }
-  long long tot = 0;
+  long long tot = 0, ref = 0;
   int bad = 0;
-  for (int k = 0; k < n; ++k) { tot += total[k]; bad += flags[k] != 0; }
+  for (int k = 0; k < n; ++k) { tot += total[k]; ref += refine[k]; bad += flags[k] != 0; }
   if (stats) {
     stats->total_ms = run_ms;
     stats->tune_ms = tune_ms;
     stats->pcg_iterations = tot;
     stats->block_threads = nt;
     stats->not_converged = bad;
+    stats->refinement_steps = ref;
+    stats->direct_instances = ndirect;
   }
   TPT_REQUIRE(bad == 0, TPTFEM_ERR_NOT_CONVERGED, "topopt: a displacement solve did not converge");
 }

@@ -52,12 +52,13 @@ class TopoptInstance(C.Structure):
 
 class TopoptOpts(C.Structure):
     _fields_ = [("rel_tol", C.c_double), ("max_pcg_iter", C.c_int32), ("block_threads", C.c_int32),
-                ("use_graph", C.c_int32), ("plain_jacobi", C.c_int32)]
+                ("use_graph", C.c_int32), ("plain_jacobi", C.c_int32), ("pcg_only", C.c_int32)]
 
 
 class TopoptStats(C.Structure):
     _fields_ = [("total_ms", C.c_double), ("tune_ms", C.c_double), ("pcg_iterations", C.c_int64),
-                ("block_threads", C.c_int32), ("not_converged", C.c_int32)]
+                ("block_threads", C.c_int32), ("not_converged", C.c_int32), ("refinement_steps", C.c_int64),
+                ("direct_instances", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -84,8 +84,12 @@ def element_stiffness_unit(nu, h):
     return ke.reshape(8, 8)
 
 
-def topopt_batch(ctx, problems, rel_tol=1e-10, max_pcg_iter=0, block_threads=0, use_graph=True, plain_jacobi=False):
+def topopt_batch(ctx, problems, rel_tol=1e-10, max_pcg_iter=0, block_threads=0, use_graph=True, plain_jacobi=False,
+                 pcg_only=False):
     """Run [(TopOptParams, f, bcs), ...] (f/bcs None: cantilever_load) on ctx's GPU.
+
+    Displacement solves: banded Cholesky per instance (grids at most 110 nodes
+    across), PCG otherwise or with pcg_only.
 
     Returns ([TopOptResult, ...], stats dict)."""
     n = len(problems)
@@ -120,7 +124,7 @@ def topopt_batch(ctx, problems, rel_tol=1e-10, max_pcg_iter=0, block_threads=0, 
     comp = np.zeros(ncomp)
     dens = np.zeros(nden)
     opts = N.TopoptOpts(float(rel_tol), int(max_pcg_iter), int(block_threads), int(bool(use_graph)),
-                        int(bool(plain_jacobi)))
+                        int(bool(plain_jacobi)), int(bool(pcg_only)))
     st = N.TopoptStats()
     ctx.check(ctx.lib.tptfem_topopt_batch(ctx.h, C.cast(arr, C.c_void_p), n, C.byref(opts), N.ptr(comp), N.ptr(dens),
                                           C.byref(st)))
