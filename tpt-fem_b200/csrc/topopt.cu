@@ -458,18 +458,54 @@ constexpr int TD_NB = 32;      // panel width
 constexpr int TD_JC = 16;      // earlier columns staged per chunk
 constexpr int TD_MAXBW = 221;  // largest half-bandwidth: the panel's rows + the right-hand-side row in 4 x 4 tiles
 constexpr int TD_RSMAX = 256;  //   (at most TD_RSMAX / 4 row tiles x TD_NB / 4 column tiles = TD_NT threads)
-constexpr int TD_PF = (TD_JC * TD_RSMAX + TD_NT - 1) / TD_NT;  // prefetch registers per thread
+constexpr int TD_NSTAGE = 4;   // chunk buffers: TD_NSTAGE - 1 chunks in flight
 constexpr int TD_REFINE = 4;   // iterative-refinement steps at most
 static_assert((TD_RSMAX / 4) * (TD_NB / 4) <= TD_NT, "panel tiles must fit the block");
 static_assert(TD_NT == 16 * TD_NB, "backward dot products use 16 lanes per panel column");
 
 // rows stored per panel: R = bw + TD_NB matrix rows, the right-hand-side row R, padding to 4
-__host__ __device__ inline int td_rs(int bw) { return (bw + TD_NB + 1 + 3) & ~3; }
+__host__ __device__ inline int td_rs(int bw) { return (bw + TD_NB + 1 + 7) & ~7; }
 __host__ __device__ inline int64_t td_smem_doubles(int bw) {
   const int rs = td_rs(bw);
-  return (int64_t)TD_NB * rs + 2LL * TD_JC * rs + 8LL * rs;
+  return (int64_t)TD_NB * rs + (int64_t)TD_NSTAGE * TD_JC * rs + 8LL * rs;
 }
-static_assert(((TD_MAXBW + TD_NB + 1 + 3) & ~3) <= TD_RSMAX, "TD_MAXBW must fit TD_RSMAX");
+static_assert(((TD_MAXBW + TD_NB + 1 + 7) & ~7) <= TD_RSMAX, "TD_MAXBW must fit TD_RSMAX");
+constexpr int TD_MAXT = (TD_RSMAX / 8) * (TD_NB / 8) / (TD_NT / 32);  // 8 x 8 product tiles per warp
+static_assert((TD_NT / 32) % (TD_NB / 8) == 0, "a warp's product tiles share one column block");
+static_assert(TD_JC == TD_NT / 32, "one staged column per warp and chunk");
+
+// 8-byte asynchronous copy global -> shared (zero-filled when !valid), and its
+// group commit / wait (cp.async, PTX ISA).
+__device__ __forceinline__ void td_cp8(double* sdst, const double* gsrc, bool valid) {
+  const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(gsrc), "r"(valid ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void td_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void td_cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// D = A B + D on one 8 x 8 x 4 FP64 tensor-core tile (mma.sync m8n8k4, PTX ISA
+// fragment layout: lane l holds A(l / 4, l % 4), B(l % 4, l / 4) and
+// D(l / 4, 2 (l % 4) + {0, 1})).
+__device__ __forceinline__ void td_mma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// 1 / x by Newton-Raphson from a single-precision seed (two steps: the seed's
+// 2^-23 relative error squares to below double rounding); x = pivots, which
+// lie well inside the single-precision range (else the plain division).
+__device__ __forceinline__ double td_rcp(double x) {
+  const double ax = fabs(x);
+  if (!(ax > 1e-30 && ax < 1e30)) return 1.0 / x;
+  double r = (double)__frcp_rn((float)x);
+  r = r * (2.0 - x * r);
+  return r * (2.0 - x * r);
+}
 
 __device__ __forceinline__ int band_index(const TopoInst& I, int i, int j, int comp) {
   return 2 * (I.yfast ? i * I.ny + j : j * I.nx + i) + comp;
@@ -491,35 +527,49 @@ __device__ __forceinline__ int dof_to_band(const TopoInst& I, int d) {
 // Entries A(row, k) of band column k for the rows of node (i + di, j + dj),
 // both components, rows >= k, into col[row - K]: the sum over the elements
 // that hold both nodes.  Identity for fixed dofs and padding unknowns k >= ndof
-// (written by the node's own entry, di = dj = 0).
+// (written by the node's own entry, di = dj = 0).  The moduli and fixed flags
+// are all loaded before any is used (one round of memory latency).
 __device__ void band_column_entries(const TopoInst& I, const double* __restrict__ E,
                                     const uint8_t* __restrict__ fixed, const double* __restrict__ ke, int k, int K,
                                     int di, int dj, double* __restrict__ col) {
   const bool self = di == 0 && dj == 0;
-  if (k >= I.ndof) {
-    if (self) col[k - K] = 1.0;
-    return;
-  }
-  const int m = k >> 1, comp = k & 1;
+  const int kk = min(k, I.ndof - 1);
+  const int m = kk >> 1, comp = kk & 1;
   const int i = I.yfast ? m / I.ny : m % I.nx;
   const int j = I.yfast ? m % I.ny : m / I.nx;
-  if (fixed[2 * (j * I.nx + i) + comp]) {
+  const int i2 = i + di, j2 = j + dj;
+  const bool node2 = i2 >= 0 && i2 < I.nx && j2 >= 0 && j2 < I.ny;
+  const int n2 = node2 ? j2 * I.nx + i2 : j * I.nx + i;
+  // the (up to) four elements around node (i, j): origins (i - 1 + a, j - 1 + b)
+  double Ee[4];
+  bool inE[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int ei = i - 1 + (q & 1), ej = j - 1 + (q >> 1);
+    inE[q] = ei >= 0 && ei < I.nelx && ej >= 0 && ej < I.nely;
+    Ee[q] = inE[q] ? E[ej * I.nelx + ei] : 0.0;
+  }
+  const bool fcol = fixed[2 * (j * I.nx + i) + comp];
+  const bool f2[2] = {fixed[2 * n2] != 0, fixed[2 * n2 + 1] != 0};
+  if (k >= I.ndof || fcol) {
     if (self) col[k - K] = 1.0;
     return;
   }
-  const int i2 = i + di, j2 = j + dj;
-  if (i2 < 0 || i2 >= I.nx || j2 < 0 || j2 >= I.ny) return;
+  if (!node2) return;
+#pragma unroll
   for (int c2 = 0; c2 < 2; ++c2) {
     const int row = band_index(I, i2, j2, c2);
-    if (row < k || fixed[2 * (j2 * I.nx + i2) + c2]) continue;
+    if (row < k || f2[c2]) continue;
     double v = 0.0;
-    for (int ej = max(j, j2) - 1; ej <= min(j, j2); ++ej)
-      for (int ei = max(i, i2) - 1; ei <= min(i, i2); ++ei) {
-        if (ei < 0 || ei >= I.nelx || ej < 0 || ej >= I.nely) continue;
-        const int lc = 2 * local_node(ei - i, ej - j) + comp;
-        const int lr = 2 * local_node(ei - i2, ej - j2) + c2;
-        v += E[ej * I.nelx + ei] * ke[lr * 8 + lc];
-      }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int ei = i - 1 + (q & 1), ej = j - 1 + (q >> 1);
+      // element (ei, ej) holds node (i2, j2) too
+      if (!inE[q] || i2 < ei || i2 > ei + 1 || j2 < ej || j2 > ej + 1) continue;
+      const int lc = 2 * local_node(ei - i, ej - j) + comp;
+      const int lr = 2 * local_node(ei - i2, ej - j2) + c2;
+      v += Ee[q] * ke[lr * 8 + lc];
+    }
     col[row - K] = v;
   }
 }
@@ -562,13 +612,35 @@ __device__ void band_forward_panel(int K, int np, int bw, int RS, const double* 
   __syncthreads();
 }
 
-// Backward substitution x = L^-T y over all panels, in place in yb.
+// Backward substitution x = L^-T y over all panels, in place in yb.  The next
+// (lower) panel's L is loaded into registers while the current one is solved.
 template <int NT>
 __device__ void band_backward(int np, int bw, int RS, const double* Lb, double* yb, double* Pa, double* tsm) {
-  const int t = threadIdx.x, R = bw + TD_NB;
+  constexpr int BPF = (TD_NB * TD_RSMAX + NT - 1) / NT;
+  const int t = threadIdx.x, R = bw + TD_NB, ld = bw + 1, nl = TD_NB * RS;
+  const int wc0 = t / RS, wr0 = t - wc0 * RS, wdc = NT / RS, wdr = NT - wdc * RS;
+  double nxt[BPF];
+#define TD_BLOAD(K_)                                                                    \
+  {                                                                                     \
+    int c = wc0, r = wr0;                                                               \
+    _Pragma("unroll") for (int q = 0; q < BPF; ++q) {                                   \
+      nxt[q] = t + q * NT < nl && r >= c && r - c <= bw && r < R                        \
+                   ? Lb[(int64_t)((K_) + c) * ld + (r - c)] : 0.0;                      \
+      c += wdc;                                                                         \
+      r += wdr;                                                                         \
+      if (r >= RS) { r -= RS; ++c; }                                                    \
+    }                                                                                   \
+  }
+#define TD_BSTORE()                                                                     \
+  {                                                                                     \
+    _Pragma("unroll") for (int q = 0; q < BPF; ++q)                                     \
+      if (t + q * NT < nl) Pa[t + q * NT] = nxt[q];                                     \
+  }
+  TD_BLOAD(np - TD_NB);
+  TD_BSTORE();
+  __syncthreads();
   for (int K = np - TD_NB; K >= 0; K -= TD_NB) {
-    band_load_panel<NT>(K, bw, RS, Lb, Pa);
-    __syncthreads();
+    if (K > 0) TD_BLOAD(K - TD_NB);
     {
       const int c = t >> 4, s = t & 15;
       double sum = 0.0;
@@ -589,7 +661,13 @@ __device__ void band_backward(int np, int bw, int RS, const double* Lb, double* 
       yb[K + t] = x;
     }
     __syncthreads();
+    if (K > 0) {
+      TD_BSTORE();
+      __syncthreads();
+    }
   }
+#undef TD_BLOAD
+#undef TD_BSTORE
 }
 
 // Factor K_FF = L L^T into Lb and solve L y = yb in place.  False on a
@@ -601,93 +679,96 @@ __device__ bool band_factor_forward(const TopoInst& I, const double* __restrict_
   const int bw = I.bw, ld = bw + 1, np = I.npad;
   const int R = bw + TD_NB, RS = td_rs(bw);  // row R: right-hand side
   double* Pa = sm;                    // TD_NB x RS, column-major: A of the panel
-  double* Wc = sm + TD_NB * RS;       // 2 x TD_JC x RS: staged earlier columns
-  double* cg = Wc + 2 * TD_JC * RS;   // 4 x RS: the eliminated column group
+  double* Wc = sm + TD_NB * RS;       // TD_NSTAGE x TD_JC x RS: staged earlier columns
+  double* cg = Wc + TD_NSTAGE * TD_JC * RS;  // 4 x RS: the eliminated column group
   double* cgs = cg + 4 * RS;          // 4 x RS: the same, divided by the pivots
   __shared__ double dfac[16], dinv[4];
   const int t = threadIdx.x;
-  const bool act = t < (RS / 4) * (TD_NB / 4);
-  const int tr = t >> 3, tc = t & 7;
+  // elimination tiles, column-tile major: the threads of a warp share their
+  // column tile (one code path per warp in each elimination phase)
+  const int nrt = RS / 4;
+  const bool act = t < nrt * (TD_NB / 4);
+  const int tc = t / nrt, tr = t - tc * nrt;
   const int r0 = 4 * tr, c0 = 4 * tc;
   const int nw = TD_JC * RS;  // staged values per chunk
-  // staged value w = t + q NT sits at column w / RS, row w % RS: stepped without divisions
-  const int wj0 = t / RS, wr0 = t - wj0 * RS, wdj = NT / RS, wdr = NT - wdj * RS;
+  const int lane = t & 31, warp = t >> 5;
+  // Pa is zero at the start of every panel: zeroed here, and each panel's
+  // write-out zeroes the entries it copies (the others are written as zero)
+  for (int q = t; q < TD_NB * RS; q += NT) Pa[q] = 0.0;
+  __syncthreads();
   for (int K = 0; K < np; K += TD_NB) {
-    for (int q = t; q < TD_NB * RS; q += NT) Pa[q] = 0.0;
-    __syncthreads();
+    // S over chunk ch of the earlier columns: staged value w = j * RS + r holds
+    // L(K + r, jlo + ch * TD_JC + j), row R holds y of that column
+    const int jlo = max(0, K - bw), nch = (K - jlo + TD_JC - 1) / TD_JC;
+    // chunk ch: warp w stages column gj = jlo + ch TD_JC + w, its lanes the rows
+    // (L(K + r, gj) sits at Lb[gj ld + K - gj + r] while K + r - gj <= bw)
+#define TD_ISSUE(ch)                                                                    \
+  {                                                                                     \
+    if ((ch) < nch) {                                                                   \
+      const int gj = jlo + (ch) * TD_JC + warp;                                         \
+      double* Wj = Wc + ((ch) % TD_NSTAGE) * nw + warp * RS;                            \
+      const bool live = gj < K;                                                         \
+      const double* col = Lb + (int64_t)gj * ld + (K - gj);                             \
+      const int rmax = bw - (K - gj);                                                   \
+      for (int r = lane; r < RS; r += 32) {                                             \
+        const bool in = live && r <= rmax;                                              \
+        if (r != R) td_cp8(Wj + r, in ? col + r : Lb, in);                              \
+      }                                                                                 \
+      if (lane == 0) td_cp8(Wj + R, live ? yb + gj : Lb, live);                         \
+    }                                                                                   \
+    td_cp_commit();                                                                     \
+  }
+    // S on the tensor cores: warp w owns the 8 x 8 tiles q = w + 16 i (row block
+    // q / 4, column block q % 4 = w % 4), two accumulators per lane and tile
+    const int ntile8 = (RS / 8) * (TD_NB / 8), cb = warp & 3;
+    double s0[TD_MAXT], s1[TD_MAXT];
+#pragma unroll
+    for (int i = 0; i < TD_MAXT; ++i) s0[i] = s1[i] = 0.0;
+#pragma unroll
+    for (int ch = 0; ch < TD_NSTAGE - 1; ++ch) TD_ISSUE(ch);  // in flight during the assembly
     if (t < TD_NB * 9) {
       const int c = t / 9, nb = t - 9 * c;
       band_column_entries(I, E, fixed, ke, K + c, K, nb % 3 - 1, nb / 3 - 1, Pa + c * RS);
       if (nb == 4) Pa[c * RS + R] = yb[K + c];
     }
-    // S over chunk ch of the earlier columns: staged value w = j * RS + r holds
-    // L(K + r, jlo + ch * TD_JC + j), row R holds y of that column
-    const int jlo = max(0, K - bw), nch = (K - jlo + TD_JC - 1) / TD_JC;
-    double pre[TD_PF];
-#define TD_LOAD(ch)                                                                     \
-  {                                                                                     \
-    int gj = jlo + (ch) * TD_JC + wj0, r = wr0;                                         \
-    _Pragma("unroll") for (int q = 0; q < TD_PF; ++q) {                                 \
-      double v = 0.0;                                                                   \
-      const int d = K + r - gj;                                                         \
-      if (t + q * NT < nw && gj < K) {                                                  \
-        if (r == R) v = yb[gj];                                                         \
-        else if (d <= bw) v = Lb[(int64_t)gj * ld + d];                                 \
-      }                                                                                 \
-      pre[q] = v;                                                                       \
-      gj += wdj;                                                                        \
-      r += wdr;                                                                         \
-      if (r >= RS) { r -= RS; ++gj; }                                                   \
-    }                                                                                   \
-  }
-#define TD_STORE(buf)                                                                   \
-  {                                                                                     \
-    double* W_ = Wc + (buf) * nw;                                                       \
-    _Pragma("unroll") for (int q = 0; q < TD_PF; ++q) {                                 \
-      const int w = t + q * NT;                                                         \
-      if (w < nw) W_[w] = pre[q];                                                       \
-    }                                                                                   \
-  }
-    double acc[4][4];
-#pragma unroll
-    for (int a2 = 0; a2 < 4; ++a2)
-#pragma unroll
-      for (int b2 = 0; b2 < 4; ++b2) acc[a2][b2] = 0.0;
-    if (nch > 0) {
-      TD_LOAD(0);
-      TD_STORE(0);
-    }
-    __syncthreads();
-    // a tile's rows are zero in columns below K + r0 - bw (band), except the right-hand-side row
-    const bool rhs_tile = r0 + 3 >= R;
     for (int ch = 0; ch < nch; ++ch) {
-      if (ch + 1 < nch) TD_LOAD(ch + 1);
+      td_cp_wait<TD_NSTAGE - 2>();  // chunk ch has landed (this thread's copies)
+      __syncthreads();               // ... everyone's; chunk ch - 1's buffer is free
+      TD_ISSUE(ch + TD_NSTAGE - 1);
       const int j0 = jlo + ch * TD_JC;
-      const double* W = Wc + (ch & 1) * nw;
-      if (act && (rhs_tile || j0 + TD_JC - 1 >= K + r0 - bw)) {
-#pragma unroll 4
-        for (int j = 0; j < TD_JC; ++j) {
-          const double2 a01 = *reinterpret_cast<const double2*>(W + j * RS + r0);
-          const double2 a23 = *reinterpret_cast<const double2*>(W + j * RS + r0 + 2);
-          const double2 b01 = *reinterpret_cast<const double2*>(W + j * RS + c0);
-          const double2 b23 = *reinterpret_cast<const double2*>(W + j * RS + c0 + 2);
-          const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
+      const double* W = Wc + (ch % TD_NSTAGE) * nw;
 #pragma unroll
-          for (int a2 = 0; a2 < 4; ++a2)
+      for (int ks = 0; ks < TD_JC / 4; ++ks) {
+        const double* Wk = W + (ks * 4 + (lane & 3)) * RS + (lane >> 2);
+        const double bf = Wk[cb * 8];
 #pragma unroll
-            for (int b2 = 0; b2 < 4; ++b2) acc[a2][b2] += av[a2] * bv[b2];
+        for (int i = 0; i < TD_MAXT; ++i) {
+          const int q = warp + (TD_NT / 32) * i, rb = q >> 2;
+          // a row block is zero in columns below K + 8 rb - bw (band), except the right-hand-side row's block
+          if (q < ntile8 && (8 * rb + 7 >= R || j0 + 4 * ks + 3 >= K + 8 * rb - bw))
+            td_mma(s0[i], s1[i], Wk[rb * 8], bf);
         }
       }
-      if (ch + 1 < nch) TD_STORE((ch + 1) & 1);
-      __syncthreads();
     }
-#undef TD_LOAD
-#undef TD_STORE
+    td_cp_wait<0>();
+    __syncthreads();  // also publishes the assembly when there are no chunks
+#undef TD_ISSUE
+    // P = A - S in Pa, then into the 4 x 4 register tiles of the elimination
+#pragma unroll
+    for (int i = 0; i < TD_MAXT; ++i) {
+      const int q = warp + (TD_NT / 32) * i;
+      if (q < ntile8) {
+        const int r = (q >> 2) * 8 + (lane >> 2), c = cb * 8 + 2 * (lane & 3);
+        Pa[c * RS + r] -= s0[i];
+        Pa[(c + 1) * RS + r] -= s1[i];
+      }
+    }
+    __syncthreads();
     double p[4][4];
 #pragma unroll
     for (int a2 = 0; a2 < 4; ++a2)
 #pragma unroll
-      for (int b2 = 0; b2 < 4; ++b2) p[a2][b2] = act ? Pa[(c0 + b2) * RS + r0 + a2] - acc[a2][b2] : 0.0;
+      for (int b2 = 0; b2 < 4; ++b2) p[a2][b2] = act ? Pa[(c0 + b2) * RS + r0 + a2] : 0.0;
     // elimination, column group g = columns 4g .. 4g + 3
     for (int g = 0; g < TD_NB / 4; ++g) {
       if (act && tr == g && tc == g) {  // the diagonal block
@@ -696,7 +777,7 @@ __device__ bool band_factor_forward(const TopoInst& I, const double* __restrict_
         for (int k = 0; k < 4; ++k) {
           const double pv = p[k][k];
           okp = okp && pv > 0.0 && isfinite(pv);
-          const double iv = 1.0 / pv;
+          const double iv = td_rcp(pv);
           dinv[k] = iv;
           piv[4 * g + k] = pv;
 #pragma unroll
@@ -750,19 +831,26 @@ __device__ bool band_factor_forward(const TopoInst& I, const double* __restrict_
     }
     __syncthreads();
     if (*bad) return false;
+    // L = P diag(pivots)^-1/2 into Pa (zero outside the band), y of the panel's unknowns
     if (act) {
 #pragma unroll
       for (int b2 = 0; b2 < 4; ++b2) {
         const int c = c0 + b2;
-        const double sc = 1.0 / sqrt(piv[c]);
+        const double sc = rsqrt(piv[c]);
 #pragma unroll
         for (int a2 = 0; a2 < 4; ++a2) {
           const int r = r0 + a2;
           if (r == R) yb[K + c] = p[a2][b2] * sc;
-          else if (r >= c && r - c <= bw && r < R) Lb[(int64_t)(K + c) * ld + (r - c)] = p[a2][b2] * sc;
+          else if (r < R) Pa[c * RS + r] = r >= c && r - c <= bw ? p[a2][b2] * sc : 0.0;
         }
       }
     }
+    __syncthreads();
+    for (int c = warp; c < TD_NB; c += NT / 32)  // coalesced copy to the band storage
+      for (int d = lane; d <= bw; d += 32) {
+        Lb[(int64_t)(K + c) * ld + d] = Pa[c * RS + c + d];
+        Pa[c * RS + c + d] = 0.0;
+      }
     __syncthreads();
   }
   return true;
