@@ -491,8 +491,9 @@ def run_topopt(args, world, rank, local):
                "config": {"workload": "topopt_batch", "instances": args.instances, "oc_iterations": args.oc_iters,
                           "sizes": "nelx x nely from {60x20, 90x30, 120x40, 180x60, 240x80}",
                           "emin": 1e-9, "filter": "density, R 1.5", "dofs_per_iteration": dofs,
-                          "solver": "two-level PCG per instance (Jacobi + plane rigid-mode aggregation coarse space), FP64, "
-                                    "rel. tol 1e-10, warm start",
+                          "solver": "banded Cholesky per instance (FP64, factor on the FP64 tensor cores, residual "
+                                    "checked and refined to rel. tol 1e-10); two-level PCG for grids too wide for the band",
+                          "direct_instances": st["direct_instances"], "refinement_steps": st["refinement_steps"],
                           "parallelism": f"replicas{world}"},
                "batch_seconds": sec, "tune_ms": st["tune_ms"], "threads_per_instance": st["block_threads"],
                "cpu_baseline": topopt_cpu_baseline(probs, args.oc_iters, sec),

@@ -166,34 +166,59 @@ __device__ double apply_k(const TopoInst& I, const double* __restrict__ E, const
   return dot;
 }
 
-// Sum over the filter window of element e: w = R - d for d <= R (sensitivity
-// filter, topopt:259-279) or w = max(0, rmin - d) (density filter).  The term
-// is val[f] (1 when val is null), divided by div[f] when div is given.
+// Filter weights w = R - d for d <= R (sensitivity filter, topopt:259-279) or
+// w = max(0, R - d) (density filter) between element centres d apart.  The
+// window spans W elements either side; windows up to TP_WMAX use a table of
+// the weights by offset, filled once per instance (negative: outside the
+// sensitivity filter's disc), so the sums need no square roots.
+constexpr int TP_WMAX = 8;
+constexpr int TP_WTAB = (2 * TP_WMAX + 1) * (2 * TP_WMAX + 1);
+
+template <bool SENS>
+__device__ __forceinline__ int filter_halfwidth(const TopoInst& I) {
+  return SENS ? (int)floor(I.radius / I.h) + 1 : (int)ceil(I.radius / I.h);
+}
+
+template <bool SENS>
+__device__ __forceinline__ double filter_weight(const TopoInst& I, double dx, double dy) {
+  const double d2 = dx * dx + dy * dy, R = I.radius;
+  if (SENS) return d2 <= R * R ? R - sqrt(d2) : -1.0;
+  return fmax(0.0, R - sqrt(d2));
+}
+
+template <bool SENS, int NT>
+__device__ void filter_table(const TopoInst& I, double* wt) {
+  const int W = filter_halfwidth<SENS>(I), n = 2 * W + 1;
+  if (W > TP_WMAX) return;
+  for (int q = threadIdx.x; q < n * n; q += NT) {
+    const int oy = q / n - W, ox = q % n - W;
+    wt[q] = filter_weight<SENS>(I, ox * I.h, oy * I.h);
+  }
+}
+
+// Sum over the filter window of element e of w * term, term = val[f] (1 when
+// val is null), divided by div[f] when div is given; den = sum of w.
 template <bool SENS>
 __device__ __forceinline__ void filter_window(const TopoInst& I, int e, const double* __restrict__ val,
-                                              const double* __restrict__ div, double& num, double& den) {
+                                              const double* __restrict__ div, const double* __restrict__ wt,
+                                              double& num, double& den) {
   const int ei = e % I.nelx, ej = e / I.nelx;
-  const double R = I.radius, r2 = R * R, h = I.h;
-  const int w = SENS ? (int)floor(R / h) + 1 : (int)ceil(R / h);
+  const double h = I.h;
+  const int w = filter_halfwidth<SENS>(I), n = 2 * w + 1;
+  const bool tab = w <= TP_WMAX;
   const double cx = ((double)ei + 0.5) * h, cy = ((double)ej + 0.5) * h;
   num = 0.0;
   den = 0.0;
   for (int fj = max(0, ej - w); fj <= min(I.nely - 1, ej + w); ++fj)
     for (int fi = max(0, ei - w); fi <= min(I.nelx - 1, ei + w); ++fi) {
-      const double dx = cx - ((double)fi + 0.5) * h, dy = cy - ((double)fj + 0.5) * h;
-      const double d2 = dx * dx + dy * dy;
+      const double wgt = tab ? wt[(fj - ej + w) * n + (fi - ei + w)]
+                             : filter_weight<SENS>(I, cx - ((double)fi + 0.5) * h, cy - ((double)fj + 0.5) * h);
+      if (SENS && wgt < 0.0) continue;
       const int f = fj * I.nelx + fi;
-      double wt;
-      if (SENS) {
-        if (!(d2 <= r2)) continue;
-        wt = R - sqrt(d2);
-      } else {
-        wt = fmax(0.0, R - sqrt(d2));
-      }
       double term = val ? val[f] : 1.0;
       if (div) term /= div[f];
-      num += wt * term;
-      den += wt;
+      num += wgt * term;
+      den += wgt;
     }
 }
 
@@ -692,6 +717,7 @@ __device__ bool band_factor_forward(const TopoInst& I, const double* __restrict_
   const int r0 = 4 * tr, c0 = 4 * tc;
   const int nw = TD_JC * RS;  // staged values per chunk
   const int lane = t & 31, warp = t >> 5;
+  const int rlast = RS - 8;   // first row of the last row block (holds row R)
   // Pa is zero at the start of every panel: zeroed here, and each panel's
   // write-out zeroes the entries it copies (the others are written as zero)
   for (int q = t; q < TD_NB * RS; q += NT) Pa[q] = 0.0;
@@ -701,7 +727,11 @@ __device__ bool band_factor_forward(const TopoInst& I, const double* __restrict_
     // L(K + r, jlo + ch * TD_JC + j), row R holds y of that column
     const int jlo = max(0, K - bw), nch = (K - jlo + TD_JC - 1) / TD_JC;
     // chunk ch: warp w stages column gj = jlo + ch TD_JC + w, its lanes the rows
-    // (L(K + r, gj) sits at Lb[gj ld + K - gj + r] while K + r - gj <= bw)
+    // (L(K + r, gj) sits at Lb[gj ld + K - gj + r] while r <= rmax = bw - K + gj).
+    // The products read a column's rows only up to rmax + 10 (the row blocks a
+    // 4-column step needs) and the last row block (right-hand side, row R), so
+    // only rows < rmax + 17 and that block are staged (zero beyond the band);
+    // columns past the panel start (gj >= K) are staged as zeros throughout.
 #define TD_ISSUE(ch)                                                                    \
   {                                                                                     \
     if ((ch) < nch) {                                                                   \
@@ -709,18 +739,20 @@ __device__ bool band_factor_forward(const TopoInst& I, const double* __restrict_
       double* Wj = Wc + ((ch) % TD_NSTAGE) * nw + warp * RS;                            \
       const bool live = gj < K;                                                         \
       const double* col = Lb + (int64_t)gj * ld + (K - gj);                             \
-      const int rmax = bw - (K - gj);                                                   \
-      for (int r = lane; r < RS; r += 32) {                                             \
-        const bool in = live && r <= rmax;                                              \
-        if (r != R) td_cp8(Wj + r, in ? col + r : Lb, in);                              \
-      }                                                                                 \
-      if (lane == 0) td_cp8(Wj + R, live ? yb + gj : Lb, live);                         \
+      const int rmax = live ? bw - (K - gj) : -1;                                       \
+      const int rz = live ? min(rmax + 17, rlast) : rlast;                              \
+      for (int r = lane; r < rz; r += 32) td_cp8(Wj + r, r <= rmax ? col + r : Lb, r <= rmax); \
+      if (lane < 8) td_cp8(Wj + rlast + lane, live && rlast + lane == R ? yb + gj : Lb,  \
+                           live && rlast + lane == R);                                  \
     }                                                                                   \
     td_cp_commit();                                                                     \
   }
-    // S on the tensor cores: warp w owns the 8 x 8 tiles q = w + 16 i (row block
-    // q / 4, column block q % 4 = w % 4), two accumulators per lane and tile
-    const int ntile8 = (RS / 8) * (TD_NB / 8), cb = warp & 3;
+    // S on the tensor cores: warp w owns the 8 x 8 tiles i = 0, 1, .. of row block
+    // rb0 + 4 i (rb0 = w / 4) and column block cb = w % 4, two accumulators per
+    // lane and tile
+    const int cb = warp & 3, rb0 = warp >> 2;
+    const int nmine = (RS / 8 - rb0 + 3) >> 2;                           // this warp's tiles
+    const int irhs = ((rlast / 8 - rb0) & 3) == 0 ? (rlast / 8 - rb0) >> 2 : -1;  // its right-hand-side tile
     double s0[TD_MAXT], s1[TD_MAXT];
 #pragma unroll
     for (int i = 0; i < TD_MAXT; ++i) s0[i] = s1[i] = 0.0;
@@ -736,18 +768,22 @@ __device__ bool band_factor_forward(const TopoInst& I, const double* __restrict_
       __syncthreads();               // ... everyone's; chunk ch - 1's buffer is free
       TD_ISSUE(ch + TD_NSTAGE - 1);
       const int j0 = jlo + ch * TD_JC;
-      const double* W = Wc + (ch % TD_NSTAGE) * nw;
+      const double* Wl = Wc + (ch % TD_NSTAGE) * nw + (lane & 3) * RS + (lane >> 2);
+      double bf[TD_JC / 4];
 #pragma unroll
-      for (int ks = 0; ks < TD_JC / 4; ++ks) {
-        const double* Wk = W + (ks * 4 + (lane & 3)) * RS + (lane >> 2);
-        const double bf = Wk[cb * 8];
+      for (int ks = 0; ks < TD_JC / 4; ++ks) bf[ks] = Wl[ks * 4 * RS + cb * 8];
+      // row block rb is zero in columns below K + 8 rb - bw (band): tile i needs the
+      // 4-column steps ks >= kmin0 + 8 i (all of them for the right-hand-side tile)
+      const int kmin0 = (K + 8 * rb0 - bw - j0) >> 2;  // ceil((K + 8 rb0 - bw - j0 - 3) / 4)
 #pragma unroll
-        for (int i = 0; i < TD_MAXT; ++i) {
-          const int q = warp + (TD_NT / 32) * i, rb = q >> 2;
-          // a row block is zero in columns below K + 8 rb - bw (band), except the right-hand-side row's block
-          if (q < ntile8 && (8 * rb + 7 >= R || j0 + 4 * ks + 3 >= K + 8 * rb - bw))
-            td_mma(s0[i], s1[i], Wk[rb * 8], bf);
-        }
+      for (int i = 0; i < TD_MAXT; ++i) {
+        if (i >= nmine) break;
+        const int km = i == irhs ? 0 : kmin0 + 8 * i;
+        if (km > TD_JC / 4 - 1) continue;
+        const double* Wi = Wl + (rb0 + 4 * i) * 8;
+#pragma unroll
+        for (int ks = 0; ks < TD_JC / 4; ++ks)
+          if (ks >= km) td_mma(s0[i], s1[i], Wi[ks * 4 * RS], bf[ks]);
       }
     }
     td_cp_wait<0>();
@@ -756,9 +792,8 @@ __device__ bool band_factor_forward(const TopoInst& I, const double* __restrict_
     // P = A - S in Pa, then into the 4 x 4 register tiles of the elimination
 #pragma unroll
     for (int i = 0; i < TD_MAXT; ++i) {
-      const int q = warp + (TD_NT / 32) * i;
-      if (q < ntile8) {
-        const int r = (q >> 2) * 8 + (lane >> 2), c = cb * 8 + 2 * (lane & 3);
+      if (i < nmine) {
+        const int r = (rb0 + 4 * i) * 8 + (lane >> 2), c = cb * 8 + 2 * (lane & 3);
         Pa[c * RS + r] -= s0[i];
         Pa[(c + 1) * RS + r] -= s1[i];
       }
@@ -1095,6 +1130,10 @@ __global__ void __launch_bounds__(NT, 1) topo_iteration(TopoArgs a) {
     if (I.max_iter > 0) a.hist[I.hoff + a.iter + 1] = c;
   }
   if (I.max_iter == 0) return;  // the initial solve only (topopt:356-360)
+  __shared__ double wtab[TP_WTAB];
+  if (I.density_filter) filter_table<false, NT>(I, wtab);
+  else filter_table<true, NT>(I, wtab);
+  __syncthreads();
   // raw sensitivity (topopt:371-375), element_quad_form (topopt:241-254)
   for (int e = threadIdx.x; e < ne; e += NT) {
     const int ei = e % I.nelx, ej = e / I.nelx;
@@ -1120,7 +1159,7 @@ __global__ void __launch_bounds__(NT, 1) topo_iteration(TopoArgs a) {
     // filter_sensitivity (topopt:259-279), then oc_update (topopt:284-331)
     for (int e = threadIdx.x; e < ne; e += NT) {
       double num, den;
-      filter_window<true>(I, e, raw, nullptr, num, den);
+      filter_window<true>(I, e, raw, nullptr, wtab, num, den);
       sens[e] = den > 0.0 ? num / den : raw[e];
     }
     __syncthreads();
@@ -1144,19 +1183,19 @@ __global__ void __launch_bounds__(NT, 1) topo_iteration(TopoArgs a) {
     // E (free until the next launch) holds Hs, sens = dc, raw = dv.
     for (int e = threadIdx.x; e < ne; e += NT) {
       double num, den;
-      filter_window<false>(I, e, nullptr, nullptr, num, den);
+      filter_window<false>(I, e, nullptr, nullptr, wtab, num, den);
       E[e] = den;
     }
     __syncthreads();
     for (int e = threadIdx.x; e < ne; e += NT) {
       double num, den;
-      filter_window<false>(I, e, raw, E, num, den);
+      filter_window<false>(I, e, raw, E, wtab, num, den);
       sens[e] = num;
     }
     __syncthreads();
     for (int e = threadIdx.x; e < ne; e += NT) {
       double num, den;
-      filter_window<false>(I, e, nullptr, E, num, den);
+      filter_window<false>(I, e, nullptr, E, wtab, num, den);
       raw[e] = num;
     }
     __syncthreads();
@@ -1172,7 +1211,7 @@ __global__ void __launch_bounds__(NT, 1) topo_iteration(TopoArgs a) {
       double s = 0.0;
       for (int e = threadIdx.x; e < ne; e += NT) {
         double num, den;
-        filter_window<false>(I, e, xnew, nullptr, num, den);
+        filter_window<false>(I, e, xnew, nullptr, wtab, num, den);
         const double v = num / E[e];
         phys[e] = v;
         s += v;
