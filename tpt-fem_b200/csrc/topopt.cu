@@ -490,9 +490,12 @@ static_assert(TD_NT == 16 * TD_NB, "backward dot products use 16 lanes per panel
 
 // rows stored per panel: R = bw + TD_NB matrix rows, the right-hand-side row R, padding to 4
 __host__ __device__ inline int td_rs(int bw) { return (bw + TD_NB + 1 + 7) & ~7; }
+// column-group buffers: row r at (r / 4) * 6 + r % 4 (two padding doubles per
+// four rows), so the 4-row tiles of consecutive threads fall in distinct banks
+__host__ __device__ inline int td_cs(int rs) { return rs / 4 * 6; }
 __host__ __device__ inline int64_t td_smem_doubles(int bw) {
   const int rs = td_rs(bw);
-  return (int64_t)TD_NB * rs + (int64_t)TD_NSTAGE * TD_JC * rs + 8LL * rs;
+  return (int64_t)TD_NB * rs + (int64_t)TD_NSTAGE * TD_JC * rs + 8LL * td_cs(rs);
 }
 static_assert(((TD_MAXBW + TD_NB + 1 + 7) & ~7) <= TD_RSMAX, "TD_MAXBW must fit TD_RSMAX");
 constexpr int TD_MAXT = (TD_RSMAX / 8) * (TD_NB / 8) / (TD_NT / 32);  // 8 x 8 product tiles per warp
@@ -705,8 +708,9 @@ __device__ bool band_factor_forward(const TopoInst& I, const double* __restrict_
   const int R = bw + TD_NB, RS = td_rs(bw);  // row R: right-hand side
   double* Pa = sm;                    // TD_NB x RS, column-major: A of the panel
   double* Wc = sm + TD_NB * RS;       // TD_NSTAGE x TD_JC x RS: staged earlier columns
-  double* cg = Wc + TD_NSTAGE * TD_JC * RS;  // 4 x RS: the eliminated column group
-  double* cgs = cg + 4 * RS;          // 4 x RS: the same, divided by the pivots
+  const int CS = td_cs(RS);
+  double* cg = Wc + TD_NSTAGE * TD_JC * RS;  // 4 x CS: the eliminated column group (padded rows)
+  double* cgs = cg + 4 * CS;                 // 4 x CS: the same, divided by the pivots
   __shared__ double dfac[16], dinv[4];
   const int t = threadIdx.x;
   // elimination tiles, column-tile major: the threads of a warp share their
@@ -801,9 +805,14 @@ __device__ bool band_factor_forward(const TopoInst& I, const double* __restrict_
     __syncthreads();
     double p[4][4];
 #pragma unroll
-    for (int a2 = 0; a2 < 4; ++a2)
-#pragma unroll
-      for (int b2 = 0; b2 < 4; ++b2) p[a2][b2] = act ? Pa[(c0 + b2) * RS + r0 + a2] : 0.0;
+    for (int b2 = 0; b2 < 4; ++b2) {
+      double2 v01 = make_double2(0.0, 0.0), v23 = v01;
+      if (act) {
+        v01 = *reinterpret_cast<const double2*>(Pa + (c0 + b2) * RS + r0);
+        v23 = *reinterpret_cast<const double2*>(Pa + (c0 + b2) * RS + r0 + 2);
+      }
+      p[0][b2] = v01.x; p[1][b2] = v01.y; p[2][b2] = v23.x; p[3][b2] = v23.y;
+    }
     // elimination, column group g = columns 4g .. 4g + 3
     for (int g = 0; g < TD_NB / 4; ++g) {
       if (act && tr == g && tc == g) {  // the diagonal block
@@ -840,23 +849,25 @@ __device__ bool band_factor_forward(const TopoInst& I, const double* __restrict_
               for (int a2 = 0; a2 < 4; ++a2) p[a2][c2] -= p[a2][k] * f;
             }
         }
+        const int o6 = 6 * tr;  // padded position of row r0
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-#pragma unroll
-          for (int a2 = 0; a2 < 4; ++a2) {
-            cg[k * RS + r0 + a2] = p[a2][k];
-            cgs[k * RS + r0 + a2] = p[a2][k] * dinv[k];
-          }
+        for (int k = 0; k < 4; ++k) {
+          const double ivk = dinv[k];
+          *reinterpret_cast<double2*>(cg + k * CS + o6) = make_double2(p[0][k], p[1][k]);
+          *reinterpret_cast<double2*>(cg + k * CS + o6 + 2) = make_double2(p[2][k], p[3][k]);
+          *reinterpret_cast<double2*>(cgs + k * CS + o6) = make_double2(p[0][k] * ivk, p[1][k] * ivk);
+          *reinterpret_cast<double2*>(cgs + k * CS + o6 + 2) = make_double2(p[2][k] * ivk, p[3][k] * ivk);
+        }
       }
       __syncthreads();
       if (act && tc > g) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-          double l[4], f[4];
-#pragma unroll
-          for (int a2 = 0; a2 < 4; ++a2) l[a2] = cg[k * RS + r0 + a2];
-#pragma unroll
-          for (int b2 = 0; b2 < 4; ++b2) f[b2] = cgs[k * RS + c0 + b2];
+          const double2 l01 = *reinterpret_cast<const double2*>(cg + k * CS + 6 * tr);
+          const double2 l23 = *reinterpret_cast<const double2*>(cg + k * CS + 6 * tr + 2);
+          const double2 f01 = *reinterpret_cast<const double2*>(cgs + k * CS + 6 * tc);
+          const double2 f23 = *reinterpret_cast<const double2*>(cgs + k * CS + 6 * tc + 2);
+          const double l[4] = {l01.x, l01.y, l23.x, l23.y}, f[4] = {f01.x, f01.y, f23.x, f23.y};
 #pragma unroll
           for (int a2 = 0; a2 < 4; ++a2)
 #pragma unroll
@@ -867,17 +878,20 @@ __device__ bool band_factor_forward(const TopoInst& I, const double* __restrict_
     __syncthreads();
     if (*bad) return false;
     // L = P diag(pivots)^-1/2 into Pa (zero outside the band), y of the panel's unknowns
-    if (act) {
+    if (act) {  // rows past R stay zero; row R's entry is rewritten by the next assembly
 #pragma unroll
       for (int b2 = 0; b2 < 4; ++b2) {
         const int c = c0 + b2;
         const double sc = rsqrt(piv[c]);
+        double v[4];
 #pragma unroll
         for (int a2 = 0; a2 < 4; ++a2) {
           const int r = r0 + a2;
+          v[a2] = r >= c && r - c <= bw && r < R ? p[a2][b2] * sc : 0.0;
           if (r == R) yb[K + c] = p[a2][b2] * sc;
-          else if (r < R) Pa[c * RS + r] = r >= c && r - c <= bw ? p[a2][b2] * sc : 0.0;
         }
+        *reinterpret_cast<double2*>(Pa + c * RS + r0) = make_double2(v[0], v[1]);
+        *reinterpret_cast<double2*>(Pa + c * RS + r0 + 2) = make_double2(v[2], v[3]);
       }
     }
     __syncthreads();
