@@ -640,35 +640,38 @@ __device__ void band_forward_panel(int K, int np, int bw, int RS, const double* 
   __syncthreads();
 }
 
-// Backward substitution x = L^-T y over all panels, in place in yb.  The next
-// (lower) panel's L is loaded into registers while the current one is solved.
+// Backward substitution x = L^-T y over all panels, in place in yb.  The
+// panels stream from the band storage through three shared-memory buffers
+// (sm, sm + TD_NB RS, sm + 2 TD_NB RS) by cp.async, two panels ahead.
 template <int NT>
-__device__ void band_backward(int np, int bw, int RS, const double* Lb, double* yb, double* Pa, double* tsm) {
-  constexpr int BPF = (TD_NB * TD_RSMAX + NT - 1) / NT;
+__device__ void band_backward(int np, int bw, int RS, const double* Lb, double* yb, double* sm, double* tsm) {
   const int t = threadIdx.x, R = bw + TD_NB, ld = bw + 1, nl = TD_NB * RS;
   const int wc0 = t / RS, wr0 = t - wc0 * RS, wdc = NT / RS, wdr = NT - wdc * RS;
-  double nxt[BPF];
-#define TD_BLOAD(K_)                                                                    \
-  {                                                                                     \
-    int c = wc0, r = wr0;                                                               \
-    _Pragma("unroll") for (int q = 0; q < BPF; ++q) {                                   \
-      nxt[q] = t + q * NT < nl && r >= c && r - c <= bw && r < R                        \
-                   ? Lb[(int64_t)((K_) + c) * ld + (r - c)] : 0.0;                      \
-      c += wdc;                                                                         \
-      r += wdr;                                                                         \
-      if (r >= RS) { r -= RS; ++c; }                                                    \
-    }                                                                                   \
-  }
-#define TD_BSTORE()                                                                     \
-  {                                                                                     \
-    _Pragma("unroll") for (int q = 0; q < BPF; ++q)                                     \
-      if (t + q * NT < nl) Pa[t + q * NT] = nxt[q];                                     \
-  }
-  TD_BLOAD(np - TD_NB);
-  TD_BSTORE();
-  __syncthreads();
-  for (int K = np - TD_NB; K >= 0; K -= TD_NB) {
-    if (K > 0) TD_BLOAD(K - TD_NB);
+  const int npan = np / TD_NB;
+  // panel p (from the last) into buffer p % 3: value w = c * RS + r holds L(K + r, K + c)
+  auto issue = [&](int pp) {
+    if (pp < npan) {
+      const int K = np - TD_NB * (pp + 1);
+      double* B = sm + (pp % 3) * nl;
+      int c = wc0, r = wr0;
+      for (int w = t; w < nl; w += NT) {
+        const bool in = r >= c && r - c <= bw && r < R;
+        td_cp8(B + w, in ? Lb + (int64_t)(K + c) * ld + (r - c) : Lb, in);
+        c += wdc;
+        r += wdr;
+        if (r >= RS) { r -= RS; ++c; }
+      }
+    }
+    td_cp_commit();
+  };
+  issue(0);
+  issue(1);
+  for (int pp = 0; pp < npan; ++pp) {
+    td_cp_wait<1>();
+    __syncthreads();  // panel pp has landed everywhere; buffer (pp + 2) % 3 is free
+    issue(pp + 2);
+    const int K = np - TD_NB * (pp + 1);
+    const double* Pa = sm + (pp % 3) * nl;
     {
       const int c = t >> 4, s = t & 15;
       double sum = 0.0;
@@ -688,14 +691,9 @@ __device__ void band_backward(int np, int bw, int RS, const double* Lb, double* 
       }
       yb[K + t] = x;
     }
-    __syncthreads();
-    if (K > 0) {
-      TD_BSTORE();
-      __syncthreads();
-    }
   }
-#undef TD_BLOAD
-#undef TD_BSTORE
+  td_cp_wait<0>();
+  __syncthreads();
 }
 
 // Factor K_FF = L L^T into Lb and solve L y = yb in place.  False on a
