@@ -161,3 +161,16 @@ def test_wide_grids_fall_back_to_pcg_in_the_same_batch(ctx):
     single, _ = T.topopt_batch(ctx, [probs[1]], rel_tol=1e-10)
     assert np.max(np.abs(single[0].compliance - res[1].compliance) / res[1].compliance) < 1e-12
     check_against_oracle(res[1], *probs[1])
+
+
+def test_largest_configuration_grid_direct_matches_pcg(ctx):
+    # the configuration's largest grid (240 x 80 elements, 39,042 dofs, half-bandwidth 165):
+    # banded Cholesky without refinement against two-level PCG, both to 1e-11
+    P = params(240, 80, 0.4, 1.5, 3, emin=1e-9, density_filter=True)
+    f, bcs = T.cantilever_load(P.grid, node=P.grid.nx * (P.grid.nely // 2) + P.grid.nelx)
+    d, std = T.topopt_batch(ctx, [(P, f, bcs)], rel_tol=1e-11)
+    p, stp = T.topopt_batch(ctx, [(P, f, bcs)], rel_tol=1e-11, pcg_only=True)
+    assert std["direct_instances"] == 1 and std["refinement_steps"] == 0 and std["not_converged"] == 0
+    assert stp["direct_instances"] == 0 and stp["not_converged"] == 0
+    assert np.max(np.abs(d[0].compliance - p[0].compliance) / p[0].compliance) < 1e-9
+    assert np.max(np.abs(d[0].densities - p[0].densities)) < 1e-7
