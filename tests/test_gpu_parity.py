@@ -374,3 +374,27 @@ def test_not_spd_and_not_converged_are_reported(ctx):
     # the context stays usable after every error
     u, st = F.solve_with_dirichlet(K, rhs, bcs)
     assert st["rel_residual"] <= 1e-10
+
+
+@pytest.mark.parametrize("dim", [3, 1])
+def test_factor_pattern_from_group_adjacency_matches_row_union(ctx, dim):
+    # With the node-block operator built (every free node has all dofs free), the
+    # factor pattern comes from its group adjacency; without it, from a sorted
+    # union per row.  Both must give the same rows, columns and values.
+    c, e = box([6, 4, 3], mx=(2.0, 1.0, 1.0))
+    c = jitter(c, 0.03, 61)
+    coef = np.random.default_rng(62).uniform(0.05, 1.0, len(e))
+    m = F.Mesh.from_arrays(F.CELL_TET4, c, e, ctx=ctx)
+    if dim == 3:
+        K = F.assemble_elasticity(m, "3d", coef, 0.3, 2)
+        bcs = [(3 * n + k, 0.0) for n in O.nodes_on_plane(c, 0, 0.0, 1e-9) for k in range(3)]
+    else:
+        K = F.assemble_poisson(m, coef, 2)
+        bcs = unit_cube_bcs(c)
+    rows = F.reduce_system(K, np.ones(K.nrows), bcs)
+    rp1, ci1, va1, s1 = rows.fsai()
+    groups = F.reduce_system(K, np.ones(K.nrows), bcs)
+    groups.solve(solver=F.SOLVER_JACOBI_PCG, tol=1e-8)  # builds the node-block operator first
+    rp2, ci2, va2, s2 = groups.fsai()
+    assert np.array_equal(rp1, rp2) and np.array_equal(ci1, ci2)
+    assert np.array_equal(va1, va2) and np.array_equal(s1, s2)

@@ -67,6 +67,37 @@ __global__ void nb_lower_pattern(int n, int dpn, const int* __restrict__ rp, con
   }
 }
 
+// The same pattern from the node-group adjacency (sorted neighbour groups of
+// each group, the union over its dofs' rows), valid when every free node has
+// all its dofs free, so that reduced dof = group * dpn + component: row
+// i = g dpn + a holds every component of the neighbour groups J < g, then the
+// node's own components c < a.  Same rows, order and overflow rule as
+// nb_lower_pattern.
+template <bool FILL>
+__global__ void nb_lower_from_groups(int n, int dpn, const int* __restrict__ gptr, const int* __restrict__ glist,
+                                     int* __restrict__ cnt, const int* __restrict__ lrp, int* __restrict__ lci,
+                                     int* __restrict__ flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int g = i / dpn, a = i - g * dpn;
+  int nlow = 0;
+  for (int k = gptr[g]; k < gptr[g + 1] && glist[k] < g; ++k) ++nlow;
+  const int len = nlow * dpn + a;
+  if (len >= FSAI_MAXM) {
+    atomicOr(flag, 1);
+    if (!FILL) cnt[i] = 0;
+    return;
+  }
+  if (!FILL) {
+    cnt[i] = len;
+  } else {
+    int* out = lci + lrp[i];
+    for (int k = gptr[g]; k < gptr[g] + nlow; ++k)
+      for (int c = 0; c < dpn; ++c) *out++ = glist[k] * dpn + c;
+    for (int c = 0; c < a; ++c) *out++ = g * dpn + c;
+  }
+}
+
 __global__ void col_counts(int64_t nnz, const int* __restrict__ gci, int* __restrict__ cnt) {
   int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k < nnz) atomicAdd(&cnt[gci[k]], 1);
@@ -224,8 +255,15 @@ void fsai_build_pattern(const SystemData& S, FsaiFactor& F) {
   DevBuf<int> cnt;
   cnt.alloc(n + 1, s);
   TPT_CUDA(cudaMemsetAsync(S.ctx->d_flag, 0, sizeof(int), s));
-  nb_lower_pattern<false><<<ceil_div(n, 128), 128, 0, s>>>(n, S.dpn, S.row_ptr.p, S.col.p, S.free_map.p,
-                                                            S.red_map.p, cnt.p, nullptr, nullptr, S.ctx->d_flag);
+  // from the node-group adjacency when the node-block operator exists (one pass
+  // over each group's neighbour list instead of a sorted union per row)
+  const bool groups = S.nb.state == 1 && S.nb.dpn == S.dpn;
+  if (groups)
+    nb_lower_from_groups<false><<<ceil_div(n, 256), 256, 0, s>>>(n, S.dpn, S.nb.gptr.p, S.nb.glist.p, cnt.p, nullptr,
+                                                                 nullptr, S.ctx->d_flag);
+  else
+    nb_lower_pattern<false><<<ceil_div(n, 128), 128, 0, s>>>(n, S.dpn, S.row_ptr.p, S.col.p, S.free_map.p,
+                                                              S.red_map.p, cnt.p, nullptr, nullptr, S.ctx->d_flag);
   TPT_CHECK_LAUNCH();
   F.rp.alloc(n + 1, s);
   F.nnz = exclusive_scan_i32(cnt.p, F.rp.p, n, s);
@@ -234,8 +272,12 @@ void fsai_build_pattern(const SystemData& S, FsaiFactor& F) {
   TPT_CUDA(cudaStreamSynchronize(s));
   F.overflow = flag != 0;
   F.ci.alloc(F.nnz, s);
-  nb_lower_pattern<true><<<ceil_div(n, 128), 128, 0, s>>>(n, S.dpn, S.row_ptr.p, S.col.p, S.free_map.p,
-                                                           S.red_map.p, nullptr, F.rp.p, F.ci.p, S.ctx->d_flag);
+  if (groups)
+    nb_lower_from_groups<true><<<ceil_div(n, 256), 256, 0, s>>>(n, S.dpn, S.nb.gptr.p, S.nb.glist.p, nullptr, F.rp.p,
+                                                                F.ci.p, S.ctx->d_flag);
+  else
+    nb_lower_pattern<true><<<ceil_div(n, 128), 128, 0, s>>>(n, S.dpn, S.row_ptr.p, S.col.p, S.free_map.p,
+                                                             S.red_map.p, nullptr, F.rp.p, F.ci.p, S.ctx->d_flag);
   TPT_CHECK_LAUNCH();
   F.sigma2.alloc(n, s);
   F.va.alloc(F.nnz, s);

@@ -484,6 +484,9 @@ bool learned_factor(SystemData& S, SolverWork& W) {
   cudaStream_t s = S.ctx->stream;
   {
     PhaseTimer t(S.ctx->stream, "factor pattern");
+    // the network inputs build the node-block operator anyway; with it the
+    // factor pattern comes from its group adjacency
+    if (S.dpn <= 3) nb_build_operator(S);
     fsai_build_pattern(S, W.lf);
   }
   if (W.lf.overflow) return false;
