@@ -153,6 +153,31 @@ __global__ void boundary_face_mask(const int* __restrict__ conn, int cell, int n
                                    const int* __restrict__ ne, int64_t n_elems, unsigned char* __restrict__ mask) {
   int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n_elems) return;
+  if (cell == TPTFEM_CELL_TET4) {
+    // Faces 1..3 (opposite vertices 1..3) contain vertex 0: one scan of vertex
+    // 0's incident elements serves all three; face 0 = (1, 2, 3) scans vertex
+    // 1's.  A face is interior iff another element holds its three vertices.
+    const int4 me = reinterpret_cast<const int4*>(conn)[e];
+    auto holds = [](const int4& c, int v) { return c.x == v || c.y == v || c.z == v || c.w == v; };
+    bool sh1 = false, sh2 = false, sh3 = false, sh0 = false;
+    for (int k = ne_ptr[me.x]; k < ne_ptr[me.x + 1]; ++k) {
+      const int o = ne[k] >> 2;
+      if (o == (int)e) continue;
+      const int4 c = reinterpret_cast<const int4*>(conn)[o];
+      const bool h1 = holds(c, me.y), h2 = holds(c, me.z), h3 = holds(c, me.w);
+      sh1 |= h2 && h3;
+      sh2 |= h1 && h3;
+      sh3 |= h1 && h2;
+    }
+    for (int k = ne_ptr[me.y]; k < ne_ptr[me.y + 1] && !sh0; ++k) {
+      const int o = ne[k] >> 2;
+      if (o == (int)e) continue;
+      const int4 c = reinterpret_cast<const int4*>(conn)[o];
+      sh0 = holds(c, me.z) && holds(c, me.w);
+    }
+    mask[e] = (unsigned char)((sh0 ? 0 : 1) | (sh1 ? 0 : 2) | (sh2 ? 0 : 4) | (sh3 ? 0 : 8));
+    return;
+  }
   const int tet_f[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
   const int quad_f[4][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}};
   const int tri_f[3][2] = {{1, 2}, {2, 0}, {0, 1}};
