@@ -132,6 +132,14 @@ tptfem_status tptfem_create(int device, tptfem_context** out) {
     TPT_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
     uint64_t keep = UINT64_MAX;
     TPT_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    // the dense-library handles of the coarse-space set-up, created with the
+    // context (their creation takes milliseconds) rather than inside a solve
+    cusolverDnHandle_t hs = nullptr;
+    TPT_REQUIRE(cusolverDnCreate(&hs) == CUSOLVER_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "cusolverDnCreate failed");
+    ctx->cusolver = hs;
+    cublasHandle_t hb = nullptr;
+    TPT_REQUIRE(cublasCreate(&hb) == CUBLAS_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "cublasCreate failed");
+    ctx->cublas = hb;
   } catch (const Error& e) {
     tptfem_destroy(ctx);
     return e.status;

@@ -15,6 +15,7 @@
 // dpotrf, cuBLAS dtrsm and dsyrk), and kept as an explicit FP32 inverse, so each iteration adds one restriction, one coarse mat-vec
 // and a prolongation that is fused into the FSAI transpose kernel.
 // Requires the node-block layout (full node groups) and the mesh geometry.
+#include <cub/device/device_radix_sort.cuh>
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 
@@ -208,6 +209,14 @@ __global__ void cs_raw(int na, int nm, const double* __restrict__ T, const doubl
   double x = 0.0;
   for (int m = 0; m < nm; ++m) x += tI[m] * uc[(int64_t)I * nm + m];
   cm[t] = x;
+}
+
+// gid[g] = g and the group count of every aggregate (input of the group-list sort).
+__global__ void cs_iota_count(int ngroups, const int* __restrict__ agg, int* __restrict__ gid, int* __restrict__ cnt) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  gid[g] = g;
+  atomicAdd(&cnt[agg[g]], 1);
 }
 
 __global__ void cs_group_colour(int ngroups, const int* __restrict__ agg, const int* __restrict__ abin,
@@ -529,18 +538,33 @@ bool coarse_build(SystemData& S, int target) {
     }
   }
   if (!ok) return false;
-  // aggregate of every group; its group list by a stable counting sort (host)
+  // aggregate of every group; the groups of each aggregate in ascending order
+  // by a stable radix sort of (aggregate, group) on the device, and the
+  // aggregates' offsets from their counts
   C.agg.alloc(ng, s);
   cs_group_agg<<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, binid.p, C.bin2agg.p, C.agg.p);
   TPT_CHECK_LAUNCH();
-  std::vector<int> agg(ng), aptr(na + 1, 0), alist(ng);
-  C.agg.download(agg.data(), ng);
-  TPT_CUDA(cudaStreamSynchronize(s));
-  for (int g = 0; g < ng; ++g) aptr[agg[g] + 1]++;
-  for (int i = 0; i < na; ++i) aptr[i + 1] += aptr[i];
+  std::vector<int> aptr(na + 1, 0);
+  C.alist.alloc(ng, s);
   {
-    std::vector<int> fill(aptr.begin(), aptr.end() - 1);
-    for (int g = 0; g < ng; ++g) alist[fill[agg[g]]++] = g;
+    DevBuf<int> gid, skey, acnt;
+    gid.alloc(ng, s);
+    skey.alloc(ng, s);
+    acnt.alloc(na + 1, s);
+    acnt.zero();
+    cs_iota_count<<<blocks_for(ng), CS_THREADS, 0, s>>>(ng, C.agg.p, gid.p, acnt.p);
+    TPT_CHECK_LAUNCH();
+    int bits = 1;
+    while ((1 << bits) < na) ++bits;
+    size_t tmp_bytes = 0;
+    TPT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, C.agg.p, skey.p, gid.p, C.alist.p, ng, 0, bits, s));
+    DevBuf<unsigned char> tmp;
+    tmp.alloc(std::max<size_t>(tmp_bytes, 1), s);
+    TPT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, C.agg.p, skey.p, gid.p, C.alist.p, ng, 0, bits, s));
+    std::vector<int> cnt(na);
+    acnt.download(cnt.data(), na);
+    TPT_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < na; ++i) aptr[i + 1] = aptr[i] + cnt[i];
   }
   constexpr int CS_SEG = 1024;  // segments of at most CS_SEG groups (restriction work items)
   std::vector<int> sb, se, aseg(na + 1, 0);
@@ -556,7 +580,6 @@ bool coarse_build(SystemData& S, int target) {
   C.nc = na * nm;
   C.nseg = (int)sb.size();
   C.aptr.alloc(na + 1, s); C.aptr.upload(aptr.data(), na + 1);
-  C.alist.alloc(ng, s); C.alist.upload(alist.data(), ng);
   C.sbeg.alloc(C.nseg, s); C.sbeg.upload(sb.data(), C.nseg);
   C.send.alloc(C.nseg, s); C.send.upload(se.data(), C.nseg);
   C.aseg.alloc(na + 1, s); C.aseg.upload(aseg.data(), na + 1);
