@@ -95,7 +95,8 @@ typedef struct tptfem_solver_opts {
   int32_t batch;         /* PCG iterations per CUDA-graph launch (0 -> auto) */
   int32_t flags;         /* TPTFEM_SOLVE_* bits */
   int32_t coarse_aggregates;  /* TPTFEM_SOLVE_COARSE: target number of aggregates
-                                 (0 -> node groups / 2800, between 8 and 1000) */
+                                 (0 -> node groups / 2800 for vector problems, / 700
+                                 for scalar ones, between 8 and 3000) */
   int32_t reserved;
 } tptfem_solver_opts;
 

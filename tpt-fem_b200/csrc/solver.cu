@@ -321,8 +321,13 @@ void select_nb_mode(SystemData& S, Engine<double>& E, const tptfem_solver_opts& 
 int select_coarse(SystemData& S, Engine<double>& E, const tptfem_solver_opts& o, bool fresh) {
   bool want = (o.flags & TPTFEM_SOLVE_COARSE) && E.nb_pc;
   PhaseTimer timer(S.ctx->stream, "coarse space");
-  // default: about one aggregate per 2800 node groups, between 8 and 1000
-  const int aggs = o.coarse_aggregates > 0 ? o.coarse_aggregates : std::max(8, std::min(1000, S.nb.ngroups / 2800));
+  // default: about one aggregate per 2800 node groups for vector problems (6 or
+  // 3 rigid modes each) and per 700 for scalar ones (one constant mode each),
+  // between 8 and 3000.  Measured optima: 504 aggregates (3000 coarse unknowns)
+  // for elasticity at 280x70x70, 2744 for the 128^3 Poisson random-field
+  // problems (23.9 ms per solve against 26.1 ms with 729).
+  const int per = S.dpn == 1 ? 700 : 2800;
+  const int aggs = o.coarse_aggregates > 0 ? o.coarse_aggregates : std::max(8, std::min(3000, S.nb.ngroups / per));
   if (want) want = coarse_build(S, aggs);
   if (want && (fresh || !S.coarse.ready)) want = coarse_assemble(S);
   if (want && !S.coarse.ready) want = false;
