@@ -504,6 +504,95 @@ def run_topopt(args, world, rank, local):
     return out
 
 
+# ncu DRAM read + write of one numeric assemble_nodes_tet launch on the
+# 140x35x35 cantilever (1,029,000 tets); scaled by tets to the measured mesh
+ASM_TRAFFIC_140 = (157.871616 + 121.000192) * 1e6
+ASM_TETS_140 = 1029000
+
+
+def assembly_cpu_baseline(n_sample=(40, 10, 10)):
+    """The reference's assembly on the host: the oracle restatement of
+    try_assemble (zero-skip COO over elements in id order) + Coo::to_csr (stable
+    sort, duplicate sum), one core, on a bounded cantilever sample; returns
+    (Melem/s, sample description)."""
+    from oracle import oracle as O
+    from tpt_fem import workloads as W
+    c, e = O.box_mesh([0.0, 0.0, 0.0], [4.0, 1.0, 1.0], list(n_sample))
+    m = O.Mesh(O.CELL_TET, c, e)
+    E = W.cantilever_young(list(n_sample))
+    O.assemble_elasticity(m, O.MODEL_3D, E, 0.3, 2).to_csr()  # warm
+    reps, t0 = 0, time.perf_counter()
+    while reps < 2 or time.perf_counter() - t0 < 10.0:
+        O.assemble_elasticity(m, O.MODEL_3D, E, 0.3, 2).to_csr()
+        reps += 1
+    dt = (time.perf_counter() - t0) / reps
+    return len(e) / dt / 1e6, (f"oracle assemble_elasticity + to_csr on the {list(n_sample)} cantilever "
+                               f"({len(e)} tets), {reps} repetitions, one core")
+
+
+def run_assembly(args, world, rank, local):
+    """Tet4 elasticity assembly of the 280x70x70 cantilever (8,232,000 tets,
+    per-element E): element throughput of the numeric re-assembly kernel
+    (pattern fixed, inputs resident; CUDA events in the library), and end to end
+    through the C ABI from host arrays (mesh upload, pattern and values)."""
+    import tpt_fem as F
+    from tpt_fem import workloads as W
+    ctx = F.Context(local)
+    mn, mx, n = W.CANTILEVERS[WORKLOAD]
+    if args.mesh:  # a smaller cantilever of the same family (ncu captures)
+        n = list(args.mesh)
+    E = W.cantilever_young(n)
+    m0 = F.Mesh.box_mesh(mn, mx, n, ctx=ctx)
+    coords, conn = m0.coords_array.copy(), m0.conn_array.copy()
+    del m0
+    mesh = F.Mesh.from_arrays(F.CELL_TET4, coords, conn, ctx=ctx)
+    K = F.assemble_elasticity(mesh, "3d", E, 0.3, 2)
+    n_el, n_nodes, nnz = len(conn), len(coords), K.nnz
+    K.profile_assembly(max(1, args.warmup))
+    barrier(world)
+    with ClockSampler(local) as clk:
+        ms = K.profile_assembly(args.steps)
+    barrier(world)
+    ms = barrier_max(ms, world)
+    # end to end: host arrays -> mesh -> assembled matrix (its size read back)
+    walls = []
+    for _ in range(3):
+        cuda_sync()
+        t0 = time.perf_counter()
+        mh = F.Mesh.from_arrays(F.CELL_TET4, coords, conn, ctx=ctx)
+        Kh = F.assemble_elasticity(mh, "3d", E, 0.3, 2)
+        _ = Kh.nnz
+        ctx.synchronize()
+        walls.append(time.perf_counter() - t0)
+        del Kh, mh
+    e2e_s = min(walls)
+    peak, kind = measured_peaks()
+    alg = 24.0 * n_nodes + 16.0 * n_el + 8.0 * n_el + 8.0 * nnz
+    out = None
+    if rank == 0:
+        cpu, sample = assembly_cpu_baseline()
+        out = {"metric": "Tet4 elasticity assembly throughput (numeric, pattern fixed)",
+               "value": world * n_el / (ms * 1e-3) / 1e6, "unit": "Melem/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded density field)",
+               "config": {"workload": "assembly_cantilever_%dx%dx%d" % tuple(n), "mesh": list(n), "tets": n_el,
+                          "nodes": n_nodes,
+                          "nnz": nnz, "per_element_E": True, "parallelism": f"replicas{world}",
+                          "l2": "inputs and output larger than L2 (values %.2f GB)" % (8e-9 * nnz)},
+               "roofline": {"bound": "hbm", "kernel": "assemble_nodes_tet<1,3> (NUMERIC: bit-exact FP64, no FMA)",
+                            "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "peak_kind": kind, "unit": "GB/s",
+                            "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": ASM_TRAFFIC_140 * n_el / ASM_TETS_140,
+                            "traffic_source": "ncu dram__bytes_read+write of the kernel at 140x35x35 scaled by tets",
+                            "algorithmic_bytes": alg,
+                            "algorithmic_formula": "24 N + 16 E + 8 E + 8 nnz (coords, connectivity, E, values)"},
+               "e2e": {"value": n_el / e2e_s / 1e6, "unit": "Melem/s", "seconds": e2e_s,
+                       "h2d_bytes_per_step": int(coords.nbytes + conn.nbytes + E.nbytes), "d2h_bytes_per_step": 8},
+               "cpu_baseline": {"value": cpu, "unit": "Melem/s", "cores": 1, "kind": "port", "sample": sample},
+               "gpu_launches": args.steps,
+               "clocks": clk.summary()}
+    return out
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
@@ -536,7 +625,7 @@ def main():
     ap.add_argument("--solver", default="learned", choices=["learned", "fsai", "jacobi", "mp"])
     ap.add_argument("--profile", action="store_true", help="run only the timed solves (ncu launch list)")
     ap.add_argument("--no-coarse", action="store_true", help="single-level preconditioner (no coarse space)")
-    ap.add_argument("--workload", default="cantilever", choices=["cantilever", "poisson_grf", "topopt"],
+    ap.add_argument("--workload", default="cantilever", choices=["cantilever", "poisson_grf", "topopt", "assembly"],
                     help="poisson_grf: the heterogeneous-Poisson learned-preconditioner configuration")
     ap.add_argument("--fields", type=int, default=32, help="poisson_grf: unseen fields timed")
     ap.add_argument("--instances", type=int, default=512, help="topopt: instances in the batch")
@@ -552,6 +641,8 @@ def main():
         out = run_poisson_grf(args, world, rank, local)
     elif args.workload == "topopt":
         out = run_topopt(args, world, rank, local)
+    elif args.workload == "assembly":
+        out = run_assembly(args, world, rank, local)
     else:
         out = run_ours(args, world, rank, local)
     if rank == 0 and out is not None:

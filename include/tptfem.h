@@ -197,6 +197,11 @@ tptfem_status tptfem_assemble_elasticity(tptfem_context* ctx, tptfem_mesh* mesh,
  * the new coefficients change which entries are non-zero, the pattern is rebuilt
  * (the result still equals a fresh assemble). */
 tptfem_status tptfem_reassemble(tptfem_context* ctx, tptfem_matrix* mat, const double* coef, int per_element);
+/* Diagnostic (no reference counterpart): average device time in ms of `reps`
+ * numeric re-assemblies of `mat` (values only, pattern fixed, coefficients
+ * already on the device), timed with CUDA events; the values are rewritten
+ * unchanged. */
+tptfem_status tptfem_matrix_profile_assembly(tptfem_context* ctx, tptfem_matrix* mat, int reps, double* ms);
 /* Csr::nrows / ncols / nnz (crates/tpt-fem-sparse/src/lib.rs:51-63, 122-143). */
 tptfem_status tptfem_matrix_sizes(const tptfem_matrix* mat, int64_t* nrows, int64_t* ncols, int64_t* nnz);
 tptfem_status tptfem_matrix_download(tptfem_context* ctx, const tptfem_matrix* mat, int64_t* row_ptrs,

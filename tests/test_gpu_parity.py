@@ -398,3 +398,17 @@ def test_factor_pattern_from_group_adjacency_matches_row_union(ctx, dim):
     rp2, ci2, va2, s2 = groups.fsai()
     assert np.array_equal(rp1, rp2) and np.array_equal(ci1, ci2)
     assert np.array_equal(va1, va2) and np.array_equal(s1, s2)
+
+
+def test_profiled_numeric_assembly_rewrites_identical_values(ctx):
+    c, e = box([5, 4, 3], mx=(2.0, 1.0, 1.0))
+    c = jitter(c, 0.03, 71)
+    E = np.random.default_rng(72).uniform(0.05, 1.0, len(e))
+    m = F.Mesh.from_arrays(F.CELL_TET4, c, e, ctx=ctx)
+    K = F.assemble_elasticity(m, "3d", E, 0.3, 2)
+    before = K.to_csr()
+    ms = K.profile_assembly(3)
+    after = K.to_csr()
+    assert ms > 0.0
+    for a, b in zip(before, after):
+        assert np.array_equal(a, b)

@@ -436,6 +436,14 @@ tptfem_status tptfem_reassemble(tptfem_context* ctx, tptfem_matrix* mat, const d
   API_CATCH(ctx)
 }
 
+tptfem_status tptfem_matrix_profile_assembly(tptfem_context* ctx, tptfem_matrix* mat, int reps, double* ms) {
+  if (!ctx || !mat || !mat->d || !ms || reps < 1) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  *ms = profile_numeric_assembly(*mat->d, reps);
+  API_CATCH(ctx)
+}
+
 tptfem_status tptfem_matrix_sizes(const tptfem_matrix* mat, int64_t* nrows, int64_t* ncols, int64_t* nnz) {
   if (!mat || !mat->d) return TPTFEM_ERR_INVALID_ARG;
   if (nrows) *nrows = mat->d->ref_nrows;

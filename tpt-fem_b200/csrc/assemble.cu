@@ -1093,6 +1093,25 @@ bool reassemble_values(MatrixData& M) {
   return (f & 2) == 0;
 }
 
+double profile_numeric_assembly(MatrixData& M, int reps) {
+  tptfem_context* ctx = M.ctx;
+  cudaStream_t s = ctx->stream;
+  set_cell_tab(*M.mesh, M.quad_order, s);
+  if (M.robin) set_robin_faces(*M.mesh, M.robin_axis, s);
+  TPT_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), s));
+  RowArgs A = row_args(M);
+  dispatch_rows(M, MODE_NUMERIC, A, s);  // warm-up (module load, caches)
+  TPT_CUDA(cudaEventRecord(ctx->ev[0], s));
+  for (int r = 0; r < reps; ++r) dispatch_rows(M, MODE_NUMERIC, A, s);
+  TPT_CUDA(cudaEventRecord(ctx->ev[1], s));
+  TPT_CUDA(cudaEventSynchronize(ctx->ev[1]));
+  float ms = 0.f;
+  TPT_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+  const int f = read_flag(ctx);
+  TPT_REQUIRE(f == 0, TPTFEM_ERR_NUMERIC, "profiled re-assembly: degenerate element or changed pattern");
+  return (double)ms / std::max(reps, 1);
+}
+
 void load_poisson_source(MeshData& m, double src, int quad_order, double* d_rhs) {
   tptfem_context* ctx = m.ctx;
   cudaStream_t s = ctx->stream;

@@ -289,6 +289,9 @@ void nb_operator_apply_modes(SystemData& S, const double* X, double* Y, const un
 // solver.cu
 int64_t system_fsai_classic(SystemData& S);  // builds (once) the classic factor; -1 on failure
 void system_fsai_download(const SystemData& S, int64_t* rp, int64_t* ci, double* lva, double* sig2);
+// average device time in ms of `reps` numeric re-assemblies (values only,
+// pattern fixed, coefficients resident), timed with CUDA events
+double profile_numeric_assembly(MatrixData& M, int reps);
 void system_profile_spmv(SystemData& S, int reps, double* ms_f64, double* ms_f32, double* ms_nb, double* nb_bytes,
                          double* ms_nbs, double* nbs_bytes);
 void system_solve(SystemData& S, const tptfem_solver_opts& o, tptfem_solve_stats& st);

@@ -239,6 +239,12 @@ class Matrix:
                                                            N.ptr(x), C.byref(it)))
         return lam.value, x, it.value
 
+    def profile_assembly(self, reps=10):
+        """Average device time (ms) of a numeric re-assembly with resident coefficients (CUDA events)."""
+        ms = C.c_double()
+        self.ctx.check(self.ctx.lib.tptfem_matrix_profile_assembly(self.ctx.h, self.h, int(reps), C.byref(ms)))
+        return ms.value
+
     def reassemble(self, coef):
         """New per-element (or constant) coefficients on the same mesh; pattern revalidated."""
         coef = np.atleast_1d(N.f64(coef))

@@ -122,6 +122,7 @@ SIGNATURES = {
     "tptfem_system_solution": (C.c_int, [_vp, _vp, _vp]),
     "tptfem_system_free": (None, [_vp]),
     "tptfem_system_profile_spmv": (C.c_int, [_vp, _vp, C.c_int, _pd, _pd, _pd, _pd, _pd, _pd]),
+    "tptfem_matrix_profile_assembly": (C.c_int, [_vp, _vp, C.c_int, _pd]),
     "tptfem_system_fsai": (C.c_int, [_vp, _vp, _pi64]),
     "tptfem_lfsai_param_count": (C.c_int64, []),
     "tptfem_lfsai_create": (C.c_int, [_vp, C.c_uint64, _pp]),
