@@ -41,7 +41,7 @@ WORKLOAD = "cantilever_280x70x70"
 TOL = 1e-10
 # FP64 Jacobi-PCG iterations to 1e-10 on this exact system (same algorithm as the
 # CPU port), measured on a B200 by this script's own FP64 Jacobi leg; used to
-# scale the reference arm's per-iteration CPU time.
+# scale the reference arm's per-iteration CPU time to the whole solve.
 JACOBI_ITERS_280 = 4881
 
 

@@ -1,6 +1,6 @@
-"""The BASELINE configurations at their full sizes, through properties that do
+"""The benchmark workloads at their full sizes, through properties that do
 not depend on size: exact pattern sizes (the nnz counts the reference's
-to_csr gives, SURVEY-recorded), symmetry and the rigid-body null space of
+to_csr gives for these meshes), symmetry and the rigid-body null space of
 the assembled operators, load totals, and solutions to the stated tolerance
 whose residual is re-checked on the host from the downloaded matrix."""
 import os
@@ -39,7 +39,7 @@ def check_operator(A, dpn, rng):
         assert np.linalg.norm(A @ t) <= 1e-12 * np.abs(A).sum(axis=1).max() * np.sqrt(A.shape[0])
 
 
-def test_config2_elasticity_64_cube(ctx):
+def test_elasticity_unit_cube_64(ctx):
     m = F.Mesh.box_mesh([0, 0, 0], [1, 1, 1], [64, 64, 64], ctx=ctx)
     K = F.assemble_elasticity(m, "3d", 1.0, 0.3, 2)
     assert (K.nrows, K.nnz) == (823875, 29801277)
@@ -60,7 +60,7 @@ def test_config2_elasticity_64_cube(ctx):
     assert np.linalg.norm(fred - A @ u[free]) <= 2e-10 * np.linalg.norm(fred)
 
 
-def test_config3_poisson_grf_128(ctx):
+def test_poisson_grf_128(ctx):
     prob = W.GrfPoisson(ctx, 128)
     K = prob.matrix(5000)
     assert K.nnz == 14926977
@@ -77,7 +77,7 @@ def test_config3_poisson_grf_128(ctx):
     assert np.linalg.norm(fred - A @ u[free]) <= 2e-8 * np.linalg.norm(fred)
 
 
-def test_config5_cantilever_280x70x70(ctx):
+def test_cantilever_280x70x70(ctx):
     mn, mx, n = W.CANTILEVERS["cantilever_280x70x70"]
     m = F.Mesh.box_mesh(mn, mx, n, ctx=ctx)
     assert (m.n_nodes, m.n_elems) == (1416521, 8232000)

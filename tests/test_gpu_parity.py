@@ -46,7 +46,7 @@ def test_device_box_mesh_offset_box(ctx):
 
 # ---- Poisson assembly ---------------------------------------------------------------
 
-def test_poisson_config1_pattern_and_values(ctx):
+def test_poisson_box8_pattern_and_values(ctx):
     c, e = box([8, 8, 8])
     m = F.Mesh.box_mesh([0, 0, 0], [1, 1, 1], [8, 8, 8], ctx=ctx)
     K = F.assemble_poisson(m, 1.0, 2)
@@ -205,7 +205,7 @@ def test_reduce_system_bit_exact(ctx):
 
 
 @pytest.mark.parametrize("solver", [F.SOLVER_JACOBI_PCG, F.SOLVER_MP_PCG, F.SOLVER_FSAI_MP_PCG])
-def test_config1_solution_vs_dense_lu(ctx, solver):
+def test_poisson_box8_solution_vs_dense_lu(ctx, solver):
     c, e = box([8, 8, 8])
     m = F.Mesh.box_mesh([0, 0, 0], [1, 1, 1], [8, 8, 8], ctx=ctx)
     bcs = unit_cube_bcs(c)

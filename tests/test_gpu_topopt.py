@@ -57,7 +57,7 @@ def test_reference_full_volume_and_denser_tests(ctx):
 
 
 def test_density_filter_mode_matches_oracle(ctx):
-    # the configuration's settings: Emin 1e-9, density filter R 1.5, mid-right load
+    # the batched workload's settings: Emin 1e-9, density filter R 1.5, mid-right load
     P = params(60, 20, 0.4, 1.5, 100, emin=1e-9, density_filter=True)
     f, bcs = T.cantilever_load(P.grid, node=P.grid.nx * (P.grid.nely // 2) + P.grid.nelx)
     res = T.topopt_simp(P, f, bcs, ctx=ctx, rel_tol=TOL)
@@ -163,8 +163,8 @@ def test_wide_grids_fall_back_to_pcg_in_the_same_batch(ctx):
     check_against_oracle(res[1], *probs[1])
 
 
-def test_largest_configuration_grid_direct_matches_pcg(ctx):
-    # the configuration's largest grid (240 x 80 elements, 39,042 dofs, half-bandwidth 165):
+def test_largest_batch_grid_direct_matches_pcg(ctx):
+    # the batched workload's largest grid (240 x 80 elements, 39,042 dofs, half-bandwidth 165):
     # banded Cholesky without refinement against two-level PCG, both to 1e-11
     P = params(240, 80, 0.4, 1.5, 3, emin=1e-9, density_filter=True)
     f, bcs = T.cantilever_load(P.grid, node=P.grid.nx * (P.grid.nely // 2) + P.grid.nelx)

@@ -179,7 +179,7 @@ def test_plane_stress_patch_test():  # elasticity:742
     assert abs(u[8] - 0.05) < 1e-9 and abs(u[9] - 0.1) < 1e-9
 
 
-def test_config1_survey_sanity_values():
+def test_poisson_box8_sanity_values():
     # Poisson on box_mesh [8,8,8], k=1, f=1, u=0 on all faces (the plain-method case).
     c, e = O.box_mesh([0, 0, 0], [1, 1, 1], [8, 8, 8])
     m = O.Mesh(O.CELL_TET, c, e)
@@ -218,7 +218,7 @@ def test_tet4_elasticity_linear_patch_on_box_mesh():
     assert np.max(np.abs(u - uex)) < 1e-12
 
 
-def test_pcg_jacobi_matches_dense_lu_on_config1():
+def test_pcg_jacobi_matches_dense_lu_on_poisson_box8():
     c, e = O.box_mesh([0, 0, 0], [1, 1, 1], [8, 8, 8])
     m = O.Mesh(O.CELL_TET, c, e)
     coo = O.assemble_poisson(m, 1.0, 2)
