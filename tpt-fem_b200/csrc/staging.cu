@@ -2,7 +2,8 @@
 //
 // The C ABI takes ordinary (pageable) host arrays.  Large ones are copied by
 // several host threads into the context's pinned staging buffer (kept between
-// calls, grown on demand) and moved by one DMA, instead of the driver's
+// calls, grown on demand) in chunks, each moved by its own DMA as soon as it is
+// filled (downloads the same way in reverse), instead of the driver's
 // single-threaded pageable path; connectivity is narrowed to int32 and
 // coefficients are checked on the way.  Small arrays go directly.
 #include <algorithm>
