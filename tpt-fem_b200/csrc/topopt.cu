@@ -1,19 +1,23 @@
 // topopt.cu -- batched 2-D SIMP topology optimisation (minimum compliance).
 //
 // Restates crates/tpt-fem-topopt/src/lib.rs (topopt_simp, topopt:342-385) for
-// many independent instances at once.  One CTA owns one instance for a whole
-// optimality-criteria iteration; one launch runs every phase of that iteration
-// for every instance:
+// many independent instances at once.  One CTA owns one instance; each
+// optimality-criteria iteration is two launches over all instances:
 //   E_e = emin + rho_e^p (e0 - emin)                     (assemble, topopt:220-238)
-//   K(E) u = f with Dirichlet dofs, matrix-free Q1 apply from the unit element
-//     matrix (element_stiffness_unit, topopt:166-217), PCG in FP64 warm-started
-//     from the previous iteration's displacement, preconditioned by Jacobi plus
-//     an aggregation coarse space of plane rigid modes (M^-1 = D^-1 + P A_c^-1 P^T,
-//     A_c assembled and inverted inside the instance's CTA every OC iteration)
+//   K(E) u = f with Dirichlet dofs (the reference uses a dense LU):
+//     topo_direct factors K_FF as a band (banded Cholesky, products on the FP64
+//     tensor cores) and refines the solution to the residual tolerance; for
+//     grids too wide for its band, or a breakdown, topo_iteration runs PCG in
+//     FP64 on the matrix-free Q1 operator from the unit element matrix
+//     (element_stiffness_unit, topopt:166-217), warm-started from the previous
+//     displacement, preconditioned by Jacobi plus an aggregation coarse space of
+//     plane rigid modes (M^-1 = D^-1 + P A_c^-1 P^T, A_c assembled and inverted
+//     inside the instance's CTA every OC iteration)
 //   c = f . u                                             (topopt:360,368)
 //   dc_e = -p rho^(p-1) (e0 - emin) u_e^T K0 u_e           (topopt:371-375)
 //   sensitivity filter (topopt:259-279) or the density filter of the 88-line
-//     SIMP code, then the OC bisection (oc_update, topopt:284-331)
+//     SIMP code, then the OC bisection (oc_update, topopt:284-331), all in
+//     topo_iteration
 // The launches of all iterations are captured in one CUDA graph.  Instances
 // never wait on each other (no inter-CTA synchronisation); blocks are issued
 // largest instance first.  The block size (threads per instance) is chosen by
