@@ -3,7 +3,8 @@
  * Drop-in boundary for tpt-fem's assemble -> CSR -> SPD-solve path.  The
  * reference is a Rust workspace with no FFI of its own; each entry point below
  * names the Rust function it replaces (path:line inside the tpt-fem project),
- * so a Rust crate can bind it 1:1 (see INTEGRATION.md for the binding stub).
+ * so a Rust crate can bind it 1:1 through a `-sys` crate of extern "C"
+ * declarations that mirror this header.
  *
  * Conventions
  *  - Every function returns tptfem_status; on failure the context keeps a
@@ -334,12 +335,17 @@ tptfem_status tptfem_system_coarse(tptfem_context* ctx, const tptfem_system* sys
  * on every call.  It calls no cudaMalloc, cudaFree or allocating routine: its
  * only scratch is a static 16,448-byte device array (2048 partial sums plus
  * counters), resident on every GPU that loads the library until exit.
- * Limits: 1 <= n <= 2147483646; column indices must lie in [0, n) (checked on
- * the device: TPTFEM_ERR_INVALID_ARG).  `stream` is a cudaStream_t (NULL: the
- * default stream); the call synchronises it before returning.  The first call
- * on a device looks up the array's device address (cudaGetSymbolAddress) and
- * should come before any stream capture.  Every call shares the array: calls
- * whose kernels overlap on the GPU race and must be serialised by the caller.
+ * Limits: 1 <= n <= 2147483646.  Preconditions: row_ptrs holds n+1 entries,
+ * col_ind and values hold row_ptrs[n] entries each.  Checked on the device
+ * (TPTFEM_ERR_INVALID_ARG, offending rows and entries skipped, never read
+ * outside those row_ptrs[n] entries): every row range 0 <= row_ptrs[i] <=
+ * row_ptrs[i+1] <= row_ptrs[n], and every column index in [0, n).  `stream`
+ * is a cudaStream_t (NULL: the default stream); the call synchronises it
+ * before returning.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and should come before any stream capture;
+ * a call that fails with TPTFEM_ERR_DEVICE forgets that address, so the next
+ * call looks it up again.  Every call shares the array: calls whose kernels
+ * overlap on the GPU race and must be serialised by the caller.
  * `err` (may be NULL) receives a message of at most err_len bytes. */
 tptfem_status tptfem_rel_residual_noalloc(int device, void* stream, int64_t n, const int32_t* row_ptrs,
                                           const int32_t* col_ind, const double* values, const double* x,
@@ -449,6 +455,17 @@ tptfem_status tptfem_topopt_batch(tptfem_context* ctx, const tptfem_topopt_insta
                                   tptfem_topopt_stats* stats);
 /* element_stiffness_unit (topopt:166-217): the 8x8 unit-modulus Q1 plane-stress matrix. */
 tptfem_status tptfem_topopt_element_stiffness(double nu, double h, double* ke);
+
+/* ---- synthetic input generator (no counterpart in the reference) ---------
+ * Gaussian random field by random Fourier features at n host points
+ * (n x 3, row-major): out[p] = scale * sum_{m=0}^{M-1} cos(w_m . x_p + phi_m),
+ * w host 3 x M row-major (row d = component d of every frequency), phi host
+ * M, M = n_features in 1..2048.  The sum runs in ascending m and the dot
+ * product as ((x w_0 + y w_1) + z w_2) + phi without contraction, so the
+ * same inputs give the same bits on every GPU.  The heterogeneous-Poisson
+ * benchmark's conductivity is k = exp(g) at the element centroids. */
+tptfem_status tptfem_grf_eval(tptfem_context* ctx, const double* points, int64_t n, const double* w,
+                              const double* phi, int32_t n_features, double scale, double* out);
 
 #ifdef __cplusplus
 }

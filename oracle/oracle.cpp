@@ -23,6 +23,7 @@
 // a textbook partial-pivot LU stands in for it here.  Below the 1e-9..1e-10
 // tolerances of the reference's own solve tests that LU is parity-unpinned.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -548,20 +549,33 @@ vector<FaceDef> faces_of(int cell) {
 
 // boundary_faces (assembly:563-583): faces whose sorted node key occurs once.
 vector<std::pair<i64, int>> boundary_faces(const OMesh& m) {
-  std::unordered_map<std::string, int> counts;
-  auto key_of = [&](i64 e, const FaceDef& f) {
-    vector<i64> key;
-    for (int i : f.nodes) key.push_back(m.elems[e][i]);
-    std::sort(key.begin(), key.end());
-    return std::string((const char*)key.data(), key.size() * sizeof(i64));
-  };
+  // Counting the sorted node keys by sorting them (rather than the reference's
+  // HashMap) gives the same set; the output keeps element-then-face order.
   auto faces = faces_of(m.cell);
-  for (size_t e = 0; e < m.elems.size(); ++e)
-    for (auto& f : faces) counts[key_of(e, f)] += 1;
+  const size_t nf = faces.size(), ne = m.elems.size();
+  struct Key { std::array<i64, 4> k; i64 idx; };
+  vector<Key> keys(ne * nf);
+  for (size_t e = 0; e < ne; ++e)
+    for (size_t fi = 0; fi < nf; ++fi) {
+      Key& kk = keys[e * nf + fi];
+      kk.k.fill(-1);
+      size_t q = 0;
+      for (int i : faces[fi].nodes) kk.k[q++] = m.elems[e][i];
+      std::sort(kk.k.begin(), kk.k.begin() + q);
+      kk.idx = (i64)(e * nf + fi);
+    }
+  std::sort(keys.begin(), keys.end(), [](const Key& a, const Key& b) { return a.k < b.k; });
+  vector<char> once(ne * nf, 0);
+  for (size_t a = 0; a < keys.size();) {
+    size_t b = a + 1;
+    while (b < keys.size() && keys[b].k == keys[a].k) ++b;
+    if (b - a == 1) once[keys[a].idx] = 1;
+    a = b;
+  }
   vector<std::pair<i64, int>> out;
-  for (size_t e = 0; e < m.elems.size(); ++e)
-    for (size_t fi = 0; fi < faces.size(); ++fi)
-      if (counts[key_of(e, faces[fi])] == 1) out.push_back({(i64)e, (int)fi});
+  for (size_t e = 0; e < ne; ++e)
+    for (size_t fi = 0; fi < nf; ++fi)
+      if (once[e * nf + fi]) out.push_back({(i64)e, (int)fi});
   return out;
 }
 
@@ -839,6 +853,110 @@ OrcCoo* orc_assemble_given(OrcMesh* h, int dpn, const double* mats) {
     scatter_element(c->c, h->m.elems[e], dpn, ke);
   }
   return c;
+}
+
+// Selected rows of Coo::to_csr(assemble(...)) (sparse:122-175 over
+// assembly:428-480) for meshes too large to hold the whole COO.  The triplets
+// that global row r receives are the zero-skipped entries of local row r of
+// each element containing r's node, pushed in element id order and, within an
+// element, in local column order (scatter_element above).  The stable sort by
+// (row, col) keeps that push order among equal columns, so sorting one row's
+// triplets stably by column and summing equal columns left to right gives
+// exactly that row of the CSR.  kind 0: poisson_element_matrix (coef = k);
+// kind 1: elasticity_element_matrix (coef = E, with model and nu).  coef holds
+// one value per element, or one value if coef_per_elem == 0.  Rows are
+// independent, so they are computed in parallel.
+struct OrcRows { vector<i64> ptr, cols; vector<double> vals; };
+
+OrcRows* orc_csr_rows(OrcMesh* h, int kind, int model, const double* coef, int coef_per_elem, double nu, int qo,
+                      const i64* rows, i64 nrows) {
+  const OMesh& m = h->m;
+  const int dpn = kind == 0 ? 1 : ref_dim(m.cell);
+  const i64 nn = (i64)m.nodes.size();
+  vector<char> need(nn, 0);
+  for (i64 k = 0; k < nrows; ++k) {
+    if (rows[k] < 0 || rows[k] / dpn >= nn) { g_err = "row outside the mesh"; return nullptr; }
+    need[rows[k] / dpn] = 1;
+  }
+  vector<vector<i64>> inc(nn);
+  for (size_t e = 0; e < m.elems.size(); ++e)
+    for (i64 nd : m.elems[e]) if (need[nd]) inc[nd].push_back((i64)e);
+  vector<vector<std::pair<i64, double>>> out(nrows);
+  int bad = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : bad)
+  for (i64 k = 0; k < nrows; ++k) {
+    const i64 node = rows[k] / dpn, comp = rows[k] % dpn;
+    vector<std::pair<i64, double>> t;
+    vector<vector<double>> ke;
+    for (i64 e : inc[node]) {
+      const double c = coef[coef_per_elem ? e : 0];
+      const bool ok = kind == 0 ? poisson_element_matrix(m, e, c, qo, ke)
+                                : elasticity_element_matrix(m, e, model, c, nu, qo, ke);
+      if (!ok) { bad = 1; break; }
+      const vector<i64>& en = m.elems[e];
+      for (size_t a = 0; a < en.size(); ++a) {
+        if (en[a] != node) continue;
+        const size_t i = a * dpn + (size_t)comp;
+        for (size_t j = 0; j < ke[i].size(); ++j) {
+          const double kij = ke[i][j];
+          if (kij == 0.0) continue;
+          t.push_back({en[j / dpn] * dpn + (i64)(j % dpn), kij});
+        }
+      }
+    }
+    std::stable_sort(t.begin(), t.end(), [](const std::pair<i64, double>& x, const std::pair<i64, double>& y) {
+      return x.first < y.first;
+    });
+    for (size_t q = 0; q < t.size();) {
+      double sum = t[q].second;
+      size_t qq = q + 1;
+      while (qq < t.size() && t[qq].first == t[q].first) sum += t[qq++].second;
+      out[k].push_back({t[q].first, sum});
+      q = qq;
+    }
+  }
+  if (bad) { g_err = "element matrix failed (quadrature order or model)"; return nullptr; }
+  OrcRows* r = new OrcRows;
+  r->ptr.assign(nrows + 1, 0);
+  for (i64 k = 0; k < nrows; ++k) {
+    r->ptr[k + 1] = r->ptr[k] + (i64)out[k].size();
+    for (auto& p : out[k]) { r->cols.push_back(p.first); r->vals.push_back(p.second); }
+  }
+  return r;
+}
+i64 orc_rows_nnz(OrcRows* r) { return (i64)r->cols.size(); }
+void orc_rows_copy(OrcRows* r, i64* ptr, i64* cols, double* vals) {
+  std::memcpy(ptr, r->ptr.data(), r->ptr.size() * sizeof(i64));
+  if (!r->cols.empty()) {
+    std::memcpy(cols, r->cols.data(), r->cols.size() * sizeof(i64));
+    std::memcpy(vals, r->vals.data(), r->vals.size() * sizeof(double));
+  }
+}
+void orc_rows_free(OrcRows* r) { delete r; }
+
+// Selected nodes of the Poisson load loop of solve_poisson (thermal:224-230):
+// rhs[node] receives f_e[i] of every element containing it, in element id
+// order, starting from 0.0 -- the same additions the whole loop makes on that
+// entry.  Source constant s.
+int orc_load_poisson_rows(OrcMesh* h, double s, int qo, const i64* nodes, i64 n, double* out) {
+  const OMesh& m = h->m;
+  const i64 nn = (i64)m.nodes.size();
+  vector<i64> slot(nn, -1);
+  for (i64 k = 0; k < n; ++k) {
+    if (nodes[k] < 0 || nodes[k] >= nn) { g_err = "node outside the mesh"; return 1; }
+    slot[nodes[k]] = k;
+  }
+  vector<double> acc(n, 0.0), f;
+  for (size_t e = 0; e < m.elems.size(); ++e) {
+    bool hit = false;
+    for (i64 nd : m.elems[e]) hit |= slot[nd] >= 0;
+    if (!hit) continue;
+    if (!poisson_source_vector(m, (i64)e, s, nullptr, nullptr, qo, f)) { g_err = "bad quadrature order"; return 1; }
+    for (size_t i = 0; i < m.elems[e].size(); ++i)
+      if (slot[m.elems[e][i]] >= 0) acc[slot[m.elems[e][i]]] += f[i];
+  }
+  for (i64 k = 0; k < n; ++k) out[k] = acc[slot[nodes[k]]];
+  return 0;
 }
 
 OrcCoo* orc_coo_new() { return new OrcCoo; }

@@ -57,6 +57,11 @@ def lib():
         "orc_assemble_poisson": (_vp, [_vp, _f64p, C.c_int, C.c_int]),
         "orc_assemble_elasticity": (_vp, [_vp, C.c_int, _f64p, C.c_int, C.c_double, C.c_int]),
         "orc_assemble_given": (_vp, [_vp, C.c_int, _f64p]),
+        "orc_csr_rows": (_vp, [_vp, C.c_int, C.c_int, _f64p, C.c_int, C.c_double, C.c_int, _i64p, _i64]),
+        "orc_rows_nnz": (_i64, [_vp]),
+        "orc_rows_copy": (None, [_vp, _i64p, _i64p, _f64p]),
+        "orc_rows_free": (None, [_vp]),
+        "orc_load_poisson_rows": (C.c_int, [_vp, C.c_double, C.c_int, _i64p, _i64, _f64p]),
         "orc_coo_new": (_vp, []),
         "orc_coo_push": (None, [_vp, _i64, _i64, C.c_double]),
         "orc_coo_len": (_i64, [_vp]),
@@ -262,6 +267,66 @@ def assemble_elasticity(mesh, model, young, nu, quad_order):
     if not h:
         raise OracleError(_err())
     return Coo(h)
+
+
+def csr_rows(mesh, kind, coef, rows, model=MODEL_3D, nu=0.3, quad_order=2):
+    """Rows `rows` of Coo::to_csr(assemble(...)) (sparse:122-175 over
+    assembly:428-480) without the whole COO: kind "poisson" (coef = k) or
+    "elasticity" (coef = E).  Returns (ptr, cols, vals) with row k of the
+    sample in cols[ptr[k]:ptr[k+1]]."""
+    c = np.atleast_1d(np.asarray(coef, dtype=np.float64)).copy()
+    per = 1 if (len(c) == mesh.n_elems and len(c) > 1) else 0
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    h = lib().orc_csr_rows(mesh.h, 0 if kind == "poisson" else 1, model, c, per, float(nu), quad_order, rows,
+                           len(rows))
+    if not h:
+        raise OracleError(_err())
+    try:
+        nnz = lib().orc_rows_nnz(h)
+        ptr = np.zeros(len(rows) + 1, np.int64)
+        cols = np.zeros(nnz, np.int64)
+        vals = np.zeros(nnz)
+        lib().orc_rows_copy(h, ptr, cols, vals)
+        return ptr, cols, vals
+    finally:
+        lib().orc_rows_free(h)
+
+
+def load_poisson_rows(mesh, source, nodes, quad_order=2):
+    """Entries `nodes` of the constant-source Poisson load (thermal:224-230)."""
+    nodes = np.ascontiguousarray(nodes, dtype=np.int64)
+    out = np.zeros(len(nodes))
+    if lib().orc_load_poisson_rows(mesh.h, float(source), quad_order, nodes, len(nodes), out):
+        raise OracleError(_err())
+    return out
+
+
+def reduced_rows(ptr, cols, vals, rhs_rows, bcs, free_index):
+    """reduce_system (assembly/src/lib.rs:504-535) restricted to the free rows
+    whose full CSR rows are given (ptr/cols/vals as csr_rows returns them, and
+    their right-hand-side entries rhs_rows).  For each row: fred = rhs minus
+    v * value of every fixed column, value from the FIRST bcs entry of that
+    column (assembly:525), subtracted in column order; the free columns keep
+    their values under the reduced numbering free_index[col] (ascending, so
+    the later to_csr keeps their order and has no duplicates to sum).
+    Returns (ptr, cols, vals, fred)."""
+    first = {}
+    for d, v in bcs:
+        first.setdefault(int(d), float(v))
+    optr, ocols, ovals, fred = [0], [], [], []
+    for k in range(len(ptr) - 1):
+        r = float(rhs_rows[k])
+        for c, v in zip(cols[ptr[k]:ptr[k + 1]], vals[ptr[k]:ptr[k + 1]]):
+            c = int(c)
+            if c in first:
+                r -= float(v) * first[c]
+            else:
+                ocols.append(int(free_index[c]))
+                ovals.append(float(v))
+        optr.append(len(ocols))
+        fred.append(r)
+    return (np.asarray(optr, np.int64), np.asarray(ocols, np.int64), np.asarray(ovals, np.float64),
+            np.asarray(fred, np.float64))
 
 
 def assemble_given(mesh, dpn, mats):

@@ -1,7 +1,8 @@
 """Regenerate the committed golden fixtures from the reference checkout.
 
-Run once in a container where the reference tree is mounted (default
-``/root/reference``); the tests only read the ``.npz`` files this writes.
+Run once where the reference tree is checked out, with its root as the one
+required argument (``python make_golden.py <tpt-fem checkout>``); the tests
+only read the ``.npz`` files this writes.
 
 Fixtures:
   box4_structured.npz   points (125,3) and connectivity (384,4) of
@@ -23,7 +24,6 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -52,12 +52,12 @@ def parse_legacy_vtk(path):
     return out
 
 
-def write_digests():
+def write_digests(ref):
     import hashlib
     import json
     out = {}
     for name in ("mesh_gen_box_structured.vtk", "thermal_solve.vtk"):
-        data = open(os.path.join(REF, name), "rb").read()
+        data = open(os.path.join(ref, name), "rb").read()
         out[name] = {"bytes": len(data), "sha256": hashlib.sha256(data).hexdigest()}
     with open(os.path.join(OUT, "vtk_digests.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
@@ -65,12 +65,15 @@ def write_digests():
 
 
 def main():
-    g = parse_legacy_vtk(os.path.join(REF, "mesh_gen_box_structured.vtk"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_golden.py <path of the tpt-fem checkout>")
+    ref = sys.argv[1]
+    g = parse_legacy_vtk(os.path.join(ref, "mesh_gen_box_structured.vtk"))
     np.savez_compressed(os.path.join(OUT, "box4_structured.npz"), points=g["points"], conn=g["conn"])
-    t = parse_legacy_vtk(os.path.join(REF, "thermal_solve.vtk"))
+    t = parse_legacy_vtk(os.path.join(ref, "thermal_solve.vtk"))
     np.savez_compressed(os.path.join(OUT, "box6_thermal_mesh.npz"), points=t["points"], conn=t["conn"],
                         stale_temperature=t["stale_temperature"])
-    write_digests()
+    write_digests(ref)
     print("wrote", OUT)
 
 

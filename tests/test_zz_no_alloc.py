@@ -31,10 +31,10 @@ def _device(arr, dtype):
     return torch.as_tensor(np.ascontiguousarray(arr, dtype=dtype)).to("cuda:0")
 
 
-def _call(lib, n, rp, ci, va, x, b):
+def _call(lib, n, rp, ci, va, x, b, stream=None):
     out = C.c_double(-1.0)
     err = C.create_string_buffer(256)
-    rc = lib.tptfem_rel_residual_noalloc(0, None, n, C.c_void_p(rp.data_ptr()), C.c_void_p(ci.data_ptr()),
+    rc = lib.tptfem_rel_residual_noalloc(0, stream, n, C.c_void_p(rp.data_ptr()), C.c_void_p(ci.data_ptr()),
                                          C.c_void_p(va.data_ptr()), C.c_void_p(x.data_ptr()),
                                          C.c_void_p(b.data_ptr()), C.byref(out), err, len(err))
     return rc, out.value, err.value.decode()
@@ -65,6 +65,22 @@ def test_noalloc_residual_matches_solver_on_two_calls():
         assert rc == N.OK, msg
         assert abs(val - st["rel_residual"]) <= REL_TOL * st["rel_residual"]
     assert first[1] == second[1]
+    # an independent host check: the same residual from a plain numpy CSR product
+    ax = np.add.reduceat(va * x[ci], rp[:-1]) if len(va) else np.zeros(S.n_free)
+    host = np.linalg.norm(fred - ax) / np.linalg.norm(fred)
+    # the naive host sum cancels: its error is ~1e-16 of ||b|| per row term,
+    # i.e. ~1e-10 of this 1e-6 residual, a few times that in practice
+    assert abs(first[1] - host) <= 1e-7 * host
+
+    # the same call ordered on a caller's stream: x is produced on that stream
+    # by a kernel the call must wait for
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        xs = torch.zeros_like(args[4])
+        xs.copy_(args[4])
+        third = _call(lib, *args[:4], xs, args[5], stream=C.c_void_p(side.cuda_stream))
+    assert third[0] == N.OK, third[2]
+    assert third[1] == first[1]
 
 
 def test_noalloc_residual_rejects_bad_sizes():
@@ -79,7 +95,20 @@ def test_noalloc_residual_rejects_bad_sizes():
     bad = _device([5], np.int32)  # column outside [0, n)
     rc, _, msg = _call(lib, 1, one, bad, v, v, v)
     assert rc == 9 and "column" in msg
+    # malformed row pointers: reversed ranges and ranges past row_ptrs[n] are
+    # flagged and skipped before any entry is read
+    col2 = _device([0, 1, 0, 1], np.int32)
+    v4 = _device([1.0, 2.0, 3.0, 4.0], np.float64)
+    x2 = _device([1.0, 1.0], np.float64)
+    for rows in ([0, 3, 2], [0, 5, 4], [-1, 2, 4], [0, 6, 4]):
+        rc, _, msg = _call(lib, 2, _device(rows, np.int32), col2, v4, x2, x2)
+        assert rc == 9 and "row_ptrs" in msg, (rows, msg)
+    rc, _, msg = _call(lib, 2, _device([0, 2, -1], np.int32), col2, v4, x2, x2)
+    assert rc == 9 and "negative" in msg
     # A = [[2]], x = [1], b = [4]: |4 - 2| / 4 = 0.5
     rc, val, msg = _call(lib, 1, one, col, v, _device([1.0], np.float64), _device([4.0], np.float64))
     assert rc == N.OK and abs(val - 0.5) < 1e-15, msg
+    # b = 0: the documented value is ||r||_2 itself, here |0 - 2 * 1.5| = 3
+    rc, val, msg = _call(lib, 1, one, col, v, _device([1.5], np.float64), _device([0.0], np.float64))
+    assert rc == N.OK and val == 3.0, msg
     torch.cuda.synchronize()

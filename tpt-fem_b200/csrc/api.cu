@@ -844,4 +844,16 @@ tptfem_status tptfem_topopt_element_stiffness(double nu, double h, double* ke) {
   return TPTFEM_OK;
 }
 
+tptfem_status tptfem_grf_eval(tptfem_context* ctx, const double* points, int64_t n, const double* w,
+                              const double* phi, int32_t n_features, double scale, double* out) {
+  if (!ctx || n < 0 || (n > 0 && (!points || !out)) || !w || !phi) return TPTFEM_ERR_INVALID_ARG;
+  if (n_features < 1 || n_features > GRF_MAX_FEATURES)
+    return fail(ctx, TPTFEM_ERR_INVALID_ARG, "n_features must be in 1..2048");
+  if (n == 0) return TPTFEM_OK;
+  API_TRY
+  set_device(ctx);
+  grf_eval(ctx, points, n, w, phi, n_features, scale, out);
+  API_CATCH(ctx)
+}
+
 }  // extern "C"

@@ -15,7 +15,10 @@
 // keeps the previous call's contents, so each call clears the ticket and flag
 // it needs at zero before launching, and calls whose kernels overlap on the
 // GPU (different streams, or several host threads) race on it and must be
-// serialised by the caller.
+// serialised by the caller.  The array's device address is looked up once per
+// device and cached; a call that fails with a device error drops the cached
+// address (and SM count), so the next call looks them up again -- after a
+// cudaDeviceReset, for instance.
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -99,14 +102,20 @@ constexpr int NOALLOC_SLOTS = NOALLOC_PARTIALS + 8;
 
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SLOTS];
 
+constexpr unsigned FLAG_COLUMN = 1u;  // a column index outside [0, n)
+constexpr unsigned FLAG_ROW = 2u;     // a row range outside [0, nnz] or reversed
+
 constexpr int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+int g_noalloc_sms[NOALLOC_MAX_DEVICES] = {};
 
-// Residual row sums as in residual_f64 (compensated), without storing r; a
-// column index outside [0, n) is flagged and skipped.
+// Residual row sums as in residual_f64 (compensated), without storing r.  A
+// row whose range [rp[row], rp[row+1]) is reversed or leaves [0, nnz), and a
+// column index outside [0, n), are flagged and skipped, so malformed arrays
+// never send a load outside the nnz entries the caller declared.
 template <int LANES>
-__global__ void __launch_bounds__(SPMV_THREADS) residual_norms_noalloc(int n, const int* __restrict__ rp,
+__global__ void __launch_bounds__(SPMV_THREADS) residual_norms_noalloc(int n, int nnz, const int* __restrict__ rp,
                                                                        const int* __restrict__ ci,
                                                                        const double* __restrict__ va,
                                                                        const double* __restrict__ x,
@@ -125,10 +134,14 @@ __global__ void __launch_bounds__(SPMV_THREADS) residual_norms_noalloc(int n, co
     const bool valid = row < n;
     double hi = 0.0, lo = 0.0;
     if (valid) {
-      const int kb = rp[row], ke = rp[row + 1];
+      int kb = rp[row], ke = rp[row + 1];
+      if (kb < 0 || ke > nnz || kb > ke) {
+        if (lane == 0) atomicOr(flag, FLAG_ROW);
+        kb = ke = 0;
+      }
       for (int k = kb + lane; k < ke; k += LANES) {
         const int c = ci[k];
-        if (c < 0 || c >= n) { atomicOr(flag, 1u); continue; }
+        if (c < 0 || c >= n) { atomicOr(flag, FLAG_COLUMN); continue; }
         double p, pe, s, se;
         two_prod(va[k], x[c], p, pe);
         two_sum(hi, p, s, se);
@@ -198,6 +211,7 @@ extern "C" tptfem_status tptfem_rel_residual_noalloc(int device, void* stream, i
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   do {
     double* scratch = nullptr;
+    int sms = 0;
     {
       // once per device, with that device current: the host-side symbol is only
       // a stand-in, the kernel needs the device address of the array
@@ -209,9 +223,17 @@ extern "C" tptfem_status tptfem_rel_residual_noalloc(int device, void* stream, i
           rc = TPTFEM_ERR_DEVICE;
           break;
         }
+        int count = 0;
+        if (cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || count < 1) {
+          put_err(err, err_len, "cannot read the device's multiprocessor count");
+          rc = TPTFEM_ERR_DEVICE;
+          break;
+        }
         g_noalloc_ptr[device] = static_cast<double*>(p);
+        g_noalloc_sms[device] = count;
       }
       scratch = g_noalloc_ptr[device];
+      sms = g_noalloc_sms[device];
     }
     int nnz = 0;
     if (cudaMemcpyAsync(&nnz, row_ptrs + n, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
@@ -220,10 +242,15 @@ extern "C" tptfem_status tptfem_rel_residual_noalloc(int device, void* stream, i
       rc = TPTFEM_ERR_DEVICE;
       break;
     }
+    if (nnz < 0) {
+      put_err(err, err_len, "row_ptrs[n] (the number of stored entries) is negative");
+      rc = TPTFEM_ERR_INVALID_ARG;
+      break;
+    }
     const double avg = (double)nnz / (double)n;
     const int lanes = avg <= 3 ? 2 : avg <= 12 ? 4 : avg <= 40 ? 8 : avg <= 96 ? 16 : 32;
     int grid = (int)std::min<int64_t>((n * lanes + SPMV_THREADS - 1) / SPMV_THREADS, NOALLOC_MAX_BLOCKS);
-    grid = std::max(1, std::min(grid, sm_count() * 8));
+    grid = std::max(1, std::min(grid, sms * 8));
     // the ticket and the flag must start at zero; partials are overwritten
     if (cudaMemsetAsync(scratch + NOALLOC_TICKET, 0, 2 * sizeof(double), s) != cudaSuccess) {
       put_err(err, err_len, "clearing the scratch array failed");
@@ -232,11 +259,11 @@ extern "C" tptfem_status tptfem_rel_residual_noalloc(int device, void* stream, i
     }
     const int nn = (int)n;
     switch (lanes) {
-      case 2: residual_norms_noalloc<2><<<grid, SPMV_THREADS, 0, s>>>(nn, row_ptrs, col_ind, values, x, b, scratch); break;
-      case 4: residual_norms_noalloc<4><<<grid, SPMV_THREADS, 0, s>>>(nn, row_ptrs, col_ind, values, x, b, scratch); break;
-      case 8: residual_norms_noalloc<8><<<grid, SPMV_THREADS, 0, s>>>(nn, row_ptrs, col_ind, values, x, b, scratch); break;
-      case 16: residual_norms_noalloc<16><<<grid, SPMV_THREADS, 0, s>>>(nn, row_ptrs, col_ind, values, x, b, scratch); break;
-      default: residual_norms_noalloc<32><<<grid, SPMV_THREADS, 0, s>>>(nn, row_ptrs, col_ind, values, x, b, scratch); break;
+      case 2: residual_norms_noalloc<2><<<grid, SPMV_THREADS, 0, s>>>(nn, nnz, row_ptrs, col_ind, values, x, b, scratch); break;
+      case 4: residual_norms_noalloc<4><<<grid, SPMV_THREADS, 0, s>>>(nn, nnz, row_ptrs, col_ind, values, x, b, scratch); break;
+      case 8: residual_norms_noalloc<8><<<grid, SPMV_THREADS, 0, s>>>(nn, nnz, row_ptrs, col_ind, values, x, b, scratch); break;
+      case 16: residual_norms_noalloc<16><<<grid, SPMV_THREADS, 0, s>>>(nn, nnz, row_ptrs, col_ind, values, x, b, scratch); break;
+      default: residual_norms_noalloc<32><<<grid, SPMV_THREADS, 0, s>>>(nn, nnz, row_ptrs, col_ind, values, x, b, scratch); break;
     }
     double out[4] = {0.0, 0.0, 0.0, 0.0};
     if (cudaGetLastError() != cudaSuccess ||
@@ -248,6 +275,11 @@ extern "C" tptfem_status tptfem_rel_residual_noalloc(int device, void* stream, i
     }
     unsigned bad = 0;
     std::memcpy(&bad, &out[3], sizeof(unsigned));
+    if (bad & FLAG_ROW) {
+      put_err(err, err_len, "row_ptrs is not non-decreasing within [0, row_ptrs[n]]");
+      rc = TPTFEM_ERR_INVALID_ARG;
+      break;
+    }
     if (bad) {
       put_err(err, err_len, "a column index is outside [0, n)");
       rc = TPTFEM_ERR_INVALID_ARG;
@@ -256,6 +288,12 @@ extern "C" tptfem_status tptfem_rel_residual_noalloc(int device, void* stream, i
     const double r2 = out[0], b2 = out[1];
     *rel_residual = b2 > 0.0 ? std::sqrt(r2) / std::sqrt(b2) : std::sqrt(r2);
   } while (false);
+  if (rc == TPTFEM_ERR_DEVICE) {
+    // the cached address may be stale (e.g. after a device reset): look it up again next time
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    g_noalloc_ptr[device] = nullptr;
+    g_noalloc_sms[device] = 0;
+  }
   cudaSetDevice(prev);
   return rc;
 }

@@ -302,6 +302,12 @@ void topopt_batch(tptfem_context* ctx, const tptfem_topopt_instance* in, int n, 
                   double* compliance, double* densities, tptfem_topopt_stats* stats);
 void topopt_element_stiffness(double nu, double h, double* ke);
 
+// grf.cu: random-Fourier-feature field scale * sum_m cos(w_m . x + phi_m) at n
+// host points (n x 3), w host 3 x M row-major, phi host M; result to host out.
+constexpr int GRF_MAX_FEATURES = 2048;
+void grf_eval(tptfem_context* ctx, const double* h_points, int64_t n, const double* h_w, const double* h_phi, int M,
+              double scale, double* h_out);
+
 }  // namespace tptfem
 
 struct tptfem_mesh {

@@ -453,6 +453,20 @@ def solve_with_dirichlet(mat, rhs, bcs, **kw):
     return u, st.as_dict()
 
 
+def grf_eval(points, w, phi, scale, ctx=None):
+    """scale * sum_m cos(w[:, m] . x + phi[m]) at each row x of points (n x 3),
+    evaluated on the GPU in a fixed operation order (tptfem_grf_eval)."""
+    ctx = _ctx(ctx)
+    pts = N.f64(points).reshape(-1, 3)
+    w = N.f64(w).reshape(3, -1)
+    phi = N.f64(phi)
+    assert w.shape[1] == len(phi)
+    out = np.zeros(len(pts))
+    ctx.check(ctx.lib.tptfem_grf_eval(ctx.h, N.ptr(pts), len(pts), N.ptr(w), N.ptr(phi), len(phi), float(scale),
+                                      N.ptr(out)))
+    return out
+
+
 class PoissonSolution:
     def __init__(self, mesh, values, stats):
         self.mesh, self.values, self.stats = mesh, values, stats

@@ -78,6 +78,8 @@ SIGNATURES = {
     "tptfem_topopt_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p]),
     "tptfem_topopt_element_stiffness": (C.c_int, [C.c_double, C.c_double, C.c_void_p]),
+    "tptfem_grf_eval": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_double,
+                                  C.c_void_p]),
     "tptfem_version": (C.c_char_p, []),
     "tptfem_create": (C.c_int, [C.c_int, _pp]),
     "tptfem_destroy": (None, [_vp]),

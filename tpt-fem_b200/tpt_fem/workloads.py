@@ -64,28 +64,10 @@ def tet_centroids(coords, conn):
     return coords[conn].mean(axis=1)
 
 
-def grf_at_centroids(coords, conn, seed, length=0.1, n_features=1024):
-    """grf_log_conductivity at the element centroids (computed on the GPU through
-    torch when one is available: input generation only)."""
-    try:
-        import torch
-        if torch.cuda.is_available():
-            rng = np.random.default_rng(seed)
-            w = rng.standard_normal((3, n_features)) / length
-            phi = rng.uniform(0.0, 2.0 * np.pi, n_features)
-            scale = np.sqrt(2.0 / n_features)
-            ct = torch.as_tensor(coords, device="cuda")
-            et = torch.as_tensor(conn, device="cuda")
-            wt = torch.as_tensor(w, device="cuda")
-            pt = torch.as_tensor(phi, device="cuda")
-            out = torch.empty(len(conn), dtype=torch.float64, device="cuda")
-            for a in range(0, len(conn), 1 << 20):
-                x = ct[et[a:a + (1 << 20)]].mean(dim=1)
-                out[a:a + len(x)] = torch.cos(x @ wt + pt).sum(dim=1) * scale
-            return out.cpu().numpy()
-    except ImportError:
-        pass
-    return grf_log_conductivity(tet_centroids(coords, conn), seed, length, n_features)
+def grf_at_centroids(coords, conn, seed, ctx=None, length=0.1, n_features=1024):
+    """grf_log_conductivity at the element centroids (mean of the element's
+    nodes, numpy)."""
+    return grf_log_conductivity(tet_centroids(coords, conn), seed, ctx, length, n_features)
 
 
 class GrfPoisson:
@@ -105,7 +87,8 @@ class GrfPoisson:
         self.bcs = [(int(i), 0.0) for i in on_b]
 
     def matrix(self, seed):
-        return self.F.assemble_poisson(self.mesh, np.exp(grf_at_centroids(self.coords, self.conn, seed)), 2)
+        k = np.exp(grf_at_centroids(self.coords, self.conn, seed, self.mesh.ctx))
+        return self.F.assemble_poisson(self.mesh, k, 2)
 
     def system(self, seed):
         return self.F.reduce_system(self.matrix(seed), self.rhs, self.bcs)
@@ -116,32 +99,18 @@ def grf_poisson_system(ctx, n, seed):
     return GrfPoisson(ctx, n).system(seed)
 
 
-def grf_log_conductivity(points, seed, length=0.1, n_features=1024):
+def grf_log_conductivity(points, seed, ctx=None, length=0.1, n_features=1024):
     """Seeded Gaussian random field (mean 0, variance 1, squared-exponential
     correlation of length `length`) by random Fourier features:
     g(x) = sqrt(2/M) sum_m cos(w_m . x + phi_m), w_m ~ N(0, length^-2 I),
-    phi_m ~ U[0, 2 pi) (numpy PCG64 stream of `seed`).  Evaluated on the GPU
-    through torch when one is available (input generation only)."""
+    phi_m ~ U[0, 2 pi) drawn from numpy's PCG64 stream of `seed`.  The sum is
+    evaluated by the library (tptfem_grf_eval, one fixed operation order), so
+    a seed gives the same field on every host."""
+    import tpt_fem as F
     rng = np.random.default_rng(seed)
     w = rng.standard_normal((3, n_features)) / length
     phi = rng.uniform(0.0, 2.0 * np.pi, n_features)
-    scale = np.sqrt(2.0 / n_features)
-    try:
-        import torch
-        if torch.cuda.is_available():
-            out = np.empty(len(points))
-            wt = torch.as_tensor(w, device="cuda")
-            pt = torch.as_tensor(phi, device="cuda")
-            for a in range(0, len(points), 1 << 20):
-                x = torch.as_tensor(points[a:a + (1 << 20)], device="cuda")
-                out[a:a + len(x)] = (torch.cos(x @ wt + pt).sum(dim=1) * scale).cpu().numpy()
-            return out
-    except ImportError:
-        pass
-    out = np.empty(len(points))
-    for a in range(0, len(points), 1 << 14):
-        out[a:a + (1 << 14)] = np.cos(points[a:a + (1 << 14)] @ w + phi).sum(axis=1) * scale
-    return out
+    return F.grf_eval(points, w, phi, np.sqrt(2.0 / n_features), ctx=ctx)
 
 
 CANTILEVERS = {
