@@ -342,8 +342,11 @@ bool elasticity_element_matrix(const OMesh& m, i64 eid, int model, double young,
   return true;
 }
 
-// elasticity_body_vector (elasticity:312-348) for a constant body force.
-bool elasticity_body_vector(const OMesh& m, i64 eid, const double* body, int qo, vector<double>& f) {
+// elasticity_body_vector (elasticity:312-348) with the body force given as a
+// callback of the physical quadrature point (or a constant when cb == nullptr).
+typedef void (*body_cb)(const double* x, int dim, double* out, void* ud);
+bool elasticity_body_vector(const OMesh& m, i64 eid, const double* body, body_cb cb, void* ud, int qo,
+                            vector<double>& f) {
   auto phys = elem_phys(m, eid);
   int dim = ref_dim(m.cell);
   size_t n = phys.size();
@@ -356,8 +359,16 @@ bool elasticity_body_vector(const OMesh& m, i64 eid, const double* body, int qo,
     auto local = ref_grad(m.cell, qp[q]);
     Map mp = map_from(phys, local);
     double det = std::fabs(mp.det);
+    vector<double> x(phys[0].size(), 0.0), bq(3, 0.0);
+    const double* b = body;
+    if (cb) {
+      for (size_t k = 0; k < n; ++k)
+        for (size_t d = 0; d < x.size(); ++d) x[d] += ns[k] * phys[k][d];
+      cb(x.data(), (int)x.size(), bq.data(), ud);
+      b = bq.data();
+    }
     for (size_t i = 0; i < n; ++i)
-      for (int a = 0; a < dim; ++a) f[i * dim + a] += w * ns[i] * body[a] * det;
+      for (int a = 0; a < dim; ++a) f[i * dim + a] += w * ns[i] * b[a] * det;
   }
   return true;
 }
@@ -1023,7 +1034,19 @@ int orc_load_body(OrcMesh* h, const double* body, int qo, double* rhs) {
   int dim = ref_dim(h->m.cell);
   vector<double> f;
   for (size_t e = 0; e < h->m.elems.size(); ++e) {
-    if (!elasticity_body_vector(h->m, (i64)e, body, qo, f)) return 1;
+    if (!elasticity_body_vector(h->m, (i64)e, body, nullptr, nullptr, qo, f)) return 1;
+    for (size_t i = 0; i < h->m.elems[e].size(); ++i)
+      for (int a = 0; a < dim; ++a) rhs[h->m.elems[e][i] * dim + a] += f[i * dim + a];
+  }
+  return 0;
+}
+
+// The same with a body-force callback of the quadrature point.
+int orc_load_body_cb(OrcMesh* h, body_cb cb, void* ud, int qo, double* rhs) {
+  int dim = ref_dim(h->m.cell);
+  vector<double> f;
+  for (size_t e = 0; e < h->m.elems.size(); ++e) {
+    if (!elasticity_body_vector(h->m, (i64)e, nullptr, cb, ud, qo, f)) return 1;
     for (size_t i = 0; i < h->m.elems[e].size(); ++i)
       for (int a = 0; a < dim; ++a) rhs[h->m.elems[e][i] * dim + a] += f[i * dim + a];
   }
@@ -1087,72 +1110,96 @@ int orc_solve_with_dirichlet(OrcCoo* c, const double* rhs, i64 n, const i64* bc_
 
 // ---- CPU Jacobi-PCG ------------------------------------------------------------
 // NOT reference code: the reference has no iterative solver.  This is the CPU
-// restatement of the plain method the GPU library runs (FP64 Jacobi-PCG, stop at
-// ||b - A x||_2 / ||b||_2 <= tol on the recursively updated residual), used as
-// the oracle for large systems and as the timed CPU baseline.  `nthreads` <= 0
-// uses every OpenMP thread.  Returns iterations; *relres gets the TRUE final
-// relative residual.  When max_it is reached before tol the return is -(iters).
-i64 orc_pcg_jacobi(i64 n, const i64* rp, const i64* ci, const double* va, const double* b, double* x, double tol,
-                   i64 max_it, int nthreads, double* relres) {
+// restatement of the plain method the GPU library runs, FP64 Jacobi-PCG, used
+// as the oracle for large systems and as the timed CPU baseline.  Like the GPU
+// solver it stops on the TRUE relative residual ||b - A x||_2 / ||b||_2 <= tol:
+// the recursion runs until its updated residual meets tol, then the true
+// residual is computed, and if that still exceeds tol the recursion restarts
+// from it (at most 8 restarts).  `nthreads` <= 0 uses every OpenMP thread.
+// Returns the total iterations, negated when max_it was reached first;
+// *relres gets the true final relative residual.
+}  // extern "C"
+template <typename I>
+i64 pcg_jacobi(i64 n, const I* rp, const I* ci, const double* va, const double* b, double* x, double tol, i64 max_it,
+               int nthreads, double* relres) {
 #ifdef _OPENMP
-  if (nthreads > 0) omp_set_num_threads(nthreads);
+  // every call sets its own team size, so a one-thread call leaves no residue
+  omp_set_num_threads(nthreads > 0 ? nthreads : omp_get_num_procs());
 #endif
   vector<double> r(n), z(n), p(n), q(n), dinv(n);
   double bb = 0.0;
 #pragma omp parallel for reduction(+ : bb) schedule(static)
   for (i64 i = 0; i < n; ++i) {
     double d = 0.0;
-    for (i64 k = rp[i]; k < rp[i + 1]; ++k) if (ci[k] == i) d += va[k];
+    for (i64 k = rp[i]; k < rp[i + 1]; ++k) if ((i64)ci[k] == i) d += va[k];
     dinv[i] = 1.0 / d;
     x[i] = 0.0;
     r[i] = b[i];
-    z[i] = dinv[i] * r[i];
-    p[i] = z[i];
     bb += b[i] * b[i];
   }
-  double bnorm = std::sqrt(bb);
+  const double bnorm = std::sqrt(bb);
   if (bnorm == 0.0) { if (relres) *relres = 0.0; return 0; }
-  double rz = 0.0;
-#pragma omp parallel for reduction(+ : rz) schedule(static)
-  for (i64 i = 0; i < n; ++i) rz += r[i] * z[i];
   i64 it = 0;
-  double rr = bb;
-  while (std::sqrt(rr) > tol * bnorm && it < max_it) {
-    double pq = 0.0;
+  double res = bb;
+  for (int restart = 0;; ++restart) {
+    double rz = 0.0, rr = 0.0;
+#pragma omp parallel for reduction(+ : rz, rr) schedule(static)
+    for (i64 i = 0; i < n; ++i) {
+      z[i] = dinv[i] * r[i];
+      p[i] = z[i];
+      rz += r[i] * z[i];
+      rr += r[i] * r[i];
+    }
+    while (std::sqrt(rr) > tol * bnorm && it < max_it) {
+      double pq = 0.0;
 #pragma omp parallel for reduction(+ : pq) schedule(static)
+      for (i64 i = 0; i < n; ++i) {
+        double s = 0.0;
+        for (i64 k = rp[i]; k < rp[i + 1]; ++k) s += va[k] * p[ci[k]];
+        q[i] = s;
+        pq += p[i] * s;
+      }
+      const double alpha = rz / pq;
+      double rz_new = 0.0, rr_new = 0.0;
+#pragma omp parallel for reduction(+ : rz_new, rr_new) schedule(static)
+      for (i64 i = 0; i < n; ++i) {
+        x[i] += alpha * p[i];
+        r[i] -= alpha * q[i];
+        z[i] = dinv[i] * r[i];
+        rz_new += r[i] * z[i];
+        rr_new += r[i] * r[i];
+      }
+      const double beta = rz_new / rz;
+      rz = rz_new;
+      rr = rr_new;
+#pragma omp parallel for schedule(static)
+      for (i64 i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+      ++it;
+    }
+    res = 0.0;
+#pragma omp parallel for reduction(+ : res) schedule(static)
     for (i64 i = 0; i < n; ++i) {
       double s = 0.0;
-      for (i64 k = rp[i]; k < rp[i + 1]; ++k) s += va[k] * p[ci[k]];
-      q[i] = s;
-      pq += p[i] * s;
+      for (i64 k = rp[i]; k < rp[i + 1]; ++k) s += va[k] * x[ci[k]];
+      r[i] = b[i] - s;
+      res += r[i] * r[i];
     }
-    double alpha = rz / pq;
-    double rz_new = 0.0, rr_new = 0.0;
-#pragma omp parallel for reduction(+ : rz_new, rr_new) schedule(static)
-    for (i64 i = 0; i < n; ++i) {
-      x[i] += alpha * p[i];
-      r[i] -= alpha * q[i];
-      z[i] = dinv[i] * r[i];
-      rz_new += r[i] * z[i];
-      rr_new += r[i] * r[i];
-    }
-    double beta = rz_new / rz;
-    rz = rz_new;
-    rr = rr_new;
-#pragma omp parallel for schedule(static)
-    for (i64 i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
-    ++it;
-  }
-  double res = 0.0;
-#pragma omp parallel for reduction(+ : res) schedule(static)
-  for (i64 i = 0; i < n; ++i) {
-    double s = 0.0;
-    for (i64 k = rp[i]; k < rp[i + 1]; ++k) s += va[k] * x[ci[k]];
-    double d = b[i] - s;
-    res += d * d;
+    if (std::sqrt(res) <= tol * bnorm || it >= max_it || restart >= 8) break;
   }
   if (relres) *relres = std::sqrt(res) / bnorm;
-  return std::sqrt(rr) > tol * bnorm ? -it : it;
+  return std::sqrt(res) > tol * bnorm ? -it : it;
+}
+extern "C" {
+
+i64 orc_pcg_jacobi(i64 n, const i64* rp, const i64* ci, const double* va, const double* b, double* x, double tol,
+                   i64 max_it, int nthreads, double* relres) {
+  return pcg_jacobi<i64>(n, rp, ci, va, b, x, tol, max_it, nthreads, relres);
+}
+// The same with int32 row pointers and columns (12 bytes per stored entry
+// instead of 16: the form a tuned CPU solver would use).
+i64 orc_pcg_jacobi_i32(i64 n, const int32_t* rp, const int32_t* ci, const double* va, const double* b, double* x,
+                       double tol, i64 max_it, int nthreads, double* relres) {
+  return pcg_jacobi<int32_t>(n, rp, ci, va, b, x, tol, max_it, nthreads, relres);
 }
 
 // Map::from_nodes_and_grad at reference point xi (element:702-724).
@@ -1234,7 +1281,7 @@ OrcCsr* orc_fsai(i64 n, const i64* rp, const i64* ci, const double* va, const i6
 
 int orc_max_threads() {
 #ifdef _OPENMP
-  return omp_get_max_threads();
+  return omp_get_num_procs();
 #else
   return 1;
 #endif

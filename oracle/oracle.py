@@ -23,11 +23,13 @@ DIM_OF_CELL = {CELL_LINE: 1, CELL_TRI: 2, CELL_QUAD: 2, CELL_TET: 3}
 
 _i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _vp = C.c_void_p
 _i64 = C.c_int64
 
 SOURCE_CB = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_int, C.c_void_p)
 FLUX_CB = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, C.c_void_p)
+BODY_CB = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.c_void_p)
 
 
 def build() -> str:
@@ -76,6 +78,7 @@ def lib():
         "orc_load_poisson_source": (C.c_int, [_vp, C.c_double, C.c_int, _f64p]),
         "orc_load_poisson_source_cb": (C.c_int, [_vp, SOURCE_CB, _vp, C.c_int, _f64p]),
         "orc_load_body": (C.c_int, [_vp, _f64p, C.c_int, _f64p]),
+        "orc_load_body_cb": (C.c_int, [_vp, BODY_CB, _vp, C.c_int, _f64p]),
         "orc_apply_neumann_cb": (None, [_vp, C.c_int, FLUX_CB, _vp, C.c_int, C.c_uint, _f64p]),
         "orc_apply_robin": (None, [_vp, _vp, C.c_int, C.c_int, C.c_double, C.c_double]),
         "orc_apply_robin_cb": (None, [_vp, _vp, C.c_int, FLUX_CB, _vp, C.c_int]),
@@ -90,6 +93,8 @@ def lib():
         "orc_solve_with_dirichlet": (C.c_int, [_vp, _f64p, _i64, _i64p, _f64p, _i64, _f64p]),
         "orc_pcg_jacobi": (_i64, [_i64, _i64p, _i64p, _f64p, _f64p, _f64p, C.c_double, _i64, C.c_int,
                                   C.POINTER(C.c_double)]),
+        "orc_pcg_jacobi_i32": (_i64, [_i64, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double, _i64, C.c_int,
+                                      C.POINTER(C.c_double)]),
         "orc_max_threads": (C.c_int, []),
         "orc_map": (None, [C.c_int, _f64p, C.c_int, C.c_int, _f64p, _f64p, C.POINTER(C.c_double), _f64p]),
         "orc_cell_quad": (C.c_int, [C.c_int, C.c_int, _f64p, _f64p]),
@@ -349,9 +354,20 @@ def load_poisson_source(mesh, source, quad_order):
 
 
 def load_body(mesh, body, quad_order):
+    """Body-force load loop of solve_elasticity (elasticity:371-379); body is a
+    constant vector or a callable body(*x) -> sequence of dim values, called
+    with the point's coordinates as arguments (like the source callbacks)."""
     dim = DIM_OF_CELL[mesh.cell]
     rhs = np.zeros(mesh.n_nodes * dim)
-    if lib().orc_load_body(mesh.h, np.ascontiguousarray(body, dtype=np.float64), quad_order, rhs):
+    if callable(body):
+        def cb(xp, cdim, out, _ud):
+            v = body(*[xp[i] for i in range(cdim)])
+            for a in range(dim):
+                out[a] = float(v[a])
+        rc = lib().orc_load_body_cb(mesh.h, BODY_CB(cb), None, quad_order, rhs)
+    else:
+        rc = lib().orc_load_body(mesh.h, np.ascontiguousarray(body, dtype=np.float64), quad_order, rhs)
+    if rc:
         raise OracleError("bad quadrature order")
     return rhs
 
@@ -433,7 +449,8 @@ def solve_with_dirichlet(coo, rhs, bcs):
 
 
 def pcg_jacobi(csr, b, tol=1e-10, max_it=100000, nthreads=0):
-    """CPU FP64 Jacobi-PCG (not reference code; see oracle.cpp).
+    """CPU FP64 Jacobi-PCG (not reference code; see oracle.cpp), stopping on
+    the true relative residual.
 
     Returns (x, iterations, true relative residual); iterations < 0 means
     max_it was reached first.
@@ -443,6 +460,19 @@ def pcg_jacobi(csr, b, tol=1e-10, max_it=100000, nthreads=0):
     rel = C.c_double()
     it = lib().orc_pcg_jacobi(csr.nrows, csr.row_ptrs, csr.col_ind, csr.values, b, x, tol, max_it, nthreads,
                               C.byref(rel))
+    return x, int(it), rel.value
+
+
+def pcg_jacobi_i32(n, row_ptrs, col_ind, values, b, tol=1e-10, max_it=100000, nthreads=0):
+    """pcg_jacobi on int32 CSR arrays (12 bytes per stored entry).
+    Returns (x, iterations, true relative residual)."""
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.zeros(n)
+    rel = C.c_double()
+    it = lib().orc_pcg_jacobi_i32(n, np.ascontiguousarray(row_ptrs, dtype=np.int32),
+                                  np.ascontiguousarray(col_ind, dtype=np.int32),
+                                  np.ascontiguousarray(values, dtype=np.float64), b, x, tol, max_it, nthreads,
+                                  C.byref(rel))
     return x, int(it), rel.value
 
 

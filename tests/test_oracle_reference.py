@@ -225,9 +225,15 @@ def test_pcg_jacobi_matches_dense_lu_on_poisson_box8():
     f = O.load_poisson_source(m, 1.0, 2)
     kred, fred, free = O.reduce_system(coo, f, unit_cube_bcs(c))
     x_lu = O.solve(kred, fred)
-    x, it, rel = O.pcg_jacobi(kred.to_csr(), fred, tol=1e-13)
-    assert it > 0 and rel < 1e-12
+    csr = kred.to_csr()
+    x, it, rel = O.pcg_jacobi(csr, fred, tol=1e-13)
+    assert it > 0 and rel < 1e-13
     assert np.max(np.abs(x - x_lu)) < 1e-12 * np.max(np.abs(x_lu))
+    # the int32-index form is the same arithmetic, bit for bit
+    x32, it32, rel32 = O.pcg_jacobi_i32(csr.nrows, csr.row_ptrs, csr.col_ind, csr.values, fred, tol=1e-13,
+                                        nthreads=1)
+    x1, it1, rel1 = O.pcg_jacobi(csr, fred, tol=1e-13, nthreads=1)
+    assert (it32, rel32) == (it1, rel1) and np.array_equal(x32, x1)
 
 
 def test_robin_conserves_total_measure():  # assembly:835
