@@ -209,22 +209,38 @@ NBS_TRAFFIC_200 = (359.652352 + 12.161024) * 1e6
 NBS_GROUPS_200 = 520200
 
 
-def e2e_once(F, LF, W, ctx, solver, host, model, coarse):
+def e2e_once(F, LF, W, ctx, solver, host, model, coarse, phases=None):
     """Host arrays -> C ABI -> host solution; returns (seconds, h2d bytes, d2h bytes, stats).
     Mesh upload, assembly, traction, Dirichlet reduction, the learned factor and
-    the solve all run inside the timed region."""
+    the solve all run inside the timed region.  With `phases` (a dict), each
+    step is synchronised and its wall time recorded there (an untimed run)."""
     coords, conn, E, dof, val = host
     cuda_sync()
     t0 = time.perf_counter()
+    last = [t0]
+
+    def mark(name):
+        if phases is not None:
+            ctx.synchronize()
+            t = time.perf_counter()
+            phases[name] = round((t - last[0]) * 1e3, 2)
+            last[0] = t
+
     mesh = F.Mesh.from_arrays(F.CELL_TET4, coords, conn, ctx=ctx)
+    mark("mesh_upload")
     K = F.assemble_elasticity(mesh, "3d", E, 0.3, 2)
+    mark("assembly")
     rhs = F.apply_traction(mesh, 3, 0, 1.0, [0.0, 0.0, -1e-3], np.zeros(K.nrows))
+    mark("traction")
     S = F.reduce_system(K, rhs, list(zip(dof, val)))
+    mark("reduction")
     if solver == F.SOLVER_LEARNED_FSAI_PCG:
         model.attach(S)
     st = S.solve(solver=solver, tol=TOL, fresh_setup=True, coarse=coarse)
+    mark("first_solve")
     u = S.solution()
     ctx.synchronize()
+    mark("solution_download")
     dt = time.perf_counter() - t0
     h2d = coords.nbytes + conn.nbytes + E.nbytes + 2 * rhs.nbytes + dof.nbytes + val.nbytes
     d2h = u.nbytes + rhs.nbytes
@@ -299,6 +315,8 @@ def run_ours(args, world, rank, local):
         conn = mesh.conn_array.copy()
         e2e = [e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model, coarse) for _ in range(2)]
         e2e_s, h2d, d2h, e2e_st = min(e2e, key=lambda t: t[0])
+        phases = {}
+        e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model, coarse, phases)
         # the plain method on the host cores: one complete solve of this exact
         # system, measured (no scaling), and the one-core iteration cost
         sysh = host_system(S)
@@ -344,7 +362,8 @@ def run_ours(args, world, rank, local):
             "speedup_vs_fp64_jacobi": seconds(jac) / step_s,
             "speedup_vs_fp64_jacobi_node_block": seconds(jac_nb) / step_s,
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "iterations": e2e_st["iterations"]},
+                    "iterations": e2e_st["iterations"], "runs_s": [round(t[0], 4) for t in e2e],
+                    "phases_ms_untimed_run": phases},
             "roofline": {"bound": "hbm", "kernel": op_name, "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "traffic_source": "ncu dram__bytes_read+write of nb_spmv_sym at "
@@ -365,6 +384,36 @@ def run_ours(args, world, rank, local):
             "wall_s_timed_region": t_wall,
         }
     return out
+
+
+def run_cantilever_sizes(args, world, rank, local):
+    """The cantilever family at its other sizes: [200,50,50] (1.56M free dofs)
+    and [400,100,100] (12.27M free dofs), same density recipe, clamp and
+    traction.  Per size: the headline solver (learned FSAI + coarse space,
+    fresh set-up) and FP64 Jacobi-PCG (node-block operator), each to the FP64
+    relative residual 1e-10, one untimed warm-up solve then one timed solve."""
+    import tpt_fem as F
+    from tpt_fem import lfsai as LF
+    from tpt_fem import workloads as W
+    ctx = F.Context(local)
+    model = LF.LearnedFsai.load(ctx, WEIGHTS)
+    out = {}
+    for name in ("cantilever_200x50x50", "cantilever_400x100x100"):
+        mesh, K, S, E, rhs, dof, val = build_system(F, W, ctx, W.CANTILEVERS[name][2])
+        model.attach(S)
+        rec = {"mesh": W.CANTILEVERS[name][2], "free_dofs": int(S.n_free), "nnz_reduced": int(S.nnz)}
+        for meth, kw in (("learned_coarse", dict(solver=F.SOLVER_LEARNED_FSAI_PCG, coarse=True)),
+                         ("fp64_jacobi_node_block", dict(solver=F.SOLVER_JACOBI_PCG))):
+            S.solve(tol=TOL, fresh_setup=True, **kw)
+            barrier(world)
+            st = S.solve(tol=TOL, fresh_setup=True, **kw)
+            rec[meth] = {"seconds": barrier_max(seconds(st), world), "iterations": st["iterations"],
+                         "rel_residual": st["rel_residual"], "setup_ms": st["setup_ms"],
+                         "fell_back": st["fell_back"]}
+        rec["speedup"] = rec["fp64_jacobi_node_block"]["seconds"] / rec["learned_coarse"]["seconds"]
+        out[name] = rec
+        del mesh, K, S
+    return out if rank == 0 else None
 
 
 CUBE_TOL_REF = 1e-12  # the FP64 reference solution the cube's solutions are measured against
@@ -749,7 +798,8 @@ def main():
         if not (args.headline_only or args.profile):
             # every other configuration, measured in the same run (records beside the headline)
             sub = {"cube_elasticity_64": run_cube, "assembly_cantilever_280x70x70": run_assembly,
-                   "poisson_grf_128": run_poisson_grf, "topopt_batch": run_topopt}
+                   "poisson_grf_128": run_poisson_grf, "topopt_batch": run_topopt,
+                   "cantilever_other_sizes": run_cantilever_sizes}
             recs = {name: fn(args, world, rank, local) for name, fn in sub.items()}
             if rank == 0:
                 out["configs"] = recs

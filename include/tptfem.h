@@ -226,6 +226,66 @@ tptfem_status tptfem_load_body(tptfem_context* ctx, tptfem_mesh* mesh, const dou
 tptfem_status tptfem_apply_traction(tptfem_context* ctx, tptfem_mesh* mesh, int dofs_per_node, int axis,
                                     double sign, const double* traction, double* rhs);
 
+/* ---- caller-evaluated sources and fluxes (the reference's closures) --------------
+ * The reference takes the volumetric source, the body force, the Neumann flux and the
+ * Robin coefficient as Rust closures of the physical point (and of the outward unit
+ * normal on the boundary): solve_poisson (crates/tpt-fem-thermal/src/lib.rs:206-240),
+ * solve_elasticity (crates/tpt-fem-elasticity/src/lib.rs:355-381), apply_neumann and
+ * apply_robin (crates/tpt-fem-assembly/src/lib.rs:591-753).  Across this ABI a closure
+ * becomes its values at the points where the reference would call it: query the points,
+ * evaluate on the host, pass the values; or pass a C function and let the library do so.
+ *
+ * Element points: n_elems * nq points, point q of element e at index e * nq + q, with
+ * x = sum_k N_k(xi_q) X_k over every stored coordinate (coord_dim values), as
+ * poisson_source_vector / elasticity_body_vector form it (thermal:163-196,
+ * elasticity:312-348).  *nq is written always; points (n_elems * nq * coord_dim
+ * doubles) only when non-NULL. */
+tptfem_status tptfem_mesh_quadrature_points(tptfem_context* ctx, tptfem_mesh* mesh, int quad_order, int32_t* nq,
+                                            double* points);
+/* Boundary points: every boundary face (boundary_faces order, assembly:563-583: by element,
+ * then by the cell's face index) and its face-rule points (assembly:336-358), with the
+ * outward unit normal of the face (assembly:394-420, 617-653).  *n_points is written
+ * always; x and normal (n_points * dim doubles each, dim = 3 for Tet4, 2 for Tri3/Quad4)
+ * when non-NULL.  Needs coord_dim == dim (TPTFEM_ERR_INVALID_ARG otherwise). */
+tptfem_status tptfem_mesh_boundary_points(tptfem_context* ctx, tptfem_mesh* mesh, int64_t* n_points, double* x,
+                                          double* normal);
+/* rhs[n_nodes] = the Poisson load loop (thermal:224-230) with the source given at every
+ * element point (n_elems * nq values). */
+tptfem_status tptfem_load_poisson_source_points(tptfem_context* ctx, tptfem_mesh* mesh, const double* source,
+                                                int quad_order, double* rhs);
+/* rhs[n_nodes*dim] = the body-force loop (elasticity:371-379) with the body force given at
+ * every element point (n_elems * nq * dim values, component-fastest). */
+tptfem_status tptfem_load_body_points(tptfem_context* ctx, tptfem_mesh* mesh, const double* body, int quad_order,
+                                      double* rhs);
+/* rhs += apply_neumann (assembly:591-667) with g given at every boundary point; as in the
+ * reference the scalar g is applied to each of the dofs_per_node components, here those
+ * whose bit is set in comp_mask (all: 0xFFFFFFFF). */
+tptfem_status tptfem_apply_neumann_points(tptfem_context* ctx, tptfem_mesh* mesh, int dofs_per_node, const double* g,
+                                          uint32_t comp_mask, double* rhs);
+/* assemble(mesh, 1, poisson_element_matrix) followed by apply_robin(mesh, 1, h, coo)
+ * (assembly:684-753) with h given at every boundary point. */
+tptfem_status tptfem_assemble_poisson_robin_points(tptfem_context* ctx, tptfem_mesh* mesh, const double* conductivity,
+                                                   int per_element, int quad_order, const double* h,
+                                                   tptfem_matrix** out);
+/* The closures as C functions.  `x` holds coord_dim values, `normal` dim values; a body
+ * force writes dim values to `out`.  The library calls them on the calling thread, once per
+ * point, in point order; values must be finite. */
+typedef double (*tptfem_source_fn)(const double* x, int dim, void* user);
+typedef double (*tptfem_flux_fn)(const double* x, const double* normal, int dim, void* user);
+typedef void (*tptfem_body_fn)(const double* x, int dim, double* out, void* user);
+/* solve_poisson (thermal:206-240) with its closures: source(x), optional Neumann flux
+ * g(x, n) and Robin coefficient h(x, n) (NULL: none).  u has n_nodes entries. */
+tptfem_status tptfem_solve_poisson_fn(tptfem_context* ctx, tptfem_mesh* mesh, double conductivity, int quad_order,
+                                      tptfem_source_fn source, void* source_user, const int64_t* bc_dof,
+                                      const double* bc_val, int64_t nbc, tptfem_flux_fn neumann,
+                                      void* neumann_user, tptfem_flux_fn robin, void* robin_user,
+                                      const tptfem_solver_opts* opts, double* u, tptfem_solve_stats* stats);
+/* solve_elasticity (elasticity:355-381) with the body force as a closure of x. */
+tptfem_status tptfem_solve_elasticity_fn(tptfem_context* ctx, tptfem_mesh* mesh, int model, double young,
+                                         double poisson, int quad_order, tptfem_body_fn body, void* body_user,
+                                         const int64_t* bc_dof, const double* bc_val, int64_t nbc,
+                                         const tptfem_solver_opts* opts, double* u, tptfem_solve_stats* stats);
+
 /* ---- row-partitioned solve over several GPUs ---------------------------------------
  * No counterpart in the reference (its solve is single-threaded).  The reduced system is
  * split into contiguous row ranges row_starts[k] .. row_starts[k+1] (node-aligned: the

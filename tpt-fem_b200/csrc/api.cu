@@ -68,6 +68,7 @@ void check_coef(const double* coef, int64_t count, const char* what) {
 struct RobinSpec {
   int on = 0, axis = -1;
   double sign = 1.0, h = 0.0;
+  const double* pts = nullptr;  // host h(x, n) per boundary-face point (replaces the selector)
 };
 
 std::unique_ptr<MatrixData> new_matrix(tptfem_context* ctx, tptfem_mesh* mesh, int physics, int model,
@@ -96,8 +97,78 @@ std::unique_ptr<MatrixData> new_matrix(tptfem_context* ctx, tptfem_mesh* mesh, i
   M->robin_axis = robin.axis;
   M->robin_sign = robin.sign;
   M->robin_h = robin.h;
+  if (robin.on && robin.pts) {
+    mesh_build_face_offsets(m);
+    const size_t np = (size_t)m.n_bfaces * face_point_count(m.cell);
+    M->robin_pts.alloc(std::max<size_t>(np, 1), ctx->stream);
+    TPT_REQUIRE(host_to_device_finite(ctx, M->robin_pts.p, robin.pts, np), TPTFEM_ERR_INVALID_ARG,
+                "robin coefficient holds a non-finite value");
+  }
   assemble_matrix(*M);
   return M;
+}
+
+void check_quad_order(const MeshData& m, int quad_order) {
+  if (m.cell == TPTFEM_CELL_QUAD4)  // Tet4 and Tri3 use one fixed rule and ignore quad_order
+    TPT_REQUIRE(quad_order >= 1 && quad_order <= 5, TPTFEM_ERR_INVALID_ARG, "quad_order must be in 1..=5");
+}
+
+int mesh_sd(const MeshData& m) { return m.cell == TPTFEM_CELL_TET4 ? 3 : 2; }
+
+// Element quadrature points on the host (n_elems * nq * cdim).
+std::vector<double> host_quad_points(tptfem_context* ctx, MeshData& m, int quad_order, int& nq) {
+  nq = cell_point_count(m.cell, quad_order);
+  const size_t n = (size_t)m.n_elems * nq * m.cdim;
+  std::vector<double> h(n);
+  DevBuf<double> d;
+  d.alloc(std::max<size_t>(n, 1), ctx->stream);
+  mesh_quad_points(m, quad_order, d.p);
+  device_to_host(ctx, h.data(), d.p, n * sizeof(double));
+  return h;
+}
+
+// Boundary-face points and normals on the host (n_points * sd each).
+void host_face_points(tptfem_context* ctx, MeshData& m, std::vector<double>& x, std::vector<double>& nrm) {
+  TPT_REQUIRE(m.cdim == mesh_sd(m), TPTFEM_ERR_INVALID_ARG,
+              "boundary points need as many stored coordinates as the cell's dimension");
+  mesh_build_face_offsets(m);
+  const size_t n = (size_t)m.n_bfaces * face_point_count(m.cell) * mesh_sd(m);
+  x.resize(n);
+  nrm.resize(n);
+  DevBuf<double> dx, dn;
+  dx.alloc(std::max<size_t>(n, 1), ctx->stream);
+  dn.alloc(std::max<size_t>(n, 1), ctx->stream);
+  mesh_face_points(m, dx.p, dn.p);
+  device_to_host(ctx, x.data(), dx.p, n * sizeof(double));
+  device_to_host(ctx, nrm.data(), dn.p, n * sizeof(double));
+}
+
+// A caller's flux g(x, n) at every boundary-face point, called in point order.
+std::vector<double> eval_flux(tptfem_context* ctx, MeshData& m, tptfem_flux_fn fn, void* user) {
+  std::vector<double> x, nrm;
+  host_face_points(ctx, m, x, nrm);
+  const int sd = mesh_sd(m);
+  std::vector<double> g(x.size() / sd);
+  for (size_t p = 0; p < g.size(); ++p) g[p] = fn(&x[p * sd], &nrm[p * sd], sd, user);
+  return g;
+}
+
+// rhs (host, in/out) += the per-point Neumann term of g on the components in comp_mask.
+void neumann_points_host(tptfem_context* ctx, MeshData& m, int dpn, const double* g, unsigned comp_mask,
+                         double* rhs) {
+  TPT_REQUIRE(dpn >= 1 && dpn <= 3, TPTFEM_ERR_INVALID_ARG, "dofs_per_node must be 1..3");
+  TPT_REQUIRE(m.cdim == mesh_sd(m), TPTFEM_ERR_INVALID_ARG,
+              "boundary points need as many stored coordinates as the cell's dimension");
+  mesh_build_face_offsets(m);
+  const size_t np = (size_t)m.n_bfaces * face_point_count(m.cell);
+  const int64_t n = m.n_nodes * dpn;
+  DevBuf<double> dg, d;
+  dg.alloc(std::max<size_t>(np, 1), ctx->stream);
+  TPT_REQUIRE(host_to_device_finite(ctx, dg.p, g, np), TPTFEM_ERR_INVALID_ARG, "flux holds a non-finite value");
+  d.alloc(n, ctx->stream);
+  host_to_device(ctx, d.p, rhs, n * sizeof(double));
+  apply_neumann_points(m, dpn, dg.p, comp_mask, d.p);
+  device_to_host(ctx, rhs, d.p, n * sizeof(double));
 }
 
 }  // namespace
@@ -842,6 +913,178 @@ tptfem_status tptfem_topopt_element_stiffness(double nu, double h, double* ke) {
   if (!ke || !(h > 0) || !(nu > -1.0 && nu < 0.5)) return TPTFEM_ERR_INVALID_ARG;
   topopt_element_stiffness(nu, h, ke);
   return TPTFEM_OK;
+}
+
+// ---- caller-evaluated sources and fluxes ---------------------------------------
+
+tptfem_status tptfem_mesh_quadrature_points(tptfem_context* ctx, tptfem_mesh* mesh, int quad_order, int32_t* nq,
+                                            double* points) {
+  if (!ctx || !mesh || !mesh->d || !nq) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  MeshData& m = *mesh->d;
+  check_quad_order(m, quad_order);
+  *nq = cell_point_count(m.cell, quad_order);
+  if (points) {
+    int q = 0;
+    std::vector<double> h = host_quad_points(ctx, m, quad_order, q);
+    std::memcpy(points, h.data(), h.size() * sizeof(double));
+  }
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_mesh_boundary_points(tptfem_context* ctx, tptfem_mesh* mesh, int64_t* n_points, double* x,
+                                          double* normal) {
+  if (!ctx || !mesh || !mesh->d || !n_points) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  MeshData& m = *mesh->d;
+  mesh_build_face_offsets(m);
+  *n_points = m.n_bfaces * face_point_count(m.cell);
+  if (x || normal) {
+    std::vector<double> hx, hn;
+    host_face_points(ctx, m, hx, hn);
+    if (x) std::memcpy(x, hx.data(), hx.size() * sizeof(double));
+    if (normal) std::memcpy(normal, hn.data(), hn.size() * sizeof(double));
+  }
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_load_poisson_source_points(tptfem_context* ctx, tptfem_mesh* mesh, const double* source,
+                                                int quad_order, double* rhs) {
+  if (!ctx || !mesh || !mesh->d || !rhs || !source) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  MeshData& m = *mesh->d;
+  check_quad_order(m, quad_order);
+  const size_t np = (size_t)m.n_elems * cell_point_count(m.cell, quad_order);
+  DevBuf<double> dv, d;
+  dv.alloc(std::max<size_t>(np, 1), ctx->stream);
+  TPT_REQUIRE(host_to_device_finite(ctx, dv.p, source, np), TPTFEM_ERR_INVALID_ARG,
+              "source holds a non-finite value");
+  d.alloc(m.n_nodes, ctx->stream);
+  load_poisson_source(m, 0.0, quad_order, d.p, dv.p);
+  device_to_host(ctx, rhs, d.p, m.n_nodes * sizeof(double));
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_load_body_points(tptfem_context* ctx, tptfem_mesh* mesh, const double* body, int quad_order,
+                                      double* rhs) {
+  if (!ctx || !mesh || !mesh->d || !rhs || !body) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  MeshData& m = *mesh->d;
+  check_quad_order(m, quad_order);
+  const int dim = mesh_sd(m);
+  const size_t np = (size_t)m.n_elems * cell_point_count(m.cell, quad_order) * dim;
+  DevBuf<double> dv, d;
+  dv.alloc(std::max<size_t>(np, 1), ctx->stream);
+  TPT_REQUIRE(host_to_device_finite(ctx, dv.p, body, np), TPTFEM_ERR_INVALID_ARG,
+              "body force holds a non-finite value");
+  d.alloc(m.n_nodes * dim, ctx->stream);
+  load_body(m, nullptr, quad_order, d.p, dv.p);
+  device_to_host(ctx, rhs, d.p, m.n_nodes * dim * sizeof(double));
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_apply_neumann_points(tptfem_context* ctx, tptfem_mesh* mesh, int dofs_per_node, const double* g,
+                                          uint32_t comp_mask, double* rhs) {
+  if (!ctx || !mesh || !mesh->d || !rhs || !g) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  neumann_points_host(ctx, *mesh->d, dofs_per_node, g, comp_mask, rhs);
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_assemble_poisson_robin_points(tptfem_context* ctx, tptfem_mesh* mesh, const double* conductivity,
+                                                   int per_element, int quad_order, const double* h,
+                                                   tptfem_matrix** out) {
+  if (!ctx || !out || !h) return TPTFEM_ERR_INVALID_ARG;
+  *out = nullptr;
+  API_TRY
+  set_device(ctx);
+  TPT_REQUIRE(mesh && mesh->d, TPTFEM_ERR_INVALID_ARG, "mesh is NULL");
+  TPT_REQUIRE(mesh->d->cdim == mesh_sd(*mesh->d), TPTFEM_ERR_INVALID_ARG,
+              "boundary points need as many stored coordinates as the cell's dimension");
+  RobinSpec r;
+  r.on = 1;
+  r.pts = h;
+  auto M = new_matrix(ctx, mesh, 0, 0, conductivity, per_element, 0.0, quad_order, r);
+  *out = new tptfem_matrix{std::move(M)};
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_solve_poisson_fn(tptfem_context* ctx, tptfem_mesh* mesh, double conductivity, int quad_order,
+                                      tptfem_source_fn source, void* source_user, const int64_t* bc_dof,
+                                      const double* bc_val, int64_t nbc, tptfem_flux_fn neumann,
+                                      void* neumann_user, tptfem_flux_fn robin, void* robin_user,
+                                      const tptfem_solver_opts* opts, double* u, tptfem_solve_stats* stats) {
+  if (!ctx || !mesh || !mesh->d || !u || !source) return TPTFEM_ERR_INVALID_ARG;
+  tptfem_matrix* K = nullptr;
+  std::vector<double> rhs;
+  tptfem_status rc = TPTFEM_OK;
+  try {
+    set_device(ctx);
+    MeshData& m = *mesh->d;
+    check_quad_order(m, quad_order);
+    // the source closure at every element quadrature point, in element order
+    int nq = 0;
+    std::vector<double> x = host_quad_points(ctx, m, quad_order, nq);
+    std::vector<double> sv((size_t)m.n_elems * nq);
+    for (size_t p = 0; p < sv.size(); ++p) sv[p] = source(&x[p * m.cdim], m.cdim, source_user);
+    std::vector<double> hv;
+    if (robin) hv = eval_flux(ctx, m, robin, robin_user);
+    rc = robin ? tptfem_assemble_poisson_robin_points(ctx, mesh, &conductivity, 0, quad_order, hv.data(), &K)
+               : tptfem_assemble_poisson(ctx, mesh, &conductivity, 0, quad_order, &K);
+    if (rc != TPTFEM_OK) return rc;
+    rhs.resize(m.n_nodes);
+    rc = tptfem_load_poisson_source_points(ctx, mesh, sv.data(), quad_order, rhs.data());
+    if (rc == TPTFEM_OK && neumann) {
+      std::vector<double> g = eval_flux(ctx, m, neumann, neumann_user);
+      neumann_points_host(ctx, m, 1, g.data(), 1u, rhs.data());
+    }
+  } catch (const Error& e) {
+    if (K) tptfem_matrix_free(K);
+    return fail(ctx, e.status, e.msg);
+  } catch (const std::bad_alloc&) {
+    if (K) tptfem_matrix_free(K);
+    return fail(ctx, TPTFEM_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+  if (rc == TPTFEM_OK)
+    rc = tptfem_solve_with_dirichlet(ctx, K, rhs.data(), (int64_t)rhs.size(), bc_dof, bc_val, nbc, opts, u, stats);
+  tptfem_matrix_free(K);
+  return rc;
+}
+
+tptfem_status tptfem_solve_elasticity_fn(tptfem_context* ctx, tptfem_mesh* mesh, int model, double young,
+                                         double poisson, int quad_order, tptfem_body_fn body, void* body_user,
+                                         const int64_t* bc_dof, const double* bc_val, int64_t nbc,
+                                         const tptfem_solver_opts* opts, double* u, tptfem_solve_stats* stats) {
+  if (!ctx || !mesh || !mesh->d || !u || !body) return TPTFEM_ERR_INVALID_ARG;
+  std::vector<double> rhs, bv;
+  try {
+    set_device(ctx);
+    MeshData& m = *mesh->d;
+    check_quad_order(m, quad_order);
+    int nq = 0;
+    std::vector<double> x = host_quad_points(ctx, m, quad_order, nq);
+    const int dim = mesh_sd(m);
+    bv.assign((size_t)m.n_elems * nq * dim, 0.0);
+    for (size_t p = 0; p < (size_t)m.n_elems * nq; ++p) body(&x[p * m.cdim], m.cdim, &bv[p * dim], body_user);
+    rhs.resize(m.n_nodes * dim);
+  } catch (const Error& e) {
+    return fail(ctx, e.status, e.msg);
+  } catch (const std::bad_alloc&) {
+    return fail(ctx, TPTFEM_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+  tptfem_matrix* K = nullptr;
+  tptfem_status rc = tptfem_assemble_elasticity(ctx, mesh, model, &young, 0, poisson, quad_order, &K);
+  if (rc != TPTFEM_OK) return rc;
+  rc = tptfem_load_body_points(ctx, mesh, bv.data(), quad_order, rhs.data());
+  if (rc == TPTFEM_OK)
+    rc = tptfem_solve_with_dirichlet(ctx, K, rhs.data(), (int64_t)rhs.size(), bc_dof, bc_val, nbc, opts, u, stats);
+  tptfem_matrix_free(K);
+  return rc;
 }
 
 tptfem_status tptfem_grf_eval(tptfem_context* ctx, const double* points, int64_t n, const double* w,

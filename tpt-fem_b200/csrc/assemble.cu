@@ -22,7 +22,9 @@
 //   tpt-fem-thermal/src/lib.rs     132-196  poisson_element_matrix / source_vector
 //   tpt-fem-elasticity/src/lib.rs  197-348  constitutive, b_matrix, element matrix, body vector
 //   tpt-fem-assembly/src/lib.rs    394-420, 601-667  surface, apply_neumann_order
+#include <climits>
 #include <cmath>
+#include <cstdlib>
 
 #include "objects.hpp"
 
@@ -524,6 +526,9 @@ struct RowArgs {
   const unsigned char* bface;
   int robin, raxis;
   double rsign, rh;
+  // per-point Robin coefficient (rpts != nullptr), indexed like TractionArgs::g
+  const double* rpts;
+  const int* face_off;
 };
 
 // One thread per global row.  Shared memory holds the row's dense accumulator
@@ -594,8 +599,10 @@ __global__ void __launch_bounds__(128) assemble_rows(RowArgs A) {
         if (kpos < 0) continue;
         double measure, nrm[SD];
         face_geometry<CELL, SD>(X, fl, measure, nrm);
-        const double h = (A.raxis < 0 || nrm[A.raxis] * A.rsign > 0.5) ? A.rh : 0.0;
+        const double hsel = (A.raxis < 0 || nrm[A.raxis] * A.rsign > 0.5) ? A.rh : 0.0;
+        const int64_t fp = A.rpts ? (int64_t)(A.face_off[e] + __popc(bm & ((1u << fi) - 1u))) * c_face.nq : 0;
         for (int q = 0; q < c_face.nq; ++q) {
+          const double h = A.rpts ? A.rpts[fp + q] : hsel;
           const double wmh = c_face.w[q] * measure * h * c_face.ns[q][kpos];
           for (int lf = 0; lf < FN; ++lf) {
             const int s = (sj[fl[lf]] * DPN + a) * T + tid;
@@ -761,6 +768,310 @@ __global__ void __launch_bounds__(32 * AN_WARPS) assemble_nodes_tet(RowArgs A, i
   }
 }
 
+// ---- Tet4 rows in two passes ------------------------------------------------------
+// assemble_nodes_tet recomputes an element's geometry for each of its four
+// nodes, and its FP64 work (no FMA, for exactness) is the limit.  Here pass 1
+// (tet_records, one thread per element) computes each element's geometry and
+// constitutive constants once into a 128-byte record; pass 2 (tet_node_rows,
+// one warp per node) forms the node's element-row blocks from those records
+// and sums them in element order exactly as assemble_nodes_tet does.  The
+// records live in a ring of `ring` elements sized to stay in L2: the nodes
+// are processed in chunks whose incident elements span at most `ring` ids,
+// each chunk's missing records are written just before it (slot e % ring),
+// and the value stores stream past L2 (st.global.cs), so the records are
+// written and read in L2 instead of making a round trip through HBM.
+//
+// Record (16 doubles): g[4][3], the element's physical gradients, then
+//   elasticity: w |det|, D00, D01, Dshear;  Poisson: w k, |det|, 0, 0.
+// Per entry the four identical quadrature points add t = (w|det|) s four
+// times from 0.0: 0 + t = t and t + t = 2t are exact, so the sum is
+// fl(fl(3t) + t), the same bits in two operations instead of four.
+constexpr int TR_DOUBLES = 16;  // doubles per element record
+constexpr int TN_WARPS = 2;     // warps (nodes) per block of tet_node_rows
+constexpr int TN_MAXDEG = 32;   // incident elements per node handled by one warp (at most)
+// Resident blocks per SM the register budget of tet_node_rows is cut for:
+// 16 (64 registers) by default; TPTFEM_TET_MINB=8 gives the compiler 80.
+int tet_minb() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = std::getenv("TPTFEM_TET_MINB");
+    v = (e && std::atoi(e) == 8) ? 8 : 16;
+  }
+  return v;
+}
+
+template <int PHYS>
+__global__ void __launch_bounds__(256) tet_records(ElemIn in, int64_t e0, int64_t e1, int64_t ring,
+                                                   double* __restrict__ rec, int* flag) {
+  const int64_t e = e0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= e1) return;
+  double X[4][3];
+  int nodes[4];
+  load_elem<TPTFEM_CELL_TET4>(in, (int)e, X, nodes);
+  TetGeom G;
+  const bool ok = tet_geom(X, G);
+  const double coef = in.coef[in.per_elem ? e : 0];
+  const double w0 = c_cell.w[0];
+  double r[TR_DOUBLES];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r[i * 3 + k] = G.g[i][k];
+  if constexpr (PHYS == 1) {
+    const Dmat D = make_d(in.model, coef, in.nu);
+    r[12] = w0 * G.adet;
+    r[13] = D.d00;
+    r[14] = D.d01;
+    r[15] = D.dsh;
+  } else {
+    r[12] = w0 * coef;
+    r[13] = G.adet;
+    r[14] = r[15] = 0.0;
+  }
+  double2* dst = reinterpret_cast<double2*>(rec + (e % ring) * TR_DOUBLES);
+#pragma unroll
+  for (int q = 0; q < TR_DOUBLES / 2; ++q) dst[q] = make_double2(r[2 * q], r[2 * q + 1]);
+  if (!ok) atomicOr(flag, 1);
+}
+
+__device__ __forceinline__ unsigned nonzero_bit(double v) {
+  return (unsigned)((__double_as_longlong(v) << 1) != 0);  // v != +-0.0, without an FP64 compare
+}
+
+// Chains (once per mesh): node n's entries in neighbour slot s are summed over
+// the incidences whose element holds slot s's node, in ascending element id;
+// give every (incidence k, element node j) a position in its slot's chain:
+// chains are stored one after another in slot order, coff[nb_ptr[n] + s] is
+// where slot s's chain starts (the last ends at 4 * deg), and cpos[k] holds
+// the positions of incidence k's four blocks.  One warp per node; one ballot
+// per slot gives the incidences of that slot in ascending order.
+__global__ void tet_chains(int64_t n_nodes, const int* __restrict__ ne_ptr, const uchar4* __restrict__ slot,
+                           const int* __restrict__ nb_ptr, uchar4* __restrict__ cpos,
+                           unsigned char* __restrict__ coff) {
+  const int lane = threadIdx.x & 31;
+  const int64_t n = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (n >= n_nodes) return;
+  const int k0 = ne_ptr[n], deg = ne_ptr[n + 1] - k0;
+  const int nb0 = nb_ptr[n], nnb = nb_ptr[n + 1] - nb0;
+  const uchar4 sl = lane < deg ? slot[k0 + lane] : make_uchar4(255, 255, 255, 255);
+  unsigned mymask = 0;
+  for (int t = 0; t < nnb; ++t) {
+    const unsigned m = __ballot_sync(0xffffffffu, sl.x == t || sl.y == t || sl.z == t || sl.w == t);
+    if (lane == t) mymask = m;
+  }
+  const int len = __popc(mymask);
+  int pre = len;
+  for (int o2 = 1; o2 < 32; o2 <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, pre, o2);
+    if (lane >= o2) pre += t;
+  }
+  if (lane < nnb) coff[nb0 + lane] = (unsigned char)(pre - len);
+  const int sj[4] = {sl.x, sl.y, sl.z, sl.w};
+  const unsigned below = (1u << lane) - 1u;
+  int pos[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int s = sj[j] & 31;
+    pos[j] = __shfl_sync(0xffffffffu, pre - len, s) + __popc(__shfl_sync(0xffffffffu, mymask, s) & below);
+  }
+  if (lane < deg) cpos[k0 + lane] = make_uchar4(pos[0], pos[1], pos[2], pos[3]);
+}
+
+// One warp per node of [n0, n1).
+//  1. Lane k takes incidence k (element e_k, the node's local index l_k), reads
+//     e_k's record and forms the node's blocks against the element's four
+//     nodes (9 entries each for elasticity), writing block j at its chain
+//     position cpos[k].j with the mask of its non-zero entries.
+//  2. Each slot's chain is summed entry by entry from +0.0 in chain order --
+//     ascending element id, Coo::to_csr's sequential duplicate sum
+//     (crates/tpt-fem-sparse/src/lib.rs:144-163) -- with the masks ORed: lane s
+//     for the other slots, D2 lanes (one entry each) for the node's own slot,
+//     whose chain holds every incident element.
+//  3. Lane s writes slot s's entries to the node's rows (one scan gives the
+//     positions in all DPN rows).
+//   COUNT / FILL / PADDED: as assemble_nodes_tet; the masks are stored per
+//     neighbour entry (nzm[nb_ptr[n] + s]).
+//   NUMERIC: the masks must equal the stored ones (else flag bit 2: the
+//     pattern changed); values go to the positions the pattern gives them,
+//     without reading the column indices back.
+template <int PHYS, int DPN, int MAXDEG, int MINB>
+__global__ void __launch_bounds__(32 * TN_WARPS, MINB) tet_node_rows(RowArgs A, int64_t n0, int64_t n1,
+                                                                     const double* __restrict__ rec, int64_t ring,
+                                                                     const uchar4* __restrict__ cpos,
+                                                                     const unsigned char* __restrict__ coff,
+                                                                     unsigned short* __restrict__ nzm, int mode) {
+  constexpr int D2 = DPN * DPN;
+  constexpr int CS = DPN == 1 ? 1 : 10;  // chain entry stride in doubles (16-byte rows for DPN 3)
+  __shared__ __align__(16) double chain[TN_WARPS][4 * MAXDEG][CS];
+  __shared__ unsigned short cnz[TN_WARPS][4 * MAXDEG];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t n = n0 + (int64_t)blockIdx.x * TN_WARPS + w;
+  if (n >= n1) return;  // whole warps leave together
+  const int k0 = A.ne_ptr[n], deg = A.ne_ptr[n + 1] - k0;
+  const int nb0 = A.nb_ptr[n], nnb = A.nb_ptr[n + 1] - nb0;
+  // slot data first, so its loads overlap the block work
+  const bool mine = lane < nnb;
+  int col = 0, c0 = 0, c1 = 0;
+  if (mine) {
+    col = A.nb[nb0 + lane];
+    c0 = coff[nb0 + lane];
+    c1 = lane + 1 < nnb ? coff[nb0 + lane + 1] : 4 * deg;
+  }
+  // 1. blocks into their chains
+  if (lane < deg) {
+    const int pe = A.ne[k0 + lane];
+    const uchar4 cp = cpos[k0 + lane];
+    const double2* src = reinterpret_cast<const double2*>(rec + ((int64_t)(pe >> 2) % ring) * TR_DOUBLES);
+    double r[TR_DOUBLES];
+#pragma unroll
+    for (int q = 0; q < TR_DOUBLES / 2; ++q) {
+      const double2 v = __ldcg(src + q);
+      r[2 * q] = v.x;
+      r[2 * q + 1] = v.y;
+    }
+    const int l = pe & 3;
+    double gl[3];  // the node's own gradient row, selected without a dynamic register index
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gl[c] = l == 0 ? r[c] : (l == 1 ? r[3 + c] : (l == 2 ? r[6 + c] : r[9 + c]));
+    const int pj[4] = {cp.x, cp.y, cp.z, cp.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const double* gj = r + 3 * j;
+      double v[D2];
+      if constexpr (PHYS == 0) {
+        const double dot = gl[0] * gj[0] + gl[1] * gj[1] + gl[2] * gj[2];
+        const double t = r[12] * dot * r[13];
+        v[0] = 3.0 * t + t;
+      } else {
+        const double wd = r[12], m = r[13], cn = r[14], d = r[15];
+        const double pm0 = gl[0] * m, pm1 = gl[1] * m, pm2 = gl[2] * m;
+        const double pc0 = gl[0] * cn, pc1 = gl[1] * cn, pc2 = gl[2] * cn;
+        const double pd0 = gl[0] * d, pd1 = gl[1] * d, pd2 = gl[2] * d;
+        // bdb3's sums, term for term
+        const double sm[9] = {(pm0 * gj[0] + pd1 * gj[1]) + pd2 * gj[2], pc0 * gj[1] + pd1 * gj[0],
+                              pc0 * gj[2] + pd2 * gj[0],                  pc1 * gj[0] + pd0 * gj[1],
+                              (pm1 * gj[1] + pd0 * gj[0]) + pd2 * gj[2], pc1 * gj[2] + pd2 * gj[1],
+                              pc2 * gj[0] + pd0 * gj[2],                  pc2 * gj[1] + pd1 * gj[2],
+                              (pm2 * gj[2] + pd1 * gj[1]) + pd0 * gj[0]};
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+          const double t = wd * sm[q];
+          v[q] = 3.0 * t + t;
+        }
+      }
+      unsigned msk = 0;
+#pragma unroll
+      for (int q = 0; q < D2; ++q) msk |= (unsigned)(v[q] != 0.0) << q;
+      double* dst = chain[w][pj[j]];
+      if constexpr (DPN == 1) {
+        dst[0] = v[0];
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) reinterpret_cast<double2*>(dst)[q] = make_double2(v[2 * q], v[2 * q + 1]);
+        dst[8] = v[8];
+      }
+      cnz[w][pj[j]] = (unsigned short)msk;
+    }
+  }
+  __syncwarp();
+  // 2. ordered chain sums, in two loops so that neither runs the other's body:
+  //  a. lane s (a slot other than the node's own) sums its chain, all D2
+  //     entries per element (its chain is short: the elements sharing an edge);
+  //  b. the node's own slot, whose chain holds every incident element: lane q
+  //     (< D2) sums entry q, and the sums move to the slot's lane.
+  const unsigned selfm = __ballot_sync(0xffffffffu, mine && col == (int)n);
+  const int self = selfm ? __ffs(selfm) - 1 : -1;
+  double acc[D2];
+#pragma unroll
+  for (int q = 0; q < D2; ++q) acc[q] = 0.0;
+  unsigned nzb = 0;
+  {
+    const bool own = mine && lane != self;
+    const int e1 = own ? c1 : 0;
+    for (int c = own ? c0 : 0; c < e1; ++c) {
+      const double* e = chain[w][c];
+      if constexpr (DPN == 1) {
+        acc[0] = acc[0] + e[0];
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double2 v = reinterpret_cast<const double2*>(e)[q];
+          acc[2 * q] = acc[2 * q] + v.x;
+          acc[2 * q + 1] = acc[2 * q + 1] + v.y;
+        }
+        acc[8] = acc[8] + e[8];
+      }
+      nzb |= cnz[w][c];
+    }
+  }
+  if (self >= 0) {
+    const int sc0 = __shfl_sync(0xffffffffu, c0, self), sc1 = __shfl_sync(0xffffffffu, c1, self);
+    double sv = 0.0;
+    unsigned snz = 0;
+    if (lane < D2)
+      for (int c = sc0; c < sc1; ++c) {
+        sv = sv + chain[w][c][lane];
+        snz |= cnz[w][c];
+      }
+#pragma unroll
+    for (int q = 0; q < D2; ++q) {
+      const double t = __shfl_sync(0xffffffffu, sv, q);
+      if (lane == self) acc[q] = t;
+    }
+    const unsigned tn = __shfl_sync(0xffffffffu, snz, 0);
+    if (lane == self) nzb = tn;
+  }
+  // 3. rows
+  const unsigned nz = mine ? nzb : 0u;
+  if (mine) {
+    if (mode == MODE_NUMERIC) {
+      if (nzm[nb0 + lane] != (unsigned short)nz) atomicOr(A.flag, 2);
+    } else {
+      nzm[nb0 + lane] = (unsigned short)nz;
+    }
+  }
+  // the DPN rows' counts packed in one word (8 bits each; a row has at most
+  // 3 * 32 entries), so one scan over the lanes gives every row's positions
+  unsigned packed = 0;
+#pragma unroll
+  for (int a = 0; a < DPN; ++a) packed |= (unsigned)__popc((nz >> (a * DPN)) & ((1u << DPN) - 1u)) << (8 * a);
+  unsigned pr = packed;
+  for (int o2 = 1; o2 < 32; o2 <<= 1) {
+    const unsigned t = __shfl_up_sync(0xffffffffu, pr, o2);
+    if (lane >= o2) pr += t;
+  }
+  const unsigned totals = __shfl_sync(0xffffffffu, pr, 31);
+  const int col0 = col * DPN;
+#pragma unroll
+  for (int a = 0; a < DPN; ++a) {
+    const int64_t r = n * DPN + a;
+    const unsigned rowbits = (nz >> (a * DPN)) & ((1u << DPN) - 1u);
+    const int total = (totals >> (8 * a)) & 255u;
+    int off = (int)((pr >> (8 * a)) & 255u) - __popc(rowbits);
+    if (mode == MODE_COUNT || mode == MODE_PADDED) {
+      if (lane == 0) A.row_cnt[r] = total;
+      if (mode == MODE_COUNT) continue;
+    }
+    int base = 0, rlen = A.maxc;
+    if (mode != MODE_PADDED) {
+      base = A.row_ptr[r];
+      rlen = A.row_ptr[r + 1] - base;
+      if (mode == MODE_NUMERIC && lane == 0 && rlen != total) atomicOr(A.flag, 2);
+    }
+    int* cdst = mode == MODE_PADDED ? A.col + r * A.maxc : A.col + base;
+    double* vdst = mode == MODE_PADDED ? A.val + r * A.maxc : A.val + base;
+#pragma unroll
+    for (int b = 0; b < DPN; ++b) {
+      if (!((rowbits >> b) & 1u)) continue;
+      if (off < rlen) {  // a changed pattern (flagged) may not fit the row
+        if (mode != MODE_NUMERIC) cdst[off] = col0 + b;
+        __stcs(vdst + off, acc[a * DPN + b]);
+      }
+      ++off;
+    }
+  }
+}
+
 // ---- loads ----------------------------------------------------------------------
 
 struct LoadArgs {
@@ -769,6 +1080,9 @@ struct LoadArgs {
   const int* ne;
   int64_t n_nodes;
   double b[3];  // source value (Poisson) or body force (elasticity)
+  // per-quadrature-point values instead of b (nullptr: constant b): KIND 0 one
+  // source value per (element, point), KIND 1 DPN body-force components
+  const double* pv;
   double* rhs;
   int* flag;
 };
@@ -793,35 +1107,38 @@ __global__ void load_rows(LoadArgs A) {
 #pragma unroll
     for (int a = 0; a < DPN; ++a) f[a] = 0.0;
     const int nq = c_cell.nq;
+    // the source value or body force at point q: the constant, or the caller's
+    // value at that point
+    auto bval = [&](int q, int a) { return A.pv ? A.pv[((int64_t)e * nq + q) * DPN + a] : A.b[a]; };
     if constexpr (CELL == TPTFEM_CELL_TET4) {
       TetGeom G;
       ok &= tet_geom(X, G);
       for (int q = 0; q < nq; ++q) {
         const double w = c_cell.w[q], N = c_cell.ns[q][l];
-        if (KIND == 0) f[0] = f[0] + w * A.b[0] * N * G.adet;
+        if (KIND == 0) f[0] = f[0] + w * bval(q, 0) * N * G.adet;
         else
 #pragma unroll
-          for (int a = 0; a < DPN; ++a) f[a] = f[a] + w * N * A.b[a] * G.adet;
+          for (int a = 0; a < DPN; ++a) f[a] = f[a] + w * N * bval(q, a) * G.adet;
       }
     } else if constexpr (CELL == TPTFEM_CELL_TRI3) {
       TriGeom G;
       ok &= tri_geom(X, G);
       for (int q = 0; q < nq; ++q) {
         const double w = c_cell.w[q], N = c_cell.ns[q][l];
-        if (KIND == 0) f[0] = f[0] + w * A.b[0] * N * G.adet;
+        if (KIND == 0) f[0] = f[0] + w * bval(q, 0) * N * G.adet;
         else
 #pragma unroll
-          for (int a = 0; a < DPN; ++a) f[a] = f[a] + w * N * A.b[a] * G.adet;
+          for (int a = 0; a < DPN; ++a) f[a] = f[a] + w * N * bval(q, a) * G.adet;
       }
     } else {
       for (int q = 0; q < nq; ++q) {
         QuadGeom G;
         ok &= quad_geom(X, q, G);
         const double w = c_cell.w[q], N = c_cell.ns[q][l];
-        if (KIND == 0) f[0] = f[0] + w * A.b[0] * N * G.adet;
+        if (KIND == 0) f[0] = f[0] + w * bval(q, 0) * N * G.adet;
         else
 #pragma unroll
-          for (int a = 0; a < DPN; ++a) f[a] = f[a] + w * N * A.b[a] * G.adet;
+          for (int a = 0; a < DPN; ++a) f[a] = f[a] + w * N * bval(q, a) * G.adet;
       }
     }
 #pragma unroll
@@ -841,6 +1158,12 @@ struct TractionArgs {
   int dpn, axis;
   double sign;
   double t[3];
+  // general flux (g != nullptr): g at every boundary-face quadrature point,
+  // indexed (face_off[e] + rank of the face among e's boundary faces) * nqf + q,
+  // added to the components in comp_mask
+  const double* g;
+  const int* face_off;
+  unsigned comp_mask;
   double* rhs;
 };
 
@@ -872,6 +1195,15 @@ __global__ void traction_rows(TractionArgs A) {
       if (kpos < 0) continue;
       double measure, nrm[SD];
       face_geometry<CELL, SD>(X, fl, measure, nrm);
+      if (A.g) {
+        const int64_t fp = (int64_t)(A.face_off[e] + __popc(bm & ((1u << fi) - 1u))) * c_face.nq;
+        for (int q = 0; q < c_face.nq; ++q) {
+          const double wm = c_face.w[q] * measure, N = c_face.ns[q][kpos], g = A.g[fp + q];
+          for (int c = 0; c < A.dpn; ++c)
+            if (A.comp_mask & (1u << c)) acc[c] = acc[c] + wm * g * N;
+        }
+        continue;
+      }
       const bool sel = nrm[A.axis] * A.sign > 0.5;
       for (int q = 0; q < c_face.nq; ++q) {
         const double wm = c_face.w[q] * measure, N = c_face.ns[q][kpos];
@@ -883,6 +1215,69 @@ __global__ void traction_rows(TractionArgs A) {
     }
   }
   for (int c = 0; c < A.dpn; ++c) A.rhs[n * A.dpn + c] = acc[c];
+}
+
+// ---- quadrature points for caller-evaluated sources and fluxes ---------------
+
+// Physical quadrature points of every element, x_q[d] = sum_k N_k(xi_q) X_k[d]
+// summed over k from 0.0 for each of the cdim stored coordinates, as
+// poisson_source_vector / elasticity_body_vector form the point they hand to
+// the source closure (thermal:163-196, elasticity:312-348).  Output
+// ((e * nq) + q) * cdim + d.
+template <int CELL>
+__global__ void quad_points(ElemIn in, int64_t n_elems, double* __restrict__ out) {
+  constexpr int NV = CellTraits<CELL>::NV;
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n_elems) return;
+  int nodes[4];
+  for (int j = 0; j < NV; ++j) nodes[j] = in.conn[e * NV + j];
+  const int nq = c_cell.nq;
+  for (int q = 0; q < nq; ++q)
+    for (int d = 0; d < in.cdim; ++d) {
+      double x = 0.0;
+      for (int k = 0; k < NV; ++k) x = x + c_cell.ns[q][k] * in.coords[(int64_t)nodes[k] * in.cdim + d];
+      out[(e * nq + q) * in.cdim + d] = x;
+    }
+}
+
+__global__ void face_counts(int64_t n_elems, const unsigned char* __restrict__ bface, int* __restrict__ cnt) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n_elems) cnt[e] = __popc((unsigned)bface[e]);
+}
+
+// Boundary-face quadrature points and outward unit normals in (element, face,
+// point) order -- the order boundary_faces lists the faces in
+// (assembly:563-583) -- with x_q summed over the face's nodes as
+// apply_neumann_order / apply_robin_order do (assembly:601-667, 684-753).
+template <int CELL>
+__global__ void face_points(ElemIn in, int64_t n_elems, const unsigned char* __restrict__ bface,
+                            const int* __restrict__ face_off, double* __restrict__ xo, double* __restrict__ no) {
+  constexpr int SD = CellTraits<CELL>::SD, FN = FaceTraits<CELL>::FN, NF = FaceTraits<CELL>::NF;
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n_elems) return;
+  const unsigned bm = bface[e];
+  if (!bm) return;
+  double X[4][SD];
+  int nodes[4];
+  load_elem<CELL>(in, (int)e, X, nodes);
+  int rank = 0;
+  for (int fi = 0; fi < NF; ++fi) {
+    if (!(bm & (1u << fi))) continue;
+    int fl[3];
+    for (int q = 0; q < FN; ++q) fl[q] = FaceTraits<CELL>::node(fi, q);
+    double measure, nrm[SD];
+    face_geometry<CELL, SD>(X, fl, measure, nrm);
+    const int64_t fp = (int64_t)(face_off[e] + rank) * c_face.nq;
+    for (int q = 0; q < c_face.nq; ++q) {
+      for (int d = 0; d < SD; ++d) {
+        double x = 0.0;
+        for (int k = 0; k < FN; ++k) x = x + c_face.ns[q][k] * X[fl[k]][d];
+        xo[(fp + q) * SD + d] = x;
+        no[(fp + q) * SD + d] = nrm[d];
+      }
+    }
+    ++rank;
+  }
 }
 
 ElemIn elem_in(const MeshData& m, const double* coef, int per_elem, int model, double nu) {
@@ -907,6 +1302,7 @@ void set_robin_faces(MeshData& m, int axis, cudaStream_t s) {
   const int sd = m.cell == TPTFEM_CELL_TET4 ? 3 : 2;
   TPT_REQUIRE(axis < sd, TPTFEM_ERR_INVALID_ARG, "robin axis out of range for the mesh dimension");
   mesh_build_boundary_faces(m);
+  mesh_build_face_offsets(m);
   FaceTab f = make_face_tab(m.cell);
   TPT_CUDA(cudaMemcpyToSymbolAsync(c_face, &f, sizeof(f), 0, cudaMemcpyHostToDevice, s));
 }
@@ -915,6 +1311,111 @@ int read_flag(tptfem_context* ctx) {
   TPT_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   TPT_CUDA(cudaStreamSynchronize(ctx->stream));
   return ctx->h_pinned[0];
+}
+
+__global__ void node_elem_span(int64_t n_nodes, const int* __restrict__ ne_ptr, const int* __restrict__ ne,
+                               int2* __restrict__ out) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= n_nodes) return;
+  const int b = ne_ptr[n], e = ne_ptr[n + 1];
+  out[n] = b < e ? make_int2(ne[b] >> 2, ne[e - 1] >> 2) : make_int2(INT_MAX, -1);
+}
+
+// Ring size of the two-pass Tet4 assembly, in MB of records (48 MB of the
+// 126 MB L2 by default; TPTFEM_TET_RING_MB overrides it for tuning).
+int64_t tet_ring_target() {
+  const char* v = std::getenv("TPTFEM_TET_RING_MB");
+  const long mb = v ? std::atol(v) : 48;
+  return std::max<int64_t>(1, (int64_t)std::max(1L, mb) * (1 << 20) / (TR_DOUBLES * 8));
+}
+
+// Node chunks whose incident elements span at most `ring` ids (the element
+// lists are sorted by id, so a node's span is its last id minus its first).
+void tet_plan(MeshData& m) {
+  if (m.tplan) return;
+  cudaStream_t s = m.ctx->stream;
+  DevBuf<int2> d;
+  d.alloc(std::max<int64_t>(m.n_nodes, 1), s);
+  node_elem_span<<<ceil_div(m.n_nodes, 256), 256, 0, s>>>(m.n_nodes, m.ne_ptr.p, m.ne.p, d.p);
+  TPT_CHECK_LAUNCH();
+  std::vector<int2> h(m.n_nodes);
+  device_to_host(m.ctx, h.data(), d.p, m.n_nodes * sizeof(int2));
+  int64_t ring = tet_ring_target();
+  for (const int2& v : h)
+    if (v.y >= 0) ring = std::max<int64_t>(ring, (int64_t)v.y - v.x + 1);
+  ring = std::max<int64_t>(1, std::min<int64_t>(ring, m.n_elems));
+  m.tp_nodes.clear();
+  m.tp_elems.clear();
+  int64_t n0 = 0, done = 0;
+  while (n0 < m.n_nodes) {
+    int64_t lo = INT64_MAX, hi = -1, n = n0;
+    for (; n < m.n_nodes; ++n) {
+      const int64_t nlo = std::min<int64_t>(lo, h[n].x), nhi = std::max<int64_t>(hi, h[n].y);
+      if (n > n0 && nhi >= 0 && nhi - nlo + 1 > ring) break;
+      lo = nlo;
+      hi = nhi;
+    }
+    done = std::max(done, hi + 1);
+    m.tp_nodes.push_back(n0);
+    m.tp_elems.push_back(done);
+    n0 = n;
+  }
+  m.tp_nodes.push_back(m.n_nodes);
+  m.tp_ring = ring;
+  m.tplan = true;
+}
+
+void tet_build_chains(MeshData& m) {
+  if (m.tchains) return;
+  cudaStream_t s = m.ctx->stream;
+  m.cpos.alloc(std::max<size_t>(m.ne.n, 1), s);
+  m.coff.alloc(std::max<size_t>(m.nb.n, 1), s);
+  tet_chains<<<ceil_div(m.n_nodes * 32, 256), 256, 0, s>>>(m.n_nodes, m.ne_ptr.p, m.slot.p, m.nb_ptr.p, m.cpos.p,
+                                                          m.coff.p);
+  TPT_CHECK_LAUNCH();
+  m.tchains = true;
+}
+
+template <int PHYS, int DPN>
+void launch_tet_two_pass(MatrixData& M, int mode, const RowArgs& A, cudaStream_t s) {
+  MeshData& m = *M.mesh;
+  tet_plan(m);
+  tet_build_chains(m);
+  if (M.nzmask.n != m.nb.n) M.nzmask.alloc(m.nb.n, s);
+  DevBuf<double> ring;
+  ring.alloc(m.tp_ring * TR_DOUBLES, s);
+  int64_t done = 0;
+  for (size_t c = 0; c + 1 < m.tp_nodes.size(); ++c) {
+    const int64_t e1 = m.tp_elems[c];
+    if (e1 > done) {
+      tet_records<PHYS><<<ceil_div(e1 - done, 256), 256, 0, s>>>(A.in, done, e1, m.tp_ring, ring.p, A.flag);
+      TPT_CHECK_LAUNCH();
+      done = e1;
+    }
+    const int64_t n0 = m.tp_nodes[c], n1 = m.tp_nodes[c + 1];
+    const int grid = ceil_div(n1 - n0, TN_WARPS);
+    // fewer incidences per node, less shared memory per warp, more warps per SM
+    const bool d24 = m.max_deg <= 24, b16 = tet_minb() == 16;
+    if (d24 && b16)
+      tet_node_rows<PHYS, DPN, 24, 16><<<grid, 32 * TN_WARPS, 0, s>>>(A, n0, n1, ring.p, m.tp_ring, m.cpos.p, m.coff.p, M.nzmask.p, mode);
+    else if (d24)
+      tet_node_rows<PHYS, DPN, 24, 8><<<grid, 32 * TN_WARPS, 0, s>>>(A, n0, n1, ring.p, m.tp_ring, m.cpos.p, m.coff.p, M.nzmask.p, mode);
+    else if (b16)
+      tet_node_rows<PHYS, DPN, 32, 16><<<grid, 32 * TN_WARPS, 0, s>>>(A, n0, n1, ring.p, m.tp_ring, m.cpos.p, m.coff.p, M.nzmask.p, mode);
+    else
+      tet_node_rows<PHYS, DPN, 32, 8><<<grid, 32 * TN_WARPS, 0, s>>>(A, n0, n1, ring.p, m.tp_ring, m.cpos.p, m.coff.p, M.nzmask.p, mode);
+    TPT_CHECK_LAUNCH();
+  }
+}
+
+// TPTFEM_TET_ONE_PASS=1 selects the one-pass kernel (assemble_nodes_tet) for A/B timing.
+bool tet_one_pass() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = std::getenv("TPTFEM_TET_ONE_PASS");
+    v = (e && e[0] == '1') ? 1 : 0;
+  }
+  return v == 1;
 }
 
 template <int PHYS, int DPN>
@@ -942,11 +1443,14 @@ void launch_rows(int mode, const RowArgs& A, cudaStream_t s) {
   else run(assemble_rows<CELL, PHYS, DPN, MODE_NUMERIC>);
 }
 
-void dispatch_rows(const MatrixData& M, int mode, const RowArgs& A, cudaStream_t s) {
+void dispatch_rows(MatrixData& M, int mode, const RowArgs& A, cudaStream_t s) {
   const int cell = M.mesh->cell;
   const MeshData& m = *M.mesh;
-  if (cell == TPTFEM_CELL_TET4 && !A.robin && m.max_nb <= 32 && m.max_deg <= AN_MAXDEG) {
-    // warp per node: at most 32 neighbour slots and AN_MAXDEG incident elements
+  if (cell == TPTFEM_CELL_TET4 && !A.robin && m.max_nb <= 32 && m.max_deg <= TN_MAXDEG && !tet_one_pass()) {
+    // element records, then a warp per node: at most 32 neighbour slots and incident elements
+    if (M.physics == 0) launch_tet_two_pass<0, 1>(M, mode, A, s);
+    else launch_tet_two_pass<1, 3>(M, mode, A, s);
+  } else if (cell == TPTFEM_CELL_TET4 && !A.robin && m.max_nb <= 32 && m.max_deg <= AN_MAXDEG) {
     if (M.physics == 0) launch_nodes_tet<0, 1>(mode, A, m.n_nodes, s);
     else launch_nodes_tet<1, 3>(mode, A, m.n_nodes, s);
   } else if (cell == TPTFEM_CELL_TET4) {
@@ -982,6 +1486,8 @@ RowArgs row_args(MatrixData& M) {
   A.raxis = M.robin_axis;
   A.rsign = M.robin_sign;
   A.rh = M.robin_h;
+  A.rpts = (M.robin && M.robin_pts.n) ? M.robin_pts.p : nullptr;
+  A.face_off = A.rpts ? m.face_off.p : nullptr;
   return A;
 }
 
@@ -1112,7 +1618,7 @@ double profile_numeric_assembly(MatrixData& M, int reps) {
   return (double)ms / std::max(reps, 1);
 }
 
-void load_poisson_source(MeshData& m, double src, int quad_order, double* d_rhs) {
+void load_poisson_source(MeshData& m, double src, int quad_order, double* d_rhs, const double* d_pts) {
   tptfem_context* ctx = m.ctx;
   cudaStream_t s = ctx->stream;
   mesh_build_adjacency(m);
@@ -1124,6 +1630,7 @@ void load_poisson_source(MeshData& m, double src, int quad_order, double* d_rhs)
   A.ne = m.ne.p;
   A.n_nodes = m.n_nodes;
   A.b[0] = src; A.b[1] = A.b[2] = 0.0;
+  A.pv = d_pts;
   A.rhs = d_rhs;
   A.flag = ctx->d_flag;
   if (m.cell == TPTFEM_CELL_TET4) load_rows<TPTFEM_CELL_TET4, 0, 1><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
@@ -1133,7 +1640,7 @@ void load_poisson_source(MeshData& m, double src, int quad_order, double* d_rhs)
   TPT_REQUIRE((read_flag(ctx) & 1) == 0, TPTFEM_ERR_NUMERIC, "degenerate element in load integration");
 }
 
-void load_body(MeshData& m, const double* body, int quad_order, double* d_rhs) {
+void load_body(MeshData& m, const double* body, int quad_order, double* d_rhs, const double* d_pts) {
   tptfem_context* ctx = m.ctx;
   cudaStream_t s = ctx->stream;
   mesh_build_adjacency(m);
@@ -1144,7 +1651,9 @@ void load_body(MeshData& m, const double* body, int quad_order, double* d_rhs) {
   A.ne_ptr = m.ne_ptr.p;
   A.ne = m.ne.p;
   A.n_nodes = m.n_nodes;
-  A.b[0] = body[0]; A.b[1] = body[1]; A.b[2] = m.cell == TPTFEM_CELL_TET4 ? body[2] : 0.0;
+  A.b[0] = A.b[1] = A.b[2] = 0.0;
+  if (body) { A.b[0] = body[0]; A.b[1] = body[1]; A.b[2] = m.cell == TPTFEM_CELL_TET4 ? body[2] : 0.0; }
+  A.pv = d_pts;
   A.rhs = d_rhs;
   A.flag = ctx->d_flag;
   if (m.cell == TPTFEM_CELL_TET4) load_rows<TPTFEM_CELL_TET4, 1, 3><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
@@ -1172,6 +1681,79 @@ void apply_traction(MeshData& m, int dpn, int axis, double sign, const double* t
   A.axis = axis;
   A.sign = sign;
   for (int c = 0; c < 3; ++c) A.t[c] = c < dpn ? t[c] : 0.0;
+  A.g = nullptr;
+  A.face_off = nullptr;
+  A.comp_mask = 0u;
+  A.rhs = d_rhs;
+  if (m.cell == TPTFEM_CELL_TET4) traction_rows<TPTFEM_CELL_TET4><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
+  else if (m.cell == TPTFEM_CELL_TRI3) traction_rows<TPTFEM_CELL_TRI3><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
+  else traction_rows<TPTFEM_CELL_QUAD4><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
+  TPT_CHECK_LAUNCH();
+}
+
+int cell_point_count(int cell, int quad_order) { return make_cell_tab(cell, quad_order).nq; }
+
+int face_point_count(int cell) { return make_face_tab(cell).nq; }
+
+void mesh_quad_points(MeshData& m, int quad_order, double* d_out) {
+  cudaStream_t s = m.ctx->stream;
+  set_cell_tab(m, quad_order, s);
+  const ElemIn in = elem_in(m, nullptr, 0, 0, 0.0);
+  const int grid = ceil_div(m.n_elems, 128);
+  if (m.cell == TPTFEM_CELL_TET4) quad_points<TPTFEM_CELL_TET4><<<grid, 128, 0, s>>>(in, m.n_elems, d_out);
+  else if (m.cell == TPTFEM_CELL_TRI3) quad_points<TPTFEM_CELL_TRI3><<<grid, 128, 0, s>>>(in, m.n_elems, d_out);
+  else quad_points<TPTFEM_CELL_QUAD4><<<grid, 128, 0, s>>>(in, m.n_elems, d_out);
+  TPT_CHECK_LAUNCH();
+}
+
+void mesh_build_face_offsets(MeshData& m) {
+  if (m.foffs) return;
+  mesh_build_boundary_faces(m);
+  cudaStream_t s = m.ctx->stream;
+  DevBuf<int> cnt;
+  cnt.alloc(m.n_elems, s);
+  face_counts<<<ceil_div(m.n_elems, 128), 128, 0, s>>>(m.n_elems, m.bface.p, cnt.p);
+  TPT_CHECK_LAUNCH();
+  m.face_off.alloc(m.n_elems + 1, s);
+  m.n_bfaces = exclusive_scan_i32(cnt.p, m.face_off.p, m.n_elems, s);
+  m.foffs = true;
+}
+
+void mesh_face_points(MeshData& m, double* d_x, double* d_n) {
+  mesh_build_face_offsets(m);
+  cudaStream_t s = m.ctx->stream;
+  FaceTab f = make_face_tab(m.cell);
+  TPT_CUDA(cudaMemcpyToSymbolAsync(c_face, &f, sizeof(f), 0, cudaMemcpyHostToDevice, s));
+  const ElemIn in = elem_in(m, nullptr, 0, 0, 0.0);
+  const int grid = ceil_div(m.n_elems, 128);
+  if (m.cell == TPTFEM_CELL_TET4)
+    face_points<TPTFEM_CELL_TET4><<<grid, 128, 0, s>>>(in, m.n_elems, m.bface.p, m.face_off.p, d_x, d_n);
+  else if (m.cell == TPTFEM_CELL_TRI3)
+    face_points<TPTFEM_CELL_TRI3><<<grid, 128, 0, s>>>(in, m.n_elems, m.bface.p, m.face_off.p, d_x, d_n);
+  else
+    face_points<TPTFEM_CELL_QUAD4><<<grid, 128, 0, s>>>(in, m.n_elems, m.bface.p, m.face_off.p, d_x, d_n);
+  TPT_CHECK_LAUNCH();
+}
+
+void apply_neumann_points(MeshData& m, int dpn, const double* d_g, unsigned comp_mask, double* d_rhs) {
+  cudaStream_t s = m.ctx->stream;
+  TPT_REQUIRE(dpn >= 1 && dpn <= 3, TPTFEM_ERR_INVALID_ARG, "dofs_per_node must be 1..3");
+  mesh_build_face_offsets(m);
+  FaceTab f = make_face_tab(m.cell);
+  TPT_CUDA(cudaMemcpyToSymbolAsync(c_face, &f, sizeof(f), 0, cudaMemcpyHostToDevice, s));
+  TractionArgs A;
+  A.in = elem_in(m, nullptr, 0, 0, 0.0);
+  A.ne_ptr = m.ne_ptr.p;
+  A.ne = m.ne.p;
+  A.bface = m.bface.p;
+  A.n_nodes = m.n_nodes;
+  A.dpn = dpn;
+  A.axis = 0;
+  A.sign = 1.0;
+  A.t[0] = A.t[1] = A.t[2] = 0.0;
+  A.g = d_g;
+  A.face_off = m.face_off.p;
+  A.comp_mask = comp_mask;
   A.rhs = d_rhs;
   if (m.cell == TPTFEM_CELL_TET4) traction_rows<TPTFEM_CELL_TET4><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);
   else if (m.cell == TPTFEM_CELL_TRI3) traction_rows<TPTFEM_CELL_TRI3><<<ceil_div(m.n_nodes, 128), 128, 0, s>>>(A);

@@ -79,6 +79,22 @@ struct MeshData {
   // per element bitmask of boundary faces (lazy)
   bool bfaces = false;
   DevBuf<unsigned char> bface;
+  // boundary faces numbered in (element, face) order: face_off[e] = faces of
+  // the elements before e (lazy, with n_bfaces)
+  bool foffs = false;
+  DevBuf<int> face_off;
+  int64_t n_bfaces = 0;
+  // Tet4 two-pass assembly plan (lazy): node chunks [tp_nodes[c], tp_nodes[c+1])
+  // whose incident element ids span at most tp_ring, and the element count whose
+  // records exist before chunk c's rows are formed (tp_elems[c])
+  bool tplan = false;
+  int64_t tp_ring = 0;
+  std::vector<int64_t> tp_nodes, tp_elems;
+  // per incidence the chain positions of its four blocks, per neighbour entry
+  // the start of that slot's chain (lazy, Tet4 two-pass assembly)
+  bool tchains = false;
+  DevBuf<uchar4> cpos;
+  DevBuf<unsigned char> coff;
 };
 
 struct MatrixData {
@@ -100,6 +116,12 @@ struct MatrixData {
   // every boundary face)
   int robin = 0, robin_axis = -1;
   double robin_sign = 1.0, robin_h = 0.0;
+  // per-point Robin coefficient h(x, n) at every boundary-face quadrature
+  // point (replaces the face selector when not empty)
+  DevBuf<double> robin_pts;
+  // Tet4 two-pass assembly: per neighbour entry of every node (nb order), the
+  // DPN x DPN mask of its non-zero entries in the current pattern
+  DevBuf<unsigned short> nzmask;
 };
 
 struct SolverWork;  // solver.cu
@@ -206,8 +228,17 @@ void mesh_build_boundary_faces(MeshData& m);
 // assemble.cu
 void assemble_matrix(MatrixData& A);             // symbolic + numeric
 bool reassemble_values(MatrixData& A);           // numeric; false if the pattern changed
-void load_poisson_source(MeshData& m, double s, int quad_order, double* d_rhs);
-void load_body(MeshData& m, const double* body, int quad_order, double* d_rhs);
+// d_pts (optional): the source / body force at every quadrature point
+// (mesh_quad_points order, 1 or dim values per point) instead of the constant.
+void load_poisson_source(MeshData& m, double s, int quad_order, double* d_rhs, const double* d_pts = nullptr);
+void load_body(MeshData& m, const double* body, int quad_order, double* d_rhs, const double* d_pts = nullptr);
+int cell_point_count(int cell, int quad_order);  // quadrature points per element
+int face_point_count(int cell);                  // quadrature points per boundary face
+void mesh_quad_points(MeshData& m, int quad_order, double* d_out);  // n_elems * nq * cdim
+void mesh_build_face_offsets(MeshData& m);
+void mesh_face_points(MeshData& m, double* d_x, double* d_n);  // n_bfaces * nqf * sd each
+// apply_neumann_order with g given at every boundary-face point, onto the components in comp_mask
+void apply_neumann_points(MeshData& m, int dpn, const double* d_g, unsigned comp_mask, double* d_rhs);
 void apply_traction(MeshData& m, int dpn, int axis, double sign, const double* t, double* d_rhs);
 void csr_matvec_f64(tptfem_context* ctx, int64_t nrows, const int* rp, const int* ci, const double* va,
                     const double* x, double* y);

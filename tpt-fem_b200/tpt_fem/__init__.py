@@ -270,15 +270,20 @@ def _coef(mesh, coef):
 def assemble_poisson(mesh, conductivity, quad_order=2, robin=None):
     """assemble(mesh, 1, poisson_element_matrix) -> Matrix (thermal/src/lib.rs:132-160).
 
-    robin=(axis, sign, h) adds apply_robin (assembly/src/lib.rs:674-753) with
-    coefficient h on the boundary faces whose outward normal n has
-    sign * n[axis] > 0.5 (axis=-1: every boundary face), as solve_poisson's
-    `robin` argument does (thermal/src/lib.rs:235-237)."""
+    robin adds apply_robin (assembly/src/lib.rs:674-753), as solve_poisson's
+    `robin` argument does (thermal/src/lib.rs:235-237): a callable h(x, n) of
+    the boundary point and its outward unit normal (numpy arrays), or
+    (axis, sign, h) for the constant h on the boundary faces whose outward
+    normal n has sign * n[axis] > 0.5 (axis=-1: every boundary face)."""
     ctx = mesh.ctx
     c, per = _coef(mesh, conductivity)
     h = C.c_void_p()
     if robin is None:
         ctx.check(ctx.lib.tptfem_assemble_poisson(ctx.h, mesh.h, N.ptr(c), per, quad_order, C.byref(h)))
+    elif callable(robin):  # h(x, n) at every boundary-face quadrature point
+        hv = _eval_flux(mesh, robin)
+        ctx.check(ctx.lib.tptfem_assemble_poisson_robin_points(ctx.h, mesh.h, N.ptr(c), per, quad_order, N.ptr(hv),
+                                                               C.byref(h)))
     else:
         axis, sign, coef = robin
         ctx.check(ctx.lib.tptfem_assemble_poisson_robin(ctx.h, mesh.h, N.ptr(c), per, quad_order, int(axis),
@@ -311,17 +316,80 @@ def assemble_elasticity(mesh, model, young, poisson, quad_order=2):
     return Matrix(h, mesh)
 
 
+def quadrature_points(mesh, quad_order=2):
+    """Physical quadrature points of every element, (n_elems, nq, coord_dim):
+    where the reference calls the source / body-force closure
+    (thermal/src/lib.rs:163-196, elasticity/src/lib.rs:312-348)."""
+    ctx = mesh.ctx
+    nq = C.c_int32()
+    ctx.check(ctx.lib.tptfem_mesh_quadrature_points(ctx.h, mesh.h, quad_order, C.byref(nq), None))
+    pts = np.zeros((mesh.n_elems, nq.value, mesh.cdim))
+    ctx.check(ctx.lib.tptfem_mesh_quadrature_points(ctx.h, mesh.h, quad_order, C.byref(nq), N.ptr(pts)))
+    return pts
+
+
+def boundary_points(mesh):
+    """(x, normal): every boundary face's quadrature points and outward unit
+    normals, (n_points, dim) each, faces in boundary_faces order
+    (assembly/src/lib.rs:563-583): where apply_neumann / apply_robin call their
+    closures."""
+    ctx = mesh.ctx
+    n = C.c_int64()
+    ctx.check(ctx.lib.tptfem_mesh_boundary_points(ctx.h, mesh.h, C.byref(n), None, None))
+    x = np.zeros((n.value, mesh.dim))
+    nrm = np.zeros((n.value, mesh.dim))
+    ctx.check(ctx.lib.tptfem_mesh_boundary_points(ctx.h, mesh.h, C.byref(n), N.ptr(x), N.ptr(nrm)))
+    return x, nrm
+
+
+def _xyz(x):
+    """The reference bindings call a source as f(x, y, z), missing coordinates 0.0."""
+    return (float(x[0]) if len(x) > 0 else 0.0, float(x[1]) if len(x) > 1 else 0.0,
+            float(x[2]) if len(x) > 2 else 0.0)
+
+
+def _eval_flux(mesh, fn):
+    x, nrm = boundary_points(mesh)
+    return np.array([float(fn(xp, n)) for xp, n in zip(x, nrm)], dtype=np.float64)
+
+
 def load_poisson_source(mesh, source, quad_order=2):
+    """The Poisson load loop of solve_poisson (thermal/src/lib.rs:224-230):
+    source is a float or a callable f(x, y, z) evaluated at every quadrature point."""
     rhs = np.zeros(mesh.n_nodes)
-    mesh.ctx.check(mesh.ctx.lib.tptfem_load_poisson_source(mesh.ctx.h, mesh.h, float(source), quad_order,
-                                                           N.ptr(rhs)))
+    ctx = mesh.ctx
+    if callable(source):
+        pts = quadrature_points(mesh, quad_order).reshape(-1, mesh.cdim)
+        sv = np.array([float(source(*_xyz(x))) for x in pts], dtype=np.float64)
+        ctx.check(ctx.lib.tptfem_load_poisson_source_points(ctx.h, mesh.h, N.ptr(sv), quad_order, N.ptr(rhs)))
+    else:
+        ctx.check(ctx.lib.tptfem_load_poisson_source(ctx.h, mesh.h, float(source), quad_order, N.ptr(rhs)))
     return rhs
 
 
 def load_body(mesh, body, quad_order=2):
-    b = N.f64(body)
+    """The body-force loop of solve_elasticity (elasticity/src/lib.rs:371-379):
+    body is a constant vector or a callable b(x, y, z) -> dim values."""
     rhs = np.zeros(mesh.n_nodes * mesh.dim)
-    mesh.ctx.check(mesh.ctx.lib.tptfem_load_body(mesh.ctx.h, mesh.h, N.ptr(b), quad_order, N.ptr(rhs)))
+    ctx = mesh.ctx
+    if callable(body):
+        pts = quadrature_points(mesh, quad_order).reshape(-1, mesh.cdim)
+        bv = np.array([[float(v) for v in list(body(*_xyz(x)))[:mesh.dim]] for x in pts], dtype=np.float64)
+        ctx.check(ctx.lib.tptfem_load_body_points(ctx.h, mesh.h, N.ptr(bv), quad_order, N.ptr(rhs)))
+    else:
+        b = N.f64(body)
+        ctx.check(ctx.lib.tptfem_load_body(ctx.h, mesh.h, N.ptr(b), quad_order, N.ptr(rhs)))
+    return rhs
+
+
+def apply_neumann(mesh, dofs_per_node, flux, rhs, comp_mask=0xFFFFFFFF):
+    """rhs += apply_neumann (assembly/src/lib.rs:591-667) with the flux g(x, n)
+    of the boundary point and its outward unit normal (numpy arrays), applied
+    to every component in comp_mask (in place)."""
+    assert rhs.dtype == np.float64 and rhs.flags["C_CONTIGUOUS"]
+    g = _eval_flux(mesh, flux)
+    ctx = mesh.ctx
+    ctx.check(ctx.lib.tptfem_apply_neumann_points(ctx.h, mesh.h, dofs_per_node, N.ptr(g), comp_mask, N.ptr(rhs)))
     return rhs
 
 
@@ -489,10 +557,19 @@ class ElasticitySolution:
         return np.asarray(self.values, dtype=np.float64).reshape(self.mesh.node_count(), self.dim)
 
 
-def solve_poisson(mesh, conductivity, quad_order, source, bcs, **kw):
-    """solve_poisson of the reference bindings (crates/tpt-fem-py/src/lib.rs:102-199), constant source."""
-    if callable(source):
-        raise NotImplementedError("callable sources: evaluate on quadrature points first")
+def solve_poisson(mesh, conductivity, quad_order, source, bcs, neumann=None, robin=None, **kw):
+    """solve_poisson of the reference bindings (crates/tpt-fem-py/src/lib.rs:102-199):
+    source is a float or a callable f(x, y, z); neumann and robin are the
+    optional flux g(x, n) and Robin coefficient h(x, n) of the Rust function
+    (crates/tpt-fem-thermal/src/lib.rs:206-240), each a callable of the boundary
+    point and its outward unit normal."""
+    if callable(source) or neumann is not None or robin is not None:
+        K = assemble_poisson(mesh, conductivity, quad_order, robin=robin)
+        rhs = load_poisson_source(mesh, source, quad_order)
+        if neumann is not None:
+            apply_neumann(mesh, 1, neumann, rhs)
+        u, st = solve_with_dirichlet(K, rhs, bcs, **kw)
+        return PoissonSolution(mesh, [float(v) for v in u], st)
     ctx = mesh.ctx
     dof, val = _bcs(bcs)
     u = np.zeros(mesh.n_nodes)
@@ -506,11 +583,16 @@ def solve_poisson(mesh, conductivity, quad_order, source, bcs, **kw):
 def solve_elasticity(mesh, model, young, poisson, quad_order, bcs, body=None, **kw):
     """solve_elasticity of the reference bindings (crates/tpt-fem-py/src/lib.rs:213-252).
 
-    ``bcs`` are (node_id, component, value) triples; zero body force unless ``body`` is given.
+    ``bcs`` are (node_id, component, value) triples; zero body force unless
+    ``body`` is given, as a constant vector or a callable b(x, y, z) -> dim values.
     """
     ctx = mesh.ctx
     dim = mesh.dim
     dofs = [(int(n) * dim + int(c), float(v)) for n, c, v in bcs]
+    if callable(body):
+        K = assemble_elasticity(mesh, model, young, poisson, quad_order)
+        u, st = solve_with_dirichlet(K, load_body(mesh, body, quad_order), dofs, **kw)
+        return ElasticitySolution(mesh, [float(v) for v in u], dim, st)
     dof, val = _bcs(dofs)
     b = N.f64(body if body is not None else np.zeros(dim))
     u = np.zeros(mesh.n_nodes * dim)

@@ -71,7 +71,21 @@ _pi64 = C.POINTER(C.c_int64)
 _pd = C.POINTER(C.c_double)
 _pint = C.POINTER(C.c_int)
 
+SOURCE_FN = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_int, C.c_void_p)
+FLUX_FN = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, C.c_void_p)
+BODY_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.c_void_p)
+
 SIGNATURES = {
+    "tptfem_mesh_quadrature_points": (C.c_int, [_vp, _vp, C.c_int, C.POINTER(C.c_int32), _vp]),
+    "tptfem_mesh_boundary_points": (C.c_int, [_vp, _vp, _pi64, _vp, _vp]),
+    "tptfem_load_poisson_source_points": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp]),
+    "tptfem_load_body_points": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp]),
+    "tptfem_apply_neumann_points": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_uint32, _vp]),
+    "tptfem_assemble_poisson_robin_points": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _vp, _pp]),
+    "tptfem_solve_poisson_fn": (C.c_int, [_vp, _vp, C.c_double, C.c_int, SOURCE_FN, _vp, _vp, _vp, _i64, FLUX_FN,
+                                          _vp, FLUX_FN, _vp, _vp, _vp, _vp]),
+    "tptfem_solve_elasticity_fn": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_double, C.c_int, BODY_FN, _vp,
+                                             _vp, _vp, _i64, _vp, _vp, _vp]),
     "tptfem_system_refresh": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "tptfem_system_coarse": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                        C.c_void_p, C.c_void_p]),
