@@ -25,6 +25,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 
 #include "objects.hpp"
 
@@ -800,11 +801,10 @@ int tet_minb() {
   return v;
 }
 
+// Element e's record (geometry and constitutive constants); false for a
+// degenerate element.
 template <int PHYS>
-__global__ void __launch_bounds__(256) tet_records(ElemIn in, int64_t e0, int64_t e1, int64_t ring,
-                                                   double* __restrict__ rec, int* flag) {
-  const int64_t e = e0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= e1) return;
+__device__ __forceinline__ bool tet_record(const ElemIn& in, int64_t e, double (&r)[TR_DOUBLES]) {
   double X[4][3];
   int nodes[4];
   load_elem<TPTFEM_CELL_TET4>(in, (int)e, X, nodes);
@@ -812,7 +812,6 @@ __global__ void __launch_bounds__(256) tet_records(ElemIn in, int64_t e0, int64_
   const bool ok = tet_geom(X, G);
   const double coef = in.coef[in.per_elem ? e : 0];
   const double w0 = c_cell.w[0];
-  double r[TR_DOUBLES];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -828,14 +827,20 @@ __global__ void __launch_bounds__(256) tet_records(ElemIn in, int64_t e0, int64_
     r[13] = G.adet;
     r[14] = r[15] = 0.0;
   }
+  return ok;
+}
+
+template <int PHYS>
+__global__ void __launch_bounds__(256) tet_records(ElemIn in, int64_t e0, int64_t e1, int64_t ring,
+                                                   double* __restrict__ rec, int* flag) {
+  const int64_t e = e0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= e1) return;
+  double r[TR_DOUBLES];
+  const bool ok = tet_record<PHYS>(in, e, r);
   double2* dst = reinterpret_cast<double2*>(rec + (e % ring) * TR_DOUBLES);
 #pragma unroll
   for (int q = 0; q < TR_DOUBLES / 2; ++q) dst[q] = make_double2(r[2 * q], r[2 * q + 1]);
   if (!ok) atomicOr(flag, 1);
-}
-
-__device__ __forceinline__ unsigned nonzero_bit(double v) {
-  return (unsigned)((__double_as_longlong(v) << 1) != 0);  // v != +-0.0, without an FP64 compare
 }
 
 // Chains (once per mesh): node n's entries in neighbour slot s are summed over
@@ -894,7 +899,7 @@ __global__ void tet_chains(int64_t n_nodes, const int* __restrict__ ne_ptr, cons
 //   NUMERIC: the masks must equal the stored ones (else flag bit 2: the
 //     pattern changed); values go to the positions the pattern gives them,
 //     without reading the column indices back.
-template <int PHYS, int DPN, int MAXDEG, int MINB>
+template <int PHYS, int DPN, int MAXDEG, int MINB, bool REC>
 __global__ void __launch_bounds__(32 * TN_WARPS, MINB) tet_node_rows(RowArgs A, int64_t n0, int64_t n1,
                                                                      const double* __restrict__ rec, int64_t ring,
                                                                      const uchar4* __restrict__ cpos,
@@ -921,13 +926,17 @@ __global__ void __launch_bounds__(32 * TN_WARPS, MINB) tet_node_rows(RowArgs A, 
   if (lane < deg) {
     const int pe = A.ne[k0 + lane];
     const uchar4 cp = cpos[k0 + lane];
-    const double2* src = reinterpret_cast<const double2*>(rec + ((int64_t)(pe >> 2) % ring) * TR_DOUBLES);
     double r[TR_DOUBLES];
+    if constexpr (REC) {  // the record of pass 1
+      const double2* src = reinterpret_cast<const double2*>(rec + ((int64_t)(pe >> 2) % ring) * TR_DOUBLES);
 #pragma unroll
-    for (int q = 0; q < TR_DOUBLES / 2; ++q) {
-      const double2 v = __ldcg(src + q);
-      r[2 * q] = v.x;
-      r[2 * q + 1] = v.y;
+      for (int q = 0; q < TR_DOUBLES / 2; ++q) {
+        const double2 v = __ldcg(src + q);
+        r[2 * q] = v.x;
+        r[2 * q + 1] = v.y;
+      }
+    } else {  // one pass: the record formed here, for each of the element's nodes
+      if (!tet_record<PHYS>(A.in, pe >> 2, r)) atomicOr(A.flag, 1);
     }
     const int l = pe & 3;
     double gl[3];  // the node's own gradient row, selected without a dynamic register index
@@ -1376,6 +1385,32 @@ void tet_build_chains(MeshData& m) {
   m.tchains = true;
 }
 
+template <int PHYS, int DPN, bool REC>
+void launch_node_rows(MatrixData& M, int mode, const RowArgs& A, int64_t n0, int64_t n1, const double* ring,
+                      cudaStream_t s) {
+  MeshData& m = *M.mesh;
+  const int grid = ceil_div(n1 - n0, TN_WARPS);
+  // fewer incidences per node, less shared memory per warp, more warps per SM
+  const bool d24 = m.max_deg <= 24, b16 = tet_minb() == 16;
+  auto go = [&](auto kern) {
+    kern<<<grid, 32 * TN_WARPS, 0, s>>>(A, n0, n1, ring, m.tp_ring, m.cpos.p, m.coff.p, M.nzmask.p, mode);
+  };
+  if (d24 && b16) go(tet_node_rows<PHYS, DPN, 24, 16, REC>);
+  else if (d24) go(tet_node_rows<PHYS, DPN, 24, 8, REC>);
+  else if (b16) go(tet_node_rows<PHYS, DPN, 32, 16, REC>);
+  else go(tet_node_rows<PHYS, DPN, 32, 8, REC>);
+  TPT_CHECK_LAUNCH();
+}
+
+// One launch over all nodes, each warp forming its elements' records itself.
+template <int PHYS, int DPN>
+void launch_tet_chain_one_pass(MatrixData& M, int mode, const RowArgs& A, cudaStream_t s) {
+  MeshData& m = *M.mesh;
+  tet_build_chains(m);
+  if (M.nzmask.n != m.nb.n) M.nzmask.alloc(m.nb.n, s);
+  launch_node_rows<PHYS, DPN, false>(M, mode, A, 0, m.n_nodes, nullptr, s);
+}
+
 template <int PHYS, int DPN>
 void launch_tet_two_pass(MatrixData& M, int mode, const RowArgs& A, cudaStream_t s) {
   MeshData& m = *M.mesh;
@@ -1392,30 +1427,21 @@ void launch_tet_two_pass(MatrixData& M, int mode, const RowArgs& A, cudaStream_t
       TPT_CHECK_LAUNCH();
       done = e1;
     }
-    const int64_t n0 = m.tp_nodes[c], n1 = m.tp_nodes[c + 1];
-    const int grid = ceil_div(n1 - n0, TN_WARPS);
-    // fewer incidences per node, less shared memory per warp, more warps per SM
-    const bool d24 = m.max_deg <= 24, b16 = tet_minb() == 16;
-    if (d24 && b16)
-      tet_node_rows<PHYS, DPN, 24, 16><<<grid, 32 * TN_WARPS, 0, s>>>(A, n0, n1, ring.p, m.tp_ring, m.cpos.p, m.coff.p, M.nzmask.p, mode);
-    else if (d24)
-      tet_node_rows<PHYS, DPN, 24, 8><<<grid, 32 * TN_WARPS, 0, s>>>(A, n0, n1, ring.p, m.tp_ring, m.cpos.p, m.coff.p, M.nzmask.p, mode);
-    else if (b16)
-      tet_node_rows<PHYS, DPN, 32, 16><<<grid, 32 * TN_WARPS, 0, s>>>(A, n0, n1, ring.p, m.tp_ring, m.cpos.p, m.coff.p, M.nzmask.p, mode);
-    else
-      tet_node_rows<PHYS, DPN, 32, 8><<<grid, 32 * TN_WARPS, 0, s>>>(A, n0, n1, ring.p, m.tp_ring, m.cpos.p, m.coff.p, M.nzmask.p, mode);
-    TPT_CHECK_LAUNCH();
+    launch_node_rows<PHYS, DPN, true>(M, mode, A, m.tp_nodes[c], m.tp_nodes[c + 1], ring.p, s);
   }
 }
 
-// TPTFEM_TET_ONE_PASS=1 selects the one-pass kernel (assemble_nodes_tet) for A/B timing.
-bool tet_one_pass() {
+// Tet4 assembly kernel (TPTFEM_TET_ASM selects one for A/B timing):
+//   0 "records": element records in an L2 ring, then tet_node_rows (default)
+//   1 "chains":  tet_node_rows forming each element's record per node, one launch
+//   2 "warp":    assemble_nodes_tet
+int tet_variant() {
   static int v = -1;
   if (v < 0) {
-    const char* e = std::getenv("TPTFEM_TET_ONE_PASS");
-    v = (e && e[0] == '1') ? 1 : 0;
+    const char* e = std::getenv("TPTFEM_TET_ASM");
+    v = !e ? 0 : (std::strcmp(e, "chains") == 0 ? 1 : (std::strcmp(e, "warp") == 0 ? 2 : 0));
   }
-  return v == 1;
+  return v;
 }
 
 template <int PHYS, int DPN>
@@ -1446,10 +1472,14 @@ void launch_rows(int mode, const RowArgs& A, cudaStream_t s) {
 void dispatch_rows(MatrixData& M, int mode, const RowArgs& A, cudaStream_t s) {
   const int cell = M.mesh->cell;
   const MeshData& m = *M.mesh;
-  if (cell == TPTFEM_CELL_TET4 && !A.robin && m.max_nb <= 32 && m.max_deg <= TN_MAXDEG && !tet_one_pass()) {
+  if (cell == TPTFEM_CELL_TET4 && !A.robin && m.max_nb <= 32 && m.max_deg <= TN_MAXDEG && tet_variant() == 0) {
     // element records, then a warp per node: at most 32 neighbour slots and incident elements
     if (M.physics == 0) launch_tet_two_pass<0, 1>(M, mode, A, s);
     else launch_tet_two_pass<1, 3>(M, mode, A, s);
+  } else if (cell == TPTFEM_CELL_TET4 && !A.robin && m.max_nb <= 32 && m.max_deg <= TN_MAXDEG &&
+             tet_variant() == 1) {
+    if (M.physics == 0) launch_tet_chain_one_pass<0, 1>(M, mode, A, s);
+    else launch_tet_chain_one_pass<1, 3>(M, mode, A, s);
   } else if (cell == TPTFEM_CELL_TET4 && !A.robin && m.max_nb <= 32 && m.max_deg <= AN_MAXDEG) {
     if (M.physics == 0) launch_nodes_tet<0, 1>(mode, A, m.n_nodes, s);
     else launch_nodes_tet<1, 3>(mode, A, m.n_nodes, s);
