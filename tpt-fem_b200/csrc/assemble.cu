@@ -769,18 +769,20 @@ __global__ void __launch_bounds__(32 * AN_WARPS) assemble_nodes_tet(RowArgs A, i
   }
 }
 
-// ---- Tet4 rows in two passes ------------------------------------------------------
-// assemble_nodes_tet recomputes an element's geometry for each of its four
-// nodes, and its FP64 work (no FMA, for exactness) is the limit.  Here pass 1
-// (tet_records, one thread per element) computes each element's geometry and
-// constitutive constants once into a 128-byte record; pass 2 (tet_node_rows,
-// one warp per node) forms the node's element-row blocks from those records
-// and sums them in element order exactly as assemble_nodes_tet does.  The
-// records live in a ring of `ring` elements sized to stay in L2: the nodes
-// are processed in chunks whose incident elements span at most `ring` ids,
-// each chunk's missing records are written just before it (slot e % ring),
-// and the value stores stream past L2 (st.global.cs), so the records are
-// written and read in L2 instead of making a round trip through HBM.
+// ---- Tet4 rows through ordered chains ---------------------------------------------
+// assemble_nodes_tet adds each incidence's blocks into the node's slots in a
+// loop over all incidences in which only the few lanes owning the element's
+// slots work, with an FP64 compare per value for the pattern; its issue slots,
+// not HBM, are the limit.  tet_node_rows keeps one warp per node but sums
+// every slot over a precomputed chain -- the incidences whose element holds
+// that slot's node, in ascending element id -- so each addition is done by
+// the lane that needs it, and the node's own slot (whose chain has every
+// incident element) is spread over one lane per entry.  A one-element
+// "record" (gradients, w|det|, constitutive constants) is formed per
+// incidence; the value stores stream past L2 (st.global.cs).  Forming the
+// records once per element in a separate pass and reading them back from an
+// L2-resident ring was measured slower (6.2 against 3.3 ms at 280x70x70)
+// than forming them per incidence, and was not kept.
 //
 // Record (16 doubles): g[4][3], the element's physical gradients, then
 //   elasticity: w |det|, D00, D01, Dshear;  Poisson: w k, |det|, 0, 0.
@@ -828,19 +830,6 @@ __device__ __forceinline__ bool tet_record(const ElemIn& in, int64_t e, double (
     r[14] = r[15] = 0.0;
   }
   return ok;
-}
-
-template <int PHYS>
-__global__ void __launch_bounds__(256) tet_records(ElemIn in, int64_t e0, int64_t e1, int64_t ring,
-                                                   double* __restrict__ rec, int* flag) {
-  const int64_t e = e0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= e1) return;
-  double r[TR_DOUBLES];
-  const bool ok = tet_record<PHYS>(in, e, r);
-  double2* dst = reinterpret_cast<double2*>(rec + (e % ring) * TR_DOUBLES);
-#pragma unroll
-  for (int q = 0; q < TR_DOUBLES / 2; ++q) dst[q] = make_double2(r[2 * q], r[2 * q + 1]);
-  if (!ok) atomicOr(flag, 1);
 }
 
 // Chains (once per mesh): node n's entries in neighbour slot s are summed over
@@ -899,9 +888,8 @@ __global__ void tet_chains(int64_t n_nodes, const int* __restrict__ ne_ptr, cons
 //   NUMERIC: the masks must equal the stored ones (else flag bit 2: the
 //     pattern changed); values go to the positions the pattern gives them,
 //     without reading the column indices back.
-template <int PHYS, int DPN, int MAXDEG, int MINB, bool REC>
+template <int PHYS, int DPN, int MAXDEG, int MINB>
 __global__ void __launch_bounds__(32 * TN_WARPS, MINB) tet_node_rows(RowArgs A, int64_t n0, int64_t n1,
-                                                                     const double* __restrict__ rec, int64_t ring,
                                                                      const uchar4* __restrict__ cpos,
                                                                      const unsigned char* __restrict__ coff,
                                                                      unsigned short* __restrict__ nzm, int mode) {
@@ -927,17 +915,7 @@ __global__ void __launch_bounds__(32 * TN_WARPS, MINB) tet_node_rows(RowArgs A, 
     const int pe = A.ne[k0 + lane];
     const uchar4 cp = cpos[k0 + lane];
     double r[TR_DOUBLES];
-    if constexpr (REC) {  // the record of pass 1
-      const double2* src = reinterpret_cast<const double2*>(rec + ((int64_t)(pe >> 2) % ring) * TR_DOUBLES);
-#pragma unroll
-      for (int q = 0; q < TR_DOUBLES / 2; ++q) {
-        const double2 v = __ldcg(src + q);
-        r[2 * q] = v.x;
-        r[2 * q + 1] = v.y;
-      }
-    } else {  // one pass: the record formed here, for each of the element's nodes
-      if (!tet_record<PHYS>(A.in, pe >> 2, r)) atomicOr(A.flag, 1);
-    }
+    if (!tet_record<PHYS>(A.in, pe >> 2, r)) atomicOr(A.flag, 1);
     const int l = pe & 3;
     double gl[3];  // the node's own gradient row, selected without a dynamic register index
 #pragma unroll
@@ -1322,58 +1300,6 @@ int read_flag(tptfem_context* ctx) {
   return ctx->h_pinned[0];
 }
 
-__global__ void node_elem_span(int64_t n_nodes, const int* __restrict__ ne_ptr, const int* __restrict__ ne,
-                               int2* __restrict__ out) {
-  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= n_nodes) return;
-  const int b = ne_ptr[n], e = ne_ptr[n + 1];
-  out[n] = b < e ? make_int2(ne[b] >> 2, ne[e - 1] >> 2) : make_int2(INT_MAX, -1);
-}
-
-// Ring size of the two-pass Tet4 assembly, in MB of records (48 MB of the
-// 126 MB L2 by default; TPTFEM_TET_RING_MB overrides it for tuning).
-int64_t tet_ring_target() {
-  const char* v = std::getenv("TPTFEM_TET_RING_MB");
-  const long mb = v ? std::atol(v) : 48;
-  return std::max<int64_t>(1, (int64_t)std::max(1L, mb) * (1 << 20) / (TR_DOUBLES * 8));
-}
-
-// Node chunks whose incident elements span at most `ring` ids (the element
-// lists are sorted by id, so a node's span is its last id minus its first).
-void tet_plan(MeshData& m) {
-  if (m.tplan) return;
-  cudaStream_t s = m.ctx->stream;
-  DevBuf<int2> d;
-  d.alloc(std::max<int64_t>(m.n_nodes, 1), s);
-  node_elem_span<<<ceil_div(m.n_nodes, 256), 256, 0, s>>>(m.n_nodes, m.ne_ptr.p, m.ne.p, d.p);
-  TPT_CHECK_LAUNCH();
-  std::vector<int2> h(m.n_nodes);
-  device_to_host(m.ctx, h.data(), d.p, m.n_nodes * sizeof(int2));
-  int64_t ring = tet_ring_target();
-  for (const int2& v : h)
-    if (v.y >= 0) ring = std::max<int64_t>(ring, (int64_t)v.y - v.x + 1);
-  ring = std::max<int64_t>(1, std::min<int64_t>(ring, m.n_elems));
-  m.tp_nodes.clear();
-  m.tp_elems.clear();
-  int64_t n0 = 0, done = 0;
-  while (n0 < m.n_nodes) {
-    int64_t lo = INT64_MAX, hi = -1, n = n0;
-    for (; n < m.n_nodes; ++n) {
-      const int64_t nlo = std::min<int64_t>(lo, h[n].x), nhi = std::max<int64_t>(hi, h[n].y);
-      if (n > n0 && nhi >= 0 && nhi - nlo + 1 > ring) break;
-      lo = nlo;
-      hi = nhi;
-    }
-    done = std::max(done, hi + 1);
-    m.tp_nodes.push_back(n0);
-    m.tp_elems.push_back(done);
-    n0 = n;
-  }
-  m.tp_nodes.push_back(m.n_nodes);
-  m.tp_ring = ring;
-  m.tplan = true;
-}
-
 void tet_build_chains(MeshData& m) {
   if (m.tchains) return;
   cudaStream_t s = m.ctx->stream;
@@ -1385,63 +1311,33 @@ void tet_build_chains(MeshData& m) {
   m.tchains = true;
 }
 
-template <int PHYS, int DPN, bool REC>
-void launch_node_rows(MatrixData& M, int mode, const RowArgs& A, int64_t n0, int64_t n1, const double* ring,
-                      cudaStream_t s) {
+template <int PHYS, int DPN>
+void launch_tet_chains(MatrixData& M, int mode, const RowArgs& A, cudaStream_t s) {
   MeshData& m = *M.mesh;
-  const int grid = ceil_div(n1 - n0, TN_WARPS);
+  tet_build_chains(m);
+  if (M.nzmask.n != m.nb.n) M.nzmask.alloc(m.nb.n, s);
+  const int grid = ceil_div(m.n_nodes, TN_WARPS);
   // fewer incidences per node, less shared memory per warp, more warps per SM
   const bool d24 = m.max_deg <= 24, b16 = tet_minb() == 16;
   auto go = [&](auto kern) {
-    kern<<<grid, 32 * TN_WARPS, 0, s>>>(A, n0, n1, ring, m.tp_ring, m.cpos.p, m.coff.p, M.nzmask.p, mode);
+    kern<<<grid, 32 * TN_WARPS, 0, s>>>(A, 0, m.n_nodes, m.cpos.p, m.coff.p, M.nzmask.p, mode);
   };
-  if (d24 && b16) go(tet_node_rows<PHYS, DPN, 24, 16, REC>);
-  else if (d24) go(tet_node_rows<PHYS, DPN, 24, 8, REC>);
-  else if (b16) go(tet_node_rows<PHYS, DPN, 32, 16, REC>);
-  else go(tet_node_rows<PHYS, DPN, 32, 8, REC>);
+  if (d24 && b16) go(tet_node_rows<PHYS, DPN, 24, 16>);
+  else if (d24) go(tet_node_rows<PHYS, DPN, 24, 8>);
+  else if (b16) go(tet_node_rows<PHYS, DPN, 32, 16>);
+  else go(tet_node_rows<PHYS, DPN, 32, 8>);
   TPT_CHECK_LAUNCH();
 }
 
-// One launch over all nodes, each warp forming its elements' records itself.
-template <int PHYS, int DPN>
-void launch_tet_chain_one_pass(MatrixData& M, int mode, const RowArgs& A, cudaStream_t s) {
-  MeshData& m = *M.mesh;
-  tet_build_chains(m);
-  if (M.nzmask.n != m.nb.n) M.nzmask.alloc(m.nb.n, s);
-  launch_node_rows<PHYS, DPN, false>(M, mode, A, 0, m.n_nodes, nullptr, s);
-}
-
-template <int PHYS, int DPN>
-void launch_tet_two_pass(MatrixData& M, int mode, const RowArgs& A, cudaStream_t s) {
-  MeshData& m = *M.mesh;
-  tet_plan(m);
-  tet_build_chains(m);
-  if (M.nzmask.n != m.nb.n) M.nzmask.alloc(m.nb.n, s);
-  DevBuf<double> ring;
-  ring.alloc(m.tp_ring * TR_DOUBLES, s);
-  int64_t done = 0;
-  for (size_t c = 0; c + 1 < m.tp_nodes.size(); ++c) {
-    const int64_t e1 = m.tp_elems[c];
-    if (e1 > done) {
-      tet_records<PHYS><<<ceil_div(e1 - done, 256), 256, 0, s>>>(A.in, done, e1, m.tp_ring, ring.p, A.flag);
-      TPT_CHECK_LAUNCH();
-      done = e1;
-    }
-    launch_node_rows<PHYS, DPN, true>(M, mode, A, m.tp_nodes[c], m.tp_nodes[c + 1], ring.p, s);
-  }
-}
-
-// Tet4 assembly kernel (TPTFEM_TET_ASM selects one for A/B timing):
-//   0 "records": element records in an L2 ring, then tet_node_rows (default)
-//   1 "chains":  tet_node_rows forming each element's record per node, one launch
-//   2 "warp":    assemble_nodes_tet
-int tet_variant() {
+// TPTFEM_TET_ASM=warp selects assemble_nodes_tet instead of tet_node_rows
+// (for A/B timing; both give the same bits).
+bool tet_warp_kernel() {
   static int v = -1;
   if (v < 0) {
     const char* e = std::getenv("TPTFEM_TET_ASM");
-    v = !e ? 0 : (std::strcmp(e, "chains") == 0 ? 1 : (std::strcmp(e, "warp") == 0 ? 2 : 0));
+    v = (e && std::strcmp(e, "warp") == 0) ? 1 : 0;
   }
-  return v;
+  return v == 1;
 }
 
 template <int PHYS, int DPN>
@@ -1472,14 +1368,10 @@ void launch_rows(int mode, const RowArgs& A, cudaStream_t s) {
 void dispatch_rows(MatrixData& M, int mode, const RowArgs& A, cudaStream_t s) {
   const int cell = M.mesh->cell;
   const MeshData& m = *M.mesh;
-  if (cell == TPTFEM_CELL_TET4 && !A.robin && m.max_nb <= 32 && m.max_deg <= TN_MAXDEG && tet_variant() == 0) {
-    // element records, then a warp per node: at most 32 neighbour slots and incident elements
-    if (M.physics == 0) launch_tet_two_pass<0, 1>(M, mode, A, s);
-    else launch_tet_two_pass<1, 3>(M, mode, A, s);
-  } else if (cell == TPTFEM_CELL_TET4 && !A.robin && m.max_nb <= 32 && m.max_deg <= TN_MAXDEG &&
-             tet_variant() == 1) {
-    if (M.physics == 0) launch_tet_chain_one_pass<0, 1>(M, mode, A, s);
-    else launch_tet_chain_one_pass<1, 3>(M, mode, A, s);
+  if (cell == TPTFEM_CELL_TET4 && !A.robin && m.max_nb <= 32 && m.max_deg <= TN_MAXDEG && !tet_warp_kernel()) {
+    // a warp per node: at most 32 neighbour slots and incident elements
+    if (M.physics == 0) launch_tet_chains<0, 1>(M, mode, A, s);
+    else launch_tet_chains<1, 3>(M, mode, A, s);
   } else if (cell == TPTFEM_CELL_TET4 && !A.robin && m.max_nb <= 32 && m.max_deg <= AN_MAXDEG) {
     if (M.physics == 0) launch_nodes_tet<0, 1>(mode, A, m.n_nodes, s);
     else launch_nodes_tet<1, 3>(mode, A, m.n_nodes, s);

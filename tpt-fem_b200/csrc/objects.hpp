@@ -84,14 +84,8 @@ struct MeshData {
   bool foffs = false;
   DevBuf<int> face_off;
   int64_t n_bfaces = 0;
-  // Tet4 two-pass assembly plan (lazy): node chunks [tp_nodes[c], tp_nodes[c+1])
-  // whose incident element ids span at most tp_ring, and the element count whose
-  // records exist before chunk c's rows are formed (tp_elems[c])
-  bool tplan = false;
-  int64_t tp_ring = 0;
-  std::vector<int64_t> tp_nodes, tp_elems;
   // per incidence the chain positions of its four blocks, per neighbour entry
-  // the start of that slot's chain (lazy, Tet4 two-pass assembly)
+  // the start of that slot's chain (lazy, Tet4 chain assembly)
   bool tchains = false;
   DevBuf<uchar4> cpos;
   DevBuf<unsigned char> coff;
@@ -119,7 +113,7 @@ struct MatrixData {
   // per-point Robin coefficient h(x, n) at every boundary-face quadrature
   // point (replaces the face selector when not empty)
   DevBuf<double> robin_pts;
-  // Tet4 two-pass assembly: per neighbour entry of every node (nb order), the
+  // Tet4 chain assembly: per neighbour entry of every node (nb order), the
   // DPN x DPN mask of its non-zero entries in the current pattern
   DevBuf<unsigned short> nzmask;
 };
