@@ -313,8 +313,11 @@ def run_ours(args, world, rank, local):
     if rank == 0:
         coords = mesh.coords_array.copy()
         conn = mesh.conn_array.copy()
-        e2e = [e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model, coarse) for _ in range(2)]
-        e2e_s, h2d, d2h, e2e_st = min(e2e, key=lambda t: t[0])
+        # one untimed run pays the first-use costs (the pinned staging buffer,
+        # library module loads); then the median of three timed runs
+        e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model, coarse)
+        e2e = [e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model, coarse) for _ in range(3)]
+        e2e_s, h2d, d2h, e2e_st = sorted(e2e, key=lambda t: t[0])[1]
         phases = {}
         e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model, coarse, phases)
         # the plain method on the host cores: one complete solve of this exact
@@ -673,9 +676,9 @@ def run_topopt(args, world, rank, local):
     return out
 
 
-# ncu DRAM read + write of one numeric assemble_nodes_tet launch on the
+# ncu DRAM read + write of one numeric tet_node_rows launch on the
 # 140x35x35 cantilever (1,029,000 tets); scaled by tets to the measured mesh
-ASM_TRAFFIC_140 = (157.871616 + 121.000192) * 1e6
+ASM_TRAFFIC_140 = (84.786688 + 110.981888) * 1e6
 ASM_TETS_140 = 1029000
 
 
@@ -748,7 +751,7 @@ def run_assembly(args, world, rank, local):
                           "nodes": n_nodes,
                           "nnz": nnz, "per_element_E": True, "parallelism": f"replicas{world}",
                           "l2": "inputs and output larger than L2 (values %.2f GB)" % (8e-9 * nnz)},
-               "roofline": {"bound": "hbm", "kernel": "assemble_nodes_tet<1,3> (NUMERIC: bit-exact FP64, no FMA)",
+               "roofline": {"bound": "hbm", "kernel": "tet_node_rows<1,3,24,16> (NUMERIC: bit-exact FP64, no FMA)",
                             "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "peak_kind": kind, "unit": "GB/s",
                             "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": ASM_TRAFFIC_140 * n_el / ASM_TETS_140,
                             "traffic_source": "ncu dram__bytes_read+write of the kernel at 140x35x35 scaled by tets",
