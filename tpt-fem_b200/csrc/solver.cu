@@ -321,12 +321,15 @@ void select_nb_mode(SystemData& S, Engine<double>& E, const tptfem_solver_opts& 
 int select_coarse(SystemData& S, Engine<double>& E, const tptfem_solver_opts& o, bool fresh) {
   bool want = (o.flags & TPTFEM_SOLVE_COARSE) && E.nb_pc;
   PhaseTimer timer(S.ctx->stream, "coarse space");
-  // default: about one aggregate per 2800 node groups for vector problems (6 or
+  // default: about one aggregate per 2000 node groups for vector problems (6 or
   // 3 rigid modes each) and per 700 for scalar ones (one constant mode each),
-  // between 8 and 3000.  Measured optima: 504 aggregates (3000 coarse unknowns)
-  // for elasticity at 280x70x70, 2744 for the 128^3 Poisson random-field
-  // problems (23.9 ms per solve against 26.1 ms with 729).
-  const int per = S.dpn == 1 ? 700 : 2800;
+  // between 8 and 3000.  Measured (fresh set-up + solve, learned FSAI): at
+  // 280x70x70, 700 aggregates (3300 coarse unknowns) 96.9 ms against 98.9 with
+  // 500, 105.3 with 350 and 103.5 with 1000, where the dense coarse set-up
+  // grows faster than the iterations fall; at 400x100x100, 1000-1365
+  // aggregates 287-291 ms against 309 with 700; for the 128^3 Poisson
+  // random-field problems 2744 (23.9 ms per solve against 26.1 ms with 729).
+  const int per = S.dpn == 1 ? 700 : 2000;
   const int aggs = o.coarse_aggregates > 0 ? o.coarse_aggregates : std::max(8, std::min(3000, S.nb.ngroups / per));
   if (want) want = coarse_build(S, aggs);
   if (want && (fresh || !S.coarse.ready)) want = coarse_assemble(S);
