@@ -995,11 +995,22 @@ __global__ void __launch_bounds__(32 * TN_WARPS, MINB) tet_node_rows(RowArgs A, 
     const int sc0 = __shfl_sync(0xffffffffu, c0, self), sc1 = __shfl_sync(0xffffffffu, c1, self);
     double sv = 0.0;
     unsigned snz = 0;
-    if (lane < D2)
-      for (int c = sc0; c < sc1; ++c) {
+    if (lane < D2) {  // loads run ahead of the dependent additions, four at a time
+      int c = sc0;
+      for (; c + 4 <= sc1; c += 4) {
+        const double v0 = chain[w][c][lane], v1 = chain[w][c + 1][lane], v2 = chain[w][c + 2][lane],
+                     v3 = chain[w][c + 3][lane];
+        snz |= cnz[w][c] | cnz[w][c + 1] | cnz[w][c + 2] | cnz[w][c + 3];
+        sv = sv + v0;
+        sv = sv + v1;
+        sv = sv + v2;
+        sv = sv + v3;
+      }
+      for (; c < sc1; ++c) {
         sv = sv + chain[w][c][lane];
         snz |= cnz[w][c];
       }
+    }
 #pragma unroll
     for (int q = 0; q < D2; ++q) {
       const double t = __shfl_sync(0xffffffffu, sv, q);
