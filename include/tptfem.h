@@ -290,7 +290,8 @@ tptfem_status tptfem_solve_elasticity_fn(tptfem_context* ctx, tptfem_mesh* mesh,
  * No counterpart in the reference (its solve is single-threaded).  The reduced system is
  * split into contiguous row ranges row_starts[k] .. row_starts[k+1] (node-aligned: the
  * x-slabs of a box mesh); rank k, on its own GPU, creates its part from the whole reduced
- * system and runs FP64 Jacobi-PCG with the caller doing the communication each iteration:
+ * system and runs FP64 PCG (Jacobi unless tptfem_dist_set_precond, below) with the caller
+ * doing the communication each iteration:
  *   tptfem_dist_start                           -> local r.r, r.z        (sum over ranks)
  *   loop: tptfem_dist_pack; exchange (send_buf segment for rank q goes to q's ghost segment
  *         for this rank, counts from tptfem_dist_counts); tptfem_dist_spmv_dot -> local p.q
@@ -313,6 +314,31 @@ tptfem_status tptfem_dist_direction(tptfem_context* ctx, tptfem_dist* d, double 
 /* the owned part of the reduced solution (n_owned doubles, host) */
 tptfem_status tptfem_dist_solution(tptfem_context* ctx, const tptfem_dist* d, double* x_owned);
 void tptfem_dist_free(tptfem_dist* d);
+
+/* Two-level preconditioner in partitioned form, instead of Jacobi:
+ *   M^-1 = blockdiag_k(G_k^T G_k) + P A_c^-1 P^T
+ * G_k: the FSAI factor of rank k's owned diagonal block -- classic values
+ * (TPTFEM_DIST_PC_FSAI) or the network attached to the system
+ * (TPTFEM_DIST_PC_LEARNED, tptfem_system_attach_lfsai); it needs no exchange.
+ * With coarse_aggregates >= 0 (0: the one-GPU solver's default count) also the
+ * aggregation coarse space of the whole system (full node groups and the mesh
+ * geometry needed, row ranges node-aligned; *coarse_size 0 when it does not
+ * apply).  sys is the system the rank was created from and must outlive it.
+ * Set-up, per rank: tptfem_dist_set_precond leaves this rank's part of A_c
+ * (nc x nc doubles) in coarse_matrix (tptfem_dist_coarse_buffers); sum it over
+ * the ranks in place, then tptfem_dist_coarse_factor.
+ * Iterations: tptfem_dist_start and tptfem_dist_update then return the local
+ * r.r in out[0] and 0 in out[1] and leave this rank's part of P^T r (nc doubles)
+ * in coarse_vector: sum it over the ranks in place (when nc > 0), then
+ * tptfem_dist_precondition -> local r.z (sum); after the start,
+ * tptfem_dist_direction(0) sets p = z. */
+enum { TPTFEM_DIST_PC_FSAI = 1, TPTFEM_DIST_PC_LEARNED = 2 };
+tptfem_status tptfem_dist_set_precond(tptfem_context* ctx, tptfem_dist* d, tptfem_system* sys, int kind,
+                                      int coarse_aggregates, int64_t* coarse_size);
+/* device pointers (NULL without a coarse space) for the caller's in-place sums */
+tptfem_status tptfem_dist_coarse_buffers(const tptfem_dist* d, double** coarse_matrix, double** coarse_vector);
+tptfem_status tptfem_dist_coarse_factor(tptfem_context* ctx, tptfem_dist* d);
+tptfem_status tptfem_dist_precondition(tptfem_context* ctx, tptfem_dist* d, double* out_rz);
 /* nranks ranks on this context's GPU in lock step, the exchange done by device copies:
  * the same arithmetic as nranks GPUs; x (n_free doubles, host), *relres the recursive
  * residual at exit.  For testing the partitioned path on one device. */

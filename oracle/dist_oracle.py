@@ -1,8 +1,14 @@
 """Test-only numpy restatement of one rank of the library's row-partitioned
-Jacobi-PCG (tpt-fem_b200/csrc/dist.cu): the same row ranges, ghost ordering
-(sorted by global column), send lists (ascending owned rows each peer reads)
-and vector updates, on host arrays.  It lets the multi-process driver
-(tpt_fem.distributed.solve over torch.distributed) be tested with gloo on CPU."""
+PCG (tpt-fem_b200/csrc/dist.cu): the same row ranges, ghost ordering (sorted by
+global column), send lists (ascending owned rows each peer reads), vector
+updates and call sequence, on host arrays.  It lets the multi-process driver
+(tpt_fem.distributed.solve over torch.distributed) be tested with gloo on CPU.
+
+The block preconditioner is restated in kind, not in the library's numbers:
+classic FSAI of the owned diagonal block (pattern: the block's strictly lower
+entries of each row) and a coarse space of contiguous row aggregates with the
+constant mode, each rank forming its part P_k^T A_k P of A_c and P_k^T r_k of
+the restriction for the driver to sum."""
 import numpy as np
 
 
@@ -35,6 +41,63 @@ class NumpyRank:
         self.send_idx = np.concatenate(send) if send else np.zeros(0, np.int64)
         self.send_buf = np.zeros(len(self.send_idx))
         self.p = np.zeros(self.n_owned + self.n_ghost)
+        self._A = A
+
+    pc = False
+    coarse_size = 0
+    coarse_ready = False
+
+    def set_precond(self, kind="fsai", coarse_aggregates=0):
+        if kind != "fsai":
+            raise ValueError("the numpy rank has the classic block FSAI only")
+        r0, r1, n = self.r0, self.r1, self.n_owned
+        B = self._A[r0:r1, r0:r1].toarray()
+        self.sig2 = np.zeros(n)
+        L = np.zeros((n, n))
+        for i in range(n):  # A[P,P] y = e_last, P = lower pattern of row i, then i
+            P = np.append(np.nonzero(B[i, :i])[0], i)
+            y = np.linalg.solve(B[np.ix_(P, P)], np.eye(len(P))[-1])
+            self.sig2[i] = y[-1]
+            L[i, P[:-1]] = y[:-1] / y[-1]
+        self.L = L
+        self.pc, self.coarse_ready = True, False
+        self.coarse_size = 0
+        if coarse_aggregates is not None:
+            nt = self._A.shape[0]
+            na = coarse_aggregates if coarse_aggregates > 0 else max(2, nt // 16)
+            agg = np.arange(nt) * na // nt
+            P = np.zeros((nt, na))
+            P[np.arange(nt), agg] = 1.0 / np.sqrt(np.bincount(agg, minlength=na))[agg]
+            self.Pk = P[r0:r1]
+            self.ac = np.ascontiguousarray(self.Pk.T @ (self._A[r0:r1] @ P))
+            self.yc = np.zeros(na)
+            self.coarse_size = na
+        return self.coarse_size
+
+    def coarse_matrix(self):
+        import torch
+        return torch.from_numpy(self.ac.reshape(-1))
+
+    def coarse_vector(self):
+        import torch
+        return torch.from_numpy(self.yc)
+
+    def coarse_factor(self):
+        self.ainv = np.linalg.inv(self.ac)
+        self.coarse_ready = True
+
+    def precondition(self):
+        t = self.sig2 * (self.r + self.L @ self.r)
+        z = t + self.L.T @ t
+        if self.coarse_size:
+            z = z + self.Pk @ (self.ainv @ self.yc)
+        self.z = z
+        return np.array([self.r @ z])
+
+    def _after_update(self):
+        if self.coarse_size:
+            self.yc[:] = self.Pk.T @ self.r
+        return np.array([self.r @ self.r, 0.0])
 
     def _segments(self, buf, counts):
         import torch
@@ -54,6 +117,9 @@ class NumpyRank:
     def start(self):
         self.x = np.zeros(self.n_owned)
         self.r = self.b.copy()
+        if self.pc:
+            self.p[:] = 0.0
+            return self._after_update()
         self.z = self.dinv * self.r
         self.p[:self.n_owned] = self.z
         return np.array([self.r @ self.r, self.r @ self.z])
@@ -68,6 +134,8 @@ class NumpyRank:
     def update(self, alpha):
         self.x += alpha * self.p[:self.n_owned]
         self.r -= alpha * self.q
+        if self.pc:
+            return self._after_update()
         self.z = self.dinv * self.r
         return np.array([self.r @ self.r, self.r @ self.z])
 

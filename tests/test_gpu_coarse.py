@@ -148,3 +148,22 @@ def test_refresh_matches_a_freshly_reduced_system(ctx):
     K3 = F.assemble_elasticity(F.Mesh.from_arrays(F.CELL_TET4, *box([8, 2, 2]), ctx=ctx), "3d", 1.0, 0.3, 2)
     with pytest.raises(F.TptFemError):
         S.refresh(K3, np.zeros(K3.nrows))
+
+
+def test_overlapped_coarse_setup_repeats_bit_for_bit(ctx):
+    # Fresh set-ups after the first form the coarse matrix and its inverse on a
+    # second stream while the network computes the factor: every repeat must
+    # give the same iterations and the same solution bits as the first solve,
+    # whose set-up ran on one stream.
+    import os
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    model = LF.LearnedFsai.load(ctx, os.path.join(root, "tpt-fem_b200", "weights", "lfsai_elasticity.bin"))
+    S, _ = cantilever(ctx, [48, 12, 12], seed=11)
+    model.attach(S)
+    runs = []
+    for _ in range(3):
+        st = S.solve(solver=F.SOLVER_LEARNED_FSAI_PCG, tol=1e-10, fresh_setup=True, coarse=True)
+        assert st["coarse_size"] > 0 and st["rel_residual"] <= 1e-10 and not st["fell_back"]
+        runs.append((st["iterations"], S.solution()))
+    for it, u in runs[1:]:
+        assert it == runs[0][0] and np.array_equal(u, runs[0][1])

@@ -426,12 +426,38 @@ tptfem_status tptfem_dist_update(tptfem_context* ctx, tptfem_dist* d, double alp
 tptfem_status tptfem_dist_direction(tptfem_context* ctx, tptfem_dist* d, double beta) {
   TPT_DIST_CALL(dist_direction(*d->d, beta))
 }
+tptfem_status tptfem_dist_precondition(tptfem_context* ctx, tptfem_dist* d, double* out_rz) {
+  TPT_DIST_CALL({
+    TPT_REQUIRE(out_rz, TPTFEM_ERR_INVALID_ARG, "out_rz is NULL");
+    *out_rz = dist_precondition(*d->d);
+  })
+}
+tptfem_status tptfem_dist_coarse_factor(tptfem_context* ctx, tptfem_dist* d) {
+  TPT_DIST_CALL(dist_coarse_factor(*d->d))
+}
 tptfem_status tptfem_dist_solution(tptfem_context* ctx, const tptfem_dist* d, double* x_owned) {
   TPT_DIST_CALL({
     if (d->d->nloc) device_to_host(ctx, x_owned, d->d->x.p, d->d->nloc * sizeof(double));
   })
 }
 #undef TPT_DIST_CALL
+
+tptfem_status tptfem_dist_set_precond(tptfem_context* ctx, tptfem_dist* d, tptfem_system* sys, int kind,
+                                      int coarse_aggregates, int64_t* coarse_size) {
+  if (!ctx || !d || !d->d || !sys || !sys->d) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  const int nc = dist_set_precond(*d->d, *sys->d, kind, coarse_aggregates);
+  if (coarse_size) *coarse_size = nc;
+  API_CATCH(ctx)
+}
+
+tptfem_status tptfem_dist_coarse_buffers(const tptfem_dist* d, double** coarse_matrix, double** coarse_vector) {
+  if (!d || !d->d || !coarse_matrix || !coarse_vector) return TPTFEM_ERR_INVALID_ARG;
+  *coarse_matrix = d->d->nc ? d->d->ac.p : nullptr;
+  *coarse_vector = d->d->nc ? d->d->yc.p : nullptr;
+  return TPTFEM_OK;
+}
 
 void tptfem_dist_free(tptfem_dist* d) { delete d; }
 

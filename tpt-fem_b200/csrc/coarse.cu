@@ -67,7 +67,8 @@ __global__ void cs_fill_modes(int ngroups, const int* __restrict__ agg, const in
 
 // Raw moments of every column m of W (interleaved) over one segment:
 // smom[(seg nm + m) nm + k] = sum over its groups of (R_g^T W_g[:, m])_k;
-// groups without a neighbour of the colour are skipped.
+// groups without a neighbour of the colour are skipped.  W holds the groups
+// from g0 on (0: all of them).
 template <int DPN>
 __global__ void __launch_bounds__(CS_THREADS) cs_moments_modes(const int* __restrict__ sbeg,
                                                                const int* __restrict__ send,
@@ -75,7 +76,8 @@ __global__ void __launch_bounds__(CS_THREADS) cs_moments_modes(const int* __rest
                                                                const float* __restrict__ y,
                                                                const double* __restrict__ W,
                                                                double* __restrict__ smom,
-                                                               const unsigned* __restrict__ gmask, int colour) {
+                                                               const unsigned* __restrict__ gmask, int colour,
+                                                               int g0) {
   constexpr int NM = rigid_modes(DPN);
   __shared__ double sh[CS_THREADS / 32][NM * NM];
   const int seg = blockIdx.x;
@@ -87,7 +89,7 @@ __global__ void __launch_bounds__(CS_THREADS) cs_moments_modes(const int* __rest
     if (!((gmask[g] >> colour) & 1u)) continue;  // W_g is zero (and not written) for this colour
     double R[DPN][NM];
     mode_rows<DPN>(y + 3 * (int64_t)g, R);
-    const double* wg = W + (int64_t)g * DPN * NM;
+    const double* wg = W + (int64_t)(g - g0) * DPN * NM;
 #pragma unroll
     for (int a = 0; a < DPN; ++a)
 #pragma unroll
@@ -114,11 +116,12 @@ __global__ void __launch_bounds__(CS_THREADS) cs_moments_modes(const int* __rest
 
 // Raw mode moments of one segment of an aggregate's group list:
 // smom[seg][k] = sum over its groups of (R_g^T w_g)_k, block-reduced in a
-// fixed order.
+// fixed order (w holds the groups from g0 on).
 template <int DPN>
 __global__ void __launch_bounds__(CS_THREADS) cs_moments(const int* __restrict__ sbeg, const int* __restrict__ send,
                                                          const int* __restrict__ alist, const float* __restrict__ y,
-                                                         const double* __restrict__ w, double* __restrict__ smom) {
+                                                         const double* __restrict__ w, double* __restrict__ smom,
+                                                         int g0) {
   constexpr int NM = rigid_modes(DPN);
   __shared__ double sh[CS_THREADS / 32][NM];
   const int seg = blockIdx.x;
@@ -131,7 +134,7 @@ __global__ void __launch_bounds__(CS_THREADS) cs_moments(const int* __restrict__
     mode_rows<DPN>(y + 3 * (int64_t)g, R);
 #pragma unroll
     for (int a = 0; a < DPN; ++a) {
-      const double wa = w[(int64_t)g * DPN + a];
+      const double wa = w[(int64_t)(g - g0) * DPN + a];
 #pragma unroll
       for (int k = 0; k < NM; ++k) s[k] += R[a][k] * wa;
     }
@@ -464,6 +467,33 @@ void sym_eig3(double a[3][3], double w[3], double v[3][3]) {
   for (int i = 0; i < 3; ++i) w[i] = a[i][i];
 }
 
+// One rank's rows of W = A (P E_colour) for every mode at once (a partitioned
+// system: local CSR rows, gcol mapping local columns to global reduced
+// indices): W[i nm + m] = sum over row i of a_ij P[j, m], the columns j of
+// aggregates of the colour only.  One thread per row, entries in row order.
+template <int DPN>
+__global__ void cs_local_apply(int64_t nloc, const int* __restrict__ rp, const int* __restrict__ ci,
+                               const double* __restrict__ va, const int* __restrict__ gcol,
+                               const double* __restrict__ Pfull, const unsigned char* __restrict__ gcolour,
+                               int colour, double* __restrict__ W) {
+  constexpr int NM = rigid_modes(DPN);
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nloc) return;
+  double s[NM];
+#pragma unroll
+  for (int m = 0; m < NM; ++m) s[m] = 0.0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const int j = gcol[ci[k]];
+    if (gcolour[j / DPN] != colour) continue;
+    const double a = va[k];
+    const double* pj = Pfull + (int64_t)j * NM;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) s[m] += a * pj[m];
+  }
+#pragma unroll
+  for (int m = 0; m < NM; ++m) W[i * NM + m] = s[m];
+}
+
 int blocks_for(int64_t n) { return (int)((n + CS_THREADS - 1) / CS_THREADS); }
 
 }  // namespace
@@ -650,12 +680,25 @@ bool coarse_build(SystemData& S, int target) {
 }
 
 bool coarse_assemble(SystemData& S) {
+  if (!coarse_assemble_async(S, S.ctx->stream)) return false;
+  return coarse_finish(S, S.ctx->stream);
+}
+
+bool coarse_finish(SystemData& S, cudaStream_t s) {
+  CoarseSpace& C = S.coarse;
+  int hinfo = 0;
+  TPT_CUDA(cudaMemcpyAsync(&hinfo, C.info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TPT_CUDA(cudaStreamSynchronize(s));
+  C.ready = hinfo == 0;  // otherwise the coarse matrix was not positive definite in FP64
+  return C.ready;
+}
+
+bool coarse_assemble_async(SystemData& S, cudaStream_t s) {
   CoarseSpace& C = S.coarse;
   C.ready = false;
   if (C.state != 1) return false;
-  cudaStream_t s = S.ctx->stream;
   const int dpn = S.dpn, nc = C.nc;
-  C.Ac.zero();
+  TPT_CUDA(cudaMemsetAsync(C.Ac.p, 0, (size_t)nc * nc * sizeof(double), s));
   DevBuf<double> w, mom;
   w.alloc(S.n_free * C.nm, s);
   mom.alloc((size_t)C.nseg * C.nm * C.nm, s);
@@ -664,10 +707,10 @@ bool coarse_assemble(SystemData& S) {
     for (int cy = 0; cy < ncy; ++cy)
       for (int cx = 0; cx < ncx; ++cx) {
         const int colour = cx + 3 * cy + 9 * cz;
-        nb_operator_apply_modes(S, C.Pfull.p, w.p, C.gcolour.p, colour, C.cmask.p);
+        nb_operator_apply_modes(S, C.Pfull.p, w.p, C.gcolour.p, colour, C.cmask.p, s);
 #define TPT_CS_COL(D)                                                                                             \
   cs_moments_modes<D><<<C.nseg, CS_THREADS, 0, s>>>(C.sbeg.p, C.send.p, C.alist.p, C.y.p, w.p, mom.p, C.gmask.p,   \
-                                                    colour);                                                      \
+                                                    colour, 0);                                                   \
   TPT_CHECK_LAUNCH();
         if (dpn == 3) { TPT_CS_COL(3) }
         else if (dpn == 2) { TPT_CS_COL(2) }
@@ -678,28 +721,41 @@ bool coarse_assemble(SystemData& S) {
             C.Ac.p, nc);
         TPT_CHECK_LAUNCH();
       }
-  cs_fix_diag<<<blocks_for(nc), CS_THREADS, 0, s>>>(nc, C.Ac.p);
+  if (!C.info.p) C.info.alloc(1, s);
+  coarse_factor_async(S.ctx, s, nc, C.ld, C.Ac.p, C.Ainv.p, C.info.p);
+  return true;
+}
+
+bool coarse_factor(tptfem_context* ctx, int nc, int ld, double* Ac, float* Ainv) {
+  cudaStream_t s = ctx->stream;
+  DevBuf<int> info;
+  info.alloc(1, s);
+  coarse_factor_async(ctx, s, nc, ld, Ac, Ainv, info.p);
+  int hinfo = 0;
+  info.download(&hinfo, 1);
+  TPT_CUDA(cudaStreamSynchronize(s));
+  return hinfo == 0;  // otherwise not positive definite in FP64
+}
+
+void coarse_factor_async(tptfem_context* ctx, cudaStream_t s, int nc, int ld, double* Ac, float* Ainv, int* d_info) {
+  cs_fix_diag<<<blocks_for(nc), CS_THREADS, 0, s>>>(nc, Ac);
   TPT_CHECK_LAUNCH();
   // Cholesky and inverse (symmetric: row-major storage = column-major storage)
-  cusolverDnHandle_t h = (cusolverDnHandle_t)S.ctx->cusolver;
+  cusolverDnHandle_t h = (cusolverDnHandle_t)ctx->cusolver;
   if (!h) {
     TPT_REQUIRE(cusolverDnCreate(&h) == CUSOLVER_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "cusolverDnCreate failed");
-    S.ctx->cusolver = h;
+    ctx->cusolver = h;
   }
   TPT_REQUIRE(cusolverDnSetStream(h, s) == CUSOLVER_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "cusolverDnSetStream failed");
   int lw1 = 0;
-  TPT_REQUIRE(cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, nc, C.Ac.p, nc, &lw1) == CUSOLVER_STATUS_SUCCESS,
+  TPT_REQUIRE(cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, nc, Ac, nc, &lw1) == CUSOLVER_STATUS_SUCCESS,
               TPTFEM_ERR_DEVICE, "dpotrf_bufferSize failed");
   DevBuf<double> work;
   work.alloc(std::max(1, lw1), s);
-  DevBuf<int> info;
-  info.alloc(1, s);
-  int hinfo = 0;
-  TPT_REQUIRE(cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, nc, C.Ac.p, nc, work.p, lw1, info.p) ==
+  TPT_REQUIRE(cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, nc, Ac, nc, work.p, lw1, d_info) ==
                   CUSOLVER_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "dpotrf failed");
-  info.download(&hinfo, 1);
-  TPT_CUDA(cudaStreamSynchronize(s));
-  if (hinfo != 0) return false;  // coarse matrix not positive definite in FP64
+  // (a failed Cholesky, d_info != 0, is left for the caller to read: the steps
+  // below then produce values that are never used)
   // A_c^-1 = L^-T L^-1: L^-1 from one triangular solve with the identity
   // (lower triangular, zeros above), then one syrk into the lower triangle of
   // Ac -- large library calls instead of potri's many small ones
@@ -707,28 +763,26 @@ bool coarse_assemble(SystemData& S) {
   linv.alloc((size_t)nc * nc, s);
   cs_identity<<<blocks_for((int64_t)nc * nc), CS_THREADS, 0, s>>>(nc, linv.p);
   TPT_CHECK_LAUNCH();
-  cublasHandle_t hb = (cublasHandle_t)S.ctx->cublas;
+  cublasHandle_t hb = (cublasHandle_t)ctx->cublas;
   if (!hb) {
     TPT_REQUIRE(cublasCreate(&hb) == CUBLAS_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "cublasCreate failed");
-    S.ctx->cublas = hb;
+    ctx->cublas = hb;
   }
   TPT_REQUIRE(cublasSetStream(hb, s) == CUBLAS_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "cublasSetStream failed");
   const double one = 1.0, zero = 0.0;
   TPT_REQUIRE(cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nc, nc,
-                          &one, C.Ac.p, nc, linv.p, nc) == CUBLAS_STATUS_SUCCESS,
+                          &one, Ac, nc, linv.p, nc) == CUBLAS_STATUS_SUCCESS,
               TPTFEM_ERR_DEVICE, "dtrsm failed");
-  TPT_REQUIRE(cublasDsyrk(hb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, nc, nc, &one, linv.p, nc, &zero, C.Ac.p, nc) ==
+  TPT_REQUIRE(cublasDsyrk(hb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, nc, nc, &one, linv.p, nc, &zero, Ac, nc) ==
                   CUBLAS_STATUS_SUCCESS, TPTFEM_ERR_DEVICE, "dsyrk failed");
-  cs_symmetrize<<<blocks_for((int64_t)nc * C.ld), CS_THREADS, 0, s>>>(nc, C.ld, C.Ac.p, C.Ainv.p);
+  cs_symmetrize<<<blocks_for((int64_t)nc * ld), CS_THREADS, 0, s>>>(nc, ld, Ac, Ainv);
   TPT_CHECK_LAUNCH();
-  C.ready = true;
-  return true;
 }
 
 void coarse_restrict_solve(const SystemData& S, const double* r, cudaStream_t s) {
   const CoarseSpace& C = S.coarse;
 #define TPT_CS_R(D)                                                                                     \
-  cs_moments<D><<<C.nseg, CS_THREADS, 0, s>>>(C.sbeg.p, C.send.p, C.alist.p, C.y.p, r, C.smom.p); \
+  cs_moments<D><<<C.nseg, CS_THREADS, 0, s>>>(C.sbeg.p, C.send.p, C.alist.p, C.y.p, r, C.smom.p, 0); \
   TPT_CHECK_LAUNCH();
   if (S.dpn == 3) { TPT_CS_R(3) }
   else if (S.dpn == 2) { TPT_CS_R(2) }
@@ -754,6 +808,116 @@ void coarse_download(const SystemData& S, int* na, int* nm, double* Ainv_out) {
     for (int i = 0; i < C.nc; ++i)
       for (int j = 0; j < C.nc; ++j) Ainv_out[(size_t)i * C.nc + j] = f[(size_t)i * C.ld + j];
   }
+}
+
+int coarse_default_aggregates(const SystemData& S) {
+  // about one aggregate per 2000 node groups for vector problems (6 or 3
+  // rigid modes each) and per 700 for scalar ones (one constant mode each),
+  // between 8 and 3000
+  const int per = S.dpn == 1 ? 700 : 2000;
+  return std::max(8, std::min(3000, S.nb.ngroups / per));
+}
+
+// ---- the coarse space of a row-partitioned system (dist.cu) -----------------------
+// Every rank holds the whole system's aggregates and P (coarse_build); these
+// work on its own groups only, so that the ranks' partial A_c and P^T r add
+// up, over the ranks, to the whole system's.
+
+void coarse_local_build(const SystemData& S, int64_t g0, int64_t g1, CoarseLocal& L) {
+  const CoarseSpace& C = S.coarse;
+  cudaStream_t s = S.ctx->stream;
+  L.g0 = g0;
+  L.g1 = g1;
+  const int64_t ngl = g1 - g0;
+  std::vector<int> agg(std::max<int64_t>(ngl, 1));
+  if (ngl) {
+    TPT_CUDA(cudaMemcpyAsync(agg.data(), C.agg.p + g0, ngl * sizeof(int), cudaMemcpyDeviceToHost, s));
+    TPT_CUDA(cudaStreamSynchronize(s));
+  }
+  // the local groups of each aggregate, ascending (counting sort by aggregate)
+  std::vector<int> cnt(C.na + 1, 0), list(std::max<int64_t>(ngl, 1));
+  for (int64_t g = 0; g < ngl; ++g) cnt[agg[g] + 1]++;
+  for (int i = 0; i < C.na; ++i) cnt[i + 1] += cnt[i];
+  std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+  for (int64_t g = 0; g < ngl; ++g) list[pos[agg[g]]++] = (int)(g0 + g);
+  constexpr int CS_SEG = 1024;
+  std::vector<int> sb, se, aseg(C.na + 1, 0);
+  for (int i = 0; i < C.na; ++i) {
+    for (int t = cnt[i]; t < cnt[i + 1]; t += CS_SEG) {
+      sb.push_back(t);
+      se.push_back(std::min(cnt[i + 1], t + CS_SEG));
+    }
+    aseg[i + 1] = (int)sb.size();
+  }
+  L.nseg = (int)sb.size();
+  L.alist.alloc(list.size(), s);
+  L.alist.upload(list.data(), list.size());
+  L.sbeg.alloc(std::max(L.nseg, 1), s);
+  L.sbeg.upload(sb.data(), L.nseg);
+  L.send.alloc(std::max(L.nseg, 1), s);
+  L.send.upload(se.data(), L.nseg);
+  L.aseg.alloc(C.na + 1, s);
+  L.aseg.upload(aseg.data(), C.na + 1);
+  L.smom.alloc((size_t)std::max(L.nseg, 1) * C.nm, s);
+  TPT_CUDA(cudaStreamSynchronize(s));  // the host vectors are released on return
+}
+
+void coarse_local_matrix(const SystemData& S, const CoarseLocal& L, int64_t nloc, const int* rp, const int* ci,
+                         const double* va, const int* gcol, double* Acp) {
+  const CoarseSpace& C = S.coarse;
+  cudaStream_t s = S.ctx->stream;
+  const int dpn = S.dpn, nc = C.nc;
+  TPT_CUDA(cudaMemsetAsync(Acp, 0, (size_t)nc * nc * sizeof(double), s));
+  if (!nloc || !L.nseg) return;
+  DevBuf<double> w, mom;
+  w.alloc(nloc * C.nm, s);
+  mom.alloc((size_t)L.nseg * C.nm * C.nm, s);
+  const int ncx = std::min(3, C.bins[0]), ncy = std::min(3, C.bins[1]), ncz = std::min(3, C.bins[2]);
+  for (int cz = 0; cz < ncz; ++cz)
+    for (int cy = 0; cy < ncy; ++cy)
+      for (int cx = 0; cx < ncx; ++cx) {
+        const int colour = cx + 3 * cy + 9 * cz;
+#define TPT_CS_LOC(D)                                                                                            \
+  cs_local_apply<D><<<blocks_for(nloc), CS_THREADS, 0, s>>>(nloc, rp, ci, va, gcol, C.Pfull.p, C.gcolour.p, colour, \
+                                                            w.p);                                                  \
+  TPT_CHECK_LAUNCH();                                                                                              \
+  cs_moments_modes<D><<<L.nseg, CS_THREADS, 0, s>>>(L.sbeg.p, L.send.p, L.alist.p, C.y.p, w.p, mom.p, C.gmask.p,   \
+                                                    colour, (int)L.g0);                                            \
+  TPT_CHECK_LAUNCH();
+        if (dpn == 3) { TPT_CS_LOC(3) }
+        else if (dpn == 2) { TPT_CS_LOC(2) }
+        else { TPT_CS_LOC(1) }
+#undef TPT_CS_LOC
+        cs_columns_par<<<blocks_for((int64_t)C.na * C.nm * C.nm), CS_THREADS, 0, s>>>(
+            C.na, C.nm, C.abin.p, C.bin2agg.p, C.bins[0], C.bins[1], C.bins[2], L.aseg.p, mom.p, C.T.p, colour, Acp,
+            nc);
+        TPT_CHECK_LAUNCH();
+      }
+}
+
+void coarse_local_restrict(const SystemData& S, CoarseLocal& L, const double* r_loc, double* yc, cudaStream_t s) {
+  const CoarseSpace& C = S.coarse;
+  if (L.nseg) {
+#define TPT_CS_LR(D)                                                                                              \
+  cs_moments<D><<<L.nseg, CS_THREADS, 0, s>>>(L.sbeg.p, L.send.p, L.alist.p, C.y.p, r_loc, L.smom.p, (int)L.g0); \
+  TPT_CHECK_LAUNCH();
+    if (S.dpn == 3) { TPT_CS_LR(3) }
+    else if (S.dpn == 2) { TPT_CS_LR(2) }
+    else { TPT_CS_LR(1) }
+#undef TPT_CS_LR
+  }
+  cs_yc<<<blocks_for(C.nc), CS_THREADS, 0, s>>>(C.na, C.nm, L.aseg.p, L.smom.p, C.T.p, yc);
+  TPT_CHECK_LAUNCH();
+}
+
+void coarse_local_solve(const SystemData& S, int ld, const float* Ainv, const double* yc, double* uc, double* cm,
+                        cudaStream_t s) {
+  const CoarseSpace& C = S.coarse;
+  cs_gemv<<<(C.nc + CS_THREADS / 32 - 1) / (CS_THREADS / 32), CS_THREADS, (size_t)ld * sizeof(double), s>>>(
+      C.nc, ld, yc, Ainv, uc);
+  TPT_CHECK_LAUNCH();
+  cs_raw<<<blocks_for(C.nc), CS_THREADS, 0, s>>>(C.na, C.nm, C.T.p, uc, cm);
+  TPT_CHECK_LAUNCH();
 }
 
 }  // namespace tptfem

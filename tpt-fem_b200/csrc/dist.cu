@@ -1,4 +1,4 @@
-// dist.cu -- row-partitioned FP64 Jacobi-PCG over several ranks (one per GPU).
+// dist.cu -- row-partitioned FP64 PCG over several ranks (one per GPU).
 //
 // The reduced system is split into contiguous, node-aligned row ranges (the
 // x-slabs of a box mesh, whose nodes are numbered x-major).  Rank k keeps its
@@ -12,12 +12,26 @@
 // different GPUs), or to tptfem_dist_solve_local, which runs several ranks on
 // one device in lock step with device copies as the exchange.  Partial sums
 // are per-block values added in a fixed order, so results are reproducible.
-// The plain method only: Jacobi preconditioning, FP64 throughout.
+//
+// Preconditioners: Jacobi (the plain method), or, after dist_set_precond, the
+// two-level method of the one-GPU solver in partitioned form:
+//   M^-1 = blockdiag_k(G_k^T G_k) + P A_c^-1 P^T
+// G_k is the FSAI factor (classic, or the attached network's values) of rank
+// k's owned diagonal block, so applying it needs no exchange.  P is the
+// aggregation coarse space of the whole system (every rank builds the same
+// aggregates from the mesh geometry); rank k forms P_k^T A_k P from its own
+// rows, the caller sums these partial coarse matrices over the ranks once
+// (an all-reduce of nc x nc values) and every rank factors the sum.  Each
+// iteration then adds one all-reduce of the nc restriction values P_k^T r_k:
+//   ... | x, r update, r.r, P_k^T r_k | sum r.r; sum P^T r | z = M r, r.z | sum | p = z + beta p
 #include <algorithm>
 #include <cmath>
 #include <memory>
 #include <vector>
 
+#include <cuda_fp16.h>
+
+#include "modes.cuh"
 #include "objects.hpp"
 
 namespace tptfem {
@@ -55,13 +69,14 @@ __global__ void __launch_bounds__(DT_THREADS) dist_spmv_dot(int64_t nloc, const 
   }
 }
 
-// x += a p, r -= a q, z = dinv r; per-block partials of r.r and r.z.
+// x += a p, r -= a q, with Jacobi z = dinv r; per-block partials of r.r and r.z
+// (r.z 0 without Jacobi: the block preconditioner forms z afterwards).
 __global__ void __launch_bounds__(DT_THREADS) dist_update(int64_t nloc, double a, double* __restrict__ x,
                                                           double* __restrict__ r, double* __restrict__ z,
                                                           const double* __restrict__ p,
                                                           const double* __restrict__ q,
                                                           const double* __restrict__ dinv,
-                                                          double* __restrict__ part) {
+                                                          double* __restrict__ part, bool jacobi) {
   __shared__ double s1[DT_THREADS], s2[DT_THREADS];
   const int64_t i = (int64_t)blockIdx.x * DT_THREADS + threadIdx.x;
   double rr = 0.0, rz = 0.0;
@@ -69,10 +84,12 @@ __global__ void __launch_bounds__(DT_THREADS) dist_update(int64_t nloc, double a
     x[i] += a * p[i];
     const double ri = r[i] - a * q[i];
     r[i] = ri;
-    const double zi = dinv[i] * ri;
-    z[i] = zi;
     rr = ri * ri;
-    rz = ri * zi;
+    if (jacobi) {
+      const double zi = dinv[i] * ri;
+      z[i] = zi;
+      rz = ri * zi;
+    }
   }
   s1[threadIdx.x] = rr;
   s2[threadIdx.x] = rz;
@@ -88,6 +105,104 @@ __global__ void __launch_bounds__(DT_THREADS) dist_update(int64_t nloc, double a
     part[2 * blockIdx.x] = s1[0];
     part[2 * blockIdx.x + 1] = s2[0];
   }
+}
+
+// Block FSAI, first half: t = sigma^2 (r + L r) (DT_LPR lanes per row).
+__global__ void __launch_bounds__(DT_THREADS) dist_fsai_lower(int64_t n, const int* __restrict__ rp,
+                                                              const int* __restrict__ ci,
+                                                              const __half* __restrict__ va,
+                                                              const float* __restrict__ sig2,
+                                                              const double* __restrict__ r, double* __restrict__ t) {
+  const int64_t tid = (int64_t)blockIdx.x * DT_THREADS + threadIdx.x;
+  const int64_t i = tid / DT_LPR;
+  const int l = (int)(tid % DT_LPR);
+  double s = 0.0;
+  if (i < n)
+    for (int k = rp[i] + l; k < rp[i + 1]; k += DT_LPR) s += (double)__half2float(va[k]) * r[ci[k]];
+  for (int o = DT_LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, DT_LPR);
+  if (i < n && l == 0) t[i] = (double)sig2[i] * (r[i] + s);
+}
+
+// Second half: z = t + L^T t, plus the coarse correction P (A_c^-1 P^T r) on
+// the owned groups when cm is given (raw-mode coefficients per aggregate);
+// per-block partials of r.z.
+template <int DPN>
+__global__ void __launch_bounds__(DT_THREADS) dist_fsai_upper(int64_t n, const int* __restrict__ trp,
+                                                              const int* __restrict__ tci,
+                                                              const __half* __restrict__ tva,
+                                                              const double* __restrict__ t,
+                                                              const double* __restrict__ r, double* __restrict__ z,
+                                                              int64_t r0, const int* __restrict__ agg,
+                                                              const float* __restrict__ y,
+                                                              const double* __restrict__ cm,
+                                                              double* __restrict__ part) {
+  constexpr int NM = rigid_modes(DPN);
+  __shared__ double sh[DT_THREADS / DT_LPR];
+  const int64_t tid = (int64_t)blockIdx.x * DT_THREADS + threadIdx.x;
+  const int64_t i = tid / DT_LPR;
+  const int l = (int)(tid % DT_LPR);
+  double s = 0.0;
+  if (i < n)
+    for (int k = trp[i] + l; k < trp[i + 1]; k += DT_LPR) s += (double)__half2float(tva[k]) * t[tci[k]];
+  for (int o = DT_LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, DT_LPR);
+  double d = 0.0;
+  if (i < n && l == 0) {
+    double zi = t[i] + s;
+    if (cm) {
+      const int64_t gi = r0 + i, g = gi / DPN;
+      const int a = (int)(gi - g * DPN);
+      double R[DPN][NM];
+      mode_rows<DPN>(y + 3 * g, R);
+      const double* c = cm + (int64_t)agg[g] * NM;
+      double pc = 0.0;
+#pragma unroll
+      for (int k = 0; k < NM; ++k) pc += R[a][k] * c[k];
+      zi += pc;
+    }
+    z[i] = zi;
+    d = r[i] * zi;
+  }
+  if (l == 0) sh[threadIdx.x / DT_LPR] = d;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double acc = 0.0;
+    for (int w = 0; w < DT_THREADS / DT_LPR; ++w) acc += sh[w];
+    part[blockIdx.x] = acc;
+  }
+}
+
+// The owned diagonal block of the local rows: per row the count of owned
+// columns (< nloc), then those entries in row order.
+__global__ void dist_block_count(int64_t nloc, const int* __restrict__ rp, const int* __restrict__ ci,
+                                 int* __restrict__ cnt) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nloc) return;
+  int c = 0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) c += ci[k] < nloc;
+  cnt[i] = c;
+}
+
+__global__ void dist_block_fill(int64_t nloc, const int* __restrict__ rp, const int* __restrict__ ci,
+                                const double* __restrict__ va, const int* __restrict__ brp, int* __restrict__ bci,
+                                double* __restrict__ bva) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nloc) return;
+  int o = brp[i];
+  for (int k = rp[i]; k < rp[i + 1]; ++k)
+    if (ci[k] < nloc) {
+      bci[o] = ci[k];
+      bva[o] = va[k];
+      ++o;
+    }
+}
+
+// full dof -> block row (-1 outside the owned range [r0, r1) of reduced rows)
+__global__ void dist_block_red_map(int64_t n, const int* __restrict__ red, int64_t r0, int64_t r1,
+                                   int* __restrict__ out) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int v = red[j];
+  out[j] = (v >= r0 && v < r1) ? (int)(v - r0) : -1;
 }
 
 __global__ void dist_direction(int64_t nloc, double beta, const double* __restrict__ z, double* __restrict__ p) {
@@ -156,6 +271,7 @@ std::unique_ptr<DistData> dist_create(tptfem_context* ctx, SystemData& S, int ra
   std::sort(ghosts.begin(), ghosts.end());
   ghosts.erase(std::unique(ghosts.begin(), ghosts.end()), ghosts.end());
   D->nghost = (int64_t)ghosts.size();
+  D->sys = &S;
   D->recv_off.assign(size + 1, 0);
   for (int g : ghosts) D->recv_off[owner(g) + 1]++;
   for (int k = 0; k < size; ++k) D->recv_off[k + 1] += D->recv_off[k];
@@ -183,6 +299,7 @@ std::unique_ptr<DistData> dist_create(tptfem_context* ctx, SystemData& S, int ra
     for (int c : need) sidx.push_back((int)(c - D->r0));
     D->send_off[qr + 1] = D->send_off[qr] + (int64_t)need.size();
   }
+  D->ghost_cols = std::move(ghosts);
   D->rp.alloc(D->nloc + 1, s);
   D->rp.upload(lrp.data(), lrp.size());
   D->ci.alloc(std::max<int64_t>(nnzl, 1), s);
@@ -218,7 +335,9 @@ std::unique_ptr<DistData> dist_create(tptfem_context* ctx, SystemData& S, int ra
   return D;
 }
 
-// x = 0, r = b, z = dinv r, p = z; partial r.r and r.z into out[0..1].
+// x = 0, r = b; Jacobi: z = dinv r, p = z; partial r.r and r.z into out[0..1].
+// With a block preconditioner: partial r.r and 0, the coarse restriction's
+// partial in yc, p = 0 (the caller sets p = z after tptfem_dist_precondition).
 void dist_start(DistData& D, double* out) {
   cudaStream_t s = D.ctx->stream;
   if (D.nloc) {
@@ -227,12 +346,11 @@ void dist_start(DistData& D, double* out) {
     TPT_CUDA(cudaMemsetAsync(D.q.p, 0, D.nloc * sizeof(double), s));
     TPT_CUDA(cudaMemsetAsync(D.p.p, 0, D.nloc * sizeof(double), s));
   }
-  dist_update<<<D.blocks_vec, DT_THREADS, 0, s>>>(D.nloc, 0.0, D.x.p, D.r.p, D.z.p, D.p.p, D.q.p, D.dinv.p, D.part.p);
-  TPT_CHECK_LAUNCH();
-  out[0] = D.sum_parts(D.blocks_vec, 2, 0);
-  out[1] = D.sum_parts(D.blocks_vec, 2, 1);
-  dist_direction<<<D.blocks_vec, DT_THREADS, 0, s>>>(D.nloc, 0.0, D.z.p, D.p.p);
-  TPT_CHECK_LAUNCH();
+  dist_update(D, 0.0, out);
+  if (!D.pc) {
+    dist_direction<<<D.blocks_vec, DT_THREADS, 0, s>>>(D.nloc, 0.0, D.z.p, D.p.p);
+    TPT_CHECK_LAUNCH();
+  }
 }
 
 void dist_pack(DistData& D) {
@@ -252,11 +370,121 @@ double dist_spmv_dot(DistData& D) {
 }
 
 void dist_update(DistData& D, double alpha, double* out) {
-  dist_update<<<D.blocks_vec, DT_THREADS, 0, D.ctx->stream>>>(D.nloc, alpha, D.x.p, D.r.p, D.z.p, D.p.p, D.q.p,
-                                                              D.dinv.p, D.part.p);
+  cudaStream_t s = D.ctx->stream;
+  dist_update<<<D.blocks_vec, DT_THREADS, 0, s>>>(D.nloc, alpha, D.x.p, D.r.p, D.z.p, D.p.p, D.q.p, D.dinv.p,
+                                                  D.part.p, D.pc == 0);
   TPT_CHECK_LAUNCH();
-  out[0] = D.sum_parts(D.blocks_vec, 2, 0);
+  if (D.nc) coarse_local_restrict(*D.sys, D.cl, D.r.p, D.yc.p, s);  // this rank's part of P^T r
+  out[0] = D.sum_parts(D.blocks_vec, 2, 0);  // (synchronises: yc is ready for the caller's sum)
   out[1] = D.sum_parts(D.blocks_vec, 2, 1);
+}
+
+int dist_set_precond(DistData& D, SystemData& S, int kind, int aggregates) {
+  TPT_REQUIRE(kind == 1 || kind == 2, TPTFEM_ERR_INVALID_ARG, "kind must be TPTFEM_DIST_PC_FSAI or _LEARNED");
+  TPT_REQUIRE(D.sys == &S, TPTFEM_ERR_INVALID_ARG, "not the system this rank was created from");
+  TPT_REQUIRE(D.pc == 0, TPTFEM_ERR_INVALID_ARG, "the rank's preconditioner is already set");
+  cudaStream_t s = D.ctx->stream;
+  const int64_t nl = std::max<int64_t>(D.nloc, 1);
+  // the owned diagonal block as a system of its own: the local rows' entries
+  // in owned columns (ascending in every row, as the global columns are)
+  auto B = std::make_unique<SystemData>();
+  B->ctx = D.ctx;
+  B->mesh = S.mesh;
+  B->lmodel = S.lmodel;
+  B->n = S.n;
+  B->n_free = D.nloc;
+  B->dpn = S.dpn;
+  B->free_map.alloc(nl, s);
+  if (D.nloc)
+    TPT_CUDA(cudaMemcpyAsync(B->free_map.p, S.free_map.p + D.r0, D.nloc * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  B->red_map.alloc(std::max<int64_t>(S.n, 1), s);
+  dist_block_red_map<<<ceil_div(std::max<int64_t>(S.n, 1), 256), 256, 0, s>>>(S.n, S.red_map.p, D.r0, D.r1,
+                                                                              B->red_map.p);
+  TPT_CHECK_LAUNCH();
+  DevBuf<int> cnt;
+  cnt.alloc(nl + 1, s);
+  B->row_ptr.alloc(D.nloc + 1, s);
+  if (D.nloc) {
+    dist_block_count<<<ceil_div(D.nloc, 256), 256, 0, s>>>(D.nloc, D.rp.p, D.ci.p, cnt.p);
+    TPT_CHECK_LAUNCH();
+  }
+  B->nnz = exclusive_scan_i32(cnt.p, B->row_ptr.p, D.nloc, s);
+  B->col.alloc(std::max<int64_t>(B->nnz, 1), s);
+  B->val.alloc(std::max<int64_t>(B->nnz, 1), s);
+  if (D.nloc) {
+    dist_block_fill<<<ceil_div(D.nloc, 256), 256, 0, s>>>(D.nloc, D.rp.p, D.ci.p, D.va.p, B->row_ptr.p, B->col.p,
+                                                           B->val.p);
+    TPT_CHECK_LAUNCH();
+  }
+  if (D.nloc) {
+    D.fac = system_block_factor(*B, kind == 2);
+    TPT_REQUIRE(D.fac, TPTFEM_ERR_NUMERIC,
+                "the block's FSAI factor could not be built (a pattern row too long or a non-positive pivot)");
+  }
+  D.blk = std::move(B);
+  D.t.alloc(nl, s);
+  D.pc = kind;
+  D.nc = 0;
+  D.coarse_ready = false;
+  // the coarse space of the whole system (geometry on every rank), this rank's part of A_c
+  if (aggregates >= 0 && nb_build_operator(S) &&
+      coarse_build(S, aggregates > 0 ? aggregates : coarse_default_aggregates(S))) {
+    const int dpn = S.dpn;
+    TPT_REQUIRE(D.r0 % dpn == 0 && D.r1 % dpn == 0, TPTFEM_ERR_INVALID_ARG,
+                "row ranges must hold whole node groups for the coarse space");
+    coarse_local_build(S, D.r0 / dpn, D.r1 / dpn, D.cl);
+    std::vector<int> gc(D.nloc + D.nghost);
+    for (int64_t i = 0; i < D.nloc; ++i) gc[i] = (int)(D.r0 + i);
+    for (int64_t k = 0; k < D.nghost; ++k) gc[D.nloc + k] = D.ghost_cols[k];
+    D.gcol.alloc(std::max<size_t>(gc.size(), 1), s);
+    D.gcol.upload(gc.data(), gc.size());
+    const int nc = S.coarse.nc;
+    D.ld = (nc + 3) & ~3;
+    D.ac.alloc((size_t)nc * nc, s);
+    D.yc.alloc(nc, s);
+    D.uc.alloc(nc, s);
+    D.cm.alloc(nc, s);
+    D.ainv.alloc((size_t)nc * D.ld, s);
+    coarse_local_matrix(S, D.cl, D.nloc, D.rp.p, D.ci.p, D.va.p, D.gcol.p, D.ac.p);
+    D.nc = nc;
+  }
+  TPT_CUDA(cudaStreamSynchronize(s));  // ac is ready for the caller's sum; host vectors are released
+  return D.nc;
+}
+
+void dist_coarse_factor(DistData& D) {
+  TPT_REQUIRE(D.nc > 0, TPTFEM_ERR_INVALID_ARG, "the rank has no coarse space");
+  TPT_REQUIRE(!D.coarse_ready, TPTFEM_ERR_INVALID_ARG, "the coarse matrix is already factored");
+  const bool ok = coarse_factor(D.ctx, D.nc, D.ld, D.ac.p, D.ainv.p);
+  TPT_REQUIRE(ok, TPTFEM_ERR_NUMERIC, "the summed coarse matrix is not positive definite");
+  TPT_CUDA(cudaStreamSynchronize(D.ctx->stream));
+  D.coarse_ready = true;
+}
+
+double dist_precondition(DistData& D) {
+  TPT_REQUIRE(D.pc != 0, TPTFEM_ERR_INVALID_ARG, "no block preconditioner set (Jacobi forms z in the update)");
+  TPT_REQUIRE(!D.nc || D.coarse_ready, TPTFEM_ERR_INVALID_ARG,
+              "the coarse matrix is not factored: sum it over the ranks, then call tptfem_dist_coarse_factor");
+  cudaStream_t s = D.ctx->stream;
+  const SystemData& S = *D.sys;
+  if (D.nc) coarse_local_solve(S, D.ld, D.ainv.p, D.yc.p, D.uc.p, D.cm.p, s);
+  const int64_t n = D.nloc;
+  const bool coarse = D.nc > 0;
+  if (n) {
+    const FsaiFactor& F = *D.fac;
+    dist_fsai_lower<<<D.blocks_spmv, DT_THREADS, 0, s>>>(n, F.rp.p, F.ci.p, F.va.p, F.sigma2.p, D.r.p, D.t.p);
+    TPT_CHECK_LAUNCH();
+  }
+#define TPT_DIST_UP(DP)                                                                                             \
+  dist_fsai_upper<DP><<<D.blocks_spmv, DT_THREADS, 0, s>>>(                                                        \
+      n, n ? D.fac->trp.p : nullptr, n ? D.fac->tci.p : nullptr, n ? D.fac->tva.p : nullptr, D.t.p, D.r.p, D.z.p, \
+      D.r0, coarse ? S.coarse.agg.p : nullptr, coarse ? S.coarse.y.p : nullptr, coarse ? D.cm.p : nullptr, D.part.p);
+  if (coarse && S.dpn == 3) { TPT_DIST_UP(3) }
+  else if (coarse && S.dpn == 2) { TPT_DIST_UP(2) }
+  else { TPT_DIST_UP(1) }
+#undef TPT_DIST_UP
+  TPT_CHECK_LAUNCH();
+  return D.sum_parts(D.blocks_spmv, 1, 0);
 }
 
 void dist_direction(DistData& D, double beta) {

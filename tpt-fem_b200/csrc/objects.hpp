@@ -180,6 +180,7 @@ struct CoarseSpace {
   DevBuf<float> y;              // per group: node position minus the aggregate centroid
   DevBuf<double> T;             // per aggregate: nm x nm mode transform (columns orthonormal modes)
   DevBuf<double> Ac;            // nc x nc, then its Cholesky factor / inverse (FP64)
+  DevBuf<int> info;             // status of the last Cholesky (0: positive definite)
   DevBuf<float> Ainv;           // nc x nc inverse (FP32, symmetric, row-major, stride ld)
   DevBuf<double> yc, uc;        // coarse vectors
   DevBuf<double> cm;            // per aggregate: raw-mode coefficients of the prolongation, T uc
@@ -272,7 +273,15 @@ void host_to_device(tptfem_context* ctx, void* dst, const void* src, size_t byte
 void device_to_host(tptfem_context* ctx, void* dst, const void* src, size_t bytes);
 bool host_to_device_ids(tptfem_context* ctx, int* dst, const int64_t* src, size_t count, int64_t limit);
 bool host_to_device_finite(tptfem_context* ctx, double* dst, const double* src, size_t count);
-// dist.cu: one rank of the row-partitioned FP64 Jacobi-PCG (see the file's header)
+// The groups [g0, g1) of a row-partitioned system (one rank's rows): their
+// part of every aggregate's group list, in segments like the whole system's.
+struct CoarseLocal {
+  int64_t g0 = 0, g1 = 0;
+  int nseg = 0;
+  DevBuf<int> sbeg, send, alist, aseg;  // aseg: na + 1 entries, empty for aggregates without local groups
+  DevBuf<double> smom;                  // restriction moments (nseg x nm)
+};
+// dist.cu: one rank of the row-partitioned FP64 PCG (see the file's header)
 struct DistData {
   tptfem_context* ctx = nullptr;
   int rank = 0, size = 1;
@@ -280,8 +289,20 @@ struct DistData {
   DevBuf<int> rp, ci, send_idx;
   DevBuf<double> va, dinv, b, x, r, z, p, q, send_buf, part;
   std::vector<int64_t> send_off, recv_off;  // per peer rank: ranges in send_buf / in the ghost part of p
+  std::vector<int> ghost_cols;              // global reduced index of every ghost column, ascending
   std::vector<double> hpart;
   int blocks_spmv = 1, blocks_vec = 1;
+  // block preconditioner (dist_set_precond); pc 0: Jacobi
+  int pc = 0;
+  SystemData* sys = nullptr;             // the whole reduced system (coarse geometry); the caller keeps it
+  std::unique_ptr<SystemData> blk;       // the owned diagonal block as a system of its own
+  const FsaiFactor* fac = nullptr;       // its factor (owned by blk)
+  int nc = 0, ld = 0;                    // coarse size (0: none) and row stride of ainv
+  bool coarse_ready = false;
+  CoarseLocal cl;
+  DevBuf<int> gcol;                      // local column -> global reduced index
+  DevBuf<double> t, ac, yc, uc, cm;      // FSAI intermediate; partial / summed A_c; coarse vectors
+  DevBuf<float> ainv;
   double sum_parts(int nb, int stride, int which);
 };
 std::unique_ptr<DistData> dist_create(tptfem_context* ctx, SystemData& S, int rank, int size,
@@ -291,6 +312,11 @@ void dist_pack(DistData& D);
 double dist_spmv_dot(DistData& D);
 void dist_update(DistData& D, double alpha, double* out);
 void dist_direction(DistData& D, double beta);
+// block FSAI (kind 1 classic, 2 learned) of the owned rows, and with aggregates >= 0
+// the rank's partial coarse matrix; returns the coarse size (0: none)
+int dist_set_precond(DistData& D, SystemData& S, int kind, int aggregates);
+void dist_coarse_factor(DistData& D);  // after the caller summed the partial A_c over ranks
+double dist_precondition(DistData& D);  // z = M r once the restriction is summed; local r.z
 int64_t dist_solve_local(tptfem_context* ctx, SystemData& S, int nranks, double tol, int64_t max_iter,
                          double* u_red, double* relres);
 // io_exodus.cu: write_exodus's NetCDF-3 classic bytes for a device-resident mesh
@@ -302,17 +328,40 @@ void nb_refresh_values(SystemData& S);  // refill the node-block values from S.v
 // coarse.cu
 bool coarse_build(SystemData& S, int target_aggregates);  // geometry (once); false: not applicable
 bool coarse_assemble(SystemData& S);                      // A_c and its inverse for the current values
+// the same enqueued on stream s with no host wait (false: no coarse geometry),
+// then, once s's work is complete or ordered before stream s2, its status
+bool coarse_assemble_async(SystemData& S, cudaStream_t s);
+bool coarse_finish(SystemData& S, cudaStream_t s2);
 void coarse_restrict_solve(const SystemData& S, const double* r, cudaStream_t s);  // uc = A_c^-1 P^T r
 void coarse_download(const SystemData& S, int* na, int* nm, double* Ainv_or_null);  // FP32 inverse, widened
+int coarse_default_aggregates(const SystemData& S);  // about one aggregate per 2000 (vector) / 700 (scalar) groups
+// Cholesky and FP32 explicit inverse of an SPD nc x nc matrix (Ac is overwritten;
+// zero rows / columns of dropped modes get a unit diagonal); false if not SPD.
+bool coarse_factor(tptfem_context* ctx, int nc, int ld, double* Ac, float* Ainv);
+// the same enqueued on stream s; the Cholesky's status (0: SPD) goes to d_info
+void coarse_factor_async(tptfem_context* ctx, cudaStream_t s, int nc, int ld, double* Ac, float* Ainv, int* d_info);
+// partitioned coarse space, the rows of the groups [g0, g1) only (dist.cu)
+void coarse_local_build(const SystemData& S, int64_t g0, int64_t g1, CoarseLocal& L);
+// this rank's part of A_c = P^T A P (nc x nc, written whole): its rows of A (local CSR,
+// gcol: local column -> global reduced index)
+void coarse_local_matrix(const SystemData& S, const CoarseLocal& L, int64_t nloc, const int* rp, const int* ci,
+                         const double* va, const int* gcol, double* Acp);
+void coarse_local_restrict(const SystemData& S, CoarseLocal& L, const double* r_loc, double* yc, cudaStream_t s);
+// uc = A_c^-1 yc and cm = T uc (raw-mode coefficients of the prolongation)
+void coarse_local_solve(const SystemData& S, int ld, const float* Ainv, const double* yc, double* uc, double* cm,
+                        cudaStream_t s);
 // solver.cu: y = A x with the system's node-block operator (no reduction)
 void nb_operator_apply(SystemData& S, const double* x, double* y);
 // Y = A X for the rigid_modes(dpn) interleaved vectors of X (symmetric half
 // storage); with gcol, only groups of colour `colour` contribute
 void nb_operator_apply_modes(SystemData& S, const double* X, double* Y, const unsigned char* gcol, int colour,
-                             const unsigned* cmask);
+                             const unsigned* cmask, cudaStream_t s);
 
 // solver.cu
 int64_t system_fsai_classic(SystemData& S);  // builds (once) the classic factor; -1 on failure
+// factor of a whole system for an explicit apply (with its transpose): classic or the
+// attached network's values; nullptr when it cannot be built
+const FsaiFactor* system_block_factor(SystemData& S, bool learned);
 void system_fsai_download(const SystemData& S, int64_t* rp, int64_t* ci, double* lva, double* sig2);
 // average device time in ms of `reps` numeric re-assemblies (values only,
 // pattern fixed, coefficients resident), timed with CUDA events

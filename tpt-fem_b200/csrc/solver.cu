@@ -283,6 +283,15 @@ SystemData::~SystemData() = default;
 
 namespace {
 
+// The coarse set-up beside the network forward (TPTFEM_COARSE_OVERLAP=0: after it).
+bool coarse_overlap() {
+  static const bool on = [] {
+    const char* e = std::getenv("TPTFEM_COARSE_OVERLAP");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 void ensure_work(SystemData& S) {
   cudaStream_t s = S.ctx->stream;
   if (!S.work) {
@@ -329,8 +338,7 @@ int select_coarse(SystemData& S, Engine<double>& E, const tptfem_solver_opts& o,
   // grows faster than the iterations fall; at 400x100x100, 1000-1365
   // aggregates 287-291 ms against 309 with 700; for the 128^3 Poisson
   // random-field problems 2744 (23.9 ms per solve against 26.1 ms with 729).
-  const int per = S.dpn == 1 ? 700 : 2000;
-  const int aggs = o.coarse_aggregates > 0 ? o.coarse_aggregates : std::max(8, std::min(3000, S.nb.ngroups / per));
+  const int aggs = o.coarse_aggregates > 0 ? o.coarse_aggregates : coarse_default_aggregates(S);
   if (want) want = coarse_build(S, aggs);
   if (want && (fresh || !S.coarse.ready)) want = coarse_assemble(S);
   if (want && !S.coarse.ready) want = false;
@@ -556,7 +564,30 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o_in, tptfem_solve_st
     TPT_CUDA(cudaEventRecord(ctx->ev[0], s));
     const bool fresh = (o.flags & TPTFEM_SOLVE_FRESH_SETUP) || !W.lf_ready;
     if (o.flags & TPTFEM_SOLVE_FRESH_SETUP) W.lgraph.ready = false;  // A^ and node features from the values again
+    // Every fresh set-up after the first (engine, node-block layout and coarse
+    // geometry in place): the coarse matrix and its inverse are formed on the
+    // engine's side stream while the network computes the factor on this one;
+    // both only read the operator values.
+    bool coarse_pending = false;
+    if (fresh && W.lf_engine && W.f64_lf.nb_pc && (o.flags & TPTFEM_SOLVE_COARSE) && coarse_overlap() &&
+        S.coarse.state == 1 &&
+        S.coarse.target == (o.coarse_aggregates > 0 ? o.coarse_aggregates : coarse_default_aggregates(S))) {
+      Engine<double>& E = W.f64_lf;
+      {
+        PhaseTimer t(S.ctx->stream, "symmetric operator");
+        select_nb_mode(S, E, o);
+      }
+      E.ensure_side();
+      TPT_CUDA(cudaEventRecord(E.ev_fork, s));
+      TPT_CUDA(cudaStreamWaitEvent(E.side, E.ev_fork, 0));
+      coarse_pending = coarse_assemble_async(S, E.side);
+      TPT_CUDA(cudaEventRecord(E.ev_join, E.side));
+    }
     bool ok = !fresh || learned_factor(S, W);
+    if (coarse_pending) {  // the inverse is needed from here on; a failed Cholesky leaves the coarse space off
+      TPT_CUDA(cudaStreamWaitEvent(s, W.f64_lf.ev_join, 0));
+      coarse_finish(S, s);
+    }
     if (fresh && ok && !W.lf_engine) {
       prepare_fsai_engine(S, W.f64_lf, W.lf, batch);
       PhaseTimer t(S.ctx->stream, "engine + node-block layout");
@@ -577,11 +608,11 @@ void system_solve(SystemData& S, const tptfem_solver_opts& o_in, tptfem_solve_st
         W.nb_factor = &W.lf;
       }
       st.solver_used = solver;
-      {
+      if (!coarse_pending) {
         PhaseTimer t(S.ctx->stream, "symmetric operator");
         select_nb_mode(S, W.f64_lf, o);
       }
-      st.coarse_size = select_coarse(S, W.f64_lf, o, fresh);
+      st.coarse_size = select_coarse(S, W.f64_lf, o, fresh && !coarse_pending);
       TPT_CUDA(cudaEventRecord(ctx->ev[1], s));
       const double bb = norm2_b(S);
       const double bnorm = std::sqrt(bb);
@@ -730,6 +761,21 @@ int64_t system_fsai_classic(SystemData& S) {
   return W.fsai_ready ? W.fsai.nnz : -1;
 }
 
+const FsaiFactor* system_block_factor(SystemData& S, bool learned) {
+  ensure_work(S);
+  SolverWork& W = *S.work;
+  FsaiFactor& F = learned ? W.lf : W.fsai;
+  if (learned) {
+    TPT_REQUIRE(S.lmodel, TPTFEM_ERR_INVALID_ARG, "no network attached to the system");
+    if (S.dpn <= 3) nb_build_operator(S);  // the pattern from the group adjacency, as in a solve
+  }
+  fsai_build_pattern(S, F);
+  if (F.overflow) return nullptr;
+  fsai_build_transpose(S, F);  // before the values, which then fill the transpose too
+  const bool ok = learned ? learned_factor(S, W) : fsai_classic(S, F);
+  return ok ? &F : nullptr;
+}
+
 namespace {
 __global__ void half_to_f64(int64_t n, const __half* __restrict__ a, double* __restrict__ b) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -869,10 +915,9 @@ void nb_operator_apply(SystemData& S, const double* x, double* y) {
 }
 
 void nb_operator_apply_modes(SystemData& S, const double* X, double* Y, const unsigned char* gcol, int colour,
-                             const unsigned* cmask) {
+                             const unsigned* cmask, cudaStream_t s) {
   nb_build_sym(S);
   const NbSell& N = S.nb;
-  cudaStream_t s = S.ctx->stream;
   const int g = std::max(1, std::min(sm_count() * NB_BLOCKS_PER_SM, ceil_div((int64_t)N.nchunks * 32, SPMV_THREADS)));
   if (N.dpn == 3)
     nb_spmv_sym_multi<3, 6><<<g, SPMV_THREADS, 0, s>>>(N.ngroups, N.l_cptr.p, N.l_col.p, N.ks_lval.p, N.ks_diag.p,

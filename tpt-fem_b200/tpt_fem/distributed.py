@@ -1,17 +1,21 @@
-"""Row-partitioned FP64 Jacobi-PCG over several GPUs (one torch.distributed rank
-per GPU).  The library does each rank's device work (tptfem_dist_*: its rows of
-the reduced system with ghost columns, q = A p, the vector updates and the
-partial dot products); this module exchanges the ghost values of p and sums the
-scalars.  The reference solves on one CPU thread; this path has no counterpart
-there.
+"""Row-partitioned FP64 PCG over several GPUs (one torch.distributed rank per
+GPU).  The library does each rank's device work (tptfem_dist_*: its rows of the
+reduced system with ghost columns, q = A p, the vector updates, the
+preconditioner and the partial dot products); this module exchanges the ghost
+values of p and sums the scalars and the coarse-space vectors.  The reference
+solves on one CPU thread; this path has no counterpart there.
 
     ranks = [LibRank(system, rank, size, partition_rows(...))]     # this process's GPU
+    ranks[0].set_precond("learned", coarse_aggregates=0)           # optional; Jacobi otherwise
     it, rel = solve(ranks, TorchComm(group))                       # NCCL across processes
 
-`solve` also runs several ranks of one process in lock step (LocalComm), which
-is how the partitioned path is tested on a single GPU.  Partial sums are added
-over local ranks in order and then across processes, so all ranks take the same
-alpha and beta.
+With a block preconditioner (block FSAI, classic or learned, plus the
+aggregation coarse space) `solve` first sums the ranks' partial coarse matrices
+and has every rank factor the sum; each iteration then sums the nc coarse
+restriction values as well.  `solve` also runs several ranks of one process in
+lock step (LocalComm), which is how the partitioned path is tested on a single
+GPU.  Partial sums are added over local ranks in order and then across
+processes, so all ranks take the same alpha and beta.
 """
 import ctypes as C
 
@@ -43,6 +47,7 @@ class LibRank:
 
     def __init__(self, system, rank, size, row_starts):
         self.ctx, self.rank, self.size = system.ctx, rank, size
+        self.system = system  # the preconditioner's coarse space reads it
         lib = self.ctx.lib
         self.starts = np.asarray(row_starts, dtype=np.int64)
         h = C.c_void_p()
@@ -72,6 +77,44 @@ class LibRank:
 
     def recv_segments(self):
         return self._segments(self._ghost_ptr, self.recv_counts)
+
+    pc = False
+    coarse_size = 0
+    coarse_ready = False
+
+    def set_precond(self, kind="fsai", coarse_aggregates=0):
+        """Block FSAI ("fsai": classic values, "learned": the network attached to
+        the system) and, unless coarse_aggregates is None, the coarse space (0: the
+        default aggregate count).  Returns the coarse size (0: none)."""
+        k = {"fsai": 1, "learned": 2}[kind]
+        nc = C.c_int64()
+        aggs = -1 if coarse_aggregates is None else int(coarse_aggregates)
+        self.ctx.check(self.ctx.lib.tptfem_dist_set_precond(self.ctx.h, self.h, self.system.h, k, aggs,
+                                                           C.byref(nc)))
+        self.pc, self.coarse_size, self.coarse_ready = True, nc.value, False
+        am, av = C.c_void_p(), C.c_void_p()
+        self.ctx.check(self.ctx.lib.tptfem_dist_coarse_buffers(self.h, C.byref(am), C.byref(av)))
+        self._am, self._av = am.value or 0, av.value or 0
+        return self.coarse_size
+
+    def _dev(self, ptr, n):
+        import torch
+        return torch.as_tensor(_DevArray(ptr, n), device="cuda")
+
+    def coarse_matrix(self):
+        return self._dev(self._am, self.coarse_size * self.coarse_size)
+
+    def coarse_vector(self):
+        return self._dev(self._av, self.coarse_size)
+
+    def coarse_factor(self):
+        self.ctx.check(self.ctx.lib.tptfem_dist_coarse_factor(self.ctx.h, self.h))
+        self.coarse_ready = True
+
+    def precondition(self):
+        v = C.c_double()
+        self.ctx.check(self.ctx.lib.tptfem_dist_precondition(self.ctx.h, self.h, C.byref(v)))
+        return np.array([v.value])
 
     def start(self):
         o = np.zeros(2)
@@ -111,6 +154,18 @@ class LocalComm:
     def allreduce(self, v):
         return v
 
+    def sum_tensors(self, ts):
+        """Every tensor becomes the sum of all (added in rank order)."""
+        if len(ts) > 1:
+            s = ts[0].clone()
+            for t in ts[1:]:
+                s += t
+            for t in ts:
+                t.copy_(s)
+        if ts and ts[0].is_cuda:
+            import torch
+            torch.cuda.synchronize()
+
     def exchange(self, ranks):
         sends = [r.send_segments() for r in ranks]
         for r in ranks:
@@ -132,6 +187,12 @@ class TorchComm:
         self.dist.all_reduce(t, group=self.group)
         return t.cpu().numpy()
 
+    def sum_tensors(self, ts):
+        (t,) = ts
+        self.dist.all_reduce(t, group=self.group)
+        if t.is_cuda:
+            self.torch.cuda.synchronize()
+
     def exchange(self, ranks):
         (r,) = ranks
         ops = []
@@ -146,15 +207,40 @@ class TorchComm:
             self.torch.cuda.synchronize()
 
 
+def prepare(ranks, comm):
+    """Sum the ranks' partial coarse matrices and factor the sum on every rank
+    (once, after set_precond; solve calls it)."""
+    r0 = ranks[0]
+    if r0.pc and r0.coarse_size and not r0.coarse_ready:
+        comm.sum_tensors([r.coarse_matrix() for r in ranks])
+        for r in ranks:
+            r.coarse_factor()
+
+
 def solve(ranks, comm, tol=1e-10, max_iter=100000):
-    """FP64 Jacobi-PCG over the partitioned system -> (iterations, recursive relative residual)."""
+    """FP64 PCG over the partitioned system -> (iterations, recursive relative residual).
+    Jacobi, or the ranks' block preconditioner when set_precond was called."""
     def total(vals):
         s = np.zeros_like(vals[0])
         for v in vals:  # local ranks in rank order
             s = s + v
         return comm.allreduce(s)
 
+    pc = bool(getattr(ranks[0], "pc", False))
+    nc = int(getattr(ranks[0], "coarse_size", 0)) if pc else 0
+    if pc:
+        prepare(ranks, comm)
+
+    def precondition():  # z = M r on every rank; the summed r.z
+        if nc:
+            comm.sum_tensors([r.coarse_vector() for r in ranks])
+        return total([r.precondition() for r in ranks])[0]
+
     rr, rz = total([r.start() for r in ranks])
+    if pc:
+        rz = precondition()
+        for r in ranks:
+            r.direction(0.0)
     bb, it = rr, 0
     while rr > tol * tol * bb and it < max_iter:
         for r in ranks:
@@ -165,6 +251,8 @@ def solve(ranks, comm, tol=1e-10, max_iter=100000):
             raise ArithmeticError("PCG breakdown: p.Ap <= 0")
         alpha = rz / pq
         rr, rz_new = total([r.update(alpha) for r in ranks])
+        if pc:
+            rz_new = precondition()
         beta = rz_new / rz
         rz = rz_new
         for r in ranks:
