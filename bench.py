@@ -309,25 +309,37 @@ def run_ours(args, world, rank, local):
         op_ms, op_bytes = prof["csr_f64_ms"], csr_bytes
         op_name = "spmv_kernel<double> (CSR, FP64)"
     achieved = op_bytes / (op_ms * 1e-3) / 1e9
+    # end to end through the C ABI from host arrays, on every rank's replica
+    # (max over ranks): one untimed run pays the first-use costs (the pinned
+    # staging buffer, library module loads); then the median of three timed runs
+    coords = mesh.coords_array.copy()
+    conn = mesh.conn_array.copy()
+    e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model, coarse)
+    barrier(world)
+    e2e = [e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model, coarse) for _ in range(3)]
+    e2e_s, h2d, d2h, e2e_st = sorted(e2e, key=lambda t: t[0])[1]
+    e2e_s = barrier_max(e2e_s, world)
     out = None
     if rank == 0:
-        coords = mesh.coords_array.copy()
-        conn = mesh.conn_array.copy()
-        # one untimed run pays the first-use costs (the pinned staging buffer,
-        # library module loads); then the median of three timed runs
-        e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model, coarse)
-        e2e = [e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model, coarse) for _ in range(3)]
-        e2e_s, h2d, d2h, e2e_st = sorted(e2e, key=lambda t: t[0])[1]
         phases = {}
         e2e_once(F, LF, W, ctx, solver, (coords, conn, E, dof, val), model, coarse, phases)
-        # the plain method on the host cores: one complete solve of this exact
-        # system, measured (no scaling), and the one-core iteration cost
-        sysh = host_system(S)
-        nthr = cpu_threads()
-        cpu_ms_per_iteration(sysh, nthr, 3)  # page in, start the thread team
-        cpu_s, cpu_it, cpu_rel = cpu_full_solve(sysh, TOL, nthr)
-        cpu_1core_ms = cpu_ms_per_iteration(sysh, 1, 5)
-        del sysh
+        # the plain method on the host cores (at N = 1 only: the other ranks
+        # would wait on rank 0 at the next collective): one complete solve of
+        # this exact system, measured (no scaling), and the one-core iteration cost
+        cpu = None
+        if world == 1:
+            sysh = host_system(S)
+            nthr = cpu_threads()
+            cpu_ms_per_iteration(sysh, nthr, 3)  # page in, start the thread team
+            cpu_s, cpu_it, cpu_rel = cpu_full_solve(sysh, TOL, nthr)
+            cpu_1core_ms = cpu_ms_per_iteration(sysh, 1, 5)
+            del sysh
+            cpu = {"value": cpu_s, "unit": "s", "cores": nthr, "kind": "port", "iterations": cpu_it,
+                   "rel_residual": cpu_rel, "one_core_ms_per_iteration": cpu_1core_ms,
+                   "sample": f"one complete oracle FP64 Jacobi-PCG solve (int32 CSR, OpenMP, {nthr} host "
+                             f"threads) of this exact reduced system from x = 0 to true rel. residual "
+                             f"{TOL:g}: {abs(cpu_it)} iterations, measured, not scaled; one core measured "
+                             f"at {cpu_1core_ms:.1f} ms per iteration over 5 iterations"}
         its = [st["iterations"] for st in steps]
         fsai_like = solver in (F.SOLVER_FSAI_MP_PCG, F.SOLVER_LEARNED_FSAI_PCG)
         kernels_per_it = (5 if fsai_like else 3) + (3 if coarse else 0)
@@ -375,17 +387,12 @@ def run_ours(args, world, rank, local):
                          "csr_formula_gbs": csr_bytes / (op_ms * 1e-3) / 1e9,
                          "nb_full_ms": prof["nb_ms"], "csr_f64_ms": prof["csr_f64_ms"],
                          "csr_f64_gbs": csr_bytes / (prof["csr_f64_ms"] * 1e-3) / 1e9},
-            "cpu_baseline": {"value": cpu_s, "unit": "s", "cores": nthr, "kind": "port",
-                             "iterations": cpu_it, "rel_residual": cpu_rel,
-                             "one_core_ms_per_iteration": cpu_1core_ms,
-                             "sample": f"one complete oracle FP64 Jacobi-PCG solve (int32 CSR, OpenMP, {nthr} host "
-                                       f"threads) of this exact reduced system from x = 0 to true rel. residual "
-                                       f"{TOL:g}: {abs(cpu_it)} iterations, measured, not scaled; one core measured "
-                                       f"at {cpu_1core_ms:.1f} ms per iteration over 5 iterations"},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "wall_s_timed_region": t_wall,
         }
+        if cpu is not None:
+            out["cpu_baseline"] = cpu
     return out
 
 
@@ -461,18 +468,19 @@ def run_box8(args, world, rank, local):
     if rank != 0:
         return None
     u_ref = cpu_once()
-    t0 = time.perf_counter()
-    for _ in range(3):
-        cpu_once()
-    cpu_s = (time.perf_counter() - t0) / 3
-    return {"metric": "solve_poisson end to end (mesh, assembly, load, reduction, solve)", "value": gpu_s,
-            "unit": "s", "higher_is_better": False,
-            "config": {"workload": "poisson_box8", "mesh": n, "nodes": len(c), "free_dofs": 343, "tol": 1e-14},
-            "max_rel_error_vs_dense_lu": float(np.max(np.abs(u - u_ref)) / np.max(np.abs(u_ref))),
-            "iterations": st["iterations"],
-            "cpu_baseline": {"value": cpu_s, "unit": "s", "cores": 1, "kind": "port",
-                             "sample": "oracle solve_with_dirichlet on the same case (COO assembly, to_csr, "
-                                       "dense LU -- the reference's own path), 3 calls, measured"}}
+    rec = {"metric": "solve_poisson end to end (mesh, assembly, load, reduction, solve)", "value": gpu_s,
+           "unit": "s", "higher_is_better": False,
+           "config": {"workload": "poisson_box8", "mesh": n, "nodes": len(c), "free_dofs": 343, "tol": 1e-14},
+           "max_rel_error_vs_dense_lu": float(np.max(np.abs(u - u_ref)) / np.max(np.abs(u_ref))),
+           "iterations": st["iterations"]}
+    if world == 1:
+        t0 = time.perf_counter()
+        for _ in range(3):
+            cpu_once()
+        rec["cpu_baseline"] = {"value": (time.perf_counter() - t0) / 3, "unit": "s", "cores": 1, "kind": "port",
+                               "sample": "oracle solve_with_dirichlet on the same case (COO assembly, to_csr, "
+                                         "dense LU -- the reference's own path), 3 calls, measured"}
+    return rec
 
 
 def run_cube(args, world, rank, local):
@@ -576,6 +584,12 @@ def run_poisson_grf(args, world, rank, local):
     prob = W.GrfPoisson(ctx, n)
     S = prob.system(4999)
     model.attach(S)
+    if args.profile:  # the headline method's solves only, on one field (for an ncu launch list)
+        S.refresh(prob.matrix(seeds[0]), prob.rhs)
+        for _ in range(args.steps):
+            S.solve(tol=POISSON_TOL, fresh_setup=True, **methods["learned_coarse"])
+        ctx.synchronize()
+        return None
     for _ in range(args.warmup):
         for kw in methods.values():
             S.solve(tol=POISSON_TOL, fresh_setup=True, **kw)
@@ -605,7 +619,7 @@ def run_poisson_grf(args, world, rank, local):
                "methods": {m: {"mean_s": mean[m], "mean_iterations": float(np.mean(r["it"])),
                                "max_rel_residual": float(np.max(r["res"])), "fell_back": r["fell_back"]}
                            for m, r in rec.items()},
-               "cpu_baseline": poisson_cpu_baseline(S, seeds[-1]),
+               "cpu_baseline": poisson_cpu_baseline(S, seeds[-1]) if world == 1 else None,
                "speedup_learned_vs_jacobi": mean["jacobi_csr"] / mean["learned"],
                "speedup_learned_coarse_vs_jacobi": mean["jacobi_csr"] / mean["learned_coarse"],
                "clocks": clk.summary()}
@@ -668,7 +682,8 @@ def run_topopt(args, world, rank, local):
                           "direct_instances": st["direct_instances"], "refinement_steps": st["refinement_steps"],
                           "parallelism": f"replicas{world}"},
                "batch_seconds": sec, "tune_ms": st["tune_ms"], "threads_per_instance": st["block_threads"],
-               "cpu_baseline": topopt_cpu_baseline(probs, world * args.instances * args.oc_iters / sec),
+               "cpu_baseline": (topopt_cpu_baseline(probs, world * args.instances * args.oc_iters / sec)
+                                if world == 1 else None),
                "pcg_iterations": st["pcg_iterations"],
                "compliance_final_over_initial": {"min": min(ratio), "median": float(np.median(ratio)),
                                                  "max": max(ratio)},
@@ -742,7 +757,7 @@ def run_assembly(args, world, rank, local):
     alg = 24.0 * n_nodes + 16.0 * n_el + 8.0 * n_el + 8.0 * nnz
     out = None
     if rank == 0:
-        cpu, sample = assembly_cpu_baseline()
+        cpu, sample = assembly_cpu_baseline() if world == 1 else (None, None)
         out = {"metric": "Tet4 elasticity assembly throughput (numeric, pattern fixed)",
                "value": world * n_el / (ms * 1e-3) / 1e6, "unit": "Melem/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -759,7 +774,8 @@ def run_assembly(args, world, rank, local):
                             "algorithmic_formula": "24 N + 16 E + 8 E + 8 nnz (coords, connectivity, E, values)"},
                "e2e": {"value": n_el / e2e_s / 1e6, "unit": "Melem/s", "seconds": e2e_s,
                        "h2d_bytes_per_step": int(coords.nbytes + conn.nbytes + E.nbytes), "d2h_bytes_per_step": 8},
-               "cpu_baseline": {"value": cpu, "unit": "Melem/s", "cores": 1, "kind": "port", "sample": sample},
+               "cpu_baseline": ({"value": cpu, "unit": "Melem/s", "cores": 1, "kind": "port", "sample": sample}
+                                if world == 1 else None),
                "gpu_launches": args.steps,
                "clocks": clk.summary()}
     return out
@@ -823,7 +839,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--solver", default="learned", choices=["learned", "fsai", "jacobi", "mp"])
-    ap.add_argument("--profile", action="store_true", help="run only the timed solves (ncu launch list)")
+    ap.add_argument("--profile", action="store_true",
+                    help="cantilever / poisson_grf: run only the headline method's solves (ncu launch list)")
     ap.add_argument("--no-coarse", action="store_true", help="single-level preconditioner (no coarse space)")
     ap.add_argument("--workload", default="cantilever",
                     choices=["cantilever", "poisson_grf", "topopt", "assembly", "cube"],
