@@ -121,7 +121,8 @@ template <int DPN>
 __global__ void __launch_bounds__(CS_THREADS) cs_moments(const int* __restrict__ sbeg, const int* __restrict__ send,
                                                          const int* __restrict__ alist, const float* __restrict__ y,
                                                          const double* __restrict__ w, double* __restrict__ smom,
-                                                         int g0) {
+                                                         int g0, const int* __restrict__ done = nullptr) {
+  if (done && *done) return;  // the PCG iteration this belongs to was not needed
   constexpr int NM = rigid_modes(DPN);
   __shared__ double sh[CS_THREADS / 32][NM];
   const int seg = blockIdx.x;
@@ -169,7 +170,8 @@ __device__ __forceinline__ double agg_moment(int I, int mp, int nm, const int* _
 
 // yc = P^T r from the segment moments.
 __global__ void cs_yc(int na, int nm, const int* __restrict__ aseg, const double* __restrict__ smom,
-                      const double* __restrict__ T, double* __restrict__ yc) {
+                      const double* __restrict__ T, double* __restrict__ yc, const int* __restrict__ done = nullptr) {
+  if (done && *done) return;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j < na * nm) yc[j] = agg_moment(j / nm, j % nm, nm, aseg, smom, T);
 }
@@ -180,7 +182,9 @@ __global__ void cs_yc(int na, int nm, const int* __restrict__ aseg, const double
 // lane, so the shared-memory reads are conflict-free); eight loads per lane are
 // kept in flight.
 __global__ void __launch_bounds__(CS_THREADS) cs_gemv(int nc, int ld, const double* __restrict__ yc,
-                                                      const float* __restrict__ Ainv, double* __restrict__ uc) {
+                                                      const float* __restrict__ Ainv, double* __restrict__ uc,
+                                                      const int* __restrict__ done = nullptr) {
+  if (done && *done) return;
   extern __shared__ double ys[];
   for (int j = threadIdx.x; j < ld; j += blockDim.x) ys[j] = j < nc ? yc[j] : 0.0;
   __syncthreads();
@@ -204,7 +208,8 @@ __global__ void __launch_bounds__(CS_THREADS) cs_gemv(int nc, int ld, const doub
 
 // cm = T uc per aggregate (raw-mode coefficients of P uc).
 __global__ void cs_raw(int na, int nm, const double* __restrict__ T, const double* __restrict__ uc,
-                       double* __restrict__ cm) {
+                       double* __restrict__ cm, const int* __restrict__ done = nullptr) {
+  if (done && *done) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= na * nm) return;
   const int I = t / nm, k = t % nm;
@@ -779,21 +784,21 @@ void coarse_factor_async(tptfem_context* ctx, cudaStream_t s, int nc, int ld, do
   TPT_CHECK_LAUNCH();
 }
 
-void coarse_restrict_solve(const SystemData& S, const double* r, cudaStream_t s) {
+void coarse_restrict_solve(const SystemData& S, const double* r, cudaStream_t s, const int* done) {
   const CoarseSpace& C = S.coarse;
-#define TPT_CS_R(D)                                                                                     \
-  cs_moments<D><<<C.nseg, CS_THREADS, 0, s>>>(C.sbeg.p, C.send.p, C.alist.p, C.y.p, r, C.smom.p, 0); \
+#define TPT_CS_R(D)                                                                                           \
+  cs_moments<D><<<C.nseg, CS_THREADS, 0, s>>>(C.sbeg.p, C.send.p, C.alist.p, C.y.p, r, C.smom.p, 0, done); \
   TPT_CHECK_LAUNCH();
   if (S.dpn == 3) { TPT_CS_R(3) }
   else if (S.dpn == 2) { TPT_CS_R(2) }
   else { TPT_CS_R(1) }
 #undef TPT_CS_R
-  cs_yc<<<blocks_for(C.nc), CS_THREADS, 0, s>>>(C.na, C.nm, C.aseg.p, C.smom.p, C.T.p, C.yc.p);
+  cs_yc<<<blocks_for(C.nc), CS_THREADS, 0, s>>>(C.na, C.nm, C.aseg.p, C.smom.p, C.T.p, C.yc.p, done);
   TPT_CHECK_LAUNCH();
   cs_gemv<<<(C.nc + CS_THREADS / 32 - 1) / (CS_THREADS / 32), CS_THREADS, (size_t)C.ld * sizeof(double), s>>>(
-      C.nc, C.ld, C.yc.p, C.Ainv.p, C.uc.p);
+      C.nc, C.ld, C.yc.p, C.Ainv.p, C.uc.p, done);
   TPT_CHECK_LAUNCH();
-  cs_raw<<<blocks_for(C.nc), CS_THREADS, 0, s>>>(C.na, C.nm, C.T.p, C.uc.p, C.cm.p);
+  cs_raw<<<blocks_for(C.nc), CS_THREADS, 0, s>>>(C.na, C.nm, C.T.p, C.uc.p, C.cm.p, done);
   TPT_CHECK_LAUNCH();
 }
 

@@ -332,7 +332,9 @@ bool coarse_assemble(SystemData& S);                      // A_c and its inverse
 // then, once s's work is complete or ordered before stream s2, its status
 bool coarse_assemble_async(SystemData& S, cudaStream_t s);
 bool coarse_finish(SystemData& S, cudaStream_t s2);
-void coarse_restrict_solve(const SystemData& S, const double* r, cudaStream_t s);  // uc = A_c^-1 P^T r
+// uc = A_c^-1 P^T r and cm = T uc; every kernel returns at once while *done != 0
+// (a PCG iteration of a captured batch that the converged solve does not need)
+void coarse_restrict_solve(const SystemData& S, const double* r, cudaStream_t s, const int* done);
 void coarse_download(const SystemData& S, int* na, int* nm, double* Ainv_or_null);  // FP32 inverse, widened
 int coarse_default_aggregates(const SystemData& S);  // about one aggregate per 2000 (vector) / 700 (scalar) groups
 // Cholesky and FP32 explicit inverse of an SPD nc x nc matrix (Ac is overwritten;

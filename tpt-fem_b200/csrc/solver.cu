@@ -199,7 +199,7 @@ struct Engine {
           ensure_side();
           TPT_CUDA(cudaEventRecord(ev_fork, s));
           TPT_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));
-          coarse_restrict_solve(*csys, r.p, side);
+          coarse_restrict_solve(*csys, r.p, side, &st.p->done);
           TPT_CUDA(cudaEventRecord(ev_join, side));
         }
 #define TPT_NB_FSAI(D)                                                                                           \
