@@ -396,6 +396,54 @@ def run_ours(args, world, rank, local):
     return out
 
 
+def run_partitioned(args, world, rank, local):
+    """The row-partitioned two-level PCG (tptfem_dist_*: block learned FSAI of
+    each rank's x-slab plus the coarse space from the ranks' summed partial
+    coarse matrices) on the headline system, 1, 2, 4 and 8 ranks run in lock
+    step on this process's GPU (tpt_fem.distributed with LocalComm: the
+    exchanges are device copies, the sums host additions).  What it measures
+    is how the partition changes the iteration count; its wall time includes
+    the Python driver's per-step host round trips, so it is no multi-GPU
+    timing."""
+    import tpt_fem as F
+    from tpt_fem import distributed as D
+    from tpt_fem import lfsai as LF
+    from tpt_fem import workloads as W
+    ctx = F.Context(local)
+    mesh, K, S, E, rhs, dof, val = build_system(F, W, ctx, args.mesh)
+    model = LF.LearnedFsai.load(ctx, WEIGHTS)
+    model.attach(S)
+    one = S.solve(solver=F.SOLVER_LEARNED_FSAI_PCG, tol=TOL, fresh_setup=True, coarse=True)
+    rec = {"one_gpu_engine": {"iterations": one["iterations"], "rel_residual": one["rel_residual"],
+                              "coarse_size": one["coarse_size"]}}
+    import scipy.sparse as sp
+    rp, ci, va, fred, _ = S.download()
+    A = sp.csr_matrix((va, ci, rp), shape=(S.n_free, S.n_free))
+    del rp, ci, va
+    for nranks in (1, 2, 4, 8):
+        starts = D.partition_rows(S.n_free, 3, nranks)
+        ranks = [D.LibRank(S, k, nranks, starts) for k in range(nranks)]
+        t0 = time.perf_counter()
+        nc = {r.set_precond("learned", 0) for r in ranks}
+        t1 = time.perf_counter()
+        it, rel = D.solve(ranks, D.LocalComm(), tol=TOL, max_iter=2000)
+        t2 = time.perf_counter()
+        x = np.concatenate([r.solution() for r in ranks])
+        rec[f"ranks_{nranks}"] = {"iterations": it, "rel_residual": rel, "coarse_size": max(nc),
+                                 "host_rel_residual": float(np.linalg.norm(fred - A @ x) / np.linalg.norm(fred)),
+                                 "setup_s": t1 - t0, "solve_wall_s": t2 - t1}
+        del ranks
+    if rank != 0:
+        return None
+    return {"metric": "iterations to FP64 rel. residual 1e-10 of the row-partitioned two-level PCG "
+                      "(lock-step ranks on one GPU)", "value": rec["ranks_8"]["iterations"], "unit": "iterations",
+            "higher_is_better": False,
+            "config": {"workload": "partitioned_" + WORKLOAD, "free_dofs": int(S.n_free),
+                       "preconditioner": "block learned FSAI per x-slab + rigid-body coarse space (summed partial "
+                                         "coarse matrices)", "tol": TOL},
+            "runs": rec}
+
+
 def run_cantilever_sizes(args, world, rank, local):
     """The cantilever family at its other sizes: [200,50,50] (1.56M free dofs)
     and [400,100,100] (12.27M free dofs), same density recipe, clamp and
@@ -843,7 +891,7 @@ def main():
                     help="cantilever / poisson_grf: run only the headline method's solves (ncu launch list)")
     ap.add_argument("--no-coarse", action="store_true", help="single-level preconditioner (no coarse space)")
     ap.add_argument("--workload", default="cantilever",
-                    choices=["cantilever", "poisson_grf", "topopt", "assembly", "cube"],
+                    choices=["cantilever", "poisson_grf", "topopt", "assembly", "cube", "partitioned"],
                     help="poisson_grf: the heterogeneous-Poisson learned-preconditioner configuration; cube: the "
                          "64^3 elasticity cube, FP64 vs FP32-inner PCG")
     ap.add_argument("--headline-only", action="store_true",
@@ -853,7 +901,7 @@ def main():
     ap.add_argument("--oc-iters", type=int, default=100, help="topopt: OC iterations")
     ap.add_argument("--poisson-n", type=int, default=128, help="poisson_grf: box_mesh cells per axis")
     ap.add_argument("--mesh", type=int, nargs=3, default=None,
-                    help="with --profile: cantilever cells (a smaller case for ncu captures)")
+                    help="with --profile (or --workload partitioned): cantilever cells, a smaller case")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -866,6 +914,8 @@ def main():
         out = run_assembly(args, world, rank, local)
     elif args.workload == "cube":
         out = run_cube(args, world, rank, local)
+    elif args.workload == "partitioned":
+        out = run_partitioned(args, world, rank, local)
     else:
         out = run_ours(args, world, rank, local)
         if not (args.headline_only or args.profile):

@@ -339,9 +339,22 @@ tptfem_status tptfem_dist_set_precond(tptfem_context* ctx, tptfem_dist* d, tptfe
 tptfem_status tptfem_dist_coarse_buffers(const tptfem_dist* d, double** coarse_matrix, double** coarse_vector);
 tptfem_status tptfem_dist_coarse_factor(tptfem_context* ctx, tptfem_dist* d);
 tptfem_status tptfem_dist_precondition(tptfem_context* ctx, tptfem_dist* d, double* out_rz);
+/* Reliable update (the true residual replaces the recursive one; the search
+ * direction is kept).  When the summed r.r of a tptfem_dist_update has dropped
+ * by 1e-12 since the last replacement, or below the target, skip that step's
+ * direction update and: tptfem_dist_residual_begin (x takes the place of p's
+ * owned part); pack and exchange as usual; tptfem_dist_residual_end computes
+ * r = b - A x (compensated sums) and returns the local r.r, r.z as
+ * tptfem_dist_update does (with a block preconditioner: r.r and 0, the
+ * restriction's part in coarse_vector, then tptfem_dist_precondition).  Stop
+ * if the true r.r meets the target; otherwise beta = r.z (true) / the r.z of
+ * the last step length, and tptfem_dist_direction(beta). */
+tptfem_status tptfem_dist_residual_begin(tptfem_context* ctx, tptfem_dist* d);
+tptfem_status tptfem_dist_residual_end(tptfem_context* ctx, tptfem_dist* d, double out_rr_rz[2]);
 /* nranks ranks on this context's GPU in lock step, the exchange done by device copies:
- * the same arithmetic as nranks GPUs; x (n_free doubles, host), *relres the recursive
- * residual at exit.  For testing the partitioned path on one device. */
+ * the same arithmetic as nranks GPUs (Jacobi, with the reliable updates above);
+ * x (n_free doubles, host), *relres the true relative residual at exit.  For testing
+ * the partitioned path on one device. */
 tptfem_status tptfem_dist_solve_local(tptfem_context* ctx, tptfem_system* sys, int nranks, double rel_tol,
                                       int64_t max_iter, double* x, int64_t* iterations, double* relres);
 

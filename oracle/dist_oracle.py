@@ -142,5 +142,17 @@ class NumpyRank:
     def direction(self, beta):
         self.p[:self.n_owned] = self.z + beta * self.p[:self.n_owned]
 
+    def residual_begin(self):
+        self.pbak = self.p[:self.n_owned].copy()
+        self.p[:self.n_owned] = self.x
+
+    def residual_end(self):
+        self.r = self.b - self.A @ self.p
+        self.p[:self.n_owned] = self.pbak
+        if self.pc:
+            return self._after_update()
+        self.z = self.dinv * self.r
+        return np.array([self.r @ self.r, self.r @ self.z])
+
     def solution(self):
         return self.x.copy()

@@ -432,11 +432,21 @@ tptfem_status tptfem_dist_precondition(tptfem_context* ctx, tptfem_dist* d, doub
     *out_rz = dist_precondition(*d->d);
   })
 }
+tptfem_status tptfem_dist_residual_begin(tptfem_context* ctx, tptfem_dist* d) {
+  TPT_DIST_CALL(dist_residual_begin(*d->d))
+}
+tptfem_status tptfem_dist_residual_end(tptfem_context* ctx, tptfem_dist* d, double out_rr_rz[2]) {
+  TPT_DIST_CALL({
+    TPT_REQUIRE(out_rr_rz, TPTFEM_ERR_INVALID_ARG, "out_rr_rz is NULL");
+    dist_residual_end(*d->d, out_rr_rz);
+  })
+}
 tptfem_status tptfem_dist_coarse_factor(tptfem_context* ctx, tptfem_dist* d) {
   TPT_DIST_CALL(dist_coarse_factor(*d->d))
 }
 tptfem_status tptfem_dist_solution(tptfem_context* ctx, const tptfem_dist* d, double* x_owned) {
   TPT_DIST_CALL({
+    dist_accumulate(*d->d);
     if (d->d->nloc) device_to_host(ctx, x_owned, d->d->x.p, d->d->nloc * sizeof(double));
   })
 }

@@ -77,6 +77,18 @@ struct DevBuf {
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
+// Error-free transformations (Knuth TwoSum; TwoProduct through FMA), for the
+// compensated FP64 residuals of the solvers.
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = a + b;
+  const double bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+__device__ __forceinline__ void two_prod(double a, double b, double& p, double& e) {
+  p = a * b;
+  e = __fma_rn(a, b, -p);
+}
+
 // Number of SMs of the current device (cached per process; all B200s have 148).
 int sm_count();
 

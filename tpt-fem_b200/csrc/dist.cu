@@ -39,6 +39,9 @@ namespace tptfem {
 namespace {
 
 constexpr int DT_THREADS = 256, DT_LPR = 8;
+// reliable updates: the true residual replaces the recursive one whenever the
+// latter has dropped by this factor, and before the solve may stop
+constexpr double DIST_DELTA = 1e-6;
 
 // q = A_loc p on the owned rows (DT_LPR lanes per row), per-block p.q partials.
 __global__ void __launch_bounds__(DT_THREADS) dist_spmv_dot(int64_t nloc, const int* __restrict__ rp,
@@ -104,6 +107,67 @@ __global__ void __launch_bounds__(DT_THREADS) dist_update(int64_t nloc, double a
   if (threadIdx.x == 0) {
     part[2 * blockIdx.x] = s1[0];
     part[2 * blockIdx.x + 1] = s2[0];
+  }
+}
+
+// r = b - A x with compensated (double-double) accumulation, so that r is the
+// residual of the FP64 x rather than a sum whose cancellation noise can exceed
+// a 1e-10 target; with Jacobi z = dinv r.  Per-block partials of r.r and r.z.
+__global__ void __launch_bounds__(DT_THREADS) dist_true_residual(int64_t nloc, const int* __restrict__ rp,
+                                                                 const int* __restrict__ ci,
+                                                                 const double* __restrict__ va,
+                                                                 const double* __restrict__ x,
+                                                                 const double* __restrict__ b,
+                                                                 double* __restrict__ r, double* __restrict__ z,
+                                                                 const double* __restrict__ dinv,
+                                                                 double* __restrict__ part, bool jacobi) {
+  __shared__ double s1[DT_THREADS / DT_LPR], s2[DT_THREADS / DT_LPR];
+  const int64_t t = (int64_t)blockIdx.x * DT_THREADS + threadIdx.x;
+  const int64_t i = t / DT_LPR;
+  const int l = (int)(t % DT_LPR);
+  double hi = 0.0, lo = 0.0;
+  if (i < nloc)
+    for (int k = rp[i] + l; k < rp[i + 1]; k += DT_LPR) {
+      double p, pe, s, se;
+      two_prod(va[k], x[ci[k]], p, pe);
+      two_sum(hi, p, s, se);
+      hi = s;
+      lo += pe + se;
+    }
+  for (int o = DT_LPR / 2; o > 0; o >>= 1) {
+    const double oh = __shfl_xor_sync(0xffffffffu, hi, o, DT_LPR);
+    const double ol = __shfl_xor_sync(0xffffffffu, lo, o, DT_LPR);
+    double s, se;
+    two_sum(hi, oh, s, se);
+    hi = s;
+    lo += ol + se;
+  }
+  double rr = 0.0, rz = 0.0;
+  if (i < nloc && l == 0) {
+    double r1, e1;
+    two_sum(b[i], -hi, r1, e1);
+    const double ri = r1 + (e1 - lo);
+    r[i] = ri;
+    rr = ri * ri;
+    if (jacobi) {
+      const double zi = dinv[i] * ri;
+      z[i] = zi;
+      rz = ri * zi;
+    }
+  }
+  if (l == 0) {
+    s1[threadIdx.x / DT_LPR] = rr;
+    s2[threadIdx.x / DT_LPR] = rz;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a1 = 0.0, a2 = 0.0;
+    for (int w = 0; w < DT_THREADS / DT_LPR; ++w) {
+      a1 += s1[w];
+      a2 += s2[w];
+    }
+    part[2 * blockIdx.x] = a1;
+    part[2 * blockIdx.x + 1] = a2;
   }
 }
 
@@ -203,6 +267,14 @@ __global__ void dist_block_red_map(int64_t n, const int* __restrict__ red, int64
   if (j >= n) return;
   const int v = red[j];
   out[j] = (v >= r0 && v < r1) ? (int)(v - r0) : -1;
+}
+
+__global__ void dist_add_clear(int64_t nloc, double* __restrict__ xl, double* __restrict__ x) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nloc) {
+    x[i] += xl[i];
+    xl[i] = 0.0;
+  }
 }
 
 __global__ void dist_direction(int64_t nloc, double beta, const double* __restrict__ z, double* __restrict__ p) {
@@ -315,6 +387,7 @@ std::unique_ptr<DistData> dist_create(tptfem_context* ctx, SystemData& S, int ra
     TPT_CUDA(cudaMemcpyAsync(D->b.p, S.fred.p + D->r0, D->nloc * sizeof(double), cudaMemcpyDeviceToDevice, s));
   D->dinv.alloc(nl, s);
   D->x.alloc(nl, s);
+  D->xl.alloc(nl, s);
   D->r.alloc(nl, s);
   D->z.alloc(nl, s);
   D->q.alloc(nl, s);
@@ -342,6 +415,7 @@ void dist_start(DistData& D, double* out) {
   cudaStream_t s = D.ctx->stream;
   if (D.nloc) {
     TPT_CUDA(cudaMemsetAsync(D.x.p, 0, D.nloc * sizeof(double), s));
+    TPT_CUDA(cudaMemsetAsync(D.xl.p, 0, D.nloc * sizeof(double), s));
     TPT_CUDA(cudaMemcpyAsync(D.r.p, D.b.p, D.nloc * sizeof(double), cudaMemcpyDeviceToDevice, s));
     TPT_CUDA(cudaMemsetAsync(D.q.p, 0, D.nloc * sizeof(double), s));
     TPT_CUDA(cudaMemsetAsync(D.p.p, 0, D.nloc * sizeof(double), s));
@@ -371,7 +445,7 @@ double dist_spmv_dot(DistData& D) {
 
 void dist_update(DistData& D, double alpha, double* out) {
   cudaStream_t s = D.ctx->stream;
-  dist_update<<<D.blocks_vec, DT_THREADS, 0, s>>>(D.nloc, alpha, D.x.p, D.r.p, D.z.p, D.p.p, D.q.p, D.dinv.p,
+  dist_update<<<D.blocks_vec, DT_THREADS, 0, s>>>(D.nloc, alpha, D.xl.p, D.r.p, D.z.p, D.p.p, D.q.p, D.dinv.p,
                                                   D.part.p, D.pc == 0);
   TPT_CHECK_LAUNCH();
   if (D.nc) coarse_local_restrict(*D.sys, D.cl, D.r.p, D.yc.p, s);  // this rank's part of P^T r
@@ -492,6 +566,41 @@ void dist_direction(DistData& D, double beta) {
   TPT_CHECK_LAUNCH();
 }
 
+// x += xl, xl = 0: the steps since the last reliable update are kept apart
+// from x (a correction far smaller than x), so their rounding does not set a
+// floor under the true residual.
+void dist_accumulate(DistData& D) {
+  if (!D.nloc) return;
+  dist_add_clear<<<D.blocks_vec, DT_THREADS, 0, D.ctx->stream>>>(D.nloc, D.xl.p, D.x.p);
+  TPT_CHECK_LAUNCH();
+}
+
+// True residual, part 1: the owned part of p is saved and replaced by x, so
+// that the caller's usual pack + exchange brings x's ghost values.
+void dist_residual_begin(DistData& D) {
+  cudaStream_t s = D.ctx->stream;
+  if (!D.nloc) return;
+  dist_accumulate(D);
+  if (!D.pbak.p) D.pbak.alloc(D.nloc, s);
+  TPT_CUDA(cudaMemcpyAsync(D.pbak.p, D.p.p, D.nloc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  TPT_CUDA(cudaMemcpyAsync(D.p.p, D.x.p, D.nloc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+}
+
+// Part 2 (after the exchange): r = b - A x replaces the recursive residual;
+// out as dist_update's (with a block preconditioner: the coarse restriction's
+// partial in yc); the search direction is restored.
+void dist_residual_end(DistData& D, double* out) {
+  cudaStream_t s = D.ctx->stream;
+  dist_true_residual<<<D.blocks_spmv, DT_THREADS, 0, s>>>(D.nloc, D.rp.p, D.ci.p, D.va.p, D.p.p, D.b.p, D.r.p, D.z.p,
+                                                          D.dinv.p, D.part.p, D.pc == 0);
+  TPT_CHECK_LAUNCH();
+  if (D.nloc)
+    TPT_CUDA(cudaMemcpyAsync(D.p.p, D.pbak.p, D.nloc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  if (D.nc) coarse_local_restrict(*D.sys, D.cl, D.r.p, D.yc.p, s);
+  out[0] = D.sum_parts(D.blocks_spmv, 2, 0);
+  out[1] = D.sum_parts(D.blocks_spmv, 2, 1);
+}
+
 // Several ranks on one device in lock step, the exchange done by device copies.
 int64_t dist_solve_local(tptfem_context* ctx, SystemData& S, int nranks, double tol, int64_t max_iter, double* u_red,
                          double* relres) {
@@ -524,29 +633,57 @@ int64_t dist_solve_local(tptfem_context* ctx, SystemData& S, int nranks, double 
   bb = rr;
   int64_t it = 0;
   const double target = tol * tol * bb;
-  while (rr > target && it < max_iter) {
+  double rr_upd = bb;  // true r.r at the last replacement
+  while (bb > 0.0) {
+    // iterate until the recursive residual has dropped by DIST_DELTA since the
+    // last replacement, or (a little below) the target; the iteration that
+    // gets there stops after the x, r update (no new direction)
+    const double until = std::max(0.25 * target, DIST_DELTA * DIST_DELTA * rr_upd);
+    while (it < max_iter) {
+      exchange();
+      double pq = 0.0;
+      for (auto& d : R) pq += dist_spmv_dot(*d);
+      TPT_REQUIRE(pq > 0.0, TPTFEM_ERR_BREAKDOWN, "PCG breakdown: p.Ap <= 0");
+      const double alpha = rz / pq;
+      double nrr = 0.0, nrz = 0.0;
+      for (auto& d : R) {
+        double o[2];
+        dist_update(*d, alpha, o);
+        nrr += o[0];
+        nrz += o[1];
+      }
+      ++it;
+      rr = nrr;
+      if (rr <= until) break;
+      const double beta = nrz / rz;
+      rz = nrz;
+      for (auto& d : R) dist_direction(*d, beta);
+    }
+    // reliable update: the true residual replaces the recursive one, and the
+    // direction continues from the last one with beta = r.z (true) / the r.z
+    // of the last step length
+    for (auto& d : R) dist_residual_begin(*d);
     exchange();
-    double pq = 0.0;
-    for (auto& d : R) pq += dist_spmv_dot(*d);
-    TPT_REQUIRE(pq > 0.0, TPTFEM_ERR_BREAKDOWN, "PCG breakdown: p.Ap <= 0");
-    const double alpha = rz / pq;
-    double nrr = 0.0, nrz = 0.0;
+    double trr = 0.0, trz = 0.0;
     for (auto& d : R) {
       double o[2];
-      dist_update(*d, alpha, o);
-      nrr += o[0];
-      nrz += o[1];
+      dist_residual_end(*d, o);
+      trr += o[0];
+      trz += o[1];
     }
-    const double beta = nrz / rz;
-    rr = nrr;
-    rz = nrz;
+    rr = trr;
+    if (rr <= target || it >= max_iter) break;
+    const double beta = trz / rz;
+    rz = trz;
+    rr_upd = rr;
     for (auto& d : R) dist_direction(*d, beta);
-    ++it;
   }
-  for (auto& d : R)
+  for (auto& d : R) {
+    dist_accumulate(*d);
     if (d->nloc) d->x.download(u_red + d->r0, d->nloc);
+  }
   TPT_CUDA(cudaStreamSynchronize(s));
-  *relres = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;  // recursive residual
+  *relres = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;  // true residual
   return it;
 }
 

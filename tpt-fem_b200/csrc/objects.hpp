@@ -287,7 +287,7 @@ struct DistData {
   int rank = 0, size = 1;
   int64_t r0 = 0, r1 = 0, nloc = 0, nghost = 0;
   DevBuf<int> rp, ci, send_idx;
-  DevBuf<double> va, dinv, b, x, r, z, p, q, send_buf, part;
+  DevBuf<double> va, dinv, b, x, xl, r, z, p, q, send_buf, part;  // x + xl: the solution
   std::vector<int64_t> send_off, recv_off;  // per peer rank: ranges in send_buf / in the ghost part of p
   std::vector<int> ghost_cols;              // global reduced index of every ghost column, ascending
   std::vector<double> hpart;
@@ -302,6 +302,7 @@ struct DistData {
   CoarseLocal cl;
   DevBuf<int> gcol;                      // local column -> global reduced index
   DevBuf<double> t, ac, yc, uc, cm;      // FSAI intermediate; partial / summed A_c; coarse vectors
+  DevBuf<double> pbak;                   // owned part of p while x takes its place (true residual)
   DevBuf<float> ainv;
   double sum_parts(int nb, int stride, int which);
 };
@@ -317,6 +318,9 @@ void dist_direction(DistData& D, double beta);
 int dist_set_precond(DistData& D, SystemData& S, int kind, int aggregates);
 void dist_coarse_factor(DistData& D);  // after the caller summed the partial A_c over ranks
 double dist_precondition(DistData& D);  // z = M r once the restriction is summed; local r.z
+void dist_accumulate(DistData& D);       // x += xl, xl = 0
+void dist_residual_begin(DistData& D);   // x in place of p's owned part, for the caller's exchange
+void dist_residual_end(DistData& D, double* out);  // r = b - A x; out as dist_update's
 int64_t dist_solve_local(tptfem_context* ctx, SystemData& S, int nranks, double tol, int64_t max_iter,
                          double* u_red, double* relres);
 // io_exodus.cu: write_exodus's NetCDF-3 classic bytes for a device-resident mesh

@@ -359,17 +359,6 @@ __global__ void jacobi_diag(int n, const int* __restrict__ rp, const int* __rest
   dinv[i] = (T)(1.0 / d);
 }
 
-// Error-free transformations (Knuth TwoSum; TwoProduct through FMA).
-__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
-  s = a + b;
-  const double bb = s - a;
-  e = (a - (s - bb)) + (b - bb);
-}
-__device__ __forceinline__ void two_prod(double a, double b, double& p, double& e) {
-  p = a * b;
-  e = __fma_rn(a, b, -p);
-}
-
 // FP64 true residual r = b - A x, computed with compensated (double-double)
 // accumulation so r is the residual of the FP64 vector x rounded once, not a
 // sum whose cancellation noise (eps * || |A||x| ||) can exceed the target;

@@ -122,6 +122,8 @@ SIGNATURES = {
     "tptfem_dist_coarse_buffers": (C.c_int, [_vp, _pp, _pp]),
     "tptfem_dist_coarse_factor": (C.c_int, [_vp, _vp]),
     "tptfem_dist_precondition": (C.c_int, [_vp, _vp, _vp]),
+    "tptfem_dist_residual_begin": (C.c_int, [_vp, _vp]),
+    "tptfem_dist_residual_end": (C.c_int, [_vp, _vp, _vp]),
     "tptfem_dist_solve_local": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_int64, _vp, _vp, _vp]),
     "tptfem_power_iteration": (C.c_int, [_vp, _vp, C.c_int, C.c_double, _vp, _vp, _vp]),
     "tptfem_assemble_poisson_robin": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,

@@ -137,6 +137,14 @@ class LibRank:
     def direction(self, beta):
         self.ctx.check(self.ctx.lib.tptfem_dist_direction(self.ctx.h, self.h, float(beta)))
 
+    def residual_begin(self):
+        self.ctx.check(self.ctx.lib.tptfem_dist_residual_begin(self.ctx.h, self.h))
+
+    def residual_end(self):
+        o = np.zeros(2)
+        self.ctx.check(self.ctx.lib.tptfem_dist_residual_end(self.ctx.h, self.h, N.ptr(o)))
+        return o
+
     def solution(self):
         x = np.zeros(self.n_owned)
         self.ctx.check(self.ctx.lib.tptfem_dist_solution(self.ctx.h, self.h, N.ptr(x)))
@@ -217,9 +225,15 @@ def prepare(ranks, comm):
             r.coarse_factor()
 
 
+DELTA = 1e-6  # reliable updates: the true residual replaces the recursive one after this drop
+
+
 def solve(ranks, comm, tol=1e-10, max_iter=100000):
-    """FP64 PCG over the partitioned system -> (iterations, recursive relative residual).
-    Jacobi, or the ranks' block preconditioner when set_precond was called."""
+    """FP64 PCG over the partitioned system -> (iterations, TRUE relative residual).
+    Jacobi, or the ranks' block preconditioner when set_precond was called.
+    As in the one-GPU solver, the true residual b - A x replaces the recursive
+    one whenever the latter has dropped by DELTA since the last replacement and
+    before the solve may stop (the search direction is kept)."""
     def total(vals):
         s = np.zeros_like(vals[0])
         for v in vals:  # local ranks in rank order
@@ -242,20 +256,42 @@ def solve(ranks, comm, tol=1e-10, max_iter=100000):
         for r in ranks:
             r.direction(0.0)
     bb, it = rr, 0
-    while rr > tol * tol * bb and it < max_iter:
+    target = tol * tol * bb
+    rr_upd = bb
+    while bb > 0:
+        # the iteration that reaches the replacement threshold stops after the
+        # x, r update; the direction then continues from the true residual
+        until = max(0.25 * target, DELTA * DELTA * rr_upd)
+        while it < max_iter:
+            for r in ranks:
+                r.pack()
+            comm.exchange(ranks)
+            pq = total([r.spmv_dot() for r in ranks])[0]
+            if not pq > 0.0:
+                raise ArithmeticError("PCG breakdown: p.Ap <= 0")
+            alpha = rz / pq
+            rr, rz_new = total([r.update(alpha) for r in ranks])
+            it += 1
+            if rr <= until:
+                break
+            if pc:
+                rz_new = precondition()
+            beta = rz_new / rz
+            rz = rz_new
+            for r in ranks:
+                r.direction(beta)
+        # reliable update: x's ghosts through the usual exchange, then r = b - A x
         for r in ranks:
+            r.residual_begin()
             r.pack()
         comm.exchange(ranks)
-        pq = total([r.spmv_dot() for r in ranks])[0]
-        if not pq > 0.0:
-            raise ArithmeticError("PCG breakdown: p.Ap <= 0")
-        alpha = rz / pq
-        rr, rz_new = total([r.update(alpha) for r in ranks])
+        rr, rz_t = total([r.residual_end() for r in ranks])
+        if rr <= target or it >= max_iter:
+            break
         if pc:
-            rz_new = precondition()
-        beta = rz_new / rz
-        rz = rz_new
+            rz_t = precondition()
+        beta = rz_t / rz
+        rz, rr_upd = rz_t, rr
         for r in ranks:
             r.direction(beta)
-        it += 1
     return it, float(np.sqrt(rr / bb)) if bb > 0 else 0.0
