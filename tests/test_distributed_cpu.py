@@ -2,8 +2,9 @@
 over torch.distributed with gloo, world size 2 and 3, on CPU: each process runs
 the numpy restatement of one library rank (oracle/dist_oracle.py), with Jacobi
 or with the block FSAI + coarse-space preconditioner (whose partial coarse
-matrices and restrictions the driver sums over the ranks); the gathered
-solution must equal a serial solve."""
+matrices and restrictions the driver sums over the ranks), and reliable
+updates (the true residual, exchanged like p, replaces the recursive one); the
+gathered solution must equal a serial solve."""
 import os
 import sys
 
@@ -118,6 +119,8 @@ def test_single_process_lockstep_equals_two_processes():
     it, rel = solve(ranks, LocalComm(), tol=1e-10)
     x = np.concatenate([r.solution() for r in ranks])
     assert rel <= 1e-10 and np.linalg.norm(A @ x - b) <= 1e-9 * np.linalg.norm(b)
+    # the residual the driver reports is the true one (the last reliable update)
+    assert abs(rel - np.linalg.norm(b - A @ x) / np.linalg.norm(b)) <= 1e-13
     # ghost receive counts mirror the peers' send counts
     for r in ranks:
         for qd in range(3):
