@@ -153,3 +153,8 @@ def test_partitioned_preconditioner_call_order_is_checked(ctx, cant):
         r.precondition()
     with pytest.raises(F.TptFemError, match="already set"):
         r.set_precond("fsai", 0)
+    # a solve that rebuilds the system's coarse space with another aggregate
+    # count leaves the rank's coarse data stale: refused, not read
+    S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=1e-8, fresh_setup=True, coarse=True, coarse_aggregates=3)
+    with pytest.raises(F.TptFemError, match="rebuilt"):
+        r.start()

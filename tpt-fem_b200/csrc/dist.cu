@@ -443,7 +443,17 @@ double dist_spmv_dot(DistData& D) {
   return D.sum_parts(D.blocks_spmv, 1, 0);
 }
 
+// The rank's coarse data index the whole system's aggregates: refuse to go on
+// if that geometry was rebuilt (another aggregate count) since the set-up.
+static void check_coarse(const DistData& D) {
+  if (!D.nc) return;
+  const CoarseSpace& C = D.sys->coarse;
+  TPT_REQUIRE(C.state == 1 && C.generation == D.cgen && C.nc == D.nc, TPTFEM_ERR_INVALID_ARG,
+              "the system's coarse space was rebuilt after tptfem_dist_set_precond");
+}
+
 void dist_update(DistData& D, double alpha, double* out) {
+  check_coarse(D);
   cudaStream_t s = D.ctx->stream;
   dist_update<<<D.blocks_vec, DT_THREADS, 0, s>>>(D.nloc, alpha, D.xl.p, D.r.p, D.z.p, D.p.p, D.q.p, D.dinv.p,
                                                   D.part.p, D.pc == 0);
@@ -521,6 +531,7 @@ int dist_set_precond(DistData& D, SystemData& S, int kind, int aggregates) {
     D.ainv.alloc((size_t)nc * D.ld, s);
     coarse_local_matrix(S, D.cl, D.nloc, D.rp.p, D.ci.p, D.va.p, D.gcol.p, D.ac.p);
     D.nc = nc;
+    D.cgen = S.coarse.generation;
   }
   TPT_CUDA(cudaStreamSynchronize(s));  // ac is ready for the caller's sum; host vectors are released
   return D.nc;
@@ -539,6 +550,7 @@ double dist_precondition(DistData& D) {
   TPT_REQUIRE(D.pc != 0, TPTFEM_ERR_INVALID_ARG, "no block preconditioner set (Jacobi forms z in the update)");
   TPT_REQUIRE(!D.nc || D.coarse_ready, TPTFEM_ERR_INVALID_ARG,
               "the coarse matrix is not factored: sum it over the ranks, then call tptfem_dist_coarse_factor");
+  check_coarse(D);
   cudaStream_t s = D.ctx->stream;
   const SystemData& S = *D.sys;
   if (D.nc) coarse_local_solve(S, D.ld, D.ainv.p, D.yc.p, D.uc.p, D.cm.p, s);
@@ -590,6 +602,7 @@ void dist_residual_begin(DistData& D) {
 // out as dist_update's (with a block preconditioner: the coarse restriction's
 // partial in yc); the search direction is restored.
 void dist_residual_end(DistData& D, double* out) {
+  check_coarse(D);
   cudaStream_t s = D.ctx->stream;
   dist_true_residual<<<D.blocks_spmv, DT_THREADS, 0, s>>>(D.nloc, D.rp.p, D.ci.p, D.va.p, D.p.p, D.b.p, D.r.p, D.z.p,
                                                           D.dinv.p, D.part.p, D.pc == 0);

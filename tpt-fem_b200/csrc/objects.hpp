@@ -298,6 +298,7 @@ struct DistData {
   std::unique_ptr<SystemData> blk;       // the owned diagonal block as a system of its own
   const FsaiFactor* fac = nullptr;       // its factor (owned by blk)
   int nc = 0, ld = 0;                    // coarse size (0: none) and row stride of ainv
+  int cgen = -1;                         // generation of the system's coarse geometry it was built on
   bool coarse_ready = false;
   CoarseLocal cl;
   DevBuf<int> gcol;                      // local column -> global reduced index
