@@ -357,6 +357,12 @@ tptfem_status tptfem_dist_residual_end(tptfem_context* ctx, tptfem_dist* d, doub
  * the partitioned path on one device. */
 tptfem_status tptfem_dist_solve_local(tptfem_context* ctx, tptfem_system* sys, int nranks, double rel_tol,
                                       int64_t max_iter, double* x, int64_t* iterations, double* relres);
+/* The same with the two-level preconditioner in partitioned form (kind and
+ * coarse_aggregates as tptfem_dist_set_precond): every rank's set-up, the
+ * partial coarse matrices and restrictions summed in rank order. */
+tptfem_status tptfem_dist_solve_local_precond(tptfem_context* ctx, tptfem_system* sys, int nranks, int kind,
+                                              int coarse_aggregates, double rel_tol, int64_t max_iter, double* x,
+                                              int64_t* iterations, double* relres);
 
 /* ---- eigenvalues (crates/tpt-fem-eigen/src/lib.rs) ---------------------------------- */
 enum { TPTFEM_EIG_SMALLEST = 0, TPTFEM_EIG_LARGEST = 1 };  /* EigWhich (eigen:122-129) */

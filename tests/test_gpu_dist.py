@@ -158,3 +158,14 @@ def test_partitioned_preconditioner_call_order_is_checked(ctx, cant):
     S.solve(solver=F.SOLVER_FSAI_MP_PCG, tol=1e-8, fresh_setup=True, coarse=True, coarse_aggregates=3)
     with pytest.raises(F.TptFemError, match="rebuilt"):
         r.start()
+
+
+def test_library_two_level_loop_equals_python_driver(ctx, cant):
+    S, A, fred, jac = cant
+    x, it, rel, nc = driver_solve(S, 3, "fsai", 0)
+    x2 = np.zeros(S.n_free)
+    it2, rel2 = C.c_int64(), C.c_double()
+    ctx.check(ctx.lib.tptfem_dist_solve_local_precond(ctx.h, S.h, 3, 1, 0, 1e-10, 0, N.ptr(x2), C.byref(it2),
+                                                      C.byref(rel2)))
+    assert nc > 0 and it2.value == it and abs(rel2.value - rel) <= 1e-15 and np.array_equal(x2, x)
+    assert rel2.value <= 1e-10 and np.linalg.norm(A @ x2 - fred) <= 2e-10 * np.linalg.norm(fred)

@@ -481,6 +481,19 @@ tptfem_status tptfem_dist_solve_local(tptfem_context* ctx, tptfem_system* sys, i
   API_CATCH(ctx)
 }
 
+tptfem_status tptfem_dist_solve_local_precond(tptfem_context* ctx, tptfem_system* sys, int nranks, int kind,
+                                              int coarse_aggregates, double rel_tol, int64_t max_iter, double* x,
+                                              int64_t* iterations, double* relres) {
+  if (!ctx || !sys || !sys->d || !x || !iterations || !relres) return TPTFEM_ERR_INVALID_ARG;
+  API_TRY
+  set_device(ctx);
+  TPT_REQUIRE(kind == TPTFEM_DIST_PC_FSAI || kind == TPTFEM_DIST_PC_LEARNED, TPTFEM_ERR_INVALID_ARG,
+              "kind must be TPTFEM_DIST_PC_FSAI or TPTFEM_DIST_PC_LEARNED");
+  *iterations = dist_solve_local(ctx, *sys->d, nranks, rel_tol > 0 ? rel_tol : 1e-10, max_iter > 0 ? max_iter : 100000,
+                                 x, relres, kind, coarse_aggregates);
+  API_CATCH(ctx)
+}
+
 void tptfem_mesh_free(tptfem_mesh* mesh) { delete mesh; }
 
 // ---- assembly -----------------------------------------------------------------

@@ -269,6 +269,11 @@ __global__ void dist_block_red_map(int64_t n, const int* __restrict__ red, int64
   out[j] = (v >= r0 && v < r1) ? (int)(v - r0) : -1;
 }
 
+__global__ void dist_add(int64_t n, const double* __restrict__ a, double* __restrict__ acc) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) acc[i] += a[i];
+}
+
 __global__ void dist_add_clear(int64_t nloc, double* __restrict__ xl, double* __restrict__ x) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nloc) {
@@ -616,7 +621,7 @@ void dist_residual_end(DistData& D, double* out) {
 
 // Several ranks on one device in lock step, the exchange done by device copies.
 int64_t dist_solve_local(tptfem_context* ctx, SystemData& S, int nranks, double tol, int64_t max_iter, double* u_red,
-                         double* relres) {
+                         double* relres, int kind, int aggregates) {
   TPT_REQUIRE(nranks >= 1, TPTFEM_ERR_INVALID_ARG, "nranks must be >= 1");
   const int64_t groups = S.n_free / std::max(1, S.dpn);
   std::vector<int64_t> starts(nranks + 1);
@@ -636,12 +641,46 @@ int64_t dist_solve_local(tptfem_context* ctx, SystemData& S, int nranks, double 
                                  cnt * sizeof(double), cudaMemcpyDeviceToDevice, s));
       }
   };
+  // block preconditioner: every rank's set-up, the partial coarse matrices
+  // summed in rank order into each rank's copy, each copy factored
+  int nc = 0;
+  DevBuf<double> csum;
+  auto sum_into_all = [&](auto get, size_t n) {
+    if (R.size() > 1) {
+      TPT_CUDA(cudaMemcpyAsync(csum.p, get(*R[0]), n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      for (size_t k = 1; k < R.size(); ++k) {
+        dist_add<<<ceil_div((int64_t)n, 256), 256, 0, s>>>((int64_t)n, get(*R[k]), csum.p);
+        TPT_CHECK_LAUNCH();
+      }
+      for (auto& d : R)
+        TPT_CUDA(cudaMemcpyAsync(get(*d), csum.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    TPT_CUDA(cudaStreamSynchronize(s));
+  };
+  if (kind) {
+    for (auto& d : R) nc = dist_set_precond(*d, S, kind, aggregates);
+    if (nc) {
+      csum.alloc((size_t)nc * nc, s);
+      sum_into_all([](DistData& d) { return d.ac.p; }, (size_t)nc * nc);
+      for (auto& d : R) dist_coarse_factor(*d);
+    }
+  }
+  auto precondition = [&]() {  // z = M r on every rank, the summed r.z
+    if (nc) sum_into_all([](DistData& d) { return d.yc.p; }, (size_t)nc);
+    double v = 0.0;
+    for (auto& d : R) v += dist_precondition(*d);
+    return v;
+  };
   double rr = 0.0, rz = 0.0, bb = 0.0;
   for (auto& d : R) {
     double o[2];
     dist_start(*d, o);
     rr += o[0];
     rz += o[1];
+  }
+  if (kind) {
+    rz = precondition();
+    for (auto& d : R) dist_direction(*d, 0.0);
   }
   bb = rr;
   int64_t it = 0;
@@ -668,6 +707,7 @@ int64_t dist_solve_local(tptfem_context* ctx, SystemData& S, int nranks, double 
       ++it;
       rr = nrr;
       if (rr <= until) break;
+      if (kind) nrz = precondition();
       const double beta = nrz / rz;
       rz = nrz;
       for (auto& d : R) dist_direction(*d, beta);
@@ -686,6 +726,7 @@ int64_t dist_solve_local(tptfem_context* ctx, SystemData& S, int nranks, double 
     }
     rr = trr;
     if (rr <= target || it >= max_iter) break;
+    if (kind) trz = precondition();
     const double beta = trz / rz;
     rz = trz;
     rr_upd = rr;

@@ -322,8 +322,9 @@ double dist_precondition(DistData& D);  // z = M r once the restriction is summe
 void dist_accumulate(DistData& D);       // x += xl, xl = 0
 void dist_residual_begin(DistData& D);   // x in place of p's owned part, for the caller's exchange
 void dist_residual_end(DistData& D, double* out);  // r = b - A x; out as dist_update's
+// kind 0: Jacobi; 1 / 2 with aggregates as dist_set_precond
 int64_t dist_solve_local(tptfem_context* ctx, SystemData& S, int nranks, double tol, int64_t max_iter,
-                         double* u_red, double* relres);
+                         double* u_red, double* relres, int kind = 0, int aggregates = -1);
 // io_exodus.cu: write_exodus's NetCDF-3 classic bytes for a device-resident mesh
 std::string exodus_bytes(const MeshData& m);
 void nb_build_sym(SystemData& S);  // after nb_build_operator succeeded

@@ -125,6 +125,8 @@ SIGNATURES = {
     "tptfem_dist_residual_begin": (C.c_int, [_vp, _vp]),
     "tptfem_dist_residual_end": (C.c_int, [_vp, _vp, _vp]),
     "tptfem_dist_solve_local": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_int64, _vp, _vp, _vp]),
+    "tptfem_dist_solve_local_precond": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int64, _vp,
+                                                  _vp, _vp]),
     "tptfem_power_iteration": (C.c_int, [_vp, _vp, C.c_int, C.c_double, _vp, _vp, _vp]),
     "tptfem_assemble_poisson_robin": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                                 _pp]),
