@@ -24,6 +24,12 @@
 // (an all-reduce of nc x nc values) and every rank factors the sum.  Each
 // iteration then adds one all-reduce of the nc restriction values P_k^T r_k:
 //   ... | x, r update, r.r, P_k^T r_k | sum r.r; sum P^T r | z = M r, r.z | sum | p = z + beta p
+//
+// Reliable updates, as in the one-GPU solver: the steps accumulate in xl,
+// apart from x, and whenever the recursive r.r has dropped by 1e-12 since the
+// last replacement (and before the solve may stop) x += xl and the true
+// residual b - A x, summed with compensation, replaces the recursive one; x's
+// ghost values travel through the same pack + exchange as p's.
 #include <algorithm>
 #include <cmath>
 #include <memory>
