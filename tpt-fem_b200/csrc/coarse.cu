@@ -657,6 +657,7 @@ bool coarse_build(SystemData& S, int target) {
   TPT_CUDA(cudaFuncSetAttribute(cs_gemv, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(CS_MAX_COARSE * sizeof(double))));
   C.Ac.alloc((size_t)C.nc * C.nc, s);
+  C.info.alloc(1, s);  // on the context's stream, which outlives the engines' second streams
   C.ld = (C.nc + 3) & ~3;
   C.Ainv.alloc((size_t)C.nc * C.ld, s);
   C.yc.alloc(C.nc, s);
@@ -726,7 +727,6 @@ bool coarse_assemble_async(SystemData& S, cudaStream_t s) {
             C.Ac.p, nc);
         TPT_CHECK_LAUNCH();
       }
-  if (!C.info.p) C.info.alloc(1, s);
   coarse_factor_async(S.ctx, s, nc, C.ld, C.Ac.p, C.Ainv.p, C.info.p);
   return true;
 }
