@@ -105,6 +105,15 @@ struct Engine {
   DevBuf<double> partials;
   DevBuf<PcgState> st;
   cudaGraphExec_t exec = nullptr;
+  // the graph of the other coarse setting (on / off), parked so that solves
+  // alternating between the two settings do not capture again
+  cudaGraphExec_t exec_alt = nullptr;
+  const SystemData* alt_csys = nullptr;
+  int alt_cgen = -1;
+  void drop_graphs() {
+    if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+    if (exec_alt) { cudaGraphExecDestroy(exec_alt); exec_alt = nullptr; }
+  }
   // node-block sliced-ELL operator / FSAI factor (FP64 engines only)
   const NbSell* nb = nullptr;
   bool nb_op = false, nb_pc = false, nb_sym = false;
@@ -118,6 +127,7 @@ struct Engine {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   ~Engine() {
     if (exec) cudaGraphExecDestroy(exec);
+    if (exec_alt) cudaGraphExecDestroy(exec_alt);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
     if (side) cudaStreamDestroy(side);
@@ -138,7 +148,7 @@ struct Engine {
     nb_pc = pcnb;
     nb_grid = std::max(1, std::min(sm_count() * NB_BLOCKS_PER_SM, ceil_div((int64_t)N->nchunks * 32, SPMV_THREADS)));
     if (partials.n < 2 * (size_t)nb_grid + 2) partials.alloc(2 * (size_t)nb_grid + 2, partials.s);
-    if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+    drop_graphs();
   }
 
   // q = A p with the pq reduction (K1).
@@ -320,7 +330,7 @@ void select_nb_mode(SystemData& S, Engine<double>& E, const tptfem_solver_opts& 
   S.nb.fresh_fill = false;
   if (E.nb_sym != sym) {
     E.nb_sym = sym;
-    if (E.exec) { cudaGraphExecDestroy(E.exec); E.exec = nullptr; }
+    E.drop_graphs();
   }
 }
 
@@ -344,6 +354,20 @@ int select_coarse(SystemData& S, Engine<double>& E, const tptfem_solver_opts& o,
   if (want && !S.coarse.ready) want = false;
   const SystemData* target = want ? &S : nullptr;
   if (E.csys != target || (want && E.cgen != S.coarse.generation)) {
+    // park the current graph; take the parked one if it was captured for the
+    // new setting (and, with the coarse space, for the same coarse geometry)
+    cudaGraphExec_t parked = E.exec;
+    const SystemData* parked_csys = E.csys;
+    const int parked_cgen = E.cgen;
+    E.exec = nullptr;
+    if (E.exec_alt && E.alt_csys == target && (!want || E.alt_cgen == S.coarse.generation)) {
+      E.exec = E.exec_alt;
+      E.exec_alt = nullptr;
+    }
+    if (E.exec_alt) cudaGraphExecDestroy(E.exec_alt);
+    E.exec_alt = parked;
+    E.alt_csys = parked_csys;
+    E.alt_cgen = parked_cgen;
     E.csys = target;
     E.cgen = S.coarse.generation;
     E.cargs = CoarseArgs{};
@@ -352,7 +376,6 @@ int select_coarse(SystemData& S, Engine<double>& E, const tptfem_solver_opts& o,
       E.cargs.y = S.coarse.y.p;
       E.cargs.cm = S.coarse.cm.p;
     }
-    if (E.exec) { cudaGraphExecDestroy(E.exec); E.exec = nullptr; }
   }
   return want ? S.coarse.nc : 0;
 }
@@ -490,7 +513,7 @@ void ensure_csr_fsai(SystemData& S, Engine<double>& E, FsaiFactor& F) {
   fsai_build_transpose(S, F);
   if (E.pc.gt_va != F.tva.p) {
     E.pc.gt_rp = F.trp.p; E.pc.gt_ci = F.tci.p; E.pc.gt_va = F.tva.p;
-    if (E.exec) { cudaGraphExecDestroy(E.exec); E.exec = nullptr; }
+    E.drop_graphs();
   }
 }
 
