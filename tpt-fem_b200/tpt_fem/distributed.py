@@ -6,7 +6,8 @@ values of p and sums the scalars and the coarse-space vectors.  The reference
 solves on one CPU thread; this path has no counterpart there.
 
     ranks = [LibRank(system, rank, size, partition_rows(...))]     # this process's GPU
-    ranks[0].set_precond("learned", coarse_aggregates=0)           # optional; Jacobi otherwise
+    for r in ranks:                                                # optional; Jacobi otherwise
+        r.set_precond("learned", coarse_aggregates=0)
     it, rel = solve(ranks, TorchComm(group))                       # NCCL across processes
 
 With a block preconditioner (block FSAI, classic or learned, plus the
