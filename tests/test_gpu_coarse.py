@@ -167,3 +167,24 @@ def test_overlapped_coarse_setup_repeats_bit_for_bit(ctx):
         runs.append((st["iterations"], S.solution()))
     for it, u in runs[1:]:
         assert it == runs[0][0] and np.array_equal(u, runs[0][1])
+
+
+def test_alternating_coarse_on_and_off_repeats_bit_for_bit(ctx):
+    # Solves that switch the coarse space on and off share one engine, which
+    # keeps the captured graph of the other setting: each setting must give
+    # the same iterations and solution bits every time it comes back.
+    import os
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    model = LF.LearnedFsai.load(ctx, os.path.join(root, "tpt-fem_b200", "weights", "lfsai_elasticity.bin"))
+    S, _ = cantilever(ctx, [40, 10, 10], seed=13)
+    model.attach(S)
+    seen = {}
+    for coarse in (True, False, True, False, True):
+        st = S.solve(solver=F.SOLVER_LEARNED_FSAI_PCG, tol=1e-10, fresh_setup=True, coarse=coarse)
+        assert st["rel_residual"] <= 1e-10 and not st["fell_back"] and (st["coarse_size"] > 0) == coarse
+        got = (st["iterations"], S.solution())
+        if coarse in seen:
+            assert got[0] == seen[coarse][0] and np.array_equal(got[1], seen[coarse][1])
+        else:
+            seen[coarse] = got
+    assert seen[True][0] < seen[False][0]
